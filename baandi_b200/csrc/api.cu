@@ -1,0 +1,721 @@
+// C ABI of libbaandi_b200.so: contexts, operators (tables in HBM, stick plan, FFT
+// plans, nonlocal operands) and the apply entry points.  See include/baandi_gpu.h.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "bg_internal.h"
+#include "hpsi.h"
+
+namespace bg {
+int configure_kernels(size_t plane_smem, size_t stick_smem);
+
+static thread_local std::string g_error;
+void set_global_error(const std::string& msg) { g_error = msg; }
+std::string global_error() { return g_error; }
+}  // namespace bg
+
+using namespace bg;
+
+struct bg_ctx {
+  int device = 0;
+  std::string error;
+  std::mutex mu;
+};
+
+namespace {
+
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  ~DevBuf() {
+    if (p) cudaFree(p);
+  }
+};
+
+}  // namespace
+
+struct bg_op {
+  bg_ctx* ctx = nullptr;
+  bool gamma = false;
+  int64_t rows = 0;
+  int64_t cap = 0;
+  int64_t cap_units = 0;
+  int dims[3] = {0, 0, 0};
+  bool has_epoch = false;
+  uint64_t epoch = 0;
+  int64_t launches = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  std::vector<double> diag;
+  OpTables t{};
+  BoxGeo g{};
+  NlTables nl{};
+  int ksplit_max = 1;
+  std::vector<std::unique_ptr<DevBuf>> bufs;
+  DevBuf* xs = nullptr;  // host-apply staging
+  DevBuf* ys = nullptr;
+  int* err_host = nullptr;  // pinned
+};
+
+namespace {
+
+int fail(bg_ctx* ctx, int code, const std::string& msg) {
+  if (ctx) {
+    ctx->error = msg;
+  } else {
+    set_global_error(msg);
+  }
+  return code;
+}
+
+int cuda_fail(bg_ctx* ctx, cudaError_t e, const char* what) {
+  return fail(ctx, BG_EDEVICE, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+template <class T>
+int upload(bg_op* op, const T* host, size_t count, T** out) {
+  auto b = std::make_unique<DevBuf>();
+  b->bytes = std::max<size_t>(count, 1) * sizeof(T);
+  cudaError_t e = cudaMalloc(&b->p, b->bytes);
+  if (e != cudaSuccess) return cuda_fail(op->ctx, e, "cudaMalloc");
+  if (count && host) {
+    e = cudaMemcpy(b->p, host, count * sizeof(T), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return cuda_fail(op->ctx, e, "cudaMemcpy");
+  }
+  *out = static_cast<T*>(b->p);
+  op->bufs.push_back(std::move(b));
+  return BG_OK;
+}
+
+int alloc(bg_op* op, size_t bytes, void** out, DevBuf** keep = nullptr) {
+  auto b = std::make_unique<DevBuf>();
+  b->bytes = std::max<size_t>(bytes, 16);
+  cudaError_t e = cudaMalloc(&b->p, b->bytes);
+  if (e != cudaSuccess) return fail(op->ctx, BG_ENOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+  *out = b->p;
+  if (keep) *keep = b.get();
+  op->bufs.push_back(std::move(b));
+  return BG_OK;
+}
+
+bool make_fft_plan(int n, FftPlan* p) {
+  if (n < 1 || n > 128) return false;
+  p->n = n;
+  p->nst = 0;
+  int m = n;
+  for (int r : {4, 2, 3, 5}) {
+    while (m % r == 0) {
+      if (p->nst == kMaxStages) return false;
+      p->radix[p->nst++] = r;
+      m /= r;
+    }
+  }
+  if (m != 1) return false;
+  for (int s = 0; s < p->nst; ++s)
+    if (n / p->radix[s] > 32 * kButterfliesPerLane) return false;
+  return true;
+}
+
+std::vector<double> twiddles(int n) {
+  std::vector<double> t(2 * n);
+  const long double two_pi = 6.283185307179586476925286766559005768L;
+  for (int q = 0; q < n; ++q) {
+    const long double a = two_pi * (long double)q / (long double)n;
+    t[2 * q] = (double)cosl(a);
+    t[2 * q + 1] = (double)sinl(a);
+  }
+  return t;
+}
+
+int ksplit_for(int64_t rows, int nproj, int64_t cols, int* kchunk) {
+  const int64_t tiles = ((nproj + 31) / 32) * ((cols + 31) / 32);
+  int64_t ks = std::max<int64_t>(1, (2 * 148 + tiles - 1) / tiles);
+  ks = std::min<int64_t>(ks, (rows + 31) / 32);
+  int64_t chunk = (rows + ks - 1) / ks;
+  chunk = ((chunk + 31) / 32) * 32;
+  ks = (rows + chunk - 1) / chunk;
+  *kchunk = (int)chunk;
+  return (int)ks;
+}
+
+// Build the stick plan, the tables and the nonlocal operands of one operator.
+int build_op(bg_ctx* ctx, const bg_basis_desc* b, const bg_projectors* pr, int64_t capacity, bool gamma,
+             bg_op** out) {
+  if (!ctx || !b || !out || !b->miller || !b->kinetic) return fail(ctx, BG_EINVAL, "null argument");
+  if (b->npw < 1 || capacity < 1 || capacity > 65535) return fail(ctx, BG_ESHAPE, "npw/capacity out of range");
+  for (int i = 0; i < 3; ++i)
+    if (b->dims[i] < 1) return fail(ctx, BG_ESHAPE, "grid dimensions");
+  const int64_t npw = b->npw;
+  for (int64_t g = 0; g < npw; ++g)
+    if (!std::isfinite(b->kinetic[g])) return fail(ctx, BG_ENONFINITE, "kinetic diagonal not finite");
+  int nproj = pr ? pr->nproj : 0;
+  if (nproj < 0 || (nproj > 0 && (!pr->table || !pr->channels || !pr->couplings)))
+    return fail(ctx, BG_EINVAL, "projector arguments");
+  cudaError_t ce = cudaSetDevice(ctx->device);
+  if (ce != cudaSuccess) return cuda_fail(ctx, ce, "cudaSetDevice");
+
+  auto op = std::make_unique<bg_op>();
+  op->ctx = ctx;
+  op->gamma = gamma;
+  op->rows = npw;
+  op->cap = capacity;
+  op->cap_units = gamma ? (capacity + 1) / 2 : capacity;
+  for (int i = 0; i < 3; ++i) op->dims[i] = b->dims[i];
+  const int n0 = b->dims[0], n1 = b->dims[1], n2 = b->dims[2];
+
+  // FFT index of every row
+  std::vector<int64_t> flat(npw);
+  const int dims[3] = {n0, n1, n2};
+  if (fft_index(b->miller, npw, dims, b->gamma != 0 || gamma, flat.data()) != BG_OK)
+    return fail(ctx, BG_ESHAPE, "Miller index outside the FFT grid or two rows on one grid point");
+
+  // Gamma mirror maps
+  std::vector<int64_t> plus, minus;
+  if (gamma) {
+    if (half_sphere(b->miller, npw, &plus, &minus) != BG_OK)
+      return fail(ctx, BG_ESHAPE, "basis is not an inversion-symmetric Gamma sphere with G=0 first");
+  }
+
+  // sticks: (x, y) lines along z; a stick and its mirror adjacent
+  std::map<int64_t, int> stick_id;  // x*n1+y -> provisional
+  for (int64_t g = 0; g < npw; ++g) stick_id[flat[g] / n2] = 0;
+  std::vector<int64_t> keys;
+  for (auto& kv : stick_id) keys.push_back(kv.first);
+  std::vector<char> used(keys.size(), 0);
+  std::map<int64_t, size_t> key_index;
+  for (size_t i = 0; i < keys.size(); ++i) key_index[keys[i]] = i;
+  std::vector<std::vector<int64_t>> units;  // groups of 1 or 2 sticks that must stay together
+  for (size_t i = 0; i < keys.size(); ++i) {
+    if (used[i]) continue;
+    used[i] = 1;
+    const int64_t x = keys[i] / n1, y = keys[i] % n1;
+    const int64_t mk = ((n0 - x) % n0) * n1 + (n1 - y) % n1;
+    auto it = key_index.find(mk);
+    if (it != key_index.end() && !used[it->second]) {
+      used[it->second] = 1;
+      units.push_back({keys[i], mk});
+    } else {
+      units.push_back({keys[i]});
+    }
+  }
+  const int sg = 32;
+  std::vector<int> grp_stick{0};
+  std::vector<int64_t> order;  // stick -> key
+  for (auto& u : units) {
+    const int cur = (int)order.size() - grp_stick.back();
+    if (cur + (int)u.size() > sg) grp_stick.push_back((int)order.size());
+    for (int64_t k : u) order.push_back(k);
+  }
+  grp_stick.push_back((int)order.size());
+  const int S = (int)order.size();
+  const int ngroups = (int)grp_stick.size() - 1;
+  std::vector<int> stick_of_key_group(S), group_of_stick(S);
+  std::map<int64_t, int> stick_of_key;
+  for (int s = 0; s < S; ++s) stick_of_key[order[s]] = s;
+  for (int gi = 0; gi < ngroups; ++gi)
+    for (int s = grp_stick[gi]; s < grp_stick[gi + 1]; ++s) group_of_stick[s] = gi;
+
+  BoxGeo& G = op->g;
+  G.n0 = n0;
+  G.n1 = n1;
+  G.n2 = n2;
+  G.ld2 = n2 | 1;
+  G.pitch = n1 | 1;
+  G.sg = sg;
+  G.inv_n = 1.0 / ((double)n0 * n1 * n2);
+  if (!make_fft_plan(n0, &G.p0) || !make_fft_plan(n1, &G.p1) || !make_fft_plan(n2, &G.p2))
+    return fail(ctx, BG_ESHAPE, "grid length must be 2,3,5-smooth and at most 128");
+
+  // position of every row in its group's shared-memory lines
+  auto pos_of = [&](int64_t g, int* group) {
+    const int s = stick_of_key[flat[g] / n2];
+    *group = group_of_stick[s];
+    return (s - grp_stick[*group]) * G.ld2 + (int)(flat[g] % n2);
+  };
+  std::vector<std::vector<std::pair<int, int>>> per_group(ngroups);
+  std::vector<int> code(npw, 0);
+  if (gamma) {
+    for (size_t i = 1; i < plus.size(); ++i) {
+      code[plus[i]] = (int)(2 * i - 1);
+      code[minus[i]] = -(int)(2 * i - 1);
+    }
+  }
+  for (int64_t g = 0; g < npw; ++g) {
+    int grp;
+    const int p = pos_of(g, &grp);
+    per_group[grp].push_back({gamma ? code[g] : (int)g, p});
+  }
+  std::vector<int> grp_entry{0};
+  std::vector<int> entries;
+  for (int gi = 0; gi < ngroups; ++gi) {
+    for (auto& e : per_group[gi]) {
+      entries.push_back(e.first);
+      entries.push_back(e.second);
+    }
+    grp_entry.push_back((int)(entries.size() / 2));
+  }
+  std::vector<int> grp_rep{0}, reps;
+  if (gamma) {
+    std::vector<std::vector<std::array<int, 4>>> rg(ngroups);
+    for (size_t i = 0; i < plus.size(); ++i) {
+      int ga, gb;
+      const int pp = pos_of(plus[i], &ga);
+      const int pm = pos_of(minus[i], &gb);
+      if (ga != gb) return fail(ctx, BG_ESHAPE, "internal: mirror split across stick groups");
+      rg[ga].push_back({i == 0 ? 0 : (int)(2 * i - 1), pp, pm, 0});
+    }
+    for (int gi = 0; gi < ngroups; ++gi) {
+      for (auto& r : rg[gi]) reps.insert(reps.end(), r.begin(), r.end());
+      grp_rep.push_back((int)(reps.size() / 4));
+    }
+  }
+  std::vector<int> stick_plane(S), xact;
+  {
+    std::vector<char> xs(n0, 0);
+    for (int s = 0; s < S; ++s) {
+      const int x = (int)(order[s] / n1), y = (int)(order[s] % n1);
+      stick_plane[s] = x * G.pitch + y;
+      xs[x] = 1;
+    }
+    for (int x = 0; x < n0; ++x)
+      if (xs[x]) xact.push_back(x);
+  }
+
+  // kinetic in row order (Gamma: ORC order, each pair row carries its representative's value)
+  std::vector<double> kin(npw);
+  if (gamma) {
+    kin[0] = b->kinetic[0];
+    for (size_t i = 1; i < plus.size(); ++i) kin[2 * i - 1] = kin[2 * i] = b->kinetic[plus[i]];
+  } else {
+    std::copy(b->kinetic, b->kinetic + npw, kin.begin());
+  }
+
+  OpTables& T = op->t;
+  T.gamma = gamma ? 1 : 0;
+  T.rows = (int)npw;
+  T.S = S;
+  T.ngroups = ngroups;
+  T.nxact = (int)xact.size();
+  int rc;
+  int* d_int;
+  if ((rc = upload(op.get(), grp_stick.data(), grp_stick.size(), &d_int))) return rc;
+  T.grp_stick = d_int;
+  if ((rc = upload(op.get(), grp_entry.data(), grp_entry.size(), &d_int))) return rc;
+  T.grp_entry = d_int;
+  if ((rc = upload(op.get(), entries.data(), entries.size(), &d_int))) return rc;
+  T.entries = reinterpret_cast<const int2*>(d_int);
+  if (gamma) {
+    if ((rc = upload(op.get(), grp_rep.data(), grp_rep.size(), &d_int))) return rc;
+    T.grp_rep = d_int;
+    if ((rc = upload(op.get(), reps.data(), reps.size(), &d_int))) return rc;
+    T.reps = reinterpret_cast<const int4*>(d_int);
+  }
+  if ((rc = upload(op.get(), stick_plane.data(), stick_plane.size(), &d_int))) return rc;
+  T.stick_plane = d_int;
+  if ((rc = upload(op.get(), xact.data(), xact.size(), &d_int))) return rc;
+  T.xact = d_int;
+  double* d_dbl;
+  if ((rc = upload(op.get(), kin.data(), kin.size(), &d_dbl))) return rc;
+  T.kinetic = d_dbl;
+  std::vector<double> nanv((size_t)n0 * n1 * n2, std::nan(""));
+  if ((rc = upload(op.get(), nanv.data(), nanv.size(), &d_dbl))) return rc;
+  T.vt = d_dbl;
+  void* vp;
+  if ((rc = alloc(op.get(), sizeof(double2) * (size_t)op->cap_units * n2 * S, &vp))) return rc;
+  T.sbuf = static_cast<double2*>(vp);
+  if ((rc = alloc(op.get(), sizeof(int) * 4, &vp))) return rc;
+  T.err = static_cast<int*>(vp);
+  cudaMemset(T.err, 0, sizeof(int) * 4);
+
+  for (int a = 0; a < 3; ++a) {
+    const int n = dims[a];
+    std::vector<double> tw = twiddles(n);
+    if ((rc = upload(op.get(), tw.data(), tw.size(), &d_dbl))) return rc;
+    const double2* p2 = reinterpret_cast<const double2*>(d_dbl);
+    if (a == 0) G.tw0 = p2;
+    if (a == 1) G.tw1 = p2;
+    if (a == 2) G.tw2 = p2;
+  }
+
+  // nonlocal operands and the static diagonal
+  NlTables& N = op->nl;
+  N.nproj = nproj;
+  op->diag.assign(npw, 0.0);
+  op->diag = kin;  // no projectors: the diagonal is the kinetic term
+  if (nproj > 0) {
+    const int natoms = pr->natoms;
+    std::vector<int> atom_off{0}, d_off;
+    int doff = 0, maxch = 0;
+    for (int a = 0; a < natoms; ++a) {
+      const int c = pr->channels[a];
+      if (c < 1 || c > 64) return fail(ctx, BG_ESHAPE, "channels per atom must be 1..64");
+      d_off.push_back(doff);
+      doff += c * c;
+      atom_off.push_back(atom_off.back() + c);
+      maxch = std::max(maxch, c);
+    }
+    if (atom_off.back() != nproj) return fail(ctx, BG_ESHAPE, "channel counts do not sum to nproj");
+    for (int i = 0; i < doff; ++i)
+      if (!std::isfinite(pr->couplings[i])) return fail(ctx, BG_ENONFINITE, "coupling not finite");
+    const std::complex<double>* P = reinterpret_cast<const std::complex<double>*>(pr->table);
+    for (int64_t i = 0; i < npw * nproj; ++i)
+      if (!std::isfinite(P[i].real()) || !std::isfinite(P[i].imag()))
+        return fail(ctx, BG_ENONFINITE, "projector table not finite");
+    // static diagonal (complex: distributed_complex.rs:29-53; Gamma: refstart.rs:605-650)
+    std::vector<double> dfull(npw);
+    for (int64_t g = 0; g < npw; ++g) dfull[g] = b->kinetic[g];
+    for (int a = 0, off = 0; a < natoms; ++a) {
+      const int c = pr->channels[a];
+      const double* D = pr->couplings + d_off[a];
+      for (int i = 0; i < c; ++i)
+        for (int j = 0; j < c; ++j) {
+          const double d = D[i * c + j];
+          if (d == 0.0) continue;
+          const std::complex<double>* pi = P + (size_t)(off + i) * npw;
+          const std::complex<double>* pj = P + (size_t)(off + j) * npw;
+          for (int64_t g = 0; g < npw; ++g) dfull[g] += (d * pi[g] * std::conj(pj[g])).real();
+        }
+      off += c;
+    }
+    if (gamma) {
+      op->diag[0] = dfull[0];
+      for (size_t i = 1; i < plus.size(); ++i) op->diag[2 * i - 1] = op->diag[2 * i] = dfull[plus[i]];
+      // ORC projector rows (distributed_real_gamma.rs:358-398)
+      std::vector<double> porc((size_t)npw * nproj);
+      const double r2 = std::sqrt(2.0);
+      for (int p = 0; p < nproj; ++p) {
+        const std::complex<double>* col = P + (size_t)p * npw;
+        double* o = porc.data() + (size_t)p * npw;
+        o[0] = col[0].real();
+        for (size_t i = 1; i < plus.size(); ++i) {
+          o[2 * i - 1] = r2 * col[plus[i]].real();
+          o[2 * i] = r2 * col[plus[i]].imag();
+        }
+      }
+      if ((rc = upload(op.get(), porc.data(), porc.size(), &d_dbl))) return rc;
+    } else {
+      op->diag = dfull;
+      if ((rc = upload(op.get(), pr->table, (size_t)2 * npw * nproj, &d_dbl))) return rc;
+    }
+    N.p = d_dbl;
+    N.natoms = natoms;
+    N.maxch = maxch;
+    if ((rc = upload(op.get(), atom_off.data(), atom_off.size(), &d_int))) return rc;
+    N.atom_off = d_int;
+    if ((rc = upload(op.get(), d_off.data(), d_off.size(), &d_int))) return rc;
+    N.d_off = d_int;
+    if ((rc = upload(op.get(), pr->couplings, (size_t)doff, &d_dbl))) return rc;
+    N.d = d_dbl;
+    int64_t maxpart = 0;
+    for (int64_t c = 1; c <= capacity; ++c) {
+      int kc;
+      const int ks = ksplit_for(npw, nproj, c, &kc);
+      maxpart = std::max<int64_t>(maxpart, (int64_t)ks * c);
+    }
+    const size_t es = gamma ? sizeof(double) : sizeof(double2);
+    if ((rc = alloc(op.get(), es * (size_t)maxpart * nproj, &vp))) return rc;
+    N.part = static_cast<double*>(vp);
+    if ((rc = alloc(op.get(), es * (size_t)capacity * nproj, &vp))) return rc;
+    N.wd = static_cast<double*>(vp);
+  }
+  for (double v : op->diag)
+    if (!std::isfinite(v)) return fail(ctx, BG_ENONFINITE, "nonfinite diagonal");
+
+  const size_t es = gamma ? sizeof(double) : sizeof(double2);
+  if ((rc = alloc(op.get(), es * (size_t)npw * capacity, &vp, &op->xs))) return rc;
+  if ((rc = alloc(op.get(), es * (size_t)npw * capacity, &vp, &op->ys))) return rc;
+  if ((ce = cudaMallocHost(&op->err_host, sizeof(int) * 4)) != cudaSuccess) return cuda_fail(ctx, ce, "cudaMallocHost");
+  if ((ce = cudaStreamCreateWithFlags(&op->stream, cudaStreamNonBlocking)) != cudaSuccess)
+    return cuda_fail(ctx, ce, "cudaStreamCreate");
+  op->own_stream = true;
+  const size_t ps = plane_smem_bytes(G), ss = stick_smem_bytes(G);
+  int dev_smem = 0;
+  cudaDeviceGetAttribute(&dev_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device);
+  if (ps > (size_t)dev_smem || ss > (size_t)dev_smem)
+    return fail(ctx, BG_ESHAPE, "FFT plane does not fit in shared memory");
+  if ((rc = configure_kernels((size_t)dev_smem, (size_t)dev_smem)) != BG_OK)
+    return fail(ctx, BG_EDEVICE, "cudaFuncSetAttribute failed");
+  if ((ce = cudaDeviceSynchronize()) != cudaSuccess) return cuda_fail(ctx, ce, "setup");
+  *out = op.release();
+  return BG_OK;
+}
+
+int check_err(bg_op* op) {
+  cudaError_t e = cudaMemcpyAsync(op->err_host, op->t.err, sizeof(int), cudaMemcpyDeviceToHost, op->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(op->stream);
+  if (e != cudaSuccess) return cuda_fail(op->ctx, e, "apply");
+  if (op->err_host[0]) {
+    cudaMemsetAsync(op->t.err, 0, sizeof(int), op->stream);
+    cudaStreamSynchronize(op->stream);
+    return fail(op->ctx, BG_ENONFINITE, "non-finite input coefficient");
+  }
+  return BG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int bg_ctx_create(const bg_device_opts* opts, bg_ctx** out) {
+  if (!out) return fail(nullptr, BG_EINVAL, "null output");
+  int count = 0;
+  cudaError_t e = cudaGetDeviceCount(&count);
+  if (e != cudaSuccess || count == 0) return fail(nullptr, BG_EDEVICE, "no CUDA device available");
+  const int dev = opts ? opts->device : 0;
+  if (dev < 0 || dev >= count) return fail(nullptr, BG_EINVAL, "device ordinal out of range");
+  cudaDeviceProp prop;
+  if ((e = cudaGetDeviceProperties(&prop, dev)) != cudaSuccess) return cuda_fail(nullptr, e, "cudaGetDeviceProperties");
+  if (prop.major != 10) return fail(nullptr, BG_EDEVICE, "libbaandi_b200 is built for sm_100a (B200)");
+  auto* c = new bg_ctx();
+  c->device = dev;
+  *out = c;
+  return BG_OK;
+}
+
+int bg_ctx_destroy(bg_ctx* ctx) {
+  delete ctx;
+  return BG_OK;
+}
+
+int bg_last_error(const bg_ctx* ctx, char* buf, size_t len) {
+  if (!buf || len == 0) return BG_EINVAL;
+  const std::string msg = ctx ? ctx->error : global_error();
+  std::snprintf(buf, len, "%s", msg.c_str());
+  return BG_OK;
+}
+
+int bg_op_create_complex(bg_ctx* ctx, const bg_basis_desc* basis, const bg_projectors* proj, int64_t capacity,
+                         bg_op** out) {
+  return build_op(ctx, basis, proj, capacity, false, out);
+}
+
+int bg_op_create_gamma_real(bg_ctx* ctx, const bg_basis_desc* basis, const bg_projectors* proj, int64_t capacity,
+                            bg_op** out) {
+  return build_op(ctx, basis, proj, capacity, true, out);
+}
+
+int bg_op_destroy(bg_op* op) {
+  if (!op) return BG_OK;
+  if (op->stream) cudaStreamSynchronize(op->stream);
+  if (op->own_stream && op->stream) cudaStreamDestroy(op->stream);
+  if (op->err_host) cudaFreeHost(op->err_host);
+  delete op;
+  return BG_OK;
+}
+
+int bg_op_set_potential(bg_op* op, const double* v, uint64_t epoch) {
+  if (!op || !v) return fail(op ? op->ctx : nullptr, BG_EINVAL, "null argument");
+  if (op->has_epoch && epoch <= op->epoch) return fail(op->ctx, BG_EEPOCH, "potential epoch must increase");
+  const int n0 = op->dims[0], n1 = op->dims[1], n2 = op->dims[2];
+  const size_t N = (size_t)n0 * n1 * n2;
+  std::vector<double> vt(N);
+  for (int x = 0; x < n0; ++x)
+    for (int y = 0; y < n1; ++y)
+      for (int z = 0; z < n2; ++z) {
+        const double w = v[((size_t)x * n1 + y) * n2 + z];
+        if (!std::isfinite(w)) return fail(op->ctx, BG_ENONFINITE, "potential not finite");
+        vt[((size_t)z * n0 + x) * n1 + y] = w;
+      }
+  cudaError_t e = cudaMemcpyAsync(const_cast<double*>(op->t.vt), vt.data(), N * sizeof(double),
+                                  cudaMemcpyHostToDevice, op->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(op->stream);
+  if (e != cudaSuccess) return cuda_fail(op->ctx, e, "set_potential");
+  op->epoch = epoch;
+  op->has_epoch = true;
+  return BG_OK;
+}
+
+int bg_op_apply_block(bg_op* op, const double* x, double* y, int64_t rows, int64_t cols, int32_t ptr_kind,
+                      int32_t precision) {
+  if (!op) return fail(nullptr, BG_EINVAL, "null operator");
+  bg_ctx* ctx = op->ctx;
+  if (precision != BG_PREC_FP64) return fail(ctx, BG_EINVAL, "unsupported precision");
+  if (ptr_kind != BG_PTR_HOST && ptr_kind != BG_PTR_DEVICE) return fail(ctx, BG_EINVAL, "pointer kind");
+  if (!op->has_epoch) return fail(ctx, BG_EEPOCH, "potential was never set");
+  if (rows != op->rows || cols < 0 || cols > op->cap) return fail(ctx, BG_ESHAPE, "block shape");
+  if (cols == 0) return BG_OK;
+  if (!x || !y || x == y) return fail(ctx, BG_EINVAL, "x and y must be distinct non-null buffers");
+  const size_t dpc = op->gamma ? (size_t)rows : (size_t)2 * rows;  // doubles per column
+  cudaError_t e = cudaSetDevice(ctx->device);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaSetDevice");
+  const double* dx = x;
+  double* dy = y;
+  if (ptr_kind == BG_PTR_HOST) {
+    for (size_t i = 0; i < dpc * cols; ++i)
+      if (!std::isfinite(x[i])) return fail(ctx, BG_ENONFINITE, "non-finite input coefficient");
+    dx = static_cast<const double*>(op->xs->p);
+    dy = static_cast<double*>(op->ys->p);
+    e = cudaMemcpyAsync(const_cast<double*>(dx), x, dpc * cols * sizeof(double), cudaMemcpyHostToDevice, op->stream);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "copy in");
+  }
+  CallArgs a;
+  a.x = dx;
+  a.y = dy;
+  a.ldx = (int64_t)dpc;
+  a.ldy = (int64_t)dpc;
+  a.cols = (int)cols;
+  a.units = op->gamma ? (int)((cols + 1) / 2) : (int)cols;
+  op->launches += launch_local(op->t, op->g, a, op->stream);
+  if (op->nl.nproj > 0) {
+    int kc;
+    op->nl.ksplit = ksplit_for(op->rows, op->nl.nproj, cols, &kc);
+    op->nl.kchunk = kc;
+    op->launches += launch_nonlocal(op->t, op->nl, a, op->stream);
+  }
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "kernel launch");
+  if (ptr_kind == BG_PTR_HOST) {
+    e = cudaMemcpyAsync(y, dy, dpc * cols * sizeof(double), cudaMemcpyDeviceToHost, op->stream);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "copy out");
+    return check_err(op);
+  }
+  return BG_OK;
+}
+
+int bg_op_sync(bg_op* op) {
+  if (!op) return fail(nullptr, BG_EINVAL, "null operator");
+  return check_err(op);
+}
+
+int bg_op_diagonal(const bg_op* op, double* out) {
+  if (!op || !out) return fail(op ? op->ctx : nullptr, BG_EINVAL, "null argument");
+  std::copy(op->diag.begin(), op->diag.end(), out);
+  return BG_OK;
+}
+
+int bg_op_rows(const bg_op* op, int64_t* rows) {
+  if (!op || !rows) return BG_EINVAL;
+  *rows = op->rows;
+  return BG_OK;
+}
+
+int bg_op_capacity(const bg_op* op, int64_t* capacity) {
+  if (!op || !capacity) return BG_EINVAL;
+  *capacity = op->cap;
+  return BG_OK;
+}
+
+int bg_op_stream(const bg_op* op, void** stream) {
+  if (!op || !stream) return BG_EINVAL;
+  *stream = op->stream;
+  return BG_OK;
+}
+
+int bg_op_set_stream(bg_op* op, void* stream) {
+  if (!op) return BG_EINVAL;
+  if (op->own_stream && op->stream) {
+    cudaStreamSynchronize(op->stream);
+    cudaStreamDestroy(op->stream);
+  }
+  op->own_stream = false;
+  op->stream = static_cast<cudaStream_t>(stream);
+  return BG_OK;
+}
+
+int bg_op_launches(const bg_op* op, int64_t* launches) {
+  if (!op || !launches) return BG_EINVAL;
+  *launches = op->launches;
+  return BG_OK;
+}
+
+// ------------------------------------------------------------------ setup ABI
+int bg_setup_volume(const double rows[9], double* volume) {
+  if (!rows || !volume) return fail(nullptr, BG_EINVAL, "null argument");
+  Cell c;
+  int rc = cell_init(rows, &c);
+  if (rc) return fail(nullptr, rc, "singular or non-finite lattice");
+  *volume = c.volume;
+  return BG_OK;
+}
+
+int bg_setup_basis(const double rows[9], double ecut, const double kfrac[3], int64_t capacity, int64_t* npw,
+                   int32_t* miller, double* kpg, double* kpg2) {
+  if (!rows || !kfrac || !npw) return fail(nullptr, BG_EINVAL, "null argument");
+  Cell c;
+  int rc = cell_init(rows, &c);
+  if (rc) return fail(nullptr, rc, "singular or non-finite lattice");
+  Basis b;
+  if ((rc = basis_build(c, ecut, kfrac, &b))) return fail(nullptr, rc, "invalid cutoff");
+  *npw = b.npw;
+  if (capacity == 0) return BG_OK;
+  if (capacity < b.npw || !miller || !kpg || !kpg2) return fail(nullptr, BG_ESHAPE, "output capacity too small");
+  std::copy(b.miller.begin(), b.miller.end(), miller);
+  std::copy(b.kpg.begin(), b.kpg.end(), kpg);
+  std::copy(b.kpg2.begin(), b.kpg2.end(), kpg2);
+  return BG_OK;
+}
+
+int bg_setup_grid(const double rows[9], double ecut, int32_t dims[3], int32_t required[3]) {
+  if (!rows || !dims || !required) return fail(nullptr, BG_EINVAL, "null argument");
+  Cell c;
+  int rc = cell_init(rows, &c);
+  if (rc) return fail(nullptr, rc, "singular or non-finite lattice");
+  int d[3], r[3];
+  if ((rc = grid_dims(c, ecut, d, r))) return fail(nullptr, rc, "invalid cutoff");
+  for (int i = 0; i < 3; ++i) {
+    dims[i] = d[i];
+    required[i] = r[i];
+  }
+  return BG_OK;
+}
+
+int bg_setup_half_sphere(const int32_t* miller, int64_t npw, int64_t* plus, int64_t* minus) {
+  if (!miller || !plus || !minus) return fail(nullptr, BG_EINVAL, "null argument");
+  std::vector<int64_t> p, m;
+  if (half_sphere(miller, npw, &p, &m)) return fail(nullptr, BG_ESHAPE, "not an inversion-symmetric Gamma sphere");
+  std::copy(p.begin(), p.end(), plus);
+  std::copy(m.begin(), m.end(), minus);
+  return BG_OK;
+}
+
+static std::vector<Species> to_species(int32_t n, const bg_species* s) {
+  std::vector<Species> out(n);
+  for (int i = 0; i < n; ++i)
+    out[i] = Species{s[i].z_valence, s[i].mesh,  s[i].r,    s[i].rab, s[i].local,  s[i].nbeta,
+                     s[i].l,         s[i].beta_len, s[i].beta, s[i].dij, s[i].natoms, s[i].positions};
+  return out;
+}
+
+int bg_setup_projector_count(int32_t nspecies, const bg_species* species, int32_t* nproj, int32_t* natoms) {
+  if (nspecies < 0 || (nspecies > 0 && !species) || !nproj || !natoms) return fail(nullptr, BG_EINVAL, "argument");
+  auto sp = to_species(nspecies, species);
+  int np, na;
+  int rc = projector_count(nspecies, sp.data(), &np, &na);
+  if (rc) return fail(nullptr, rc, "projector angular momentum must be 0..3");
+  *nproj = np;
+  *natoms = na;
+  return BG_OK;
+}
+
+int bg_setup_projectors(double volume, int64_t npw, const double* kpg, const double* kpg2, int32_t nspecies,
+                        const bg_species* species, double* table, int32_t* channels, double* couplings) {
+  if (!kpg || !kpg2 || (nspecies > 0 && !species) || !table || !channels || !couplings)
+    return fail(nullptr, BG_EINVAL, "null argument");
+  auto sp = to_species(nspecies, species);
+  for (auto& s : sp)
+    for (int i = 0; i < s.nbeta; ++i)
+      if (s.ulen[i] < 1 || s.ulen[i] > s.mesh) return fail(nullptr, BG_ESHAPE, "projector samples exceed the mesh");
+  int rc = projectors_build(volume, npw, kpg, kpg2, nspecies, sp.data(),
+                            reinterpret_cast<std::complex<double>*>(table), channels, couplings);
+  if (rc) return fail(nullptr, rc, "projector table");
+  return BG_OK;
+}
+
+int bg_setup_local_form_factor(const bg_species* species, double volume, int64_t n, const double* g, double* out) {
+  if (!species || !g || !out || !(volume > 0.0)) return fail(nullptr, BG_EINVAL, "argument");
+  auto sp = to_species(1, species);
+  int rc = local_form_factor(sp[0], volume, n, g, out);
+  if (rc) return fail(nullptr, rc, "local form factor");
+  return BG_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,81 @@
+// Device-side layout of one Hamiltonian operator (one k point) and the launchers of
+// the H.x pipeline.  Shared by the CUDA kernels and the host runtime.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+
+#include "fft_dev.cuh"
+
+namespace bg {
+
+// Immutable per-operator tables, resident in HBM.  The FFT box is n0 x n1 x n2
+// (C order, z fastest).  Plane waves sit on S "sticks" (lines along z at fixed x, y);
+// sticks are numbered so that a stick and its mirror (-x, -y) are adjacent and fall
+// in the same group of at most `sg` sticks.
+struct OpTables {
+  int gamma;      // 1: real ORC rows, two columns per complex FFT
+  int rows;       // npw (complex) or n ORC rows (Gamma)
+  int S;          // sticks
+  int ngroups;    // stick groups
+  int nxact;      // x rows of the plane holding at least one stick
+  const int* grp_stick;   // ngroups+1: first stick of each group
+  const int* grp_entry;   // ngroups+1: entry range of each group
+  const int2* entries;    // complex: (row g, pos); Gamma: (code, pos), code 0 for G=0,
+                          // +(2i-1) at plus[i], -(2i-1) at minus[i]; pos = local stick * ld2 + z
+  const int* grp_rep;     // Gamma: ngroups+1 representative range of each group
+  const int4* reps;       // Gamma: (ORC row 2i-1 or 0, pos of plus, pos of minus, 0)
+  const int* stick_plane; // S: x * pitch + y, offset inside the shared-memory plane
+  const int* xact;        // nxact x rows
+  const double* kinetic;  // rows
+  const double* vt;       // V(r) transposed to [z][x][y]
+  double2* sbuf;          // stick buffer [unit][z][S]
+  int* err;               // device error word (bit 0: non-finite input)
+};
+
+// Shape of the FFT box shared by every operator of one launch.
+struct BoxGeo {
+  int n0, n1, n2;
+  int ld2;     // stride of a z line in the stick kernels' shared memory (odd)
+  int pitch;   // row pitch of the shared-memory plane (odd)
+  int sg;      // max sticks per group
+  double inv_n;
+  FftPlan p0, p1, p2;
+  const double2* tw0;  // exp(+2 pi i q/n0), q < n0
+  const double2* tw1;
+  const double2* tw2;
+};
+
+// Per-call arguments of one operator.
+struct CallArgs {
+  const double* x;  // complex: interleaved; Gamma: real ORC
+  double* y;
+  int64_t ldx, ldy; // column strides in doubles
+  int cols;         // complex columns or real ORC columns
+  int units;        // complex columns or column pairs
+};
+
+// Nonlocal operands of one operator.
+struct NlTables {
+  int nproj;
+  int natoms;
+  int maxch;
+  const double* p;        // complex: 2*npw*nproj interleaved col-major; Gamma: real ORC n*nproj
+  const int* atom_off;    // natoms+1 projector column offsets
+  const int* d_off;       // natoms coupling offsets
+  const double* d;        // concatenated row-major D blocks
+  double* part;           // split-K partials [ks][col][nproj] (complex: x2)
+  double* wd;             // coupled projections [col][nproj] (complex: x2)
+  int ksplit;
+  int kchunk;
+};
+
+// Enqueue the local + kinetic part: y = gather(FFT(V IFFT(scatter x)))/N + T x.
+// Returns the number of kernel launches.
+int launch_local(const OpTables& t, const BoxGeo& g, const CallArgs& a, cudaStream_t s);
+// Enqueue y += P (D (P^H x)) (complex) or y += P (D (P^T x)) (Gamma).
+int launch_nonlocal(const OpTables& t, const NlTables& nl, const CallArgs& a, cudaStream_t s);
+
+size_t plane_smem_bytes(const BoxGeo& g);
+size_t stick_smem_bytes(const BoxGeo& g);
+
+}  // namespace bg

@@ -1,0 +1,398 @@
+// sm_100a kernels of the Hamiltonian apply H.x (FP64).
+//
+// Local part, three passes over a stick buffer in HBM (layout [unit][z][stick]):
+//   k_sticks_inverse  scatter the sphere coefficients of one stick group into zeroed
+//                     z lines in shared memory (Gamma: pack two ORC columns into one
+//                     complex vector), inverse FFT along z, store [z][stick].
+//   k_planes          one (unit, z) plane in shared memory: inverse FFT along y on
+//                     the x rows holding sticks, along x on every column, times V(r),
+//                     forward x, forward y, store the stick values back.
+//   k_sticks_forward  forward FFT along z, x 1/N, gather to the sphere and add the
+//                     kinetic term (Gamma: unpack the pair into two ORC columns).
+// Nonlocal part, y += P (D (P^H x)):
+//   k_project         split-K partial products of P^H X (P^T X on Gamma ORC rows)
+//   k_couple          ordered sum of the partials and the per-atom D blocks
+//   k_back            y += P W
+//
+// Reference (paths inside the reference project): crates/dft-solvers/src/
+// distributed_fft.rs:837-1130, 1198-1288 (scatter, pruned transforms, x V, 1/N,
+// gather); crates/dft-physics/src/distributed_complex.rs:340-386 (complex apply);
+// crates/dft-physics/src/distributed_real_gamma.rs:654-689 (pair pack), :1307-1347
+// (unpack + kinetic), :957-1017, 1184-1248 (nonlocal).
+#include "hpsi.h"
+
+namespace bg {
+
+namespace {
+
+constexpr double kSqrt2 = 1.4142135623730951;
+constexpr double kInvSqrt2 = 0.7071067811865476;
+
+struct LineOffStride {
+  int stride;
+  __device__ __forceinline__ int operator()(int l) const { return l * stride; }
+};
+struct LineOffRows {
+  const int* rows;
+  int pitch;
+  __device__ __forceinline__ int operator()(int l) const { return rows[l] * pitch; }
+};
+struct LineOffCols {
+  __device__ __forceinline__ int operator()(int l) const { return l; }
+};
+
+__device__ __forceinline__ bool finite2(double a, double b) { return isfinite(a) && isfinite(b); }
+
+// ---------------------------------------------------------------- pass 1
+template <bool GAMMA>
+__global__ void __launch_bounds__(256) k_sticks_inverse(OpTables t, BoxGeo g, CallArgs a) {
+  const int grp = blockIdx.x, unit = blockIdx.y;
+  if (grp >= t.ngroups || unit >= a.units) return;
+  extern __shared__ double2 sm[];
+  double2* tw = sm;
+  double2* st = sm + g.n2;
+  const int s0 = t.grp_stick[grp], cnt = t.grp_stick[grp + 1] - s0;
+  for (int i = threadIdx.x; i < g.n2; i += blockDim.x) tw[i] = g.tw2[i];
+  for (int i = threadIdx.x; i < cnt * g.ld2; i += blockDim.x) st[i] = make_double2(0.0, 0.0);
+  __syncthreads();
+  const int e0 = t.grp_entry[grp], e1 = t.grp_entry[grp + 1];
+  bool bad = false;
+  if (!GAMMA) {
+    const double2* x = reinterpret_cast<const double2*>(a.x + (int64_t)unit * a.ldx);
+    for (int e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
+      const int2 en = t.entries[e];
+      const double2 v = x[en.x];
+      bad |= !finite2(v.x, v.y);
+      st[en.y] = v;
+    }
+  } else {
+    const int ca = 2 * unit;
+    const bool hasb = ca + 1 < a.cols;
+    const double* xa = a.x + (int64_t)ca * a.ldx;
+    const double* xb = a.x + (int64_t)(hasb ? ca + 1 : ca) * a.ldx;
+    for (int e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
+      const int2 en = t.entries[e];
+      const int code = en.x;
+      double2 v;
+      if (code == 0) {
+        v = make_double2(xa[0], hasb ? xb[0] : 0.0);
+      } else {
+        const int r = code > 0 ? code : -code;
+        const double2 pa = make_double2(xa[r] * kInvSqrt2, xa[r + 1] * kInvSqrt2);
+        const double2 pb = hasb ? make_double2(xb[r] * kInvSqrt2, xb[r + 1] * kInvSqrt2) : make_double2(0.0, 0.0);
+        // plus: a + i b ; minus: conj(a) + i conj(b)
+        v = code > 0 ? make_double2(pa.x - pb.y, pa.y + pb.x) : make_double2(pa.x + pb.y, -pa.y + pb.x);
+      }
+      bad |= !finite2(v.x, v.y);
+      st[en.y] = v;
+    }
+  }
+  if (bad) atomicOr(t.err, 1);
+  fft_lines<1>(st, cnt, LineOffStride{g.ld2}, 1, g.p2, tw);
+  double2* out = t.sbuf + (int64_t)unit * g.n2 * t.S + s0;
+  for (int i = threadIdx.x; i < cnt * g.n2; i += blockDim.x) {
+    const int z = i / cnt, sl = i - z * cnt;
+    out[(int64_t)z * t.S + sl] = st[sl * g.ld2 + z];
+  }
+}
+
+// ---------------------------------------------------------------- pass 2
+__global__ void __launch_bounds__(512) k_planes(OpTables t, BoxGeo g, CallArgs a) {
+  const int unit = blockIdx.x, z = blockIdx.y;
+  if (unit >= a.units) return;
+  extern __shared__ double2 sm[];
+  double2* tw0 = sm;
+  double2* tw1 = tw0 + g.n0;
+  double2* pl = tw1 + g.n1;
+  for (int i = threadIdx.x; i < g.n0; i += blockDim.x) tw0[i] = g.tw0[i];
+  for (int i = threadIdx.x; i < g.n1; i += blockDim.x) tw1[i] = g.tw1[i];
+  const int np = g.n0 * g.pitch;
+  for (int i = threadIdx.x; i < np; i += blockDim.x) pl[i] = make_double2(0.0, 0.0);
+  __syncthreads();
+  double2* row = t.sbuf + ((int64_t)unit * g.n2 + z) * t.S;
+  for (int s = threadIdx.x; s < t.S; s += blockDim.x) pl[t.stick_plane[s]] = row[s];
+  // inverse: y on the occupied x rows, x on every column
+  fft_lines<1>(pl, t.nxact, LineOffRows{t.xact, g.pitch}, 1, g.p1, tw1);
+  fft_lines<1>(pl, g.n1, LineOffCols{}, g.pitch, g.p0, tw0);
+  const double* v = t.vt + (int64_t)z * g.n0 * g.n1;
+  for (int i = threadIdx.x; i < g.n0 * g.n1; i += blockDim.x) {
+    const int x = i / g.n1, y = i - x * g.n1;
+    const double w = v[i];
+    double2& p = pl[x * g.pitch + y];
+    p.x *= w;
+    p.y *= w;
+  }
+  fft_lines<-1>(pl, g.n1, LineOffCols{}, g.pitch, g.p0, tw0);
+  fft_lines<-1>(pl, t.nxact, LineOffRows{t.xact, g.pitch}, 1, g.p1, tw1);
+  for (int s = threadIdx.x; s < t.S; s += blockDim.x) row[s] = pl[t.stick_plane[s]];
+}
+
+// ---------------------------------------------------------------- pass 3
+template <bool GAMMA>
+__global__ void __launch_bounds__(256) k_sticks_forward(OpTables t, BoxGeo g, CallArgs a) {
+  const int grp = blockIdx.x, unit = blockIdx.y;
+  if (grp >= t.ngroups || unit >= a.units) return;
+  extern __shared__ double2 sm[];
+  double2* tw = sm;
+  double2* st = sm + g.n2;
+  const int s0 = t.grp_stick[grp], cnt = t.grp_stick[grp + 1] - s0;
+  for (int i = threadIdx.x; i < g.n2; i += blockDim.x) tw[i] = g.tw2[i];
+  const double2* in = t.sbuf + (int64_t)unit * g.n2 * t.S + s0;
+  for (int i = threadIdx.x; i < cnt * g.n2; i += blockDim.x) {
+    const int z = i / cnt, sl = i - z * cnt;
+    st[sl * g.ld2 + z] = in[(int64_t)z * t.S + sl];
+  }
+  fft_lines<-1>(st, cnt, LineOffStride{g.ld2}, 1, g.p2, tw);
+  const double s = g.inv_n;
+  if (!GAMMA) {
+    const int e0 = t.grp_entry[grp], e1 = t.grp_entry[grp + 1];
+    const double2* x = reinterpret_cast<const double2*>(a.x + (int64_t)unit * a.ldx);
+    double2* y = reinterpret_cast<double2*>(a.y + (int64_t)unit * a.ldy);
+    for (int e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
+      const int2 en = t.entries[e];
+      const double2 h = st[en.y];
+      const double tk = t.kinetic[en.x];
+      const double2 xv = x[en.x];
+      y[en.x] = make_double2(h.x * s + tk * xv.x, h.y * s + tk * xv.y);
+    }
+  } else {
+    const int r0 = t.grp_rep[grp], r1 = t.grp_rep[grp + 1];
+    const int ca = 2 * unit;
+    const bool hasb = ca + 1 < a.cols;
+    const double* xa = a.x + (int64_t)ca * a.ldx;
+    const double* xb = a.x + (int64_t)(hasb ? ca + 1 : ca) * a.ldx;
+    double* ya = a.y + (int64_t)ca * a.ldy;
+    double* yb = a.y + (int64_t)(hasb ? ca + 1 : ca) * a.ldy;
+    for (int e = r0 + threadIdx.x; e < r1; e += blockDim.x) {
+      const int4 rp = t.reps[e];
+      const int r = rp.x;
+      double2 hp = st[rp.y];
+      hp.x *= s;
+      hp.y *= s;
+      if (r == 0) {
+        const double tk = t.kinetic[0];
+        ya[0] = hp.x + tk * xa[0];
+        if (hasb) yb[0] = hp.y + tk * xb[0];
+      } else {
+        double2 hm = st[rp.z];
+        hm.x *= s;
+        hm.y *= s;
+        // even = (hp + conj hm)/2, odd = (hp - conj hm)/2
+        const double ex = 0.5 * (hp.x + hm.x), ey = 0.5 * (hp.y - hm.y);
+        const double ox = 0.5 * (hp.x - hm.x), oy = 0.5 * (hp.y + hm.y);
+        const double t1 = t.kinetic[r], t2 = t.kinetic[r + 1];
+        ya[r] = ex * kSqrt2 + t1 * xa[r];
+        ya[r + 1] = ey * kSqrt2 + t2 * xa[r + 1];
+        if (hasb) {
+          yb[r] = oy * kSqrt2 + t1 * xb[r];
+          yb[r + 1] = -ox * kSqrt2 + t2 * xb[r + 1];
+        }
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------- nonlocal
+template <class T>
+struct Ops;
+template <>
+struct Ops<double> {
+  __device__ static double zero() { return 0.0; }
+  __device__ static double cmac(double acc, double a, double b) { return fma(a, b, acc); }  // a^* b
+  __device__ static double mac(double acc, double a, double b) { return fma(a, b, acc); }
+  __device__ static double add(double a, double b) { return a + b; }
+  __device__ static double scale(double d, double a) { return d * a; }
+};
+template <>
+struct Ops<double2> {
+  __device__ static double2 zero() { return make_double2(0.0, 0.0); }
+  __device__ static double2 cmac(double2 acc, double2 a, double2 b) {
+    acc.x = fma(a.x, b.x, fma(a.y, b.y, acc.x));
+    acc.y = fma(a.x, b.y, fma(-a.y, b.x, acc.y));
+    return acc;
+  }
+  __device__ static double2 mac(double2 acc, double2 a, double2 b) {
+    acc.x = fma(a.x, b.x, fma(-a.y, b.y, acc.x));
+    acc.y = fma(a.x, b.y, fma(a.y, b.x, acc.y));
+    return acc;
+  }
+  __device__ static double2 add(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+  __device__ static double2 scale(double d, double2 a) { return make_double2(d * a.x, d * a.y); }
+};
+
+// part[ks][c][p] = sum_{rows of chunk ks} P[p][row]^* X[c][row]; tile 32 p x 32 c.
+template <class T>
+__global__ void __launch_bounds__(256) k_project(const T* __restrict__ P, int rows, int nproj, const T* __restrict__ X,
+                                                 int64_t ldx, int cols, T* __restrict__ part, int kchunk) {
+  __shared__ T As[32][33];
+  __shared__ T Bs[32][33];
+  const int p0 = blockIdx.x * 32, c0 = blockIdx.y * 32, ks = blockIdx.z;
+  const int tp = threadIdx.x & 15, tc = threadIdx.x >> 4;
+  T acc[2][2];
+#pragma unroll
+  for (int i = 0; i < 2; ++i)
+#pragma unroll
+    for (int j = 0; j < 2; ++j) acc[i][j] = Ops<T>::zero();
+  const int g0 = ks * kchunk, g1 = min(rows, g0 + kchunk);
+  for (int gb = g0; gb < g1; gb += 32) {
+    for (int i = threadIdx.x; i < 1024; i += 256) {
+      const int gg = i & 31, q = i >> 5;
+      const int g = gb + gg;
+      As[gg][q] = (g < g1 && p0 + q < nproj) ? P[(int64_t)(p0 + q) * rows + g] : Ops<T>::zero();
+      Bs[gg][q] = (g < g1 && c0 + q < cols) ? X[(int64_t)(c0 + q) * ldx + g] : Ops<T>::zero();
+    }
+    __syncthreads();
+#pragma unroll 8
+    for (int gg = 0; gg < 32; ++gg) {
+      const T a0 = As[gg][tp], a1 = As[gg][tp + 16];
+      const T b0 = Bs[gg][tc], b1 = Bs[gg][tc + 16];
+      acc[0][0] = Ops<T>::cmac(acc[0][0], a0, b0);
+      acc[1][0] = Ops<T>::cmac(acc[1][0], a1, b0);
+      acc[0][1] = Ops<T>::cmac(acc[0][1], a0, b1);
+      acc[1][1] = Ops<T>::cmac(acc[1][1], a1, b1);
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int i = 0; i < 2; ++i)
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+      const int p = p0 + tp + 16 * i, c = c0 + tc + 16 * j;
+      if (p < nproj && c < cols) part[((int64_t)ks * cols + c) * nproj + p] = acc[i][j];
+    }
+}
+
+// wd[c][off+i] = sum_j D[i][j] (sum_ks part[ks][c][off+j]) for one (atom, column).
+template <class T>
+__global__ void k_couple(const T* __restrict__ part, int ksplit, int cols, int nproj, const int* __restrict__ atom_off,
+                         const int* __restrict__ d_off, const double* __restrict__ d, T* __restrict__ wd) {
+  __shared__ T w[64];
+  const int atom = blockIdx.x, c = blockIdx.y;
+  const int off = atom_off[atom], cnt = atom_off[atom + 1] - off;
+  const int i = threadIdx.x;
+  if (i < cnt) {
+    T s = Ops<T>::zero();
+    for (int ks = 0; ks < ksplit; ++ks) s = Ops<T>::add(s, part[((int64_t)ks * cols + c) * nproj + off + i]);
+    w[i] = s;
+  }
+  __syncthreads();
+  if (i < cnt) {
+    const double* dd = d + d_off[atom] + i * cnt;
+    T s = Ops<T>::zero();
+    for (int j = 0; j < cnt; ++j) s = Ops<T>::add(s, Ops<T>::scale(dd[j], w[j]));
+    wd[(int64_t)c * nproj + off + i] = s;
+  }
+}
+
+// y[c][row] += sum_p P[p][row] wd[c][p]; tile 64 rows x 32 columns.
+template <class T>
+__global__ void __launch_bounds__(256) k_back(const T* __restrict__ P, int rows, int nproj, const T* __restrict__ wd,
+                                              int cols, T* __restrict__ Y, int64_t ldy) {
+  __shared__ T Ps[16][64];
+  __shared__ T Ws[16][33];
+  const int r0 = blockIdx.x * 64, c0 = blockIdx.y * 32;
+  const int tg = threadIdx.x & 31, tc = threadIdx.x >> 5;
+  T acc[2][4];
+#pragma unroll
+  for (int i = 0; i < 2; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[i][j] = Ops<T>::zero();
+  for (int pb = 0; pb < nproj; pb += 16) {
+    for (int i = threadIdx.x; i < 16 * 64; i += 256) {
+      const int rr = i & 63, q = i >> 6;
+      const int p = pb + q, r = r0 + rr;
+      Ps[q][rr] = (p < nproj && r < rows) ? P[(int64_t)p * rows + r] : Ops<T>::zero();
+    }
+    for (int i = threadIdx.x; i < 16 * 32; i += 256) {
+      const int q = i & 15, cc = i >> 4;
+      const int p = pb + q, c = c0 + cc;
+      Ws[q][cc] = (p < nproj && c < cols) ? wd[(int64_t)c * nproj + p] : Ops<T>::zero();
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < 16; ++q) {
+      const T a0 = Ps[q][tg], a1 = Ps[q][tg + 32];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const T b = Ws[q][tc + 8 * j];
+        acc[0][j] = Ops<T>::mac(acc[0][j], a0, b);
+        acc[1][j] = Ops<T>::mac(acc[1][j], a1, b);
+      }
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int i = 0; i < 2; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int r = r0 + tg + 32 * i, c = c0 + tc + 8 * j;
+      if (r < rows && c < cols) {
+        T& out = Y[(int64_t)c * ldy + r];
+        out = Ops<T>::add(out, acc[i][j]);
+      }
+    }
+}
+
+}  // namespace
+
+size_t plane_smem_bytes(const BoxGeo& g) { return sizeof(double2) * ((size_t)g.n0 + g.n1 + (size_t)g.n0 * g.pitch); }
+size_t stick_smem_bytes(const BoxGeo& g) { return sizeof(double2) * ((size_t)g.n2 + (size_t)g.sg * g.ld2); }
+
+int launch_local(const OpTables& t, const BoxGeo& g, const CallArgs& a, cudaStream_t s) {
+  if (a.units == 0) return 0;
+  const size_t ss = stick_smem_bytes(g), ps = plane_smem_bytes(g);
+  const dim3 sgrid(t.ngroups, a.units);
+  const dim3 pgrid(a.units, g.n2);
+  if (t.gamma) {
+    k_sticks_inverse<true><<<sgrid, 256, ss, s>>>(t, g, a);
+    k_planes<<<pgrid, 512, ps, s>>>(t, g, a);
+    k_sticks_forward<true><<<sgrid, 256, ss, s>>>(t, g, a);
+  } else {
+    k_sticks_inverse<false><<<sgrid, 256, ss, s>>>(t, g, a);
+    k_planes<<<pgrid, 512, ps, s>>>(t, g, a);
+    k_sticks_forward<false><<<sgrid, 256, ss, s>>>(t, g, a);
+  }
+  return 3;
+}
+
+int launch_nonlocal(const OpTables& t, const NlTables& nl, const CallArgs& a, cudaStream_t s) {
+  if (nl.nproj == 0 || a.cols == 0) return 0;
+  const dim3 pg((nl.nproj + 31) / 32, (a.cols + 31) / 32, nl.ksplit);
+  const dim3 cg(nl.natoms, a.cols);
+  const dim3 bg_((t.rows + 63) / 64, (a.cols + 31) / 32);
+  const int cth = ((nl.maxch + 31) / 32) * 32;
+  if (t.gamma) {
+    k_project<double><<<pg, 256, 0, s>>>(nl.p, t.rows, nl.nproj, a.x, a.ldx, a.cols, nl.part, nl.kchunk);
+    k_couple<double><<<cg, cth, 0, s>>>(nl.part, nl.ksplit, a.cols, nl.nproj, nl.atom_off, nl.d_off, nl.d, nl.wd);
+    k_back<double><<<bg_, 256, 0, s>>>(nl.p, t.rows, nl.nproj, nl.wd, a.cols, a.y, a.ldy);
+  } else {
+    const double2* P = reinterpret_cast<const double2*>(nl.p);
+    double2* part = reinterpret_cast<double2*>(nl.part);
+    double2* wd = reinterpret_cast<double2*>(nl.wd);
+    k_project<double2><<<pg, 256, 0, s>>>(P, t.rows, nl.nproj, reinterpret_cast<const double2*>(a.x), a.ldx / 2,
+                                          a.cols, part, nl.kchunk);
+    k_couple<double2><<<cg, cth, 0, s>>>(part, nl.ksplit, a.cols, nl.nproj, nl.atom_off, nl.d_off, nl.d, wd);
+    k_back<double2><<<bg_, 256, 0, s>>>(P, t.rows, nl.nproj, wd, a.cols, reinterpret_cast<double2*>(a.y), a.ldy / 2);
+  }
+  return 3;
+}
+
+}  // namespace bg
+
+namespace bg {
+
+// Opt every kernel with dynamic shared memory into the sizes one operator needs.
+int configure_kernels(size_t plane_smem, size_t stick_smem) {
+  cudaError_t e = cudaSuccess;
+  auto set = [&](const void* f, size_t bytes) {
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  };
+  set((const void*)k_sticks_inverse<true>, stick_smem);
+  set((const void*)k_sticks_inverse<false>, stick_smem);
+  set((const void*)k_sticks_forward<true>, stick_smem);
+  set((const void*)k_sticks_forward<false>, stick_smem);
+  set((const void*)k_planes, plane_smem);
+  return e == cudaSuccess ? 0 : 1;
+}
+
+}  // namespace bg

@@ -1,0 +1,235 @@
+"""Host-side mirror of the reference's Hamiltonian operators over the C ABI.
+
+`ComplexHamiltonian` stands in for DistributedComplexHamiltonian (reference:
+crates/dft-physics/src/distributed_complex.rs:58-386) and `RealGammaHamiltonian` for
+DistributedRealHamiltonian (crates/dft-physics/src/distributed_real_gamma.rs:120-1352),
+both with one rank, so the method names, argument meaning and errors follow the
+reference: `new_owned`, `set_owned_potential(values, epoch)` (epochs strictly
+increasing), `apply_block(x, out)` (out completely overwritten, shape of x,
+at most `capacity` columns), `global_len`, `local_rows`, `diagonal_static`,
+`kinetic_diagonal`.  Blocks are numpy arrays (host; synchronous) or CUDA torch
+tensors (device; enqueued on the operator stream).
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _lib as L
+from .operands import NonlocalTable, PlaneWaves
+
+
+class SolverError(RuntimeError):
+    """Reference SolverError::InvalidParameter / Application (crates/dft-solvers/src/lib.rs:42-57)."""
+
+    def __init__(self, code, message):
+        super().__init__(message)
+        self.code = code
+
+
+class Context:
+    """One CUDA device (bg_ctx)."""
+
+    def __init__(self, device: int = 0):
+        self._lib = L.load()
+        opts = L.DeviceOpts(device)
+        h = ctypes.c_void_p()
+        rc = self._lib.bg_ctx_create(ctypes.byref(opts), ctypes.byref(h))
+        if rc != L.BG_OK:
+            raise L.BaandiError(rc, L.last_error(None))
+        self.handle = h
+        self.device = device
+
+    def close(self):
+        if self.handle:
+            self._lib.bg_ctx_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+_default_ctx = None
+
+
+def default_context() -> Context:
+    global _default_ctx
+    if _default_ctx is None:
+        _default_ctx = Context(0)
+    return _default_ctx
+
+
+def _p(a):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+class _Operator:
+    _gamma = False
+
+    def __init__(self, pw: PlaneWaves, dims, nl: NonlocalTable | None, capacity: int, ctx: Context | None = None):
+        self.ctx = ctx or default_context()
+        self._lib = self.ctx._lib
+        self.dims = [int(d) for d in dims]
+        self.npw = pw.npw
+        self._miller = np.ascontiguousarray(pw.miller, dtype=np.int32)
+        self._kinetic = np.ascontiguousarray(0.5 * pw.kpg2, dtype=np.float64)
+        desc = L.BasisDesc(self.npw, _p(self._miller), _p(self._kinetic), (ctypes.c_int32 * 3)(*self.dims),
+                           1 if pw.gamma else 0)
+        if nl is not None and nl.table.shape[1] > 0:
+            self._table = np.ascontiguousarray(nl.table.T).view(np.float64)
+            self._channels = np.ascontiguousarray(nl.channels, dtype=np.int32)
+            self._couplings = np.ascontiguousarray(nl.couplings, dtype=np.float64)
+            proj = L.Projectors(nl.table.shape[1], _p(self._table), len(self._channels), _p(self._channels),
+                                _p(self._couplings))
+            pproj = ctypes.byref(proj)
+        else:
+            pproj = None
+        h = ctypes.c_void_p()
+        create = self._lib.bg_op_create_gamma_real if self._gamma else self._lib.bg_op_create_complex
+        rc = create(self.ctx.handle, ctypes.byref(desc), pproj, int(capacity), ctypes.byref(h))
+        self._check(rc)
+        self.handle = h
+        self._capacity = int(capacity)
+        self._epoch = None
+
+    # -- reference accessors
+    def global_len(self) -> int:
+        return self.npw
+
+    def local_rows(self):
+        return np.arange(self.npw)
+
+    def capacity(self) -> int:
+        return self._capacity
+
+    def owned_epoch(self):
+        return self._epoch
+
+    def diagonal_static(self) -> np.ndarray:
+        out = np.zeros(self.npw)
+        self._check(self._lib.bg_op_diagonal(self.handle, _p(out)))
+        return out
+
+    def _check(self, rc):
+        if rc != L.BG_OK:
+            raise SolverError(rc, f"{L.CODE_NAMES.get(rc, rc)}: {L.last_error(self.ctx.handle)}")
+
+    def set_owned_potential(self, values, epoch: int):
+        v = np.ascontiguousarray(np.asarray(values, dtype=np.float64).reshape(-1))
+        if v.size != self.dims[0] * self.dims[1] * self.dims[2]:
+            raise SolverError(L.BG_ESHAPE, "potential must be the full grid in C order")
+        self._check(self._lib.bg_op_set_potential(self.handle, _p(v), int(epoch)))
+        self._epoch = int(epoch)
+
+    def stream(self):
+        s = ctypes.c_void_p()
+        self._check(self._lib.bg_op_stream(self.handle, ctypes.byref(s)))
+        return s.value
+
+    def set_stream(self, stream_ptr: int):
+        self._check(self._lib.bg_op_set_stream(self.handle, ctypes.c_void_p(stream_ptr)))
+
+    def sync(self):
+        self._check(self._lib.bg_op_sync(self.handle))
+
+    def launches(self) -> int:
+        n = ctypes.c_int64()
+        self._check(self._lib.bg_op_launches(self.handle, ctypes.byref(n)))
+        return n.value
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self._lib.bg_op_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- apply
+    def _apply_raw(self, x_ptr, y_ptr, cols, kind):
+        self._check(self._lib.bg_op_apply_block(self.handle, ctypes.c_void_p(x_ptr), ctypes.c_void_p(y_ptr),
+                                                self.npw, int(cols), kind, L.BG_PREC_FP64))
+
+
+class ComplexHamiltonian(_Operator):
+    """y = H x on complex plane-wave rows of one k point."""
+
+    _gamma = False
+
+    @classmethod
+    def new_owned(cls, pw, dims, nl, capacity, ctx=None):
+        return cls(pw, dims, nl, capacity, ctx)
+
+    def kinetic_diagonal(self) -> np.ndarray:
+        return self._kinetic.copy()
+
+    def apply_block(self, x, out=None):
+        """x: (npw, m) complex128 numpy array or CUDA complex128 torch tensor whose
+        columns are contiguous (Fortran order / .T of a row-major (m, npw))."""
+        if isinstance(x, np.ndarray):
+            if x.ndim != 2 or x.shape[0] != self.npw:
+                raise SolverError(L.BG_ESHAPE, "block rows")
+            xin = np.asfortranarray(x, dtype=np.complex128)
+            y = np.zeros_like(xin, order="F") if out is None else out
+            if not (y.flags.f_contiguous and y.dtype == np.complex128 and y.shape == xin.shape):
+                raise SolverError(L.BG_ESHAPE, "out must be a Fortran-ordered complex128 array of x's shape")
+            self._apply_raw(xin.ctypes.data, y.ctypes.data, xin.shape[1], L.BG_PTR_HOST)
+            return y
+        return _apply_torch(self, x, out, complex_rows=True)
+
+
+class RealGammaHamiltonian(_Operator):
+    """y = H x on real ORC rows of the Gamma sphere (two columns per complex FFT)."""
+
+    _gamma = True
+
+    @classmethod
+    def new_owned(cls, pw, dims, nl, capacity, ctx=None):
+        if not pw.gamma:
+            raise SolverError(L.BG_ESHAPE, "the real operator needs the Gamma sphere")
+        return cls(pw, dims, nl, capacity, ctx)
+
+    def kinetic_diagonal(self) -> np.ndarray:
+        from .operands import half_sphere
+        plus, _ = half_sphere(self._miller)
+        out = np.empty(self.npw)
+        out[0] = self._kinetic[0]
+        i = np.arange(1, len(plus))
+        out[2 * i - 1] = self._kinetic[plus[1:]]
+        out[2 * i] = self._kinetic[plus[1:]]
+        return out
+
+    def apply_block(self, x, out=None):
+        if isinstance(x, np.ndarray):
+            if x.ndim != 2 or x.shape[0] != self.npw:
+                raise SolverError(L.BG_ESHAPE, "block rows")
+            xin = np.asfortranarray(x, dtype=np.float64)
+            y = np.zeros_like(xin, order="F") if out is None else out
+            if not (y.flags.f_contiguous and y.dtype == np.float64 and y.shape == xin.shape):
+                raise SolverError(L.BG_ESHAPE, "out must be a Fortran-ordered float64 array of x's shape")
+            self._apply_raw(xin.ctypes.data, y.ctypes.data, xin.shape[1], L.BG_PTR_HOST)
+            return y
+        return _apply_torch(self, x, out, complex_rows=False)
+
+
+def _apply_torch(op, x, out, complex_rows):
+    """Device path: x, out are CUDA tensors shaped (m, npw) row-major (one band per
+    row, i.e. column-major (npw, m)); enqueued on the operator's stream."""
+    import torch
+
+    want = torch.complex128 if complex_rows else torch.float64
+    if x.dtype != want or not x.is_cuda or x.dim() != 2 or x.shape[1] != op.npw or not x.is_contiguous():
+        raise SolverError(L.BG_ESHAPE, f"device blocks are contiguous {want} CUDA tensors shaped (m, npw)")
+    if out is None:
+        out = torch.empty_like(x)
+    if out.shape != x.shape or out.dtype != x.dtype or not out.is_contiguous():
+        raise SolverError(L.BG_ESHAPE, "out must match x")
+    op._apply_raw(x.data_ptr(), out.data_ptr(), x.shape[0], L.BG_PTR_DEVICE)
+    return out

@@ -1,0 +1,174 @@
+/* baandi_gpu.h -- C ABI of the B200 Hamiltonian-apply library (libbaandi_b200.so).
+ *
+ * The library applies the Kohn-Sham Hamiltonian H = T + V_loc(r) + V_NL to blocks of
+ * plane-wave coefficient columns on one GPU, and builds the operands of that apply.
+ * Every entry point returns an int status: BG_OK (0) or one of the BG_E* codes below;
+ * bg_last_error() gives the message of the last failure on a context.
+ *
+ * Layouts.  Coefficient blocks are column-major, one column per band.  Complex values
+ * are interleaved (re, im) doubles.  The local potential is the full real grid in C
+ * order, flat index (i*n1 + j)*n2 + k for grid point r = i/n0 a1 + j/n1 a2 + k/n2 a3.
+ *
+ * Each operator mirrors one reference Hamiltonian (paths inside the reference project):
+ *   complex (k point)  crates/dft-physics/src/distributed_complex.rs:58-386
+ *                      (trait DistributedComplexOperator, crates/dft-solvers/src/
+ *                      ref_davidson_complex.rs:41-56)
+ *   real Gamma (ORC)   crates/dft-physics/src/distributed_real_gamma.rs:120-1352
+ *                      (trait DistributedRealOperator, crates/dft-solvers/src/
+ *                      distributed_davidson.rs:23-40)
+ * with one rank: the communicator argument of the reference calls has no counterpart.
+ */
+#ifndef BAANDI_GPU_H
+#define BAANDI_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ----------------------------------------------------------------- status codes */
+#define BG_OK 0
+#define BG_ESHAPE 1     /* dimensions, row/column counts or layout mismatch        */
+#define BG_ENONFINITE 2 /* a NaN or infinity in an input                           */
+#define BG_EEPOCH 3     /* potential epoch not strictly increasing / never set     */
+#define BG_EDEVICE 4    /* CUDA runtime or kernel failure                          */
+#define BG_ETIMEOUT 5   /* a bounded device wait gave up                           */
+#define BG_EINVAL 6     /* invalid argument (null pointer, bad option)            */
+#define BG_ENOMEM 7     /* device or host allocation failed                        */
+
+/* pointer kinds of bg_op_apply_block */
+#define BG_PTR_HOST 0   /* synchronous: copies in, applies, copies out, validates   */
+#define BG_PTR_DEVICE 1 /* asynchronous on the operator's stream                    */
+
+/* arithmetic of bg_op_apply_block */
+#define BG_PREC_FP64 0
+
+typedef struct bg_ctx bg_ctx;
+typedef struct bg_op bg_op;
+
+typedef struct {
+  int32_t device;       /* CUDA ordinal */
+  int32_t reserved[7];  /* zero */
+} bg_device_opts;
+
+/* --------------------------------------------------------------------- context */
+int bg_ctx_create(const bg_device_opts* opts, bg_ctx** out);
+int bg_ctx_destroy(bg_ctx* ctx);
+/* Copies the last failure message of `ctx` (or of context-free calls when ctx is
+ * NULL) into buf, NUL-terminated, truncated to len. */
+int bg_last_error(const bg_ctx* ctx, char* buf, size_t len);
+
+/* ------------------------------------------------------------------- operators */
+/* Plane-wave basis of one k point.  miller: npw integer triples (G = sum m_j b_j),
+ * in the caller's row order; kinetic: 1/2 |k+G|^2 (Ha) per row; dims: FFT grid.
+ * k != 0 maps Miller indices modulo the grid; at Gamma they must lie in the
+ * canonical interval [-n/2, (n-1)/2] (crates/dft-basis/src/lib.rs:380-398, 491-502). */
+typedef struct {
+  int64_t npw;
+  const int32_t* miller;
+  const double* kinetic;
+  int32_t dims[3];
+  int32_t gamma; /* 1: exactly Gamma (canonical-interval check applies) */
+} bg_basis_desc;
+
+/* Nonlocal projectors: table is column-major npw x nproj complex (interleaved), the
+ * reference's beta(k+G) columns (crates/dft-physics/src/hamiltonian.rs:2605-2760);
+ * channels[a] columns belong to atom a, in order; couplings are the per-atom
+ * channels[a] x channels[a] row-major D blocks (Ha), concatenated. */
+typedef struct {
+  int32_t nproj;
+  const double* table;
+  int32_t natoms;
+  const int32_t* channels;
+  const double* couplings;
+} bg_projectors;
+
+/* Replaces DistributedComplexHamiltonian::new_owned (distributed_complex.rs:88-167)
+ * with one rank.  capacity = widest block bg_op_apply_block accepts. */
+int bg_op_create_complex(bg_ctx* ctx, const bg_basis_desc* basis, const bg_projectors* proj,
+                         int64_t capacity, bg_op** out);
+
+/* Replaces DistributedRealHamiltonian::new_owned (distributed_real_gamma.rs:228-247,
+ * from_parts :249-420) with one rank.  `basis` is the full Gamma sphere (row 0 = G=0,
+ * every -G present); `proj` its complex table; rows of the operator are the ORC rows
+ * of crates/dft-basis/src/half.rs:31-37 (n = npw real rows). */
+int bg_op_create_gamma_real(bg_ctx* ctx, const bg_basis_desc* basis, const bg_projectors* proj,
+                            int64_t capacity, bg_op** out);
+
+int bg_op_destroy(bg_op* op);
+
+/* Replaces set_owned_potential (distributed_complex.rs:252-264): v is the full real
+ * grid (n0*n1*n2, C order, host memory); epoch must exceed the previous one. */
+int bg_op_set_potential(bg_op* op, const double* v_grid, uint64_t epoch);
+
+/* Replaces apply_block (distributed_complex.rs:340-386; distributed_real_gamma.rs:
+ * 1062-1264): y = H x, y completely overwritten.  rows must equal the operator's row
+ * count (npw), 0 <= cols <= capacity.  Complex operators take interleaved complex
+ * columns, the Gamma operator real ORC columns.  ptr_kind BG_PTR_HOST: synchronous,
+ * x is checked finite (BG_ENONFINITE) before any work.  BG_PTR_DEVICE: enqueued on
+ * the operator's stream; x must not alias y. */
+int bg_op_apply_block(bg_op* op, const double* x, double* y, int64_t rows, int64_t cols,
+                      int32_t ptr_kind, int32_t precision);
+
+/* Kinetic plus nonlocal diagonal T_g + sum D_ij Re(P_gi conj(P_gj)) per row (Ha),
+ * the reference's static_diagonal (distributed_complex.rs:29-53); host buffer of
+ * `rows` doubles (ORC order for the Gamma operator). */
+int bg_op_diagonal(const bg_op* op, double* out);
+
+/* Row count (global_len), capacity, and the operator's CUDA stream (cudaStream_t). */
+int bg_op_rows(const bg_op* op, int64_t* rows);
+int bg_op_capacity(const bg_op* op, int64_t* capacity);
+int bg_op_stream(const bg_op* op, void** stream);
+/* Use the caller's stream (cudaStream_t, e.g. a torch stream) for BG_PTR_DEVICE work. */
+int bg_op_set_stream(bg_op* op, void* stream);
+/* Wait for the operator's stream and report a device error recorded by earlier
+ * BG_PTR_DEVICE applies (BG_ENONFINITE for a non-finite input column). */
+int bg_op_sync(bg_op* op);
+/* Count of this library's kernel launches issued by the operator so far. */
+int bg_op_launches(const bg_op* op, int64_t* launches);
+
+/* ------------------------------------------------------------ operand builders */
+/* Restatements of the reference setup (host, FP64) for callers without the
+ * reference engine.  Lattice vectors are the ROWS of rows[9] (Bohr). */
+int bg_setup_volume(const double rows[9], double* volume);
+/* Plane waves with 1/2|k+G|^2 <= ecut (Ha), sorted by |G|^2 then Miller index
+ * (crates/dft-basis/src/lib.rs:233-265).  Call with capacity 0 to get *npw. */
+int bg_setup_basis(const double rows[9], double ecut_ha, const double kfrac[3], int64_t capacity,
+                   int64_t* npw, int32_t* miller, double* kpg, double* kpg2);
+/* Alias-free grid over the 4*ecut density sphere (crates/dft-basis/src/lib.rs:414-455). */
+int bg_setup_grid(const double rows[9], double ecut_ha, int32_t dims[3], int32_t required[3]);
+/* Gamma mirror maps (crates/dft-basis/src/half.rs:41-99): nh = (npw+1)/2 entries each. */
+int bg_setup_half_sphere(const int32_t* miller, int64_t npw, int64_t* plus, int64_t* minus);
+
+/* One pseudopotential species on a radial mesh (Bohr), local part and D in Ha. */
+typedef struct {
+  double z_valence;
+  int32_t mesh;
+  const double* r;
+  const double* rab;
+  const double* local;        /* V_loc(r), Ha (form factor only)                 */
+  int32_t nbeta;
+  const int32_t* l;           /* angular momentum per projector                 */
+  const int32_t* beta_len;    /* samples per projector (prefix of the mesh)     */
+  const double* const* beta;  /* r*beta(r) per projector                        */
+  const double* dij;          /* nbeta x nbeta row-major, Ha                     */
+  int32_t natoms;
+  const double* positions;    /* 3*natoms Cartesian Bohr                         */
+} bg_species;
+
+int bg_setup_projector_count(int32_t nspecies, const bg_species* species, int32_t* nproj,
+                             int32_t* natoms);
+/* Projector table at the momenta k+G (kpg 3*npw, kpg2 npw) of one basis. */
+int bg_setup_projectors(double volume, int64_t npw, const double* kpg, const double* kpg2,
+                        int32_t nspecies, const bg_species* species, double* table,
+                        int32_t* channels, double* couplings);
+/* V_loc(|G|) (Ha) of one species at n wave numbers (crates/dft-upf/src/radial.rs:246-305). */
+int bg_setup_local_form_factor(const bg_species* species, double volume, int64_t n,
+                               const double* g, double* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* BAANDI_GPU_H */
