@@ -70,6 +70,17 @@ SIGNATURES = {
     "bg_op_set_stream": [_p, _p],
     "bg_op_sync": [_p],
     "bg_op_launches": [_p, ctypes.POINTER(_i64)],
+    "bg_op_profile": [_p, _i32],
+    "bg_op_stage_times": [_p, _p],
+    "bg_kset_create": [_p, _i32, _p, _pp],
+    "bg_kset_destroy": [_p],
+    "bg_kset_apply": [_p, _p, _p, _p, _i32, _i32],
+    "bg_kset_sync": [_p],
+    "bg_kset_stream": [_p, _pp],
+    "bg_kset_set_stream": [_p, _p],
+    "bg_kset_launches": [_p, ctypes.POINTER(_i64)],
+    "bg_kset_profile": [_p, _i32],
+    "bg_kset_stage_times": [_p, _p],
     "bg_setup_volume": [_p, ctypes.POINTER(_dbl)],
     "bg_setup_basis": [_p, _dbl, _p, _i64, ctypes.POINTER(_i64), _p, _p, _p],
     "bg_setup_grid": [_p, _dbl, _p, _p],

@@ -16,8 +16,6 @@
 #include "hpsi.h"
 
 namespace bg {
-int configure_kernels(size_t plane_smem, size_t stick_smem);
-
 static thread_local std::string g_error;
 void set_global_error(const std::string& msg) { g_error = msg; }
 std::string global_error() { return g_error; }
@@ -58,8 +56,12 @@ struct bg_op {
   std::vector<double> diag;
   OpTables t{};
   BoxGeo g{};
-  NlTables nl{};
-  int ksplit_max = 1;
+  NlDev nl{};
+  NlShape shape{};
+  int64_t part_cols = 0;        // capacity of nl.part in (ksplit x columns) units
+  OpTables* d_tabs = nullptr;   // device copy of t (a batch of one)
+  NlDev* d_nl = nullptr;        // device copy of nl
+  StageEvents ev;
   std::vector<std::unique_ptr<DevBuf>> bufs;
   DevBuf* xs = nullptr;  // host-apply staging
   DevBuf* ys = nullptr;
@@ -134,6 +136,19 @@ std::vector<double> twiddles(int n) {
     t[2 * q + 1] = (double)sinl(a);
   }
   return t;
+}
+
+// Split of the P^H X reduction over rows: enough (tile, split) blocks to fill the
+// 148 SMs twice, chunks a multiple of 32 rows.
+int ksplit_tiles(int64_t rows, int64_t tiles, int* kchunk, int64_t ks_cap = 1 << 30) {
+  int64_t ks = std::max<int64_t>(1, (2 * 148 + tiles - 1) / tiles);
+  ks = std::min<int64_t>(ks, std::max<int64_t>(1, ks_cap));
+  ks = std::min<int64_t>(ks, (rows + 31) / 32);
+  int64_t chunk = (rows + ks - 1) / ks;
+  chunk = ((chunk + 31) / 32) * 32;
+  ks = (rows + chunk - 1) / chunk;
+  *kchunk = (int)chunk;
+  return (int)ks;
 }
 
 int ksplit_for(int64_t rows, int nproj, int64_t cols, int* kchunk) {
@@ -347,8 +362,9 @@ int build_op(bg_ctx* ctx, const bg_basis_desc* b, const bg_projectors* pr, int64
   }
 
   // nonlocal operands and the static diagonal
-  NlTables& N = op->nl;
-  N.nproj = nproj;
+  NlDev& N = op->nl;
+  N.rows = (int)npw;
+  op->shape.nproj = nproj;
   op->diag.assign(npw, 0.0);
   op->diag = kin;  // no projectors: the diagonal is the kinetic term
   if (nproj > 0) {
@@ -407,8 +423,8 @@ int build_op(bg_ctx* ctx, const bg_basis_desc* b, const bg_projectors* pr, int64
       if ((rc = upload(op.get(), pr->table, (size_t)2 * npw * nproj, &d_dbl))) return rc;
     }
     N.p = d_dbl;
-    N.natoms = natoms;
-    N.maxch = maxch;
+    op->shape.natoms = natoms;
+    op->shape.maxch = maxch;
     if ((rc = upload(op.get(), atom_off.data(), atom_off.size(), &d_int))) return rc;
     N.atom_off = d_int;
     if ((rc = upload(op.get(), d_off.data(), d_off.size(), &d_int))) return rc;
@@ -422,6 +438,7 @@ int build_op(bg_ctx* ctx, const bg_basis_desc* b, const bg_projectors* pr, int64
       maxpart = std::max<int64_t>(maxpart, (int64_t)ks * c);
     }
     const size_t es = gamma ? sizeof(double) : sizeof(double2);
+    op->part_cols = maxpart;
     if ((rc = alloc(op.get(), es * (size_t)maxpart * nproj, &vp))) return rc;
     N.part = static_cast<double*>(vp);
     if ((rc = alloc(op.get(), es * (size_t)capacity * nproj, &vp))) return rc;
@@ -444,6 +461,10 @@ int build_op(bg_ctx* ctx, const bg_basis_desc* b, const bg_projectors* pr, int64
     return fail(ctx, BG_ESHAPE, "FFT plane does not fit in shared memory");
   if ((rc = configure_kernels((size_t)dev_smem, (size_t)dev_smem)) != BG_OK)
     return fail(ctx, BG_EDEVICE, "cudaFuncSetAttribute failed");
+  if ((rc = upload(op.get(), &op->t, 1, &op->d_tabs))) return rc;
+  if ((rc = upload(op.get(), &op->nl, 1, &op->d_nl))) return rc;
+  for (int i = 0; i < 2 * kStages; ++i)
+    if ((ce = cudaEventCreate(&op->ev.ev[i])) != cudaSuccess) return cuda_fail(ctx, ce, "cudaEventCreate");
   if ((ce = cudaDeviceSynchronize()) != cudaSuccess) return cuda_fail(ctx, ce, "setup");
   *out = op.release();
   return BG_OK;
@@ -506,6 +527,8 @@ int bg_op_create_gamma_real(bg_ctx* ctx, const bg_basis_desc* basis, const bg_pr
 int bg_op_destroy(bg_op* op) {
   if (!op) return BG_OK;
   if (op->stream) cudaStreamSynchronize(op->stream);
+  for (int i = 0; i < 2 * kStages; ++i)
+    if (op->ev.ev[i]) cudaEventDestroy(op->ev.ev[i]);
   if (op->own_stream && op->stream) cudaStreamDestroy(op->stream);
   if (op->err_host) cudaFreeHost(op->err_host);
   delete op;
@@ -550,26 +573,27 @@ int bg_op_apply_block(bg_op* op, const double* x, double* y, int64_t rows, int64
   const double* dx = x;
   double* dy = y;
   if (ptr_kind == BG_PTR_HOST) {
-    for (size_t i = 0; i < dpc * cols; ++i)
-      if (!std::isfinite(x[i])) return fail(ctx, BG_ENONFINITE, "non-finite input coefficient");
+    // Finiteness is checked on the device by the scatter pass (every input value is
+    // read there) and reported after the copy back, before this call returns.
     dx = static_cast<const double*>(op->xs->p);
     dy = static_cast<double*>(op->ys->p);
     e = cudaMemcpyAsync(const_cast<double*>(dx), x, dpc * cols * sizeof(double), cudaMemcpyHostToDevice, op->stream);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "copy in");
   }
-  CallArgs a;
+  Batch bt;
+  bt.nk = 1;
+  CallArgs& a = bt.a[0];
   a.x = dx;
   a.y = dy;
   a.ldx = (int64_t)dpc;
   a.ldy = (int64_t)dpc;
   a.cols = (int)cols;
   a.units = op->gamma ? (int)((cols + 1) / 2) : (int)cols;
-  op->launches += launch_local(op->t, op->g, a, op->stream);
-  if (op->nl.nproj > 0) {
-    int kc;
-    op->nl.ksplit = ksplit_for(op->rows, op->nl.nproj, cols, &kc);
-    op->nl.kchunk = kc;
-    op->launches += launch_nonlocal(op->t, op->nl, a, op->stream);
+  op->launches += launch_local(op->d_tabs, op->gamma ? 1 : 0, op->t.ngroups, op->g, bt, op->stream, &op->ev);
+  if (op->shape.nproj > 0) {
+    NlShape sh = op->shape;
+    sh.ksplit = ksplit_for(op->rows, sh.nproj, cols, &sh.kchunk);
+    op->launches += launch_nonlocal(op->d_nl, op->gamma ? 1 : 0, sh, (int)op->rows, bt, op->stream, &op->ev);
   }
   e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(ctx, e, "kernel launch");
@@ -625,6 +649,222 @@ int bg_op_launches(const bg_op* op, int64_t* launches) {
   if (!op || !launches) return BG_EINVAL;
   *launches = op->launches;
   return BG_OK;
+}
+
+int bg_op_profile(bg_op* op, int32_t enable) {
+  if (!op) return BG_EINVAL;
+  op->ev.on = enable != 0;
+  return BG_OK;
+}
+
+static int stage_times(bg_ctx* ctx, cudaStream_t stream, const StageEvents& ev, double* ms) {
+  if (!ms) return fail(ctx, BG_EINVAL, "null output");
+  cudaError_t e = cudaStreamSynchronize(stream);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "stage_times");
+  for (int s = 0; s < kStages; ++s) {
+    float t = 0.0f;
+    ms[s] = 0.0;
+    if (ev.on && cudaEventQuery(ev.ev[2 * s]) == cudaSuccess && cudaEventQuery(ev.ev[2 * s + 1]) == cudaSuccess &&
+        cudaEventElapsedTime(&t, ev.ev[2 * s], ev.ev[2 * s + 1]) == cudaSuccess)
+      ms[s] = t;
+  }
+  cudaGetLastError();
+  return BG_OK;
+}
+
+int bg_op_stage_times(bg_op* op, double* ms) {
+  if (!op) return BG_EINVAL;
+  return stage_times(op->ctx, op->stream, op->ev, ms);
+}
+
+}  // extern "C"
+
+struct bg_kset {
+  bg_ctx* ctx = nullptr;
+  std::vector<bg_op*> ops;
+  int gamma = 0;
+  int max_groups = 0;
+  int max_rows = 0;
+  NlShape shape{};
+  BoxGeo g{};
+  OpTables* d_tabs = nullptr;
+  NlDev* d_nl = nullptr;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  StageEvents ev;
+  int64_t launches = 0;
+};
+
+extern "C" {
+
+int bg_kset_create(bg_ctx* ctx, int32_t n, bg_op* const* ops, bg_kset** out) {
+  if (!ctx || !ops || !out) return fail(ctx, BG_EINVAL, "null argument");
+  if (n < 1 || n > kMaxBatch) return fail(ctx, BG_ESHAPE, "a k-point set holds 1..64 operators");
+  auto ks = std::make_unique<bg_kset>();
+  ks->ctx = ctx;
+  const bg_op* o0 = ops[0];
+  if (!o0) return fail(ctx, BG_EINVAL, "null operator");
+  std::vector<OpTables> tabs;
+  std::vector<NlDev> nls;
+  for (int i = 0; i < n; ++i) {
+    const bg_op* o = ops[i];
+    if (!o || o->ctx != ctx) return fail(ctx, BG_EINVAL, "operators must belong to this context");
+    if (o->gamma != o0->gamma || std::memcmp(o->dims, o0->dims, sizeof o->dims) != 0 ||
+        o->shape.nproj != o0->shape.nproj || o->shape.natoms != o0->shape.natoms)
+      return fail(ctx, BG_ESHAPE, "operators of a set need one grid, one kind and one projector layout");
+    ks->ops.push_back(const_cast<bg_op*>(o));
+    tabs.push_back(o->t);
+    nls.push_back(o->nl);
+    ks->max_groups = std::max(ks->max_groups, o->t.ngroups);
+    ks->max_rows = std::max<int>(ks->max_rows, (int)o->rows);
+    ks->shape.maxch = std::max(ks->shape.maxch, o->shape.maxch);
+  }
+  ks->gamma = o0->gamma ? 1 : 0;
+  ks->shape.nproj = o0->shape.nproj;
+  ks->shape.natoms = o0->shape.natoms;
+  ks->g = o0->g;
+  cudaError_t e = cudaSetDevice(ctx->device);
+  if (e == cudaSuccess) e = cudaMalloc(&ks->d_tabs, sizeof(OpTables) * n);
+  if (e == cudaSuccess) e = cudaMalloc(&ks->d_nl, sizeof(NlDev) * n);
+  if (e == cudaSuccess) e = cudaMemcpy(ks->d_tabs, tabs.data(), sizeof(OpTables) * n, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(ks->d_nl, nls.data(), sizeof(NlDev) * n, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ks->stream, cudaStreamNonBlocking);
+  for (int i = 0; i < 2 * kStages && e == cudaSuccess; ++i) e = cudaEventCreate(&ks->ev.ev[i]);
+  if (e != cudaSuccess) {
+    if (ks->d_tabs) cudaFree(ks->d_tabs);
+    if (ks->d_nl) cudaFree(ks->d_nl);
+    return cuda_fail(ctx, e, "k-point set");
+  }
+  ks->own_stream = true;
+  *out = ks.release();
+  return BG_OK;
+}
+
+int bg_kset_destroy(bg_kset* ks) {
+  if (!ks) return BG_OK;
+  if (ks->stream) cudaStreamSynchronize(ks->stream);
+  for (int i = 0; i < 2 * kStages; ++i)
+    if (ks->ev.ev[i]) cudaEventDestroy(ks->ev.ev[i]);
+  if (ks->own_stream && ks->stream) cudaStreamDestroy(ks->stream);
+  cudaFree(ks->d_tabs);
+  cudaFree(ks->d_nl);
+  delete ks;
+  return BG_OK;
+}
+
+int bg_kset_apply(bg_kset* ks, const double* const* x, double* const* y, const int64_t* cols, int32_t ptr_kind,
+                  int32_t precision) {
+  if (!ks || !x || !y || !cols) return fail(ks ? ks->ctx : nullptr, BG_EINVAL, "null argument");
+  bg_ctx* ctx = ks->ctx;
+  if (precision != BG_PREC_FP64) return fail(ctx, BG_EINVAL, "unsupported precision");
+  if (ptr_kind != BG_PTR_HOST && ptr_kind != BG_PTR_DEVICE) return fail(ctx, BG_EINVAL, "pointer kind");
+  const int n = (int)ks->ops.size();
+  Batch bt;
+  bt.nk = n;
+  int64_t max_cols = 0;
+  for (int k = 0; k < n; ++k) {
+    bg_op* op = ks->ops[k];
+    if (!op->has_epoch) return fail(ctx, BG_EEPOCH, "potential was never set on an operator of the set");
+    if (cols[k] < 0 || cols[k] > op->cap) return fail(ctx, BG_ESHAPE, "block shape");
+    if (cols[k] > 0 && (!x[k] || !y[k] || x[k] == y[k]))
+      return fail(ctx, BG_EINVAL, "x and y must be distinct non-null buffers");
+    max_cols = std::max(max_cols, cols[k]);
+  }
+  cudaError_t e = cudaSetDevice(ctx->device);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaSetDevice");
+  for (int k = 0; k < n; ++k) {
+    bg_op* op = ks->ops[k];
+    const size_t dpc = op->gamma ? (size_t)op->rows : (size_t)2 * op->rows;
+    CallArgs& a = bt.a[k];
+    a.x = x[k];
+    a.y = y[k];
+    if (ptr_kind == BG_PTR_HOST && cols[k] > 0) {
+      a.x = static_cast<const double*>(op->xs->p);
+      a.y = static_cast<double*>(op->ys->p);
+      e = cudaMemcpyAsync(const_cast<double*>(a.x), x[k], dpc * cols[k] * sizeof(double), cudaMemcpyHostToDevice,
+                          ks->stream);
+      if (e != cudaSuccess) return cuda_fail(ctx, e, "copy in");
+    }
+    a.ldx = a.ldy = (int64_t)dpc;
+    a.cols = (int)cols[k];
+    a.units = op->gamma ? (int)((cols[k] + 1) / 2) : (int)cols[k];
+  }
+  if (max_cols == 0) return BG_OK;
+  ks->launches += launch_local(ks->d_tabs, ks->gamma, ks->max_groups, ks->g, bt, ks->stream, &ks->ev);
+  if (ks->shape.nproj > 0) {
+    NlShape sh = ks->shape;
+    int64_t tiles = 0, cap = 1 << 30;
+    for (int k = 0; k < n; ++k) {
+      tiles += ((sh.nproj + 31) / 32) * ((cols[k] + 31) / 32);
+      if (cols[k] > 0) cap = std::min<int64_t>(cap, ks->ops[k]->part_cols / cols[k]);
+    }
+    sh.ksplit = ksplit_tiles(ks->max_rows, std::max<int64_t>(tiles, 1), &sh.kchunk, cap);
+    ks->launches += launch_nonlocal(ks->d_nl, ks->gamma, sh, ks->max_rows, bt, ks->stream, &ks->ev);
+  }
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "kernel launch");
+  if (ptr_kind == BG_PTR_HOST) {
+    for (int k = 0; k < n; ++k) {
+      bg_op* op = ks->ops[k];
+      if (cols[k] == 0) continue;
+      const size_t dpc = op->gamma ? (size_t)op->rows : (size_t)2 * op->rows;
+      e = cudaMemcpyAsync(y[k], bt.a[k].y, dpc * cols[k] * sizeof(double), cudaMemcpyDeviceToHost, ks->stream);
+      if (e != cudaSuccess) return cuda_fail(ctx, e, "copy out");
+    }
+    return bg_kset_sync(ks);
+  }
+  return BG_OK;
+}
+
+int bg_kset_sync(bg_kset* ks) {
+  if (!ks) return BG_EINVAL;
+  cudaError_t e = cudaStreamSynchronize(ks->stream);
+  if (e != cudaSuccess) return cuda_fail(ks->ctx, e, "k-point set");
+  int bad = 0;
+  for (bg_op* op : ks->ops) {
+    e = cudaMemcpy(op->err_host, op->t.err, sizeof(int), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cuda_fail(ks->ctx, e, "k-point set");
+    if (op->err_host[0]) {
+      bad = 1;
+      cudaMemset(op->t.err, 0, sizeof(int));
+    }
+  }
+  if (bad) return fail(ks->ctx, BG_ENONFINITE, "non-finite input coefficient");
+  return BG_OK;
+}
+
+int bg_kset_stream(const bg_kset* ks, void** stream) {
+  if (!ks || !stream) return BG_EINVAL;
+  *stream = ks->stream;
+  return BG_OK;
+}
+
+int bg_kset_set_stream(bg_kset* ks, void* stream) {
+  if (!ks) return BG_EINVAL;
+  if (ks->own_stream && ks->stream) {
+    cudaStreamSynchronize(ks->stream);
+    cudaStreamDestroy(ks->stream);
+  }
+  ks->own_stream = false;
+  ks->stream = static_cast<cudaStream_t>(stream);
+  return BG_OK;
+}
+
+int bg_kset_launches(const bg_kset* ks, int64_t* launches) {
+  if (!ks || !launches) return BG_EINVAL;
+  *launches = ks->launches;
+  return BG_OK;
+}
+
+int bg_kset_profile(bg_kset* ks, int32_t enable) {
+  if (!ks) return BG_EINVAL;
+  ks->ev.on = enable != 0;
+  return BG_OK;
+}
+
+int bg_kset_stage_times(bg_kset* ks, double* ms) {
+  if (!ks) return BG_EINVAL;
+  return stage_times(ks->ctx, ks->stream, ks->ev, ms);
 }
 
 // ------------------------------------------------------------------ setup ABI

@@ -54,28 +54,48 @@ struct CallArgs {
   int units;        // complex columns or column pairs
 };
 
+// One launch covers up to kMaxBatch operators (k points) of the same grid; operator
+// b of a launch works on blockIdx.z (local passes) with its own tables and blocks.
+constexpr int kMaxBatch = 64;
+struct Batch {
+  int nk;
+  CallArgs a[kMaxBatch];
+};
+
 // Nonlocal operands of one operator.
-struct NlTables {
-  int nproj;
-  int natoms;
-  int maxch;
+struct NlDev {
   const double* p;        // complex: 2*npw*nproj interleaved col-major; Gamma: real ORC n*nproj
+  double* part;           // split-K partials [ks][col][nproj] (complex: x2)
+  double* wd;             // coupled projections [col][nproj] (complex: x2)
   const int* atom_off;    // natoms+1 projector column offsets
   const int* d_off;       // natoms coupling offsets
   const double* d;        // concatenated row-major D blocks
-  double* part;           // split-K partials [ks][col][nproj] (complex: x2)
-  double* wd;             // coupled projections [col][nproj] (complex: x2)
-  int ksplit;
-  int kchunk;
+  int rows;
+};
+
+struct NlShape {
+  int nproj, natoms, maxch;
+  int ksplit, kchunk;
+};
+
+// Optional CUDA-event timing of every stage of an apply (stage s brackets its
+// launch between ev[2s] and ev[2s+1] on the launching stream).
+constexpr int kStages = 6;  // sticks_inverse, planes, sticks_forward, project, couple, back
+struct StageEvents {
+  bool on = false;
+  cudaEvent_t ev[2 * kStages] = {};
 };
 
 // Enqueue the local + kinetic part: y = gather(FFT(V IFFT(scatter x)))/N + T x.
-// Returns the number of kernel launches.
-int launch_local(const OpTables& t, const BoxGeo& g, const CallArgs& a, cudaStream_t s);
+// tabs: device array of b.nk operator tables.  Returns the number of launches.
+int launch_local(const OpTables* tabs, int gamma, int max_groups, const BoxGeo& g, const Batch& b, cudaStream_t s,
+                 StageEvents* ev);
 // Enqueue y += P (D (P^H x)) (complex) or y += P (D (P^T x)) (Gamma).
-int launch_nonlocal(const OpTables& t, const NlTables& nl, const CallArgs& a, cudaStream_t s);
+int launch_nonlocal(const NlDev* nl, int gamma, const NlShape& sh, int max_rows, const Batch& b, cudaStream_t s,
+                    StageEvents* ev);
 
 size_t plane_smem_bytes(const BoxGeo& g);
 size_t stick_smem_bytes(const BoxGeo& g);
+int configure_kernels(size_t plane_smem, size_t stick_smem);
 
 }  // namespace bg

@@ -45,7 +45,9 @@ __device__ __forceinline__ bool finite2(double a, double b) { return isfinite(a)
 
 // ---------------------------------------------------------------- pass 1
 template <bool GAMMA>
-__global__ void __launch_bounds__(256) k_sticks_inverse(OpTables t, BoxGeo g, CallArgs a) {
+__global__ void __launch_bounds__(256) k_sticks_inverse(const OpTables* __restrict__ tabs, BoxGeo g, Batch b) {
+  const OpTables& t = tabs[blockIdx.z];
+  const CallArgs& a = b.a[blockIdx.z];
   const int grp = blockIdx.x, unit = blockIdx.y;
   if (grp >= t.ngroups || unit >= a.units) return;
   extern __shared__ double2 sm[];
@@ -97,7 +99,9 @@ __global__ void __launch_bounds__(256) k_sticks_inverse(OpTables t, BoxGeo g, Ca
 }
 
 // ---------------------------------------------------------------- pass 2
-__global__ void __launch_bounds__(512) k_planes(OpTables t, BoxGeo g, CallArgs a) {
+__global__ void __launch_bounds__(512) k_planes(const OpTables* __restrict__ tabs, BoxGeo g, Batch b) {
+  const OpTables& t = tabs[blockIdx.z];
+  const CallArgs& a = b.a[blockIdx.z];
   const int unit = blockIdx.x, z = blockIdx.y;
   if (unit >= a.units) return;
   extern __shared__ double2 sm[];
@@ -129,7 +133,9 @@ __global__ void __launch_bounds__(512) k_planes(OpTables t, BoxGeo g, CallArgs a
 
 // ---------------------------------------------------------------- pass 3
 template <bool GAMMA>
-__global__ void __launch_bounds__(256) k_sticks_forward(OpTables t, BoxGeo g, CallArgs a) {
+__global__ void __launch_bounds__(256) k_sticks_forward(const OpTables* __restrict__ tabs, BoxGeo g, Batch b) {
+  const OpTables& t = tabs[blockIdx.z];
+  const CallArgs& a = b.a[blockIdx.z];
   const int grp = blockIdx.x, unit = blockIdx.y;
   if (grp >= t.ngroups || unit >= a.units) return;
   extern __shared__ double2 sm[];
@@ -222,11 +228,20 @@ struct Ops<double2> {
 
 // part[ks][c][p] = sum_{rows of chunk ks} P[p][row]^* X[c][row]; tile 32 p x 32 c.
 template <class T>
-__global__ void __launch_bounds__(256) k_project(const T* __restrict__ P, int rows, int nproj, const T* __restrict__ X,
-                                                 int64_t ldx, int cols, T* __restrict__ part, int kchunk) {
+__global__ void __launch_bounds__(256) k_project(const NlDev* __restrict__ nls, int nproj, int ksplit, int kchunk,
+                                                 Batch b) {
   __shared__ T As[32][33];
   __shared__ T Bs[32][33];
-  const int p0 = blockIdx.x * 32, c0 = blockIdx.y * 32, ks = blockIdx.z;
+  const int kb = blockIdx.z / ksplit, ks = blockIdx.z - kb * ksplit;
+  const NlDev& nl = nls[kb];
+  const CallArgs& ca = b.a[kb];
+  const int cols = ca.cols, rows = nl.rows;
+  if ((int)blockIdx.y * 32 >= cols) return;
+  const T* __restrict__ P = reinterpret_cast<const T*>(nl.p);
+  const T* __restrict__ X = reinterpret_cast<const T*>(ca.x);
+  const int64_t ldx = ca.ldx / (int64_t)(sizeof(T) / sizeof(double));
+  T* __restrict__ part = reinterpret_cast<T*>(nl.part);
+  const int p0 = blockIdx.x * 32, c0 = blockIdx.y * 32;
   const int tp = threadIdx.x & 15, tc = threadIdx.x >> 4;
   T acc[2][2];
 #pragma unroll
@@ -264,10 +279,17 @@ __global__ void __launch_bounds__(256) k_project(const T* __restrict__ P, int ro
 
 // wd[c][off+i] = sum_j D[i][j] (sum_ks part[ks][c][off+j]) for one (atom, column).
 template <class T>
-__global__ void k_couple(const T* __restrict__ part, int ksplit, int cols, int nproj, const int* __restrict__ atom_off,
-                         const int* __restrict__ d_off, const double* __restrict__ d, T* __restrict__ wd) {
+__global__ void k_couple(const NlDev* __restrict__ nls, int nproj, int ksplit, Batch b) {
   __shared__ T w[64];
+  const NlDev& nl = nls[blockIdx.z];
+  const int cols = b.a[blockIdx.z].cols;
   const int atom = blockIdx.x, c = blockIdx.y;
+  if (c >= cols) return;
+  const T* __restrict__ part = reinterpret_cast<const T*>(nl.part);
+  T* __restrict__ wd = reinterpret_cast<T*>(nl.wd);
+  const int* __restrict__ atom_off = nl.atom_off;
+  const int* __restrict__ d_off = nl.d_off;
+  const double* __restrict__ d = nl.d;
   const int off = atom_off[atom], cnt = atom_off[atom + 1] - off;
   const int i = threadIdx.x;
   if (i < cnt) {
@@ -286,11 +308,18 @@ __global__ void k_couple(const T* __restrict__ part, int ksplit, int cols, int n
 
 // y[c][row] += sum_p P[p][row] wd[c][p]; tile 64 rows x 32 columns.
 template <class T>
-__global__ void __launch_bounds__(256) k_back(const T* __restrict__ P, int rows, int nproj, const T* __restrict__ wd,
-                                              int cols, T* __restrict__ Y, int64_t ldy) {
+__global__ void __launch_bounds__(256) k_back(const NlDev* __restrict__ nls, int nproj, Batch b) {
   __shared__ T Ps[16][64];
   __shared__ T Ws[16][33];
+  const NlDev& nl = nls[blockIdx.z];
+  const CallArgs& ca = b.a[blockIdx.z];
+  const int cols = ca.cols, rows = nl.rows;
   const int r0 = blockIdx.x * 64, c0 = blockIdx.y * 32;
+  if (r0 >= rows || c0 >= cols) return;
+  const T* __restrict__ P = reinterpret_cast<const T*>(nl.p);
+  const T* __restrict__ wd = reinterpret_cast<const T*>(nl.wd);
+  T* __restrict__ Y = reinterpret_cast<T*>(ca.y);
+  const int64_t ldy = ca.ldy / (int64_t)(sizeof(T) / sizeof(double));
   const int tg = threadIdx.x & 31, tc = threadIdx.x >> 5;
   T acc[2][4];
 #pragma unroll
@@ -338,41 +367,57 @@ __global__ void __launch_bounds__(256) k_back(const T* __restrict__ P, int rows,
 size_t plane_smem_bytes(const BoxGeo& g) { return sizeof(double2) * ((size_t)g.n0 + g.n1 + (size_t)g.n0 * g.pitch); }
 size_t stick_smem_bytes(const BoxGeo& g) { return sizeof(double2) * ((size_t)g.n2 + (size_t)g.sg * g.ld2); }
 
-int launch_local(const OpTables& t, const BoxGeo& g, const CallArgs& a, cudaStream_t s) {
-  if (a.units == 0) return 0;
+namespace {
+struct StageScope {
+  StageEvents* ev;
+  int s;
+  cudaStream_t st;
+  StageScope(StageEvents* e, int stage, cudaStream_t stream) : ev(e), s(stage), st(stream) {
+    if (ev && ev->on) cudaEventRecord(ev->ev[2 * s], st);
+  }
+  ~StageScope() {
+    if (ev && ev->on) cudaEventRecord(ev->ev[2 * s + 1], st);
+  }
+};
+}  // namespace
+
+int launch_local(const OpTables* tabs, int gamma, int max_groups, const BoxGeo& g, const Batch& b, cudaStream_t s,
+                 StageEvents* ev) {
+  int max_units = 0;
+  for (int k = 0; k < b.nk; ++k) max_units = max(max_units, b.a[k].units);
+  if (max_units == 0 || b.nk == 0) return 0;
   const size_t ss = stick_smem_bytes(g), ps = plane_smem_bytes(g);
-  const dim3 sgrid(t.ngroups, a.units);
-  const dim3 pgrid(a.units, g.n2);
-  if (t.gamma) {
-    k_sticks_inverse<true><<<sgrid, 256, ss, s>>>(t, g, a);
-    k_planes<<<pgrid, 512, ps, s>>>(t, g, a);
-    k_sticks_forward<true><<<sgrid, 256, ss, s>>>(t, g, a);
+  const dim3 sgrid(max_groups, max_units, b.nk);
+  const dim3 pgrid(max_units, g.n2, b.nk);
+  if (gamma) {
+    { StageScope sc(ev, 0, s); k_sticks_inverse<true><<<sgrid, 256, ss, s>>>(tabs, g, b); }
+    { StageScope sc(ev, 1, s); k_planes<<<pgrid, 512, ps, s>>>(tabs, g, b); }
+    { StageScope sc(ev, 2, s); k_sticks_forward<true><<<sgrid, 256, ss, s>>>(tabs, g, b); }
   } else {
-    k_sticks_inverse<false><<<sgrid, 256, ss, s>>>(t, g, a);
-    k_planes<<<pgrid, 512, ps, s>>>(t, g, a);
-    k_sticks_forward<false><<<sgrid, 256, ss, s>>>(t, g, a);
+    { StageScope sc(ev, 0, s); k_sticks_inverse<false><<<sgrid, 256, ss, s>>>(tabs, g, b); }
+    { StageScope sc(ev, 1, s); k_planes<<<pgrid, 512, ps, s>>>(tabs, g, b); }
+    { StageScope sc(ev, 2, s); k_sticks_forward<false><<<sgrid, 256, ss, s>>>(tabs, g, b); }
   }
   return 3;
 }
 
-int launch_nonlocal(const OpTables& t, const NlTables& nl, const CallArgs& a, cudaStream_t s) {
-  if (nl.nproj == 0 || a.cols == 0) return 0;
-  const dim3 pg((nl.nproj + 31) / 32, (a.cols + 31) / 32, nl.ksplit);
-  const dim3 cg(nl.natoms, a.cols);
-  const dim3 bg_((t.rows + 63) / 64, (a.cols + 31) / 32);
-  const int cth = ((nl.maxch + 31) / 32) * 32;
-  if (t.gamma) {
-    k_project<double><<<pg, 256, 0, s>>>(nl.p, t.rows, nl.nproj, a.x, a.ldx, a.cols, nl.part, nl.kchunk);
-    k_couple<double><<<cg, cth, 0, s>>>(nl.part, nl.ksplit, a.cols, nl.nproj, nl.atom_off, nl.d_off, nl.d, nl.wd);
-    k_back<double><<<bg_, 256, 0, s>>>(nl.p, t.rows, nl.nproj, nl.wd, a.cols, a.y, a.ldy);
+int launch_nonlocal(const NlDev* nl, int gamma, const NlShape& sh, int max_rows, const Batch& b, cudaStream_t s,
+                    StageEvents* ev) {
+  int max_cols = 0;
+  for (int k = 0; k < b.nk; ++k) max_cols = max(max_cols, b.a[k].cols);
+  if (sh.nproj == 0 || max_cols == 0 || b.nk == 0) return 0;
+  const dim3 pg((sh.nproj + 31) / 32, (max_cols + 31) / 32, sh.ksplit * b.nk);
+  const dim3 cg(sh.natoms, max_cols, b.nk);
+  const dim3 bg_((max_rows + 63) / 64, (max_cols + 31) / 32, b.nk);
+  const int cth = ((sh.maxch + 31) / 32) * 32;
+  if (gamma) {
+    { StageScope sc(ev, 3, s); k_project<double><<<pg, 256, 0, s>>>(nl, sh.nproj, sh.ksplit, sh.kchunk, b); }
+    { StageScope sc(ev, 4, s); k_couple<double><<<cg, cth, 0, s>>>(nl, sh.nproj, sh.ksplit, b); }
+    { StageScope sc(ev, 5, s); k_back<double><<<bg_, 256, 0, s>>>(nl, sh.nproj, b); }
   } else {
-    const double2* P = reinterpret_cast<const double2*>(nl.p);
-    double2* part = reinterpret_cast<double2*>(nl.part);
-    double2* wd = reinterpret_cast<double2*>(nl.wd);
-    k_project<double2><<<pg, 256, 0, s>>>(P, t.rows, nl.nproj, reinterpret_cast<const double2*>(a.x), a.ldx / 2,
-                                          a.cols, part, nl.kchunk);
-    k_couple<double2><<<cg, cth, 0, s>>>(part, nl.ksplit, a.cols, nl.nproj, nl.atom_off, nl.d_off, nl.d, wd);
-    k_back<double2><<<bg_, 256, 0, s>>>(P, t.rows, nl.nproj, wd, a.cols, reinterpret_cast<double2*>(a.y), a.ldy / 2);
+    { StageScope sc(ev, 3, s); k_project<double2><<<pg, 256, 0, s>>>(nl, sh.nproj, sh.ksplit, sh.kchunk, b); }
+    { StageScope sc(ev, 4, s); k_couple<double2><<<cg, cth, 0, s>>>(nl, sh.nproj, sh.ksplit, b); }
+    { StageScope sc(ev, 5, s); k_back<double2><<<bg_, 256, 0, s>>>(nl, sh.nproj, b); }
   }
   return 3;
 }

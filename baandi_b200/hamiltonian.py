@@ -20,6 +20,9 @@ from . import _lib as L
 from .operands import NonlocalTable, PlaneWaves
 
 
+STAGES = ("sticks_inverse", "planes", "sticks_forward", "project", "couple", "back")
+
+
 class SolverError(RuntimeError):
     """Reference SolverError::InvalidParameter / Application (crates/dft-solvers/src/lib.rs:42-57)."""
 
@@ -141,6 +144,16 @@ class _Operator:
         self._check(self._lib.bg_op_launches(self.handle, ctypes.byref(n)))
         return n.value
 
+    def profile(self, enable: bool = True):
+        """Record CUDA events around every stage of the following applies."""
+        self._check(self._lib.bg_op_profile(self.handle, 1 if enable else 0))
+
+    def stage_times(self) -> np.ndarray:
+        """Milliseconds of the last apply's six stages (STAGES order)."""
+        out = np.zeros(len(STAGES))
+        self._check(self._lib.bg_op_stage_times(self.handle, _p(out)))
+        return out
+
     def close(self):
         if getattr(self, "handle", None):
             self._lib.bg_op_destroy(self.handle)
@@ -233,3 +246,78 @@ def _apply_torch(op, x, out, complex_rows):
         raise SolverError(L.BG_ESHAPE, "out must match x")
     op._apply_raw(x.data_ptr(), out.data_ptr(), x.shape[0], L.BG_PTR_DEVICE)
     return out
+
+
+class KPointSet:
+    """Several k-point operators of one grid applied in one batched launch per stage
+    (bg_kset_*).  The reference applies them one after another
+    (crates/dft-engine/src/refscf/k_map.rs:136-210); results are identical to the
+    per-operator applies."""
+
+    def __init__(self, ops, ctx: Context | None = None):
+        self.ctx = ctx or ops[0].ctx
+        self._lib = self.ctx._lib
+        self.ops = list(ops)
+        arr = (ctypes.c_void_p * len(ops))(*[o.handle.value for o in ops])
+        h = ctypes.c_void_p()
+        rc = self._lib.bg_kset_create(self.ctx.handle, len(ops), ctypes.cast(arr, ctypes.c_void_p), ctypes.byref(h))
+        if rc != L.BG_OK:
+            raise SolverError(rc, f"{L.CODE_NAMES.get(rc, rc)}: {L.last_error(self.ctx.handle)}")
+        self.handle = h
+
+    def _check(self, rc):
+        if rc != L.BG_OK:
+            raise SolverError(rc, f"{L.CODE_NAMES.get(rc, rc)}: {L.last_error(self.ctx.handle)}")
+
+    def apply_raw(self, x_ptrs, y_ptrs, cols, kind):
+        n = len(self.ops)
+        xa = (ctypes.c_void_p * n)(*x_ptrs)
+        ya = (ctypes.c_void_p * n)(*y_ptrs)
+        ca = (ctypes.c_int64 * n)(*[int(c) for c in cols])
+        self._check(self._lib.bg_kset_apply(self.handle, ctypes.cast(xa, ctypes.c_void_p),
+                                            ctypes.cast(ya, ctypes.c_void_p), ctypes.cast(ca, ctypes.c_void_p),
+                                            kind, L.BG_PREC_FP64))
+
+    def apply_blocks(self, xs, outs=None):
+        """Host blocks (list of Fortran-ordered arrays, one per operator) -> list of H x."""
+        if isinstance(xs[0], np.ndarray):
+            xin = [np.asfortranarray(x) for x in xs]
+            ys = outs if outs is not None else [np.zeros_like(x, order="F") for x in xin]
+            self.apply_raw([x.ctypes.data for x in xin], [y.ctypes.data for y in ys], [x.shape[1] for x in xin],
+                           L.BG_PTR_HOST)
+            return ys
+        import torch
+        ys = outs if outs is not None else [torch.empty_like(x) for x in xs]
+        self.apply_raw([x.data_ptr() for x in xs], [y.data_ptr() for y in ys], [x.shape[0] for x in xs],
+                       L.BG_PTR_DEVICE)
+        return ys
+
+    def set_stream(self, stream_ptr: int):
+        self._check(self._lib.bg_kset_set_stream(self.handle, ctypes.c_void_p(stream_ptr)))
+
+    def sync(self):
+        self._check(self._lib.bg_kset_sync(self.handle))
+
+    def launches(self) -> int:
+        n = ctypes.c_int64()
+        self._check(self._lib.bg_kset_launches(self.handle, ctypes.byref(n)))
+        return n.value
+
+    def profile(self, enable: bool = True):
+        self._check(self._lib.bg_kset_profile(self.handle, 1 if enable else 0))
+
+    def stage_times(self) -> np.ndarray:
+        out = np.zeros(len(STAGES))
+        self._check(self._lib.bg_kset_stage_times(self.handle, _p(out)))
+        return out
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self._lib.bg_kset_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,402 @@
+#!/usr/bin/env python
+"""Hamiltonian-apply benchmark: H psi throughput in bands/s on one B200 per rank.
+
+One step applies H to every k point of the workload, 2*bands columns each (the Davidson
+block width at capacity), through one batched launch per stage (bg_kset_apply).  The
+default workload is Si8 in the conventional cube, 4x4x4 k mesh reduced to 36 k points,
+40 Ry, 24 bands: 36 x 48 = 1728 band applies per step, FP64.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload si8]
+
+Prints ONE JSON line on rank 0.  `value` is device-timed (CUDA events on the launching
+stream, inputs resident in HBM, L2 flushed between timed steps); `e2e` is the same
+metric through the public API with pinned host buffers (host->device copy of the step's
+inputs and device->host copy of H x inside the timed region).  `--impl reference` times
+the CPU restatement of the reference's apply on the host cores (the reference itself is
+Rust and cannot be built here).  Multi-GPU: every rank applies its own replica of the
+workload (independent k-point sets, no data-path collective; weak scaling); timing is
+the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+STAGES = ("sticks_inverse", "planes", "sticks_forward", "project", "couple", "back")
+KERNELS = {"sticks_inverse": "k_sticks_inverse", "planes": "k_planes", "sticks_forward": "k_sticks_forward",
+           "project": "k_project", "couple": "k_couple", "back": "k_back"}
+
+
+def parse_args(argv=None):
+    p = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    p.add_argument("--workload", default="si8")
+    p.add_argument("--cpu-seconds", type=float, default=10.0, help="bound of the CPU baseline sample")
+    return p.parse_args(argv)
+
+
+# ---------------------------------------------------------------- distributed plumbing
+def dist_env():
+    return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), int(
+        os.environ.get("LOCAL_RANK", "0"))
+
+
+def dist_init(world, backend="nccl"):
+    if world <= 1:
+        return None
+    import datetime
+
+    import torch.distributed as dist
+    dist.init_process_group(backend, timeout=datetime.timedelta(seconds=180))
+    return dist
+
+
+def max_over_ranks(value: float, dist, device=None) -> float:
+    """Max of a per-rank float over all ranks (identity on one rank)."""
+    if dist is None:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def shard_seeds(rank: int, base: int = 2028) -> int:
+    """Each rank's replica uses its own seeded inputs (independent objects)."""
+    return base + 1000 * rank
+
+
+# ---------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi samples (200 ms) of SM clock, power and throttle reasons."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.file, stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.file.flush()
+        rows = []
+        with open(self.file.name) as f:
+            for line in f:
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.file.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows),
+                "power_w_max": max(float(r[3]) for r in rows if r[3].replace(".", "").isdigit())
+                if any(r[3].replace(".", "").isdigit() for r in rows) else None}
+
+
+# ---------------------------------------------------------------- workload
+def build_workload(name: str):
+    from baandi_b200 import systems
+    w = systems.WORKLOADS[name]()
+    if w.gamma_real:
+        raise SystemExit("bench workloads use the complex k-point path")
+    return w
+
+
+def sticks_of(pw, dims):
+    from baandi_b200 import operands
+    idx = operands.fft_index(pw.miller, dims, pw.gamma)
+    return len(np.unique(idx // dims[2]))
+
+
+def stage_bytes(shapes, dims, cols, nproj):
+    """Algorithmic HBM bytes per launch of each stage over the whole k-point set.
+    shapes: [(npw, S)] per k point; complex FP64 (16 B per value)."""
+    n2 = dims[2]
+    n3 = dims[0] * dims[1] * dims[2]
+    out = dict.fromkeys(STAGES, 0.0)
+    for npw, S in shapes:
+        stick = 16.0 * S * n2 * cols          # one pass over the stick buffer
+        out["sticks_inverse"] += 16.0 * npw * cols + stick
+        out["planes"] += 2.0 * stick + 8.0 * n3
+        out["sticks_forward"] += stick + 2.0 * 16.0 * npw * cols
+        out["project"] += 16.0 * npw * (nproj + cols)
+        out["back"] += 16.0 * npw * (nproj + 2.0 * cols)
+        out["couple"] += 16.0 * nproj * cols * 2
+    return out
+
+
+def stage_flops(shapes, dims, cols, nproj, xact_frac):
+    """Nominal FP64 flops per launch (5 n log2 n per complex line; 8 per complex MAC)."""
+    import math
+    n0, n1, n2 = dims
+    f = dict.fromkeys(STAGES, 0.0)
+    line = lambda n: 5.0 * n * math.log2(n)
+    for npw, S in shapes:
+        f["sticks_inverse"] += cols * S * line(n2)
+        f["sticks_forward"] += cols * S * line(n2)
+        f["planes"] += cols * n2 * 2.0 * (xact_frac * n0 * line(n1) + n1 * line(n0))
+        f["project"] += 8.0 * npw * nproj * cols
+        f["back"] += 8.0 * npw * nproj * cols
+    return f
+
+
+def load_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as fh:
+            d = json.load(fh)
+        return float(d["hbm_gbs"]), float(d["bf16_tflops"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, 1590.0, "fallback"
+
+
+def load_traffic(kernel: str, workload: str):
+    path = os.path.join(ROOT, "profiles", "traffic.json")
+    try:
+        with open(path) as fh:
+            d = json.load(fh)
+        e = d.get(workload, {}).get(kernel)
+        return float(e) if e is not None else None
+    except (OSError, ValueError):
+        return None
+
+
+# ---------------------------------------------------------------- CPU arm
+def cpu_sample(w, kpts, cols, budget_s, threads):
+    """Time the oracle's C++ FP64 restatement of the apply on a bounded sample of the
+    workload; returns (bands/s, sample description, seconds)."""
+    from oracle import oracle as OR
+    from oracle import setup_ref as S
+    dims = w.dims()
+    v = w.ionic_potential()
+    cell = S.Cell(w.rows)
+    species = []
+    for s in w.species:
+        p = s.pseudo
+        ps = S.Pseudo(p.z, p.r, p.rab, p.local, [S.Projector(l, u) for l, u in zip(p.l, p.beta)], p.dij)
+        species.append(S.Species(ps, s.positions))
+    done_bands, spent, used = 0, 0.0, 0
+    for (k, _) in kpts:
+        b = S.basis_at_k(cell, w.ecut_ha, k)
+        nl = S.nonlocal_table(b, cell.volume, species)
+        idx = S.fft_flat(S.g_to_fft(b, dims), dims)
+        x = w.random_block(b.npw, cols, seed_offset=used)
+        t0 = time.perf_counter()
+        OR.apply_complex(dims, idx, v, 0.5 * b.kpg2, nl, x, threads=threads)
+        spent += time.perf_counter() - t0
+        done_bands += cols
+        used += 1
+        if spent >= budget_s:
+            break
+    return done_bands / spent, f"{used} of {len(kpts)} k points x {cols} columns", spent
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return 0
+    w = build_workload(args.workload)
+    cols = 2 * w.bands
+    threads = len(os.sched_getaffinity(0))
+    per_step_budget = max(1.0, min(8.0, 150.0 / max(1, args.steps + args.warmup)))
+    for _ in range(args.warmup):
+        cpu_sample(w, w.kpoints[:1], cols, 0.0, threads)
+    rates, samples = [], []
+    for _ in range(args.steps):
+        rate, desc, _ = cpu_sample(w, w.kpoints, cols, per_step_budget, threads)
+        rates.append(rate)
+        samples.append(desc)
+    value = statistics.median(rates)
+    line = {
+        "impl": "reference", "metric": "H psi apply throughput (FP64)", "value": value, "unit": "bands/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1000.0 * len(w.kpoints) * cols / value, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": w.name, "kpoints": len(w.kpoints), "columns_per_k": cols, "grid": w.dims()},
+        "cpu_baseline": {"value": value, "unit": "bands/s", "cores": threads, "kind": "port",
+                         "sample": samples[0] + " per step (oracle C++ FP64 restatement, OpenMP over columns)"},
+        "e2e": {"value": value, "unit": "bands/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------- GPU arm
+def run_ours(args):
+    import torch
+
+    from baandi_b200 import hamiltonian as H
+
+    rank, world, local = dist_env()
+    if not torch.cuda.is_available():
+        raise SystemExit("bench.py needs a CUDA device")
+    torch.cuda.set_device(local)
+    dist = dist_init(world)
+    w = build_workload(args.workload)
+    w.seed = shard_seeds(rank, w.seed)
+    dims = w.dims()
+    cols = 2 * w.bands
+    v = w.ionic_potential()
+    ctx = H.Context(local)
+    ops, xs, ys, shapes = [], [], [], []
+    for i, (k, _) in enumerate(w.kpoints):
+        pw = w.plane_waves(k)
+        nl = w.nonlocal_table(pw)
+        op = H.ComplexHamiltonian.new_owned(pw, dims, nl, cols, ctx)
+        op.set_owned_potential(v, 1)
+        ops.append(op)
+        shapes.append((pw.npw, sticks_of(pw, dims)))
+        x = w.random_block(pw.npw, cols, seed_offset=i)
+        xs.append(torch.from_numpy(np.ascontiguousarray(x.T)).cuda())
+        ys.append(torch.empty_like(xs[-1]))
+    nproj = int(nl.table.shape[1])
+    kset = H.KPointSet(ops, ctx)
+    stream = torch.cuda.current_stream()
+    kset.set_stream(stream.cuda_stream)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    for _ in range(max(3, args.warmup)):
+        kset.apply_blocks(xs, ys)
+    torch.cuda.synchronize()
+    kset.profile(True)
+    stage_ms = np.zeros(len(STAGES))
+    launches0 = kset.launches()
+    sampler = ClockSampler(local)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    sampler.start()
+    step_ms = []
+    for _ in range(args.steps):
+        flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        kset.apply_blocks(xs, ys)
+        e1.record(stream)
+        e1.synchronize()
+        step_ms.append(e0.elapsed_time(e1))
+        stage_ms += kset.stage_times()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clocks = sampler.stop()
+    launches = kset.launches() - launches0
+    kset.profile(False)
+    kset.sync()
+    total_ms = max_over_ranks(float(sum(step_ms)), dist, "cuda")
+    bands_step = len(w.kpoints) * cols
+    value = bands_step * args.steps * world / (total_ms / 1000.0)
+
+    # end to end through the public API with pinned host buffers
+    hx, hy = [], []
+    for x in xs:
+        hx_t = torch.empty(x.shape, dtype=x.dtype, pin_memory=True)
+        hx_t.copy_(x)
+        hx.append(hx_t.numpy().T)
+        hy.append(torch.empty(x.shape, dtype=x.dtype, pin_memory=True).numpy().T)
+    kset.set_stream(0)
+    for _ in range(2):
+        kset.apply_blocks(hx, hy)
+    if dist:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        kset.apply_blocks(hx, hy)
+    e2e_s = max_over_ranks(time.perf_counter() - t0, dist, "cuda")
+    e2e_value = bands_step * args.steps * world / e2e_s
+    h2d = sum(x.nbytes for x in hx)
+    d2h = sum(y.nbytes for y in hy)
+
+    # roofline of the dominant kernel
+    hbm_peak, _, peak_kind = load_peaks()
+    sbytes = stage_bytes(shapes, dims, cols, nproj)
+    xact = 0.5
+    sflops = stage_flops(shapes, dims, cols, nproj, xact)
+    avg_ms = stage_ms / args.steps
+    dom = int(np.argmax(avg_ms))
+    dname = STAGES[dom]
+    achieved = sbytes[dname] / (avg_ms[dom] / 1000.0) / 1e9
+    traffic = load_traffic(KERNELS[dname], w.name)
+    roofline = {"bound": "hbm", "kernel": KERNELS[dname], "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+                "frac": achieved / hbm_peak, "peak_kind": peak_kind, "traffic": traffic,
+                "algorithmic_bytes_per_launch": sbytes[dname],
+                "fp64_tflops": sflops[dname] / (avg_ms[dom] / 1000.0) / 1e12,
+                "stage_ms": {s: float(m) for s, m in zip(STAGES, avg_ms)}}
+
+    # CPU baseline: rank 0, N=1 only
+    cpu = None
+    if rank == 0 and world == 1:
+        threads = len(os.sched_getaffinity(0))
+        rate, desc, spent = cpu_sample(w, w.kpoints, cols, args.cpu_seconds, threads)
+        cpu = {"value": rate, "unit": "bands/s", "cores": threads, "kind": "port",
+               "sample": desc + f" ({spent:.1f} s; oracle C++ FP64 restatement, OpenMP over columns)"}
+    if rank == 0:
+        line = {
+            "metric": "H psi apply throughput (FP64)", "value": value, "unit": "bands/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": w.name, "kpoints": len(w.kpoints), "columns_per_k": cols, "grid": dims,
+                       "npw_min": min(s[0] for s in shapes), "npw_max": max(s[0] for s in shapes),
+                       "nproj": nproj, "l2": "flushed between timed steps (256 MiB write)",
+                       "parallelism": f"replica x{world}"},
+            "e2e": {"value": e2e_value, "unit": "bands/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "gpu_launches": launches, "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    kset.close()
+    for op in ops:
+        op.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main(argv=None):
+    args = parse_args(argv)
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -106,9 +106,10 @@ int bg_op_set_potential(bg_op* op, const double* v_grid, uint64_t epoch);
 /* Replaces apply_block (distributed_complex.rs:340-386; distributed_real_gamma.rs:
  * 1062-1264): y = H x, y completely overwritten.  rows must equal the operator's row
  * count (npw), 0 <= cols <= capacity.  Complex operators take interleaved complex
- * columns, the Gamma operator real ORC columns.  ptr_kind BG_PTR_HOST: synchronous,
- * x is checked finite (BG_ENONFINITE) before any work.  BG_PTR_DEVICE: enqueued on
- * the operator's stream; x must not alias y. */
+ * columns, the Gamma operator real ORC columns.  ptr_kind BG_PTR_HOST: synchronous;
+ * a non-finite x returns BG_ENONFINITE (y is then unspecified).  BG_PTR_DEVICE:
+ * enqueued on the operator's stream, a non-finite x is reported by bg_op_sync; x must
+ * not alias y. */
 int bg_op_apply_block(bg_op* op, const double* x, double* y, int64_t rows, int64_t cols,
                       int32_t ptr_kind, int32_t precision);
 
@@ -128,6 +129,34 @@ int bg_op_set_stream(bg_op* op, void* stream);
 int bg_op_sync(bg_op* op);
 /* Count of this library's kernel launches issued by the operator so far. */
 int bg_op_launches(const bg_op* op, int64_t* launches);
+
+/* Per-stage CUDA-event timing (tracing): when enabled, every apply records events
+ * around its six launches (sticks_inverse, planes, sticks_forward, project, couple,
+ * back); stage_times waits for the stream and returns the last apply's stage times in
+ * milliseconds (ms[6]). */
+int bg_op_profile(bg_op* op, int32_t enable);
+int bg_op_stage_times(bg_op* op, double* ms);
+
+/* ------------------------------------------------------------ k-point sets */
+/* All bands of several k points in one launch per stage.  The reference solves the k
+ * points of a map one after another (crates/dft-engine/src/refscf/k_map.rs:136-210,
+ * each calling apply_block of its own DistributedComplexHamiltonian); a set keeps
+ * each operator's tables and applies every operator's block in one batched launch.
+ * Operators must share the context, grid, kind and projector layout; 1..64 of them.
+ * The set borrows the operators: destroy it before them. */
+typedef struct bg_kset bg_kset;
+int bg_kset_create(bg_ctx* ctx, int32_t n, bg_op* const* ops, bg_kset** out);
+int bg_kset_destroy(bg_kset* set);
+/* y[k] = H_k x[k] for every operator k of the set (cols[k] columns, 0 allowed);
+ * pointer kinds and precision as bg_op_apply_block. */
+int bg_kset_apply(bg_kset* set, const double* const* x, double* const* y, const int64_t* cols,
+                  int32_t ptr_kind, int32_t precision);
+int bg_kset_sync(bg_kset* set);
+int bg_kset_stream(const bg_kset* set, void** stream);
+int bg_kset_set_stream(bg_kset* set, void* stream);
+int bg_kset_launches(const bg_kset* set, int64_t* launches);
+int bg_kset_profile(bg_kset* set, int32_t enable);
+int bg_kset_stage_times(bg_kset* set, double* ms);
 
 /* ------------------------------------------------------------ operand builders */
 /* Restatements of the reference setup (host, FP64) for callers without the
