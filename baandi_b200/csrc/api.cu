@@ -546,7 +546,7 @@ int bg_op_set_potential(bg_op* op, const double* v, uint64_t epoch) {
       for (int z = 0; z < n2; ++z) {
         const double w = v[((size_t)x * n1 + y) * n2 + z];
         if (!std::isfinite(w)) return fail(op->ctx, BG_ENONFINITE, "potential not finite");
-        vt[((size_t)z * n0 + x) * n1 + y] = w;
+        vt[((size_t)z * n1 + y) * n0 + x] = w;
       }
   cudaError_t e = cudaMemcpyAsync(const_cast<double*>(op->t.vt), vt.data(), N * sizeof(double),
                                   cudaMemcpyHostToDevice, op->stream);

@@ -1,0 +1,282 @@
+// Compile-time line FFTs for the grid lengths of the benchmark cells (FP64 complex).
+//
+// A pass transforms L lines held in shared memory.  Each warp owns a contiguous block
+// of lines and carries it through every radix stage alone, separated only by
+// __syncwarp, so the block meets at a barrier once per pass instead of once per stage.
+// Each stage is the in-place Stockham decimation-in-time step of fft_dev.cuh (element
+// j + t N/R of butterfly j in, (j / Ns) Ns R + j mod Ns + u Ns out) with every index a
+// constant expression.  A stage runs in rounds of whole lines (32 / (N/R) lines per
+// round, one butterfly per lane): a round loads its butterflies' inputs, __syncwarp,
+// stores the outputs in place, so a lane holds only R values.  Radices 2, 3, 4, 5, 6,
+// 8, 9 and 12; the 6-, 8-, 9- and 12-point DFTs are Cooley-Tukey splits (2x3, 2x4,
+// 3x3, 3x4) done in registers.
+//
+// Twiddles w^(t k N/(Ns R)) come from the length-N table exp(+2 pi i q/N) in shared
+// memory (conjugated for the forward sign).
+#pragma once
+#include "fft_dev.cuh"
+
+namespace bg {
+namespace fast {
+
+// --------------------------------------------------------------------- plans
+template <int N>
+struct Plan {
+  static constexpr bool ok = false;
+};
+#define BG_PLAN(NN, ...)                                    \
+  template <>                                               \
+  struct Plan<NN> {                                         \
+    static constexpr bool ok = true;                        \
+    static constexpr int radix[] = {__VA_ARGS__};           \
+    static constexpr int nst = sizeof(radix) / sizeof(int); \
+  };
+BG_PLAN(25, 5, 5)
+BG_PLAN(45, 5, 9)
+BG_PLAN(54, 6, 9)
+BG_PLAN(60, 12, 5)
+BG_PLAN(72, 8, 9)
+BG_PLAN(108, 12, 9)
+#undef BG_PLAN
+
+// --------------------------------------------------------------------- butterflies
+template <int SIGN>
+__device__ __forceinline__ double2 w_mul(double2 a, double c, double s) {
+  // a * (c + i SIGN s)
+  const double ss = SIGN > 0 ? s : -s;
+  return make_double2(a.x * c - a.y * ss, a.x * ss + a.y * c);
+}
+
+template <int R, int SIGN>
+struct Dft;
+
+template <int SIGN>
+struct Dft<2, SIGN> {
+  __device__ __forceinline__ static void run(double2* v) {
+    const double2 a = v[0], b = v[1];
+    v[0] = cadd(a, b);
+    v[1] = csub(a, b);
+  }
+};
+template <int SIGN>
+struct Dft<3, SIGN> {
+  __device__ __forceinline__ static void run(double2* v) {
+    const double h = 0.8660254037844386;
+    const double2 t1 = cadd(v[1], v[2]);
+    const double2 t2 = make_double2(v[0].x - 0.5 * t1.x, v[0].y - 0.5 * t1.y);
+    const double2 t3 = irot<SIGN>(cscale(csub(v[1], v[2]), h));
+    v[0] = cadd(v[0], t1);
+    v[1] = cadd(t2, t3);
+    v[2] = csub(t2, t3);
+  }
+};
+template <int SIGN>
+struct Dft<4, SIGN> {
+  __device__ __forceinline__ static void run(double2* v) {
+    const double2 a = cadd(v[0], v[2]), b = csub(v[0], v[2]);
+    const double2 c = cadd(v[1], v[3]), d = irot<SIGN>(csub(v[1], v[3]));
+    v[0] = cadd(a, c);
+    v[2] = csub(a, c);
+    v[1] = cadd(b, d);
+    v[3] = csub(b, d);
+  }
+};
+template <int SIGN>
+struct Dft<5, SIGN> {
+  __device__ __forceinline__ static void run(double2* v) {
+    const double c1 = 0.30901699437494745, c2 = -0.8090169943749475;
+    const double s1 = 0.9510565162951535, s2 = 0.5877852522924731;
+    const double2 p1 = cadd(v[1], v[4]), m1 = csub(v[1], v[4]);
+    const double2 p2 = cadd(v[2], v[3]), m2 = csub(v[2], v[3]);
+    const double2 a1 = make_double2(v[0].x + c1 * p1.x + c2 * p2.x, v[0].y + c1 * p1.y + c2 * p2.y);
+    const double2 a2 = make_double2(v[0].x + c2 * p1.x + c1 * p2.x, v[0].y + c2 * p1.y + c1 * p2.y);
+    const double2 b1 = irot<SIGN>(make_double2(s1 * m1.x + s2 * m2.x, s1 * m1.y + s2 * m2.y));
+    const double2 b2 = irot<SIGN>(make_double2(s2 * m1.x - s1 * m2.x, s2 * m1.y - s1 * m2.y));
+    v[0] = cadd(v[0], cadd(p1, p2));
+    v[1] = cadd(a1, b1);
+    v[4] = csub(a1, b1);
+    v[2] = cadd(a2, b2);
+    v[3] = csub(a2, b2);
+  }
+};
+// 6 = 3 x 2: a = DFT3(v0, v2, v4), b = DFT3(v1, v3, v5); X[u] = a[u] + w6^u b[u],
+// X[u+3] = a[u] - w6^u b[u].
+template <int SIGN>
+struct Dft<6, SIGN> {
+  __device__ __forceinline__ static void run(double2* v) {
+    double2 a[3] = {v[0], v[2], v[4]}, b[3] = {v[1], v[3], v[5]};
+    Dft<3, SIGN>::run(a);
+    Dft<3, SIGN>::run(b);
+    const double h = 0.8660254037844386;
+    const double2 b1 = w_mul<SIGN>(b[1], 0.5, h);
+    const double2 b2 = w_mul<SIGN>(b[2], -0.5, h);
+    v[0] = cadd(a[0], b[0]);
+    v[3] = csub(a[0], b[0]);
+    v[1] = cadd(a[1], b1);
+    v[4] = csub(a[1], b1);
+    v[2] = cadd(a[2], b2);
+    v[5] = csub(a[2], b2);
+  }
+};
+// 8 = 4 x 2: a = DFT4(evens), b = DFT4(odds); X[u] = a[u] + w8^u b[u], X[u+4] = a[u] - w8^u b[u].
+template <int SIGN>
+struct Dft<8, SIGN> {
+  __device__ __forceinline__ static void run(double2* v) {
+    double2 a[4] = {v[0], v[2], v[4], v[6]}, b[4] = {v[1], v[3], v[5], v[7]};
+    Dft<4, SIGN>::run(a);
+    Dft<4, SIGN>::run(b);
+    const double r = 0.7071067811865476;
+    const double2 b1 = w_mul<SIGN>(b[1], r, r);
+    const double2 b2 = irot<SIGN>(b[2]);
+    const double2 b3 = w_mul<SIGN>(b[3], -r, r);
+    v[0] = cadd(a[0], b[0]);
+    v[4] = csub(a[0], b[0]);
+    v[1] = cadd(a[1], b1);
+    v[5] = csub(a[1], b1);
+    v[2] = cadd(a[2], b2);
+    v[6] = csub(a[2], b2);
+    v[3] = cadd(a[3], b3);
+    v[7] = csub(a[3], b3);
+  }
+};
+// 9 = 3 x 3: a_m = DFT3(v_m, v_{m+3}, v_{m+6}); b_m[k1] = a_m[k1] w9^(m k1);
+// X[k1 + 3 k2] = DFT3 over m of b_m[k1].
+template <int SIGN>
+struct Dft<9, SIGN> {
+  __device__ __forceinline__ static void run(double2* v) {
+    double2 a0[3] = {v[0], v[3], v[6]}, a1[3] = {v[1], v[4], v[7]}, a2[3] = {v[2], v[5], v[8]};
+    Dft<3, SIGN>::run(a0);
+    Dft<3, SIGN>::run(a1);
+    Dft<3, SIGN>::run(a2);
+    const double c1 = 0.766044443118978, s1 = 0.6427876096865394;    // 2 pi/9
+    const double c2 = 0.17364817766693036, s2 = 0.984807753012208;   // 4 pi/9
+    const double c4 = -0.9396926207859084, s4 = 0.3420201433256687;  // 8 pi/9
+    a1[1] = w_mul<SIGN>(a1[1], c1, s1);
+    a1[2] = w_mul<SIGN>(a1[2], c2, s2);
+    a2[1] = w_mul<SIGN>(a2[1], c2, s2);
+    a2[2] = w_mul<SIGN>(a2[2], c4, s4);
+#pragma unroll
+    for (int k1 = 0; k1 < 3; ++k1) {
+      double2 t[3] = {a0[k1], a1[k1], a2[k1]};
+      Dft<3, SIGN>::run(t);
+      v[k1] = t[0];
+      v[k1 + 3] = t[1];
+      v[k1 + 6] = t[2];
+    }
+  }
+};
+
+// 12 = 3 x 4: a_m = DFT4(v_m, v_{m+3}, v_{m+6}, v_{m+9}); b_m[k1] = a_m[k1] w12^(m k1);
+// X[k1 + 4 k2] = DFT3 over m of b_m[k1].
+template <int SIGN>
+struct Dft<12, SIGN> {
+  __device__ __forceinline__ static void run(double2* v) {
+    double2 a0[4] = {v[0], v[3], v[6], v[9]}, a1[4] = {v[1], v[4], v[7], v[10]}, a2[4] = {v[2], v[5], v[8], v[11]};
+    Dft<4, SIGN>::run(a0);
+    Dft<4, SIGN>::run(a1);
+    Dft<4, SIGN>::run(a2);
+    const double h = 0.8660254037844386;
+    a1[1] = w_mul<SIGN>(a1[1], h, 0.5);   // w12^1
+    a1[2] = w_mul<SIGN>(a1[2], 0.5, h);   // w12^2
+    a1[3] = irot<SIGN>(a1[3]);            // w12^3
+    a2[1] = w_mul<SIGN>(a2[1], 0.5, h);   // w12^2
+    a2[2] = w_mul<SIGN>(a2[2], -0.5, h);  // w12^4
+    a2[3] = make_double2(-a2[3].x, -a2[3].y);  // w12^6
+#pragma unroll
+    for (int k1 = 0; k1 < 4; ++k1) {
+      double2 t[3] = {a0[k1], a1[k1], a2[k1]};
+      Dft<3, SIGN>::run(t);
+      v[k1] = t[0];
+      v[k1 + 4] = t[1];
+      v[k1 + 8] = t[2];
+    }
+  }
+};
+
+// --------------------------------------------------------------------- stages
+// Stage (R, NS) on lines first .. first+count-1 of this warp.
+template <int N, int R, int NS, int SIGN, class Off>
+__device__ __forceinline__ void stage(double2* base, int first, int count, Off off, int es,
+                                      const double2* __restrict__ tw, int lane) {
+  constexpr int SPAN = N / R;
+  constexpr int STEP = N / (NS * R);
+  constexpr int K = (SPAN + 31) / 32;                 // butterflies per lane when a line exceeds a warp
+  constexpr int LPR = SPAN <= 32 ? 32 / SPAN : 1;     // whole lines per round
+  for (int r0 = 0; r0 < count; r0 += LPR) {
+    double2 v[K][R];
+    int lo[K];
+    int jj[K];
+#pragma unroll
+    for (int q = 0; q < K; ++q) {
+      const int slot = lane + 32 * q;
+      const int li = K == 1 ? slot / SPAN : 0;
+      const int j = K == 1 ? slot - li * SPAN : slot;
+      const bool act = (K == 1 ? li < LPR : j < SPAN) && r0 + li < count;
+      jj[q] = act ? j : -1;
+      lo[q] = act ? off(first + r0 + li) : 0;
+      if (act) {
+#pragma unroll
+        for (int t = 0; t < R; ++t) v[q][t] = base[lo[q] + (j + t * SPAN) * es];
+      }
+    }
+    __syncwarp();
+#pragma unroll
+    for (int q = 0; q < K; ++q) {
+      if (jj[q] >= 0) {
+        const int j = jj[q];
+        const int k = NS > 1 ? j % NS : 0;
+        if (NS > 1) {
+#pragma unroll
+          for (int t = 1; t < R; ++t) {
+            double2 w = tw[t * k * STEP];
+            if (SIGN < 0) w.y = -w.y;
+            v[q][t] = cmul(v[q][t], w);
+          }
+        }
+        Dft<R, SIGN>::run(v[q]);
+        const int o = (NS > 1 ? (j / NS) * NS * R : j * R) + k;
+#pragma unroll
+        for (int u = 0; u < R; ++u) base[lo[q] + (o + u * NS) * es] = v[q][u];
+      }
+    }
+    __syncwarp();
+  }
+}
+
+template <int N, int SIGN, int S, int NS, class Off>
+__device__ __forceinline__ void stages_from(double2* base, int first, int count, Off off, int es,
+                                            const double2* __restrict__ tw, int lane) {
+  using P = Plan<N>;
+  if constexpr (S < P::nst) {
+    constexpr int R = P::radix[S];
+    stage<N, R, NS, SIGN>(base, first, count, off, es, tw, lane);
+    stages_from<N, SIGN, S + 1, NS * R>(base, first, count, off, es, tw, lane);
+  }
+}
+
+// Every stage of lines first .. first+count-1 (one warp; ends with __syncwarp).
+template <int N, int SIGN, class Off>
+__device__ __forceinline__ void group(double2* base, int first, int count, Off off, int es,
+                                      const double2* __restrict__ tw, int lane) {
+  stages_from<N, SIGN, 0, 1>(base, first, count, off, es, tw, lane);
+}
+
+// Lines of a pass owned by this warp: a contiguous block of ceil(L / warps).
+__device__ __forceinline__ void owned_lines(int nlines, int* first, int* count) {
+  const int nw = blockDim.x >> 5, warp = threadIdx.x >> 5;
+  const int per = (nlines + nw - 1) / nw;
+  *first = min(nlines, warp * per);
+  *count = min(nlines, *first + per) - *first;
+}
+
+// A whole pass over nlines lines; ends with __syncthreads.
+template <int N, int SIGN, class Off>
+__device__ __forceinline__ void pass(double2* base, int nlines, Off off, int es, const double2* __restrict__ tw) {
+  int first, count;
+  owned_lines(nlines, &first, &count);
+  if (count > 0) group<N, SIGN>(base, first, count, off, es, tw, threadIdx.x & 31);
+  __syncthreads();
+}
+
+}  // namespace fast
+}  // namespace bg

@@ -27,7 +27,7 @@ struct OpTables {
   const int* stick_plane; // S: x * pitch + y, offset inside the shared-memory plane
   const int* xact;        // nxact x rows
   const double* kinetic;  // rows
-  const double* vt;       // V(r) transposed to [z][x][y]
+  const double* vt;       // V(r) transposed to [z][y][x]
   double2* sbuf;          // stick buffer [unit][z][S]
   int* err;               // device error word (bit 0: non-finite input)
 };

@@ -20,6 +20,7 @@
 // crates/dft-physics/src/distributed_real_gamma.rs:654-689 (pair pack), :1307-1347
 // (unpack + kinetic), :957-1017, 1184-1248 (nonlocal).
 #include "hpsi.h"
+#include "fft_fast.cuh"
 
 namespace bg {
 
@@ -44,8 +45,8 @@ struct LineOffCols {
 __device__ __forceinline__ bool finite2(double a, double b) { return isfinite(a) && isfinite(b); }
 
 // ---------------------------------------------------------------- pass 1
-template <bool GAMMA>
-__global__ void __launch_bounds__(256) k_sticks_inverse(const OpTables* __restrict__ tabs, BoxGeo g, Batch b) {
+template <bool GAMMA, int N>
+__global__ void __launch_bounds__(256, 2) k_sticks_inverse(const OpTables* __restrict__ tabs, BoxGeo g, Batch b) {
   const OpTables& t = tabs[blockIdx.z];
   const CallArgs& a = b.a[blockIdx.z];
   const int grp = blockIdx.x, unit = blockIdx.y;
@@ -90,7 +91,12 @@ __global__ void __launch_bounds__(256) k_sticks_inverse(const OpTables* __restri
     }
   }
   if (bad) atomicOr(t.err, 1);
-  fft_lines<1>(st, cnt, LineOffStride{g.ld2}, 1, g.p2, tw);
+  if constexpr (N == 0) {
+    fft_lines<1>(st, cnt, LineOffStride{g.ld2}, 1, g.p2, tw);
+  } else {
+    __syncthreads();
+    fast::pass<N, 1>(st, cnt, LineOffStride{g.ld2}, 1, tw);
+  }
   double2* out = t.sbuf + (int64_t)unit * g.n2 * t.S + s0;
   for (int i = threadIdx.x; i < cnt * g.n2; i += blockDim.x) {
     const int z = i / cnt, sl = i - z * cnt;
@@ -120,7 +126,7 @@ __global__ void __launch_bounds__(512) k_planes(const OpTables* __restrict__ tab
   fft_lines<1>(pl, g.n1, LineOffCols{}, g.pitch, g.p0, tw0);
   const double* v = t.vt + (int64_t)z * g.n0 * g.n1;
   for (int i = threadIdx.x; i < g.n0 * g.n1; i += blockDim.x) {
-    const int x = i / g.n1, y = i - x * g.n1;
+    const int y = i / g.n0, x = i - y * g.n0;
     const double w = v[i];
     double2& p = pl[x * g.pitch + y];
     p.x *= w;
@@ -131,9 +137,49 @@ __global__ void __launch_bounds__(512) k_planes(const OpTables* __restrict__ tab
   for (int s = threadIdx.x; s < t.S; s += blockDim.x) row[s] = pl[t.stick_plane[s]];
 }
 
+// Cubic grids with a compile-time plan: the x pass runs inverse, x V(r) and forward on
+// each warp's column group without a block barrier in between.
+template <int N>
+__global__ void __launch_bounds__(256, 2) k_planes_fast(const OpTables* __restrict__ tabs, BoxGeo g, Batch b) {
+  const OpTables& t = tabs[blockIdx.z];
+  const CallArgs& a = b.a[blockIdx.z];
+  const int unit = blockIdx.x, z = blockIdx.y;
+  if (unit >= a.units) return;
+  extern __shared__ double2 sm[];
+  double2* tw = sm;
+  double2* pl = sm + N;
+  const int pitch = g.pitch;
+  for (int i = threadIdx.x; i < N; i += blockDim.x) tw[i] = g.tw0[i];
+  for (int i = threadIdx.x; i < N * pitch; i += blockDim.x) pl[i] = make_double2(0.0, 0.0);
+  __syncthreads();
+  double2* row = t.sbuf + ((int64_t)unit * N + z) * t.S;
+  for (int s = threadIdx.x; s < t.S; s += blockDim.x) pl[t.stick_plane[s]] = row[s];
+  __syncthreads();
+  fast::pass<N, 1>(pl, t.nxact, LineOffRows{t.xact, pitch}, 1, tw);
+  const int lane = threadIdx.x & 31;
+  const double* v = t.vt + (int64_t)z * N * N;
+  int first, count;
+  fast::owned_lines(N, &first, &count);
+  if (count > 0) {
+    fast::group<N, 1>(pl, first, count, LineOffCols{}, pitch, tw, lane);
+    for (int e = lane; e < count * N; e += 32) {
+      const int li = e / N, x = e - li * N, y = first + li;
+      const double w = v[y * N + x];
+      double2& p = pl[x * pitch + y];
+      p.x *= w;
+      p.y *= w;
+    }
+    __syncwarp();
+    fast::group<N, -1>(pl, first, count, LineOffCols{}, pitch, tw, lane);
+  }
+  __syncthreads();
+  fast::pass<N, -1>(pl, t.nxact, LineOffRows{t.xact, pitch}, 1, tw);
+  for (int s = threadIdx.x; s < t.S; s += blockDim.x) row[s] = pl[t.stick_plane[s]];
+}
+
 // ---------------------------------------------------------------- pass 3
-template <bool GAMMA>
-__global__ void __launch_bounds__(256) k_sticks_forward(const OpTables* __restrict__ tabs, BoxGeo g, Batch b) {
+template <bool GAMMA, int N>
+__global__ void __launch_bounds__(256, 2) k_sticks_forward(const OpTables* __restrict__ tabs, BoxGeo g, Batch b) {
   const OpTables& t = tabs[blockIdx.z];
   const CallArgs& a = b.a[blockIdx.z];
   const int grp = blockIdx.x, unit = blockIdx.y;
@@ -148,7 +194,12 @@ __global__ void __launch_bounds__(256) k_sticks_forward(const OpTables* __restri
     const int z = i / cnt, sl = i - z * cnt;
     st[sl * g.ld2 + z] = in[(int64_t)z * t.S + sl];
   }
-  fft_lines<-1>(st, cnt, LineOffStride{g.ld2}, 1, g.p2, tw);
+  if constexpr (N == 0) {
+    fft_lines<-1>(st, cnt, LineOffStride{g.ld2}, 1, g.p2, tw);
+  } else {
+    __syncthreads();
+    fast::pass<N, -1>(st, cnt, LineOffStride{g.ld2}, 1, tw);
+  }
   const double s = g.inv_n;
   if (!GAMMA) {
     const int e0 = t.grp_entry[grp], e1 = t.grp_entry[grp + 1];
@@ -381,6 +432,37 @@ struct StageScope {
 };
 }  // namespace
 
+template <bool GAMMA, int N>
+static void local_kernels(const OpTables* tabs, const BoxGeo& g, const Batch& b, dim3 sgrid, dim3 pgrid, size_t ss,
+                          size_t ps, cudaStream_t s, StageEvents* ev) {
+  { StageScope sc(ev, 0, s); k_sticks_inverse<GAMMA, N><<<sgrid, 256, ss, s>>>(tabs, g, b); }
+  if constexpr (N == 0) {
+    StageScope sc(ev, 1, s);
+    k_planes<<<pgrid, 512, ps, s>>>(tabs, g, b);
+  } else {
+    StageScope sc(ev, 1, s);
+    if (g.n0 == N && g.n1 == N)
+      k_planes_fast<N><<<pgrid, 256, ps, s>>>(tabs, g, b);
+    else
+      k_planes<<<pgrid, 512, ps, s>>>(tabs, g, b);
+  }
+  { StageScope sc(ev, 2, s); k_sticks_forward<GAMMA, N><<<sgrid, 256, ss, s>>>(tabs, g, b); }
+}
+
+template <bool GAMMA>
+static void local_dispatch(const OpTables* tabs, const BoxGeo& g, const Batch& b, dim3 sgrid, dim3 pgrid, size_t ss,
+                           size_t ps, cudaStream_t s, StageEvents* ev) {
+  switch (g.n2) {
+    case 25: local_kernels<GAMMA, 25>(tabs, g, b, sgrid, pgrid, ss, ps, s, ev); break;
+    case 45: local_kernels<GAMMA, 45>(tabs, g, b, sgrid, pgrid, ss, ps, s, ev); break;
+    case 54: local_kernels<GAMMA, 54>(tabs, g, b, sgrid, pgrid, ss, ps, s, ev); break;
+    case 60: local_kernels<GAMMA, 60>(tabs, g, b, sgrid, pgrid, ss, ps, s, ev); break;
+    case 72: local_kernels<GAMMA, 72>(tabs, g, b, sgrid, pgrid, ss, ps, s, ev); break;
+    case 108: local_kernels<GAMMA, 108>(tabs, g, b, sgrid, pgrid, ss, ps, s, ev); break;
+    default: local_kernels<GAMMA, 0>(tabs, g, b, sgrid, pgrid, ss, ps, s, ev); break;
+  }
+}
+
 int launch_local(const OpTables* tabs, int gamma, int max_groups, const BoxGeo& g, const Batch& b, cudaStream_t s,
                  StageEvents* ev) {
   int max_units = 0;
@@ -389,15 +471,10 @@ int launch_local(const OpTables* tabs, int gamma, int max_groups, const BoxGeo& 
   const size_t ss = stick_smem_bytes(g), ps = plane_smem_bytes(g);
   const dim3 sgrid(max_groups, max_units, b.nk);
   const dim3 pgrid(max_units, g.n2, b.nk);
-  if (gamma) {
-    { StageScope sc(ev, 0, s); k_sticks_inverse<true><<<sgrid, 256, ss, s>>>(tabs, g, b); }
-    { StageScope sc(ev, 1, s); k_planes<<<pgrid, 512, ps, s>>>(tabs, g, b); }
-    { StageScope sc(ev, 2, s); k_sticks_forward<true><<<sgrid, 256, ss, s>>>(tabs, g, b); }
-  } else {
-    { StageScope sc(ev, 0, s); k_sticks_inverse<false><<<sgrid, 256, ss, s>>>(tabs, g, b); }
-    { StageScope sc(ev, 1, s); k_planes<<<pgrid, 512, ps, s>>>(tabs, g, b); }
-    { StageScope sc(ev, 2, s); k_sticks_forward<false><<<sgrid, 256, ss, s>>>(tabs, g, b); }
-  }
+  if (gamma)
+    local_dispatch<true>(tabs, g, b, sgrid, pgrid, ss, ps, s, ev);
+  else
+    local_dispatch<false>(tabs, g, b, sgrid, pgrid, ss, ps, s, ev);
   return 3;
 }
 
@@ -427,16 +504,33 @@ int launch_nonlocal(const NlDev* nl, int gamma, const NlShape& sh, int max_rows,
 namespace bg {
 
 // Opt every kernel with dynamic shared memory into the sizes one operator needs.
-int configure_kernels(size_t plane_smem, size_t stick_smem) {
-  cudaError_t e = cudaSuccess;
+template <bool GAMMA, int N>
+static void configure_one(cudaError_t& e, size_t plane_smem, size_t stick_smem) {
   auto set = [&](const void* f, size_t bytes) {
     if (e == cudaSuccess) e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
   };
-  set((const void*)k_sticks_inverse<true>, stick_smem);
-  set((const void*)k_sticks_inverse<false>, stick_smem);
-  set((const void*)k_sticks_forward<true>, stick_smem);
-  set((const void*)k_sticks_forward<false>, stick_smem);
-  set((const void*)k_planes, plane_smem);
+  set((const void*)k_sticks_inverse<GAMMA, N>, stick_smem);
+  set((const void*)k_sticks_forward<GAMMA, N>, stick_smem);
+  if constexpr (N != 0) set((const void*)k_planes_fast<N>, plane_smem);
+}
+
+int configure_kernels(size_t plane_smem, size_t stick_smem) {
+  cudaError_t e = cudaSuccess;
+  e = cudaFuncSetAttribute((const void*)k_planes, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)plane_smem);
+  configure_one<true, 0>(e, plane_smem, stick_smem);
+  configure_one<false, 0>(e, plane_smem, stick_smem);
+  configure_one<true, 25>(e, plane_smem, stick_smem);
+  configure_one<false, 25>(e, plane_smem, stick_smem);
+  configure_one<true, 45>(e, plane_smem, stick_smem);
+  configure_one<false, 45>(e, plane_smem, stick_smem);
+  configure_one<true, 54>(e, plane_smem, stick_smem);
+  configure_one<false, 54>(e, plane_smem, stick_smem);
+  configure_one<true, 60>(e, plane_smem, stick_smem);
+  configure_one<false, 60>(e, plane_smem, stick_smem);
+  configure_one<true, 72>(e, plane_smem, stick_smem);
+  configure_one<false, 72>(e, plane_smem, stick_smem);
+  configure_one<true, 108>(e, plane_smem, stick_smem);
+  configure_one<false, 108>(e, plane_smem, stick_smem);
   return e == cudaSuccess ? 0 : 1;
 }
 

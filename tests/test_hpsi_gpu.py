@@ -113,7 +113,8 @@ def test_static_diagonal_matches_dense(ctx):
 
 
 def test_kpoint_set_equals_single_applies(ctx):
-    """One batched launch per stage over 36 k points gives the per-operator results bit for bit."""
+    """One batched launch per stage over 36 k points gives the per-operator results (the
+    split of the P^H x row sum may differ from a single apply's: rounding only)."""
     from baandi_b200.hamiltonian import KPointSet
     w = W.si8_k444()
     v = w.ionic_potential()
@@ -126,7 +127,7 @@ def test_kpoint_set_equals_single_applies(ctx):
     ks = KPointSet(ops)
     ys = ks.apply_blocks(xs)
     for op, x, y in zip(ops, xs, ys):
-        assert np.array_equal(op.apply_block(x), y)
+        assert colwise_rel(y, op.apply_block(x)) < 1e-14
     ref = oracle_apply(w, w.kpoints[11][0], w.dims(), v, xs[11])
     assert colwise_rel(ys[11], ref) <= TOL
     ks.close()
