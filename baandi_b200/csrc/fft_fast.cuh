@@ -194,71 +194,76 @@ struct Dft<12, SIGN> {
 };
 
 // --------------------------------------------------------------------- stages
-// Stage (R, NS) on lines first .. first+count-1 of this warp.
-template <int N, int R, int NS, int SIGN, class Off>
-__device__ __forceinline__ void stage(double2* base, int first, int count, Off off, int es,
-                                      const double2* __restrict__ tw, int lane) {
+// Stage (R, NS) on lines first .. first+count-1 of this warp; ES = element stride.
+// A lane's butterfly index j is the same in every round.
+template <int N, int R, int NS, int SIGN, int ES, class Off>
+__device__ __forceinline__ void stage(double2* base, int first, int count, Off off, const double2* __restrict__ tw,
+                                      int lane) {
   constexpr int SPAN = N / R;
   constexpr int STEP = N / (NS * R);
   constexpr int K = (SPAN + 31) / 32;                 // butterflies per lane when a line exceeds a warp
   constexpr int LPR = SPAN <= 32 ? 32 / SPAN : 1;     // whole lines per round
+  int jj[K], li[K], oo[K], kk[K];
+#pragma unroll
+  for (int q = 0; q < K; ++q) {
+    const int slot = lane + 32 * q;
+    li[q] = K == 1 ? slot / SPAN : 0;
+    jj[q] = K == 1 ? slot - li[q] * SPAN : slot;
+    if (K == 1 ? li[q] >= LPR : jj[q] >= SPAN) li[q] = 1 << 20;  // idle lane
+    const int j = jj[q];
+    const int k = NS > 1 ? j % NS : 0;
+    oo[q] = (NS > 1 ? (j / NS) * NS * R : j * R) + k;
+    kk[q] = k * STEP;
+  }
   for (int r0 = 0; r0 < count; r0 += LPR) {
     double2 v[K][R];
     int lo[K];
-    int jj[K];
 #pragma unroll
     for (int q = 0; q < K; ++q) {
-      const int slot = lane + 32 * q;
-      const int li = K == 1 ? slot / SPAN : 0;
-      const int j = K == 1 ? slot - li * SPAN : slot;
-      const bool act = (K == 1 ? li < LPR : j < SPAN) && r0 + li < count;
-      jj[q] = act ? j : -1;
-      lo[q] = act ? off(first + r0 + li) : 0;
+      const bool act = r0 + li[q] < count;
+      lo[q] = act ? off(first + r0 + li[q]) : -1;
       if (act) {
 #pragma unroll
-        for (int t = 0; t < R; ++t) v[q][t] = base[lo[q] + (j + t * SPAN) * es];
+        for (int t = 0; t < R; ++t) v[q][t] = base[lo[q] + (jj[q] + t * SPAN) * ES];
       }
     }
     __syncwarp();
 #pragma unroll
     for (int q = 0; q < K; ++q) {
-      if (jj[q] >= 0) {
-        const int j = jj[q];
-        const int k = NS > 1 ? j % NS : 0;
+      if (lo[q] >= 0) {
         if (NS > 1) {
 #pragma unroll
           for (int t = 1; t < R; ++t) {
-            double2 w = tw[t * k * STEP];
-            if (SIGN < 0) w.y = -w.y;
-            v[q][t] = cmul(v[q][t], w);
+            double2 x = tw[t * kk[q]];
+            if (SIGN < 0) x.y = -x.y;
+            v[q][t] = cmul(v[q][t], x);
           }
         }
         Dft<R, SIGN>::run(v[q]);
-        const int o = (NS > 1 ? (j / NS) * NS * R : j * R) + k;
 #pragma unroll
-        for (int u = 0; u < R; ++u) base[lo[q] + (o + u * NS) * es] = v[q][u];
+        for (int u = 0; u < R; ++u) base[lo[q] + (oo[q] + u * NS) * ES] = v[q][u];
       }
     }
     __syncwarp();
   }
 }
 
-template <int N, int SIGN, int S, int NS, class Off>
-__device__ __forceinline__ void stages_from(double2* base, int first, int count, Off off, int es,
+template <int N, int SIGN, int ES, int S, int NS, class Off>
+__device__ __forceinline__ void stages_from(double2* base, int first, int count, Off off,
                                             const double2* __restrict__ tw, int lane) {
   using P = Plan<N>;
   if constexpr (S < P::nst) {
     constexpr int R = P::radix[S];
-    stage<N, R, NS, SIGN>(base, first, count, off, es, tw, lane);
-    stages_from<N, SIGN, S + 1, NS * R>(base, first, count, off, es, tw, lane);
+    stage<N, R, NS, SIGN, ES>(base, first, count, off, tw, lane);
+    stages_from<N, SIGN, ES, S + 1, NS * R>(base, first, count, off, tw, lane);
   }
 }
 
 // Every stage of lines first .. first+count-1 (one warp; ends with __syncwarp).
-template <int N, int SIGN, class Off>
-__device__ __forceinline__ void group(double2* base, int first, int count, Off off, int es,
-                                      const double2* __restrict__ tw, int lane) {
-  stages_from<N, SIGN, 0, 1>(base, first, count, off, es, tw, lane);
+template <int N, int SIGN, int ES, class Off>
+__device__ __forceinline__ void group(double2* base, int first, int count, Off off, const double2* __restrict__ tw,
+                                      int lane) {
+  stages_from<N, SIGN, ES, 0, 1>(base, first, count, off, tw, lane);
 }
 
 // Lines of a pass owned by this warp: a contiguous block of ceil(L / warps).
@@ -270,12 +275,19 @@ __device__ __forceinline__ void owned_lines(int nlines, int* first, int* count) 
 }
 
 // A whole pass over nlines lines; ends with __syncthreads.
-template <int N, int SIGN, class Off>
-__device__ __forceinline__ void pass(double2* base, int nlines, Off off, int es, const double2* __restrict__ tw) {
+template <int N, int SIGN, int ES, class Off>
+__device__ __forceinline__ void pass(double2* base, int nlines, Off off, const double2* __restrict__ tw) {
   int first, count;
   owned_lines(nlines, &first, &count);
-  if (count > 0) group<N, SIGN>(base, first, count, off, es, tw, threadIdx.x & 31);
+  if (count > 0) group<N, SIGN, ES>(base, first, count, off, tw, threadIdx.x & 31);
   __syncthreads();
+}
+
+// Row pitch of a shared-memory plane of N x N: odd, so that a column line (stride
+// pitch) and a row line both touch distinct banks in every 8-lane phase.
+template <int N>
+__host__ __device__ constexpr int pitch_of() {
+  return N | 1;
 }
 
 }  // namespace fast

@@ -38,6 +38,10 @@ struct LineOffRows {
   int pitch;
   __device__ __forceinline__ int operator()(int l) const { return rows[l] * pitch; }
 };
+struct LineOffTable {
+  const int* off;
+  __device__ __forceinline__ int operator()(int l) const { return off[l]; }
+};
 struct LineOffCols {
   __device__ __forceinline__ int operator()(int l) const { return l; }
 };
@@ -46,7 +50,7 @@ __device__ __forceinline__ bool finite2(double a, double b) { return isfinite(a)
 
 // ---------------------------------------------------------------- pass 1
 template <bool GAMMA, int N>
-__global__ void __launch_bounds__(256, 2) k_sticks_inverse(const OpTables* __restrict__ tabs, BoxGeo g, Batch b) {
+__global__ void __launch_bounds__(256, N == 0 ? 1 : 3) k_sticks_inverse(const OpTables* __restrict__ tabs, BoxGeo g, Batch b) {
   const OpTables& t = tabs[blockIdx.z];
   const CallArgs& a = b.a[blockIdx.z];
   const int grp = blockIdx.x, unit = blockIdx.y;
@@ -95,7 +99,7 @@ __global__ void __launch_bounds__(256, 2) k_sticks_inverse(const OpTables* __res
     fft_lines<1>(st, cnt, LineOffStride{g.ld2}, 1, g.p2, tw);
   } else {
     __syncthreads();
-    fast::pass<N, 1>(st, cnt, LineOffStride{g.ld2}, 1, tw);
+    fast::pass<N, 1, 1>(st, cnt, LineOffStride{fast::pitch_of<N>()}, tw);
   }
   double2* out = t.sbuf + (int64_t)unit * g.n2 * t.S + s0;
   for (int i = threadIdx.x; i < cnt * g.n2; i += blockDim.x) {
@@ -140,46 +144,49 @@ __global__ void __launch_bounds__(512) k_planes(const OpTables* __restrict__ tab
 // Cubic grids with a compile-time plan: the x pass runs inverse, x V(r) and forward on
 // each warp's column group without a block barrier in between.
 template <int N>
-__global__ void __launch_bounds__(256, 2) k_planes_fast(const OpTables* __restrict__ tabs, BoxGeo g, Batch b) {
+__global__ void __launch_bounds__(256, 3) k_planes_fast(const OpTables* __restrict__ tabs, BoxGeo g, Batch b) {
   const OpTables& t = tabs[blockIdx.z];
   const CallArgs& a = b.a[blockIdx.z];
   const int unit = blockIdx.x, z = blockIdx.y;
   if (unit >= a.units) return;
+  constexpr int P = fast::pitch_of<N>();
   extern __shared__ double2 sm[];
   double2* tw = sm;
   double2* pl = sm + N;
-  const int pitch = g.pitch;
+  int* rows = reinterpret_cast<int*>(pl + N * P);
+  const int nx = t.nxact;
   for (int i = threadIdx.x; i < N; i += blockDim.x) tw[i] = g.tw0[i];
-  for (int i = threadIdx.x; i < N * pitch; i += blockDim.x) pl[i] = make_double2(0.0, 0.0);
+  for (int i = threadIdx.x; i < nx; i += blockDim.x) rows[i] = t.xact[i] * P;
+  for (int i = threadIdx.x; i < N * P; i += blockDim.x) pl[i] = make_double2(0.0, 0.0);
   __syncthreads();
   double2* row = t.sbuf + ((int64_t)unit * N + z) * t.S;
   for (int s = threadIdx.x; s < t.S; s += blockDim.x) pl[t.stick_plane[s]] = row[s];
   __syncthreads();
-  fast::pass<N, 1>(pl, t.nxact, LineOffRows{t.xact, pitch}, 1, tw);
+  fast::pass<N, 1, 1>(pl, nx, LineOffTable{rows}, tw);
   const int lane = threadIdx.x & 31;
   const double* v = t.vt + (int64_t)z * N * N;
   int first, count;
   fast::owned_lines(N, &first, &count);
   if (count > 0) {
-    fast::group<N, 1>(pl, first, count, LineOffCols{}, pitch, tw, lane);
+    fast::group<N, 1, P>(pl, first, count, LineOffCols{}, tw, lane);
     for (int e = lane; e < count * N; e += 32) {
       const int li = e / N, x = e - li * N, y = first + li;
       const double w = v[y * N + x];
-      double2& p = pl[x * pitch + y];
+      double2& p = pl[x * P + y];
       p.x *= w;
       p.y *= w;
     }
     __syncwarp();
-    fast::group<N, -1>(pl, first, count, LineOffCols{}, pitch, tw, lane);
+    fast::group<N, -1, P>(pl, first, count, LineOffCols{}, tw, lane);
   }
   __syncthreads();
-  fast::pass<N, -1>(pl, t.nxact, LineOffRows{t.xact, pitch}, 1, tw);
+  fast::pass<N, -1, 1>(pl, nx, LineOffTable{rows}, tw);
   for (int s = threadIdx.x; s < t.S; s += blockDim.x) row[s] = pl[t.stick_plane[s]];
 }
 
 // ---------------------------------------------------------------- pass 3
 template <bool GAMMA, int N>
-__global__ void __launch_bounds__(256, 2) k_sticks_forward(const OpTables* __restrict__ tabs, BoxGeo g, Batch b) {
+__global__ void __launch_bounds__(256, N == 0 ? 1 : 3) k_sticks_forward(const OpTables* __restrict__ tabs, BoxGeo g, Batch b) {
   const OpTables& t = tabs[blockIdx.z];
   const CallArgs& a = b.a[blockIdx.z];
   const int grp = blockIdx.x, unit = blockIdx.y;
@@ -198,7 +205,7 @@ __global__ void __launch_bounds__(256, 2) k_sticks_forward(const OpTables* __res
     fft_lines<-1>(st, cnt, LineOffStride{g.ld2}, 1, g.p2, tw);
   } else {
     __syncthreads();
-    fast::pass<N, -1>(st, cnt, LineOffStride{g.ld2}, 1, tw);
+    fast::pass<N, -1, 1>(st, cnt, LineOffStride{fast::pitch_of<N>()}, tw);
   }
   const double s = g.inv_n;
   if (!GAMMA) {
@@ -415,7 +422,9 @@ __global__ void __launch_bounds__(256) k_back(const NlDev* __restrict__ nls, int
 
 }  // namespace
 
-size_t plane_smem_bytes(const BoxGeo& g) { return sizeof(double2) * ((size_t)g.n0 + g.n1 + (size_t)g.n0 * g.pitch); }
+size_t plane_smem_bytes(const BoxGeo& g) {
+  return sizeof(double2) * ((size_t)g.n0 + g.n1 + (size_t)g.n0 * g.pitch) + sizeof(int) * (size_t)g.n0;
+}
 size_t stick_smem_bytes(const BoxGeo& g) { return sizeof(double2) * ((size_t)g.n2 + (size_t)g.sg * g.ld2); }
 
 namespace {

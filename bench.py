@@ -35,7 +35,7 @@ if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 
 STAGES = ("sticks_inverse", "planes", "sticks_forward", "project", "couple", "back")
-KERNELS = {"sticks_inverse": "k_sticks_inverse", "planes": "k_planes", "sticks_forward": "k_sticks_forward",
+KERNELS = {"sticks_inverse": "k_sticks_inverse", "planes": "k_planes_fast", "sticks_forward": "k_sticks_forward",
            "project": "k_project", "couple": "k_couple", "back": "k_back"}
 
 
