@@ -246,6 +246,7 @@ int build_op(bg_ctx* ctx, const bg_basis_desc* b, const bg_projectors* pr, int64
   G.ld2 = n2 | 1;
   G.pitch = n1 | 1;
   G.sg = sg;
+  G.vstride = (n0 * n1 + 1) & ~1;
   G.inv_n = 1.0 / ((double)n0 * n1 * n2);
   if (!make_fft_plan(n0, &G.p0) || !make_fft_plan(n1, &G.p1) || !make_fft_plan(n2, &G.p2))
     return fail(ctx, BG_ESHAPE, "grid length must be 2,3,5-smooth and at most 128");
@@ -341,7 +342,7 @@ int build_op(bg_ctx* ctx, const bg_basis_desc* b, const bg_projectors* pr, int64
   double* d_dbl;
   if ((rc = upload(op.get(), kin.data(), kin.size(), &d_dbl))) return rc;
   T.kinetic = d_dbl;
-  std::vector<double> nanv((size_t)n0 * n1 * n2, std::nan(""));
+  std::vector<double> nanv((size_t)G.vstride * n2, std::nan(""));
   if ((rc = upload(op.get(), nanv.data(), nanv.size(), &d_dbl))) return rc;
   T.vt = d_dbl;
   void* vp;
@@ -539,16 +540,16 @@ int bg_op_set_potential(bg_op* op, const double* v, uint64_t epoch) {
   if (!op || !v) return fail(op ? op->ctx : nullptr, BG_EINVAL, "null argument");
   if (op->has_epoch && epoch <= op->epoch) return fail(op->ctx, BG_EEPOCH, "potential epoch must increase");
   const int n0 = op->dims[0], n1 = op->dims[1], n2 = op->dims[2];
-  const size_t N = (size_t)n0 * n1 * n2;
-  std::vector<double> vt(N);
+  const size_t vs = (size_t)op->g.vstride;
+  std::vector<double> vt(vs * n2, 0.0);
   for (int x = 0; x < n0; ++x)
     for (int y = 0; y < n1; ++y)
       for (int z = 0; z < n2; ++z) {
         const double w = v[((size_t)x * n1 + y) * n2 + z];
         if (!std::isfinite(w)) return fail(op->ctx, BG_ENONFINITE, "potential not finite");
-        vt[((size_t)z * n1 + y) * n0 + x] = w;
+        vt[(size_t)z * vs + (size_t)y * n0 + x] = w;
       }
-  cudaError_t e = cudaMemcpyAsync(const_cast<double*>(op->t.vt), vt.data(), N * sizeof(double),
+  cudaError_t e = cudaMemcpyAsync(const_cast<double*>(op->t.vt), vt.data(), vt.size() * sizeof(double),
                                   cudaMemcpyHostToDevice, op->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(op->stream);
   if (e != cudaSuccess) return cuda_fail(op->ctx, e, "set_potential");

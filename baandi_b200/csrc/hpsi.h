@@ -38,6 +38,7 @@ struct BoxGeo {
   int ld2;     // stride of a z line in the stick kernels' shared memory (odd)
   int pitch;   // row pitch of the shared-memory plane (odd)
   int sg;      // max sticks per group
+  int vstride; // doubles between z planes of the transposed potential (even: 16-byte aligned planes)
   double inv_n;
   FftPlan p0, p1, p2;
   const double2* tw0;  // exp(+2 pi i q/n0), q < n0

@@ -128,7 +128,7 @@ __global__ void __launch_bounds__(512) k_planes(const OpTables* __restrict__ tab
   // inverse: y on the occupied x rows, x on every column
   fft_lines<1>(pl, t.nxact, LineOffRows{t.xact, g.pitch}, 1, g.p1, tw1);
   fft_lines<1>(pl, g.n1, LineOffCols{}, g.pitch, g.p0, tw0);
-  const double* v = t.vt + (int64_t)z * g.n0 * g.n1;
+  const double* v = t.vt + (int64_t)z * g.vstride;
   for (int i = threadIdx.x; i < g.n0 * g.n1; i += blockDim.x) {
     const int y = i / g.n0, x = i - y * g.n0;
     const double w = v[i];
@@ -144,7 +144,7 @@ __global__ void __launch_bounds__(512) k_planes(const OpTables* __restrict__ tab
 // Cubic grids with a compile-time plan: the x pass runs inverse, x V(r) and forward on
 // each warp's column group without a block barrier in between.
 template <int N>
-__global__ void __launch_bounds__(256, 3) k_planes_fast(const OpTables* __restrict__ tabs, BoxGeo g, Batch b) {
+__global__ void __launch_bounds__(256, 4) k_planes_fast(const OpTables* __restrict__ tabs, BoxGeo g, Batch b) {
   const OpTables& t = tabs[blockIdx.z];
   const CallArgs& a = b.a[blockIdx.z];
   const int unit = blockIdx.x, z = blockIdx.y;
@@ -153,8 +153,20 @@ __global__ void __launch_bounds__(256, 3) k_planes_fast(const OpTables* __restri
   extern __shared__ double2 sm[];
   double2* tw = sm;
   double2* pl = sm + N;
-  int* rows = reinterpret_cast<int*>(pl + N * P);
+  double* vs = reinterpret_cast<double*>(pl + N * P);   // V(r) of this plane, [y][x]
+  int* rows = reinterpret_cast<int*>(vs + N * N);
   const int nx = t.nxact;
+  // V(r) of the plane arrives asynchronously while the y pass runs (16-byte cp.async).
+  const double* v = t.vt + (int64_t)z * g.vstride;  // 16-byte aligned: vstride is even
+  {
+    const unsigned dst = static_cast<unsigned>(__cvta_generic_to_shared(vs));
+    for (int i = threadIdx.x; i < N * N / 2; i += blockDim.x)
+      asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst + 16u * i), "l"(v + 2 * i));
+    if ((N * N) & 1) {
+      if (threadIdx.x == 0) vs[N * N - 1] = v[N * N - 1];
+    }
+    asm volatile("cp.async.commit_group;\n" ::);
+  }
   for (int i = threadIdx.x; i < N; i += blockDim.x) tw[i] = g.tw0[i];
   for (int i = threadIdx.x; i < nx; i += blockDim.x) rows[i] = t.xact[i] * P;
   for (int i = threadIdx.x; i < N * P; i += blockDim.x) pl[i] = make_double2(0.0, 0.0);
@@ -163,15 +175,16 @@ __global__ void __launch_bounds__(256, 3) k_planes_fast(const OpTables* __restri
   for (int s = threadIdx.x; s < t.S; s += blockDim.x) pl[t.stick_plane[s]] = row[s];
   __syncthreads();
   fast::pass<N, 1, 1>(pl, nx, LineOffTable{rows}, tw);
+  asm volatile("cp.async.wait_all;\n" ::);
+  __syncthreads();
   const int lane = threadIdx.x & 31;
-  const double* v = t.vt + (int64_t)z * N * N;
   int first, count;
   fast::owned_lines(N, &first, &count);
   if (count > 0) {
     fast::group<N, 1, P>(pl, first, count, LineOffCols{}, tw, lane);
     for (int e = lane; e < count * N; e += 32) {
       const int li = e / N, x = e - li * N, y = first + li;
-      const double w = v[y * N + x];
+      const double w = vs[y * N + x];
       double2& p = pl[x * P + y];
       p.x *= w;
       p.y *= w;
@@ -423,7 +436,8 @@ __global__ void __launch_bounds__(256) k_back(const NlDev* __restrict__ nls, int
 }  // namespace
 
 size_t plane_smem_bytes(const BoxGeo& g) {
-  return sizeof(double2) * ((size_t)g.n0 + g.n1 + (size_t)g.n0 * g.pitch) + sizeof(int) * (size_t)g.n0;
+  return sizeof(double2) * ((size_t)g.n0 + g.n1 + (size_t)g.n0 * g.pitch) + sizeof(double) * (size_t)g.n0 * g.n1 +
+         sizeof(int) * (size_t)g.n0;
 }
 size_t stick_smem_bytes(const BoxGeo& g) { return sizeof(double2) * ((size_t)g.n2 + (size_t)g.sg * g.ld2); }
 
@@ -518,9 +532,17 @@ static void configure_one(cudaError_t& e, size_t plane_smem, size_t stick_smem) 
   auto set = [&](const void* f, size_t bytes) {
     if (e == cudaSuccess) e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
   };
+  auto carve = [&](const void* f) {
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(f, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+  };
   set((const void*)k_sticks_inverse<GAMMA, N>, stick_smem);
   set((const void*)k_sticks_forward<GAMMA, N>, stick_smem);
-  if constexpr (N != 0) set((const void*)k_planes_fast<N>, plane_smem);
+  carve((const void*)k_sticks_inverse<GAMMA, N>);
+  carve((const void*)k_sticks_forward<GAMMA, N>);
+  if constexpr (N != 0) {
+    set((const void*)k_planes_fast<N>, plane_smem);
+    carve((const void*)k_planes_fast<N>);
+  }
 }
 
 int configure_kernels(size_t plane_smem, size_t stick_smem) {
