@@ -38,6 +38,10 @@ struct LineOffRows {
   int pitch;
   __device__ __forceinline__ int operator()(int l) const { return rows[l] * pitch; }
 };
+// The fast plane kernel stages V(r) of its plane in shared memory when plane and
+// potential fit together (N <= 90: 90 x 91 x 16 + 90 x 90 x 8 bytes = 196 KB).
+__host__ __device__ constexpr bool v_in_smem(int n) { return n <= 90; }
+
 struct LineOffTable {
   const int* off;
   __device__ __forceinline__ int operator()(int l) const { return off[l]; }
@@ -150,15 +154,16 @@ __global__ void __launch_bounds__(256, 4) k_planes_fast(const OpTables* __restri
   const int unit = blockIdx.x, z = blockIdx.y;
   if (unit >= a.units) return;
   constexpr int P = fast::pitch_of<N>();
+  constexpr bool VS = v_in_smem(N);
   extern __shared__ double2 sm[];
   double2* tw = sm;
   double2* pl = sm + N;
   double* vs = reinterpret_cast<double*>(pl + N * P);   // V(r) of this plane, [y][x]
-  int* rows = reinterpret_cast<int*>(vs + N * N);
+  int* rows = reinterpret_cast<int*>(vs + (VS ? N * N : 0));
   const int nx = t.nxact;
   // V(r) of the plane arrives asynchronously while the y pass runs (16-byte cp.async).
   const double* v = t.vt + (int64_t)z * g.vstride;  // 16-byte aligned: vstride is even
-  {
+  if constexpr (VS) {
     const unsigned dst = static_cast<unsigned>(__cvta_generic_to_shared(vs));
     for (int i = threadIdx.x; i < N * N / 2; i += blockDim.x)
       asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst + 16u * i), "l"(v + 2 * i));
@@ -184,7 +189,7 @@ __global__ void __launch_bounds__(256, 4) k_planes_fast(const OpTables* __restri
     fast::group<N, 1, P>(pl, first, count, LineOffCols{}, tw, lane);
     for (int e = lane; e < count * N; e += 32) {
       const int li = e / N, x = e - li * N, y = first + li;
-      const double w = vs[y * N + x];
+      const double w = VS ? vs[y * N + x] : v[y * N + x];
       double2& p = pl[x * P + y];
       p.x *= w;
       p.y *= w;
@@ -436,8 +441,9 @@ __global__ void __launch_bounds__(256) k_back(const NlDev* __restrict__ nls, int
 }  // namespace
 
 size_t plane_smem_bytes(const BoxGeo& g) {
-  return sizeof(double2) * ((size_t)g.n0 + g.n1 + (size_t)g.n0 * g.pitch) + sizeof(double) * (size_t)g.n0 * g.n1 +
-         sizeof(int) * (size_t)g.n0;
+  const bool vs = g.n0 == g.n1 && v_in_smem(g.n0);
+  return sizeof(double2) * ((size_t)g.n0 + g.n1 + (size_t)g.n0 * g.pitch) +
+         (vs ? sizeof(double) * (size_t)g.n0 * g.n1 : 0) + sizeof(int) * (size_t)g.n0;
 }
 size_t stick_smem_bytes(const BoxGeo& g) { return sizeof(double2) * ((size_t)g.n2 + (size_t)g.sg * g.ld2); }
 
