@@ -81,6 +81,7 @@ SIGNATURES = {
     "bg_kset_launches": [_p, ctypes.POINTER(_i64)],
     "bg_kset_profile": [_p, _i32],
     "bg_kset_stage_times": [_p, _p],
+    "bg_local_apply_noalloc": [_p, _i64, _p, _p, _p, _p, _p, _i64, _p],
     "bg_setup_volume": [_p, ctypes.POINTER(_dbl)],
     "bg_setup_basis": [_p, _dbl, _p, _i64, ctypes.POINTER(_i64), _p, _p, _p],
     "bg_setup_grid": [_p, _dbl, _p, _p],

@@ -158,6 +158,26 @@ int bg_kset_launches(const bg_kset* set, int64_t* launches);
 int bg_kset_profile(bg_kset* set, int32_t enable);
 int bg_kset_stage_times(bg_kset* set, double* ms);
 
+/* ------------------------------------------------------------ no-allocation apply */
+/* No counterpart in the reference.  The local and kinetic part of H x for one k point,
+ * y = gather(FFT(V(r) IFFT(scatter x)))/N + T x, computed without allocating device
+ * memory: for callers whose device memory belongs to another runtime's pool (a
+ * framework caching allocator, a server arena) or that may not allocate after start-up,
+ * since cudaMalloc/cudaFree can synchronise the device and stall other streams.  All
+ * pointers are device memory the caller owns: fft_index (npw flat C-order grid indices,
+ * Miller modulo the grid), v_grid (n0*n1*n2 real, C order), kinetic (npw, Ha), x and y
+ * (npw x cols complex, interleaved, column-major).  Intermediates live in one 32 MiB
+ * scratch array that the library keeps on every device it is loaded on until the
+ * process exits; cols*n0*n1*n2 must not exceed 2,097,152 (BG_ESHAPE otherwise).  The
+ * first call on a device resolves the scratch array's device address (so make it
+ * before any stream capture on that device).  The work is enqueued on `stream`
+ * (cudaStream_t, NULL for the legacy stream).  Every call reuses the same scratch:
+ * calls whose work may overlap on the GPU (other streams, other host threads) race and
+ * must be serialised by the caller. */
+int bg_local_apply_noalloc(const int32_t dims[3], int64_t npw, const int32_t* fft_index,
+                           const double* v_grid, const double* kinetic, const double* x, double* y,
+                           int64_t cols, void* stream);
+
 /* ------------------------------------------------------------ operand builders */
 /* Restatements of the reference setup (host, FP64) for callers without the
  * reference engine.  Lattice vectors are the ROWS of rows[9] (Bohr). */
