@@ -49,6 +49,16 @@ class Projectors(ctypes.Structure):
     _fields_ = [("nproj", _i32), ("table", _p), ("natoms", _i32), ("channels", _p), ("couplings", _p)]
 
 
+class DavidsonOptions(ctypes.Structure):
+    _fields_ = [("bands", _i64), ("threshold", _dbl), ("occupied", _i64), ("first_step", _i32), ("capacity", _i64),
+                ("max_iterations", _i32), ("reserved", _i32 * 4)]
+
+
+class DavidsonStats(ctypes.Structure):
+    _fields_ = [("iterations", _i32), ("reduced_solves", _i32), ("h_calls", _i64), ("h_columns", _i64),
+                ("repairs", _i32), ("contractions", _i32), ("dropped", _i32), ("converged_count", _i32)]
+
+
 class SpeciesDesc(ctypes.Structure):
     _fields_ = [("z_valence", _dbl), ("mesh", _i32), ("r", _p), ("rab", _p), ("local", _p), ("nbeta", _i32),
                 ("l", _p), ("beta_len", _p), ("beta", _p), ("dij", _p), ("natoms", _i32), ("positions", _p)]
@@ -81,6 +91,8 @@ SIGNATURES = {
     "bg_kset_launches": [_p, ctypes.POINTER(_i64)],
     "bg_kset_profile": [_p, _i32],
     "bg_kset_stage_times": [_p, _p],
+    "bg_davidson_solve": [_p, _p, _p, ctypes.POINTER(DavidsonOptions), _p, _p, _p, ctypes.POINTER(DavidsonStats)],
+    "bg_op_create_dense": [_p, _i64, _p, _i32, _i64, _pp],
     "bg_local_apply_noalloc": [_p, _i64, _p, _p, _p, _p, _p, _i64, _p],
     "bg_setup_volume": [_p, ctypes.POINTER(_dbl)],
     "bg_setup_basis": [_p, _dbl, _p, _i64, ctypes.POINTER(_i64), _p, _p, _p],

@@ -12,8 +12,7 @@
 #include <string>
 #include <vector>
 
-#include "bg_internal.h"
-#include "hpsi.h"
+#include "op_internal.h"
 
 namespace bg {
 static thread_local std::string g_error;
@@ -23,53 +22,7 @@ std::string global_error() { return g_error; }
 
 using namespace bg;
 
-struct bg_ctx {
-  int device = 0;
-  std::string error;
-  std::mutex mu;
-};
-
-namespace {
-
-struct DevBuf {
-  void* p = nullptr;
-  size_t bytes = 0;
-  ~DevBuf() {
-    if (p) cudaFree(p);
-  }
-};
-
-}  // namespace
-
-struct bg_op {
-  bg_ctx* ctx = nullptr;
-  bool gamma = false;
-  int64_t rows = 0;
-  int64_t cap = 0;
-  int64_t cap_units = 0;
-  int dims[3] = {0, 0, 0};
-  bool has_epoch = false;
-  uint64_t epoch = 0;
-  int64_t launches = 0;
-  cudaStream_t stream = nullptr;
-  bool own_stream = false;
-  std::vector<double> diag;
-  OpTables t{};
-  BoxGeo g{};
-  NlDev nl{};
-  NlShape shape{};
-  int64_t part_cols = 0;        // capacity of nl.part in (ksplit x columns) units
-  OpTables* d_tabs = nullptr;   // device copy of t (a batch of one)
-  NlDev* d_nl = nullptr;        // device copy of nl
-  StageEvents ev;
-  std::vector<std::unique_ptr<DevBuf>> bufs;
-  DevBuf* xs = nullptr;  // host-apply staging
-  DevBuf* ys = nullptr;
-  int* err_host = nullptr;  // pinned
-};
-
-namespace {
-
+namespace bg {
 int fail(bg_ctx* ctx, int code, const std::string& msg) {
   if (ctx) {
     ctx->error = msg;
@@ -82,6 +35,9 @@ int fail(bg_ctx* ctx, int code, const std::string& msg) {
 int cuda_fail(bg_ctx* ctx, cudaError_t e, const char* what) {
   return fail(ctx, BG_EDEVICE, std::string(what) + ": " + cudaGetErrorString(e));
 }
+}  // namespace bg
+
+namespace {
 
 template <class T>
 int upload(bg_op* op, const T* host, size_t count, T** out) {
@@ -581,6 +537,10 @@ int bg_op_apply_block(bg_op* op, const double* x, double* y, int64_t rows, int64
     e = cudaMemcpyAsync(const_cast<double*>(dx), x, dpc * cols * sizeof(double), cudaMemcpyHostToDevice, op->stream);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "copy in");
   }
+  if (op->is_dense) {
+    int rc = dense_apply(op, dx, dy, cols);
+    if (rc != BG_OK) return rc;
+  } else {
   Batch bt;
   bt.nk = 1;
   CallArgs& a = bt.a[0];
@@ -595,6 +555,7 @@ int bg_op_apply_block(bg_op* op, const double* x, double* y, int64_t rows, int64
     NlShape sh = op->shape;
     sh.ksplit = ksplit_for(op->rows, sh.nproj, cols, &sh.kchunk);
     op->launches += launch_nonlocal(op->d_nl, op->gamma ? 1 : 0, sh, (int)op->rows, bt, op->stream, &op->ev);
+  }
   }
   e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(ctx, e, "kernel launch");
@@ -710,6 +671,7 @@ int bg_kset_create(bg_ctx* ctx, int32_t n, bg_op* const* ops, bg_kset** out) {
   for (int i = 0; i < n; ++i) {
     const bg_op* o = ops[i];
     if (!o || o->ctx != ctx) return fail(ctx, BG_EINVAL, "operators must belong to this context");
+    if (o->is_dense) return fail(ctx, BG_EINVAL, "dense operators cannot join a k-point set");
     if (o->gamma != o0->gamma || std::memcmp(o->dims, o0->dims, sizeof o->dims) != 0 ||
         o->shape.nproj != o0->shape.nproj || o->shape.natoms != o0->shape.natoms)
       return fail(ctx, BG_ESHAPE, "operators of a set need one grid, one kind and one projector layout");

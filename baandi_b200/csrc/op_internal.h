@@ -1,0 +1,64 @@
+// Operator and context objects shared by the C ABI implementation files.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "bg_internal.h"
+#include "hpsi.h"
+
+struct bg_ctx {
+  int device = 0;
+  std::string error;
+  std::mutex mu;
+};
+
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  ~DevBuf() {
+    if (p) cudaFree(p);
+  }
+};
+
+struct bg_op {
+  bg_ctx* ctx = nullptr;
+  bool gamma = false;
+  int64_t rows = 0;
+  int64_t cap = 0;
+  int64_t cap_units = 0;
+  int dims[3] = {0, 0, 0};
+  bool has_epoch = false;
+  uint64_t epoch = 0;
+  int64_t launches = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  std::vector<double> diag;
+  bg::OpTables t{};
+  bg::BoxGeo g{};
+  bg::NlDev nl{};
+  bg::NlShape shape{};
+  int64_t part_cols = 0;        // capacity of nl.part in (ksplit x columns) units
+  bg::OpTables* d_tabs = nullptr;   // device copy of t (a batch of one)
+  bg::NlDev* d_nl = nullptr;        // device copy of nl
+  bg::StageEvents ev;
+  std::vector<std::unique_ptr<DevBuf>> bufs;
+  DevBuf* xs = nullptr;  // host-apply staging
+  DevBuf* ys = nullptr;
+  int* err_host = nullptr;  // pinned
+  // Dense operator (tests and fixtures): H is rows x rows on the device.
+  bool is_dense = false;
+  double* dense = nullptr;
+};
+
+
+namespace bg {
+// Failure message on the context (or the thread's context-free slot) and status.
+int fail(bg_ctx* ctx, int code, const std::string& msg);
+int cuda_fail(bg_ctx* ctx, cudaError_t e, const char* what);
+// y = H x for a dense operator (device pointers, op stream).
+int dense_apply(bg_op* op, const double* x, double* y, int64_t cols);
+}  // namespace bg

@@ -1,0 +1,78 @@
+"""Host-side mirror of the reference block Davidson over the C ABI (bg_davidson_solve).
+
+Options/Solution mirror crates/dft-solvers/src/ref_davidson.rs:39-93: `bands`,
+`threshold` (occupied Ritz-change threshold, Ha), `occupied`, `first_step`,
+`capacity` (0 = 2 bands), `max_iterations` (default 20); the band threshold rule is
+ref_davidson.rs:70-76.  The solver applies H and forms every subspace product on the
+GPU; exhaustion of max_iterations returns an explicitly unconverged solution.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _lib as L
+from .hamiltonian import SolverError, _Operator
+
+
+@dataclass
+class Options:
+    bands: int
+    threshold: float
+    occupied: int
+    first_step: bool = False
+    capacity: int = 0
+    max_iterations: int = 20
+
+    def band_threshold(self, band: int) -> float:
+        if self.first_step or band < self.occupied:
+            return self.threshold
+        return max(5.0 * self.threshold, 5e-6)
+
+
+@dataclass
+class Solution:
+    eigenvalues: np.ndarray
+    eigenvectors: np.ndarray
+    converged: np.ndarray
+    iterations: int
+    reduced_solves: int
+    h_calls: int
+    h_columns: int
+    repairs: int
+    contractions: int
+    dropped: int
+
+
+def preconditioner_denominator(hamiltonian_diagonal_ha, eigenvalue_ha):
+    """Smooth positive diagonal regulariser of ref_davidson.rs:418-422 (the device kernel
+    uses the same formula)."""
+    x = 2.0 * (np.asarray(hamiltonian_diagonal_ha, dtype=np.float64) - eigenvalue_ha)
+    z = np.abs(x - 1.0)
+    return 0.25 * (np.where(x >= 1.0, 2.0 * x, 2.0) + 1.0 / (np.hypot(z, 1.0) + z))
+
+
+def solve(operator: _Operator, start: np.ndarray, hamiltonian_diagonal: np.ndarray, options: Options) -> Solution:
+    """Lowest `options.bands` eigenpairs of `operator` from `start` (rows x bands)."""
+    lib = L.load()
+    real = operator.is_real()
+    dt = np.float64 if real else np.complex128
+    x0 = np.asfortranarray(start, dtype=dt)
+    rows, n = x0.shape
+    if rows != operator.global_len() or n != options.bands:
+        raise SolverError(L.BG_ESHAPE, "start must be rows x bands")
+    diag = np.ascontiguousarray(hamiltonian_diagonal, dtype=np.float64)
+    o = L.DavidsonOptions(options.bands, options.threshold, options.occupied, 1 if options.first_step else 0,
+                          options.capacity, options.max_iterations)
+    vals = np.zeros(n)
+    vecs = np.zeros((rows, n), dtype=dt, order="F")
+    conv = np.zeros(n, np.int32)
+    st = L.DavidsonStats()
+    p = lambda a: a.ctypes.data_as(ctypes.c_void_p)
+    rc = lib.bg_davidson_solve(operator.handle, p(x0), p(diag), ctypes.byref(o), p(vals), p(vecs), p(conv),
+                               ctypes.byref(st))
+    operator._check(rc)
+    return Solution(vals, vecs, conv.astype(bool), st.iterations, st.reduced_solves, st.h_calls, st.h_columns,
+                    st.repairs, st.contractions, st.dropped)

@@ -165,6 +165,9 @@ class _Operator:
         except Exception:
             pass
 
+    def is_real(self) -> bool:
+        return self._gamma
+
     # -- apply
     def _apply_raw(self, x_ptr, y_ptr, cols, kind):
         self._check(self._lib.bg_op_apply_block(self.handle, ctypes.c_void_p(x_ptr), ctypes.c_void_p(y_ptr),
@@ -321,3 +324,30 @@ class KPointSet:
             self.close()
         except Exception:
             pass
+
+
+class DenseOperator(_Operator):
+    """y = H x for an explicit rows x rows matrix (fixtures and exact small tests of the
+    solver); real when H is real, complex otherwise."""
+
+    def __init__(self, h: np.ndarray, capacity: int, ctx: Context | None = None):
+        self.ctx = ctx or default_context()
+        self._lib = self.ctx._lib
+        h = np.asarray(h)
+        self._gamma = not np.iscomplexobj(h)
+        self._h = np.asfortranarray(h, dtype=np.float64 if self._gamma else np.complex128)
+        self.npw = h.shape[0]
+        self.dims = [0, 0, 0]
+        hh = ctypes.c_void_p()
+        self._check(self._lib.bg_op_create_dense(self.ctx.handle, self.npw, self._h.ctypes.data_as(ctypes.c_void_p),
+                                                 0 if self._gamma else 1, int(capacity), ctypes.byref(hh)))
+        self.handle = hh
+        self._capacity = int(capacity)
+        self._epoch = 0
+
+    def apply_block(self, x, out=None):
+        dt = np.float64 if self._gamma else np.complex128
+        xin = np.asfortranarray(x, dtype=dt)
+        y = np.zeros_like(xin, order="F") if out is None else out
+        self._apply_raw(xin.ctypes.data, y.ctypes.data, xin.shape[1], L.BG_PTR_HOST)
+        return y

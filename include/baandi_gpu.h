@@ -158,6 +158,47 @@ int bg_kset_launches(const bg_kset* set, int64_t* launches);
 int bg_kset_profile(bg_kset* set, int32_t enable);
 int bg_kset_stage_times(bg_kset* set, double* ms);
 
+/* ------------------------------------------------------------ block Davidson */
+/* Options and Solution mirror crates/dft-solvers/src/ref_davidson.rs:39-93. */
+typedef struct {
+  int64_t bands;          /* n: lowest eigenpairs wanted                                 */
+  double threshold;       /* occupied Ritz-change threshold (Ha, strict inequality)       */
+  int64_t occupied;       /* leading occupied bands; others use max(5 threshold, 5e-6)   */
+  int32_t first_step;     /* nonzero: every band uses `threshold`                       */
+  int64_t capacity;       /* basis columns; 0 selects min(rows, 2 bands)                 */
+  int32_t max_iterations; /* correction iterations (reference default 20)               */
+  int32_t reserved[4];
+} bg_davidson_options;
+
+typedef struct {
+  int32_t iterations;
+  int32_t reduced_solves;
+  int64_t h_calls;
+  int64_t h_columns;
+  int32_t repairs;
+  int32_t contractions;
+  int32_t dropped;         /* corrections dropped as dependent or of vanishing norm     */
+  int32_t converged_count;
+} bg_davidson_stats;
+
+/* Reference block Davidson (crates/dft-solvers/src/ref_davidson.rs:117-366 for the
+ * Gamma operator, ref_davidson_complex.rs:641-1110 for complex operators): H applies
+ * and subspace products on the GPU, the reduced problem on the host.  start: rows x
+ * bands column-major host block (interleaved complex for complex operators);
+ * diagonal: rows host doubles (kinetic + nonlocal diagonal + mean local potential).
+ * Outputs (host): eigenvalues[bands] ascending, eigenvectors rows x bands, converged
+ * flags (Ritz change below the band threshold).  An iteration limit returns BG_OK
+ * with unconverged flags, as the reference does.  The operator's capacity must be at
+ * least the Davidson capacity. */
+int bg_davidson_solve(bg_op* op, const double* start, const double* diagonal,
+                      const bg_davidson_options* options, double* eigenvalues, double* eigenvectors,
+                      int32_t* converged, bg_davidson_stats* stats);
+
+/* Dense operator y = H x of a rows x rows column-major matrix (interleaved complex when
+ * is_complex), for fixtures and small exact tests of the solver. */
+int bg_op_create_dense(bg_ctx* ctx, int64_t rows, const double* h, int32_t is_complex, int64_t capacity,
+                       bg_op** out);
+
 /* ------------------------------------------------------------ no-allocation apply */
 /* No counterpart in the reference.  The local and kinetic part of H x for one k point,
  * y = gather(FFT(V(r) IFFT(scatter x)))/N + T x, computed without allocating device
