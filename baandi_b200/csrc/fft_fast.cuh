@@ -266,6 +266,57 @@ __device__ __forceinline__ void group(double2* base, int first, int count, Off o
   stages_from<N, SIGN, ES, 0, 1>(base, first, count, off, tw, lane);
 }
 
+// Inverse transform, x w(element), forward transform of this warp's lines for a
+// two-stage plan (R1, R2), with the middle in registers: the inverse's last stage
+// (radix R2, span R1) leaves butterfly j holding elements j + u R1 (u < R2) in natural
+// order, exactly the inputs of the first stage of a forward transform run with the
+// plan reversed (R2, R1).  So that butterfly multiplies by w, runs the forward radix-R2
+// DFT and stores once; shared memory sees load, store, load, store, load, store per
+// element instead of ten accesses.  w(line, x) is read through `wgt`.
+template <int N, int ES, class Off, class W>
+__device__ __forceinline__ void inverse_weight_forward(double2* base, int first, int count, Off off,
+                                                       const double2* __restrict__ tw, W wgt, int lane) {
+  using P = Plan<N>;
+  static_assert(P::nst == 2, "two-stage plans only");
+  constexpr int R1 = P::radix[0];
+  constexpr int R2 = P::radix[1];
+  stage<N, R1, 1, 1, ES>(base, first, count, off, tw, lane);
+  constexpr int SPAN = N / R2;  // == R1
+  static_assert(SPAN <= 32, "one butterfly per lane");
+  constexpr int LPR = 32 / SPAN;
+  const int li = lane / SPAN;
+  const int j = lane - li * SPAN;
+  const bool lane_ok = li < LPR;
+  for (int r0 = 0; r0 < count; r0 += LPR) {
+    double2 v[R2];
+    const bool act = lane_ok && r0 + li < count;
+    const int line = first + r0 + li;
+    const int lo = act ? off(line) : 0;
+    if (act) {
+#pragma unroll
+      for (int t = 0; t < R2; ++t) v[t] = base[lo + (j + t * SPAN) * ES];
+    }
+    __syncwarp();
+    if (act) {
+#pragma unroll
+      for (int t = 1; t < R2; ++t) v[t] = cmul(v[t], tw[t * j]);  // w^(t k N/(R1 R2)), k = j
+      Dft<R2, 1>::run(v);
+#pragma unroll
+      for (int u = 0; u < R2; ++u) {
+        const double w = wgt(line, j + u * R1);
+        v[u].x *= w;
+        v[u].y *= w;
+      }
+      Dft<R2, -1>::run(v);
+#pragma unroll
+      for (int u = 0; u < R2; ++u) base[lo + (j * R2 + u) * ES] = v[u];
+    }
+    __syncwarp();
+  }
+  // forward: remaining stage of the reversed plan, radix R1 after span R2
+  stage<N, R1, R2, -1, ES>(base, first, count, off, tw, lane);
+}
+
 // Lines of a pass owned by this warp: a contiguous block of ceil(L / warps).
 __device__ __forceinline__ void owned_lines(int nlines, int* first, int* count) {
   const int nw = blockDim.x >> 5, warp = threadIdx.x >> 5;

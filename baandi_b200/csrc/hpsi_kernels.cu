@@ -186,16 +186,22 @@ __global__ void __launch_bounds__(256, 4) k_planes_fast(const OpTables* __restri
   int first, count;
   fast::owned_lines(N, &first, &count);
   if (count > 0) {
-    fast::group<N, 1, P>(pl, first, count, LineOffCols{}, tw, lane);
-    for (int e = lane; e < count * N; e += 32) {
-      const int li = e / N, x = e - li * N, y = first + li;
-      const double w = VS ? vs[y * N + x] : v[y * N + x];
-      double2& p = pl[x * P + y];
-      p.x *= w;
-      p.y *= w;
+    if constexpr (fast::Plan<N>::nst == 2) {
+      // line = column y, element = x: weight V(x, y, z)
+      auto wgt = [&](int y, int x) -> double { return VS ? vs[y * N + x] : v[y * N + x]; };
+      fast::inverse_weight_forward<N, P>(pl, first, count, LineOffCols{}, tw, wgt, lane);
+    } else {
+      fast::group<N, 1, P>(pl, first, count, LineOffCols{}, tw, lane);
+      for (int e = lane; e < count * N; e += 32) {
+        const int li = e / N, x = e - li * N, y = first + li;
+        const double w = VS ? vs[y * N + x] : v[y * N + x];
+        double2& p = pl[x * P + y];
+        p.x *= w;
+        p.y *= w;
+      }
+      __syncwarp();
+      fast::group<N, -1, P>(pl, first, count, LineOffCols{}, tw, lane);
     }
-    __syncwarp();
-    fast::group<N, -1, P>(pl, first, count, LineOffCols{}, tw, lane);
   }
   __syncthreads();
   fast::pass<N, -1, 1>(pl, nx, LineOffTable{rows}, tw);
