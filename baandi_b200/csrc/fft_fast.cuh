@@ -11,8 +11,8 @@
 // 8, 9 and 12; the 6-, 8-, 9- and 12-point DFTs are Cooley-Tukey splits (2x3, 2x4,
 // 3x3, 3x4) done in registers.
 //
-// Twiddles w^(t k N/(Ns R)) come from the length-N table exp(+2 pi i q/N) in shared
-// memory (conjugated for the forward sign).
+// Twiddles w^(t k N/(Ns R)) are powers of one entry of the length-N table
+// exp(+2 pi i q/N) in shared memory (conjugated for the forward sign).
 #pragma once
 #include "fft_dev.cuh"
 
@@ -232,11 +232,15 @@ __device__ __forceinline__ void stage(double2* base, int first, int count, Off o
     for (int q = 0; q < K; ++q) {
       if (lo[q] >= 0) {
         if (NS > 1) {
+          // w^(t k STEP) as powers of one table entry: one shared-memory load per
+          // butterfly instead of R - 1 (relative error grows by about one ulp per power)
+          double2 w1 = tw[kk[q]];
+          if (SIGN < 0) w1.y = -w1.y;
+          double2 x = w1;
 #pragma unroll
           for (int t = 1; t < R; ++t) {
-            double2 x = tw[t * kk[q]];
-            if (SIGN < 0) x.y = -x.y;
             v[q][t] = cmul(v[q][t], x);
+            if (t + 1 < R) x = cmul(x, w1);
           }
         }
         Dft<R, SIGN>::run(v[q]);
@@ -298,8 +302,15 @@ __device__ __forceinline__ void inverse_weight_forward(double2* base, int first,
     }
     __syncwarp();
     if (act) {
+      {
+        const double2 w1 = tw[j];  // w^(t k N/(R1 R2)) with k = j, as powers of w^j
+        double2 x = w1;
 #pragma unroll
-      for (int t = 1; t < R2; ++t) v[t] = cmul(v[t], tw[t * j]);  // w^(t k N/(R1 R2)), k = j
+        for (int t = 1; t < R2; ++t) {
+          v[t] = cmul(v[t], x);
+          if (t + 1 < R2) x = cmul(x, w1);
+        }
+      }
       Dft<R2, 1>::run(v);
 #pragma unroll
       for (int u = 0; u < R2; ++u) {

@@ -54,7 +54,7 @@ __device__ __forceinline__ bool finite2(double a, double b) { return isfinite(a)
 
 // ---------------------------------------------------------------- pass 1
 template <bool GAMMA, int N>
-__global__ void __launch_bounds__(256, N == 0 ? 1 : 3) k_sticks_inverse(const OpTables* __restrict__ tabs, BoxGeo g, Batch b) {
+__global__ void __launch_bounds__(N == 0 ? 256 : 128, N == 0 ? 1 : 6) k_sticks_inverse(const OpTables* __restrict__ tabs, BoxGeo g, Batch b) {
   const OpTables& t = tabs[blockIdx.z];
   const CallArgs& a = b.a[blockIdx.z];
   const int grp = blockIdx.x, unit = blockIdx.y;
@@ -210,7 +210,7 @@ __global__ void __launch_bounds__(256, 4) k_planes_fast(const OpTables* __restri
 
 // ---------------------------------------------------------------- pass 3
 template <bool GAMMA, int N>
-__global__ void __launch_bounds__(256, N == 0 ? 1 : 3) k_sticks_forward(const OpTables* __restrict__ tabs, BoxGeo g, Batch b) {
+__global__ void __launch_bounds__(N == 0 ? 256 : 128, N == 0 ? 1 : 6) k_sticks_forward(const OpTables* __restrict__ tabs, BoxGeo g, Batch b) {
   const OpTables& t = tabs[blockIdx.z];
   const CallArgs& a = b.a[blockIdx.z];
   const int grp = blockIdx.x, unit = blockIdx.y;
@@ -470,7 +470,8 @@ struct StageScope {
 template <bool GAMMA, int N>
 static void local_kernels(const OpTables* tabs, const BoxGeo& g, const Batch& b, dim3 sgrid, dim3 pgrid, size_t ss,
                           size_t ps, cudaStream_t s, StageEvents* ev) {
-  { StageScope sc(ev, 0, s); k_sticks_inverse<GAMMA, N><<<sgrid, 256, ss, s>>>(tabs, g, b); }
+  constexpr int st = N == 0 ? 256 : 128;
+  { StageScope sc(ev, 0, s); k_sticks_inverse<GAMMA, N><<<sgrid, st, ss, s>>>(tabs, g, b); }
   if constexpr (N == 0) {
     StageScope sc(ev, 1, s);
     k_planes<<<pgrid, 512, ps, s>>>(tabs, g, b);
@@ -481,7 +482,7 @@ static void local_kernels(const OpTables* tabs, const BoxGeo& g, const Batch& b,
     else
       k_planes<<<pgrid, 512, ps, s>>>(tabs, g, b);
   }
-  { StageScope sc(ev, 2, s); k_sticks_forward<GAMMA, N><<<sgrid, 256, ss, s>>>(tabs, g, b); }
+  { StageScope sc(ev, 2, s); k_sticks_forward<GAMMA, N><<<sgrid, st, ss, s>>>(tabs, g, b); }
 }
 
 template <bool GAMMA>
