@@ -655,7 +655,41 @@ struct bg_kset {
   bool own_stream = false;
   StageEvents ev;
   int64_t launches = 0;
+  // host-buffer applies: copy-in, compute and copy-out streams pipelined over chunks
+  static constexpr int kChunks = 4;
+  cudaStream_t pipe[3] = {nullptr, nullptr, nullptr};
+  cudaEvent_t in_done[kChunks] = {}, work_done[kChunks] = {};
 };
+
+namespace {
+// Launch the local and nonlocal stages of operators [k0, k1) of a set on one stream.
+int enqueue_range(bg_kset* ks, int k0, int k1, const CallArgs* args, const int64_t* cols, cudaStream_t s,
+                  StageEvents* ev) {
+  Batch bt;
+  bt.nk = k1 - k0;
+  int max_groups = 0, max_rows = 0;
+  int64_t max_cols = 0;
+  for (int k = k0; k < k1; ++k) {
+    bt.a[k - k0] = args[k];
+    max_groups = std::max(max_groups, ks->ops[k]->t.ngroups);
+    max_rows = std::max(max_rows, (int)ks->ops[k]->rows);
+    max_cols = std::max(max_cols, cols[k]);
+  }
+  if (max_cols == 0) return 0;
+  int launches = launch_local(ks->d_tabs + k0, ks->gamma, max_groups, ks->g, bt, s, ev);
+  if (ks->shape.nproj > 0) {
+    NlShape sh = ks->shape;
+    int64_t tiles = 0, cap = 1 << 30;
+    for (int k = k0; k < k1; ++k) {
+      tiles += ((sh.nproj + 31) / 32) * ((cols[k] + 31) / 32);
+      if (cols[k] > 0) cap = std::min<int64_t>(cap, ks->ops[k]->part_cols / cols[k]);
+    }
+    sh.ksplit = ksplit_tiles(max_rows, std::max<int64_t>(tiles, 1), &sh.kchunk, cap);
+    launches += launch_nonlocal(ks->d_nl + k0, ks->gamma, sh, max_rows, bt, s, ev);
+  }
+  return launches;
+}
+}  // namespace
 
 extern "C" {
 
@@ -693,6 +727,11 @@ int bg_kset_create(bg_ctx* ctx, int32_t n, bg_op* const* ops, bg_kset** out) {
   if (e == cudaSuccess) e = cudaMemcpy(ks->d_nl, nls.data(), sizeof(NlDev) * n, cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ks->stream, cudaStreamNonBlocking);
   for (int i = 0; i < 2 * kStages && e == cudaSuccess; ++i) e = cudaEventCreate(&ks->ev.ev[i]);
+  for (int i = 0; i < 3 && e == cudaSuccess; ++i) e = cudaStreamCreateWithFlags(&ks->pipe[i], cudaStreamNonBlocking);
+  for (int i = 0; i < bg_kset::kChunks && e == cudaSuccess; ++i) {
+    e = cudaEventCreateWithFlags(&ks->in_done[i], cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ks->work_done[i], cudaEventDisableTiming);
+  }
   if (e != cudaSuccess) {
     if (ks->d_tabs) cudaFree(ks->d_tabs);
     if (ks->d_nl) cudaFree(ks->d_nl);
@@ -709,6 +748,15 @@ int bg_kset_destroy(bg_kset* ks) {
   for (int i = 0; i < 2 * kStages; ++i)
     if (ks->ev.ev[i]) cudaEventDestroy(ks->ev.ev[i]);
   if (ks->own_stream && ks->stream) cudaStreamDestroy(ks->stream);
+  for (int i = 0; i < 3; ++i)
+    if (ks->pipe[i]) {
+      cudaStreamSynchronize(ks->pipe[i]);
+      cudaStreamDestroy(ks->pipe[i]);
+    }
+  for (int i = 0; i < bg_kset::kChunks; ++i) {
+    if (ks->in_done[i]) cudaEventDestroy(ks->in_done[i]);
+    if (ks->work_done[i]) cudaEventDestroy(ks->work_done[i]);
+  }
   cudaFree(ks->d_tabs);
   cudaFree(ks->d_nl);
   delete ks;
@@ -735,48 +783,61 @@ int bg_kset_apply(bg_kset* ks, const double* const* x, double* const* y, const i
   }
   cudaError_t e = cudaSetDevice(ctx->device);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaSetDevice");
+  std::vector<CallArgs> args(n);
   for (int k = 0; k < n; ++k) {
     bg_op* op = ks->ops[k];
     const size_t dpc = op->gamma ? (size_t)op->rows : (size_t)2 * op->rows;
-    CallArgs& a = bt.a[k];
+    CallArgs& a = args[k];
     a.x = x[k];
     a.y = y[k];
-    if (ptr_kind == BG_PTR_HOST && cols[k] > 0) {
+    if (ptr_kind == BG_PTR_HOST) {
       a.x = static_cast<const double*>(op->xs->p);
       a.y = static_cast<double*>(op->ys->p);
-      e = cudaMemcpyAsync(const_cast<double*>(a.x), x[k], dpc * cols[k] * sizeof(double), cudaMemcpyHostToDevice,
-                          ks->stream);
-      if (e != cudaSuccess) return cuda_fail(ctx, e, "copy in");
     }
     a.ldx = a.ldy = (int64_t)dpc;
     a.cols = (int)cols[k];
     a.units = op->gamma ? (int)((cols[k] + 1) / 2) : (int)cols[k];
   }
   if (max_cols == 0) return BG_OK;
-  ks->launches += launch_local(ks->d_tabs, ks->gamma, ks->max_groups, ks->g, bt, ks->stream, &ks->ev);
-  if (ks->shape.nproj > 0) {
-    NlShape sh = ks->shape;
-    int64_t tiles = 0, cap = 1 << 30;
-    for (int k = 0; k < n; ++k) {
-      tiles += ((sh.nproj + 31) / 32) * ((cols[k] + 31) / 32);
-      if (cols[k] > 0) cap = std::min<int64_t>(cap, ks->ops[k]->part_cols / cols[k]);
+  if (ptr_kind == BG_PTR_DEVICE) {
+    ks->launches += enqueue_range(ks, 0, n, args.data(), cols, ks->stream, &ks->ev);
+    e = cudaGetLastError();
+    return e == cudaSuccess ? BG_OK : cuda_fail(ctx, e, "kernel launch");
+  }
+  // Host buffers: chunks of operators flow through copy-in, compute and copy-out streams,
+  // so the transfers of one chunk overlap the kernels of its neighbours.
+  const int nch = std::min(n, (int)bg_kset::kChunks);
+  cudaStream_t in = ks->pipe[0], work = ks->pipe[1], out = ks->pipe[2];
+  for (int c = 0; c < nch; ++c) {
+    const int k0 = (int)((int64_t)n * c / nch), k1 = (int)((int64_t)n * (c + 1) / nch);
+    for (int k = k0; k < k1; ++k) {
+      if (cols[k] == 0) continue;
+      bg_op* op = ks->ops[k];
+      const size_t dpc = op->gamma ? (size_t)op->rows : (size_t)2 * op->rows;
+      e = cudaMemcpyAsync(const_cast<double*>(args[k].x), x[k], dpc * cols[k] * sizeof(double),
+                          cudaMemcpyHostToDevice, in);
+      if (e != cudaSuccess) return cuda_fail(ctx, e, "copy in");
     }
-    sh.ksplit = ksplit_tiles(ks->max_rows, std::max<int64_t>(tiles, 1), &sh.kchunk, cap);
-    ks->launches += launch_nonlocal(ks->d_nl, ks->gamma, sh, ks->max_rows, bt, ks->stream, &ks->ev);
+    cudaEventRecord(ks->in_done[c], in);
+    cudaStreamWaitEvent(work, ks->in_done[c], 0);
+    ks->launches += enqueue_range(ks, k0, k1, args.data(), cols, work, nullptr);
+    cudaEventRecord(ks->work_done[c], work);
+    cudaStreamWaitEvent(out, ks->work_done[c], 0);
+    for (int k = k0; k < k1; ++k) {
+      if (cols[k] == 0) continue;
+      bg_op* op = ks->ops[k];
+      const size_t dpc = op->gamma ? (size_t)op->rows : (size_t)2 * op->rows;
+      e = cudaMemcpyAsync(y[k], args[k].y, dpc * cols[k] * sizeof(double), cudaMemcpyDeviceToHost, out);
+      if (e != cudaSuccess) return cuda_fail(ctx, e, "copy out");
+    }
   }
   e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(ctx, e, "kernel launch");
-  if (ptr_kind == BG_PTR_HOST) {
-    for (int k = 0; k < n; ++k) {
-      bg_op* op = ks->ops[k];
-      if (cols[k] == 0) continue;
-      const size_t dpc = op->gamma ? (size_t)op->rows : (size_t)2 * op->rows;
-      e = cudaMemcpyAsync(y[k], bt.a[k].y, dpc * cols[k] * sizeof(double), cudaMemcpyDeviceToHost, ks->stream);
-      if (e != cudaSuccess) return cuda_fail(ctx, e, "copy out");
-    }
-    return bg_kset_sync(ks);
+  for (int i = 0; i < 3; ++i) {
+    e = cudaStreamSynchronize(ks->pipe[i]);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "k-point set");
   }
-  return BG_OK;
+  return bg_kset_sync(ks);
 }
 
 int bg_kset_sync(bg_kset* ks) {

@@ -332,7 +332,6 @@ def run_ours(args):
         hx_t.copy_(x)
         hx.append(hx_t.numpy().T)
         hy.append(torch.empty(x.shape, dtype=x.dtype, pin_memory=True).numpy().T)
-    kset.set_stream(0)
     for _ in range(2):
         kset.apply_blocks(hx, hy)
     if dist:
