@@ -32,6 +32,7 @@
 #include <vector>
 
 #include "blas_dev.cuh"
+#include "gemm_tiles.cuh"
 #include "dense_host.h"
 #include "op_internal.h"
 
@@ -184,7 +185,7 @@ int Solver<T>::gram(const D* A, int m, const D* B, int k, T* G, int ldg) {
   chunk = ((chunk + 31) / 32) * 32;
   ks = (rows_ + chunk - 1) / chunk;
   const dim3 grid((m + 31) / 32, (k + 31) / 32, (unsigned)ks);
-  k_gemm_tn<D><<<grid, 256, 0, s_>>>(A, rows_, B, rows_, part_, m, k, rows_, chunk);
+  k_gemm_tn<D><<<grid, 64, 0, s_>>>(A, rows_, B, rows_, part_, m, k, rows_, chunk);
   k_sum_parts<D><<<(unsigned)std::min<int64_t>(((int64_t)m * k + 255) / 256, 4096), 256, 0, s_>>>(part_, (int)ks, m, k,
                                                                                                   small_, m);
   std::vector<T> h((size_t)m * k);
@@ -201,7 +202,7 @@ int Solver<T>::rotate(const D* A, int m, const T* coef, int k, D* Cout, bool acc
   if (k == 0) return BG_OK;
   cudaMemcpyAsync(coef_, coef, sizeof(T) * (size_t)m * k, cudaMemcpyHostToDevice, s_);
   const dim3 grid((unsigned)((rows_ + 63) / 64), (k + 31) / 32);
-  k_gemm_nn<D><<<grid, 256, 0, s_>>>(A, rows_, coef_, m, Cout, rows_, rows_, k, m, accumulate ? 1 : 0);
+  k_gemm_nn<D><<<grid, 128, 0, s_>>>(A, rows_, coef_, m, Cout, rows_, rows_, k, m, accumulate ? 1 : 0);
   int rc = sync("rotate");  // coef host buffer is reused by the caller
   return rc ? rc : check("rotate");
 }
@@ -538,9 +539,9 @@ int dense_apply(bg_op* op, const double* x, double* y, int64_t cols) {
   const int64_t n = op->rows;
   const dim3 grid((unsigned)((n + 63) / 64), (unsigned)((cols + 31) / 32));
   if (op->gamma)
-    k_gemm_nn<double><<<grid, 256, 0, op->stream>>>(op->dense, n, x, n, y, n, n, (int)cols, (int)n, 0);
+    k_gemm_nn<double><<<grid, 128, 0, op->stream>>>(op->dense, n, x, n, y, n, n, (int)cols, (int)n, 0);
   else
-    k_gemm_nn<double2><<<grid, 256, 0, op->stream>>>(reinterpret_cast<const double2*>(op->dense), n,
+    k_gemm_nn<double2><<<grid, 128, 0, op->stream>>>(reinterpret_cast<const double2*>(op->dense), n,
                                                     reinterpret_cast<const double2*>(x), n,
                                                     reinterpret_cast<double2*>(y), n, n, (int)cols, (int)n, 0);
   op->launches += 1;

@@ -194,6 +194,15 @@ struct Dft<12, SIGN> {
 };
 
 // --------------------------------------------------------------------- stages
+// Lane index read with a volatile instruction: the per-lane butterfly indices of a stage
+// are then recomputed where the stage runs instead of being hoisted out of an enclosing
+// loop (a persistent kernel would otherwise keep every stage's indices live in registers).
+__device__ __forceinline__ int lane_id() {
+  int l;
+  asm volatile("mov.u32 %0, %%laneid;" : "=r"(l));
+  return l;
+}
+
 // Stage (R, NS) on lines first .. first+count-1 of this warp; ES = element stride.
 // A lane's butterfly index j is the same in every round.
 template <int N, int R, int NS, int SIGN, int ES, class Off>
@@ -203,6 +212,7 @@ __device__ __forceinline__ void stage(double2* base, int first, int count, Off o
   constexpr int STEP = N / (NS * R);
   constexpr int K = (SPAN + 31) / 32;                 // butterflies per lane when a line exceeds a warp
   constexpr int LPR = SPAN <= 32 ? 32 / SPAN : 1;     // whole lines per round
+  lane = lane_id();
   int jj[K], li[K], oo[K], kk[K];
 #pragma unroll
   for (int q = 0; q < K; ++q) {
@@ -288,6 +298,7 @@ __device__ __forceinline__ void inverse_weight_forward(double2* base, int first,
   constexpr int SPAN = N / R2;  // == R1
   static_assert(SPAN <= 32, "one butterfly per lane");
   constexpr int LPR = 32 / SPAN;
+  lane = lane_id();
   const int li = lane / SPAN;
   const int j = lane - li * SPAN;
   const bool lane_ok = li < LPR;

@@ -21,6 +21,7 @@
 // (unpack + kinetic), :957-1017, 1184-1248 (nonlocal).
 #include "hpsi.h"
 #include "fft_fast.cuh"
+#include "gemm_tiles.cuh"
 
 namespace bg {
 
@@ -310,53 +311,17 @@ struct Ops<double2> {
 
 // part[ks][c][p] = sum_{rows of chunk ks} P[p][row]^* X[c][row]; tile 32 p x 32 c.
 template <class T>
-__global__ void __launch_bounds__(256) k_project(const NlDev* __restrict__ nls, int nproj, int ksplit, int kchunk,
-                                                 Batch b) {
-  __shared__ T As[32][33];
-  __shared__ T Bs[32][33];
+__global__ void __launch_bounds__(64) k_project(const NlDev* __restrict__ nls, int nproj, int ksplit, int kchunk,
+                                                Batch b) {
   const int kb = blockIdx.z / ksplit, ks = blockIdx.z - kb * ksplit;
   const NlDev& nl = nls[kb];
   const CallArgs& ca = b.a[kb];
   const int cols = ca.cols, rows = nl.rows;
   if ((int)blockIdx.y * 32 >= cols) return;
-  const T* __restrict__ P = reinterpret_cast<const T*>(nl.p);
-  const T* __restrict__ X = reinterpret_cast<const T*>(ca.x);
-  const int64_t ldx = ca.ldx / (int64_t)(sizeof(T) / sizeof(double));
-  T* __restrict__ part = reinterpret_cast<T*>(nl.part);
-  const int p0 = blockIdx.x * 32, c0 = blockIdx.y * 32;
-  const int tp = threadIdx.x & 15, tc = threadIdx.x >> 4;
-  T acc[2][2];
-#pragma unroll
-  for (int i = 0; i < 2; ++i)
-#pragma unroll
-    for (int j = 0; j < 2; ++j) acc[i][j] = Ops<T>::zero();
-  const int g0 = ks * kchunk, g1 = min(rows, g0 + kchunk);
-  for (int gb = g0; gb < g1; gb += 32) {
-    for (int i = threadIdx.x; i < 1024; i += 256) {
-      const int gg = i & 31, q = i >> 5;
-      const int g = gb + gg;
-      As[gg][q] = (g < g1 && p0 + q < nproj) ? P[(int64_t)(p0 + q) * rows + g] : Ops<T>::zero();
-      Bs[gg][q] = (g < g1 && c0 + q < cols) ? X[(int64_t)(c0 + q) * ldx + g] : Ops<T>::zero();
-    }
-    __syncthreads();
-#pragma unroll 8
-    for (int gg = 0; gg < 32; ++gg) {
-      const T a0 = As[gg][tp], a1 = As[gg][tp + 16];
-      const T b0 = Bs[gg][tc], b1 = Bs[gg][tc + 16];
-      acc[0][0] = Ops<T>::cmac(acc[0][0], a0, b0);
-      acc[1][0] = Ops<T>::cmac(acc[1][0], a1, b0);
-      acc[0][1] = Ops<T>::cmac(acc[0][1], a0, b1);
-      acc[1][1] = Ops<T>::cmac(acc[1][1], a1, b1);
-    }
-    __syncthreads();
-  }
-#pragma unroll
-  for (int i = 0; i < 2; ++i)
-#pragma unroll
-    for (int j = 0; j < 2; ++j) {
-      const int p = p0 + tp + 16 * i, c = c0 + tc + 16 * j;
-      if (p < nproj && c < cols) part[((int64_t)ks * cols + c) * nproj + p] = acc[i][j];
-    }
+  const int64_t r0 = (int64_t)ks * kchunk, r1 = min((int64_t)rows, r0 + kchunk);
+  tiles::tn_tile<T>(reinterpret_cast<const T*>(nl.p), rows, reinterpret_cast<const T*>(ca.x),
+                    ca.ldx / (int64_t)(sizeof(T) / sizeof(double)), blockIdx.x * 32, blockIdx.y * 32, nproj, cols, r0,
+                    r1, reinterpret_cast<T*>(nl.part) + (int64_t)ks * cols * nproj, nproj);
 }
 
 // wd[c][off+i] = sum_j D[i][j] (sum_ks part[ks][c][off+j]) for one (atom, column).
@@ -390,58 +355,16 @@ __global__ void k_couple(const NlDev* __restrict__ nls, int nproj, int ksplit, B
 
 // y[c][row] += sum_p P[p][row] wd[c][p]; tile 64 rows x 32 columns.
 template <class T>
-__global__ void __launch_bounds__(256) k_back(const NlDev* __restrict__ nls, int nproj, Batch b) {
-  __shared__ T Ps[16][64];
-  __shared__ T Ws[16][33];
+__global__ void __launch_bounds__(128) k_back(const NlDev* __restrict__ nls, int nproj, Batch b) {
   const NlDev& nl = nls[blockIdx.z];
   const CallArgs& ca = b.a[blockIdx.z];
   const int cols = ca.cols, rows = nl.rows;
-  const int r0 = blockIdx.x * 64, c0 = blockIdx.y * 32;
-  if (r0 >= rows || c0 >= cols) return;
-  const T* __restrict__ P = reinterpret_cast<const T*>(nl.p);
-  const T* __restrict__ wd = reinterpret_cast<const T*>(nl.wd);
-  T* __restrict__ Y = reinterpret_cast<T*>(ca.y);
-  const int64_t ldy = ca.ldy / (int64_t)(sizeof(T) / sizeof(double));
-  const int tg = threadIdx.x & 31, tc = threadIdx.x >> 5;
-  T acc[2][4];
-#pragma unroll
-  for (int i = 0; i < 2; ++i)
-#pragma unroll
-    for (int j = 0; j < 4; ++j) acc[i][j] = Ops<T>::zero();
-  for (int pb = 0; pb < nproj; pb += 16) {
-    for (int i = threadIdx.x; i < 16 * 64; i += 256) {
-      const int rr = i & 63, q = i >> 6;
-      const int p = pb + q, r = r0 + rr;
-      Ps[q][rr] = (p < nproj && r < rows) ? P[(int64_t)p * rows + r] : Ops<T>::zero();
-    }
-    for (int i = threadIdx.x; i < 16 * 32; i += 256) {
-      const int q = i & 15, cc = i >> 4;
-      const int p = pb + q, c = c0 + cc;
-      Ws[q][cc] = (p < nproj && c < cols) ? wd[(int64_t)c * nproj + p] : Ops<T>::zero();
-    }
-    __syncthreads();
-#pragma unroll
-    for (int q = 0; q < 16; ++q) {
-      const T a0 = Ps[q][tg], a1 = Ps[q][tg + 32];
-#pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        const T b = Ws[q][tc + 8 * j];
-        acc[0][j] = Ops<T>::mac(acc[0][j], a0, b);
-        acc[1][j] = Ops<T>::mac(acc[1][j], a1, b);
-      }
-    }
-    __syncthreads();
-  }
-#pragma unroll
-  for (int i = 0; i < 2; ++i)
-#pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      const int r = r0 + tg + 32 * i, c = c0 + tc + 8 * j;
-      if (r < rows && c < cols) {
-        T& out = Y[(int64_t)c * ldy + r];
-        out = Ops<T>::add(out, acc[i][j]);
-      }
-    }
+  const int64_t r0 = (int64_t)blockIdx.x * 64;
+  const int j0 = blockIdx.y * 32;
+  if (r0 >= rows || j0 >= cols) return;
+  tiles::nn_tile<T>(reinterpret_cast<const T*>(nl.p), rows, reinterpret_cast<const T*>(nl.wd), nproj,
+                    reinterpret_cast<T*>(ca.y), ca.ldy / (int64_t)(sizeof(T) / sizeof(double)), rows, cols, nproj, r0,
+                    j0, true);
 }
 
 }  // namespace
@@ -524,13 +447,13 @@ int launch_nonlocal(const NlDev* nl, int gamma, const NlShape& sh, int max_rows,
   const dim3 bg_((max_rows + 63) / 64, (max_cols + 31) / 32, b.nk);
   const int cth = ((sh.maxch + 31) / 32) * 32;
   if (gamma) {
-    { StageScope sc(ev, 3, s); k_project<double><<<pg, 256, 0, s>>>(nl, sh.nproj, sh.ksplit, sh.kchunk, b); }
+    { StageScope sc(ev, 3, s); k_project<double><<<pg, 64, 0, s>>>(nl, sh.nproj, sh.ksplit, sh.kchunk, b); }
     { StageScope sc(ev, 4, s); k_couple<double><<<cg, cth, 0, s>>>(nl, sh.nproj, sh.ksplit, b); }
-    { StageScope sc(ev, 5, s); k_back<double><<<bg_, 256, 0, s>>>(nl, sh.nproj, b); }
+    { StageScope sc(ev, 5, s); k_back<double><<<bg_, 128, 0, s>>>(nl, sh.nproj, b); }
   } else {
-    { StageScope sc(ev, 3, s); k_project<double2><<<pg, 256, 0, s>>>(nl, sh.nproj, sh.ksplit, sh.kchunk, b); }
+    { StageScope sc(ev, 3, s); k_project<double2><<<pg, 64, 0, s>>>(nl, sh.nproj, sh.ksplit, sh.kchunk, b); }
     { StageScope sc(ev, 4, s); k_couple<double2><<<cg, cth, 0, s>>>(nl, sh.nproj, sh.ksplit, b); }
-    { StageScope sc(ev, 5, s); k_back<double2><<<bg_, 256, 0, s>>>(nl, sh.nproj, b); }
+    { StageScope sc(ev, 5, s); k_back<double2><<<bg_, 128, 0, s>>>(nl, sh.nproj, b); }
   }
   return 3;
 }
