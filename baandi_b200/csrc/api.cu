@@ -94,10 +94,10 @@ std::vector<double> twiddles(int n) {
   return t;
 }
 
-// Split of the P^H X reduction over rows: enough (tile, split) blocks to fill the
-// 148 SMs twice, chunks a multiple of 32 rows.
+// Split of the P^H X reduction over rows: enough (tile, split) blocks for about eight
+// 64-thread tile blocks per SM (148 SMs), chunks a multiple of 32 rows.
 int ksplit_tiles(int64_t rows, int64_t tiles, int* kchunk, int64_t ks_cap = 1 << 30) {
-  int64_t ks = std::max<int64_t>(1, (2 * 148 + tiles - 1) / tiles);
+  int64_t ks = std::max<int64_t>(1, (8 * 148 + tiles - 1) / tiles);
   ks = std::min<int64_t>(ks, std::max<int64_t>(1, ks_cap));
   ks = std::min<int64_t>(ks, (rows + 31) / 32);
   int64_t chunk = (rows + ks - 1) / ks;
@@ -109,7 +109,7 @@ int ksplit_tiles(int64_t rows, int64_t tiles, int* kchunk, int64_t ks_cap = 1 <<
 
 int ksplit_for(int64_t rows, int nproj, int64_t cols, int* kchunk) {
   const int64_t tiles = ((nproj + 31) / 32) * ((cols + 31) / 32);
-  int64_t ks = std::max<int64_t>(1, (2 * 148 + tiles - 1) / tiles);
+  int64_t ks = std::max<int64_t>(1, (8 * 148 + tiles - 1) / tiles);
   ks = std::min<int64_t>(ks, (rows + 31) / 32);
   int64_t chunk = (rows + ks - 1) / ks;
   chunk = ((chunk + 31) / 32) * 32;

@@ -178,7 +178,7 @@ template <class T>
 int Solver<T>::gram(const D* A, int m, const D* B, int k, T* G, int ldg) {
   if (m == 0 || k == 0) return BG_OK;
   const int64_t tiles = (int64_t)((m + 31) / 32) * ((k + 31) / 32);
-  int64_t ks = std::max<int64_t>(1, (2 * 148 + tiles - 1) / tiles);
+  int64_t ks = std::max<int64_t>(1, (8 * 148 + tiles - 1) / tiles);
   ks = std::min<int64_t>(ks, (rows_ + 255) / 256);
   ks = std::max<int64_t>(1, std::min<int64_t>(ks, (int64_t)(part_elems_ / ((size_t)m * k))));
   int64_t chunk = (rows_ + ks - 1) / ks;
@@ -393,7 +393,7 @@ int Solver<T>::run(const T* start, const double* diagonal, double* values_out, T
   if ((rc = alloc(&V_, rc_)) || (rc = alloc(&HV_, rc_)) || (rc = alloc(&X_, rc_)) || (rc = alloc(&HX_, rc_)) ||
       (rc = alloc(&E_, rc_)) || (rc = alloc(&Er_, rc_)) || (rc = alloc(&HE_, rc_)))
     return rc;
-  part_elems_ = std::max<size_t>((size_t)cap_ * cap_ * 8, (size_t)296 * 32 * 32);
+  part_elems_ = std::max<size_t>((size_t)cap_ * cap_ * 8, (size_t)8 * 148 * 32 * 32);
   if ((rc = alloc(&part_, part_elems_)) || (rc = alloc(&small_, (size_t)cap_ * cap_)) ||
       (rc = alloc(&coef_, (size_t)cap_ * cap_)) || (rc = alloc(&diag_, rows_)) || (rc = alloc(&lam_, cap_)) ||
       (rc = alloc(&norms_, cap_)) || (rc = alloc(&scale_, cap_)) || (rc = alloc(&map_, cap_)))
