@@ -82,6 +82,14 @@ SIGNATURES = {
     "bg_op_launches": [_p, ctypes.POINTER(_i64)],
     "bg_op_profile": [_p, _i32],
     "bg_op_stage_times": [_p, _p],
+    "bg_op_set_potential_ptr": [_p, _p, _u64, _i32],
+    "bg_op_add_local_change": [_p, _p, _p, _p, _i64, _i64, _i32],
+    "bg_op_band_density_sum": [_p, _p, _i64, _i64, _p, _dbl, _p, _i32, _i32],
+    "bg_fields_create": [_p, _p, _p, _pp],
+    "bg_fields_destroy": [_p],
+    "bg_fields_set_stream": [_p, _p],
+    "bg_fields_volume": [_p, ctypes.POINTER(_dbl)],
+    "bg_fields_lda_hartree": [_p, _p, _p, _p, _p, _i32],
     "bg_kset_create": [_p, _i32, _p, _pp],
     "bg_kset_destroy": [_p],
     "bg_kset_apply": [_p, _p, _p, _p, _i32, _i32],

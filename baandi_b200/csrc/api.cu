@@ -65,6 +65,9 @@ int alloc(bg_op* op, size_t bytes, void** out, DevBuf** keep = nullptr) {
   return BG_OK;
 }
 
+}  // namespace
+
+namespace bg {
 bool make_fft_plan(int n, FftPlan* p) {
   if (n < 1 || n > 128) return false;
   p->n = n;
@@ -93,6 +96,9 @@ std::vector<double> twiddles(int n) {
   }
   return t;
 }
+}  // namespace bg
+
+namespace {
 
 // Split of the P^H X reduction over rows: enough (tile, split) blocks for about eight
 // 64-thread tile blocks per SM (148 SMs), chunks a multiple of 32 rows.
@@ -427,15 +433,53 @@ int build_op(bg_ctx* ctx, const bg_basis_desc* b, const bg_projectors* pr, int64
   return BG_OK;
 }
 
+// Wait for the operator stream and report (then clear) the device error word:
+// bit 0 a non-finite coefficient read by a kernel, bit 1 a non-finite potential value.
 int check_err(bg_op* op) {
   cudaError_t e = cudaMemcpyAsync(op->err_host, op->t.err, sizeof(int), cudaMemcpyDeviceToHost, op->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(op->stream);
   if (e != cudaSuccess) return cuda_fail(op->ctx, e, "apply");
-  if (op->err_host[0]) {
+  const int bits = op->err_host[0];
+  if (bits) {
     cudaMemsetAsync(op->t.err, 0, sizeof(int), op->stream);
     cudaStreamSynchronize(op->stream);
-    return fail(op->ctx, BG_ENONFINITE, "non-finite input coefficient");
+    return fail(op->ctx, BG_ENONFINITE, (bits & 2) ? "non-finite potential value" : "non-finite input coefficient");
   }
+  return BG_OK;
+}
+
+// Lazily allocated operator buffers (kept for the operator's lifetime).
+int ensure_buf(bg_op* op, double** p, size_t doubles) {
+  if (*p) return BG_OK;
+  void* vp = nullptr;
+  int rc = alloc(op, doubles * sizeof(double), &vp);
+  if (rc) return rc;
+  *p = static_cast<double*>(vp);
+  return BG_OK;
+}
+
+size_t grid_points(const bg_op* op) { return (size_t)op->dims[0] * op->dims[1] * op->dims[2]; }
+
+// Install a C-order grid (device pointer) into `dst` in the layout of t.vt; waits and
+// reports a non-finite value before returning, leaving `dst` unspecified in that case.
+int transpose_grid(bg_op* op, const double* v_dev, double* dst) {
+  launch_potential_transpose(v_dev, op->g, dst, op->t.err, op->stream);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(op->ctx, e, "kernel launch");
+  return check_err(op);
+}
+
+// Stage a grid given by pointer kind on the device (host grids go through op->grid).
+int grid_on_device(bg_op* op, const double* v, int32_t ptr_kind, const double** out) {
+  if (ptr_kind == BG_PTR_DEVICE) {
+    *out = v;
+    return BG_OK;
+  }
+  int rc = ensure_buf(op, &op->grid, grid_points(op));
+  if (rc) return rc;
+  cudaError_t e = cudaMemcpyAsync(op->grid, v, grid_points(op) * sizeof(double), cudaMemcpyHostToDevice, op->stream);
+  if (e != cudaSuccess) return cuda_fail(op->ctx, e, "copy in");
+  *out = op->grid;
   return BG_OK;
 }
 
@@ -637,6 +681,148 @@ static int stage_times(bg_ctx* ctx, cudaStream_t stream, const StageEvents& ev, 
 int bg_op_stage_times(bg_op* op, double* ms) {
   if (!op) return BG_EINVAL;
   return stage_times(op->ctx, op->stream, op->ev, ms);
+}
+
+int bg_op_set_potential_ptr(bg_op* op, const double* v, uint64_t epoch, int32_t ptr_kind) {
+  if (!op || !v) return fail(op ? op->ctx : nullptr, BG_EINVAL, "null argument");
+  if (ptr_kind == BG_PTR_HOST) return bg_op_set_potential(op, v, epoch);
+  if (ptr_kind != BG_PTR_DEVICE) return fail(op->ctx, BG_EINVAL, "pointer kind");
+  if (op->is_dense) return fail(op->ctx, BG_EINVAL, "a dense operator has no potential grid");
+  if (op->has_epoch && epoch <= op->epoch) return fail(op->ctx, BG_EEPOCH, "potential epoch must increase");
+  cudaError_t e = cudaSetDevice(op->ctx->device);
+  if (e != cudaSuccess) return cuda_fail(op->ctx, e, "cudaSetDevice");
+  // Checked in a scratch copy first so that a rejected potential leaves the old one.
+  int rc = ensure_buf(op, &op->vchange, (size_t)op->g.vstride * op->dims[2]);
+  if (rc) return rc;
+  if ((rc = transpose_grid(op, v, op->vchange))) return rc;
+  e = cudaMemcpyAsync(const_cast<double*>(op->t.vt), op->vchange, sizeof(double) * op->g.vstride * op->dims[2],
+                      cudaMemcpyDeviceToDevice, op->stream);
+  if (e != cudaSuccess) return cuda_fail(op->ctx, e, "set_potential");
+  op->epoch = epoch;
+  op->has_epoch = true;
+  return BG_OK;
+}
+
+int bg_op_add_local_change(bg_op* op, const double* x, const double* change, double* hx, int64_t rows, int64_t cols,
+                           int32_t ptr_kind) {
+  if (!op) return fail(nullptr, BG_EINVAL, "null operator");
+  bg_ctx* ctx = op->ctx;
+  if (ptr_kind != BG_PTR_HOST && ptr_kind != BG_PTR_DEVICE) return fail(ctx, BG_EINVAL, "pointer kind");
+  if (op->is_dense) return fail(ctx, BG_EINVAL, "a dense operator has no potential grid");
+  if (rows != op->rows || cols < 0 || cols > op->cap) return fail(ctx, BG_ESHAPE, "block shape");
+  if (!x || !hx || !change || (const double*)hx == x) return fail(ctx, BG_EINVAL, "x, change and hx must be distinct non-null buffers");
+  cudaError_t e = cudaSetDevice(ctx->device);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaSetDevice");
+  int rc = ensure_buf(op, &op->vchange, (size_t)op->g.vstride * op->dims[2]);
+  if (rc) return rc;
+  const double* dv = nullptr;
+  if ((rc = grid_on_device(op, change, ptr_kind, &dv))) return rc;
+  if ((rc = transpose_grid(op, dv, op->vchange))) return rc;  // change checked before hx is touched
+  if (cols == 0) return BG_OK;
+  const size_t dpc = op->gamma ? (size_t)rows : (size_t)2 * rows;
+  const double* dx = x;
+  double* dhx = hx;
+  if (ptr_kind == BG_PTR_HOST) {
+    dx = static_cast<const double*>(op->xs->p);
+    dhx = static_cast<double*>(op->ys->p);
+    e = cudaMemcpyAsync(const_cast<double*>(dx), x, dpc * cols * sizeof(double), cudaMemcpyHostToDevice, op->stream);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(dhx, hx, dpc * cols * sizeof(double), cudaMemcpyHostToDevice, op->stream);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "copy in");
+  }
+  Batch bt;
+  bt.nk = 1;
+  CallArgs& a = bt.a[0];
+  a.x = dx;
+  a.y = dhx;
+  a.ldx = a.ldy = (int64_t)dpc;
+  a.cols = (int)cols;
+  a.units = op->gamma ? (int)((cols + 1) / 2) : (int)cols;
+  a.vt = op->vchange;
+  a.accumulate = 1;
+  op->launches += launch_local(op->d_tabs, op->gamma ? 1 : 0, op->t.ngroups, op->g, bt, op->stream, nullptr);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "kernel launch");
+  if (ptr_kind == BG_PTR_HOST) {
+    if ((rc = check_err(op))) return rc;  // hx on the host stays untouched on a non-finite input
+    e = cudaMemcpyAsync(hx, dhx, dpc * cols * sizeof(double), cudaMemcpyDeviceToHost, op->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(op->stream);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "copy out");
+  }
+  return BG_OK;
+}
+
+int bg_op_band_density_sum(bg_op* op, const double* x, int64_t rows, int64_t cols, const double* weights,
+                           double volume, double* density, int32_t accumulate, int32_t ptr_kind) {
+  if (!op) return fail(nullptr, BG_EINVAL, "null operator");
+  bg_ctx* ctx = op->ctx;
+  if (ptr_kind != BG_PTR_HOST && ptr_kind != BG_PTR_DEVICE) return fail(ctx, BG_EINVAL, "pointer kind");
+  if (op->is_dense) return fail(ctx, BG_EINVAL, "a dense operator has no grid");
+  if (rows != op->rows || cols < 0 || cols > op->cap) return fail(ctx, BG_ESHAPE, "block shape");
+  if (!density || (cols > 0 && (!x || !weights))) return fail(ctx, BG_EINVAL, "null argument");
+  if (!std::isfinite(volume) || volume <= 0.0) return fail(ctx, BG_ESHAPE, "volume must be finite and positive");
+  for (int64_t c = 0; c < cols; ++c)
+    if (!std::isfinite(weights[c]) || weights[c] < 0.0)
+      return fail(ctx, BG_ESHAPE, "band weights must be finite and non-negative");
+  cudaError_t e = cudaSetDevice(ctx->device);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaSetDevice");
+  const size_t pts = grid_points(op);
+  int rc;
+  double* dd = density;
+  if (ptr_kind == BG_PTR_HOST) {
+    if ((rc = ensure_buf(op, &op->grid, pts))) return rc;
+    dd = op->grid;
+    if (accumulate) {
+      e = cudaMemcpyAsync(dd, density, pts * sizeof(double), cudaMemcpyHostToDevice, op->stream);
+      if (e != cudaSuccess) return cuda_fail(ctx, e, "copy in");
+    }
+  }
+  if (cols == 0) {
+    if (!accumulate) {
+      e = cudaMemsetAsync(dd, 0, pts * sizeof(double), op->stream);
+      if (e != cudaSuccess) return cuda_fail(ctx, e, "memset");
+    }
+  } else {
+    const int units = op->gamma ? (int)((cols + 1) / 2) : (int)cols;
+    // Enough (plane, chunk) blocks for two waves of 148 SMs; chunks sum in order.
+    const int max_chunks = std::max<int>(1, std::min<int64_t>(op->cap_units, (2 * 148 + op->dims[2] - 1) / op->dims[2]));
+    if (!op->dens_part) {
+      if ((rc = ensure_buf(op, &op->dens_part, (size_t)max_chunks * pts))) return rc;
+      op->dens_chunks = max_chunks;
+    }
+    if ((rc = ensure_buf(op, &op->dens_w, (size_t)op->cap))) return rc;
+    const int want = std::min(units, op->dens_chunks);
+    const int per_chunk = (units + want - 1) / want;
+    const int chunks = (units + per_chunk - 1) / per_chunk;
+    const size_t dpc = op->gamma ? (size_t)rows : (size_t)2 * rows;
+    const double* dx = x;
+    if (ptr_kind == BG_PTR_HOST) {
+      dx = static_cast<const double*>(op->xs->p);
+      e = cudaMemcpyAsync(const_cast<double*>(dx), x, dpc * cols * sizeof(double), cudaMemcpyHostToDevice, op->stream);
+      if (e != cudaSuccess) return cuda_fail(ctx, e, "copy in");
+    }
+    e = cudaMemcpyAsync(op->dens_w, weights, cols * sizeof(double), cudaMemcpyHostToDevice, op->stream);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "copy in");
+    CallArgs a;
+    a.x = dx;
+    a.y = nullptr;
+    a.ldx = a.ldy = (int64_t)dpc;
+    a.cols = (int)cols;
+    a.units = units;
+    op->launches += launch_density(op->d_tabs, op->gamma ? 1 : 0, op->t.ngroups, op->g, a, op->dens_w, per_chunk,
+                                   op->dens_part, op->stream);
+    launch_density_reduce(op->dens_part, chunks, op->g, volume, accumulate, dd, op->stream);
+    op->launches += 1;
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "kernel launch");
+  }
+  if (ptr_kind == BG_PTR_HOST) {
+    if ((rc = check_err(op))) return rc;
+    e = cudaMemcpyAsync(density, dd, pts * sizeof(double), cudaMemcpyDeviceToHost, op->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(op->stream);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "copy out");
+  }
+  return BG_OK;
 }
 
 }  // extern "C"

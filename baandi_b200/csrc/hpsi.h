@@ -3,6 +3,7 @@
 #pragma once
 #include <cuda_runtime.h>
 #include <cstdint>
+#include <vector>
 
 #include "fft_dev.cuh"
 
@@ -53,6 +54,8 @@ struct CallArgs {
   int64_t ldx, ldy; // column strides in doubles
   int cols;         // complex columns or real ORC columns
   int units;        // complex columns or column pairs
+  const double* vt = nullptr;  // potential in the layout of OpTables::vt; nullptr: the operator's own
+  int accumulate = 0;          // 1: y += FFT(V IFFT(scatter x))/N, no kinetic term (potential change)
 };
 
 // One launch covers up to kMaxBatch operators (k points) of the same grid; operator
@@ -94,6 +97,23 @@ int launch_local(const OpTables* tabs, int gamma, int max_groups, const BoxGeo& 
 // Enqueue y += P (D (P^H x)) (complex) or y += P (D (P^T x)) (Gamma).
 int launch_nonlocal(const NlDev* nl, int gamma, const NlShape& sh, int max_rows, const Batch& b, cudaStream_t s,
                     StageEvents* ev);
+
+// Band density of one operator's block: part[c][z][y n0 + x] = sum over the units of
+// chunk c (in unit order) of w |psi(r)|^2, psi the unscaled inverse transform
+// (Gamma: w_a Re^2 + w_b Im^2 of a column pair).  `weights` is a device array of
+// a.cols values; chunks of `per_chunk` units.  Uses the stick buffer of tabs[0].
+int launch_density(const OpTables* tabs, int gamma, int max_groups, const BoxGeo& g, const CallArgs& a,
+                   const double* weights, int per_chunk, double* part, cudaStream_t s);
+// out[x][y][z] (C order; = or +=) = scale * sum_c part[c][z][y n0 + x] in chunk order.
+void launch_density_reduce(const double* part, int chunks, const BoxGeo& g, double scale, int accumulate,
+                           double* out, cudaStream_t s);
+// vt[z vstride + y n0 + x] = v[x][y][z] (C order, device); *err |= 2 on a non-finite value.
+void launch_potential_transpose(const double* v, const BoxGeo& g, double* vt, int* err, cudaStream_t s);
+
+// Radix plan of a line of n <= 128 points (2, 3, 4, 5) for fft_lines; false if n has
+// another prime factor.  twiddles(n): exp(+2 pi i q/n), q < n, interleaved (re, im).
+bool make_fft_plan(int n, FftPlan* p);
+std::vector<double> twiddles(int n);
 
 size_t plane_smem_bytes(const BoxGeo& g);
 size_t stick_smem_bytes(const BoxGeo& g);

@@ -23,6 +23,8 @@
 #include "fft_fast.cuh"
 #include "gemm_tiles.cuh"
 
+#include <algorithm>
+
 namespace bg {
 
 namespace {
@@ -133,7 +135,7 @@ __global__ void __launch_bounds__(512) k_planes(const OpTables* __restrict__ tab
   // inverse: y on the occupied x rows, x on every column
   fft_lines<1>(pl, t.nxact, LineOffRows{t.xact, g.pitch}, 1, g.p1, tw1);
   fft_lines<1>(pl, g.n1, LineOffCols{}, g.pitch, g.p0, tw0);
-  const double* v = t.vt + (int64_t)z * g.vstride;
+  const double* v = (a.vt ? a.vt : t.vt) + (int64_t)z * g.vstride;
   for (int i = threadIdx.x; i < g.n0 * g.n1; i += blockDim.x) {
     const int y = i / g.n0, x = i - y * g.n0;
     const double w = v[i];
@@ -163,7 +165,7 @@ __global__ void __launch_bounds__(256, 4) k_planes_fast(const OpTables* __restri
   int* rows = reinterpret_cast<int*>(vs + (VS ? N * N : 0));
   const int nx = t.nxact;
   // V(r) of the plane arrives asynchronously while the y pass runs (16-byte cp.async).
-  const double* v = t.vt + (int64_t)z * g.vstride;  // 16-byte aligned: vstride is even
+  const double* v = (a.vt ? a.vt : t.vt) + (int64_t)z * g.vstride;  // 16-byte aligned: vstride is even
   if constexpr (VS) {
     const unsigned dst = static_cast<unsigned>(__cvta_generic_to_shared(vs));
     for (int i = threadIdx.x; i < N * N / 2; i += blockDim.x)
@@ -233,7 +235,57 @@ __global__ void __launch_bounds__(N == 0 ? 256 : 128, N == 0 ? 1 : 6) k_sticks_f
     fast::pass<N, -1, 1>(st, cnt, LineOffStride{fast::pitch_of<N>()}, tw);
   }
   const double s = g.inv_n;
-  if (!GAMMA) {
+  if (a.accumulate) {
+    // Potential change: y += FFT(dV IFFT x)/N on top of a kept H x (no kinetic term).
+    bool bad = false;
+    if (!GAMMA) {
+      const int e0 = t.grp_entry[grp], e1 = t.grp_entry[grp + 1];
+      double2* y = reinterpret_cast<double2*>(a.y + (int64_t)unit * a.ldy);
+      for (int e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
+        const int2 en = t.entries[e];
+        const double2 h = st[en.y];
+        const double2 old = y[en.x];
+        bad |= !finite2(old.x, old.y);
+        y[en.x] = make_double2(old.x + h.x * s, old.y + h.y * s);
+      }
+    } else {
+      const int r0 = t.grp_rep[grp], r1 = t.grp_rep[grp + 1];
+      const int ca = 2 * unit;
+      const bool hasb = ca + 1 < a.cols;
+      double* ya = a.y + (int64_t)ca * a.ldy;
+      double* yb = a.y + (int64_t)(hasb ? ca + 1 : ca) * a.ldy;
+      for (int e = r0 + threadIdx.x; e < r1; e += blockDim.x) {
+        const int4 rp = t.reps[e];
+        const int r = rp.x;
+        double2 hp = st[rp.y];
+        hp.x *= s;
+        hp.y *= s;
+        if (r == 0) {
+          bad |= !isfinite(ya[0]);
+          ya[0] += hp.x;
+          if (hasb) {
+            bad |= !isfinite(yb[0]);
+            yb[0] += hp.y;
+          }
+        } else {
+          double2 hm = st[rp.z];
+          hm.x *= s;
+          hm.y *= s;
+          const double ex = 0.5 * (hp.x + hm.x), ey = 0.5 * (hp.y - hm.y);
+          const double ox = 0.5 * (hp.x - hm.x), oy = 0.5 * (hp.y + hm.y);
+          bad |= !finite2(ya[r], ya[r + 1]);
+          ya[r] += ex * kSqrt2;
+          ya[r + 1] += ey * kSqrt2;
+          if (hasb) {
+            bad |= !finite2(yb[r], yb[r + 1]);
+            yb[r] += oy * kSqrt2;
+            yb[r + 1] += -ox * kSqrt2;
+          }
+        }
+      }
+    }
+    if (bad) atomicOr(t.err, 1);
+  } else if (!GAMMA) {
     const int e0 = t.grp_entry[grp], e1 = t.grp_entry[grp + 1];
     const double2* x = reinterpret_cast<const double2*>(a.x + (int64_t)unit * a.ldx);
     double2* y = reinterpret_cast<double2*>(a.y + (int64_t)unit * a.ldy);
@@ -367,6 +419,131 @@ __global__ void __launch_bounds__(128) k_back(const NlDev* __restrict__ nls, int
                     j0, true);
 }
 
+// ---------------------------------------------------------------- band density
+// One (z plane, chunk of units) per block: for each unit of the chunk in order, the
+// plane of its inverse transform (y on the occupied x rows, x on every column) is
+// built in shared memory and w |psi|^2 is added to the block's own slice of `part`
+// (each thread owns the same points for every unit, so no barrier guards the sums).
+// Reference: crates/dft-physics/src/distributed_complex.rs:485-547 (complex, sum in
+// band order of weight |u(r)|^2 / volume), distributed_real_gamma.rs:744-785 (Gamma
+// pairs: weight_a Re^2 + weight_b Im^2).
+__device__ __forceinline__ void density_weights(const CallArgs& a, int gamma, const double* __restrict__ w, int unit,
+                                                double* wa, double* wb) {
+  if (gamma) {
+    *wa = w[2 * unit];
+    *wb = 2 * unit + 1 < a.cols ? w[2 * unit + 1] : 0.0;
+  } else {
+    *wa = *wb = w[unit];
+  }
+}
+
+// One block per SM's worth of registers: inside the loop over units the compiler keeps
+// the butterfly indices of every stage live across iterations (no spills at <= 255).
+template <int N>
+__global__ void __launch_bounds__(256, 1) k_density_planes_fast(const OpTables* __restrict__ tabs, BoxGeo g, CallArgs a,
+                                                              int gamma, const double* __restrict__ w, int per_chunk,
+                                                              double* __restrict__ part) {
+  const OpTables& t = tabs[0];
+  const int z = blockIdx.x, chunk = blockIdx.y;
+  const int u0 = chunk * per_chunk, u1 = min(a.units, u0 + per_chunk);
+  constexpr int P = fast::pitch_of<N>();
+  extern __shared__ double2 sm[];
+  double2* tw = sm;
+  double2* pl = sm + N;
+  int* rows = reinterpret_cast<int*>(pl + N * P);
+  const int nx = t.nxact;
+  for (int i = threadIdx.x; i < N; i += blockDim.x) tw[i] = g.tw0[i];
+  for (int i = threadIdx.x; i < nx; i += blockDim.x) rows[i] = t.xact[i] * P;
+  double* acc = part + ((int64_t)chunk * N + z) * (N * N);
+  for (int unit = u0; unit < u1; ++unit) {
+    for (int i = threadIdx.x; i < N * P; i += blockDim.x) pl[i] = make_double2(0.0, 0.0);
+    __syncthreads();
+    const double2* row = t.sbuf + ((int64_t)unit * N + z) * t.S;
+    for (int s = threadIdx.x; s < t.S; s += blockDim.x) pl[t.stick_plane[s]] = row[s];
+    __syncthreads();
+    fast::pass<N, 1, 1>(pl, nx, LineOffTable{rows}, tw);
+    fast::pass<N, 1, P>(pl, N, LineOffCols{}, tw);
+    double wa, wb;
+    density_weights(a, gamma, w, unit, &wa, &wb);
+    for (int i = threadIdx.x; i < N * N; i += blockDim.x) {
+      const int y = i / N, x = i - y * N;
+      const double2 p = pl[x * P + y];
+      double d = unit == u0 ? 0.0 : acc[i];
+      d += wa * (p.x * p.x);
+      d += wb * (p.y * p.y);
+      acc[i] = d;
+    }
+    __syncthreads();
+  }
+}
+
+__global__ void __launch_bounds__(256, 1) k_density_planes(const OpTables* __restrict__ tabs, BoxGeo g, CallArgs a,
+                                                        int gamma, const double* __restrict__ w, int per_chunk,
+                                                        double* __restrict__ part) {
+  const OpTables& t = tabs[0];
+  const int z = blockIdx.x, chunk = blockIdx.y;
+  const int u0 = chunk * per_chunk, u1 = min(a.units, u0 + per_chunk);
+  extern __shared__ double2 sm[];
+  double2* tw0 = sm;
+  double2* tw1 = tw0 + g.n0;
+  double2* pl = tw1 + g.n1;
+  for (int i = threadIdx.x; i < g.n0; i += blockDim.x) tw0[i] = g.tw0[i];
+  for (int i = threadIdx.x; i < g.n1; i += blockDim.x) tw1[i] = g.tw1[i];
+  const int np = g.n0 * g.pitch, pts = g.n0 * g.n1;
+  double* acc = part + ((int64_t)chunk * g.n2 + z) * pts;
+  for (int unit = u0; unit < u1; ++unit) {
+    for (int i = threadIdx.x; i < np; i += blockDim.x) pl[i] = make_double2(0.0, 0.0);
+    __syncthreads();
+    const double2* row = t.sbuf + ((int64_t)unit * g.n2 + z) * t.S;
+    for (int s = threadIdx.x; s < t.S; s += blockDim.x) pl[t.stick_plane[s]] = row[s];
+    fft_lines<1>(pl, t.nxact, LineOffRows{t.xact, g.pitch}, 1, g.p1, tw1);
+    fft_lines<1>(pl, g.n1, LineOffCols{}, g.pitch, g.p0, tw0);
+    double wa, wb;
+    density_weights(a, gamma, w, unit, &wa, &wb);
+    for (int i = threadIdx.x; i < pts; i += blockDim.x) {
+      const int y = i / g.n0, x = i - y * g.n0;
+      const double2 p = pl[x * g.pitch + y];
+      double d = unit == u0 ? 0.0 : acc[i];
+      d += wa * (p.x * p.x);
+      d += wb * (p.y * p.y);
+      acc[i] = d;
+    }
+    __syncthreads();
+  }
+}
+
+// out[x][y][z] (= or +=) sum_c part[c][z][y n0 + x] / volume, chunks in order.
+__global__ void k_density_reduce(const double* __restrict__ part, int chunks, int n0, int n1, int n2, double volume,
+                                 int accumulate, double* __restrict__ out) {
+  const int64_t pts = (int64_t)n0 * n1, total = pts * n2;
+  for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < total; p += (int64_t)gridDim.x * blockDim.x) {
+    const int z = (int)(p % n2);
+    const int64_t xy = p / n2;
+    const int y = (int)(xy % n1), x = (int)(xy / n1);
+    const int64_t q = (int64_t)z * pts + (int64_t)y * n0 + x;
+    double s = 0.0;
+    for (int c = 0; c < chunks; ++c) s += part[c * total + q];
+    s /= volume;
+    out[p] = accumulate ? out[p] + s : s;
+  }
+}
+
+// vt[z vstride + y n0 + x] = v[(x n1 + y) n2 + z]; non-finite values set bit 1 of err.
+__global__ void k_potential_transpose(const double* __restrict__ v, int n0, int n1, int n2, int vstride,
+                                      double* __restrict__ vt, int* err) {
+  const int64_t pts = (int64_t)n0 * n1, total = pts * n2;
+  bool bad = false;
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < total; q += (int64_t)gridDim.x * blockDim.x) {
+    const int z = (int)(q / pts);
+    const int64_t xy = q - z * pts;
+    const int y = (int)(xy / n0), x = (int)(xy - (int64_t)y * n0);
+    const double w = v[((int64_t)x * n1 + y) * n2 + z];
+    bad |= !isfinite(w);
+    vt[(int64_t)z * vstride + xy] = w;
+  }
+  if (bad) atomicOr(err, 2);
+}
+
 }  // namespace
 
 size_t plane_smem_bytes(const BoxGeo& g) {
@@ -437,6 +614,62 @@ int launch_local(const OpTables* tabs, int gamma, int max_groups, const BoxGeo& 
   return 3;
 }
 
+size_t density_smem_bytes(const BoxGeo& g) {
+  const bool fast = g.n0 == g.n1 && g.n1 == g.n2;
+  return sizeof(double2) * ((size_t)g.n0 + g.n1 + (size_t)g.n0 * g.pitch) + (fast ? sizeof(int) * (size_t)g.n0 : 0);
+}
+
+template <int N>
+static void density_kernels(const OpTables* tabs, int gamma, int max_groups, const BoxGeo& g, const CallArgs& a,
+                            const double* w, int per_chunk, double* part, cudaStream_t s) {
+  Batch b;
+  b.nk = 1;
+  b.a[0] = a;
+  constexpr int st = N == 0 ? 256 : 128;
+  const dim3 sgrid(max_groups, a.units, 1);
+  const size_t ss = stick_smem_bytes(g), ds = density_smem_bytes(g);
+  if (gamma)
+    k_sticks_inverse<true, N><<<sgrid, st, ss, s>>>(tabs, g, b);
+  else
+    k_sticks_inverse<false, N><<<sgrid, st, ss, s>>>(tabs, g, b);
+  const dim3 dgrid(g.n2, (a.units + per_chunk - 1) / per_chunk, 1);
+  if constexpr (N != 0) {
+    if (g.n0 == N && g.n1 == N) {
+      k_density_planes_fast<N><<<dgrid, 256, ds, s>>>(tabs, g, a, gamma, w, per_chunk, part);
+      return;
+    }
+  }
+  k_density_planes<<<dgrid, 256, ds, s>>>(tabs, g, a, gamma, w, per_chunk, part);
+}
+
+int launch_density(const OpTables* tabs, int gamma, int max_groups, const BoxGeo& g, const CallArgs& a,
+                   const double* weights, int per_chunk, double* part, cudaStream_t s) {
+  if (a.units == 0) return 0;
+  switch (g.n2) {
+    case 25: density_kernels<25>(tabs, gamma, max_groups, g, a, weights, per_chunk, part, s); break;
+    case 45: density_kernels<45>(tabs, gamma, max_groups, g, a, weights, per_chunk, part, s); break;
+    case 54: density_kernels<54>(tabs, gamma, max_groups, g, a, weights, per_chunk, part, s); break;
+    case 60: density_kernels<60>(tabs, gamma, max_groups, g, a, weights, per_chunk, part, s); break;
+    case 72: density_kernels<72>(tabs, gamma, max_groups, g, a, weights, per_chunk, part, s); break;
+    case 108: density_kernels<108>(tabs, gamma, max_groups, g, a, weights, per_chunk, part, s); break;
+    default: density_kernels<0>(tabs, gamma, max_groups, g, a, weights, per_chunk, part, s); break;
+  }
+  return 2;
+}
+
+void launch_density_reduce(const double* part, int chunks, const BoxGeo& g, double volume, int accumulate,
+                           double* out, cudaStream_t s) {
+  const int64_t total = (int64_t)g.n0 * g.n1 * g.n2;
+  const int blocks = (int)std::min<int64_t>((total + 255) / 256, 148 * 8);
+  k_density_reduce<<<blocks, 256, 0, s>>>(part, chunks, g.n0, g.n1, g.n2, volume, accumulate, out);
+}
+
+void launch_potential_transpose(const double* v, const BoxGeo& g, double* vt, int* err, cudaStream_t s) {
+  const int64_t total = (int64_t)g.n0 * g.n1 * g.n2;
+  const int blocks = (int)std::min<int64_t>((total + 255) / 256, 148 * 8);
+  k_potential_transpose<<<blocks, 256, 0, s>>>(v, g.n0, g.n1, g.n2, g.vstride, vt, err);
+}
+
 int launch_nonlocal(const NlDev* nl, int gamma, const NlShape& sh, int max_rows, const Batch& b, cudaStream_t s,
                     StageEvents* ev) {
   int max_cols = 0;
@@ -478,12 +711,18 @@ static void configure_one(cudaError_t& e, size_t plane_smem, size_t stick_smem) 
   if constexpr (N != 0) {
     set((const void*)k_planes_fast<N>, plane_smem);
     carve((const void*)k_planes_fast<N>);
+    if constexpr (GAMMA) {
+      set((const void*)k_density_planes_fast<N>, plane_smem);
+      carve((const void*)k_density_planes_fast<N>);
+    }
   }
 }
 
 int configure_kernels(size_t plane_smem, size_t stick_smem) {
   cudaError_t e = cudaSuccess;
   e = cudaFuncSetAttribute((const void*)k_planes, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)plane_smem);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute((const void*)k_density_planes, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)plane_smem);
   configure_one<true, 0>(e, plane_smem, stick_smem);
   configure_one<false, 0>(e, plane_smem, stick_smem);
   configure_one<true, 25>(e, plane_smem, stick_smem);

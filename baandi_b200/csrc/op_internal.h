@@ -52,6 +52,13 @@ struct bg_op {
   // Dense operator (tests and fixtures): H is rows x rows on the device.
   bool is_dense = false;
   double* dense = nullptr;
+  // Lazily allocated: a potential change in the layout of t.vt, a C-order grid for
+  // host potentials and densities, band weights, per-chunk density partial sums.
+  double* vchange = nullptr;
+  double* grid = nullptr;
+  double* dens_w = nullptr;
+  double* dens_part = nullptr;
+  int dens_chunks = 0;  // chunks dens_part holds
 };
 
 

@@ -1,0 +1,91 @@
+"""Field step of an SCF map on the GPU: Hartree and LDA-PZ fields of a density.
+
+`FieldGrid` holds one FFT box (bg_fields_*); `lda_hartree(density)` returns the
+Hartree-plus-xc potential, the Hartree potential and the three energies of
+crates/dft-engine/src/refscf/map.rs:41-198 (LDA-PZ, no core density): `hartree` =
+dV/2 sum rho V_H, `xc` = dV sum |rho| eps_xc, `xc_integral` = dV sum rho v_xc (Ha).
+Densities are C-order grids, numpy (synchronous) or CUDA float64 tensors (results on
+the device).
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _lib as L
+from .hamiltonian import Context, SolverError, default_context
+
+
+@dataclass
+class Fields:
+    hxc: object
+    vh: object
+    hartree: float
+    xc: float
+    xc_integral: float
+
+
+class FieldGrid:
+    def __init__(self, rows, dims, ctx: Context | None = None):
+        self.ctx = ctx or default_context()
+        self._lib = self.ctx._lib
+        self.dims = [int(d) for d in dims]
+        r = np.ascontiguousarray(np.asarray(rows, dtype=np.float64).reshape(9))
+        d = (ctypes.c_int32 * 3)(*self.dims)
+        h = ctypes.c_void_p()
+        self._check(self._lib.bg_fields_create(self.ctx.handle, r.ctypes.data_as(ctypes.c_void_p),
+                                               ctypes.cast(d, ctypes.c_void_p), ctypes.byref(h)))
+        self.handle = h
+
+    def _check(self, rc):
+        if rc != L.BG_OK:
+            raise SolverError(rc, f"{L.CODE_NAMES.get(rc, rc)}: {L.last_error(self.ctx.handle)}")
+
+    def volume(self) -> float:
+        v = ctypes.c_double()
+        self._check(self._lib.bg_fields_volume(self.handle, ctypes.byref(v)))
+        return v.value
+
+    def set_stream(self, stream_ptr: int):
+        self._check(self._lib.bg_fields_set_stream(self.handle, ctypes.c_void_p(stream_ptr)))
+
+    def lda_hartree(self, density, hxc=None, vh=None) -> Fields:
+        n = int(np.prod(self.dims))
+        e = np.zeros(3)
+        if isinstance(density, np.ndarray):
+            rho = np.ascontiguousarray(density, dtype=np.float64)
+            if rho.size != n:
+                raise SolverError(L.BG_ESHAPE, "density must be the full grid")
+            hxc = np.empty(self.dims) if hxc is None else hxc
+            vh = np.empty(self.dims) if vh is None else vh
+            for a in (hxc, vh):
+                if a.dtype != np.float64 or not a.flags.c_contiguous or a.size != n:
+                    raise SolverError(L.BG_ESHAPE, "outputs must be C-ordered float64 grids")
+            ptrs = (rho.ctypes.data, hxc.ctypes.data, vh.ctypes.data)
+            kind = L.BG_PTR_HOST
+        else:
+            import torch
+            for a in (density, hxc, vh):
+                if a is not None and (a.dtype != torch.float64 or not a.is_cuda or not a.is_contiguous()
+                                      or a.numel() != n):
+                    raise SolverError(L.BG_ESHAPE, "device grids are contiguous float64 CUDA tensors")
+            hxc = torch.empty(self.dims, dtype=torch.float64, device=density.device) if hxc is None else hxc
+            vh = torch.empty(self.dims, dtype=torch.float64, device=density.device) if vh is None else vh
+            ptrs = (density.data_ptr(), hxc.data_ptr(), vh.data_ptr())
+            kind = L.BG_PTR_DEVICE
+        self._check(self._lib.bg_fields_lda_hartree(self.handle, *(ctypes.c_void_p(p) for p in ptrs),
+                                                    e.ctypes.data_as(ctypes.c_void_p), kind))
+        return Fields(hxc, vh, float(e[0]), float(e[1]), float(e[2]))
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self._lib.bg_fields_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

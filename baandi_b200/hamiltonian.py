@@ -128,6 +128,85 @@ class _Operator:
         self._check(self._lib.bg_op_set_potential(self.handle, _p(v), int(epoch)))
         self._epoch = int(epoch)
 
+    def set_owned_potential_device(self, values, epoch: int):
+        """set_owned_potential from a CUDA float64 tensor holding the C-order grid
+        (checked on the device; a non-finite grid keeps the old potential)."""
+        self._grid_tensor(values, "potential")
+        self._check(self._lib.bg_op_set_potential_ptr(self.handle, ctypes.c_void_p(values.data_ptr()), int(epoch),
+                                                      L.BG_PTR_DEVICE))
+        self._epoch = int(epoch)
+
+    def _grid_points(self) -> int:
+        return self.dims[0] * self.dims[1] * self.dims[2]
+
+    def _grid_tensor(self, t, what):
+        import torch
+        if t.dtype != torch.float64 or not t.is_cuda or not t.is_contiguous() or t.numel() != self._grid_points():
+            raise SolverError(L.BG_ESHAPE, f"{what} must be a contiguous float64 CUDA tensor of the full grid")
+
+    def _block_kind(self, x):
+        """(pointer, columns, kind) of a block: numpy (npw, m) Fortran order or a CUDA
+        tensor shaped (m, npw) row-major, the layouts of apply_block."""
+        if isinstance(x, np.ndarray):
+            want = np.float64 if self._gamma else np.complex128
+            if x.ndim != 2 or x.shape[0] != self.npw or x.dtype != want or not x.flags.f_contiguous:
+                raise SolverError(L.BG_ESHAPE, f"host blocks are Fortran-ordered {np.dtype(want).name} (npw, m)")
+            return x.ctypes.data, x.shape[1], L.BG_PTR_HOST
+        import torch
+        want = torch.float64 if self._gamma else torch.complex128
+        if x.dtype != want or not x.is_cuda or x.dim() != 2 or x.shape[1] != self.npw or not x.is_contiguous():
+            raise SolverError(L.BG_ESHAPE, f"device blocks are contiguous {want} CUDA tensors shaped (m, npw)")
+        return x.data_ptr(), x.shape[0], L.BG_PTR_DEVICE
+
+    def add_local_change(self, x, change, hx):
+        """hx += (change(r) x) on the plane-wave rows: the kept-HX update
+        H_new x = H_old x + (V_new - V_old) x (reference add_local_change,
+        crates/dft-physics/src/distributed_complex.rs:388-420).  x and hx are blocks in
+        the layout of apply_block (both numpy or both CUDA tensors, hx updated in place);
+        change is the C-order grid, numpy with numpy blocks, a CUDA float64 tensor with
+        device blocks."""
+        px, cols, kind = self._block_kind(x)
+        ph, hcols, hkind = self._block_kind(hx)
+        if hcols != cols or hkind != kind:
+            raise SolverError(L.BG_ESHAPE, "hx must match x")
+        if kind == L.BG_PTR_HOST:
+            dv = np.ascontiguousarray(np.asarray(change, dtype=np.float64).reshape(-1))
+            if dv.size != self._grid_points():
+                raise SolverError(L.BG_ESHAPE, "change must be the full grid in C order")
+            pc = dv.ctypes.data
+        else:
+            self._grid_tensor(change, "change")
+            pc = change.data_ptr()
+        self._check(self._lib.bg_op_add_local_change(self.handle, ctypes.c_void_p(px), ctypes.c_void_p(pc),
+                                                     ctypes.c_void_p(ph), self.npw, int(cols), kind))
+        return hx
+
+    def band_density_sum(self, x, weights, volume: float, out=None, accumulate: bool = False):
+        """sum_b weights[b] |psi_b(r)|^2 / volume on the C-order grid, bands in order
+        (reference band_density_sum, distributed_complex.rs:485-547 and
+        distributed_real_gamma.rs:744-785).  Numpy x gives a numpy (n0, n1, n2) grid;
+        a CUDA x a CUDA float64 tensor.  accumulate adds into `out` (k-point sums)."""
+        px, cols, kind = self._block_kind(x)
+        w = np.ascontiguousarray(np.asarray(weights, dtype=np.float64).reshape(-1))
+        if w.size != cols:
+            raise SolverError(L.BG_ESHAPE, "one weight per column")
+        if kind == L.BG_PTR_HOST:
+            if out is None:
+                out = np.zeros(self.dims)
+            if out.dtype != np.float64 or not out.flags.c_contiguous or out.size != self._grid_points():
+                raise SolverError(L.BG_ESHAPE, "out must be a C-ordered float64 grid")
+            pd = out.ctypes.data
+        else:
+            import torch
+            if out is None:
+                out = torch.zeros(self.dims, dtype=torch.float64, device=x.device)
+            self._grid_tensor(out, "out")
+            pd = out.data_ptr()
+        self._check(self._lib.bg_op_band_density_sum(self.handle, ctypes.c_void_p(px), self.npw, int(cols), _p(w),
+                                                     float(volume), ctypes.c_void_p(pd), 1 if accumulate else 0,
+                                                     kind))
+        return out
+
     def stream(self):
         s = ctypes.c_void_p()
         self._check(self._lib.bg_op_stream(self.handle, ctypes.byref(s)))

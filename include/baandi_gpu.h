@@ -137,6 +137,57 @@ int bg_op_launches(const bg_op* op, int64_t* launches);
 int bg_op_profile(bg_op* op, int32_t enable);
 int bg_op_stage_times(bg_op* op, double* ms);
 
+/* ------------------------------------------------------------ SCF map steps */
+/* set_owned_potential with the grid given by pointer kind: BG_PTR_HOST is
+ * bg_op_set_potential; BG_PTR_DEVICE takes a C-order grid in device memory, checks it
+ * on the device and returns BG_ENONFINITE (old potential kept) before installing it. */
+int bg_op_set_potential_ptr(bg_op* op, const double* v_grid, uint64_t epoch, int32_t ptr_kind);
+
+/* Replaces add_local_change (distributed_complex.rs:388-420; the Gamma form is
+ * distributed_real_gamma.rs:1370-1430 followed by the sum of
+ * crates/dft-engine/src/refscf/kept_hx.rs:98-160): hx += FFT(change(r) IFFT(x))/N, the
+ * kept-HX update H_new x = H_old x + (V_new - V_old) x, no kinetic or nonlocal term.
+ * change is a C-order grid (n0*n1*n2), x and hx blocks as in bg_op_apply_block, all
+ * three of the same pointer kind.  A non-finite change returns BG_ENONFINITE before
+ * hx is touched.  A non-finite x or hx: BG_PTR_HOST returns BG_ENONFINITE and leaves
+ * the caller's hx unchanged; BG_PTR_DEVICE reports it at bg_op_sync (hx unspecified). */
+int bg_op_add_local_change(bg_op* op, const double* x, const double* change, double* hx,
+                           int64_t rows, int64_t cols, int32_t ptr_kind);
+
+/* Replaces band_density_sum (distributed_complex.rs:485-547; Gamma ORC columns:
+ * distributed_real_gamma.rs:744-785): density(r) = sum_b weights[b] |psi_b(r)|^2 /
+ * volume over the cols columns of x in band order, psi_b the unscaled inverse
+ * transform sum_G x_bG e^{iGr} (Gamma: the real function of ORC column b).  density is
+ * a C-order grid (n0*n1*n2), overwritten (accumulate 0) or added to (accumulate 1:
+ * the k-point sum of a map).  weights (host, cols values) must be finite and >= 0,
+ * volume finite and > 0 (BG_ESHAPE).  x and density have the pointer kind; a
+ * non-finite x is reported like bg_op_apply_block's. */
+int bg_op_band_density_sum(bg_op* op, const double* x, int64_t rows, int64_t cols,
+                           const double* weights, double volume, double* density,
+                           int32_t accumulate, int32_t ptr_kind);
+
+/* ------------------------------------------------------------ fields of a map */
+/* Hartree and LDA-PZ fields of a density on the FFT box, the field step of a map
+ * (crates/dft-engine/src/refscf/map.rs:41-198 with LDA-PZ, crates/dft-physics/src/
+ * xc.rs:39-77).  A fields object holds the box (lattice vectors as the ROWS of rows[9],
+ * Bohr; dims 2,3,5-smooth, each at most 128), its transforms and work grids. */
+typedef struct bg_fields bg_fields;
+int bg_fields_create(bg_ctx* ctx, const double rows[9], const int32_t dims[3], bg_fields** out);
+int bg_fields_destroy(bg_fields* f);
+/* Use the caller's stream (cudaStream_t) for the field kernels. */
+int bg_fields_set_stream(bg_fields* f, void* stream);
+/* Cell volume (Bohr^3) of the box. */
+int bg_fields_volume(const bg_fields* f, double* volume);
+/* density (C-order grid, signed) -> v_hxc = V_H + v_xc and V_H (v_h may be NULL) on
+ * the same grid: rho(G) = to_reciprocal(density) (1/N), V_H(G) = 4 pi rho(G) / |G|^2
+ * with V_H(0) = 0 and G from the canonical Miller index of every grid point,
+ * V_H(r) = Re sum_G V_H(G) e^{iGr}; v_xc = LDA-PZ of |density| (0 at or below 1e-10).
+ * energies (host, 3 values, Ha): dV/2 sum rho V_H, dV sum |rho| eps_xc, dV sum rho v_xc.
+ * density, v_hxc and v_h have the pointer kind; the call returns when the energies
+ * are on the host.  A non-finite density value returns BG_ENONFINITE. */
+int bg_fields_lda_hartree(bg_fields* f, const double* density, double* v_hxc, double* v_h,
+                          double energies[3], int32_t ptr_kind);
+
 /* ------------------------------------------------------------ k-point sets */
 /* All bands of several k points in one launch per stage.  The reference solves the k
  * points of a map one after another (crates/dft-engine/src/refscf/k_map.rs:136-210,
