@@ -100,6 +100,7 @@ SIGNATURES = {
     "bg_kset_profile": [_p, _i32],
     "bg_kset_stage_times": [_p, _p],
     "bg_davidson_solve": [_p, _p, _p, ctypes.POINTER(DavidsonOptions), _p, _p, _p, ctypes.POINTER(DavidsonStats)],
+    "bg_kset_davidson_solve": [_p, _p, _p, ctypes.POINTER(DavidsonOptions), _i32, _p, _p, _p, _p],
     "bg_op_create_dense": [_p, _i64, _p, _i32, _i64, _pp],
     "bg_local_apply_noalloc": [_p, _i64, _p, _p, _p, _p, _p, _i64, _p],
     "bg_setup_volume": [_p, ctypes.POINTER(_dbl)],

@@ -827,27 +827,7 @@ int bg_op_band_density_sum(bg_op* op, const double* x, int64_t rows, int64_t col
 
 }  // extern "C"
 
-struct bg_kset {
-  bg_ctx* ctx = nullptr;
-  std::vector<bg_op*> ops;
-  int gamma = 0;
-  int max_groups = 0;
-  int max_rows = 0;
-  NlShape shape{};
-  BoxGeo g{};
-  OpTables* d_tabs = nullptr;
-  NlDev* d_nl = nullptr;
-  cudaStream_t stream = nullptr;
-  bool own_stream = false;
-  StageEvents ev;
-  int64_t launches = 0;
-  // host-buffer applies: copy-in, compute and copy-out streams pipelined over chunks
-  static constexpr int kChunks = 4;
-  cudaStream_t pipe[3] = {nullptr, nullptr, nullptr};
-  cudaEvent_t in_done[kChunks] = {}, work_done[kChunks] = {};
-};
-
-namespace {
+namespace bg {
 // Launch the local and nonlocal stages of operators [k0, k1) of a set on one stream.
 int enqueue_range(bg_kset* ks, int k0, int k1, const CallArgs* args, const int64_t* cols, cudaStream_t s,
                   StageEvents* ev) {
@@ -875,7 +855,7 @@ int enqueue_range(bg_kset* ks, int k0, int k1, const CallArgs* args, const int64
   }
   return launches;
 }
-}  // namespace
+}  // namespace bg
 
 extern "C" {
 
@@ -891,7 +871,7 @@ int bg_kset_create(bg_ctx* ctx, int32_t n, bg_op* const* ops, bg_kset** out) {
   for (int i = 0; i < n; ++i) {
     const bg_op* o = ops[i];
     if (!o || o->ctx != ctx) return fail(ctx, BG_EINVAL, "operators must belong to this context");
-    if (o->is_dense) return fail(ctx, BG_EINVAL, "dense operators cannot join a k-point set");
+    if (o->is_dense != o0->is_dense) return fail(ctx, BG_EINVAL, "a k-point set is all dense or all grid operators");
     if (o->gamma != o0->gamma || std::memcmp(o->dims, o0->dims, sizeof o->dims) != 0 ||
         o->shape.nproj != o0->shape.nproj || o->shape.natoms != o0->shape.natoms)
       return fail(ctx, BG_ESHAPE, "operators of a set need one grid, one kind and one projector layout");
@@ -903,6 +883,7 @@ int bg_kset_create(bg_ctx* ctx, int32_t n, bg_op* const* ops, bg_kset** out) {
     ks->shape.maxch = std::max(ks->shape.maxch, o->shape.maxch);
   }
   ks->gamma = o0->gamma ? 1 : 0;
+  ks->dense = o0->is_dense;
   ks->shape.nproj = o0->shape.nproj;
   ks->shape.natoms = o0->shape.natoms;
   ks->g = o0->g;
@@ -955,6 +936,7 @@ int bg_kset_apply(bg_kset* ks, const double* const* x, double* const* y, const i
   bg_ctx* ctx = ks->ctx;
   if (precision != BG_PREC_FP64) return fail(ctx, BG_EINVAL, "unsupported precision");
   if (ptr_kind != BG_PTR_HOST && ptr_kind != BG_PTR_DEVICE) return fail(ctx, BG_EINVAL, "pointer kind");
+  if (ks->dense) return fail(ctx, BG_EINVAL, "a set of dense operators only runs bg_kset_davidson_solve");
   const int n = (int)ks->ops.size();
   Batch bt;
   bt.nk = n;

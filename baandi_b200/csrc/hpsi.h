@@ -47,6 +47,15 @@ struct BoxGeo {
   const double2* tw2;
 };
 
+// Block of one operator whose columns are decided on the device (a solver's correction
+// block): kernels read x, y and the column count from here when CallArgs::dyn is set.
+struct DynCols {
+  const double* x;
+  double* y;
+  int cols;
+  int units;
+};
+
 // Per-call arguments of one operator.
 struct CallArgs {
   const double* x;  // complex: interleaved; Gamma: real ORC
@@ -56,7 +65,20 @@ struct CallArgs {
   int units;        // complex columns or column pairs
   const double* vt = nullptr;  // potential in the layout of OpTables::vt; nullptr: the operator's own
   int accumulate = 0;          // 1: y += FFT(V IFFT(scatter x))/N, no kinetic term (potential change)
+  const DynCols* dyn = nullptr;  // device-side x, y, cols, units (grids sized for `cols`/`units`)
 };
+
+// The arguments with a device-side block resolved.
+__device__ __forceinline__ CallArgs resolve(const CallArgs& in) {
+  CallArgs a = in;
+  if (a.dyn) {
+    a.x = a.dyn->x;
+    a.y = a.dyn->y;
+    a.cols = a.dyn->cols;
+    a.units = a.dyn->units;
+  }
+  return a;
+}
 
 // One launch covers up to kMaxBatch operators (k points) of the same grid; operator
 // b of a launch works on blockIdx.z (local passes) with its own tables and blocks.

@@ -59,7 +59,7 @@ __device__ __forceinline__ bool finite2(double a, double b) { return isfinite(a)
 template <bool GAMMA, int N>
 __global__ void __launch_bounds__(N == 0 ? 256 : 128, N == 0 ? 1 : 6) k_sticks_inverse(const OpTables* __restrict__ tabs, BoxGeo g, Batch b) {
   const OpTables& t = tabs[blockIdx.z];
-  const CallArgs& a = b.a[blockIdx.z];
+  const CallArgs a = resolve(b.a[blockIdx.z]);
   const int grp = blockIdx.x, unit = blockIdx.y;
   if (grp >= t.ngroups || unit >= a.units) return;
   extern __shared__ double2 sm[];
@@ -118,7 +118,7 @@ __global__ void __launch_bounds__(N == 0 ? 256 : 128, N == 0 ? 1 : 6) k_sticks_i
 // ---------------------------------------------------------------- pass 2
 __global__ void __launch_bounds__(512) k_planes(const OpTables* __restrict__ tabs, BoxGeo g, Batch b) {
   const OpTables& t = tabs[blockIdx.z];
-  const CallArgs& a = b.a[blockIdx.z];
+  const CallArgs a = resolve(b.a[blockIdx.z]);
   const int unit = blockIdx.x, z = blockIdx.y;
   if (unit >= a.units) return;
   extern __shared__ double2 sm[];
@@ -153,7 +153,7 @@ __global__ void __launch_bounds__(512) k_planes(const OpTables* __restrict__ tab
 template <int N>
 __global__ void __launch_bounds__(256, 4) k_planes_fast(const OpTables* __restrict__ tabs, BoxGeo g, Batch b) {
   const OpTables& t = tabs[blockIdx.z];
-  const CallArgs& a = b.a[blockIdx.z];
+  const CallArgs a = resolve(b.a[blockIdx.z]);
   const int unit = blockIdx.x, z = blockIdx.y;
   if (unit >= a.units) return;
   constexpr int P = fast::pitch_of<N>();
@@ -215,7 +215,7 @@ __global__ void __launch_bounds__(256, 4) k_planes_fast(const OpTables* __restri
 template <bool GAMMA, int N>
 __global__ void __launch_bounds__(N == 0 ? 256 : 128, N == 0 ? 1 : 6) k_sticks_forward(const OpTables* __restrict__ tabs, BoxGeo g, Batch b) {
   const OpTables& t = tabs[blockIdx.z];
-  const CallArgs& a = b.a[blockIdx.z];
+  const CallArgs a = resolve(b.a[blockIdx.z]);
   const int grp = blockIdx.x, unit = blockIdx.y;
   if (grp >= t.ngroups || unit >= a.units) return;
   extern __shared__ double2 sm[];
@@ -367,7 +367,7 @@ __global__ void __launch_bounds__(64) k_project(const NlDev* __restrict__ nls, i
                                                 Batch b) {
   const int kb = blockIdx.z / ksplit, ks = blockIdx.z - kb * ksplit;
   const NlDev& nl = nls[kb];
-  const CallArgs& ca = b.a[kb];
+  const CallArgs ca = resolve(b.a[kb]);
   const int cols = ca.cols, rows = nl.rows;
   if ((int)blockIdx.y * 32 >= cols) return;
   const int64_t r0 = (int64_t)ks * kchunk, r1 = min((int64_t)rows, r0 + kchunk);
@@ -381,7 +381,7 @@ template <class T>
 __global__ void k_couple(const NlDev* __restrict__ nls, int nproj, int ksplit, Batch b) {
   __shared__ T w[64];
   const NlDev& nl = nls[blockIdx.z];
-  const int cols = b.a[blockIdx.z].cols;
+  const int cols = resolve(b.a[blockIdx.z]).cols;
   const int atom = blockIdx.x, c = blockIdx.y;
   if (c >= cols) return;
   const T* __restrict__ part = reinterpret_cast<const T*>(nl.part);
@@ -409,7 +409,7 @@ __global__ void k_couple(const NlDev* __restrict__ nls, int nproj, int ksplit, B
 template <class T>
 __global__ void __launch_bounds__(128) k_back(const NlDev* __restrict__ nls, int nproj, Batch b) {
   const NlDev& nl = nls[blockIdx.z];
-  const CallArgs& ca = b.a[blockIdx.z];
+  const CallArgs ca = resolve(b.a[blockIdx.z]);
   const int cols = ca.cols, rows = nl.rows;
   const int64_t r0 = (int64_t)blockIdx.x * 64;
   const int j0 = blockIdx.y * 32;

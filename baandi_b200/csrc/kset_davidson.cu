@@ -1,0 +1,1312 @@
+// Batched block Davidson over every k point of a k-point set, driven from the device.
+//
+// The algorithm is the reference Davidson of davidson.cu (crates/dft-solvers/src/
+// ref_davidson.rs:117-366 real Gamma ORC rows, ref_davidson_complex.rs:641-1110
+// complex), run for all k points of a bg_kset at once:
+//   * every large product (rotations V C, Gram blocks V^H W, corrections, the H apply
+//     of the correction blocks) is ONE launch over all k points (blockIdx.z = k);
+//   * the small reduced problem of each k point -- bordered Cholesky with the pivot
+//     rule, A = L^-1 H_r L^-H, Householder tridiagonalisation, implicit QL with
+//     Wilkinson shifts, C = L^-H Y -- and every control decision (contraction,
+//     dropped corrections, repair, convergence) run in a one-block-per-k "control"
+//     kernel, which writes the dimensions and pointers of the next large products into
+//     per-k descriptors in device memory;
+//   * so one iteration is a fixed sequence of launches whose work depends only on
+//     device state: it is captured once as a CUDA graph and replayed until every k
+//     point has finished (the host reads one status word per replay).
+// Branches that a k point does not take this iteration (contraction, repair) are
+// launches whose blocks for that k point return at once.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <complex>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "blas_dev.cuh"
+#include "gemm_tiles.cuh"
+#include "op_internal.h"
+
+namespace bg {
+namespace dv {
+
+constexpr double kEps = 2.220446049250313e-16;
+constexpr double kPivotRatioMin = kEps / 1e-12;   // crates/dft-solvers/src/lean_davidson.rs:62-70
+constexpr double kDependence = 1e-12;             // crates/dft-numerics/src/linalg.rs:12
+constexpr int kCtlThreads = 256;
+constexpr int kQlMaxIter = 60;
+
+// Errors recorded by a k point's control kernel (status = -id).
+enum : int {
+  kErrStartDependent = 1,
+  kErrBasisDependent,
+  kErrNonfiniteCorrection,
+  kErrCapacity,
+  kErrRepairDependent,
+  kErrEigen,
+};
+
+// ------------------------------------------------------------------ scalar helpers
+template <class D>
+struct Cx;
+template <>
+struct Cx<double> {
+  __device__ static double zero() { return 0.0; }
+  __device__ static double one() { return 1.0; }
+  __device__ static double real(double v) { return v; }
+  __device__ static double from_real(double v) { return v; }
+  __device__ static double conj(double a) { return a; }
+  __device__ static double mul(double a, double b) { return a * b; }
+  __device__ static double sub(double a, double b) { return a - b; }
+  __device__ static double add(double a, double b) { return a + b; }
+  __device__ static double scale(double s, double a) { return s * a; }
+  __device__ static double abs2(double a) { return a * a; }
+  __device__ static double abs(double a) { return fabs(a); }
+  __device__ static double neg(double a) { return -a; }
+  __device__ static bool finite(double a) { return isfinite(a); }
+  __device__ static double div(double a, double r) { return a / r; }
+  __device__ static double dot_re(double a, double b) { return a * b; }
+  __device__ static double shfl_down(double a, int o) { return __shfl_down_sync(0xffffffffu, a, o); }
+};
+template <>
+struct Cx<double2> {
+  __device__ static double2 zero() { return make_double2(0.0, 0.0); }
+  __device__ static double2 one() { return make_double2(1.0, 0.0); }
+  __device__ static double real(double2 v) { return v.x; }
+  __device__ static double2 from_real(double v) { return make_double2(v, 0.0); }
+  __device__ static double2 conj(double2 a) { return make_double2(a.x, -a.y); }
+  __device__ static double2 mul(double2 a, double2 b) {
+    return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+  }
+  __device__ static double2 sub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+  __device__ static double2 add(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+  __device__ static double2 scale(double s, double2 a) { return make_double2(s * a.x, s * a.y); }
+  __device__ static double abs2(double2 a) { return a.x * a.x + a.y * a.y; }
+  __device__ static double abs(double2 a) { return hypot(a.x, a.y); }
+  __device__ static double2 neg(double2 a) { return make_double2(-a.x, -a.y); }
+  __device__ static bool finite(double2 a) { return isfinite(a.x) && isfinite(a.y); }
+  __device__ static double2 div(double2 a, double r) { return make_double2(a.x / r, a.y / r); }
+  __device__ static double dot_re(double2 a, double2 b) { return a.x * b.x + a.y * b.y; }  // Re(conj(a) b)
+  __device__ static double2 shfl_down(double2 a, int o) {
+    return make_double2(__shfl_down_sync(0xffffffffu, a.x, o), __shfl_down_sync(0xffffffffu, a.y, o));
+  }
+};
+
+// ------------------------------------------------------------------ device state
+// Per-k buffers (device pointers; an array of these lives in device memory).
+template <class D>
+struct Bufs {
+  D *V, *HV, *X, *HX, *E, *Er;   // rows x cap, ld rows
+  D *S, *Hr, *L, *C, *A, *Y, *P; // cap x cap, ld cap
+  D *Q;                          // Householder accumulation, cap x cap
+  double* Z;                     // tridiagonal eigenvectors, cap x cap (real)
+  double *w, *old, *lam, *norms, *scale, *td, *te;  // cap
+  D* off;                        // cap: Householder off-diagonal
+  D* ph;                         // cap: phases of the real tridiagonal
+  D *hv, *hp, *hq;               // cap: Householder vectors
+  int *active, *map, *conv, *order;  // cap
+  D* part;                       // split-K partials
+  double* rot;                   // QL rotations of one sweep: 2 * cap
+  int* rot_i;                    // cap
+  const double* diag;            // rows
+  int rows;
+};
+
+// Per-k control scalars.
+struct Ctl {
+  int m, nact, kept, status, iterations;
+  int contract, repair, need_repair;
+  int reduced_solves, h_calls, h_columns, repairs, contractions, dropped;
+};
+
+// Descriptors of the large products of one slot (written by the control kernel).
+template <class D>
+struct NN {  // C[:, 0:n] (+)= A[:, 0:k] B, B k x n (ld ldb); A and C ld rows
+  const D* A;
+  const D* B;
+  D* C;
+  int ldb, n, k, accumulate;
+};
+template <class D>
+struct TN {  // G[0:m, 0:n] (ld ldg) = A[:, 0:m]^H B[:, 0:n]
+  const D* A;
+  const D* B;
+  D* G;
+  int ldg, m, n;
+};
+template <class D>
+struct CP {  // dst[:, c] = src[:, c] (scale[c] src[:, map[c]] when pick)
+  const D* src;
+  D* dst;
+  int cols, pick;
+};
+
+// Options shared by every k point (crates/dft-solvers/src/ref_davidson.rs:39-77).
+struct Opts {
+  int n, cap, occupied, first_step, max_iterations;
+  double threshold;
+};
+
+// ------------------------------------------------------------------ block-wide small algebra
+// Every routine below is called by all threads of a control block (kCtlThreads) and
+// ends with the block synchronised.
+
+__device__ __forceinline__ double block_sum(double v, double* red) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  __syncthreads();
+  if (lane == 0) red[warp] = v;
+  __syncthreads();
+  double t = 0.0;
+  for (int i = 0; i < (int)(blockDim.x >> 5); ++i) t += red[i];
+  __syncthreads();
+  return t;
+}
+
+template <class D>
+__device__ __forceinline__ D warp_sum(D v) {
+  for (int o = 16; o > 0; o >>= 1) v = Cx<D>::add(v, Cx<D>::shfl_down(v, o));
+  return v;
+}
+
+// Extend the lower Cholesky factor L of S (both ld, columns 0..m0-1 of L valid) to
+// columns m0..m-1 with the reference's pivot rule (squared pivot over the overlap
+// diagonal >= eps / 1e-12, crates/dft-solvers/src/lean_davidson.rs:62-70).  The part of
+// the new rows left of m0 is a forward substitution per row (one thread per row, the
+// host's summation order); the new diagonal block is factored by warp 0.
+template <class D>
+__device__ bool chol_extend(const D* S, int ld, D* L, int m0, int m, int* flag) {
+  using X = Cx<D>;
+  if (m0 > 0) {
+    for (int j = m0 + (int)threadIdx.x; j < m; j += blockDim.x) {
+      for (int k = 0; k < m0; ++k) {
+        D x = S[j + (size_t)k * ld];
+        for (int p = 0; p < k; ++p) x = X::sub(x, X::mul(L[j + (size_t)p * ld], X::conj(L[k + (size_t)p * ld])));
+        L[j + (size_t)k * ld] = X::div(x, X::real(L[k + (size_t)k * ld]));
+      }
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    const int lane = threadIdx.x;
+    bool ok = true;
+    for (int j = m0; j < m && ok; ++j) {
+      for (int k = m0; k < j; ++k) {
+        D part = X::zero();
+        for (int p = lane; p < k; p += 32) part = X::add(part, X::mul(L[j + (size_t)p * ld], X::conj(L[k + (size_t)p * ld])));
+        part = warp_sum(part);
+        if (lane == 0) L[j + (size_t)k * ld] = X::div(X::sub(S[j + (size_t)k * ld], part), X::real(L[k + (size_t)k * ld]));
+        __syncwarp();
+      }
+      double dp = 0.0;
+      for (int p = lane; p < j; p += 32) dp += X::abs2(L[j + (size_t)p * ld]);
+      for (int o = 16; o > 0; o >>= 1) dp += __shfl_down_sync(0xffffffffu, dp, o);
+      dp = __shfl_sync(0xffffffffu, dp, 0);
+      const double sjj = X::real(S[j + (size_t)j * ld]);
+      const double d = sjj - dp;
+      const double ratio = d / sjj;
+      if (!(ratio >= kPivotRatioMin) || !isfinite(ratio)) {
+        ok = false;
+      } else {
+        if (lane == 0) L[j + (size_t)j * ld] = X::from_real(sqrt(d));
+        for (int i = lane; i < j; i += 32) L[i + (size_t)j * ld] = X::zero();
+      }
+      __syncwarp();
+    }
+    if (lane == 0) *flag = ok ? 1 : 0;
+  }
+  __syncthreads();
+  const bool ok = *flag != 0;
+  __syncthreads();
+  return ok;
+}
+
+// B <- L^-1 B (L lower m x m, B m x ncols), one thread per column.
+template <class D>
+__device__ void trsm_lower(const D* L, int ldl, D* B, int ldb, int m, int ncols) {
+  using X = Cx<D>;
+  for (int c = threadIdx.x; c < ncols; c += blockDim.x) {
+    D* b = B + (size_t)c * ldb;
+    for (int i = 0; i < m; ++i) {
+      D x = b[i];
+      for (int k = 0; k < i; ++k) x = X::sub(x, X::mul(L[i + (size_t)k * ldl], b[k]));
+      b[i] = X::div(x, X::real(L[i + (size_t)i * ldl]));
+    }
+  }
+  __syncthreads();
+}
+
+// B <- L^-H B.
+template <class D>
+__device__ void trsm_lower_adjoint(const D* L, int ldl, D* B, int ldb, int m, int ncols) {
+  using X = Cx<D>;
+  for (int c = threadIdx.x; c < ncols; c += blockDim.x) {
+    D* b = B + (size_t)c * ldb;
+    for (int i = m - 1; i >= 0; --i) {
+      D x = b[i];
+      for (int k = i + 1; k < m; ++k) x = X::sub(x, X::mul(X::conj(L[k + (size_t)i * ldl]), b[k]));
+      b[i] = X::div(x, X::real(L[i + (size_t)i * ldl]));
+    }
+  }
+  __syncthreads();
+}
+
+// dst (m x m, ld) = conj(src)^T.
+template <class D>
+__device__ void adjoint(const D* src, D* dst, int ld, int m) {
+  for (int t = threadIdx.x; t < m * m; t += blockDim.x) {
+    const int i = t % m, j = t / m;
+    dst[i + (size_t)j * ld] = Cx<D>::conj(src[j + (size_t)i * ld]);
+  }
+  __syncthreads();
+}
+
+// Hermitian eigensolver of the m x m matrix A (ld lda, overwritten), eigenvalues
+// ascending in w, eigenvectors in V (ld ldv); the algorithm of the host solver
+// (dense_host.h heev): Householder reduction to a Hermitian tridiagonal matrix, a
+// unitary diagonal scaling to a real symmetric one, implicit QL with Wilkinson shifts,
+// back-transformation.  Work arrays come from the k point's Bufs (ld ldq = cap).
+// Parallel layout: the Householder products and rank-2 updates over rows/elements; QL
+// runs its scalar recurrence on thread 0, which records each sweep's rotations, and
+// every thread then applies them to its own rows of Z.  Returns false on a non-finite
+// input or a QL sweep count above 60 for one eigenvalue.
+template <class D>
+__device__ bool heev(D* A, int lda, int m, double* w, D* V, int ldv, const Bufs<D>& b, int ldq, double* red,
+                     int* sh) {
+  using X = Cx<D>;
+  // finite input
+  int bad = 0;
+  for (int t = threadIdx.x; t < m * m; t += blockDim.x) bad |= !X::finite(A[(t % m) + (size_t)(t / m) * lda]);
+  if (block_sum((double)bad, red) != 0.0) return false;
+  // symmetrise the rounding of the input
+  for (int t = threadIdx.x; t < m * m; t += blockDim.x) {
+    const int i = t % m, j = t / m;
+    if (i == j) {
+      A[i + (size_t)i * lda] = X::from_real(X::real(A[i + (size_t)i * lda]));
+    } else if (i > j) {
+      const D avg = X::scale(0.5, X::add(A[i + (size_t)j * lda], X::conj(A[j + (size_t)i * lda])));
+      A[i + (size_t)j * lda] = avg;
+      A[j + (size_t)i * lda] = X::conj(avg);
+    }
+  }
+  D* Q = b.Q;
+  for (int t = threadIdx.x; t < m * m; t += blockDim.x) {
+    const int i = t % m, j = t / m;
+    Q[i + (size_t)j * ldq] = i == j ? X::one() : X::zero();
+  }
+  for (int t = threadIdx.x; t < m; t += blockDim.x) b.off[t] = X::zero();
+  __syncthreads();
+  D* v = b.hv;
+  D* p = b.hp;
+  D* q = b.hq;
+  for (int k = 0; k + 2 < m; ++k) {
+    const int L = m - k - 1;
+    D* x = A + (k + 1) + (size_t)k * lda;
+    double part = 0.0;
+    for (int i = threadIdx.x; i < L; i += blockDim.x) part += X::abs2(x[i]);
+    const double xn = sqrt(block_sum(part, red));
+    if (xn == 0.0) {
+      if (threadIdx.x == 0) b.off[k] = X::zero();
+      __syncthreads();
+      continue;
+    }
+    const D x0 = x[0];
+    const double ax0 = X::abs(x0);
+    const D phase = ax0 > 0.0 ? X::div(x0, ax0) : X::one();
+    const D alpha = X::scale(-xn, phase);
+    for (int i = threadIdx.x; i < L; i += blockDim.x) v[i] = i == 0 ? X::sub(x0, alpha) : x[i];
+    __syncthreads();
+    part = 0.0;
+    for (int i = threadIdx.x; i < L; i += blockDim.x) part += X::abs2(v[i]);
+    const double vn2 = block_sum(part, red);
+    if (vn2 == 0.0) {
+      if (threadIdx.x == 0) b.off[k] = x0;
+      __syncthreads();
+      continue;
+    }
+    const double beta = 2.0 / vn2;
+    // p = beta B v, B = A[k+1:, k+1:]
+    for (int i = threadIdx.x; i < L; i += blockDim.x) {
+      D acc = X::zero();
+      for (int j = 0; j < L; ++j) acc = X::add(acc, X::mul(A[(k + 1 + i) + (size_t)(k + 1 + j) * lda], v[j]));
+      p[i] = X::scale(beta, acc);
+    }
+    __syncthreads();
+    part = 0.0;
+    for (int i = threadIdx.x; i < L; i += blockDim.x) part += X::dot_re(v[i], p[i]);
+    const double K = 0.5 * beta * block_sum(part, red);
+    for (int i = threadIdx.x; i < L; i += blockDim.x) q[i] = X::sub(p[i], X::scale(K, v[i]));
+    __syncthreads();
+    for (int t = threadIdx.x; t < L * L; t += blockDim.x) {
+      const int i = t % L, j = t / L;
+      D& a = A[(k + 1 + i) + (size_t)(k + 1 + j) * lda];
+      a = X::sub(a, X::add(X::mul(v[i], X::conj(q[j])), X::mul(q[i], X::conj(v[j]))));
+    }
+    if (threadIdx.x == 0) b.off[k] = alpha;
+    __syncthreads();
+    for (int i = threadIdx.x; i < L; i += blockDim.x) {
+      x[i] = X::zero();
+      A[k + (size_t)(k + 1 + i) * lda] = X::zero();
+    }
+    // Q <- Q H on columns k+1..m-1
+    for (int r = threadIdx.x; r < m; r += blockDim.x) {
+      D acc = X::zero();
+      for (int j = 0; j < L; ++j) acc = X::add(acc, X::mul(Q[r + (size_t)(k + 1 + j) * ldq], v[j]));
+      acc = X::scale(beta, acc);
+      for (int j = 0; j < L; ++j) {
+        D& e = Q[r + (size_t)(k + 1 + j) * ldq];
+        e = X::sub(e, X::mul(acc, X::conj(v[j])));
+      }
+    }
+    __syncthreads();
+  }
+  double* d = b.td;
+  double* e = b.te;
+  D* s = b.ph;
+  if (threadIdx.x == 0) {
+    if (m >= 2) b.off[m - 2] = A[(m - 1) + (size_t)(m - 2) * lda];
+    for (int i = 0; i < m; ++i) d[i] = X::real(A[i + (size_t)i * lda]);
+    s[0] = X::one();
+    for (int i = 0; i + 1 < m; ++i) {
+      const double a = X::abs(b.off[i]);
+      e[i] = a;
+      s[i + 1] = a > 0.0 ? X::mul(s[i], X::div(b.off[i], a)) : s[i];
+    }
+    e[m - 1] = 0.0;
+  }
+  double* Z = b.Z;
+  for (int t = threadIdx.x; t < m * m; t += blockDim.x) {
+    const int i = t % m, j = t / m;
+    Z[i + (size_t)j * ldq] = i == j ? 1.0 : 0.0;
+  }
+  __syncthreads();
+  // implicit QL (the recurrence of the host's tridiagonal_ql)
+  int* s_m = sh;       // sh[0]: m of the sweep, sh[1]: rotations, sh[2]: failed
+  for (int l = 0; l < m; ++l) {
+    int iter = 0;
+    for (;;) {
+      if (threadIdx.x == 0) {
+        int mm;
+        for (mm = l; mm < m - 1; ++mm) {
+          const double dd = fabs(d[mm]) + fabs(d[mm + 1]);
+          if (fabs(e[mm]) <= kEps * dd) break;
+        }
+        int nrot = 0;
+        int fail = 0;
+        if (mm != l) {
+          if (iter++ == kQlMaxIter) {
+            fail = 1;
+          } else {
+            double g = (d[l + 1] - d[l]) / (2.0 * e[l]);
+            double r = hypot(g, 1.0);
+            g = d[mm] - d[l] + e[l] / (g + (g >= 0.0 ? r : -r));
+            double sn = 1.0, c = 1.0, pp = 0.0;
+            int i;
+            bool broke = false;
+            for (i = mm - 1; i >= l; --i) {
+              double f = sn * e[i];
+              const double bb = c * e[i];
+              r = hypot(f, g);
+              e[i + 1] = r;
+              if (r == 0.0) {
+                d[i + 1] -= pp;
+                e[mm] = 0.0;
+                broke = true;
+                break;
+              }
+              sn = f / r;
+              c = g / r;
+              g = d[i + 1] - pp;
+              r = (d[i] - g) * sn + 2.0 * c * bb;
+              pp = sn * r;
+              d[i + 1] = g + pp;
+              g = c * r - bb;
+              b.rot[2 * nrot] = sn;
+              b.rot[2 * nrot + 1] = c;
+              b.rot_i[nrot] = i;
+              ++nrot;
+            }
+            if (!broke) {
+              d[l] -= pp;
+              e[l] = g;
+              e[mm] = 0.0;
+            }
+          }
+        }
+        s_m[0] = mm;
+        s_m[1] = nrot;
+        s_m[2] = fail;
+        s_m[3] = iter;
+      }
+      __syncthreads();
+      const int mm = s_m[0], nrot = s_m[1], fail = s_m[2];
+      iter = s_m[3];
+      if (fail) {
+        __syncthreads();
+        return false;
+      }
+      for (int row = threadIdx.x; row < m; row += blockDim.x) {
+        for (int t = 0; t < nrot; ++t) {
+          const int i = b.rot_i[t];
+          const double sn = b.rot[2 * t], c = b.rot[2 * t + 1];
+          const double f = Z[row + (size_t)(i + 1) * ldq];
+          const double zi = Z[row + (size_t)i * ldq];
+          Z[row + (size_t)(i + 1) * ldq] = sn * zi + c * f;
+          Z[row + (size_t)i * ldq] = c * zi - sn * f;
+        }
+      }
+      __syncthreads();
+      if (mm == l) break;
+    }
+  }
+  // stable ascending order of the eigenvalues (rank of each entry)
+  for (int i = threadIdx.x; i < m; i += blockDim.x) {
+    int rank = 0;
+    const double di = d[i];
+    for (int j = 0; j < m; ++j) rank += (d[j] < di) || (d[j] == di && j < i);
+    b.order[rank] = i;
+  }
+  __syncthreads();
+  for (int c = threadIdx.x; c < m; c += blockDim.x) w[c] = d[b.order[c]];
+  for (int t = threadIdx.x; t < m * m; t += blockDim.x) {
+    const int r = t % m, c = t / m;
+    const int src = b.order[c];
+    D acc = X::zero();
+    for (int k = 0; k < m; ++k) acc = X::add(acc, X::mul(Q[r + (size_t)k * ldq], X::scale(Z[k + (size_t)src * ldq], s[k])));
+    V[r + (size_t)c * ldv] = acc;
+  }
+  __syncthreads();
+  return true;
+}
+
+// Reduced eigenproblem of the first m basis columns: A = L^-1 H_r L^-H, A Y = Y diag(w),
+// C = L^-H Y (crates/dft-numerics/src/linalg.rs:234-444 for the complex form,
+// crates/dft-solvers/src/ref_davidson/workspace.rs:385-499 for the real one).
+template <class D>
+__device__ bool eigen(const Bufs<D>& b, int cap, int m, double* red, int* sh) {
+  for (int t = threadIdx.x; t < m * m; t += blockDim.x) {
+    const int i = t % m, j = t / m;
+    b.A[i + (size_t)j * cap] = b.Hr[i + (size_t)j * cap];
+  }
+  __syncthreads();
+  trsm_lower(b.L, cap, b.A, cap, m, m);
+  adjoint(b.A, b.Y, cap, m);
+  trsm_lower(b.L, cap, b.Y, cap, m, m);
+  adjoint(b.Y, b.A, cap, m);
+  if (!heev(b.A, cap, m, b.w, b.Y, cap, b, cap, red, sh)) return false;
+  trsm_lower_adjoint(b.L, cap, b.Y, cap, m, m);
+  for (int t = threadIdx.x; t < m * m; t += blockDim.x) {
+    const int i = t % m, j = t / m;
+    b.C[i + (size_t)j * cap] = b.Y[i + (size_t)j * cap];
+  }
+  __syncthreads();
+  return true;
+}
+
+// ------------------------------------------------------------------ batched large products
+// Descriptor arrays are laid out [slot][k]; blockIdx.z enumerates (slot, k).
+
+// C (+)= A B for every (slot, k) with a non-empty descriptor; 64 x 32 tiles.
+template <class D>
+__global__ void __launch_bounds__(128) k_dv_nn(const Bufs<D>* __restrict__ bufs, const NN<D>* __restrict__ desc,
+                                               int nk) {
+  const int z = blockIdx.z, k = z % nk;
+  const NN<D> d = desc[z];
+  const int rows = bufs[k].rows;
+  const int64_t r0 = (int64_t)blockIdx.x * 64;
+  const int j0 = blockIdx.y * 32;
+  if (d.n <= 0 || j0 >= d.n || r0 >= rows) return;
+  tiles::nn_tile<D>(d.A, rows, d.B, d.ldb, d.C, rows, rows, d.n, d.k, r0, j0, d.accumulate != 0);
+}
+
+// Split-K partial Gram products: part[slot][s][j][i] = sum over row slice s of
+// conj(A[r][i]) B[r][j]; blockIdx.z = (slot * nk + k) * ks + s.
+template <class D>
+__global__ void __launch_bounds__(64) k_dv_tn(const Bufs<D>* __restrict__ bufs, const TN<D>* __restrict__ desc, int nk,
+                                              int ks, int64_t slot_elems) {
+  const int zz = blockIdx.z / ks, sidx = blockIdx.z % ks;
+  const int slot = zz / nk, k = zz % nk;
+  const TN<D> d = desc[zz];
+  if (d.m <= 0 || d.n <= 0 || (int)blockIdx.x * 32 >= d.m || (int)blockIdx.y * 32 >= d.n) return;
+  const int64_t rows = bufs[k].rows;
+  int64_t chunk = (rows + ks - 1) / ks;
+  chunk = ((chunk + 31) / 32) * 32;
+  const int64_t r0 = min(rows, (int64_t)sidx * chunk), r1 = min(rows, r0 + chunk);
+  D* part = bufs[k].part + slot * slot_elems + (int64_t)sidx * d.m * d.n;
+  tiles::tn_tile<D>(d.A, rows, d.B, rows, blockIdx.x * 32, blockIdx.y * 32, d.m, d.n, r0, r1, part, d.m);
+}
+
+// G[i + j ldg] = sum_s part[slot][s][j][i] in slice order.
+template <class D>
+__global__ void k_dv_tn_sum(const Bufs<D>* __restrict__ bufs, const TN<D>* __restrict__ desc, int nk, int ks,
+                            int64_t slot_elems) {
+  const int zz = blockIdx.z, slot = zz / nk, k = zz % nk;
+  const TN<D> d = desc[zz];
+  if (d.m <= 0 || d.n <= 0) return;
+  const D* part = bufs[k].part + slot * slot_elems;
+  const int64_t total = (int64_t)d.m * d.n;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t j = t / d.m, i = t - j * d.m;
+    D acc = Arith<D>::zero();
+    for (int q = 0; q < ks; ++q) acc = Arith<D>::add(acc, part[(int64_t)q * total + t]);
+    d.G[i + j * d.ldg] = acc;
+  }
+}
+
+// dst[:, c] = src[:, c], or scale[c] src[:, map[c]] for a pick; blockIdx.y = column.
+template <class D>
+__global__ void k_dv_copy(const Bufs<D>* __restrict__ bufs, const CP<D>* __restrict__ desc, int nk) {
+  const int z = blockIdx.z, k = z % nk;
+  const CP<D> d = desc[z];
+  const int c = blockIdx.y;
+  if (c >= d.cols) return;
+  const Bufs<D>& b = bufs[k];
+  const int64_t rows = b.rows;
+  const D* src = d.src + (int64_t)(d.pick ? b.map[c] : c) * rows;
+  D* dst = d.dst + (int64_t)c * rows;
+  const double sc = d.pick ? b.scale[c] : 1.0;
+  for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < rows; r += (int64_t)gridDim.x * blockDim.x)
+    dst[r] = d.pick ? Arith<D>::scale(sc, src[r]) : src[r];
+}
+
+// Dense test operators: y[:, 0:cols] = H x for every k point, cols read from dyn.
+template <class D>
+__global__ void __launch_bounds__(128) k_dv_dense(const D* const* __restrict__ H, const Bufs<D>* __restrict__ bufs,
+                                                  const DynCols* __restrict__ dyn) {
+  const int k = blockIdx.z;
+  const DynCols dc = dyn[k];
+  const int rows = bufs[k].rows;
+  const int64_t r0 = (int64_t)blockIdx.x * 64;
+  const int j0 = blockIdx.y * 32;
+  if (j0 >= dc.cols || r0 >= rows) return;
+  tiles::nn_tile<D>(H[k], rows, reinterpret_cast<const D*>(dc.x), rows, reinterpret_cast<D*>(dc.y), rows, rows,
+                    dc.cols, rows, r0, j0, false);
+}
+
+__device__ __forceinline__ double denominator(double h, double e) {
+  const double x = 2.0 * (h - e);
+  const double z = fabs(x - 1.0);
+  return 0.25 * (2.0 * fmax(x, 1.0) + 1.0 / (sqrt(1.0 + z * z) + z));
+}
+
+// Er[:, j] = (HX[:, j] - lambda_j X[:, j]) / d(h, lambda_j), norms[j] = |Er[:, j]|^2 for
+// the active bands of every running k point (ref_davidson.rs:418-422, stream.rs:16-67).
+template <class D>
+__global__ void __launch_bounds__(256) k_dv_corrections(const Bufs<D>* __restrict__ bufs, const Ctl* __restrict__ ctl) {
+  const int j = blockIdx.x, k = blockIdx.y;
+  const Ctl& c = ctl[k];
+  if (c.status != 0 || j >= c.nact) return;
+  const Bufs<D>& b = bufs[k];
+  const int64_t rows = b.rows;
+  const double e = b.lam[j];
+  const D* x = b.X + j * rows;
+  const D* hx = b.HX + j * rows;
+  D* out = b.Er + j * rows;
+  double acc = 0.0;
+  for (int64_t r = threadIdx.x; r < rows; r += blockDim.x) {
+    const double inv = 1.0 / denominator(b.diag[r], e);
+    D v = Arith<D>::add(hx[r], Arith<D>::scale(-e, x[r]));
+    v = Arith<D>::scale(inv, v);
+    out[r] = v;
+    acc += Arith<D>::norm2(v);
+  }
+  __shared__ double red[256];
+  red[threadIdx.x] = acc;
+  __syncthreads();
+  for (int st = blockDim.x / 2; st > 0; st >>= 1) {
+    if ((int)threadIdx.x < st) red[threadIdx.x] += red[threadIdx.x + st];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) b.norms[j] = red[0];
+}
+
+// ------------------------------------------------------------------ control kernel
+enum Phase : int {
+  kSetup = 0,   // after H V and the Grams of the start block: factor, eigensolve
+  kBegin,       // contraction at the top of an iteration
+  kRefresh,     // contraction factor/eigensolve; capacity; correction rotations
+  kSelect,      // drop and normalise corrections; append or stage for the repair
+  kExtend,      // border the overlap factor; stage the repair
+  kRepair1,     // reset to the Ritz basis; first projection Gram
+  kRepair2,     // first projection; second Gram
+  kRepair3,     // second projection; in-block Gram
+  kRepair4,     // in-block orthonormalisation; append
+  kApply,       // repair border; the apply block
+  kFinish,      // border H_r, eigensolve, convergence
+  kFinal,       // X = V C[:, :n]
+};
+
+constexpr int kNnSlots = 2, kTnSlots = 2, kCpSlots = 3;
+
+template <class D>
+__global__ void __launch_bounds__(kCtlThreads, 1) k_dv_ctl(int phase, const Bufs<D>* __restrict__ bufs, Ctl* ctl,
+                                                        NN<D>* nn, TN<D>* tn, CP<D>* cp, DynCols* dyn, Opts o, int nk,
+                                                        int gamma) {
+  using X = Cx<D>;
+  const int k = blockIdx.x;
+  const Bufs<D>& b = bufs[k];
+  const int cap = o.cap, n = o.n;
+  const int64_t rows = b.rows;
+  __shared__ Ctl c;
+  __shared__ double red[32];
+  __shared__ int sh[8];
+  if (threadIdx.x == 0) {
+    c = ctl[k];
+    for (int sl = 0; sl < kNnSlots; ++sl) nn[sl * nk + k] = NN<D>{nullptr, nullptr, nullptr, 0, 0, 0, 0};
+    for (int sl = 0; sl < kTnSlots; ++sl) tn[sl * nk + k] = TN<D>{nullptr, nullptr, nullptr, 0, 0, 0};
+    for (int sl = 0; sl < kCpSlots; ++sl) cp[sl * nk + k] = CP<D>{nullptr, nullptr, 0, 0};
+    dyn[k] = DynCols{reinterpret_cast<const double*>(b.V), reinterpret_cast<double*>(b.HV), 0, 0};
+  }
+  __syncthreads();
+  if (c.status != 0 && phase != kFinal) return;
+  auto set_err = [&](int id) {
+    if (threadIdx.x == 0) c.status = -id;
+  };
+  auto mirror = [&](D* M, int m0, int m1) {  // M[j][i] = conj(M[i][j]) for the new columns j in [m0, m1), i <= j
+    for (int t = threadIdx.x; t < (m1 - m0) * m1; t += blockDim.x) {
+      const int j = m0 + t / m1, i = t % m1;
+      if (i <= j) M[j + (size_t)i * cap] = X::conj(M[i + (size_t)j * cap]);
+    }
+    __syncthreads();
+  };
+  D* Vt = b.V + (int64_t)c.m * rows;    // first free basis column
+  switch (phase) {
+    case kSetup: {
+      if (!chol_extend(b.S, cap, b.L, 0, n, &sh[4])) {
+        set_err(kErrStartDependent);
+        break;
+      }
+      if (!eigen(b, cap, n, red, sh)) {
+        set_err(kErrEigen);
+        break;
+      }
+      if (threadIdx.x == 0) {
+        c.reduced_solves += 1;
+        c.m = n;
+        c.nact = n;
+        for (int i = 0; i < n; ++i) b.active[i] = i;
+      }
+      break;
+    }
+    case kBegin: {
+      if (threadIdx.x == 0) {
+        c.contract = c.contract || (c.m + c.nact > cap && c.m > n);
+        if (c.contract) {
+          nn[0 * nk + k] = NN<D>{b.V, b.C, b.X, cap, n, c.m, 0};
+          nn[1 * nk + k] = NN<D>{b.HV, b.C, b.HX, cap, n, c.m, 0};
+          cp[0 * nk + k] = CP<D>{b.X, b.V, n, 0};
+          cp[1 * nk + k] = CP<D>{b.HX, b.HV, n, 0};
+          tn[0 * nk + k] = TN<D>{b.V, b.V, b.S, cap, n, n};
+          tn[1 * nk + k] = TN<D>{b.V, b.HV, b.Hr, cap, n, n};
+        }
+      }
+      break;
+    }
+    case kRefresh: {
+      if (c.contract) {
+        if (!chol_extend(b.S, cap, b.L, 0, n, &sh[4])) {
+          set_err(kErrBasisDependent);
+          break;
+        }
+        if (!eigen(b, cap, n, red, sh)) {
+          set_err(kErrEigen);
+          break;
+        }
+        if (threadIdx.x == 0) {
+          c.contractions += 1;
+          c.reduced_solves += 1;
+          c.m = n;
+          c.contract = 0;
+        }
+        __syncthreads();
+      }
+      if (c.m + c.nact > cap && cap < rows) {
+        set_err(kErrCapacity);
+        break;
+      }
+      const int m = c.m, na = c.nact;
+      for (int t = threadIdx.x; t < m * na; t += blockDim.x) {
+        const int i = t % m, j = t / m;
+        b.P[i + (size_t)j * cap] = b.C[i + (size_t)b.active[j] * cap];
+      }
+      for (int j = threadIdx.x; j < na; j += blockDim.x) b.lam[j] = b.w[b.active[j]];
+      if (threadIdx.x == 0) {
+        nn[0 * nk + k] = NN<D>{b.V, b.P, b.X, cap, na, m, 0};
+        nn[1 * nk + k] = NN<D>{b.HV, b.P, b.HX, cap, na, m, 0};
+      }
+      break;
+    }
+    case kSelect: {
+      if (threadIdx.x == 0) {
+        int kept = 0;
+        for (int j = 0; j < c.nact; ++j) {
+          const double nrm = sqrt(b.norms[j]);
+          if (!isfinite(nrm)) {
+            c.status = -kErrNonfiniteCorrection;
+            break;
+          }
+          if (nrm <= 32.0 * kEps) {
+            c.dropped += 1;
+            continue;
+          }
+          b.map[kept] = j;
+          b.scale[kept] = 1.0 / nrm;
+          ++kept;
+        }
+        c.kept = kept;
+        c.need_repair = (c.m + kept > cap) || kept == 0;
+        c.repair = 0;
+        if (c.status == 0) {
+          if (!c.need_repair) {
+            cp[0 * nk + k] = CP<D>{b.Er, Vt, kept, 1};
+            tn[0 * nk + k] = TN<D>{b.V, Vt, b.S + (size_t)c.m * cap, cap, c.m + kept, kept};
+          } else {
+            cp[0 * nk + k] = CP<D>{b.Er, b.E, kept, 1};
+          }
+        }
+      }
+      break;
+    }
+    case kExtend: {
+      const int m = c.m, kk = c.kept;
+      bool repair = c.need_repair != 0;
+      if (!repair) {
+        mirror(b.S, m, m + kk);
+        if (!chol_extend(b.S, cap, b.L, m, m + kk, &sh[4])) repair = true;
+      }
+      if (threadIdx.x == 0 && repair) {
+        c.repair = 1;
+        c.repairs += 1;
+        if (!c.need_repair) cp[0 * nk + k] = CP<D>{Vt, b.E, kk, 0};  // corrections were appended already
+        nn[0 * nk + k] = NN<D>{b.V, b.C, b.X, cap, m, m, 0};
+        nn[1 * nk + k] = NN<D>{b.HV, b.C, b.HX, cap, m, m, 0};
+        cp[1 * nk + k] = CP<D>{b.X, b.V, m, 0};
+        cp[2 * nk + k] = CP<D>{b.HX, b.HV, m, 0};
+      }
+      break;
+    }
+    case kRepair1: {
+      if (!c.repair) break;
+      const int m = c.m;
+      for (int t = threadIdx.x; t < m * m; t += blockDim.x) {
+        const int i = t % m, j = t / m;
+        const bool dg = i == j;
+        b.S[i + (size_t)j * cap] = dg ? X::one() : X::zero();
+        b.L[i + (size_t)j * cap] = dg ? X::one() : X::zero();
+        b.Hr[i + (size_t)j * cap] = dg ? X::from_real(b.w[i]) : X::zero();
+        b.C[i + (size_t)j * cap] = dg ? X::one() : X::zero();
+      }
+      if (threadIdx.x == 0 && c.kept > 0) tn[0 * nk + k] = TN<D>{b.V, b.E, b.P, cap, m, c.kept};
+      break;
+    }
+    case kRepair2:
+    case kRepair3: {
+      if (!c.repair || c.kept == 0) break;
+      const int m = c.m, kk = c.kept;
+      for (int t = threadIdx.x; t < m * kk; t += blockDim.x) {
+        const int i = t % m, j = t / m;
+        b.P[i + (size_t)j * cap] = X::neg(b.P[i + (size_t)j * cap]);
+      }
+      if (threadIdx.x == 0) {
+        nn[0 * nk + k] = NN<D>{b.V, b.P, b.E, cap, kk, m, 1};
+        tn[0 * nk + k] = phase == kRepair2 ? TN<D>{b.V, b.E, b.P, cap, m, kk} : TN<D>{b.E, b.E, b.A, cap, kk, kk};
+      }
+      break;
+    }
+    case kRepair4: {
+      if (!c.repair || c.kept == 0) break;
+      const int kraw = c.kept;
+      const D* G = b.A;
+      D* Qc = b.P;   // orthonormal combinations, column q of kept j
+      D* q = b.hv;
+      D* dots = b.hp;
+      D* t = b.hq;
+      if (threadIdx.x == 0) sh[5] = 0;
+      __syncthreads();
+      for (int j = 0; j < kraw; ++j) {
+        const int nkeep = sh[5];
+        // dots with the kept combinations: q_c^H G e_j
+        for (int cc = threadIdx.x; cc < nkeep; cc += blockDim.x) {
+          D acc = X::zero();
+          for (int a = 0; a < kraw; ++a) acc = X::add(acc, X::mul(X::conj(Qc[a + (size_t)cc * cap]), G[a + (size_t)j * cap]));
+          dots[cc] = acc;
+        }
+        __syncthreads();
+        for (int a = threadIdx.x; a < kraw; a += blockDim.x) {
+          D v = a == j ? X::one() : X::zero();
+          for (int cc = 0; cc < nkeep; ++cc) v = X::sub(v, X::mul(dots[cc], Qc[a + (size_t)cc * cap]));
+          q[a] = v;
+        }
+        __syncthreads();
+        double part = 0.0;
+        for (int a = threadIdx.x; a < kraw; a += blockDim.x) {
+          D acc = X::zero();
+          for (int bb = 0; bb < kraw; ++bb) acc = X::add(acc, X::mul(G[a + (size_t)bb * cap], q[bb]));
+          t[a] = acc;
+          part += X::dot_re(q[a], acc);
+        }
+        const double len = sqrt(fmax(block_sum(part, red), 0.0));
+        if (!(len > kDependence)) {
+          if (threadIdx.x == 0) c.dropped += 1;
+          __syncthreads();
+          continue;
+        }
+        for (int a = threadIdx.x; a < kraw; a += blockDim.x) Qc[a + (size_t)nkeep * cap] = X::div(q[a], len);
+        __syncthreads();
+        if (threadIdx.x == 0) sh[5] = nkeep + 1;
+        __syncthreads();
+      }
+      if (threadIdx.x == 0) {
+        const int kk = min(sh[5], cap - c.m);
+        c.kept = kk;
+        if (kk > 0) {
+          nn[0 * nk + k] = NN<D>{b.E, Qc, b.Er, cap, kk, kraw, 0};
+          cp[0 * nk + k] = CP<D>{b.Er, Vt, kk, 0};
+          tn[0 * nk + k] = TN<D>{b.V, Vt, b.S + (size_t)c.m * cap, cap, c.m + kk, kk};
+        }
+      }
+      break;
+    }
+    case kApply: {
+      const int m = c.m, kk = c.kept;
+      if (c.repair && kk > 0) {
+        mirror(b.S, m, m + kk);
+        if (!chol_extend(b.S, cap, b.L, m, m + kk, &sh[4])) {
+          set_err(kErrRepairDependent);
+          break;
+        }
+      }
+      for (int i = threadIdx.x; i < n; i += blockDim.x) b.old[i] = b.w[i];
+      if (threadIdx.x == 0 && kk > 0) {
+        c.h_calls += 1;
+        c.h_columns += kk;
+        dyn[k] = DynCols{reinterpret_cast<const double*>(Vt), reinterpret_cast<double*>(b.HV + (int64_t)m * rows), kk,
+                         gamma ? (kk + 1) / 2 : kk};
+        tn[0 * nk + k] = TN<D>{b.V, b.HV + (int64_t)m * rows, b.Hr + (size_t)m * cap, cap, m + kk, kk};
+      }
+      break;
+    }
+    case kFinish: {
+      const int kk = c.kept;
+      if (kk > 0) {
+        mirror(b.Hr, c.m, c.m + kk);
+        if (!eigen(b, cap, c.m + kk, red, sh)) {
+          set_err(kErrEigen);
+          break;
+        }
+      }
+      if (threadIdx.x == 0) {
+        if (kk > 0) {
+          c.m += kk;
+          c.reduced_solves += 1;
+        }
+        int na = 0;
+        for (int i = 0; i < n; ++i) {
+          const double thr = (o.first_step || i < o.occupied) ? o.threshold : fmax(5.0 * o.threshold, 5e-6);
+          const bool cv = fabs(b.w[i] - b.old[i]) < thr;
+          b.conv[i] = cv ? 1 : 0;
+          if (!cv) b.active[na++] = i;
+        }
+        c.nact = na;
+        c.iterations += 1;
+        if (na == 0 || c.iterations == o.max_iterations) {
+          c.status = 1;
+        } else if (c.m + na > cap) {
+          c.contract = 1;   // the reference contracts at the end of this iteration
+        }
+      }
+      break;
+    }
+    case kFinal: {
+      if (c.status < 0) break;
+      if (threadIdx.x == 0) nn[0 * nk + k] = NN<D>{b.V, b.C, b.X, cap, n, c.m, 0};
+      break;
+    }
+    default:
+      break;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) ctl[k] = c;
+}
+
+// ------------------------------------------------------------------ host side
+template <class T>
+struct DevOf;
+template <>
+struct DevOf<double> {
+  using type = double;
+};
+template <>
+struct DevOf<std::complex<double>> {
+  using type = double2;
+};
+
+const char* error_text(int id) {
+  switch (id) {
+    case kErrStartDependent: return "reference Davidson start is numerically dependent";
+    case kErrBasisDependent: return "reference Davidson basis is numerically dependent";
+    case kErrNonfiniteCorrection: return "nonfinite reference correction";
+    case kErrCapacity: return "capacity cannot hold the active correction block; use at least 2*bands";
+    case kErrRepairDependent: return "reference overlap remains dependent after repair";
+    case kErrEigen: return "reference reduced eigensolve failed";
+    default: return "reference Davidson failed";
+  }
+}
+
+template <class T>
+class KsetSolver {
+ public:
+  using D = typename DevOf<T>::type;
+  KsetSolver(bg_kset* ks, const Opts& o, bool graph) : ks_(ks), nk_((int)ks->ops.size()), o_(o), want_graph_(graph) {
+    s_ = ks->stream;
+  }
+  ~KsetSolver() {
+    if (exec_) cudaGraphExecDestroy(exec_);
+    if (graph_) cudaGraphDestroy(graph_);
+    for (void* p : dev_) cudaFree(p);
+    if (h_ctl_) cudaFreeHost(h_ctl_);
+  }
+  int run(const double* const* start, const double* const* diagonal, int32_t ptr_kind, double* const* values,
+          double* const* vectors, int32_t* const* converged, bg_davidson_stats* stats);
+  const std::string& error() const { return err_; }
+  int64_t launches() const { return launches_; }
+
+ private:
+  bg_kset* ks_;
+  int nk_;
+  Opts o_;
+  bool want_graph_;
+  cudaStream_t s_;
+  std::vector<void*> dev_;
+  std::vector<Bufs<D>> hb_;
+  Bufs<D>* d_bufs_ = nullptr;
+  Ctl* d_ctl_ = nullptr;
+  Ctl* h_ctl_ = nullptr;
+  NN<D>* d_nn_ = nullptr;
+  TN<D>* d_tn_ = nullptr;
+  CP<D>* d_cp_ = nullptr;
+  DynCols* d_dyn_ = nullptr;
+  const D** d_dense_ = nullptr;
+  int ksplit_ = 1;
+  int64_t slot_elems_ = 0;
+  int max_rows_ = 0;
+  std::vector<CallArgs> args_;
+  std::vector<int64_t> cols_;
+  cudaGraph_t graph_ = nullptr;
+  cudaGraphExec_t exec_ = nullptr;
+  int64_t per_iteration_ = 0;
+  int64_t launches_ = 0;
+  std::string err_;
+
+  template <class P>
+  int alloc(P** p, size_t count) {
+    void* q = nullptr;
+    if (cudaMalloc(&q, std::max<size_t>(count, 1) * sizeof(P)) != cudaSuccess) {
+      err_ = "cudaMalloc failed";
+      return BG_ENOMEM;
+    }
+    dev_.push_back(q);
+    *p = static_cast<P*>(q);
+    return BG_OK;
+  }
+  int cuda(cudaError_t e, const char* what) {
+    if (e == cudaSuccess) return BG_OK;
+    err_ = std::string(what) + ": " + cudaGetErrorString(e);
+    return BG_EDEVICE;
+  }
+  int64_t ctl(int phase) {
+    k_dv_ctl<D><<<nk_, kCtlThreads, 0, s_>>>(phase, d_bufs_, d_ctl_, d_nn_, d_tn_, d_cp_, d_dyn_, o_, nk_,
+                                            ks_->gamma);
+    return 1;
+  }
+  int64_t nn(int nslots) {
+    const dim3 grid((unsigned)((max_rows_ + 63) / 64), (unsigned)((o_.cap + 31) / 32), (unsigned)(nslots * nk_));
+    k_dv_nn<D><<<grid, 128, 0, s_>>>(d_bufs_, d_nn_, nk_);
+    return 1;
+  }
+  int64_t tn(int nslots) {
+    const unsigned t = (unsigned)((o_.cap + 31) / 32);
+    k_dv_tn<D><<<dim3(t, t, (unsigned)(nslots * nk_ * ksplit_)), 64, 0, s_>>>(d_bufs_, d_tn_, nk_, ksplit_,
+                                                                             slot_elems_);
+    const unsigned blocks = (unsigned)std::min<int64_t>(((int64_t)o_.cap * o_.cap + 255) / 256, 64);
+    k_dv_tn_sum<D><<<dim3(blocks, 1, (unsigned)(nslots * nk_)), 256, 0, s_>>>(d_bufs_, d_tn_, nk_, ksplit_,
+                                                                              slot_elems_);
+    return 2;
+  }
+  int64_t cp(int slot0, int nslots) {
+    const dim3 grid((unsigned)std::min((max_rows_ + 255) / 256, 64), (unsigned)o_.cap, (unsigned)(nslots * nk_));
+    k_dv_copy<D><<<grid, 256, 0, s_>>>(d_bufs_, d_cp_ + (size_t)slot0 * nk_, nk_);
+    return 1;
+  }
+  int64_t corr() {
+    k_dv_corrections<D><<<dim3((unsigned)o_.n, (unsigned)nk_), 256, 0, s_>>>(d_bufs_, d_ctl_);
+    return 1;
+  }
+  int64_t apply() {
+    if (ks_->dense) {
+      const dim3 grid((unsigned)((max_rows_ + 63) / 64), (unsigned)((o_.n + 31) / 32), (unsigned)nk_);
+      k_dv_dense<D><<<grid, 128, 0, s_>>>(d_dense_, d_bufs_, d_dyn_);
+      return 1;
+    }
+    return enqueue_range(ks_, 0, nk_, args_.data(), cols_.data(), s_, nullptr);
+  }
+  int64_t iteration() {
+    int64_t l = 0;
+    l += ctl(kBegin) + nn(2) + cp(0, 2) + tn(2);
+    l += ctl(kRefresh) + nn(2) + corr();
+    l += ctl(kSelect) + cp(0, 1) + tn(1);
+    l += ctl(kExtend) + cp(0, 1) + nn(2) + cp(1, 2);
+    l += ctl(kRepair1) + tn(1);
+    l += ctl(kRepair2) + nn(1) + tn(1);
+    l += ctl(kRepair3) + nn(1) + tn(1);
+    l += ctl(kRepair4) + nn(1) + cp(0, 1) + tn(1);
+    l += ctl(kApply) + apply() + tn(1);
+    l += ctl(kFinish);
+    return l;
+  }
+  int poll(bool* all_done) {
+    int rc = cuda(cudaMemcpyAsync(h_ctl_, d_ctl_, sizeof(Ctl) * nk_, cudaMemcpyDeviceToHost, s_), "poll");
+    if (!rc) rc = cuda(cudaStreamSynchronize(s_), "Davidson iteration");
+    if (rc) return rc;
+    *all_done = true;
+    for (int k = 0; k < nk_; ++k) {
+      if (h_ctl_[k].status < 0) {
+        err_ = std::string(error_text(-h_ctl_[k].status)) + " (k point " + std::to_string(k) + ")";
+        return BG_EINVAL;
+      }
+      if (h_ctl_[k].status == 0) *all_done = false;
+    }
+    return BG_OK;
+  }
+};
+
+template <class T>
+int KsetSolver<T>::run(const double* const* start, const double* const* diagonal, int32_t ptr_kind,
+                       double* const* values, double* const* vectors, int32_t* const* converged,
+                       bg_davidson_stats* stats) {
+  const int n = o_.n, cap = o_.cap;
+  int rc;
+  hb_.resize(nk_);
+  max_rows_ = 0;
+  for (int k = 0; k < nk_; ++k) max_rows_ = std::max<int>(max_rows_, (int)ks_->ops[k]->rows);
+  const int64_t tiles = (int64_t)((cap + 31) / 32) * ((cap + 31) / 32);
+  ksplit_ = (int)std::max<int64_t>(1, std::min<int64_t>((8 * 148 + tiles * nk_ - 1) / (tiles * nk_), 32));
+  ksplit_ = (int)std::max<int64_t>(1, std::min<int64_t>(ksplit_, (max_rows_ + 255) / 256));
+  slot_elems_ = (int64_t)ksplit_ * cap * cap;
+  const size_t cc = (size_t)cap * cap;
+  for (int k = 0; k < nk_; ++k) {
+    Bufs<D>& b = hb_[k];
+    const size_t rc_ = (size_t)ks_->ops[k]->rows * cap;
+    b.rows = (int)ks_->ops[k]->rows;
+    if ((rc = alloc(&b.V, rc_)) || (rc = alloc(&b.HV, rc_)) || (rc = alloc(&b.X, rc_)) || (rc = alloc(&b.HX, rc_)) ||
+        (rc = alloc(&b.E, rc_)) || (rc = alloc(&b.Er, rc_)) || (rc = alloc(&b.S, cc)) || (rc = alloc(&b.Hr, cc)) ||
+        (rc = alloc(&b.L, cc)) || (rc = alloc(&b.C, cc)) || (rc = alloc(&b.A, cc)) || (rc = alloc(&b.Y, cc)) ||
+        (rc = alloc(&b.P, cc)) || (rc = alloc(&b.Q, cc)) || (rc = alloc(&b.Z, cc)) || (rc = alloc(&b.w, cap)) ||
+        (rc = alloc(&b.old, cap)) || (rc = alloc(&b.lam, cap)) || (rc = alloc(&b.norms, cap)) ||
+        (rc = alloc(&b.scale, cap)) || (rc = alloc(&b.td, cap)) || (rc = alloc(&b.te, cap)) ||
+        (rc = alloc(&b.off, cap)) || (rc = alloc(&b.ph, cap)) || (rc = alloc(&b.hv, cap)) || (rc = alloc(&b.hp, cap)) ||
+        (rc = alloc(&b.hq, cap)) || (rc = alloc(&b.active, cap)) || (rc = alloc(&b.map, cap)) ||
+        (rc = alloc(&b.conv, cap)) || (rc = alloc(&b.order, cap)) || (rc = alloc(&b.part, 2 * (size_t)slot_elems_)) ||
+        (rc = alloc(&b.rot, 2 * (size_t)cap)) || (rc = alloc(&b.rot_i, cap)))
+      return rc;
+    double* dg = nullptr;
+    if ((rc = alloc(&dg, b.rows))) return rc;
+    b.diag = dg;
+    if ((rc = cuda(cudaMemsetAsync(b.S, 0, sizeof(D) * cc, s_), "memset")) ||
+        (rc = cuda(cudaMemsetAsync(b.Hr, 0, sizeof(D) * cc, s_), "memset")) ||
+        (rc = cuda(cudaMemsetAsync(b.L, 0, sizeof(D) * cc, s_), "memset")) ||
+        (rc = cuda(cudaMemsetAsync(b.C, 0, sizeof(D) * cc, s_), "memset")))
+      return rc;
+    const cudaMemcpyKind kind = ptr_kind == BG_PTR_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    if ((rc = cuda(cudaMemcpyAsync(b.V, start[k], sizeof(D) * (size_t)b.rows * n, kind, s_), "copy in")) ||
+        (rc = cuda(cudaMemcpyAsync(dg, diagonal[k], sizeof(double) * b.rows, kind, s_), "copy in")))
+      return rc;
+  }
+  if ((rc = alloc(&d_bufs_, nk_)) || (rc = alloc(&d_ctl_, nk_)) || (rc = alloc(&d_nn_, (size_t)kNnSlots * nk_)) ||
+      (rc = alloc(&d_tn_, (size_t)kTnSlots * nk_)) || (rc = alloc(&d_cp_, (size_t)kCpSlots * nk_)) ||
+      (rc = alloc(&d_dyn_, nk_)))
+    return rc;
+  if ((rc = cuda(cudaMallocHost(&h_ctl_, sizeof(Ctl) * nk_), "cudaMallocHost"))) return rc;
+  if (ks_->dense) {
+    std::vector<const D*> hd(nk_);
+    for (int k = 0; k < nk_; ++k) hd[k] = reinterpret_cast<const D*>(ks_->ops[k]->dense);
+    if ((rc = alloc(&d_dense_, nk_))) return rc;
+    if ((rc = cuda(cudaMemcpyAsync(d_dense_, hd.data(), sizeof(const D*) * nk_, cudaMemcpyHostToDevice, s_), "upload")))
+      return rc;
+  }
+  // start: H V and the Grams of the start block, descriptors written from the host
+  std::vector<Ctl> c0(nk_);
+  std::vector<DynCols> dy(nk_);
+  std::vector<TN<D>> t0((size_t)kTnSlots * nk_);
+  for (int k = 0; k < nk_; ++k) {
+    Ctl& c = c0[k];
+    std::memset(&c, 0, sizeof c);
+    c.m = n;
+    c.nact = n;
+    c.h_calls = 1;
+    c.h_columns = n;
+    const Bufs<D>& b = hb_[k];
+    dy[k] = DynCols{reinterpret_cast<const double*>(b.V), reinterpret_cast<double*>(b.HV), n,
+                    ks_->gamma ? (n + 1) / 2 : n};
+    t0[k] = TN<D>{b.V, b.V, b.S, cap, n, n};
+    t0[(size_t)nk_ + k] = TN<D>{b.V, b.HV, b.Hr, cap, n, n};
+  }
+  if ((rc = cuda(cudaMemcpyAsync(d_bufs_, hb_.data(), sizeof(Bufs<D>) * nk_, cudaMemcpyHostToDevice, s_), "upload")) ||
+      (rc = cuda(cudaMemcpyAsync(d_ctl_, c0.data(), sizeof(Ctl) * nk_, cudaMemcpyHostToDevice, s_), "upload")) ||
+      (rc = cuda(cudaMemcpyAsync(d_dyn_, dy.data(), sizeof(DynCols) * nk_, cudaMemcpyHostToDevice, s_), "upload")) ||
+      (rc = cuda(cudaMemcpyAsync(d_tn_, t0.data(), sizeof(TN<D>) * t0.size(), cudaMemcpyHostToDevice, s_), "upload")))
+    return rc;
+  args_.assign(nk_, CallArgs{});
+  cols_.assign(nk_, n);
+  for (int k = 0; k < nk_; ++k) {
+    CallArgs& a = args_[k];
+    const int64_t dpc = ks_->gamma ? hb_[k].rows : 2 * (int64_t)hb_[k].rows;
+    a.x = reinterpret_cast<const double*>(hb_[k].V);
+    a.y = reinterpret_cast<double*>(hb_[k].HV);
+    a.ldx = a.ldy = dpc;
+    a.cols = n;
+    a.units = ks_->gamma ? (n + 1) / 2 : n;
+    a.dyn = d_dyn_ + k;
+  }
+  launches_ += apply() + tn(2) + ctl(kSetup);
+  bool done = false;
+  if ((rc = poll(&done))) return rc;
+  // iterations: one captured graph replayed until every k point has finished
+  bool graph_ok = false;
+  if (want_graph_) {
+    cudaStreamCaptureStatus st;
+    if (cudaStreamIsCapturing(s_, &st) == cudaSuccess && st == cudaStreamCaptureStatusNone &&
+        cudaStreamBeginCapture(s_, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+      const int64_t per = iteration();
+      if (cudaStreamEndCapture(s_, &graph_) == cudaSuccess && graph_ &&
+          cudaGraphInstantiate(&exec_, graph_, 0) == cudaSuccess) {
+        graph_ok = true;
+        per_iteration_ = per;
+      }
+    }
+    cudaGetLastError();
+  }
+  for (int it = 0; it < o_.max_iterations && !done; ++it) {
+    if (graph_ok) {
+      if ((rc = cuda(cudaGraphLaunch(exec_, s_), "cudaGraphLaunch"))) return rc;
+      launches_ += per_iteration_;
+    } else {
+      launches_ += iteration();
+    }
+    if ((rc = cuda(cudaGetLastError(), "Davidson launch"))) return rc;
+    if ((rc = poll(&done))) return rc;
+  }
+  // X = V C[:, :n]; outputs
+  launches_ += ctl(kFinal) + nn(1);
+  if ((rc = poll(&done))) return rc;
+  std::vector<double> w(n);
+  std::vector<int> cv(n);
+  for (int k = 0; k < nk_; ++k) {
+    const Bufs<D>& b = hb_[k];
+    const cudaMemcpyKind kind = ptr_kind == BG_PTR_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+    if ((rc = cuda(cudaMemcpyAsync(vectors[k], b.X, sizeof(D) * (size_t)b.rows * n, kind, s_), "copy out")) ||
+        (rc = cuda(cudaMemcpyAsync(w.data(), b.w, sizeof(double) * n, cudaMemcpyDeviceToHost, s_), "copy out")) ||
+        (rc = cuda(cudaMemcpyAsync(cv.data(), b.conv, sizeof(int) * n, cudaMemcpyDeviceToHost, s_), "copy out")) ||
+        (rc = cuda(cudaStreamSynchronize(s_), "copy out")))
+      return rc;
+    const Ctl& c = h_ctl_[k];
+    bg_davidson_stats st{};
+    for (int i = 0; i < n; ++i) {
+      values[k][i] = w[i];
+      converged[k][i] = c.iterations > 0 ? cv[i] : 0;
+      st.converged_count += converged[k][i];
+    }
+    st.iterations = c.iterations;
+    st.reduced_solves = c.reduced_solves;
+    st.h_calls = c.h_calls;
+    st.h_columns = c.h_columns;
+    st.repairs = c.repairs;
+    st.contractions = c.contractions;
+    st.dropped = c.dropped;
+    if (stats) stats[k] = st;
+  }
+  // a non-finite block met by the applies
+  for (int k = 0; k < nk_; ++k) {
+    bg_op* op = ks_->ops[k];
+    int errw = 0;
+    if ((rc = cuda(cudaMemcpyAsync(&errw, op->t.err, sizeof(int), cudaMemcpyDeviceToHost, s_), "error word")) ||
+        (rc = cuda(cudaStreamSynchronize(s_), "error word")))
+      return rc;
+    if (errw) {
+      cudaMemsetAsync(op->t.err, 0, sizeof(int), s_);
+      cudaStreamSynchronize(s_);
+      err_ = "non-finite block in a Davidson apply (k point " + std::to_string(k) + ")";
+      return BG_ENONFINITE;
+    }
+  }
+  return BG_OK;
+}
+
+}  // namespace dv
+}  // namespace bg
+
+using namespace bg;
+using namespace bg::dv;
+
+extern "C" int bg_kset_davidson_solve(bg_kset* ks, const double* const* start, const double* const* diagonal,
+                                      const bg_davidson_options* options, int32_t ptr_kind, double* const* eigenvalues,
+                                      double* const* eigenvectors, int32_t* const* converged,
+                                      bg_davidson_stats* stats) {
+  if (!ks) return fail(nullptr, BG_EINVAL, "null k-point set");
+  bg_ctx* ctx = ks->ctx;
+  if (!start || !diagonal || !options || !eigenvalues || !eigenvectors || !converged)
+    return fail(ctx, BG_EINVAL, "null argument");
+  if (ptr_kind != BG_PTR_HOST && ptr_kind != BG_PTR_DEVICE) return fail(ctx, BG_EINVAL, "pointer kind");
+  const bg_davidson_options o = *options;
+  const int nk = (int)ks->ops.size();
+  const int64_t n = o.bands;
+  int64_t cap = o.capacity == 0 ? 2 * n : o.capacity;
+  bool bad = n <= 0 || o.occupied > n || o.occupied < 0 || o.max_iterations <= 0 || !std::isfinite(o.threshold) ||
+             o.threshold <= 0.0;
+  for (int k = 0; k < nk && !bad; ++k) {
+    const bg_op* op = ks->ops[k];
+    const int64_t rows = op->rows;
+    // crates/dft-solvers/src/ref_davidson.rs:133-146, per k point
+    const int64_t capk = std::min<int64_t>(cap, rows);
+    bad = n > rows || capk < std::min<int64_t>(2 * n, rows) || n > op->cap;
+    cap = std::min(cap, capk);
+  }
+  if (bad || cap > 4096)
+    return fail(ctx, BG_EINVAL, "reference Davidson dimensions/threshold (bands must fit every operator's capacity)");
+  for (int k = 0; k < nk; ++k) {
+    if (!start[k] || !diagonal[k] || !eigenvalues[k] || !eigenvectors[k] || !converged[k])
+      return fail(ctx, BG_EINVAL, "null per-k argument");
+    if (!ks->ops[k]->has_epoch) return fail(ctx, BG_EEPOCH, "potential was never set");
+    if (ptr_kind == BG_PTR_HOST) {
+      const size_t per = ks->gamma ? 1 : 2;
+      const int64_t rows = ks->ops[k]->rows;
+      for (size_t i = 0; i < (size_t)rows * n * per; ++i)
+        if (!std::isfinite(start[k][i])) return fail(ctx, BG_ENONFINITE, "reference Davidson start not finite");
+      for (int64_t i = 0; i < rows; ++i)
+        if (!std::isfinite(diagonal[k][i])) return fail(ctx, BG_ENONFINITE, "reference Davidson diagonal not finite");
+    }
+  }
+  cudaError_t e = cudaSetDevice(ctx->device);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaSetDevice");
+  Opts op{(int)n, (int)cap, (int)o.occupied, o.first_step ? 1 : 0, o.max_iterations, o.threshold};
+  const bool graph = (o.reserved[0] & 1) == 0;
+  int rc;
+  std::string err;
+  int64_t launches = 0;
+  if (ks->gamma) {
+    KsetSolver<double> s(ks, op, graph);
+    rc = s.run(start, diagonal, ptr_kind, eigenvalues, eigenvectors, converged, stats);
+    err = s.error();
+    launches = s.launches();
+  } else {
+    KsetSolver<std::complex<double>> s(ks, op, graph);
+    rc = s.run(start, diagonal, ptr_kind, eigenvalues, eigenvectors, converged, stats);
+    err = s.error();
+    launches = s.launches();
+  }
+  ks->launches += launches;
+  if (rc != BG_OK) return fail(ctx, rc, err.empty() ? "reference Davidson failed" : err);
+  return BG_OK;
+}

@@ -62,7 +62,33 @@ struct bg_op {
 };
 
 
+// A set of operators of one grid applied in batched launches (bg_kset_*).
+struct bg_kset {
+  bg_ctx* ctx = nullptr;
+  std::vector<bg_op*> ops;
+  int gamma = 0;
+  bool dense = false;  // dense test operators: only bg_kset_davidson_solve accepts the set
+  int max_groups = 0;
+  int max_rows = 0;
+  bg::NlShape shape{};
+  bg::BoxGeo g{};
+  bg::OpTables* d_tabs = nullptr;
+  bg::NlDev* d_nl = nullptr;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  bg::StageEvents ev;
+  int64_t launches = 0;
+  // host-buffer applies: copy-in, compute and copy-out streams pipelined over chunks
+  static constexpr int kChunks = 4;
+  cudaStream_t pipe[3] = {nullptr, nullptr, nullptr};
+  cudaEvent_t in_done[kChunks] = {}, work_done[kChunks] = {};
+};
+
 namespace bg {
+// Launch the local and nonlocal stages of operators [k0, k1) of a set on one stream
+// (cols[k]: the widest block of operator k, used to size the grids).
+int enqueue_range(bg_kset* ks, int k0, int k1, const CallArgs* args, const int64_t* cols, cudaStream_t s,
+                  StageEvents* ev);
 // Failure message on the context (or the thread's context-free slot) and status.
 int fail(bg_ctx* ctx, int code, const std::string& msg);
 int cuda_fail(bg_ctx* ctx, cudaError_t e, const char* what);

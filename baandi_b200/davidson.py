@@ -76,3 +76,39 @@ def solve(operator: _Operator, start: np.ndarray, hamiltonian_diagonal: np.ndarr
     operator._check(rc)
     return Solution(vals, vecs, conv.astype(bool), st.iterations, st.reduced_solves, st.h_calls, st.h_columns,
                     st.repairs, st.contractions, st.dropped)
+
+
+def solve_kset(kset, starts, diagonals, options: Options, graph: bool = True):
+    """The reference Davidson for every k point of a KPointSet at once
+    (bg_kset_davidson_solve): each large product is one launch over all k points, the
+    reduced problems and control decisions run on the GPU, and an iteration is one
+    replayed CUDA graph (graph=False launches the same kernels one by one).  starts /
+    diagonals: one (rows_k x bands) block and one rows_k diagonal per k point (host).
+    Returns one Solution per k point."""
+    lib = L.load()
+    real = kset.ops[0].is_real()
+    dt = np.float64 if real else np.complex128
+    nk = len(kset.ops)
+    if len(starts) != nk or len(diagonals) != nk:
+        raise SolverError(L.BG_ESHAPE, "one start block and one diagonal per k point")
+    x0 = [np.asfortranarray(x, dtype=dt) for x in starts]
+    dg = [np.ascontiguousarray(d, dtype=np.float64) for d in diagonals]
+    n = options.bands
+    for op, x, d in zip(kset.ops, x0, dg):
+        if x.shape != (op.global_len(), n) or d.shape != (op.global_len(),):
+            raise SolverError(L.BG_ESHAPE, "start must be rows x bands, diagonal rows")
+    vals = [np.zeros(n) for _ in range(nk)]
+    vecs = [np.zeros((op.global_len(), n), dtype=dt, order="F") for op in kset.ops]
+    conv = [np.zeros(n, np.int32) for _ in range(nk)]
+    stats = (L.DavidsonStats * nk)()
+    o = L.DavidsonOptions(options.bands, options.threshold, options.occupied, 1 if options.first_step else 0,
+                          options.capacity, options.max_iterations)
+    if not graph:
+        o.reserved[0] = 1
+    arr = lambda lst: (ctypes.c_void_p * nk)(*[a.ctypes.data for a in lst])
+    rc = lib.bg_kset_davidson_solve(kset.handle, arr(x0), arr(dg), ctypes.byref(o), L.BG_PTR_HOST, arr(vals),
+                                    arr(vecs), arr(conv), stats)
+    kset._check(rc)
+    return [Solution(vals[k], vecs[k], conv[k].astype(bool), stats[k].iterations, stats[k].reduced_solves,
+                     stats[k].h_calls, stats[k].h_columns, stats[k].repairs, stats[k].contractions, stats[k].dropped)
+            for k in range(nk)]

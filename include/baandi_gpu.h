@@ -245,6 +245,24 @@ int bg_davidson_solve(bg_op* op, const double* start, const double* diagonal,
                       const bg_davidson_options* options, double* eigenvalues, double* eigenvectors,
                       int32_t* converged, bg_davidson_stats* stats);
 
+/* The same reference Davidson for every k point of a set at once, driven from the GPU
+ * (the reference solves the k points of a map one after another,
+ * crates/dft-engine/src/refscf/k_map.rs:136-210, each with ref_davidson_complex.rs:
+ * 798-1082).  Every large product is one launch over all k points, the reduced problem
+ * (bordered Cholesky, Householder tridiagonalisation, implicit QL) and the control
+ * decisions (contraction, dropped corrections, repair, convergence) run in a
+ * one-block-per-k-point kernel, and one iteration is a CUDA graph replayed until all k
+ * points finish.  Per-k arrays (nk = set size): start[k] rows_k x bands, diagonal[k]
+ * rows_k, eigenvalues[k] bands, eigenvectors[k] rows_k x bands, converged[k] bands;
+ * start/diagonal/eigenvectors have ptr_kind (eigenvalues and converged are host);
+ * stats: nk entries or NULL.  options.reserved[0] bit 0 set: launch the iteration's
+ * kernels directly instead of replaying the graph (same results).  The Davidson
+ * capacity is the smallest over the k points; bands must fit every operator's capacity.
+ * Errors name the k point; the solve runs on the set's stream and returns when done. */
+int bg_kset_davidson_solve(bg_kset* set, const double* const* start, const double* const* diagonal,
+                           const bg_davidson_options* options, int32_t ptr_kind, double* const* eigenvalues,
+                           double* const* eigenvectors, int32_t* const* converged, bg_davidson_stats* stats);
+
 /* Dense operator y = H x of a rows x rows column-major matrix (interleaved complex when
  * is_complex), for fixtures and small exact tests of the solver. */
 int bg_op_create_dense(bg_ctx* ctx, int64_t rows, const double* h, int32_t is_complex, int64_t capacity,
