@@ -59,6 +59,15 @@ class DavidsonStats(ctypes.Structure):
                 ("repairs", _i32), ("contractions", _i32), ("dropped", _i32), ("converged_count", _i32)]
 
 
+class MixerProfile(ctypes.Structure):
+    _fields_ = [("beta", _dbl), ("history", _i32), ("thomas_fermi", _i32), ("reserved", _i32 * 4)]
+
+
+class MixerDiagnostics(ctypes.Structure):
+    _fields_ = [("iteration", _i32), ("occupancy", _i32), ("inserted_slot", _i32), ("reserved", _i32),
+                ("gamma_l2", _dbl), ("gamma_max", _dbl), ("condition", _dbl)]
+
+
 class SpeciesDesc(ctypes.Structure):
     _fields_ = [("z_valence", _dbl), ("mesh", _i32), ("r", _p), ("rab", _p), ("local", _p), ("nbeta", _i32),
                 ("l", _p), ("beta_len", _p), ("beta", _p), ("dij", _p), ("natoms", _i32), ("positions", _p)]
@@ -90,6 +99,13 @@ SIGNATURES = {
     "bg_fields_set_stream": [_p, _p],
     "bg_fields_volume": [_p, ctypes.POINTER(_dbl)],
     "bg_fields_lda_hartree": [_p, _p, _p, _p, _p, _i32],
+    "bg_mixer_create": [_p, ctypes.POINTER(MixerProfile), _i64, _p, _p, _dbl, _dbl, _dbl, _pp],
+    "bg_mixer_destroy": [_p],
+    "bg_mixer_set_stream": [_p, _p],
+    "bg_mixer_update": [_p, _p, _p, _p, _i32, ctypes.POINTER(MixerDiagnostics)],
+    "bg_mixer_gamma": [_p, _p, ctypes.POINTER(_i32)],
+    "bg_mixer_reduced_residual": [_p, _p, _i32],
+    "bg_mixer_metric": [_p, _p, _p, _p, _i32],
     "bg_kset_create": [_p, _i32, _p, _pp],
     "bg_kset_destroy": [_p],
     "bg_kset_apply": [_p, _p, _p, _p, _i32, _i32],

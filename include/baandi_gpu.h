@@ -188,6 +188,46 @@ int bg_fields_volume(const bg_fields* f, double* volume);
 int bg_fields_lda_hartree(bg_fields* f, const double* density, double* v_hxc, double* v_h,
                           double energies[3], int32_t ptr_kind);
 
+/* ------------------------------------------------------------ density mixing */
+/* The reference mixer (crates/dft-engine/src/refscf/broyden.rs, metric.rs) on the GPU:
+ * an unnormalised difference-history Anderson update of complex reciprocal-space
+ * vectors of n entries (interleaved doubles) under the Hartree metric
+ * w_G = 8 pi metric_volume / G^2 on smooth G != 0 (0 elsewhere), Ry. */
+typedef struct bg_mixer bg_mixer;
+typedef struct {
+  double beta;           /* (0, 1], reference default 0.7                              */
+  int32_t history;       /* 1..25, reference default 8                                 */
+  int32_t thomas_fermi;  /* nonzero: screen F~ by G^2 / (G^2 + a) on smooth G         */
+  int32_t reserved[4];
+} bg_mixer_profile;
+typedef struct {
+  int32_t iteration;     /* updates so far, this one included                          */
+  int32_t occupancy;     /* secant pairs used                                          */
+  int32_t inserted_slot; /* ring slot written by this update, -1 on the first          */
+  int32_t reserved;
+  double gamma_l2, gamma_max;
+  double condition;      /* lambda_max / lambda_min of the history Gram (0: no history) */
+} bg_mixer_diagnostics;
+/* g2: n values |G|^2 (Bohr^-2), smooth: n flags; volume and electrons set the Thomas-
+ * Fermi wave number (broyden.rs:96-123); metric_volume the metric weights. */
+int bg_mixer_create(bg_ctx* ctx, const bg_mixer_profile* profile, int64_t n, const double* g2,
+                    const int32_t* smooth, double volume, double electrons, double metric_volume,
+                    bg_mixer** out);
+int bg_mixer_destroy(bg_mixer* m);
+int bg_mixer_set_stream(bg_mixer* m, void* stream);
+/* Broyden::update (broyden.rs:319-435): next from x and F = y - x.  A numerically
+ * rank-deficient history (lambda_min <= p eps lambda_max) returns BG_EINVAL ("singular
+ * Broyden history ...") and, like a non-finite result (BG_ENONFINITE), ends the mixer:
+ * later updates fail.  Returns when next is ready (x, f, next have ptr_kind). */
+int bg_mixer_update(bg_mixer* m, const double* x, const double* f, double* next, int32_t ptr_kind,
+                    bg_mixer_diagnostics* diag);
+/* gamma of the last update (host, up to 25 values; *count = its occupancy). */
+int bg_mixer_gamma(const bg_mixer* m, double* gamma, int32_t* count);
+/* F~ = F - gamma.dF of the last update before screening (broyden.rs:200-206). */
+int bg_mixer_reduced_residual(bg_mixer* m, double* out, int32_t ptr_kind);
+/* The metric form <a, b> (metric.rs:147-200), Ry. */
+int bg_mixer_metric(bg_mixer* m, const double* a, const double* b, double* out, int32_t ptr_kind);
+
 /* ------------------------------------------------------------ k-point sets */
 /* All bands of several k points in one launch per stage.  The reference solves the k
  * points of a map one after another (crates/dft-engine/src/refscf/k_map.rs:136-210,
