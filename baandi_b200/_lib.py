@@ -19,6 +19,7 @@ BG_EDEVICE = 4
 BG_ETIMEOUT = 5
 BG_EINVAL = 6
 BG_ENOMEM = 7
+BG_PRECOND_SMOOTH, BG_PRECOND_TPA, BG_PRECOND_RITZ_SHIFT = 0, 1, 2
 BG_PTR_HOST = 0
 BG_PTR_DEVICE = 1
 BG_PREC_FP64 = 0
@@ -51,7 +52,7 @@ class Projectors(ctypes.Structure):
 
 class DavidsonOptions(ctypes.Structure):
     _fields_ = [("bands", _i64), ("threshold", _dbl), ("occupied", _i64), ("first_step", _i32), ("capacity", _i64),
-                ("max_iterations", _i32), ("reserved", _i32 * 4)]
+                ("max_iterations", _i32), ("flags", _i32), ("preconditioner", _i32), ("reserved", _i32 * 2)]
 
 
 class DavidsonStats(ctypes.Structure):

@@ -38,6 +38,77 @@ struct Arith<double2> {
   __device__ static double norm2(double2 a) { return a.x * a.x + a.y * a.y; }
 };
 
+// Positive TPA damping of kinetic coordinate t at band scale s (crates/dft-solvers/src/
+// lib.rs:194-206; the reciprocal form for t > s avoids polynomial overflow).
+__device__ __forceinline__ double tpa_weight(double t, double s) {
+  const double x = t / s;
+  if (x <= 1.0) {
+    const double p = 27.0 + x * (18.0 + x * (12.0 + x * 8.0));
+    return p / (p + 16.0 * x * x * x * x);
+  }
+  const double y = s / t;
+  const double p = y * (8.0 + y * (12.0 + y * (18.0 + y * 27.0)));
+  return p / (p + 16.0);
+}
+
+// Reference Davidson smooth denominator (crates/dft-solvers/src/ref_davidson.rs:418-422).
+__device__ __forceinline__ double smooth_denominator(double h, double e) {
+  const double x = 2.0 * (h - e);
+  const double z = fabs(x - 1.0);
+  return 0.25 * (2.0 * fmax(x, 1.0) + 1.0 / (sqrt(1.0 + z * z) + z));
+}
+
+// Block-wide sum (blockDim.x = 256) through a shared array of 256 doubles.
+__device__ __forceinline__ double block_sum256(double v, double* red) {
+  red[threadIdx.x] = v;
+  __syncthreads();
+  for (int s = 128; s > 0; s >>= 1) {
+    if ((int)threadIdx.x < s) red[threadIdx.x] += red[threadIdx.x + s];
+    __syncthreads();
+  }
+  const double r = red[0];
+  __syncthreads();
+  return r;
+}
+
+// Correction of one band column from its Ritz vector x and H x (rows entries):
+// kind 0 (smooth) out = (hx - e x) / d(diag, e); kind 1 (TPA) out = -(hx - e x)
+// tpa(diag, s) with s = max(0.1, sum |x|^2 diag / sum |x|^2), diag = kinetic;
+// kind 2 (Ritz shift) out = -(hx - e x) / max(diag - e, 0.1).  Returns |out|^2 (all
+// threads of the 256-thread block).
+template <class D>
+__device__ double correction_column(const D* __restrict__ x, const D* __restrict__ hx,
+                                    const double* __restrict__ diag, double e, int kind, int64_t rows,
+                                    D* __restrict__ out, double* red) {
+  double scale = 0.0;
+  if (kind == 1) {
+    double w = 0.0, wt = 0.0;
+    for (int64_t r = threadIdx.x; r < rows; r += blockDim.x) {
+      const double a = Arith<D>::norm2(x[r]);
+      w += a;
+      wt += a * diag[r];
+    }
+    w = block_sum256(w, red);
+    wt = block_sum256(wt, red);
+    scale = fmax(wt / w, 0.1);
+  }
+  double acc = 0.0;
+  for (int64_t r = threadIdx.x; r < rows; r += blockDim.x) {
+    const D res = Arith<D>::add(hx[r], Arith<D>::scale(-e, x[r]));
+    double f;
+    if (kind == 1)
+      f = -tpa_weight(diag[r], scale);
+    else if (kind == 2)
+      f = -1.0 / fmax(diag[r] - e, 0.1);
+    else
+      f = 1.0 / smooth_denominator(diag[r], e);
+    const D v = Arith<D>::scale(f, res);
+    out[r] = v;
+    acc += Arith<D>::norm2(v);
+  }
+  return block_sum256(acc, red);
+}
+
 template <class D>
 __global__ void k_sum_parts(const D* __restrict__ P, int ks, int m, int n, D* __restrict__ C, int64_t ldc) {
   const int64_t total = (int64_t)m * n;

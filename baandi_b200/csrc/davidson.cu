@@ -43,38 +43,17 @@ constexpr double kEps = 2.220446049250313e-16;
 constexpr double kDependence = 1e-12;  // crates/dft-numerics/src/linalg.rs:12
 
 // ------------------------------------------------------------------ kernels
-__device__ __forceinline__ double denominator(double h, double e) {
-  const double x = 2.0 * (h - e);
-  const double z = fabs(x - 1.0);
-  return 0.25 * (2.0 * fmax(x, 1.0) + 1.0 / (sqrt(1.0 + z * z) + z));
-}
-
-// E[:, j] = (HX[:, j] - lambda_j X[:, j]) / d(h, lambda_j); norms2[j] = |E[:, j]|^2.
+// E[:, j] = correction of band j (correction_column, preconditioner `kind`);
+// norms2[j] = |E[:, j]|^2.
 template <class D>
 __global__ void __launch_bounds__(256) k_corrections(const D* __restrict__ X, const D* __restrict__ HX, int64_t ld,
                                                      const double* __restrict__ diag, const double* __restrict__ lambda,
-                                                     D* __restrict__ E, double* __restrict__ norms2, int64_t rows) {
-  const int j = blockIdx.x;
-  const double e = lambda[j];
-  const D* x = X + j * ld;
-  const D* hx = HX + j * ld;
-  D* out = E + j * ld;
-  double acc = 0.0;
-  for (int64_t r = threadIdx.x; r < rows; r += blockDim.x) {
-    const double inv = 1.0 / denominator(diag[r], e);
-    D v = Arith<D>::add(hx[r], Arith<D>::scale(-e, x[r]));
-    v = Arith<D>::scale(inv, v);
-    out[r] = v;
-    acc += Arith<D>::norm2(v);
-  }
+                                                     D* __restrict__ E, double* __restrict__ norms2, int64_t rows,
+                                                     int kind) {
   __shared__ double red[256];
-  red[threadIdx.x] = acc;
-  __syncthreads();
-  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
-    if (threadIdx.x < s) red[threadIdx.x] += red[threadIdx.x + s];
-    __syncthreads();
-  }
-  if (threadIdx.x == 0) norms2[j] = red[0];
+  const int j = blockIdx.x;
+  const double n2 = correction_column(X + j * ld, HX + j * ld, diag, lambda[j], kind, rows, E + j * ld, red);
+  if (threadIdx.x == 0) norms2[j] = n2;
 }
 
 // out[:, c] = scale[c] * in[:, map[c]]
@@ -278,7 +257,7 @@ int Solver<T>::corrections(const std::vector<int>& active, int m, const double* 
   if (!rc) rc = rotate(HV_, m, cs.data(), k, HX_);
   if (rc) return rc;
   cudaMemcpyAsync(lam_, lam.data(), sizeof(double) * k, cudaMemcpyHostToDevice, s_);
-  k_corrections<D><<<k, 256, 0, s_>>>(X_, HX_, rows_, diag_, lam_, Er_, norms_, rows_);
+  k_corrections<D><<<k, 256, 0, s_>>>(X_, HX_, rows_, diag_, lam_, Er_, norms_, rows_, o_.preconditioner);
   std::vector<double> n2(k);
   cudaMemcpyAsync(n2.data(), norms_, sizeof(double) * k, cudaMemcpyDeviceToHost, s_);
   if ((rc = sync("corrections"))) return rc;
@@ -508,7 +487,8 @@ extern "C" int bg_davidson_solve(bg_op* op, const double* start, const double* d
   const int64_t cap = std::min<int64_t>(o.capacity == 0 ? 2 * n : o.capacity, dim);
   // crates/dft-solvers/src/ref_davidson.rs:133-146
   const bool bad = n == 0 || n > dim || cap < std::min<int64_t>(2 * n, dim) || o.occupied > n || o.occupied < 0 ||
-                   o.max_iterations <= 0 || !std::isfinite(o.threshold) || o.threshold <= 0.0 || cap > op->cap;
+                   o.max_iterations <= 0 || !std::isfinite(o.threshold) || o.threshold <= 0.0 || cap > op->cap ||
+                   o.preconditioner < BG_PRECOND_SMOOTH || o.preconditioner > BG_PRECOND_RITZ_SHIFT;
   if (bad) return fail(op->ctx, BG_EINVAL, "reference Davidson dimensions/threshold/start (capacity must also fit the operator)");
   const size_t per = op->gamma ? 1 : 2;
   for (size_t i = 0; i < (size_t)dim * n * per; ++i)

@@ -147,6 +147,7 @@ struct CP {  // dst[:, c] = src[:, c] (scale[c] src[:, map[c]] when pick)
 struct Opts {
   int n, cap, occupied, first_step, max_iterations;
   double threshold;
+  int preconditioner;
 };
 
 // ------------------------------------------------------------------ block-wide small algebra
@@ -585,41 +586,19 @@ __global__ void __launch_bounds__(128) k_dv_dense(const D* const* __restrict__ H
                     dc.cols, rows, r0, j0, false);
 }
 
-__device__ __forceinline__ double denominator(double h, double e) {
-  const double x = 2.0 * (h - e);
-  const double z = fabs(x - 1.0);
-  return 0.25 * (2.0 * fmax(x, 1.0) + 1.0 / (sqrt(1.0 + z * z) + z));
-}
-
-// Er[:, j] = (HX[:, j] - lambda_j X[:, j]) / d(h, lambda_j), norms[j] = |Er[:, j]|^2 for
-// the active bands of every running k point (ref_davidson.rs:418-422, stream.rs:16-67).
+// Corrections of the active bands of every running k point (correction_column with the
+// solver's preconditioner), norms[j] = |Er[:, j]|^2.
 template <class D>
-__global__ void __launch_bounds__(256) k_dv_corrections(const Bufs<D>* __restrict__ bufs, const Ctl* __restrict__ ctl) {
+__global__ void __launch_bounds__(256) k_dv_corrections(const Bufs<D>* __restrict__ bufs, const Ctl* __restrict__ ctl,
+                                                        int kind) {
+  __shared__ double red[256];
   const int j = blockIdx.x, k = blockIdx.y;
   const Ctl& c = ctl[k];
   if (c.status != 0 || j >= c.nact) return;
   const Bufs<D>& b = bufs[k];
   const int64_t rows = b.rows;
-  const double e = b.lam[j];
-  const D* x = b.X + j * rows;
-  const D* hx = b.HX + j * rows;
-  D* out = b.Er + j * rows;
-  double acc = 0.0;
-  for (int64_t r = threadIdx.x; r < rows; r += blockDim.x) {
-    const double inv = 1.0 / denominator(b.diag[r], e);
-    D v = Arith<D>::add(hx[r], Arith<D>::scale(-e, x[r]));
-    v = Arith<D>::scale(inv, v);
-    out[r] = v;
-    acc += Arith<D>::norm2(v);
-  }
-  __shared__ double red[256];
-  red[threadIdx.x] = acc;
-  __syncthreads();
-  for (int st = blockDim.x / 2; st > 0; st >>= 1) {
-    if ((int)threadIdx.x < st) red[threadIdx.x] += red[threadIdx.x + st];
-    __syncthreads();
-  }
-  if (threadIdx.x == 0) b.norms[j] = red[0];
+  const double n2 = correction_column(b.X + j * rows, b.HX + j * rows, b.diag, b.lam[j], kind, rows, b.Er + j * rows, red);
+  if (threadIdx.x == 0) b.norms[j] = n2;
 }
 
 // ------------------------------------------------------------------ control kernel
@@ -1041,7 +1020,7 @@ class KsetSolver {
     return 1;
   }
   int64_t corr() {
-    k_dv_corrections<D><<<dim3((unsigned)o_.n, (unsigned)nk_), 256, 0, s_>>>(d_bufs_, d_ctl_);
+    k_dv_corrections<D><<<dim3((unsigned)o_.n, (unsigned)nk_), 256, 0, s_>>>(d_bufs_, d_ctl_, o_.preconditioner);
     return 1;
   }
   int64_t apply() {
@@ -1264,7 +1243,7 @@ extern "C" int bg_kset_davidson_solve(bg_kset* ks, const double* const* start, c
   const int64_t n = o.bands;
   int64_t cap = o.capacity == 0 ? 2 * n : o.capacity;
   bool bad = n <= 0 || o.occupied > n || o.occupied < 0 || o.max_iterations <= 0 || !std::isfinite(o.threshold) ||
-             o.threshold <= 0.0;
+             o.threshold <= 0.0 || o.preconditioner < BG_PRECOND_SMOOTH || o.preconditioner > BG_PRECOND_RITZ_SHIFT;
   for (int k = 0; k < nk && !bad; ++k) {
     const bg_op* op = ks->ops[k];
     const int64_t rows = op->rows;
@@ -1290,8 +1269,8 @@ extern "C" int bg_kset_davidson_solve(bg_kset* ks, const double* const* start, c
   }
   cudaError_t e = cudaSetDevice(ctx->device);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaSetDevice");
-  Opts op{(int)n, (int)cap, (int)o.occupied, o.first_step ? 1 : 0, o.max_iterations, o.threshold};
-  const bool graph = (o.reserved[0] & 1) == 0;
+  Opts op{(int)n, (int)cap, (int)o.occupied, o.first_step ? 1 : 0, o.max_iterations, o.threshold, o.preconditioner};
+  const bool graph = (o.flags & 1) == 0;
   int rc;
   std::string err;
   int64_t launches = 0;

@@ -25,6 +25,7 @@ class Options:
     first_step: bool = False
     capacity: int = 0
     max_iterations: int = 20
+    preconditioner: str = "smooth"   # "smooth" (reference Davidson), "tpa", "ritz_shift"
 
     def band_threshold(self, band: int) -> float:
         if self.first_step or band < self.occupied:
@@ -54,8 +55,21 @@ def preconditioner_denominator(hamiltonian_diagonal_ha, eigenvalue_ha):
     return 0.25 * (np.where(x >= 1.0, 2.0 * x, 2.0) + 1.0 / (np.hypot(z, 1.0) + z))
 
 
+PRECONDITIONERS = {"smooth": L.BG_PRECOND_SMOOTH, "tpa": L.BG_PRECOND_TPA, "ritz_shift": L.BG_PRECOND_RITZ_SHIFT}
+
+
+def _options(options: Options, flags: int = 0):
+    if options.preconditioner not in PRECONDITIONERS:
+        raise SolverError(L.BG_EINVAL, f"preconditioner {options.preconditioner!r}")
+    return L.DavidsonOptions(options.bands, options.threshold, options.occupied, 1 if options.first_step else 0,
+                             options.capacity, options.max_iterations, flags, PRECONDITIONERS[options.preconditioner])
+
+
 def solve(operator: _Operator, start: np.ndarray, hamiltonian_diagonal: np.ndarray, options: Options) -> Solution:
-    """Lowest `options.bands` eigenpairs of `operator` from `start` (rows x bands)."""
+    """Lowest `options.bands` eigenpairs of `operator` from `start` (rows x bands).
+    `hamiltonian_diagonal` is the H diagonal for the smooth and Ritz-shift corrections
+    and the kinetic diagonal for TPA (the reference builds TPA on kinetic_diagonal,
+    crates/dft-engine/src/oracle/scf.rs:2346-2350)."""
     lib = L.load()
     real = operator.is_real()
     dt = np.float64 if real else np.complex128
@@ -64,8 +78,7 @@ def solve(operator: _Operator, start: np.ndarray, hamiltonian_diagonal: np.ndarr
     if rows != operator.global_len() or n != options.bands:
         raise SolverError(L.BG_ESHAPE, "start must be rows x bands")
     diag = np.ascontiguousarray(hamiltonian_diagonal, dtype=np.float64)
-    o = L.DavidsonOptions(options.bands, options.threshold, options.occupied, 1 if options.first_step else 0,
-                          options.capacity, options.max_iterations)
+    o = _options(options)
     vals = np.zeros(n)
     vecs = np.zeros((rows, n), dtype=dt, order="F")
     conv = np.zeros(n, np.int32)
@@ -101,10 +114,7 @@ def solve_kset(kset, starts, diagonals, options: Options, graph: bool = True):
     vecs = [np.zeros((op.global_len(), n), dtype=dt, order="F") for op in kset.ops]
     conv = [np.zeros(n, np.int32) for _ in range(nk)]
     stats = (L.DavidsonStats * nk)()
-    o = L.DavidsonOptions(options.bands, options.threshold, options.occupied, 1 if options.first_step else 0,
-                          options.capacity, options.max_iterations)
-    if not graph:
-        o.reserved[0] = 1
+    o = _options(options, 0 if graph else 1)
     arr = lambda lst: (ctypes.c_void_p * nk)(*[a.ctypes.data for a in lst])
     rc = lib.bg_kset_davidson_solve(kset.handle, arr(x0), arr(dg), ctypes.byref(o), L.BG_PTR_HOST, arr(vals),
                                     arr(vecs), arr(conv), stats)

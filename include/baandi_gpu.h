@@ -258,8 +258,22 @@ typedef struct {
   int32_t first_step;     /* nonzero: every band uses `threshold`                       */
   int64_t capacity;       /* basis columns; 0 selects min(rows, 2 bands)                 */
   int32_t max_iterations; /* correction iterations (reference default 20)               */
-  int32_t reserved[4];
+  int32_t flags;          /* bg_kset_davidson_solve: bit 0 launches directly (no graph)  */
+  int32_t preconditioner; /* BG_PRECOND_*                                                */
+  int32_t reserved[2];
 } bg_davidson_options;
+
+/* Correction of band j from its residual r = HX_j - lambda_j X_j on row g (the
+ * Preconditioner seam, crates/dft-solvers/src/lib.rs:83-102, and its variants
+ * :176-207, real_davidson.rs:1130-1170):
+ *   BG_PRECOND_SMOOTH      r / d(h_g, lambda_j), the reference Davidson's smooth
+ *                          denominator (ref_davidson.rs:418-422); diagonal = H diagonal
+ *   BG_PRECOND_TPA         -r tpa(t_g, s_j) with s_j = max(0.1, sum |X_gj|^2 t_g /
+ *                          sum |X_gj|^2) (lib.rs:176-206); diagonal = kinetic t_g
+ *   BG_PRECOND_RITZ_SHIFT  -r / max(h_g - lambda_j, 0.1); diagonal = H diagonal */
+#define BG_PRECOND_SMOOTH 0
+#define BG_PRECOND_TPA 1
+#define BG_PRECOND_RITZ_SHIFT 2
 
 typedef struct {
   int32_t iterations;
@@ -295,7 +309,7 @@ int bg_davidson_solve(bg_op* op, const double* start, const double* diagonal,
  * points finish.  Per-k arrays (nk = set size): start[k] rows_k x bands, diagonal[k]
  * rows_k, eigenvalues[k] bands, eigenvectors[k] rows_k x bands, converged[k] bands;
  * start/diagonal/eigenvectors have ptr_kind (eigenvalues and converged are host);
- * stats: nk entries or NULL.  options.reserved[0] bit 0 set: launch the iteration's
+ * stats: nk entries or NULL.  options.flags bit 0 set: launch the iteration's
  * kernels directly instead of replaying the graph (same results).  The Davidson
  * capacity is the smallest over the k points; bands must fit every operator's capacity.
  * Errors name the k point; the solve runs on the set's stream and returns when done. */

@@ -32,6 +32,38 @@ def preconditioner_denominator(h, e):
     return 0.25 * (np.where(x >= 1.0, 2.0 * x, 2.0) + 1.0 / (np.hypot(z, 1.0) + z))
 
 
+def tpa_weight(kinetic, scale):
+    """crates/dft-solvers/src/lib.rs:194-206 (reciprocal form above the scale)."""
+    t = np.asarray(kinetic, dtype=np.float64)
+    x = t / scale
+    with np.errstate(divide="ignore", invalid="ignore", over="ignore"):
+        p_lo = 27.0 + x * (18.0 + x * (12.0 + x * 8.0))
+        lo = p_lo / (p_lo + 16.0 * x ** 4)
+        y = scale / t
+        p_hi = y * (8.0 + y * (12.0 + y * (18.0 + y * 27.0)))
+        hi = p_hi / (p_hi + 16.0)
+    return np.where(x <= 1.0, lo, hi)
+
+
+def kinetic_scale(weights, kinetic):
+    """Weighted mean kinetic energy with the 0.1 Ha floor (lib.rs:176-192)."""
+    w = np.asarray(weights, dtype=np.float64)
+    return max(float(np.sum(w * kinetic) / np.sum(w)), 0.1)
+
+
+def correction(kind, residual, x, diagonal, e):
+    """One band's correction from its residual (the solver's preconditioner seam):
+    'smooth' r / d(h, e) (ref_davidson.rs:418-422), 'tpa' -r tpa(t, s) with s the
+    band's kinetic scale (lib.rs:240-277), 'ritz_shift' -r / max(h - e, 0.1)
+    (lib.rs:300-309)."""
+    d = np.asarray(diagonal)
+    if kind == "tpa":
+        return -residual * tpa_weight(d, kinetic_scale(np.abs(x) ** 2, d))
+    if kind == "ritz_shift":
+        return -residual / np.maximum(d - e, 0.1)
+    return residual / preconditioner_denominator(d, e)
+
+
 @dataclass
 class Options:
     bands: int
@@ -40,6 +72,7 @@ class Options:
     first_step: bool = False
     capacity: int = 0
     max_iterations: int = 20
+    preconditioner: str = "smooth"
 
     def band_threshold(self, band: int) -> float:
         if self.first_step or band < self.occupied:
@@ -134,8 +167,8 @@ def solve(apply, start, diagonal, opts: Options) -> Solution:
         Xs = V[:, :m] @ Cs
         HXs = HV[:, :m] @ Cs
         lam = w[active]
-        d = preconditioner_denominator(np.asarray(diagonal)[:, None], lam[None, :])
-        E = (HXs - Xs * lam[None, :]) / d
+        E = np.stack([correction(opts.preconditioner, HXs[:, j] - Xs[:, j] * lam[j], Xs[:, j], diagonal, lam[j])
+                      for j in range(len(active))], axis=1)
         norms = np.sqrt(np.sum(np.abs(E) ** 2, axis=0))
         if not np.all(np.isfinite(norms)):
             raise ValueError("nonfinite reference correction")

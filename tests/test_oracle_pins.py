@@ -177,3 +177,20 @@ def test_band_thresholds_and_denominator():
         assert abs(2.0 * float(D.preconditioner_denominator(h, e)) - d_ry) < 2e-15
         assert abs(float(D.preconditioner_denominator(h, e)) - float(D.preconditioner_denominator(h + .25, e + .25))) \
             < 2e-15
+
+
+def test_tpa_and_ritz_shift_corrections():
+    """crates/dft-solvers/tests/all/preconditioner_variants.rs:9-37: TPA uses the
+    selected band's kinetic expectation with the 0.1 Ha floor (-1 at t = 0, -65/81 at
+    t = s, finite and negative at t = 1e200); Ritz shift floors h - lambda at 0.1."""
+    d = np.array([0.0, 0.1, 0.2, 1e200])
+    r = np.ones(4)
+    v0 = np.array([0.0, 0.0, 2.0, 0.0])
+    y = D.correction("tpa", r, v0, d, 0.0)
+    assert y[0] == -1.0
+    assert abs(y[2] + 65.0 / 81.0) < 1e-15
+    assert y[3] < 0 and np.isfinite(y[3])
+    y = D.correction("tpa", r, np.array([1.0, 0, 0, 0]), d, 0.0)
+    assert abs(y[1] + 65.0 / 81.0) < 1e-15
+    y = D.correction("ritz_shift", r, v0, d, 0.2)
+    assert np.all(y[:3] == -10.0) and y[3] < 0
