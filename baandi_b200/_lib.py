@@ -100,6 +100,9 @@ SIGNATURES = {
     "bg_fields_set_stream": [_p, _p],
     "bg_fields_volume": [_p, ctypes.POINTER(_dbl)],
     "bg_fields_lda_hartree": [_p, _p, _p, _p, _p, _i32],
+    "bg_fields_set_sphere": [_p, _i64, _p],
+    "bg_fields_sphere_forward": [_p, _p, _p, _i32],
+    "bg_fields_sphere_inverse": [_p, _p, _p, _i32],
     "bg_mixer_create": [_p, ctypes.POINTER(MixerProfile), _i64, _p, _p, _dbl, _dbl, _dbl, _pp],
     "bg_mixer_destroy": [_p],
     "bg_mixer_set_stream": [_p, _p],
@@ -127,6 +130,7 @@ SIGNATURES = {
     "bg_setup_projector_count": [_i32, ctypes.POINTER(SpeciesDesc), ctypes.POINTER(_i32), ctypes.POINTER(_i32)],
     "bg_setup_projectors": [_dbl, _i64, _p, _p, _i32, ctypes.POINTER(SpeciesDesc), _p, _p, _p],
     "bg_setup_local_form_factor": [ctypes.POINTER(SpeciesDesc), _dbl, _i64, _p, _p],
+    "bg_setup_ewald": [_p, _i32, _p, _p, ctypes.POINTER(_dbl)],
 }
 
 _lib = None

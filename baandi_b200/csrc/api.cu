@@ -1142,6 +1142,18 @@ int bg_setup_projectors(double volume, int64_t npw, const double* kpg, const dou
   return BG_OK;
 }
 
+int bg_setup_ewald(const double rows[9], int32_t natoms, const double* positions, const double* charges,
+                   double* energy) {
+  if (!rows || !positions || !charges || !energy || natoms < 1) return fail(nullptr, BG_EINVAL, "argument");
+  Cell c;
+  if (cell_init(rows, &c) != BG_OK) return fail(nullptr, BG_EINVAL, "lattice rows are singular or not finite");
+  for (int i = 0; i < 3 * natoms; ++i)
+    if (!std::isfinite(positions[i])) return fail(nullptr, BG_ENONFINITE, "ion position not finite");
+  const int rc = ewald_energy(c, natoms, positions, charges, energy);
+  if (rc) return fail(nullptr, rc, "Ewald energy");
+  return BG_OK;
+}
+
 int bg_setup_local_form_factor(const bg_species* species, double volume, int64_t n, const double* g, double* out) {
   if (!species || !g || !out || !(volume > 0.0)) return fail(nullptr, BG_EINVAL, "argument");
   auto sp = to_species(1, species);

@@ -219,6 +219,41 @@ __global__ void k_f_energies(const double* __restrict__ part, int blocks, double
   out[2] = dv * s[2];
 }
 
+// Density sphere transforms of the mixer (crates/dft-engine/src/refscf/density.rs:
+// 173-237): forward picks FFT(rho)/N on the half-sphere indices; inverse forms
+// 2 Re(sum_half c_G e^{iGr}) - Re c_0 from the half-sphere coefficients alone.
+__global__ void k_f_load_real(const double* __restrict__ rho, int64_t total, double2* __restrict__ work) {
+  for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < total; p += (int64_t)gridDim.x * blockDim.x)
+    work[p] = make_double2(rho[p], 0.0);
+}
+__global__ void k_f_zero(double2* __restrict__ work, int64_t total) {
+  for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < total; p += (int64_t)gridDim.x * blockDim.x)
+    work[p] = make_double2(0.0, 0.0);
+}
+__global__ void k_f_pick(const double2* __restrict__ work, const int64_t* __restrict__ idx, int64_t n, double inv_n,
+                         double2* __restrict__ out) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const double2 z = work[idx[i]];
+    out[i] = make_double2(z.x * inv_n, z.y * inv_n);
+  }
+}
+__global__ void k_f_place(const double2* __restrict__ c, const int64_t* __restrict__ idx, int64_t n,
+                          double2* __restrict__ work, int* err) {
+  bool bad = false;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const double2 z = c[i];
+    bad |= !(isfinite(z.x) && isfinite(z.y));
+    work[idx[i]] = z;
+  }
+  if (bad) atomicOr(err, 1);
+}
+__global__ void k_f_half_real(const double2* __restrict__ work, const double2* __restrict__ c, int64_t i0,
+                              int64_t total, double* __restrict__ rho) {
+  const double g0 = i0 >= 0 ? c[i0].x : 0.0;
+  for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < total; p += (int64_t)gridDim.x * blockDim.x)
+    rho[p] = 2.0 * work[p].x - g0;
+}
+
 }  // namespace
 }  // namespace bg
 
@@ -244,6 +279,11 @@ struct bg_fields {
   cudaStream_t stream = nullptr;
   bool own_stream = false;
   std::vector<std::unique_ptr<DevBuf>> bufs;
+  // density half-sphere of the mixer
+  int64_t nsphere = 0;
+  int64_t sphere_g0 = -1;   // position of G = 0 in the sphere list
+  int64_t* sphere = nullptr;
+  double2* stage_c = nullptr;
 };
 
 namespace {
@@ -411,6 +451,129 @@ int bg_fields_lda_hartree(bg_fields* f, const double* density, double* v_hxc, do
     if ((e = cudaStreamSynchronize(f->stream)) != cudaSuccess) return cuda_fail(ctx, e, "copy out");
   }
   for (int i = 0; i < 3; ++i) energies[i] = f->energies_host[i];
+  return BG_OK;
+}
+
+int bg_fields_set_sphere(bg_fields* f, int64_t n, const int64_t* flat_index) {
+  if (!f || !flat_index || n < 1) return fail(f ? f->ctx : nullptr, BG_EINVAL, "argument");
+  if (f->sphere) return fail(f->ctx, BG_EINVAL, "the density sphere is already set");
+  int64_t g0 = -1;
+  for (int64_t i = 0; i < n; ++i) {
+    if (flat_index[i] < 0 || flat_index[i] >= f->box.total) return fail(f->ctx, BG_ESHAPE, "sphere index outside the box");
+    if (flat_index[i] == 0) g0 = i;
+  }
+  cudaError_t e = cudaSetDevice(f->ctx->device);
+  if (e != cudaSuccess) return cuda_fail(f->ctx, e, "cudaSetDevice");
+  void* vp;
+  int rc;
+  if ((rc = falloc(f, sizeof(int64_t) * n, &vp))) return rc;
+  f->sphere = static_cast<int64_t*>(vp);
+  if ((rc = falloc(f, sizeof(double2) * n, &vp))) return rc;
+  f->stage_c = static_cast<double2*>(vp);
+  if ((e = cudaMemcpy(f->sphere, flat_index, sizeof(int64_t) * n, cudaMemcpyHostToDevice)) != cudaSuccess)
+    return cuda_fail(f->ctx, e, "upload");
+  f->nsphere = n;
+  f->sphere_g0 = g0;
+  return BG_OK;
+}
+
+static void f_transform(bg_fields* f, int sign) {
+  const Box3 b = f->box;
+  for (int i = 0; i < 3; ++i) {
+    const int a = sign < 0 ? 2 - i : i;
+    const int blocks = (int)((b.total / b.n[a] + kLines - 1) / kLines);
+    if (sign < 0)
+      k_f_lines<-1><<<blocks, kFieldThreads, lines_smem(b.n[a]), f->stream>>>(f->work, b, a, f->plan[a], f->tw[a]);
+    else
+      k_f_lines<1><<<blocks, kFieldThreads, lines_smem(b.n[a]), f->stream>>>(f->work, b, a, f->plan[a], f->tw[a]);
+  }
+}
+
+int bg_fields_sphere_forward(bg_fields* f, const double* density, double* coeffs, int32_t ptr_kind) {
+  if (!f || !density || !coeffs) return fail(f ? f->ctx : nullptr, BG_EINVAL, "null argument");
+  bg_ctx* ctx = f->ctx;
+  if (!f->sphere) return fail(ctx, BG_EINVAL, "set the density sphere first");
+  if (ptr_kind != BG_PTR_HOST && ptr_kind != BG_PTR_DEVICE) return fail(ctx, BG_EINVAL, "pointer kind");
+  cudaError_t e = cudaSetDevice(ctx->device);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaSetDevice");
+  const int64_t total = f->box.total;
+  const double* rho = density;
+  double2* out = reinterpret_cast<double2*>(coeffs);
+  void* vp;
+  int rc;
+  if (ptr_kind == BG_PTR_HOST) {
+    if (!f->stage_in) {
+      if ((rc = falloc(f, sizeof(double) * total, &vp))) return rc;
+      f->stage_in = static_cast<double*>(vp);
+      if ((rc = falloc(f, sizeof(double) * total, &vp))) return rc;
+      f->stage_out = static_cast<double*>(vp);
+      if ((rc = falloc(f, sizeof(double) * total, &vp))) return rc;
+      f->stage_vh = static_cast<double*>(vp);
+    }
+    if ((e = cudaMemcpyAsync(f->stage_in, density, sizeof(double) * total, cudaMemcpyHostToDevice, f->stream)) !=
+        cudaSuccess)
+      return cuda_fail(ctx, e, "copy in");
+    rho = f->stage_in;
+    out = f->stage_c;
+  }
+  const unsigned g = (unsigned)std::min<int64_t>((total + 255) / 256, kFieldBlocks);
+  k_f_load_real<<<g, 256, 0, f->stream>>>(rho, total, f->work);
+  f_transform(f, -1);
+  const unsigned gs = (unsigned)std::min<int64_t>((f->nsphere + 255) / 256, kFieldBlocks);
+  k_f_pick<<<gs, 256, 0, f->stream>>>(f->work, f->sphere, f->nsphere, 1.0 / (double)total, out);
+  if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(ctx, e, "kernel launch");
+  if (ptr_kind == BG_PTR_HOST &&
+      (e = cudaMemcpyAsync(coeffs, out, sizeof(double2) * f->nsphere, cudaMemcpyDeviceToHost, f->stream)) != cudaSuccess)
+    return cuda_fail(ctx, e, "copy out");
+  if ((e = cudaStreamSynchronize(f->stream)) != cudaSuccess) return cuda_fail(ctx, e, "sphere forward");
+  return BG_OK;
+}
+
+int bg_fields_sphere_inverse(bg_fields* f, const double* coeffs, double* density, int32_t ptr_kind) {
+  if (!f || !density || !coeffs) return fail(f ? f->ctx : nullptr, BG_EINVAL, "null argument");
+  bg_ctx* ctx = f->ctx;
+  if (!f->sphere) return fail(ctx, BG_EINVAL, "set the density sphere first");
+  if (ptr_kind != BG_PTR_HOST && ptr_kind != BG_PTR_DEVICE) return fail(ctx, BG_EINVAL, "pointer kind");
+  cudaError_t e = cudaSetDevice(ctx->device);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaSetDevice");
+  const int64_t total = f->box.total;
+  const double2* c = reinterpret_cast<const double2*>(coeffs);
+  double* rho = density;
+  void* vp;
+  int rc;
+  if (ptr_kind == BG_PTR_HOST) {
+    if (!f->stage_in) {
+      if ((rc = falloc(f, sizeof(double) * total, &vp))) return rc;
+      f->stage_in = static_cast<double*>(vp);
+      if ((rc = falloc(f, sizeof(double) * total, &vp))) return rc;
+      f->stage_out = static_cast<double*>(vp);
+      if ((rc = falloc(f, sizeof(double) * total, &vp))) return rc;
+      f->stage_vh = static_cast<double*>(vp);
+    }
+    if ((e = cudaMemcpyAsync(f->stage_c, coeffs, sizeof(double2) * f->nsphere, cudaMemcpyHostToDevice, f->stream)) !=
+        cudaSuccess)
+      return cuda_fail(ctx, e, "copy in");
+    c = f->stage_c;
+    rho = f->stage_out;
+  }
+  const unsigned g = (unsigned)std::min<int64_t>((total + 255) / 256, kFieldBlocks);
+  const unsigned gs = (unsigned)std::min<int64_t>((f->nsphere + 255) / 256, kFieldBlocks);
+  k_f_zero<<<g, 256, 0, f->stream>>>(f->work, total);
+  k_f_place<<<gs, 256, 0, f->stream>>>(c, f->sphere, f->nsphere, f->work, f->err);
+  f_transform(f, 1);
+  k_f_half_real<<<g, 256, 0, f->stream>>>(f->work, c, f->sphere_g0, total, rho);
+  if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(ctx, e, "kernel launch");
+  if (ptr_kind == BG_PTR_HOST &&
+      (e = cudaMemcpyAsync(density, rho, sizeof(double) * total, cudaMemcpyDeviceToHost, f->stream)) != cudaSuccess)
+    return cuda_fail(ctx, e, "copy out");
+  if ((e = cudaMemcpyAsync(f->err_host, f->err, sizeof(int), cudaMemcpyDeviceToHost, f->stream)) != cudaSuccess ||
+      (e = cudaStreamSynchronize(f->stream)) != cudaSuccess)
+    return cuda_fail(ctx, e, "sphere inverse");
+  if (f->err_host[0]) {
+    cudaMemsetAsync(f->err, 0, sizeof(int), f->stream);
+    cudaStreamSynchronize(f->stream);
+    return fail(ctx, BG_ENONFINITE, "non-finite density coefficient");
+  }
   return BG_OK;
 }
 

@@ -96,28 +96,45 @@ def solve_kset(kset, starts, diagonals, options: Options, graph: bool = True):
     (bg_kset_davidson_solve): each large product is one launch over all k points, the
     reduced problems and control decisions run on the GPU, and an iteration is one
     replayed CUDA graph (graph=False launches the same kernels one by one).  starts /
-    diagonals: one (rows_k x bands) block and one rows_k diagonal per k point (host).
-    Returns one Solution per k point."""
+    diagonals: one (rows_k x bands) block and one rows_k diagonal per k point, numpy
+    (host) or CUDA tensors (device; blocks shaped (bands, rows_k) row-major, the layout
+    of apply_block).  Returns one Solution per k point, eigenvectors on the same side."""
     lib = L.load()
     real = kset.ops[0].is_real()
-    dt = np.float64 if real else np.complex128
     nk = len(kset.ops)
     if len(starts) != nk or len(diagonals) != nk:
         raise SolverError(L.BG_ESHAPE, "one start block and one diagonal per k point")
-    x0 = [np.asfortranarray(x, dtype=dt) for x in starts]
-    dg = [np.ascontiguousarray(d, dtype=np.float64) for d in diagonals]
     n = options.bands
-    for op, x, d in zip(kset.ops, x0, dg):
-        if x.shape != (op.global_len(), n) or d.shape != (op.global_len(),):
-            raise SolverError(L.BG_ESHAPE, "start must be rows x bands, diagonal rows")
+    device = not isinstance(starts[0], np.ndarray)
+    if device:
+        import torch
+        want = torch.float64 if real else torch.complex128
+        x0, dg = list(starts), list(diagonals)
+        for op, x, d in zip(kset.ops, x0, dg):
+            if (x.dtype != want or not x.is_cuda or not x.is_contiguous() or tuple(x.shape) != (n, op.global_len())
+                    or d.dtype != torch.float64 or not d.is_cuda or d.numel() != op.global_len()):
+                raise SolverError(L.BG_ESHAPE, "device starts are contiguous (bands, rows) CUDA tensors")
+        vecs = [torch.empty_like(x) for x in x0]
+        ptr = lambda a: a.data_ptr()
+        kind = L.BG_PTR_DEVICE
+    else:
+        dt = np.float64 if real else np.complex128
+        x0 = [np.asfortranarray(x, dtype=dt) for x in starts]
+        dg = [np.ascontiguousarray(d, dtype=np.float64) for d in diagonals]
+        for op, x, d in zip(kset.ops, x0, dg):
+            if x.shape != (op.global_len(), n) or d.shape != (op.global_len(),):
+                raise SolverError(L.BG_ESHAPE, "start must be rows x bands, diagonal rows")
+        vecs = [np.zeros((op.global_len(), n), dtype=dt, order="F") for op in kset.ops]
+        ptr = lambda a: a.ctypes.data
+        kind = L.BG_PTR_HOST
     vals = [np.zeros(n) for _ in range(nk)]
-    vecs = [np.zeros((op.global_len(), n), dtype=dt, order="F") for op in kset.ops]
     conv = [np.zeros(n, np.int32) for _ in range(nk)]
     stats = (L.DavidsonStats * nk)()
     o = _options(options, 0 if graph else 1)
-    arr = lambda lst: (ctypes.c_void_p * nk)(*[a.ctypes.data for a in lst])
-    rc = lib.bg_kset_davidson_solve(kset.handle, arr(x0), arr(dg), ctypes.byref(o), L.BG_PTR_HOST, arr(vals),
-                                    arr(vecs), arr(conv), stats)
+    arr = lambda lst, f: (ctypes.c_void_p * nk)(*[f(a) for a in lst])
+    host = lambda a: a.ctypes.data
+    rc = lib.bg_kset_davidson_solve(kset.handle, arr(x0, ptr), arr(dg, ptr), ctypes.byref(o), kind, arr(vals, host),
+                                    arr(vecs, ptr), arr(conv, host), stats)
     kset._check(rc)
     return [Solution(vals[k], vecs[k], conv[k].astype(bool), stats[k].iterations, stats[k].reduced_solves,
                      stats[k].h_calls, stats[k].h_columns, stats[k].repairs, stats[k].contractions, stats[k].dropped)

@@ -79,6 +79,38 @@ class FieldGrid:
                                                     e.ctypes.data_as(ctypes.c_void_p), kind))
         return Fields(hxc, vh, float(e[0]), float(e[1]), float(e[2]))
 
+    # -- the mixer's coefficient space (density half-sphere)
+    def set_sphere(self, flat_index):
+        idx = np.ascontiguousarray(flat_index, dtype=np.int64)
+        self._check(self._lib.bg_fields_set_sphere(self.handle, idx.size, idx.ctypes.data_as(ctypes.c_void_p)))
+        self.nsphere = idx.size
+
+    def sphere_forward(self, density, out=None):
+        """FFT(density)/N on the half sphere (complex coefficients)."""
+        if isinstance(density, np.ndarray):
+            rho = np.ascontiguousarray(density, dtype=np.float64)
+            out = np.empty(self.nsphere, np.complex128) if out is None else out
+            kind, pr, po = L.BG_PTR_HOST, rho.ctypes.data, out.ctypes.data
+        else:
+            import torch
+            out = torch.empty(self.nsphere, dtype=torch.complex128, device=density.device) if out is None else out
+            kind, pr, po = L.BG_PTR_DEVICE, density.data_ptr(), out.data_ptr()
+        self._check(self._lib.bg_fields_sphere_forward(self.handle, ctypes.c_void_p(pr), ctypes.c_void_p(po), kind))
+        return out
+
+    def sphere_inverse(self, coeffs, out=None):
+        """2 Re(sum_half c e^{iGr}) - Re c_0 on the grid."""
+        if isinstance(coeffs, np.ndarray):
+            c = np.ascontiguousarray(coeffs, dtype=np.complex128)
+            out = np.empty(self.dims) if out is None else out
+            kind, pc, po = L.BG_PTR_HOST, c.ctypes.data, out.ctypes.data
+        else:
+            import torch
+            out = torch.empty(self.dims, dtype=torch.float64, device=coeffs.device) if out is None else out
+            kind, pc, po = L.BG_PTR_DEVICE, coeffs.data_ptr(), out.data_ptr()
+        self._check(self._lib.bg_fields_sphere_inverse(self.handle, ctypes.c_void_p(pc), ctypes.c_void_p(po), kind))
+        return out
+
     def close(self):
         if getattr(self, "handle", None):
             self._lib.bg_fields_destroy(self.handle)

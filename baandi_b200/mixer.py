@@ -85,6 +85,9 @@ class Broyden:
         return out, Diagnostics(d.iteration, d.occupancy, None if d.inserted_slot < 0 else d.inserted_slot,
                                 d.gamma_l2, d.gamma_max, d.condition if d.occupancy > 0 else None)
 
+    def set_stream(self, stream_ptr: int):
+        self._check(self._lib.bg_mixer_set_stream(self.handle, ctypes.c_void_p(stream_ptr)))
+
     def gamma(self) -> np.ndarray:
         g = np.zeros(25)
         c = ctypes.c_int32()

@@ -163,6 +163,16 @@ def projectors(vol: float, pw: PlaneWaves, species) -> NonlocalTable:
     return NonlocalTable(table.T, channels[:na], couplings[:nd])
 
 
+def ewald(rows, species) -> float:
+    """Ion-ion Ewald energy (Ha) of the species' ions with charge Z_valence."""
+    pos = np.ascontiguousarray(np.concatenate([np.atleast_2d(s.positions) for s in species]), dtype=np.float64)
+    z = np.ascontiguousarray(np.concatenate([np.full(np.atleast_2d(s.positions).shape[0], s.pseudo.z)
+                                             for s in species]), dtype=np.float64)
+    out = ctypes.c_double()
+    L.check(L.load().bg_setup_ewald(_ptr(_rows(rows)), len(z), _ptr(pos), _ptr(z), ctypes.byref(out)))
+    return out.value
+
+
 def local_form_factor(species: Species, vol: float, g: np.ndarray) -> np.ndarray:
     g = np.ascontiguousarray(np.asarray(g, dtype=np.float64).reshape(-1))
     out = np.zeros_like(g)

@@ -1,0 +1,221 @@
+"""SCF driver over the GPU steps: the reference's map and outer loop restated on the
+host, with every grid, block and coefficient vector resident on the device.
+
+Reference (paths inside the reference project):
+  outer loop         crates/dft-engine/src/refscf/driver.rs:479, 589-660 (ethr schedule,
+                     first-map redo), 838-870 (Broyden mix, density inverse)
+  map                crates/dft-engine/src/refscf/map.rs:200-384 (V = V_ion + V_Hxc, v0,
+                     diagonal_static + v0, Davidson with threshold ethr/2 and the
+                     occupied count N_e/2, band density) and :413-467 (Harris-Foulkes
+                     energy: band sum - E_H + E_xc - int rho v_xc + E_ewald)
+  k points           crates/dft-engine/src/refscf/k_map.rs:136-210 (one Davidson per k,
+                     density summed with the k weights); here all k points of the cell
+                     run in one device-driven batched Davidson
+  mixed space        crates/dft-engine/src/refscf/density.rs:27-237 (half of the density
+                     sphere; G = 0 fixed at N_e / Omega, driver.rs:1303-1309)
+  ethr               crates/dft-engine/src/refscf/profile.rs:49-51
+One map per iteration: fields of the input density, potential install, Davidson over all
+k points (device), band density (device), sphere transform and residual F = y - x
+(device), metric norm dr2 (Ry), Broyden update and inverse transform (device).  The
+host reads scalars only (eigenvalues for the band sum and occupations, energies, dr2).
+Occupations are fixed (2 per occupied band, insulators) or Fermi-Dirac
+(occupations.py; crates/dft-physics/src/occupations.rs), whose entropy term gives the
+free energy E - TS; the Davidson's occupied count is ceil(N_e / 2).  The start density
+is uniform (the reference's fallback when the species carry no atomic charge,
+refstart.rs:725-735).
+"""
+from __future__ import annotations
+
+import math
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _lib as L
+from . import davidson as DV
+from . import operands as O
+from .fields import FieldGrid
+from .hamiltonian import ComplexHamiltonian, Context, KPointSet, RealGammaHamiltonian, SolverError, default_context
+from .mixer import Broyden, Profile
+from .occupations import fermi_dirac
+
+
+def next_ethr_ry(previous: float, dr2_ry: float, electrons: float) -> float:
+    """crates/dft-engine/src/refscf/profile.rs:49-51."""
+    return max(min(previous, 0.1 * dr2_ry / max(electrons, 1.0)), 1e-13)
+
+
+def half(m) -> bool:
+    """crates/dft-engine/src/refscf/density.rs:14-16."""
+    return m[0] > 0 or (m[0] == 0 and (m[1] > 0 or (m[1] == 0 and m[2] >= 0)))
+
+
+@dataclass
+class ScfOptions:
+    threshold_ha: float = 5e-9        # standard class: threshold_ry = 2 threshold_ha (profile.rs:39-47)
+    max_iterations: int = 60
+    beta: float = 0.7
+    history: int = 8
+    davidson_max_iterations: int = 20
+    preconditioner: str = "smooth"
+    graph: bool = True
+    smearing_ha: float | None = None  # Fermi-Dirac width; None: fixed occupations (insulators)
+
+
+@dataclass
+class MapRecord:
+    iteration: int
+    kind: str                 # "ordinary" or "retry" (the first-map redo)
+    dr2_ry: float
+    energy_ha: float
+    entropy_term_ha: float
+    ethr_ry: float
+    h_columns: int
+    davidson_iterations: int
+    seconds: float
+
+
+@dataclass
+class ScfResult:
+    energy_ha: float          # Harris-Foulkes energy of the last map
+    converged: bool
+    iterations: int
+    free_energy_ha: float = float("nan")   # energy - TS (smearing)
+    records: list = field(default_factory=list)
+    eigenvalues: list = field(default_factory=list)
+    seconds: float = 0.0
+    ewald_ha: float = 0.0
+
+
+class GpuScf:
+    """SCF of one workload (systems.Workload) on cuda:ctx.device."""
+
+    def __init__(self, workload, ctx: Context | None = None, options: ScfOptions | None = None):
+        import torch
+        self.torch = torch
+        self.w = w = workload
+        self.ctx = ctx or default_context()
+        self.o = options or ScfOptions()
+        self.stream = torch.cuda.Stream()
+        dev = torch.device("cuda", self.ctx.device)
+        self.dev = dev
+        dims = w.dims()
+        self.dims = dims
+        self.volume = w.volume
+        self.electrons = float(sum(s.pseudo.z * np.atleast_2d(s.positions).shape[0] for s in w.species))
+        nocc = self.electrons / 2.0
+        if self.o.smearing_ha is None and (abs(nocc - round(nocc)) > 1e-12 or round(nocc) > w.bands):
+            raise SolverError(L.BG_EINVAL, "fixed occupations need an even electron count within the bands")
+        self.nocc = int(math.ceil(nocc - 1e-12))
+        self.occupations = np.array([2.0 if b < self.nocc else 0.0 for b in range(w.bands)])
+        cap = 2 * w.bands
+        self.ops, self.weights, self.diag_static, self.starts = [], [], [], []
+        for i, (k, wk) in enumerate(w.kpoints):
+            pw = w.plane_waves(k)
+            gamma = w.gamma_real and pw.gamma
+            cls = RealGammaHamiltonian if gamma else ComplexHamiltonian
+            op = cls.new_owned(pw, dims, w.nonlocal_table(pw), cap, self.ctx)
+            self.ops.append(op)
+            self.weights.append(wk)
+            d = op.kinetic_diagonal() if self.o.preconditioner == "tpa" else op.diagonal_static()
+            self.diag_static.append(torch.from_numpy(np.ascontiguousarray(d)).to(dev))
+            x0 = w.random_block(pw.npw, w.bands, seed_offset=100 + i, real=gamma)
+            self.starts.append(torch.from_numpy(np.ascontiguousarray(x0.T)).to(dev))
+        self.gamma = self.ops[0].is_real()
+        self.kset = KPointSet(self.ops, self.ctx)
+        self.v_ion = torch.from_numpy(np.ascontiguousarray(w.ionic_potential())).to(dev)
+        self.ewald = O.ewald(w.rows, w.species)
+        # mixed space: half of the density sphere (4 Ecut)
+        dens = O.plane_waves(w.rows, 4.0 * w.ecut_ha)
+        keep = np.array([half(m) for m in dens.miller.tolist()])
+        miller = dens.miller[keep].astype(np.int64)
+        flat = O.fft_index(miller, dims, False).astype(np.int64)
+        self.g0 = int(np.nonzero(flat == 0)[0][0])
+        self.fields = FieldGrid(w.rows, dims, self.ctx)
+        self.fields.set_sphere(flat)
+        g2 = np.ascontiguousarray(dens.kpg2[keep])
+        self.mixer = Broyden(g2, np.ones(g2.size, bool), self.volume, self.electrons, self.volume,
+                             Profile(beta=self.o.beta, history=self.o.history), self.ctx)
+        s = self.stream.cuda_stream
+        for op in self.ops:
+            op.set_stream(s)
+        self.kset.set_stream(s)
+        self.fields.set_stream(s)
+        self.mixer.set_stream(s)
+        self.epoch = 0
+        torch.cuda.synchronize()
+
+    # -- one map (crates/dft-engine/src/refscf/map.rs:200-384)
+    def _map(self, n, x, ethr, first_step):
+        torch = self.torch
+        f = self.fields.lda_hartree(n)
+        v = self.v_ion + f.hxc
+        v0 = float(v.mean())
+        self.epoch += 1
+        for op in self.ops:
+            op.set_owned_potential_device(v, self.epoch)
+        diags = [d + v0 for d in self.diag_static] if self.o.preconditioner != "tpa" else self.diag_static
+        opts = DV.Options(self.w.bands, ethr / 2.0, self.nocc, first_step=first_step,
+                          max_iterations=self.o.davidson_max_iterations, preconditioner=self.o.preconditioner)
+        sols = DV.solve_kset(self.kset, self.starts, diags, opts, graph=self.o.graph)
+        ts = 0.0
+        if self.o.smearing_ha is None:
+            occ = [self.occupations] * len(sols)
+        else:
+            occ, _, ts = fermi_dirac([s.eigenvalues for s in sols], self.weights, self.electrons, self.o.smearing_ha)
+        rho = torch.zeros(self.dims, dtype=torch.float64, device=self.dev)
+        band_sum = 0.0
+        for k, (op, sol) in enumerate(zip(self.ops, sols)):
+            wk = self.weights[k] * occ[k]
+            op.band_density_sum(sol.eigenvectors, wk, self.volume, out=rho, accumulate=k > 0)
+            band_sum += float(np.dot(wk, sol.eigenvalues))
+        energy = band_sum - f.hartree + f.xc - f.xc_integral + self.ewald
+        y = self.fields.sphere_forward(rho)
+        y[self.g0] = self.electrons / self.volume
+        fres = y - x
+        dr2 = self.mixer.metric(fres, fres)
+        return sols, rho, y, fres, dr2, energy, ts
+
+    def run(self) -> ScfResult:
+        torch = self.torch
+        o = self.o
+        threshold_ry = 2.0 * o.threshold_ha
+        t0 = time.perf_counter()
+        with torch.cuda.stream(self.stream):
+            n = torch.full(self.dims, self.electrons / self.volume, dtype=torch.float64, device=self.dev)
+            x = self.fields.sphere_forward(n)
+            x[self.g0] = self.electrons / self.volume
+            ethr, last_dr2 = 1e-2, float("inf")
+            records, result = [], ScfResult(float("nan"), False, 0, ewald_ha=self.ewald)
+            for it in range(1, o.max_iterations + 1):
+                if it > 1:
+                    ethr = next_ethr_ry(1e-2 if it == 2 else ethr, last_dr2, self.electrons)
+                redo = False
+                while True:
+                    tm = time.perf_counter()
+                    sols, rho, y, fres, dr2, energy, ts = self._map(n, x, ethr, it == 1 and not redo)
+                    records.append(MapRecord(it, "retry" if redo else "ordinary", dr2, energy, ts, ethr,
+                                             sum(s.h_columns for s in sols), max(s.iterations for s in sols),
+                                             time.perf_counter() - tm))
+                    self.starts = [s.eigenvectors for s in sols]
+                    if it == 1 and not redo and dr2 < ethr * max(self.electrons, 1.0):
+                        ethr = next_ethr_ry(ethr, dr2, self.electrons)
+                        redo = True
+                        continue
+                    break
+                last_dr2 = dr2
+                result.energy_ha = energy
+                result.free_energy_ha = energy - ts
+                result.iterations = it
+                result.eigenvalues = [s.eigenvalues for s in sols]
+                if dr2 < threshold_ry:
+                    result.converged = True
+                    break
+                nxt, _ = self.mixer.update(x, fres)
+                n = self.fields.sphere_inverse(nxt)
+                x = nxt
+            torch.cuda.synchronize()
+        result.records = records
+        result.seconds = time.perf_counter() - t0
+        return result

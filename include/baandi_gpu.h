@@ -187,6 +187,14 @@ int bg_fields_volume(const bg_fields* f, double* volume);
  * are on the host.  A non-finite density value returns BG_ENONFINITE. */
 int bg_fields_lda_hartree(bg_fields* f, const double* density, double* v_hxc, double* v_h,
                           double energies[3], int32_t ptr_kind);
+/* The mixer's coefficient space (crates/dft-engine/src/refscf/density.rs:27-237): the
+ * half sphere of the density basis, given once as n flat C-order grid indices (host).
+ * sphere_forward: coeffs[i] = FFT(density)/N at index i (complex, interleaved);
+ * sphere_inverse: density = 2 Re(sum_i c_i e^{iG_i r}) - Re c_0 (the inverse of the
+ * positive half alone).  Both synchronous; arrays have ptr_kind. */
+int bg_fields_set_sphere(bg_fields* f, int64_t n, const int64_t* flat_index);
+int bg_fields_sphere_forward(bg_fields* f, const double* density, double* coeffs, int32_t ptr_kind);
+int bg_fields_sphere_inverse(bg_fields* f, const double* coeffs, double* density, int32_t ptr_kind);
 
 /* ------------------------------------------------------------ density mixing */
 /* The reference mixer (crates/dft-engine/src/refscf/broyden.rs, metric.rs) on the GPU:
@@ -377,6 +385,11 @@ int bg_setup_projector_count(int32_t nspecies, const bg_species* species, int32_
 int bg_setup_projectors(double volume, int64_t npw, const double* kpg, const double* kpg2,
                         int32_t nspecies, const bg_species* species, double* table,
                         int32_t* channels, double* couplings);
+/* Ewald ion-ion energy (Ha) of natoms point charges (Cartesian Bohr positions, 3 per
+ * ion) in a neutralising background, eta = sqrt(pi) / Omega^(1/3) (the reference's
+ * default scheme, crates/dft-physics/src/ewald.rs:376-447). */
+int bg_setup_ewald(const double rows[9], int32_t natoms, const double* positions, const double* charges,
+                   double* energy);
 /* V_loc(|G|) (Ha) of one species at n wave numbers (crates/dft-upf/src/radial.rs:246-305). */
 int bg_setup_local_form_factor(const bg_species* species, double volume, int64_t n,
                                const double* g, double* out);
