@@ -924,6 +924,7 @@ int bg_kset_destroy(bg_kset* ks) {
     if (ks->in_done[i]) cudaEventDestroy(ks->in_done[i]);
     if (ks->work_done[i]) cudaEventDestroy(ks->work_done[i]);
   }
+  if (ks->dv_cache && ks->dv_free) ks->dv_free(ks->dv_cache);
   cudaFree(ks->d_tabs);
   cudaFree(ks->d_nl);
   delete ks;

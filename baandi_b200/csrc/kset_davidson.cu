@@ -23,6 +23,7 @@
 #include <complex>
 #include <memory>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "blas_dev.cuh"
@@ -37,6 +38,7 @@ constexpr double kPivotRatioMin = kEps / 1e-12;   // crates/dft-solvers/src/lean
 constexpr double kDependence = 1e-12;             // crates/dft-numerics/src/linalg.rs:12
 constexpr int kCtlThreads = 256;
 constexpr int kQlMaxIter = 60;
+constexpr int kRotBuffer = 4096;  // QL rotations recorded between applications
 
 // Errors recorded by a k point's control kernel (status = -id).
 enum : int {
@@ -108,8 +110,8 @@ struct Bufs {
   D *hv, *hp, *hq;               // cap: Householder vectors
   int *active, *map, *conv, *order;  // cap
   D* part;                       // split-K partials
-  double* rot;                   // QL rotations of one sweep: 2 * cap
-  int* rot_i;                    // cap
+  double* rot;                   // QL rotations (s, c) recorded between applications
+  int* rot_i;                    // their first column i
   const double* diag;            // rows
   int rows;
 };
@@ -148,6 +150,7 @@ struct Opts {
   int n, cap, occupied, first_step, max_iterations;
   double threshold;
   int preconditioner;
+  int smem_matrices;  // the control kernel keeps A, Y, Q, Z in shared memory
 };
 
 // ------------------------------------------------------------------ block-wide small algebra
@@ -175,18 +178,32 @@ __device__ __forceinline__ D warp_sum(D v) {
 // Extend the lower Cholesky factor L of S (both ld, columns 0..m0-1 of L valid) to
 // columns m0..m-1 with the reference's pivot rule (squared pivot over the overlap
 // diagonal >= eps / 1e-12, crates/dft-solvers/src/lean_davidson.rs:62-70).  The part of
-// the new rows left of m0 is a forward substitution per row (one thread per row, the
-// host's summation order); the new diagonal block is factored by warp 0.
+// the new rows left of m0 is a right-looking forward substitution, parallel over the new
+// rows and columns; the new diagonal block is factored by warp 0.
 template <class D>
 __device__ bool chol_extend(const D* S, int ld, D* L, int m0, int m, int* flag) {
   using X = Cx<D>;
   if (m0 > 0) {
-    for (int j = m0 + (int)threadIdx.x; j < m; j += blockDim.x) {
-      for (int k = 0; k < m0; ++k) {
-        D x = S[j + (size_t)k * ld];
-        for (int p = 0; p < k; ++p) x = X::sub(x, X::mul(L[j + (size_t)p * ld], X::conj(L[k + (size_t)p * ld])));
-        L[j + (size_t)k * ld] = X::div(x, X::real(L[k + (size_t)k * ld]));
+    // right-looking: L[j][k] holds S[j][k] minus the updates of columns p < k until
+    // column k is divided by its pivot; every step is parallel over the new rows
+    const int nr = m - m0;
+    for (int t = threadIdx.x; t < nr * m0; t += blockDim.x) {
+      const int j = m0 + t % nr, k = t / nr;
+      L[j + (size_t)k * ld] = S[j + (size_t)k * ld];
+    }
+    __syncthreads();
+    for (int p = 0; p < m0; ++p) {
+      const double piv = X::real(L[p + (size_t)p * ld]);
+      for (int j = m0 + (int)threadIdx.x; j < m; j += blockDim.x)
+        L[j + (size_t)p * ld] = X::div(L[j + (size_t)p * ld], piv);
+      __syncthreads();
+      const int cols = m0 - p - 1;
+      for (int t = threadIdx.x; t < nr * cols; t += blockDim.x) {
+        const int j = m0 + t % nr, k = p + 1 + t / nr;
+        L[j + (size_t)k * ld] =
+            X::sub(L[j + (size_t)k * ld], X::mul(L[j + (size_t)p * ld], X::conj(L[k + (size_t)p * ld])));
       }
+      __syncthreads();
     }
   }
   __syncthreads();
@@ -383,84 +400,101 @@ __device__ bool heev(D* A, int lda, int m, double* w, D* V, int ldv, const Bufs<
     Z[i + (size_t)j * ldq] = i == j ? 1.0 : 0.0;
   }
   __syncthreads();
-  // implicit QL (the recurrence of the host's tridiagonal_ql)
-  int* s_m = sh;       // sh[0]: m of the sweep, sh[1]: rotations, sh[2]: failed
-  for (int l = 0; l < m; ++l) {
-    int iter = 0;
-    for (;;) {
-      if (threadIdx.x == 0) {
+  // implicit QL (the recurrence of the host's tridiagonal_ql).  Thread 0 runs the
+  // scalar recurrence for as many sweeps as the rotation buffer holds, recording each
+  // rotation (i, s, c); then every thread applies the recorded rotations, in order, to
+  // its rows of Z.  The same rotations in the same order as applying them sweep by
+  // sweep, with one block barrier per buffer instead of two per sweep.
+  const int cap_rot = kRotBuffer + 4 * ldq;
+  int* s_m = sh;  // sh[0]: recorded rotations, sh[1]: finished, sh[2]: failed
+  int ql_l = 0, ql_iter = 0;  // thread 0's position in the recurrence
+  for (;;) {
+    if (threadIdx.x == 0) {
+      int nrec = 0, fail = 0;
+      while (ql_l < m && nrec + m <= cap_rot) {
+        const int l = ql_l;
         int mm;
         for (mm = l; mm < m - 1; ++mm) {
           const double dd = fabs(d[mm]) + fabs(d[mm + 1]);
           if (fabs(e[mm]) <= kEps * dd) break;
         }
-        int nrot = 0;
-        int fail = 0;
-        if (mm != l) {
-          if (iter++ == kQlMaxIter) {
-            fail = 1;
-          } else {
-            double g = (d[l + 1] - d[l]) / (2.0 * e[l]);
-            double r = hypot(g, 1.0);
-            g = d[mm] - d[l] + e[l] / (g + (g >= 0.0 ? r : -r));
-            double sn = 1.0, c = 1.0, pp = 0.0;
-            int i;
-            bool broke = false;
-            for (i = mm - 1; i >= l; --i) {
-              double f = sn * e[i];
-              const double bb = c * e[i];
-              r = hypot(f, g);
-              e[i + 1] = r;
-              if (r == 0.0) {
-                d[i + 1] -= pp;
-                e[mm] = 0.0;
-                broke = true;
-                break;
-              }
-              sn = f / r;
-              c = g / r;
-              g = d[i + 1] - pp;
-              r = (d[i] - g) * sn + 2.0 * c * bb;
-              pp = sn * r;
-              d[i + 1] = g + pp;
-              g = c * r - bb;
-              b.rot[2 * nrot] = sn;
-              b.rot[2 * nrot + 1] = c;
-              b.rot_i[nrot] = i;
-              ++nrot;
-            }
-            if (!broke) {
-              d[l] -= pp;
-              e[l] = g;
-              e[mm] = 0.0;
-            }
+        if (mm == l) {
+          ++ql_l;
+          ql_iter = 0;
+          continue;
+        }
+        if (ql_iter++ == kQlMaxIter) {
+          fail = 1;
+          break;
+        }
+        double g = (d[l + 1] - d[l]) / (2.0 * e[l]);
+        double r = hypot(g, 1.0);
+        g = d[mm] - d[l] + e[l] / (g + (g >= 0.0 ? r : -r));
+        double sn = 1.0, c = 1.0, pp = 0.0;
+        bool broke = false;
+        for (int i = mm - 1; i >= l; --i) {
+          const double f = sn * e[i];
+          const double bb = c * e[i];
+          // r = |(f, g)| and (sn, c) = (f, g) / r with one reciprocal square root: the
+          // operands are bounded by the reduced matrix's norm, far from overflow, and
+          // the recurrence runs on one thread, where every dependent instruction counts
+          const double t2 = f * f + g * g;
+          if (t2 == 0.0) {
+            e[i + 1] = 0.0;
+            d[i + 1] -= pp;
+            e[mm] = 0.0;
+            broke = true;
+            break;
           }
+          const double rinv = rsqrt(t2);
+          r = t2 * rinv;
+          e[i + 1] = r;
+          sn = f * rinv;
+          c = g * rinv;
+          g = d[i + 1] - pp;
+          r = (d[i] - g) * sn + 2.0 * c * bb;
+          pp = sn * r;
+          d[i + 1] = g + pp;
+          g = c * r - bb;
+          b.rot[2 * nrec] = sn;
+          b.rot[2 * nrec + 1] = c;
+          b.rot_i[nrec] = i;
+          ++nrec;
         }
-        s_m[0] = mm;
-        s_m[1] = nrot;
-        s_m[2] = fail;
-        s_m[3] = iter;
-      }
-      __syncthreads();
-      const int mm = s_m[0], nrot = s_m[1], fail = s_m[2];
-      iter = s_m[3];
-      if (fail) {
-        __syncthreads();
-        return false;
-      }
-      for (int row = threadIdx.x; row < m; row += blockDim.x) {
-        for (int t = 0; t < nrot; ++t) {
-          const int i = b.rot_i[t];
-          const double sn = b.rot[2 * t], c = b.rot[2 * t + 1];
-          const double f = Z[row + (size_t)(i + 1) * ldq];
-          const double zi = Z[row + (size_t)i * ldq];
-          Z[row + (size_t)(i + 1) * ldq] = sn * zi + c * f;
-          Z[row + (size_t)i * ldq] = c * zi - sn * f;
+        if (!broke) {
+          d[l] -= pp;
+          e[l] = g;
+          e[mm] = 0.0;
         }
       }
-      __syncthreads();
-      if (mm == l) break;
+      s_m[0] = nrec;
+      s_m[1] = ql_l >= m;
+      s_m[2] = fail;
     }
+    __syncthreads();
+    const int nrec = s_m[0], finished = s_m[1], fail = s_m[2];
+    // apply in order; consecutive rotations (i, i+1), (i-1, i) pass column i's value
+    // in a register
+    for (int row = threadIdx.x; row < m; row += blockDim.x) {
+      int t = 0;
+      while (t < nrec) {
+        int i = b.rot_i[t];
+        double carry = Z[row + (size_t)(i + 1) * ldq];
+        for (;;) {
+          const double sn = b.rot[2 * t], c = b.rot[2 * t + 1];
+          const double zi = Z[row + (size_t)i * ldq];
+          Z[row + (size_t)(i + 1) * ldq] = sn * zi + c * carry;
+          carry = c * zi - sn * carry;
+          ++t;
+          if (t == nrec || b.rot_i[t] != i - 1) break;
+          i = b.rot_i[t];
+        }
+        Z[row + (size_t)i * ldq] = carry;
+      }
+    }
+    __syncthreads();
+    if (fail) return false;
+    if (finished) break;
   }
   // stable ascending order of the eigenvalues (rank of each entry)
   for (int i = threadIdx.x; i < m; i += blockDim.x) {
@@ -590,8 +624,9 @@ __global__ void __launch_bounds__(128) k_dv_dense(const D* const* __restrict__ H
 // solver's preconditioner), norms[j] = |Er[:, j]|^2.
 template <class D>
 __global__ void __launch_bounds__(256) k_dv_corrections(const Bufs<D>* __restrict__ bufs, const Ctl* __restrict__ ctl,
-                                                        int kind) {
+                                                        const Opts* __restrict__ opts) {
   __shared__ double red[256];
+  const int kind = opts->preconditioner;
   const int j = blockIdx.x, k = blockIdx.y;
   const Ctl& c = ctl[k];
   if (c.status != 0 || j >= c.nact) return;
@@ -621,11 +656,38 @@ constexpr int kNnSlots = 2, kTnSlots = 2, kCpSlots = 3;
 
 template <class D>
 __global__ void __launch_bounds__(kCtlThreads, 1) k_dv_ctl(int phase, const Bufs<D>* __restrict__ bufs, Ctl* ctl,
-                                                        NN<D>* nn, TN<D>* tn, CP<D>* cp, DynCols* dyn, Opts o, int nk,
-                                                        int gamma) {
+                                                        NN<D>* nn, TN<D>* tn, CP<D>* cp, DynCols* dyn,
+                                                        const Opts* __restrict__ opts, int nk, int gamma) {
   using X = Cx<D>;
+  const Opts o = *opts;
   const int k = blockIdx.x;
-  const Bufs<D>& b = bufs[k];
+  // The eigensolver's and the repair's short vectors live in shared memory (the scalar
+  // QL recurrence on thread 0 reads and writes them on every rotation).
+  Bufs<D> b = bufs[k];
+  {
+    extern __shared__ __align__(16) unsigned char dv_sm[];
+    const int c = o.cap;
+    D* dp = reinterpret_cast<D*>(dv_sm);
+    b.off = dp;
+    b.ph = dp + c;
+    b.hv = dp + 2 * c;
+    b.hp = dp + 3 * c;
+    b.hq = dp + 4 * c;
+    double* fp = reinterpret_cast<double*>(dp + 5 * c);
+    b.td = fp;
+    b.te = fp + c;
+    int* ip = reinterpret_cast<int*>(fp + 4 * c);
+    b.order = ip + c;
+    if (o.smem_matrices) {
+      // small capacities: the eigensolver's matrices in shared memory as well
+      D* mp = reinterpret_cast<D*>(ip + 2 * c + (2 * c & 2));  // 16-byte aligned
+      const size_t cc = (size_t)c * c;
+      b.A = mp;
+      b.Y = mp + cc;
+      b.Q = mp + 2 * cc;
+      b.Z = reinterpret_cast<double*>(mp + 3 * cc);
+    }
+  }
   const int cap = o.cap, n = o.n;
   const int64_t rows = b.rows;
   __shared__ Ctl c;
@@ -790,14 +852,15 @@ __global__ void __launch_bounds__(kCtlThreads, 1) k_dv_ctl(int phase, const Bufs
       }
       if (threadIdx.x == 0) {
         nn[0 * nk + k] = NN<D>{b.V, b.P, b.E, cap, kk, m, 1};
-        tn[0 * nk + k] = phase == kRepair2 ? TN<D>{b.V, b.E, b.P, cap, m, kk} : TN<D>{b.E, b.E, b.A, cap, kk, kk};
+        // the in-block Gram goes to the global A (another kernel writes it)
+        tn[0 * nk + k] = phase == kRepair2 ? TN<D>{b.V, b.E, b.P, cap, m, kk} : TN<D>{b.E, b.E, bufs[k].A, cap, kk, kk};
       }
       break;
     }
     case kRepair4: {
       if (!c.repair || c.kept == 0) break;
       const int kraw = c.kept;
-      const D* G = b.A;
+      const D* G = bufs[k].A;
       D* Qc = b.P;   // orthonormal combinations, column q of kept j
       D* q = b.hv;
       D* dots = b.hp;
@@ -938,8 +1001,17 @@ template <class T>
 class KsetSolver {
  public:
   using D = typename DevOf<T>::type;
-  KsetSolver(bg_kset* ks, const Opts& o, bool graph) : ks_(ks), nk_((int)ks->ops.size()), o_(o), want_graph_(graph) {
-    s_ = ks->stream;
+  KsetSolver(bg_kset* ks, int n, int cap) : ks_(ks), nk_((int)ks->ops.size()) {
+    o_.n = n;
+    o_.cap = cap;
+    o_.smem_matrices = small(cap) ? 1 : 0;
+  }
+  bool matches(int n, int cap) const { return o_.n == n && o_.cap == cap; }
+  // Per-call options (threshold, occupied, first_step, iterations, preconditioner).
+  void set_options(const Opts& o, bool graph) {
+    o_ = o;
+    o_.smem_matrices = small(o.cap) ? 1 : 0;
+    want_graph_ = graph;
   }
   ~KsetSolver() {
     if (exec_) cudaGraphExecDestroy(exec_);
@@ -956,8 +1028,11 @@ class KsetSolver {
   bg_kset* ks_;
   int nk_;
   Opts o_;
-  bool want_graph_;
-  cudaStream_t s_;
+  bool want_graph_ = true;
+  bool prepared_ = false;
+  bool graph_tried_ = false;
+  Opts* d_opts_ = nullptr;
+  cudaStream_t s_ = nullptr;
   std::vector<void*> dev_;
   std::vector<Bufs<D>> hb_;
   Bufs<D>* d_bufs_ = nullptr;
@@ -995,9 +1070,16 @@ class KsetSolver {
     err_ = std::string(what) + ": " + cudaGetErrorString(e);
     return BG_EDEVICE;
   }
+  static size_t vec_smem(int cap) {
+    return (size_t)cap * (5 * sizeof(D) + 4 * sizeof(double) + 2 * sizeof(int)) + 16;
+  }
+  static size_t mat_smem(int cap) { return (size_t)cap * cap * (3 * sizeof(D) + sizeof(double)); }
+  // A, Y, Q and Z join the vectors in shared memory when all fit in 200 KB.
+  static bool small(int cap) { return vec_smem(cap) + mat_smem(cap) <= 200 * 1024; }
+  size_t ctl_smem() const { return vec_smem(o_.cap) + (o_.smem_matrices ? mat_smem(o_.cap) : 0); }
   int64_t ctl(int phase) {
-    k_dv_ctl<D><<<nk_, kCtlThreads, 0, s_>>>(phase, d_bufs_, d_ctl_, d_nn_, d_tn_, d_cp_, d_dyn_, o_, nk_,
-                                            ks_->gamma);
+    k_dv_ctl<D><<<nk_, kCtlThreads, ctl_smem(), s_>>>(phase, d_bufs_, d_ctl_, d_nn_, d_tn_, d_cp_, d_dyn_, d_opts_,
+                                                     nk_, ks_->gamma);
     return 1;
   }
   int64_t nn(int nslots) {
@@ -1020,7 +1102,7 @@ class KsetSolver {
     return 1;
   }
   int64_t corr() {
-    k_dv_corrections<D><<<dim3((unsigned)o_.n, (unsigned)nk_), 256, 0, s_>>>(d_bufs_, d_ctl_, o_.preconditioner);
+    k_dv_corrections<D><<<dim3((unsigned)o_.n, (unsigned)nk_), 256, 0, s_>>>(d_bufs_, d_ctl_, d_opts_);
     return 1;
   }
   int64_t apply() {
@@ -1045,6 +1127,7 @@ class KsetSolver {
     l += ctl(kFinish);
     return l;
   }
+  int prepare();
   int poll(bool* all_done) {
     int rc = cuda(cudaMemcpyAsync(h_ctl_, d_ctl_, sizeof(Ctl) * nk_, cudaMemcpyDeviceToHost, s_), "poll");
     if (!rc) rc = cuda(cudaStreamSynchronize(s_), "Davidson iteration");
@@ -1062,9 +1145,7 @@ class KsetSolver {
 };
 
 template <class T>
-int KsetSolver<T>::run(const double* const* start, const double* const* diagonal, int32_t ptr_kind,
-                       double* const* values, double* const* vectors, int32_t* const* converged,
-                       bg_davidson_stats* stats) {
+int KsetSolver<T>::prepare() {
   const int n = o_.n, cap = o_.cap;
   int rc;
   hb_.resize(nk_);
@@ -1088,11 +1169,58 @@ int KsetSolver<T>::run(const double* const* start, const double* const* diagonal
         (rc = alloc(&b.off, cap)) || (rc = alloc(&b.ph, cap)) || (rc = alloc(&b.hv, cap)) || (rc = alloc(&b.hp, cap)) ||
         (rc = alloc(&b.hq, cap)) || (rc = alloc(&b.active, cap)) || (rc = alloc(&b.map, cap)) ||
         (rc = alloc(&b.conv, cap)) || (rc = alloc(&b.order, cap)) || (rc = alloc(&b.part, 2 * (size_t)slot_elems_)) ||
-        (rc = alloc(&b.rot, 2 * (size_t)cap)) || (rc = alloc(&b.rot_i, cap)))
+        (rc = alloc(&b.rot, 2 * ((size_t)kRotBuffer + 4 * cap))) || (rc = alloc(&b.rot_i, (size_t)kRotBuffer + 4 * cap)))
       return rc;
     double* dg = nullptr;
     if ((rc = alloc(&dg, b.rows))) return rc;
     b.diag = dg;
+  }
+  if ((rc = alloc(&d_bufs_, nk_)) || (rc = alloc(&d_ctl_, nk_)) || (rc = alloc(&d_nn_, (size_t)kNnSlots * nk_)) ||
+      (rc = alloc(&d_tn_, (size_t)kTnSlots * nk_)) || (rc = alloc(&d_cp_, (size_t)kCpSlots * nk_)) ||
+      (rc = alloc(&d_dyn_, nk_)) || (rc = alloc(&d_opts_, 1)))
+    return rc;
+  if ((rc = cuda(cudaMallocHost(&h_ctl_, sizeof(Ctl) * nk_), "cudaMallocHost"))) return rc;
+  if ((rc = cuda(cudaFuncSetAttribute((const void*)k_dv_ctl<D>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)ctl_smem()),
+                 "cudaFuncSetAttribute")))
+    return rc;
+  if (ks_->dense) {
+    std::vector<const D*> hd(nk_);
+    for (int k = 0; k < nk_; ++k) hd[k] = reinterpret_cast<const D*>(ks_->ops[k]->dense);
+    if ((rc = alloc(&d_dense_, nk_))) return rc;
+    if ((rc = cuda(cudaMemcpy(d_dense_, hd.data(), sizeof(const D*) * nk_, cudaMemcpyHostToDevice), "upload")))
+      return rc;
+  }
+  if ((rc = cuda(cudaMemcpy(d_bufs_, hb_.data(), sizeof(Bufs<D>) * nk_, cudaMemcpyHostToDevice), "upload")))
+    return rc;
+  args_.assign(nk_, CallArgs{});
+  cols_.assign(nk_, n);
+  for (int k = 0; k < nk_; ++k) {
+    CallArgs& a = args_[k];
+    const int64_t dpc = ks_->gamma ? hb_[k].rows : 2 * (int64_t)hb_[k].rows;
+    a.x = reinterpret_cast<const double*>(hb_[k].V);
+    a.y = reinterpret_cast<double*>(hb_[k].HV);
+    a.ldx = a.ldy = dpc;
+    a.cols = n;
+    a.units = ks_->gamma ? (n + 1) / 2 : n;
+    a.dyn = d_dyn_ + k;
+  }
+  prepared_ = true;
+  return BG_OK;
+}
+
+template <class T>
+int KsetSolver<T>::run(const double* const* start, const double* const* diagonal, int32_t ptr_kind,
+                       double* const* values, double* const* vectors, int32_t* const* converged,
+                       bg_davidson_stats* stats) {
+  const int n = o_.n, cap = o_.cap;
+  int rc;
+  s_ = ks_->stream;
+  launches_ = 0;
+  if (!prepared_ && (rc = prepare())) return rc;
+  const size_t cc = (size_t)cap * cap;
+  for (int k = 0; k < nk_; ++k) {
+    const Bufs<D>& b = hb_[k];
     if ((rc = cuda(cudaMemsetAsync(b.S, 0, sizeof(D) * cc, s_), "memset")) ||
         (rc = cuda(cudaMemsetAsync(b.Hr, 0, sizeof(D) * cc, s_), "memset")) ||
         (rc = cuda(cudaMemsetAsync(b.L, 0, sizeof(D) * cc, s_), "memset")) ||
@@ -1100,21 +1228,11 @@ int KsetSolver<T>::run(const double* const* start, const double* const* diagonal
       return rc;
     const cudaMemcpyKind kind = ptr_kind == BG_PTR_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
     if ((rc = cuda(cudaMemcpyAsync(b.V, start[k], sizeof(D) * (size_t)b.rows * n, kind, s_), "copy in")) ||
-        (rc = cuda(cudaMemcpyAsync(dg, diagonal[k], sizeof(double) * b.rows, kind, s_), "copy in")))
+        (rc = cuda(cudaMemcpyAsync(const_cast<double*>(b.diag), diagonal[k], sizeof(double) * b.rows, kind, s_),
+                   "copy in")))
       return rc;
   }
-  if ((rc = alloc(&d_bufs_, nk_)) || (rc = alloc(&d_ctl_, nk_)) || (rc = alloc(&d_nn_, (size_t)kNnSlots * nk_)) ||
-      (rc = alloc(&d_tn_, (size_t)kTnSlots * nk_)) || (rc = alloc(&d_cp_, (size_t)kCpSlots * nk_)) ||
-      (rc = alloc(&d_dyn_, nk_)))
-    return rc;
-  if ((rc = cuda(cudaMallocHost(&h_ctl_, sizeof(Ctl) * nk_), "cudaMallocHost"))) return rc;
-  if (ks_->dense) {
-    std::vector<const D*> hd(nk_);
-    for (int k = 0; k < nk_; ++k) hd[k] = reinterpret_cast<const D*>(ks_->ops[k]->dense);
-    if ((rc = alloc(&d_dense_, nk_))) return rc;
-    if ((rc = cuda(cudaMemcpyAsync(d_dense_, hd.data(), sizeof(const D*) * nk_, cudaMemcpyHostToDevice, s_), "upload")))
-      return rc;
-  }
+  if ((rc = cuda(cudaMemcpyAsync(d_opts_, &o_, sizeof(Opts), cudaMemcpyHostToDevice, s_), "upload"))) return rc;
   // start: H V and the Grams of the start block, descriptors written from the host
   std::vector<Ctl> c0(nk_);
   std::vector<DynCols> dy(nk_);
@@ -1132,41 +1250,31 @@ int KsetSolver<T>::run(const double* const* start, const double* const* diagonal
     t0[k] = TN<D>{b.V, b.V, b.S, cap, n, n};
     t0[(size_t)nk_ + k] = TN<D>{b.V, b.HV, b.Hr, cap, n, n};
   }
-  if ((rc = cuda(cudaMemcpyAsync(d_bufs_, hb_.data(), sizeof(Bufs<D>) * nk_, cudaMemcpyHostToDevice, s_), "upload")) ||
-      (rc = cuda(cudaMemcpyAsync(d_ctl_, c0.data(), sizeof(Ctl) * nk_, cudaMemcpyHostToDevice, s_), "upload")) ||
+  if ((rc = cuda(cudaMemcpyAsync(d_ctl_, c0.data(), sizeof(Ctl) * nk_, cudaMemcpyHostToDevice, s_), "upload")) ||
       (rc = cuda(cudaMemcpyAsync(d_dyn_, dy.data(), sizeof(DynCols) * nk_, cudaMemcpyHostToDevice, s_), "upload")) ||
       (rc = cuda(cudaMemcpyAsync(d_tn_, t0.data(), sizeof(TN<D>) * t0.size(), cudaMemcpyHostToDevice, s_), "upload")))
     return rc;
-  args_.assign(nk_, CallArgs{});
-  cols_.assign(nk_, n);
-  for (int k = 0; k < nk_; ++k) {
-    CallArgs& a = args_[k];
-    const int64_t dpc = ks_->gamma ? hb_[k].rows : 2 * (int64_t)hb_[k].rows;
-    a.x = reinterpret_cast<const double*>(hb_[k].V);
-    a.y = reinterpret_cast<double*>(hb_[k].HV);
-    a.ldx = a.ldy = dpc;
-    a.cols = n;
-    a.units = ks_->gamma ? (n + 1) / 2 : n;
-    a.dyn = d_dyn_ + k;
-  }
   launches_ += apply() + tn(2) + ctl(kSetup);
   bool done = false;
   if ((rc = poll(&done))) return rc;
   // iterations: one captured graph replayed until every k point has finished
-  bool graph_ok = false;
-  if (want_graph_) {
+  if (want_graph_ && !graph_tried_) {
+    graph_tried_ = true;
     cudaStreamCaptureStatus st;
     if (cudaStreamIsCapturing(s_, &st) == cudaSuccess && st == cudaStreamCaptureStatusNone &&
         cudaStreamBeginCapture(s_, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
       const int64_t per = iteration();
       if (cudaStreamEndCapture(s_, &graph_) == cudaSuccess && graph_ &&
-          cudaGraphInstantiate(&exec_, graph_, 0) == cudaSuccess) {
-        graph_ok = true;
+          cudaGraphInstantiate(&exec_, graph_, 0) == cudaSuccess)
         per_iteration_ = per;
+      else if (exec_) {
+        cudaGraphExecDestroy(exec_);
+        exec_ = nullptr;
       }
     }
     cudaGetLastError();
   }
+  const bool graph_ok = want_graph_ && exec_ != nullptr;
   for (int it = 0; it < o_.max_iterations && !done; ++it) {
     if (graph_ok) {
       if ((rc = cuda(cudaGraphLaunch(exec_, s_), "cudaGraphLaunch"))) return rc;
@@ -1252,7 +1360,7 @@ extern "C" int bg_kset_davidson_solve(bg_kset* ks, const double* const* start, c
     bad = n > rows || capk < std::min<int64_t>(2 * n, rows) || n > op->cap;
     cap = std::min(cap, capk);
   }
-  if (bad || cap > 4096)
+  if (bad || cap > 1536)
     return fail(ctx, BG_EINVAL, "reference Davidson dimensions/threshold (bands must fit every operator's capacity)");
   for (int k = 0; k < nk; ++k) {
     if (!start[k] || !diagonal[k] || !eigenvalues[k] || !eigenvectors[k] || !converged[k])
@@ -1269,22 +1377,36 @@ extern "C" int bg_kset_davidson_solve(bg_kset* ks, const double* const* start, c
   }
   cudaError_t e = cudaSetDevice(ctx->device);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaSetDevice");
-  Opts op{(int)n, (int)cap, (int)o.occupied, o.first_step ? 1 : 0, o.max_iterations, o.threshold, o.preconditioner};
+  Opts op{(int)n, (int)cap, (int)o.occupied, o.first_step ? 1 : 0, o.max_iterations, o.threshold, o.preconditioner, 0};
   const bool graph = (o.flags & 1) == 0;
   int rc;
   std::string err;
   int64_t launches = 0;
-  if (ks->gamma) {
-    KsetSolver<double> s(ks, op, graph);
-    rc = s.run(start, diagonal, ptr_kind, eigenvalues, eigenvectors, converged, stats);
-    err = s.error();
-    launches = s.launches();
-  } else {
-    KsetSolver<std::complex<double>> s(ks, op, graph);
-    rc = s.run(start, diagonal, ptr_kind, eigenvalues, eigenvectors, converged, stats);
-    err = s.error();
-    launches = s.launches();
-  }
+  // The solver (device work arrays, descriptors and the captured iteration graph) lives
+  // on the set and is reused while bands and capacity stay the same.
+  auto solve = [&](auto* tag) -> int {
+    using S = std::remove_pointer_t<decltype(tag)>;
+    S* s = static_cast<S*>(ks->dv_cache);
+    if (s && !s->matches(op.n, op.cap)) {
+      ks->dv_free(ks->dv_cache);
+      ks->dv_cache = nullptr;
+      s = nullptr;
+    }
+    if (!s) {
+      s = new S(ks, op.n, op.cap);
+      ks->dv_cache = s;
+      ks->dv_free = [](void* p) { delete static_cast<S*>(p); };
+    }
+    s->set_options(op, graph);
+    const int r = s->run(start, diagonal, ptr_kind, eigenvalues, eigenvectors, converged, stats);
+    err = s->error();
+    launches = s->launches();
+    return r;
+  };
+  if (ks->gamma)
+    rc = solve(static_cast<KsetSolver<double>*>(nullptr));
+  else
+    rc = solve(static_cast<KsetSolver<std::complex<double>>*>(nullptr));
   ks->launches += launches;
   if (rc != BG_OK) return fail(ctx, rc, err.empty() ? "reference Davidson failed" : err);
   return BG_OK;

@@ -82,6 +82,9 @@ struct bg_kset {
   static constexpr int kChunks = 4;
   cudaStream_t pipe[3] = {nullptr, nullptr, nullptr};
   cudaEvent_t in_done[kChunks] = {}, work_done[kChunks] = {};
+  // bg_kset_davidson_solve's solver (work arrays and iteration graph), kept between solves
+  void* dv_cache = nullptr;
+  void (*dv_free)(void*) = nullptr;
 };
 
 namespace bg {
