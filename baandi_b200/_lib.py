@@ -22,7 +22,7 @@ BG_ENOMEM = 7
 BG_PRECOND_SMOOTH, BG_PRECOND_TPA, BG_PRECOND_RITZ_SHIFT = 0, 1, 2
 BG_PTR_HOST = 0
 BG_PTR_DEVICE = 1
-BG_PREC_FP64 = 0
+BG_PREC_FP64, BG_PREC_FP32 = 0, 1
 
 CODE_NAMES = {
     BG_ESHAPE: "BG_ESHAPE", BG_ENONFINITE: "BG_ENONFINITE", BG_EEPOCH: "BG_EEPOCH",
@@ -52,7 +52,8 @@ class Projectors(ctypes.Structure):
 
 class DavidsonOptions(ctypes.Structure):
     _fields_ = [("bands", _i64), ("threshold", _dbl), ("occupied", _i64), ("first_step", _i32), ("capacity", _i64),
-                ("max_iterations", _i32), ("flags", _i32), ("preconditioner", _i32), ("reserved", _i32 * 2)]
+                ("max_iterations", _i32), ("flags", _i32), ("preconditioner", _i32), ("apply_precision", _i32),
+                ("reserved", _i32 * 1)]
 
 
 class DavidsonStats(ctypes.Structure):

@@ -209,6 +209,7 @@ int build_op(bg_ctx* ctx, const bg_basis_desc* b, const bg_projectors* pr, int64
   G.pitch = n1 | 1;
   G.sg = sg;
   G.vstride = (n0 * n1 + 1) & ~1;
+  G.vstridef = (n0 * n1 + 3) & ~3;
   G.inv_n = 1.0 / ((double)n0 * n1 * n2);
   if (!make_fft_plan(n0, &G.p0) || !make_fft_plan(n1, &G.p1) || !make_fft_plan(n2, &G.p2))
     return fail(ctx, BG_ESHAPE, "grid length must be 2,3,5-smooth and at most 128");
@@ -307,6 +308,10 @@ int build_op(bg_ctx* ctx, const bg_basis_desc* b, const bg_projectors* pr, int64
   std::vector<double> nanv((size_t)G.vstride * n2, std::nan(""));
   if ((rc = upload(op.get(), nanv.data(), nanv.size(), &d_dbl))) return rc;
   T.vt = d_dbl;
+  std::vector<float> nanf((size_t)G.vstridef * n2, std::nanf(""));
+  float* d_flt;
+  if ((rc = upload(op.get(), nanf.data(), nanf.size(), &d_flt))) return rc;
+  T.vtf = d_flt;
   void* vp;
   if ((rc = alloc(op.get(), sizeof(double2) * (size_t)op->cap_units * n2 * S, &vp))) return rc;
   T.sbuf = static_cast<double2*>(vp);
@@ -322,6 +327,14 @@ int build_op(bg_ctx* ctx, const bg_basis_desc* b, const bg_projectors* pr, int64
     if (a == 0) G.tw0 = p2;
     if (a == 1) G.tw1 = p2;
     if (a == 2) G.tw2 = p2;
+    std::vector<float> twf(tw.size());
+    for (size_t i = 0; i < tw.size(); ++i) twf[i] = (float)tw[i];
+    float* d_tf;
+    if ((rc = upload(op.get(), twf.data(), twf.size(), &d_tf))) return rc;
+    const float2* f2 = reinterpret_cast<const float2*>(d_tf);
+    if (a == 0) G.tw0f = f2;
+    if (a == 1) G.tw1f = f2;
+    if (a == 2) G.tw2f = f2;
   }
 
   // nonlocal operands and the static diagonal
@@ -551,6 +564,10 @@ int bg_op_set_potential(bg_op* op, const double* v, uint64_t epoch) {
       }
   cudaError_t e = cudaMemcpyAsync(const_cast<double*>(op->t.vt), vt.data(), vt.size() * sizeof(double),
                                   cudaMemcpyHostToDevice, op->stream);
+  if (e == cudaSuccess) {
+    launch_potential_float(op->t.vt, op->g, const_cast<float*>(op->t.vtf), op->stream);
+    e = cudaGetLastError();
+  }
   if (e == cudaSuccess) e = cudaStreamSynchronize(op->stream);
   if (e != cudaSuccess) return cuda_fail(op->ctx, e, "set_potential");
   op->epoch = epoch;
@@ -562,7 +579,9 @@ int bg_op_apply_block(bg_op* op, const double* x, double* y, int64_t rows, int64
                       int32_t precision) {
   if (!op) return fail(nullptr, BG_EINVAL, "null operator");
   bg_ctx* ctx = op->ctx;
-  if (precision != BG_PREC_FP64) return fail(ctx, BG_EINVAL, "unsupported precision");
+  if (precision != BG_PREC_FP64 && precision != BG_PREC_FP32) return fail(ctx, BG_EINVAL, "unsupported precision");
+  if (precision == BG_PREC_FP32 && (op->is_dense || !fp32_supported(op->g)))
+    return fail(ctx, BG_EINVAL, "the FP32 apply needs a cubic grid of 25, 45, 54, 60, 72 or 108 points");
   if (ptr_kind != BG_PTR_HOST && ptr_kind != BG_PTR_DEVICE) return fail(ctx, BG_EINVAL, "pointer kind");
   if (!op->has_epoch) return fail(ctx, BG_EEPOCH, "potential was never set");
   if (rows != op->rows || cols < 0 || cols > op->cap) return fail(ctx, BG_ESHAPE, "block shape");
@@ -594,7 +613,8 @@ int bg_op_apply_block(bg_op* op, const double* x, double* y, int64_t rows, int64
   a.ldy = (int64_t)dpc;
   a.cols = (int)cols;
   a.units = op->gamma ? (int)((cols + 1) / 2) : (int)cols;
-  op->launches += launch_local(op->d_tabs, op->gamma ? 1 : 0, op->t.ngroups, op->g, bt, op->stream, &op->ev);
+  op->launches += launch_local(op->d_tabs, op->gamma ? 1 : 0, op->t.ngroups, op->g, bt, op->stream, &op->ev,
+                               precision == BG_PREC_FP32 ? 1 : 0);
   if (op->shape.nproj > 0) {
     NlShape sh = op->shape;
     sh.ksplit = ksplit_for(op->rows, sh.nproj, cols, &sh.kchunk);
@@ -697,6 +717,10 @@ int bg_op_set_potential_ptr(bg_op* op, const double* v, uint64_t epoch, int32_t 
   if ((rc = transpose_grid(op, v, op->vchange))) return rc;
   e = cudaMemcpyAsync(const_cast<double*>(op->t.vt), op->vchange, sizeof(double) * op->g.vstride * op->dims[2],
                       cudaMemcpyDeviceToDevice, op->stream);
+  if (e == cudaSuccess) {
+    launch_potential_float(op->t.vt, op->g, const_cast<float*>(op->t.vtf), op->stream);
+    e = cudaGetLastError();
+  }
   if (e != cudaSuccess) return cuda_fail(op->ctx, e, "set_potential");
   op->epoch = epoch;
   op->has_epoch = true;
@@ -830,7 +854,7 @@ int bg_op_band_density_sum(bg_op* op, const double* x, int64_t rows, int64_t col
 namespace bg {
 // Launch the local and nonlocal stages of operators [k0, k1) of a set on one stream.
 int enqueue_range(bg_kset* ks, int k0, int k1, const CallArgs* args, const int64_t* cols, cudaStream_t s,
-                  StageEvents* ev) {
+                  StageEvents* ev, int fp32) {
   Batch bt;
   bt.nk = k1 - k0;
   int max_groups = 0, max_rows = 0;
@@ -842,7 +866,7 @@ int enqueue_range(bg_kset* ks, int k0, int k1, const CallArgs* args, const int64
     max_cols = std::max(max_cols, cols[k]);
   }
   if (max_cols == 0) return 0;
-  int launches = launch_local(ks->d_tabs + k0, ks->gamma, max_groups, ks->g, bt, s, ev);
+  int launches = launch_local(ks->d_tabs + k0, ks->gamma, max_groups, ks->g, bt, s, ev, fp32);
   if (ks->shape.nproj > 0) {
     NlShape sh = ks->shape;
     int64_t tiles = 0, cap = 1 << 30;
@@ -935,9 +959,12 @@ int bg_kset_apply(bg_kset* ks, const double* const* x, double* const* y, const i
                   int32_t precision) {
   if (!ks || !x || !y || !cols) return fail(ks ? ks->ctx : nullptr, BG_EINVAL, "null argument");
   bg_ctx* ctx = ks->ctx;
-  if (precision != BG_PREC_FP64) return fail(ctx, BG_EINVAL, "unsupported precision");
+  if (precision != BG_PREC_FP64 && precision != BG_PREC_FP32) return fail(ctx, BG_EINVAL, "unsupported precision");
   if (ptr_kind != BG_PTR_HOST && ptr_kind != BG_PTR_DEVICE) return fail(ctx, BG_EINVAL, "pointer kind");
   if (ks->dense) return fail(ctx, BG_EINVAL, "a set of dense operators only runs bg_kset_davidson_solve");
+  if (precision == BG_PREC_FP32 && !fp32_supported(ks->g))
+    return fail(ctx, BG_EINVAL, "the FP32 apply needs a cubic grid of 25, 45, 54, 60, 72 or 108 points");
+  const int fp32 = precision == BG_PREC_FP32 ? 1 : 0;
   const int n = (int)ks->ops.size();
   Batch bt;
   bt.nk = n;
@@ -969,7 +996,7 @@ int bg_kset_apply(bg_kset* ks, const double* const* x, double* const* y, const i
   }
   if (max_cols == 0) return BG_OK;
   if (ptr_kind == BG_PTR_DEVICE) {
-    ks->launches += enqueue_range(ks, 0, n, args.data(), cols, ks->stream, &ks->ev);
+    ks->launches += enqueue_range(ks, 0, n, args.data(), cols, ks->stream, &ks->ev, fp32);
     e = cudaGetLastError();
     return e == cudaSuccess ? BG_OK : cuda_fail(ctx, e, "kernel launch");
   }
@@ -989,7 +1016,7 @@ int bg_kset_apply(bg_kset* ks, const double* const* x, double* const* y, const i
     }
     cudaEventRecord(ks->in_done[c], in);
     cudaStreamWaitEvent(work, ks->in_done[c], 0);
-    ks->launches += enqueue_range(ks, k0, k1, args.data(), cols, work, nullptr);
+    ks->launches += enqueue_range(ks, k0, k1, args.data(), cols, work, nullptr, fp32);
     cudaEventRecord(ks->work_done[c], work);
     cudaStreamWaitEvent(out, ks->work_done[c], 0);
     for (int k = k0; k < k1; ++k) {

@@ -192,7 +192,7 @@ int Solver<T>::apply(const D* x, D* y, int k) {
   stats_.h_calls += 1;
   stats_.h_columns += k;
   int rc = bg_op_apply_block(op_, reinterpret_cast<const double*>(x), reinterpret_cast<double*>(y), rows_, k,
-                             BG_PTR_DEVICE, BG_PREC_FP64);
+                             BG_PTR_DEVICE, o_.apply_precision);
   if (rc != BG_OK) {
     err_ = "operator apply failed: " + op_->ctx->error;
     return rc;
@@ -488,7 +488,8 @@ extern "C" int bg_davidson_solve(bg_op* op, const double* start, const double* d
   // crates/dft-solvers/src/ref_davidson.rs:133-146
   const bool bad = n == 0 || n > dim || cap < std::min<int64_t>(2 * n, dim) || o.occupied > n || o.occupied < 0 ||
                    o.max_iterations <= 0 || !std::isfinite(o.threshold) || o.threshold <= 0.0 || cap > op->cap ||
-                   o.preconditioner < BG_PRECOND_SMOOTH || o.preconditioner > BG_PRECOND_RITZ_SHIFT;
+                   o.preconditioner < BG_PRECOND_SMOOTH || o.preconditioner > BG_PRECOND_RITZ_SHIFT ||
+                   (o.apply_precision != BG_PREC_FP64 && o.apply_precision != BG_PREC_FP32);
   if (bad) return fail(op->ctx, BG_EINVAL, "reference Davidson dimensions/threshold/start (capacity must also fit the operator)");
   const size_t per = op->gamma ? 1 : 2;
   for (size_t i = 0; i < (size_t)dim * n * per; ++i)

@@ -27,6 +27,37 @@ struct FftPlan {
   int radix[kMaxStages];
 };
 
+// Complex element types of the line transforms: double2 (FP64) and float2 (FP32).
+template <class C>
+struct Cplx;
+template <>
+struct Cplx<double2> {
+  using R = double;
+  __device__ __forceinline__ static double2 make(double x, double y) { return make_double2(x, y); }
+};
+template <>
+struct Cplx<float2> {
+  using R = float;
+  __device__ __forceinline__ static float2 make(float x, float y) { return make_float2(x, y); }
+};
+template <class C>
+using RealOf = typename Cplx<C>::R;
+template <class C>
+__device__ __forceinline__ C mkc(RealOf<C> x, RealOf<C> y) {
+  return Cplx<C>::make(x, y);
+}
+
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+  return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ float2 cscale(float2 a, float s) { return make_float2(a.x * s, a.y * s); }
+template <int SIGN>
+__device__ __forceinline__ float2 irot(float2 a) {
+  return SIGN > 0 ? make_float2(-a.y, a.x) : make_float2(a.y, -a.x);
+}
+
 __device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
 __device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
 __device__ __forceinline__ double2 cmul(double2 a, double2 b) {

@@ -1,4 +1,4 @@
-// Compile-time line FFTs for the grid lengths of the benchmark cells (FP64 complex).
+// Compile-time line FFTs for the grid lengths of the benchmark cells (FP64 or FP32 complex).
 //
 // A pass transforms L lines held in shared memory.  Each warp owns a contiguous block
 // of lines and carries it through every radix stage alone, separated only by
@@ -40,58 +40,61 @@ BG_PLAN(108, 12, 9)
 #undef BG_PLAN
 
 // --------------------------------------------------------------------- butterflies
-template <int SIGN>
-__device__ __forceinline__ double2 w_mul(double2 a, double c, double s) {
+// C = double2 or float2; constants are rounded to the element's precision.
+template <int SIGN, class C>
+__device__ __forceinline__ C w_mul(C a, RealOf<C> c, RealOf<C> s) {
   // a * (c + i SIGN s)
-  const double ss = SIGN > 0 ? s : -s;
-  return make_double2(a.x * c - a.y * ss, a.x * ss + a.y * c);
+  const RealOf<C> ss = SIGN > 0 ? s : -s;
+  return mkc<C>(a.x * c - a.y * ss, a.x * ss + a.y * c);
 }
 
-template <int R, int SIGN>
+template <int R, int SIGN, class C>
 struct Dft;
 
-template <int SIGN>
-struct Dft<2, SIGN> {
-  __device__ __forceinline__ static void run(double2* v) {
-    const double2 a = v[0], b = v[1];
+template <int SIGN, class C>
+struct Dft<2, SIGN, C> {
+  __device__ __forceinline__ static void run(C* v) {
+    const C a = v[0], b = v[1];
     v[0] = cadd(a, b);
     v[1] = csub(a, b);
   }
 };
-template <int SIGN>
-struct Dft<3, SIGN> {
-  __device__ __forceinline__ static void run(double2* v) {
-    const double h = 0.8660254037844386;
-    const double2 t1 = cadd(v[1], v[2]);
-    const double2 t2 = make_double2(v[0].x - 0.5 * t1.x, v[0].y - 0.5 * t1.y);
-    const double2 t3 = irot<SIGN>(cscale(csub(v[1], v[2]), h));
+template <int SIGN, class C>
+struct Dft<3, SIGN, C> {
+  __device__ __forceinline__ static void run(C* v) {
+    using T = RealOf<C>;
+    const T h = T(0.8660254037844386), half = T(0.5);
+    const C t1 = cadd(v[1], v[2]);
+    const C t2 = mkc<C>(v[0].x - half * t1.x, v[0].y - half * t1.y);
+    const C t3 = irot<SIGN>(cscale(csub(v[1], v[2]), h));
     v[0] = cadd(v[0], t1);
     v[1] = cadd(t2, t3);
     v[2] = csub(t2, t3);
   }
 };
-template <int SIGN>
-struct Dft<4, SIGN> {
-  __device__ __forceinline__ static void run(double2* v) {
-    const double2 a = cadd(v[0], v[2]), b = csub(v[0], v[2]);
-    const double2 c = cadd(v[1], v[3]), d = irot<SIGN>(csub(v[1], v[3]));
+template <int SIGN, class C>
+struct Dft<4, SIGN, C> {
+  __device__ __forceinline__ static void run(C* v) {
+    const C a = cadd(v[0], v[2]), b = csub(v[0], v[2]);
+    const C c = cadd(v[1], v[3]), d = irot<SIGN>(csub(v[1], v[3]));
     v[0] = cadd(a, c);
     v[2] = csub(a, c);
     v[1] = cadd(b, d);
     v[3] = csub(b, d);
   }
 };
-template <int SIGN>
-struct Dft<5, SIGN> {
-  __device__ __forceinline__ static void run(double2* v) {
-    const double c1 = 0.30901699437494745, c2 = -0.8090169943749475;
-    const double s1 = 0.9510565162951535, s2 = 0.5877852522924731;
-    const double2 p1 = cadd(v[1], v[4]), m1 = csub(v[1], v[4]);
-    const double2 p2 = cadd(v[2], v[3]), m2 = csub(v[2], v[3]);
-    const double2 a1 = make_double2(v[0].x + c1 * p1.x + c2 * p2.x, v[0].y + c1 * p1.y + c2 * p2.y);
-    const double2 a2 = make_double2(v[0].x + c2 * p1.x + c1 * p2.x, v[0].y + c2 * p1.y + c1 * p2.y);
-    const double2 b1 = irot<SIGN>(make_double2(s1 * m1.x + s2 * m2.x, s1 * m1.y + s2 * m2.y));
-    const double2 b2 = irot<SIGN>(make_double2(s2 * m1.x - s1 * m2.x, s2 * m1.y - s1 * m2.y));
+template <int SIGN, class C>
+struct Dft<5, SIGN, C> {
+  __device__ __forceinline__ static void run(C* v) {
+    using T = RealOf<C>;
+    const T c1 = T(0.30901699437494745), c2 = T(-0.8090169943749475);
+    const T s1 = T(0.9510565162951535), s2 = T(0.5877852522924731);
+    const C p1 = cadd(v[1], v[4]), m1 = csub(v[1], v[4]);
+    const C p2 = cadd(v[2], v[3]), m2 = csub(v[2], v[3]);
+    const C a1 = mkc<C>(v[0].x + c1 * p1.x + c2 * p2.x, v[0].y + c1 * p1.y + c2 * p2.y);
+    const C a2 = mkc<C>(v[0].x + c2 * p1.x + c1 * p2.x, v[0].y + c2 * p1.y + c1 * p2.y);
+    const C b1 = irot<SIGN>(mkc<C>(s1 * m1.x + s2 * m2.x, s1 * m1.y + s2 * m2.y));
+    const C b2 = irot<SIGN>(mkc<C>(s2 * m1.x - s1 * m2.x, s2 * m1.y - s1 * m2.y));
     v[0] = cadd(v[0], cadd(p1, p2));
     v[1] = cadd(a1, b1);
     v[4] = csub(a1, b1);
@@ -101,15 +104,16 @@ struct Dft<5, SIGN> {
 };
 // 6 = 3 x 2: a = DFT3(v0, v2, v4), b = DFT3(v1, v3, v5); X[u] = a[u] + w6^u b[u],
 // X[u+3] = a[u] - w6^u b[u].
-template <int SIGN>
-struct Dft<6, SIGN> {
-  __device__ __forceinline__ static void run(double2* v) {
-    double2 a[3] = {v[0], v[2], v[4]}, b[3] = {v[1], v[3], v[5]};
-    Dft<3, SIGN>::run(a);
-    Dft<3, SIGN>::run(b);
-    const double h = 0.8660254037844386;
-    const double2 b1 = w_mul<SIGN>(b[1], 0.5, h);
-    const double2 b2 = w_mul<SIGN>(b[2], -0.5, h);
+template <int SIGN, class C>
+struct Dft<6, SIGN, C> {
+  __device__ __forceinline__ static void run(C* v) {
+    using T = RealOf<C>;
+    C a[3] = {v[0], v[2], v[4]}, b[3] = {v[1], v[3], v[5]};
+    Dft<3, SIGN, C>::run(a);
+    Dft<3, SIGN, C>::run(b);
+    const T h = T(0.8660254037844386);
+    const C b1 = w_mul<SIGN>(b[1], T(0.5), h);
+    const C b2 = w_mul<SIGN>(b[2], T(-0.5), h);
     v[0] = cadd(a[0], b[0]);
     v[3] = csub(a[0], b[0]);
     v[1] = cadd(a[1], b1);
@@ -119,16 +123,17 @@ struct Dft<6, SIGN> {
   }
 };
 // 8 = 4 x 2: a = DFT4(evens), b = DFT4(odds); X[u] = a[u] + w8^u b[u], X[u+4] = a[u] - w8^u b[u].
-template <int SIGN>
-struct Dft<8, SIGN> {
-  __device__ __forceinline__ static void run(double2* v) {
-    double2 a[4] = {v[0], v[2], v[4], v[6]}, b[4] = {v[1], v[3], v[5], v[7]};
-    Dft<4, SIGN>::run(a);
-    Dft<4, SIGN>::run(b);
-    const double r = 0.7071067811865476;
-    const double2 b1 = w_mul<SIGN>(b[1], r, r);
-    const double2 b2 = irot<SIGN>(b[2]);
-    const double2 b3 = w_mul<SIGN>(b[3], -r, r);
+template <int SIGN, class C>
+struct Dft<8, SIGN, C> {
+  __device__ __forceinline__ static void run(C* v) {
+    using T = RealOf<C>;
+    C a[4] = {v[0], v[2], v[4], v[6]}, b[4] = {v[1], v[3], v[5], v[7]};
+    Dft<4, SIGN, C>::run(a);
+    Dft<4, SIGN, C>::run(b);
+    const T r = T(0.7071067811865476);
+    const C b1 = w_mul<SIGN>(b[1], r, r);
+    const C b2 = irot<SIGN>(b[2]);
+    const C b3 = w_mul<SIGN>(b[3], -r, r);
     v[0] = cadd(a[0], b[0]);
     v[4] = csub(a[0], b[0]);
     v[1] = cadd(a[1], b1);
@@ -141,24 +146,25 @@ struct Dft<8, SIGN> {
 };
 // 9 = 3 x 3: a_m = DFT3(v_m, v_{m+3}, v_{m+6}); b_m[k1] = a_m[k1] w9^(m k1);
 // X[k1 + 3 k2] = DFT3 over m of b_m[k1].
-template <int SIGN>
-struct Dft<9, SIGN> {
-  __device__ __forceinline__ static void run(double2* v) {
-    double2 a0[3] = {v[0], v[3], v[6]}, a1[3] = {v[1], v[4], v[7]}, a2[3] = {v[2], v[5], v[8]};
-    Dft<3, SIGN>::run(a0);
-    Dft<3, SIGN>::run(a1);
-    Dft<3, SIGN>::run(a2);
-    const double c1 = 0.766044443118978, s1 = 0.6427876096865394;    // 2 pi/9
-    const double c2 = 0.17364817766693036, s2 = 0.984807753012208;   // 4 pi/9
-    const double c4 = -0.9396926207859084, s4 = 0.3420201433256687;  // 8 pi/9
+template <int SIGN, class C>
+struct Dft<9, SIGN, C> {
+  __device__ __forceinline__ static void run(C* v) {
+    using T = RealOf<C>;
+    C a0[3] = {v[0], v[3], v[6]}, a1[3] = {v[1], v[4], v[7]}, a2[3] = {v[2], v[5], v[8]};
+    Dft<3, SIGN, C>::run(a0);
+    Dft<3, SIGN, C>::run(a1);
+    Dft<3, SIGN, C>::run(a2);
+    const T c1 = T(0.766044443118978), s1 = T(0.6427876096865394);    // 2 pi/9
+    const T c2 = T(0.17364817766693036), s2 = T(0.984807753012208);   // 4 pi/9
+    const T c4 = T(-0.9396926207859084), s4 = T(0.3420201433256687);  // 8 pi/9
     a1[1] = w_mul<SIGN>(a1[1], c1, s1);
     a1[2] = w_mul<SIGN>(a1[2], c2, s2);
     a2[1] = w_mul<SIGN>(a2[1], c2, s2);
     a2[2] = w_mul<SIGN>(a2[2], c4, s4);
 #pragma unroll
     for (int k1 = 0; k1 < 3; ++k1) {
-      double2 t[3] = {a0[k1], a1[k1], a2[k1]};
-      Dft<3, SIGN>::run(t);
+      C t[3] = {a0[k1], a1[k1], a2[k1]};
+      Dft<3, SIGN, C>::run(t);
       v[k1] = t[0];
       v[k1 + 3] = t[1];
       v[k1 + 6] = t[2];
@@ -168,24 +174,25 @@ struct Dft<9, SIGN> {
 
 // 12 = 3 x 4: a_m = DFT4(v_m, v_{m+3}, v_{m+6}, v_{m+9}); b_m[k1] = a_m[k1] w12^(m k1);
 // X[k1 + 4 k2] = DFT3 over m of b_m[k1].
-template <int SIGN>
-struct Dft<12, SIGN> {
-  __device__ __forceinline__ static void run(double2* v) {
-    double2 a0[4] = {v[0], v[3], v[6], v[9]}, a1[4] = {v[1], v[4], v[7], v[10]}, a2[4] = {v[2], v[5], v[8], v[11]};
-    Dft<4, SIGN>::run(a0);
-    Dft<4, SIGN>::run(a1);
-    Dft<4, SIGN>::run(a2);
-    const double h = 0.8660254037844386;
-    a1[1] = w_mul<SIGN>(a1[1], h, 0.5);   // w12^1
-    a1[2] = w_mul<SIGN>(a1[2], 0.5, h);   // w12^2
-    a1[3] = irot<SIGN>(a1[3]);            // w12^3
-    a2[1] = w_mul<SIGN>(a2[1], 0.5, h);   // w12^2
-    a2[2] = w_mul<SIGN>(a2[2], -0.5, h);  // w12^4
-    a2[3] = make_double2(-a2[3].x, -a2[3].y);  // w12^6
+template <int SIGN, class C>
+struct Dft<12, SIGN, C> {
+  __device__ __forceinline__ static void run(C* v) {
+    using T = RealOf<C>;
+    C a0[4] = {v[0], v[3], v[6], v[9]}, a1[4] = {v[1], v[4], v[7], v[10]}, a2[4] = {v[2], v[5], v[8], v[11]};
+    Dft<4, SIGN, C>::run(a0);
+    Dft<4, SIGN, C>::run(a1);
+    Dft<4, SIGN, C>::run(a2);
+    const T h = T(0.8660254037844386), half = T(0.5);
+    a1[1] = w_mul<SIGN>(a1[1], h, half);   // w12^1
+    a1[2] = w_mul<SIGN>(a1[2], half, h);   // w12^2
+    a1[3] = irot<SIGN>(a1[3]);             // w12^3
+    a2[1] = w_mul<SIGN>(a2[1], half, h);   // w12^2
+    a2[2] = w_mul<SIGN>(a2[2], -half, h);  // w12^4
+    a2[3] = mkc<C>(-a2[3].x, -a2[3].y);    // w12^6
 #pragma unroll
     for (int k1 = 0; k1 < 4; ++k1) {
-      double2 t[3] = {a0[k1], a1[k1], a2[k1]};
-      Dft<3, SIGN>::run(t);
+      C t[3] = {a0[k1], a1[k1], a2[k1]};
+      Dft<3, SIGN, C>::run(t);
       v[k1] = t[0];
       v[k1 + 4] = t[1];
       v[k1 + 8] = t[2];
@@ -205,9 +212,8 @@ __device__ __forceinline__ int lane_id() {
 
 // Stage (R, NS) on lines first .. first+count-1 of this warp; ES = element stride.
 // A lane's butterfly index j is the same in every round.
-template <int N, int R, int NS, int SIGN, int ES, class Off>
-__device__ __forceinline__ void stage(double2* base, int first, int count, Off off, const double2* __restrict__ tw,
-                                      int lane) {
+template <int N, int R, int NS, int SIGN, int ES, class Off, class C>
+__device__ __forceinline__ void stage(C* base, int first, int count, Off off, const C* __restrict__ tw, int lane) {
   constexpr int SPAN = N / R;
   constexpr int STEP = N / (NS * R);
   constexpr int K = (SPAN + 31) / 32;                 // butterflies per lane when a line exceeds a warp
@@ -226,7 +232,7 @@ __device__ __forceinline__ void stage(double2* base, int first, int count, Off o
     kk[q] = k * STEP;
   }
   for (int r0 = 0; r0 < count; r0 += LPR) {
-    double2 v[K][R];
+    C v[K][R];
     int lo[K];
 #pragma unroll
     for (int q = 0; q < K; ++q) {
@@ -244,16 +250,16 @@ __device__ __forceinline__ void stage(double2* base, int first, int count, Off o
         if (NS > 1) {
           // w^(t k STEP) as powers of one table entry: one shared-memory load per
           // butterfly instead of R - 1 (relative error grows by about one ulp per power)
-          double2 w1 = tw[kk[q]];
+          C w1 = tw[kk[q]];
           if (SIGN < 0) w1.y = -w1.y;
-          double2 x = w1;
+          C x = w1;
 #pragma unroll
           for (int t = 1; t < R; ++t) {
             v[q][t] = cmul(v[q][t], x);
             if (t + 1 < R) x = cmul(x, w1);
           }
         }
-        Dft<R, SIGN>::run(v[q]);
+        Dft<R, SIGN, C>::run(v[q]);
 #pragma unroll
         for (int u = 0; u < R; ++u) base[lo[q] + (oo[q] + u * NS) * ES] = v[q][u];
       }
@@ -262,9 +268,9 @@ __device__ __forceinline__ void stage(double2* base, int first, int count, Off o
   }
 }
 
-template <int N, int SIGN, int ES, int S, int NS, class Off>
-__device__ __forceinline__ void stages_from(double2* base, int first, int count, Off off,
-                                            const double2* __restrict__ tw, int lane) {
+template <int N, int SIGN, int ES, int S, int NS, class Off, class C>
+__device__ __forceinline__ void stages_from(C* base, int first, int count, Off off, const C* __restrict__ tw,
+                                            int lane) {
   using P = Plan<N>;
   if constexpr (S < P::nst) {
     constexpr int R = P::radix[S];
@@ -274,9 +280,8 @@ __device__ __forceinline__ void stages_from(double2* base, int first, int count,
 }
 
 // Every stage of lines first .. first+count-1 (one warp; ends with __syncwarp).
-template <int N, int SIGN, int ES, class Off>
-__device__ __forceinline__ void group(double2* base, int first, int count, Off off, const double2* __restrict__ tw,
-                                      int lane) {
+template <int N, int SIGN, int ES, class Off, class C>
+__device__ __forceinline__ void group(C* base, int first, int count, Off off, const C* __restrict__ tw, int lane) {
   stages_from<N, SIGN, ES, 0, 1>(base, first, count, off, tw, lane);
 }
 
@@ -287,9 +292,9 @@ __device__ __forceinline__ void group(double2* base, int first, int count, Off o
 // plan reversed (R2, R1).  So that butterfly multiplies by w, runs the forward radix-R2
 // DFT and stores once; shared memory sees load, store, load, store, load, store per
 // element instead of ten accesses.  w(line, x) is read through `wgt`.
-template <int N, int ES, class Off, class W>
-__device__ __forceinline__ void inverse_weight_forward(double2* base, int first, int count, Off off,
-                                                       const double2* __restrict__ tw, W wgt, int lane) {
+template <int N, int ES, class Off, class W, class C>
+__device__ __forceinline__ void inverse_weight_forward(C* base, int first, int count, Off off,
+                                                       const C* __restrict__ tw, W wgt, int lane) {
   using P = Plan<N>;
   static_assert(P::nst == 2, "two-stage plans only");
   constexpr int R1 = P::radix[0];
@@ -303,7 +308,7 @@ __device__ __forceinline__ void inverse_weight_forward(double2* base, int first,
   const int j = lane - li * SPAN;
   const bool lane_ok = li < LPR;
   for (int r0 = 0; r0 < count; r0 += LPR) {
-    double2 v[R2];
+    C v[R2];
     const bool act = lane_ok && r0 + li < count;
     const int line = first + r0 + li;
     const int lo = act ? off(line) : 0;
@@ -314,22 +319,22 @@ __device__ __forceinline__ void inverse_weight_forward(double2* base, int first,
     __syncwarp();
     if (act) {
       {
-        const double2 w1 = tw[j];  // w^(t k N/(R1 R2)) with k = j, as powers of w^j
-        double2 x = w1;
+        const C w1 = tw[j];  // w^(t k N/(R1 R2)) with k = j, as powers of w^j
+        C x = w1;
 #pragma unroll
         for (int t = 1; t < R2; ++t) {
           v[t] = cmul(v[t], x);
           if (t + 1 < R2) x = cmul(x, w1);
         }
       }
-      Dft<R2, 1>::run(v);
+      Dft<R2, 1, C>::run(v);
 #pragma unroll
       for (int u = 0; u < R2; ++u) {
-        const double w = wgt(line, j + u * R1);
+        const RealOf<C> w = wgt(line, j + u * R1);
         v[u].x *= w;
         v[u].y *= w;
       }
-      Dft<R2, -1>::run(v);
+      Dft<R2, -1, C>::run(v);
 #pragma unroll
       for (int u = 0; u < R2; ++u) base[lo + (j * R2 + u) * ES] = v[u];
     }
@@ -348,8 +353,8 @@ __device__ __forceinline__ void owned_lines(int nlines, int* first, int* count) 
 }
 
 // A whole pass over nlines lines; ends with __syncthreads.
-template <int N, int SIGN, int ES, class Off>
-__device__ __forceinline__ void pass(double2* base, int nlines, Off off, const double2* __restrict__ tw) {
+template <int N, int SIGN, int ES, class Off, class C>
+__device__ __forceinline__ void pass(C* base, int nlines, Off off, const C* __restrict__ tw) {
   int first, count;
   owned_lines(nlines, &first, &count);
   if (count > 0) group<N, SIGN, ES>(base, first, count, off, tw, threadIdx.x & 31);

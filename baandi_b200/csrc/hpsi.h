@@ -29,6 +29,7 @@ struct OpTables {
   const int* xact;        // nxact x rows
   const double* kinetic;  // rows
   const double* vt;       // V(r) transposed to [z][y][x]
+  const float* vtf;       // the same in FP32 (the FP32 apply), plane stride BoxGeo::vstridef
   double2* sbuf;          // stick buffer [unit][z][S]
   int* err;               // device error word (bit 0: non-finite input)
 };
@@ -40,11 +41,15 @@ struct BoxGeo {
   int pitch;   // row pitch of the shared-memory plane (odd)
   int sg;      // max sticks per group
   int vstride; // doubles between z planes of the transposed potential (even: 16-byte aligned planes)
+  int vstridef; // floats between z planes of the FP32 potential (multiple of 4: 16-byte aligned planes)
   double inv_n;
   FftPlan p0, p1, p2;
   const double2* tw0;  // exp(+2 pi i q/n0), q < n0
   const double2* tw1;
   const double2* tw2;
+  const float2* tw0f;  // FP32 copies (rounded from the same long double values)
+  const float2* tw1f;
+  const float2* tw2f;
 };
 
 // Block of one operator whose columns are decided on the device (a solver's correction
@@ -115,7 +120,9 @@ struct StageEvents {
 // Enqueue the local + kinetic part: y = gather(FFT(V IFFT(scatter x)))/N + T x.
 // tabs: device array of b.nk operator tables.  Returns the number of launches.
 int launch_local(const OpTables* tabs, int gamma, int max_groups, const BoxGeo& g, const Batch& b, cudaStream_t s,
-                 StageEvents* ev);
+                 StageEvents* ev, int fp32 = 0);
+// The FP32 local apply needs a cubic box with a compile-time plan.
+bool fp32_supported(const BoxGeo& g);
 // Enqueue y += P (D (P^H x)) (complex) or y += P (D (P^T x)) (Gamma).
 int launch_nonlocal(const NlDev* nl, int gamma, const NlShape& sh, int max_rows, const Batch& b, cudaStream_t s,
                     StageEvents* ev);
@@ -131,6 +138,8 @@ void launch_density_reduce(const double* part, int chunks, const BoxGeo& g, doub
                            double* out, cudaStream_t s);
 // vt[z vstride + y n0 + x] = v[x][y][z] (C order, device); *err |= 2 on a non-finite value.
 void launch_potential_transpose(const double* v, const BoxGeo& g, double* vt, int* err, cudaStream_t s);
+// vtf = (float) vt plane by plane (the FP32 apply's potential).
+void launch_potential_float(const double* vt, const BoxGeo& g, float* vtf, cudaStream_t s);
 
 // Radix plan of a line of n <= 128 points (2, 3, 4, 5) for fft_lines; false if n has
 // another prime factor.  twiddles(n): exp(+2 pi i q/n), q < n, interleaved (re, im).

@@ -44,6 +44,11 @@ struct LineOffRows {
 // The fast plane kernel stages V(r) of its plane in shared memory when plane and
 // potential fit together (N <= 90: 90 x 91 x 16 + 90 x 90 x 8 bytes = 196 KB).
 __host__ __device__ constexpr bool v_in_smem(int n) { return n <= 90; }
+// FP32 planes are half the size: V(r) fits beside them up to N = 128.
+template <class C>
+__host__ __device__ constexpr bool v_in_smem_t(int n) {
+  return sizeof(C) == sizeof(double2) ? v_in_smem(n) : n <= 128;
+}
 
 struct LineOffTable {
   const int* off;
@@ -55,19 +60,42 @@ struct LineOffCols {
 
 __device__ __forceinline__ bool finite2(double a, double b) { return isfinite(a) && isfinite(b); }
 
+// FP64 (double2) or FP32 (float2) local apply: twiddles, stick buffer and potential of
+// the element type.  The FP32 stick buffer reuses the FP64 one's memory.
+template <class C>
+__device__ __forceinline__ const C* tw_axis(const BoxGeo& g, int axis);
+template <>
+__device__ __forceinline__ const double2* tw_axis<double2>(const BoxGeo& g, int axis) {
+  return axis == 0 ? g.tw0 : axis == 1 ? g.tw1 : g.tw2;
+}
+template <>
+__device__ __forceinline__ const float2* tw_axis<float2>(const BoxGeo& g, int axis) {
+  return axis == 0 ? g.tw0f : axis == 1 ? g.tw1f : g.tw2f;
+}
+template <class C>
+__device__ __forceinline__ C* sticks_of(const OpTables& t) {
+  return reinterpret_cast<C*>(t.sbuf);
+}
+template <class C>
+__device__ __forceinline__ C to_elem(double x, double y) {
+  return mkc<C>(RealOf<C>(x), RealOf<C>(y));
+}
+
 // ---------------------------------------------------------------- pass 1
-template <bool GAMMA, int N>
+template <bool GAMMA, int N, class C = double2>
 __global__ void __launch_bounds__(N == 0 ? 256 : 128, N == 0 ? 1 : 6) k_sticks_inverse(const OpTables* __restrict__ tabs, BoxGeo g, Batch b) {
+  static_assert(N != 0 || sizeof(C) == sizeof(double2), "the runtime-plan engine is FP64 only");
   const OpTables& t = tabs[blockIdx.z];
   const CallArgs a = resolve(b.a[blockIdx.z]);
   const int grp = blockIdx.x, unit = blockIdx.y;
   if (grp >= t.ngroups || unit >= a.units) return;
-  extern __shared__ double2 sm[];
-  double2* tw = sm;
-  double2* st = sm + g.n2;
+  extern __shared__ __align__(16) unsigned char si_raw[];
+  C* tw = reinterpret_cast<C*>(si_raw);
+  C* st = tw + g.n2;
   const int s0 = t.grp_stick[grp], cnt = t.grp_stick[grp + 1] - s0;
-  for (int i = threadIdx.x; i < g.n2; i += blockDim.x) tw[i] = g.tw2[i];
-  for (int i = threadIdx.x; i < cnt * g.ld2; i += blockDim.x) st[i] = make_double2(0.0, 0.0);
+  const C* twg = tw_axis<C>(g, 2);
+  for (int i = threadIdx.x; i < g.n2; i += blockDim.x) tw[i] = twg[i];
+  for (int i = threadIdx.x; i < cnt * g.ld2; i += blockDim.x) st[i] = to_elem<C>(0.0, 0.0);
   __syncthreads();
   const int e0 = t.grp_entry[grp], e1 = t.grp_entry[grp + 1];
   bool bad = false;
@@ -77,7 +105,7 @@ __global__ void __launch_bounds__(N == 0 ? 256 : 128, N == 0 ? 1 : 6) k_sticks_i
       const int2 en = t.entries[e];
       const double2 v = x[en.x];
       bad |= !finite2(v.x, v.y);
-      st[en.y] = v;
+      st[en.y] = to_elem<C>(v.x, v.y);
     }
   } else {
     const int ca = 2 * unit;
@@ -98,7 +126,7 @@ __global__ void __launch_bounds__(N == 0 ? 256 : 128, N == 0 ? 1 : 6) k_sticks_i
         v = code > 0 ? make_double2(pa.x - pb.y, pa.y + pb.x) : make_double2(pa.x + pb.y, -pa.y + pb.x);
       }
       bad |= !finite2(v.x, v.y);
-      st[en.y] = v;
+      st[en.y] = to_elem<C>(v.x, v.y);
     }
   }
   if (bad) atomicOr(t.err, 1);
@@ -108,7 +136,7 @@ __global__ void __launch_bounds__(N == 0 ? 256 : 128, N == 0 ? 1 : 6) k_sticks_i
     __syncthreads();
     fast::pass<N, 1, 1>(st, cnt, LineOffStride{fast::pitch_of<N>()}, tw);
   }
-  double2* out = t.sbuf + (int64_t)unit * g.n2 * t.S + s0;
+  C* out = sticks_of<C>(t) + (int64_t)unit * g.n2 * t.S + s0;
   for (int i = threadIdx.x; i < cnt * g.n2; i += blockDim.x) {
     const int z = i / cnt, sl = i - z * cnt;
     out[(int64_t)z * t.S + sl] = st[sl * g.ld2 + z];
@@ -150,36 +178,42 @@ __global__ void __launch_bounds__(512) k_planes(const OpTables* __restrict__ tab
 
 // Cubic grids with a compile-time plan: the x pass runs inverse, x V(r) and forward on
 // each warp's column group without a block barrier in between.
-template <int N>
+template <int N, class C = double2>
 __global__ void __launch_bounds__(256, 4) k_planes_fast(const OpTables* __restrict__ tabs, BoxGeo g, Batch b) {
+  using T = RealOf<C>;
   const OpTables& t = tabs[blockIdx.z];
   const CallArgs a = resolve(b.a[blockIdx.z]);
   const int unit = blockIdx.x, z = blockIdx.y;
   if (unit >= a.units) return;
   constexpr int P = fast::pitch_of<N>();
-  constexpr bool VS = v_in_smem(N);
-  extern __shared__ double2 sm[];
-  double2* tw = sm;
-  double2* pl = sm + N;
-  double* vs = reinterpret_cast<double*>(pl + N * P);   // V(r) of this plane, [y][x]
+  constexpr bool VS = v_in_smem_t<C>(N);
+  constexpr int EPC = 16 / (int)sizeof(T);  // potential values per 16-byte copy
+  extern __shared__ __align__(16) unsigned char pf_raw[];
+  C* tw = reinterpret_cast<C*>(pf_raw);
+  C* pl = tw + N;
+  T* vs = reinterpret_cast<T*>(pl + N * P);   // V(r) of this plane, [y][x]
   int* rows = reinterpret_cast<int*>(vs + (VS ? N * N : 0));
   const int nx = t.nxact;
-  // V(r) of the plane arrives asynchronously while the y pass runs (16-byte cp.async).
-  const double* v = (a.vt ? a.vt : t.vt) + (int64_t)z * g.vstride;  // 16-byte aligned: vstride is even
+  // V(r) of the plane arrives asynchronously while the y pass runs (16-byte cp.async;
+  // the plane strides keep every plane 16-byte aligned)
+  const T* v;
+  if constexpr (sizeof(T) == sizeof(double))
+    v = reinterpret_cast<const T*>((a.vt ? a.vt : t.vt) + (int64_t)z * g.vstride);
+  else
+    v = reinterpret_cast<const T*>(t.vtf + (int64_t)z * g.vstridef);
   if constexpr (VS) {
     const unsigned dst = static_cast<unsigned>(__cvta_generic_to_shared(vs));
-    for (int i = threadIdx.x; i < N * N / 2; i += blockDim.x)
-      asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst + 16u * i), "l"(v + 2 * i));
-    if ((N * N) & 1) {
-      if (threadIdx.x == 0) vs[N * N - 1] = v[N * N - 1];
-    }
+    for (int i = threadIdx.x; i < N * N / EPC; i += blockDim.x)
+      asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst + 16u * i), "l"(v + EPC * i));
+    for (int i = (N * N / EPC) * EPC + threadIdx.x; i < N * N; i += blockDim.x) vs[i] = v[i];
     asm volatile("cp.async.commit_group;\n" ::);
   }
-  for (int i = threadIdx.x; i < N; i += blockDim.x) tw[i] = g.tw0[i];
+  const C* twg = tw_axis<C>(g, 0);
+  for (int i = threadIdx.x; i < N; i += blockDim.x) tw[i] = twg[i];
   for (int i = threadIdx.x; i < nx; i += blockDim.x) rows[i] = t.xact[i] * P;
-  for (int i = threadIdx.x; i < N * P; i += blockDim.x) pl[i] = make_double2(0.0, 0.0);
+  for (int i = threadIdx.x; i < N * P; i += blockDim.x) pl[i] = to_elem<C>(0.0, 0.0);
   __syncthreads();
-  double2* row = t.sbuf + ((int64_t)unit * N + z) * t.S;
+  C* row = sticks_of<C>(t) + ((int64_t)unit * N + z) * t.S;
   for (int s = threadIdx.x; s < t.S; s += blockDim.x) pl[t.stick_plane[s]] = row[s];
   __syncthreads();
   fast::pass<N, 1, 1>(pl, nx, LineOffTable{rows}, tw);
@@ -191,14 +225,14 @@ __global__ void __launch_bounds__(256, 4) k_planes_fast(const OpTables* __restri
   if (count > 0) {
     if constexpr (fast::Plan<N>::nst == 2) {
       // line = column y, element = x: weight V(x, y, z)
-      auto wgt = [&](int y, int x) -> double { return VS ? vs[y * N + x] : v[y * N + x]; };
+      auto wgt = [&](int y, int x) -> T { return VS ? vs[y * N + x] : v[y * N + x]; };
       fast::inverse_weight_forward<N, P>(pl, first, count, LineOffCols{}, tw, wgt, lane);
     } else {
       fast::group<N, 1, P>(pl, first, count, LineOffCols{}, tw, lane);
       for (int e = lane; e < count * N; e += 32) {
         const int li = e / N, x = e - li * N, y = first + li;
-        const double w = VS ? vs[y * N + x] : v[y * N + x];
-        double2& p = pl[x * P + y];
+        const T w = VS ? vs[y * N + x] : v[y * N + x];
+        C& p = pl[x * P + y];
         p.x *= w;
         p.y *= w;
       }
@@ -212,18 +246,20 @@ __global__ void __launch_bounds__(256, 4) k_planes_fast(const OpTables* __restri
 }
 
 // ---------------------------------------------------------------- pass 3
-template <bool GAMMA, int N>
+template <bool GAMMA, int N, class C = double2>
 __global__ void __launch_bounds__(N == 0 ? 256 : 128, N == 0 ? 1 : 6) k_sticks_forward(const OpTables* __restrict__ tabs, BoxGeo g, Batch b) {
+  static_assert(N != 0 || sizeof(C) == sizeof(double2), "the runtime-plan engine is FP64 only");
   const OpTables& t = tabs[blockIdx.z];
   const CallArgs a = resolve(b.a[blockIdx.z]);
   const int grp = blockIdx.x, unit = blockIdx.y;
   if (grp >= t.ngroups || unit >= a.units) return;
-  extern __shared__ double2 sm[];
-  double2* tw = sm;
-  double2* st = sm + g.n2;
+  extern __shared__ __align__(16) unsigned char sf_raw[];
+  C* tw = reinterpret_cast<C*>(sf_raw);
+  C* st = tw + g.n2;
   const int s0 = t.grp_stick[grp], cnt = t.grp_stick[grp + 1] - s0;
-  for (int i = threadIdx.x; i < g.n2; i += blockDim.x) tw[i] = g.tw2[i];
-  const double2* in = t.sbuf + (int64_t)unit * g.n2 * t.S + s0;
+  const C* twg = tw_axis<C>(g, 2);
+  for (int i = threadIdx.x; i < g.n2; i += blockDim.x) tw[i] = twg[i];
+  const C* in = sticks_of<C>(t) + (int64_t)unit * g.n2 * t.S + s0;
   for (int i = threadIdx.x; i < cnt * g.n2; i += blockDim.x) {
     const int z = i / cnt, sl = i - z * cnt;
     st[sl * g.ld2 + z] = in[(int64_t)z * t.S + sl];
@@ -243,7 +279,7 @@ __global__ void __launch_bounds__(N == 0 ? 256 : 128, N == 0 ? 1 : 6) k_sticks_f
       double2* y = reinterpret_cast<double2*>(a.y + (int64_t)unit * a.ldy);
       for (int e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
         const int2 en = t.entries[e];
-        const double2 h = st[en.y];
+        const double2 h = make_double2(st[en.y].x, st[en.y].y);
         const double2 old = y[en.x];
         bad |= !finite2(old.x, old.y);
         y[en.x] = make_double2(old.x + h.x * s, old.y + h.y * s);
@@ -257,7 +293,7 @@ __global__ void __launch_bounds__(N == 0 ? 256 : 128, N == 0 ? 1 : 6) k_sticks_f
       for (int e = r0 + threadIdx.x; e < r1; e += blockDim.x) {
         const int4 rp = t.reps[e];
         const int r = rp.x;
-        double2 hp = st[rp.y];
+        double2 hp = make_double2(st[rp.y].x, st[rp.y].y);
         hp.x *= s;
         hp.y *= s;
         if (r == 0) {
@@ -268,7 +304,7 @@ __global__ void __launch_bounds__(N == 0 ? 256 : 128, N == 0 ? 1 : 6) k_sticks_f
             yb[0] += hp.y;
           }
         } else {
-          double2 hm = st[rp.z];
+          double2 hm = make_double2(st[rp.z].x, st[rp.z].y);
           hm.x *= s;
           hm.y *= s;
           const double ex = 0.5 * (hp.x + hm.x), ey = 0.5 * (hp.y - hm.y);
@@ -291,7 +327,7 @@ __global__ void __launch_bounds__(N == 0 ? 256 : 128, N == 0 ? 1 : 6) k_sticks_f
     double2* y = reinterpret_cast<double2*>(a.y + (int64_t)unit * a.ldy);
     for (int e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
       const int2 en = t.entries[e];
-      const double2 h = st[en.y];
+      const double2 h = make_double2(st[en.y].x, st[en.y].y);
       const double tk = t.kinetic[en.x];
       const double2 xv = x[en.x];
       y[en.x] = make_double2(h.x * s + tk * xv.x, h.y * s + tk * xv.y);
@@ -307,7 +343,7 @@ __global__ void __launch_bounds__(N == 0 ? 256 : 128, N == 0 ? 1 : 6) k_sticks_f
     for (int e = r0 + threadIdx.x; e < r1; e += blockDim.x) {
       const int4 rp = t.reps[e];
       const int r = rp.x;
-      double2 hp = st[rp.y];
+      double2 hp = make_double2(st[rp.y].x, st[rp.y].y);
       hp.x *= s;
       hp.y *= s;
       if (r == 0) {
@@ -315,7 +351,7 @@ __global__ void __launch_bounds__(N == 0 ? 256 : 128, N == 0 ? 1 : 6) k_sticks_f
         ya[0] = hp.x + tk * xa[0];
         if (hasb) yb[0] = hp.y + tk * xb[0];
       } else {
-        double2 hm = st[rp.z];
+        double2 hm = make_double2(st[rp.z].x, st[rp.z].y);
         hm.x *= s;
         hm.y *= s;
         // even = (hp + conj hm)/2, odd = (hp - conj hm)/2
@@ -552,6 +588,19 @@ size_t plane_smem_bytes(const BoxGeo& g) {
          (vs ? sizeof(double) * (size_t)g.n0 * g.n1 : 0) + sizeof(int) * (size_t)g.n0;
 }
 size_t stick_smem_bytes(const BoxGeo& g) { return sizeof(double2) * ((size_t)g.n2 + (size_t)g.sg * g.ld2); }
+static size_t plane_smem_bytes_f32(const BoxGeo& g) {
+  return sizeof(float2) * ((size_t)g.n0 + (size_t)g.n0 * g.pitch) +
+         (v_in_smem_t<float2>(g.n0) ? sizeof(float) * (size_t)g.n0 * g.n1 : 0) + sizeof(int) * (size_t)g.n0;
+}
+static size_t stick_smem_bytes_f32(const BoxGeo& g) { return sizeof(float2) * ((size_t)g.n2 + (size_t)g.sg * g.ld2); }
+
+bool fp32_supported(const BoxGeo& g) {
+  if (g.n0 != g.n1 || g.n1 != g.n2) return false;
+  switch (g.n2) {
+    case 25: case 45: case 54: case 60: case 72: case 108: return true;
+    default: return false;
+  }
+}
 
 namespace {
 struct StageScope {
@@ -567,51 +616,81 @@ struct StageScope {
 };
 }  // namespace
 
-template <bool GAMMA, int N>
+template <bool GAMMA, int N, class C>
 static void local_kernels(const OpTables* tabs, const BoxGeo& g, const Batch& b, dim3 sgrid, dim3 pgrid, size_t ss,
                           size_t ps, cudaStream_t s, StageEvents* ev) {
   constexpr int st = N == 0 ? 256 : 128;
-  { StageScope sc(ev, 0, s); k_sticks_inverse<GAMMA, N><<<sgrid, st, ss, s>>>(tabs, g, b); }
-  if constexpr (N == 0) {
-    StageScope sc(ev, 1, s);
-    k_planes<<<pgrid, 512, ps, s>>>(tabs, g, b);
+  if constexpr (N == 0 && sizeof(C) != sizeof(double2)) {
+    return;  // the FP32 apply needs a compile-time plan (checked by the callers)
   } else {
-    StageScope sc(ev, 1, s);
-    if (g.n0 == N && g.n1 == N)
-      k_planes_fast<N><<<pgrid, 256, ps, s>>>(tabs, g, b);
-    else
+    { StageScope sc(ev, 0, s); k_sticks_inverse<GAMMA, N, C><<<sgrid, st, ss, s>>>(tabs, g, b); }
+    if constexpr (N == 0) {
+      StageScope sc(ev, 1, s);
       k_planes<<<pgrid, 512, ps, s>>>(tabs, g, b);
+    } else {
+      StageScope sc(ev, 1, s);
+      if (g.n0 == N && g.n1 == N)
+        k_planes_fast<N, C><<<pgrid, 256, ps, s>>>(tabs, g, b);
+      else if constexpr (sizeof(C) == sizeof(double2))
+        k_planes<<<pgrid, 512, ps, s>>>(tabs, g, b);
+    }
+    { StageScope sc(ev, 2, s); k_sticks_forward<GAMMA, N, C><<<sgrid, st, ss, s>>>(tabs, g, b); }
   }
-  { StageScope sc(ev, 2, s); k_sticks_forward<GAMMA, N><<<sgrid, st, ss, s>>>(tabs, g, b); }
 }
 
-template <bool GAMMA>
+template <bool GAMMA, class C>
 static void local_dispatch(const OpTables* tabs, const BoxGeo& g, const Batch& b, dim3 sgrid, dim3 pgrid, size_t ss,
                            size_t ps, cudaStream_t s, StageEvents* ev) {
   switch (g.n2) {
-    case 25: local_kernels<GAMMA, 25>(tabs, g, b, sgrid, pgrid, ss, ps, s, ev); break;
-    case 45: local_kernels<GAMMA, 45>(tabs, g, b, sgrid, pgrid, ss, ps, s, ev); break;
-    case 54: local_kernels<GAMMA, 54>(tabs, g, b, sgrid, pgrid, ss, ps, s, ev); break;
-    case 60: local_kernels<GAMMA, 60>(tabs, g, b, sgrid, pgrid, ss, ps, s, ev); break;
-    case 72: local_kernels<GAMMA, 72>(tabs, g, b, sgrid, pgrid, ss, ps, s, ev); break;
-    case 108: local_kernels<GAMMA, 108>(tabs, g, b, sgrid, pgrid, ss, ps, s, ev); break;
-    default: local_kernels<GAMMA, 0>(tabs, g, b, sgrid, pgrid, ss, ps, s, ev); break;
+    case 25: local_kernels<GAMMA, 25, C>(tabs, g, b, sgrid, pgrid, ss, ps, s, ev); break;
+    case 45: local_kernels<GAMMA, 45, C>(tabs, g, b, sgrid, pgrid, ss, ps, s, ev); break;
+    case 54: local_kernels<GAMMA, 54, C>(tabs, g, b, sgrid, pgrid, ss, ps, s, ev); break;
+    case 60: local_kernels<GAMMA, 60, C>(tabs, g, b, sgrid, pgrid, ss, ps, s, ev); break;
+    case 72: local_kernels<GAMMA, 72, C>(tabs, g, b, sgrid, pgrid, ss, ps, s, ev); break;
+    case 108: local_kernels<GAMMA, 108, C>(tabs, g, b, sgrid, pgrid, ss, ps, s, ev); break;
+    default: local_kernels<GAMMA, 0, C>(tabs, g, b, sgrid, pgrid, ss, ps, s, ev); break;
   }
 }
 
 int launch_local(const OpTables* tabs, int gamma, int max_groups, const BoxGeo& g, const Batch& b, cudaStream_t s,
-                 StageEvents* ev) {
+                 StageEvents* ev, int fp32) {
   int max_units = 0;
   for (int k = 0; k < b.nk; ++k) max_units = max(max_units, b.a[k].units);
   if (max_units == 0 || b.nk == 0) return 0;
-  const size_t ss = stick_smem_bytes(g), ps = plane_smem_bytes(g);
   const dim3 sgrid(max_groups, max_units, b.nk);
   const dim3 pgrid(max_units, g.n2, b.nk);
+  if (fp32) {
+    if (!fp32_supported(g)) return 0;
+    const size_t ss = stick_smem_bytes_f32(g), ps = plane_smem_bytes_f32(g);
+    if (gamma)
+      local_dispatch<true, float2>(tabs, g, b, sgrid, pgrid, ss, ps, s, ev);
+    else
+      local_dispatch<false, float2>(tabs, g, b, sgrid, pgrid, ss, ps, s, ev);
+    return 3;
+  }
+  const size_t ss = stick_smem_bytes(g), ps = plane_smem_bytes(g);
   if (gamma)
-    local_dispatch<true>(tabs, g, b, sgrid, pgrid, ss, ps, s, ev);
+    local_dispatch<true, double2>(tabs, g, b, sgrid, pgrid, ss, ps, s, ev);
   else
-    local_dispatch<false>(tabs, g, b, sgrid, pgrid, ss, ps, s, ev);
+    local_dispatch<false, double2>(tabs, g, b, sgrid, pgrid, ss, ps, s, ev);
   return 3;
+}
+
+// vtf[z vsf + q] = (float) vt[z vs + q], q < n0 n1.
+__global__ void k_potential_float(const double* __restrict__ vt, int vs, float* __restrict__ vtf, int vsf, int plane,
+                                  int n2) {
+  const int64_t total = (int64_t)plane * n2;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t z = t / plane, q = t - z * plane;
+    vtf[z * vsf + q] = (float)vt[z * vs + q];
+  }
+}
+
+void launch_potential_float(const double* vt, const BoxGeo& g, float* vtf, cudaStream_t s) {
+  const int plane = g.n0 * g.n1;
+  const int64_t total = (int64_t)plane * g.n2;
+  const int blocks = (int)std::min<int64_t>((total + 255) / 256, 148 * 8);
+  k_potential_float<<<blocks, 256, 0, s>>>(vt, g.vstride, vtf, g.vstridef, plane, g.n2);
 }
 
 size_t density_smem_bytes(const BoxGeo& g) {
@@ -711,6 +790,12 @@ static void configure_one(cudaError_t& e, size_t plane_smem, size_t stick_smem) 
   if constexpr (N != 0) {
     set((const void*)k_planes_fast<N>, plane_smem);
     carve((const void*)k_planes_fast<N>);
+    set((const void*)k_planes_fast<N, float2>, plane_smem);
+    carve((const void*)k_planes_fast<N, float2>);
+    set((const void*)k_sticks_inverse<GAMMA, N, float2>, stick_smem);
+    set((const void*)k_sticks_forward<GAMMA, N, float2>, stick_smem);
+    carve((const void*)k_sticks_inverse<GAMMA, N, float2>);
+    carve((const void*)k_sticks_forward<GAMMA, N, float2>);
     if constexpr (GAMMA) {
       set((const void*)k_density_planes_fast<N>, plane_smem);
       carve((const void*)k_density_planes_fast<N>);

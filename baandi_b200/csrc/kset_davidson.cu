@@ -151,6 +151,7 @@ struct Opts {
   double threshold;
   int preconditioner;
   int smem_matrices;  // the control kernel keeps A, Y, Q, Z in shared memory
+  int fp32;           // H applies with the FP32 local part
 };
 
 // ------------------------------------------------------------------ block-wide small algebra
@@ -1009,6 +1010,13 @@ class KsetSolver {
   bool matches(int n, int cap) const { return o_.n == n && o_.cap == cap; }
   // Per-call options (threshold, occupied, first_step, iterations, preconditioner).
   void set_options(const Opts& o, bool graph) {
+    if (prepared_ && o.fp32 != o_.fp32 && exec_) {  // the captured graph holds the apply's kernels
+      cudaGraphExecDestroy(exec_);
+      cudaGraphDestroy(graph_);
+      exec_ = nullptr;
+      graph_ = nullptr;
+      graph_tried_ = false;
+    }
     o_ = o;
     o_.smem_matrices = small(o.cap) ? 1 : 0;
     want_graph_ = graph;
@@ -1111,7 +1119,7 @@ class KsetSolver {
       k_dv_dense<D><<<grid, 128, 0, s_>>>(d_dense_, d_bufs_, d_dyn_);
       return 1;
     }
-    return enqueue_range(ks_, 0, nk_, args_.data(), cols_.data(), s_, nullptr);
+    return enqueue_range(ks_, 0, nk_, args_.data(), cols_.data(), s_, nullptr, o_.fp32);
   }
   int64_t iteration() {
     int64_t l = 0;
@@ -1377,7 +1385,12 @@ extern "C" int bg_kset_davidson_solve(bg_kset* ks, const double* const* start, c
   }
   cudaError_t e = cudaSetDevice(ctx->device);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaSetDevice");
-  Opts op{(int)n, (int)cap, (int)o.occupied, o.first_step ? 1 : 0, o.max_iterations, o.threshold, o.preconditioner, 0};
+  if (o.apply_precision != BG_PREC_FP64 && o.apply_precision != BG_PREC_FP32)
+    return fail(ctx, BG_EINVAL, "unsupported apply precision");
+  if (o.apply_precision == BG_PREC_FP32 && (ks->dense || !fp32_supported(ks->g)))
+    return fail(ctx, BG_EINVAL, "the FP32 apply needs a cubic grid of 25, 45, 54, 60, 72 or 108 points");
+  Opts op{(int)n, (int)cap, (int)o.occupied, o.first_step ? 1 : 0, o.max_iterations, o.threshold, o.preconditioner, 0,
+          o.apply_precision == BG_PREC_FP32 ? 1 : 0};
   const bool graph = (o.flags & 1) == 0;
   int rc;
   std::string err;

@@ -91,7 +91,7 @@ namespace bg {
 // Launch the local and nonlocal stages of operators [k0, k1) of a set on one stream
 // (cols[k]: the widest block of operator k, used to size the grids).
 int enqueue_range(bg_kset* ks, int k0, int k1, const CallArgs* args, const int64_t* cols, cudaStream_t s,
-                  StageEvents* ev);
+                  StageEvents* ev, int fp32 = 0);
 // Failure message on the context (or the thread's context-free slot) and status.
 int fail(bg_ctx* ctx, int code, const std::string& msg);
 int cuda_fail(bg_ctx* ctx, cudaError_t e, const char* what);

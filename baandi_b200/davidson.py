@@ -26,6 +26,7 @@ class Options:
     capacity: int = 0
     max_iterations: int = 20
     preconditioner: str = "smooth"   # "smooth" (reference Davidson), "tpa", "ritz_shift"
+    apply_precision: str = "fp64"    # "fp64", or "fp32" (the local part of every H apply in FP32)
 
     def band_threshold(self, band: int) -> float:
         if self.first_step or band < self.occupied:
@@ -61,8 +62,11 @@ PRECONDITIONERS = {"smooth": L.BG_PRECOND_SMOOTH, "tpa": L.BG_PRECOND_TPA, "ritz
 def _options(options: Options, flags: int = 0):
     if options.preconditioner not in PRECONDITIONERS:
         raise SolverError(L.BG_EINVAL, f"preconditioner {options.preconditioner!r}")
+    if options.apply_precision not in ("fp64", "fp32"):
+        raise SolverError(L.BG_EINVAL, f"apply precision {options.apply_precision!r}")
     return L.DavidsonOptions(options.bands, options.threshold, options.occupied, 1 if options.first_step else 0,
-                             options.capacity, options.max_iterations, flags, PRECONDITIONERS[options.preconditioner])
+                             options.capacity, options.max_iterations, flags, PRECONDITIONERS[options.preconditioner],
+                             L.BG_PREC_FP32 if options.apply_precision == "fp32" else L.BG_PREC_FP64)
 
 
 def solve(operator: _Operator, start: np.ndarray, hamiltonian_diagonal: np.ndarray, options: Options) -> Solution:

@@ -248,9 +248,11 @@ class _Operator:
         return self._gamma
 
     # -- apply
+    precision = L.BG_PREC_FP64   # BG_PREC_FP32: the local part of apply_block in FP32
+
     def _apply_raw(self, x_ptr, y_ptr, cols, kind):
         self._check(self._lib.bg_op_apply_block(self.handle, ctypes.c_void_p(x_ptr), ctypes.c_void_p(y_ptr),
-                                                self.npw, int(cols), kind, L.BG_PREC_FP64))
+                                                self.npw, int(cols), kind, self.precision))
 
 
 class ComplexHamiltonian(_Operator):
@@ -336,6 +338,8 @@ class KPointSet:
     (crates/dft-engine/src/refscf/k_map.rs:136-210); results are identical to the
     per-operator applies."""
 
+    precision = L.BG_PREC_FP64   # BG_PREC_FP32: the local part of every apply in FP32
+
     def __init__(self, ops, ctx: Context | None = None):
         self.ctx = ctx or ops[0].ctx
         self._lib = self.ctx._lib
@@ -358,7 +362,7 @@ class KPointSet:
         ca = (ctypes.c_int64 * n)(*[int(c) for c in cols])
         self._check(self._lib.bg_kset_apply(self.handle, ctypes.cast(xa, ctypes.c_void_p),
                                             ctypes.cast(ya, ctypes.c_void_p), ctypes.cast(ca, ctypes.c_void_p),
-                                            kind, L.BG_PREC_FP64))
+                                            kind, self.precision))
 
     def apply_blocks(self, xs, outs=None):
         """Host blocks (list of Fortran-ordered arrays, one per operator) -> list of H x."""

@@ -42,8 +42,12 @@ extern "C" {
 #define BG_PTR_HOST 0   /* synchronous: copies in, applies, copies out, validates   */
 #define BG_PTR_DEVICE 1 /* asynchronous on the operator's stream                    */
 
-/* arithmetic of bg_op_apply_block */
+/* arithmetic of bg_op_apply_block: FP64, or the precision form with the local part
+ * (scatter, 3D transforms, x V(r), gather) in FP32 on the element stream and the
+ * kinetic and nonlocal parts in FP64; blocks stay FP64 in memory.  FP32 needs a cubic
+ * grid of 25, 45, 54, 60, 72 or 108 points. */
 #define BG_PREC_FP64 0
+#define BG_PREC_FP32 1
 
 typedef struct bg_ctx bg_ctx;
 typedef struct bg_op bg_op;
@@ -268,7 +272,8 @@ typedef struct {
   int32_t max_iterations; /* correction iterations (reference default 20)               */
   int32_t flags;          /* bg_kset_davidson_solve: bit 0 launches directly (no graph)  */
   int32_t preconditioner; /* BG_PRECOND_*                                                */
-  int32_t reserved[2];
+  int32_t apply_precision; /* BG_PREC_* of the solver's H applies                        */
+  int32_t reserved[1];
 } bg_davidson_options;
 
 /* Correction of band j from its residual r = HX_j - lambda_j X_j on row g (the
