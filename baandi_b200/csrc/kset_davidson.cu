@@ -1009,21 +1009,18 @@ class KsetSolver {
   }
   bool matches(int n, int cap) const { return o_.n == n && o_.cap == cap; }
   // Per-call options (threshold, occupied, first_step, iterations, preconditioner).
+  // The captured iteration holds the apply's kernels, so each apply precision keeps a
+  // graph of its own.
   void set_options(const Opts& o, bool graph) {
-    if (prepared_ && o.fp32 != o_.fp32 && exec_) {  // the captured graph holds the apply's kernels
-      cudaGraphExecDestroy(exec_);
-      cudaGraphDestroy(graph_);
-      exec_ = nullptr;
-      graph_ = nullptr;
-      graph_tried_ = false;
-    }
     o_ = o;
     o_.smem_matrices = small(o.cap) ? 1 : 0;
     want_graph_ = graph;
   }
   ~KsetSolver() {
-    if (exec_) cudaGraphExecDestroy(exec_);
-    if (graph_) cudaGraphDestroy(graph_);
+    for (int p = 0; p < 2; ++p) {
+      if (exec_[p]) cudaGraphExecDestroy(exec_[p]);
+      if (graph_[p]) cudaGraphDestroy(graph_[p]);
+    }
     for (void* p : dev_) cudaFree(p);
     if (h_ctl_) cudaFreeHost(h_ctl_);
   }
@@ -1038,7 +1035,7 @@ class KsetSolver {
   Opts o_;
   bool want_graph_ = true;
   bool prepared_ = false;
-  bool graph_tried_ = false;
+  bool graph_tried_[2] = {false, false};   // by apply precision (0 FP64, 1 FP32)
   Opts* d_opts_ = nullptr;
   cudaStream_t s_ = nullptr;
   std::vector<void*> dev_;
@@ -1056,9 +1053,9 @@ class KsetSolver {
   int max_rows_ = 0;
   std::vector<CallArgs> args_;
   std::vector<int64_t> cols_;
-  cudaGraph_t graph_ = nullptr;
-  cudaGraphExec_t exec_ = nullptr;
-  int64_t per_iteration_ = 0;
+  cudaGraph_t graph_[2] = {nullptr, nullptr};
+  cudaGraphExec_t exec_[2] = {nullptr, nullptr};
+  int64_t per_iteration_[2] = {0, 0};
   int64_t launches_ = 0;
   std::string err_;
 
@@ -1266,27 +1263,28 @@ int KsetSolver<T>::run(const double* const* start, const double* const* diagonal
   bool done = false;
   if ((rc = poll(&done))) return rc;
   // iterations: one captured graph replayed until every k point has finished
-  if (want_graph_ && !graph_tried_) {
-    graph_tried_ = true;
+  const int gp = o_.fp32 ? 1 : 0;
+  if (want_graph_ && !graph_tried_[gp]) {
+    graph_tried_[gp] = true;
     cudaStreamCaptureStatus st;
     if (cudaStreamIsCapturing(s_, &st) == cudaSuccess && st == cudaStreamCaptureStatusNone &&
         cudaStreamBeginCapture(s_, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
       const int64_t per = iteration();
-      if (cudaStreamEndCapture(s_, &graph_) == cudaSuccess && graph_ &&
-          cudaGraphInstantiate(&exec_, graph_, 0) == cudaSuccess)
-        per_iteration_ = per;
-      else if (exec_) {
-        cudaGraphExecDestroy(exec_);
-        exec_ = nullptr;
+      if (cudaStreamEndCapture(s_, &graph_[gp]) == cudaSuccess && graph_[gp] &&
+          cudaGraphInstantiate(&exec_[gp], graph_[gp], 0) == cudaSuccess)
+        per_iteration_[gp] = per;
+      else if (exec_[gp]) {
+        cudaGraphExecDestroy(exec_[gp]);
+        exec_[gp] = nullptr;
       }
     }
     cudaGetLastError();
   }
-  const bool graph_ok = want_graph_ && exec_ != nullptr;
+  const bool graph_ok = want_graph_ && exec_[gp] != nullptr;
   for (int it = 0; it < o_.max_iterations && !done; ++it) {
     if (graph_ok) {
-      if ((rc = cuda(cudaGraphLaunch(exec_, s_), "cudaGraphLaunch"))) return rc;
-      launches_ += per_iteration_;
+      if ((rc = cuda(cudaGraphLaunch(exec_[gp], s_), "cudaGraphLaunch"))) return rc;
+      launches_ += per_iteration_[gp];
     } else {
       launches_ += iteration();
     }

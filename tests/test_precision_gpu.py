@@ -76,3 +76,18 @@ def test_fp32_needs_a_compile_time_grid(ctx):
     op.precision = L.BG_PREC_FP32
     with pytest.raises(SolverError):
         op.apply_block(w.random_block(pw.npw, 4))
+
+
+def test_scf_with_fp32_early_maps_reaches_the_fp64_energy(ctx):
+    """Si2 Gamma SCF to 1e-8 Ha with FP32 applies in the maps whose ethr is at least
+    1e-5 Ry: the converged energy equals the FP64 run's within 1e-7 Ha/atom, and the
+    early maps did run in FP32."""
+    from baandi_b200.scf import GpuScf, ScfOptions
+    w = W.si2_gamma()
+    plain = GpuScf(w, ctx, ScfOptions(threshold_ha=1e-8, smearing_ha=0.01)).run()
+    tuned = GpuScf(w, ctx, ScfOptions(threshold_ha=1e-8, smearing_ha=0.01, fp32_ethr_ry=1e-5)).run()
+    assert plain.converged and tuned.converged
+    assert any(r.precision == "fp32" for r in tuned.records)
+    assert tuned.records[-1].precision == "fp64"
+    assert abs(tuned.energy_ha - plain.energy_ha) <= 1e-7 * w.natoms
+    assert abs(tuned.iterations - plain.iterations) <= 2
