@@ -257,16 +257,23 @@ int build_op(bg_ctx* ctx, const bg_basis_desc* b, const bg_projectors* pr, int64
       grp_rep.push_back((int)(reps.size() / 4));
     }
   }
-  std::vector<int> stick_plane(S), xact;
+  std::vector<int> stick_plane(S), xact, line_stick;
+  unsigned xbits[4] = {0u, 0u, 0u, 0u};
   {
     std::vector<char> xs(n0, 0);
+    std::vector<int> at((size_t)n0 * n1, -1);
     for (int s = 0; s < S; ++s) {
       const int x = (int)(order[s] / n1), y = (int)(order[s] % n1);
       stick_plane[s] = x * G.pitch + y;
+      at[(size_t)x * n1 + y] = s;
       xs[x] = 1;
     }
     for (int x = 0; x < n0; ++x)
-      if (xs[x]) xact.push_back(x);
+      if (xs[x]) {
+        xact.push_back(x);
+        line_stick.insert(line_stick.end(), at.begin() + (size_t)x * n1, at.begin() + (size_t)(x + 1) * n1);
+        xbits[x >> 5] |= 1u << (x & 31);
+      }
   }
 
   // kinetic in row order (Gamma: ORC order, each pair row carries its representative's value)
@@ -302,6 +309,9 @@ int build_op(bg_ctx* ctx, const bg_basis_desc* b, const bg_projectors* pr, int64
   T.stick_plane = d_int;
   if ((rc = upload(op.get(), xact.data(), xact.size(), &d_int))) return rc;
   T.xact = d_int;
+  if ((rc = upload(op.get(), line_stick.data(), line_stick.size(), &d_int))) return rc;
+  T.line_stick = d_int;
+  for (int w = 0; w < 4; ++w) T.xbits[w] = xbits[w];
   double* d_dbl;
   if ((rc = upload(op.get(), kin.data(), kin.size(), &d_dbl))) return rc;
   T.kinetic = d_dbl;

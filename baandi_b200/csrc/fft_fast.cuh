@@ -210,37 +210,78 @@ __device__ __forceinline__ int lane_id() {
   return l;
 }
 
+// Where a stage reads its inputs and writes its outputs.  IO = 0: the warp's lines in
+// shared memory (base + off(line) + element ES).  Bits of IO change one side:
+//   kInGlobal   inputs of line i from the stick row in global memory: element e is
+//               row[tab[i N + e]], zero where tab holds -1 (no stick at that position)
+//   kOutGlobal  outputs of line i to row[tab[i N + e]], dropped where tab holds -1
+//   kInMask     inputs at elements whose bit is clear in xb are zero (not loaded)
+//   kOutMask    outputs at elements whose bit is clear in xb are not stored
+constexpr int kInGlobal = 1, kOutGlobal = 2, kInMask = 4, kOutMask = 8;
+template <class C>
+struct StageIo {
+  const int* tab = nullptr;
+  C* row = nullptr;
+  const unsigned* xb = nullptr;  // element bits (4 words, N <= 128)
+};
+
+__device__ __forceinline__ unsigned xbit(const unsigned* xb, int e) { return (__ldg(xb + (e >> 5)) >> (e & 31)) & 1u; }
+
 // Stage (R, NS) on lines first .. first+count-1 of this warp; ES = element stride.
-// A lane's butterfly index j is the same in every round.
-template <int N, int R, int NS, int SIGN, int ES, class Off, class C>
-__device__ __forceinline__ void stage(C* base, int first, int count, Off off, const C* __restrict__ tw, int lane) {
+// A lane's butterfly index j, its twiddle and its element masks are the same in every
+// round, so they are set up once before the rounds.
+template <int N, int R, int NS, int SIGN, int ES, int IO = 0, class Off, class C>
+__device__ __forceinline__ void stage(C* base, int first, int count, Off off, const C* __restrict__ tw, int lane,
+                                      const StageIo<C>& io = StageIo<C>{}) {
   constexpr int SPAN = N / R;
   constexpr int STEP = N / (NS * R);
   constexpr int K = (SPAN + 31) / 32;                 // butterflies per lane when a line exceeds a warp
   constexpr int LPR = SPAN <= 32 ? 32 / SPAN : 1;     // whole lines per round
   lane = lane_id();
-  int jj[K], li[K], oo[K], kk[K];
+  int jj[K], li[K], oo[K];
+  unsigned tin[K], tout[K];
+  int kk[K];
 #pragma unroll
   for (int q = 0; q < K; ++q) {
     const int slot = lane + 32 * q;
     li[q] = K == 1 ? slot / SPAN : 0;
     jj[q] = K == 1 ? slot - li[q] * SPAN : slot;
     if (K == 1 ? li[q] >= LPR : jj[q] >= SPAN) li[q] = 1 << 20;  // idle lane
-    const int j = jj[q];
+    const int j = jj[q] < SPAN ? jj[q] : 0;
     const int k = NS > 1 ? j % NS : 0;
     oo[q] = (NS > 1 ? (j / NS) * NS * R : j * R) + k;
     kk[q] = k * STEP;
+    tin[q] = tout[q] = 0u;
+    if constexpr ((IO & kInMask) != 0) {
+#pragma unroll
+      for (int t = 0; t < R; ++t) tin[q] |= xbit(io.xb, j + t * SPAN) << t;
+    }
+    if constexpr ((IO & kOutMask) != 0) {
+#pragma unroll
+      for (int u = 0; u < R; ++u) tout[q] |= xbit(io.xb, oo[q] + u * NS) << u;
+    }
   }
   for (int r0 = 0; r0 < count; r0 += LPR) {
     C v[K][R];
-    int lo[K];
+    int lo[K], ln[K];
 #pragma unroll
     for (int q = 0; q < K; ++q) {
       const bool act = r0 + li[q] < count;
-      lo[q] = act ? off(first + r0 + li[q]) : -1;
+      ln[q] = first + r0 + li[q];
+      lo[q] = act ? off(ln[q]) : -1;
       if (act) {
+        if constexpr ((IO & kInGlobal) != 0) {
+          int sidx[R];
 #pragma unroll
-        for (int t = 0; t < R; ++t) v[q][t] = base[lo[q] + (jj[q] + t * SPAN) * ES];
+          for (int t = 0; t < R; ++t) sidx[t] = __ldg(io.tab + ln[q] * N + jj[q] + t * SPAN);
+#pragma unroll
+          for (int t = 0; t < R; ++t) v[q][t] = sidx[t] >= 0 ? io.row[sidx[t]] : mkc<C>(0.0, 0.0);
+        } else {
+#pragma unroll
+          for (int t = 0; t < R; ++t)
+            v[q][t] = ((IO & kInMask) == 0 || ((tin[q] >> t) & 1u)) ? base[lo[q] + (jj[q] + t * SPAN) * ES]
+                                                                   : mkc<C>(0.0, 0.0);
+        }
       }
     }
     __syncwarp();
@@ -260,8 +301,17 @@ __device__ __forceinline__ void stage(C* base, int first, int count, Off off, co
           }
         }
         Dft<R, SIGN, C>::run(v[q]);
+        if constexpr ((IO & kOutGlobal) != 0) {
 #pragma unroll
-        for (int u = 0; u < R; ++u) base[lo[q] + (oo[q] + u * NS) * ES] = v[q][u];
+          for (int u = 0; u < R; ++u) {
+            const int sx = __ldg(io.tab + ln[q] * N + oo[q] + u * NS);
+            if (sx >= 0) io.row[sx] = v[q][u];
+          }
+        } else {
+#pragma unroll
+          for (int u = 0; u < R; ++u)
+            if ((IO & kOutMask) == 0 || ((tout[q] >> u) & 1u)) base[lo[q] + (oo[q] + u * NS) * ES] = v[q][u];
+        }
       }
     }
     __syncwarp();
@@ -291,15 +341,17 @@ __device__ __forceinline__ void group(C* base, int first, int count, Off off, co
 // order, exactly the inputs of the first stage of a forward transform run with the
 // plan reversed (R2, R1).  So that butterfly multiplies by w, runs the forward radix-R2
 // DFT and stores once; shared memory sees load, store, load, store, load, store per
-// element instead of ten accesses.  w(line, x) is read through `wgt`.
-template <int N, int ES, class Off, class W, class C>
+// element instead of ten accesses.  w(line, x) is read through `wgt`.  MASK: only the
+// elements whose bit is set in io.xb are nonzero on input and wanted on output.
+template <int N, int ES, bool MASK = false, class Off, class W, class C>
 __device__ __forceinline__ void inverse_weight_forward(C* base, int first, int count, Off off,
-                                                       const C* __restrict__ tw, W wgt, int lane) {
+                                                       const C* __restrict__ tw, W wgt, int lane,
+                                                       const StageIo<C>& io = StageIo<C>{}) {
   using P = Plan<N>;
   static_assert(P::nst == 2, "two-stage plans only");
   constexpr int R1 = P::radix[0];
   constexpr int R2 = P::radix[1];
-  stage<N, R1, 1, 1, ES>(base, first, count, off, tw, lane);
+  stage<N, R1, 1, 1, ES, MASK ? kInMask : 0>(base, first, count, off, tw, lane, io);
   constexpr int SPAN = N / R2;  // == R1
   static_assert(SPAN <= 32, "one butterfly per lane");
   constexpr int LPR = 32 / SPAN;
@@ -307,6 +359,7 @@ __device__ __forceinline__ void inverse_weight_forward(C* base, int first, int c
   const int li = lane / SPAN;
   const int j = lane - li * SPAN;
   const bool lane_ok = li < LPR;
+  const C w1 = tw[j];  // w^(t k N/(R1 R2)) with k = j, as powers of w^j
   for (int r0 = 0; r0 < count; r0 += LPR) {
     C v[R2];
     const bool act = lane_ok && r0 + li < count;
@@ -319,7 +372,6 @@ __device__ __forceinline__ void inverse_weight_forward(C* base, int first, int c
     __syncwarp();
     if (act) {
       {
-        const C w1 = tw[j];  // w^(t k N/(R1 R2)) with k = j, as powers of w^j
         C x = w1;
 #pragma unroll
         for (int t = 1; t < R2; ++t) {
@@ -341,7 +393,7 @@ __device__ __forceinline__ void inverse_weight_forward(C* base, int first, int c
     __syncwarp();
   }
   // forward: remaining stage of the reversed plan, radix R1 after span R2
-  stage<N, R1, R2, -1, ES>(base, first, count, off, tw, lane);
+  stage<N, R1, R2, -1, ES, MASK ? kOutMask : 0>(base, first, count, off, tw, lane, io);
 }
 
 // Lines of a pass owned by this warp: a contiguous block of ceil(L / warps).

@@ -27,6 +27,8 @@ struct OpTables {
   const int4* reps;       // Gamma: (ORC row 2i-1 or 0, pos of plus, pos of minus, 0)
   const int* stick_plane; // S: x * pitch + y, offset inside the shared-memory plane
   const int* xact;        // nxact x rows
+  const int* line_stick;  // nxact x n1: stick at (xact[i], y), -1 where the plane has none
+  unsigned xbits[4];      // bit x set for every x row in xact (n0 <= 128)
   const double* kinetic;  // rows
   const double* vt;       // V(r) transposed to [z][y][x]
   const float* vtf;       // the same in FP32 (the FP32 apply), plane stride BoxGeo::vstridef

@@ -176,11 +176,35 @@ __global__ void __launch_bounds__(512) k_planes(const OpTables* __restrict__ tab
   for (int s = threadIdx.x; s < t.S; s += blockDim.x) row[s] = pl[t.stick_plane[s]];
 }
 
-// Cubic grids with a compile-time plan: the x pass runs inverse, x V(r) and forward on
-// each warp's column group without a block barrier in between.
+// Cubic grids with a compile-time two-stage plan (R1, R2).  One block per (unit, z
+// plane, k):
+//   y inverse  on the x rows that hold sticks: the first stage reads its butterflies'
+//              inputs straight from the stick row in global memory (zero where the plane
+//              has no stick), the second stage runs in the shared-memory plane
+//   x pass     on every column y: inverse, x V(r), forward with the middle in registers;
+//              inputs outside the stick rows are zero and not loaded, outputs are kept
+//              only in the stick rows
+//   y forward  on the stick rows: the last stage writes the stick positions straight
+//              back to the stick row
+// The plane is never cleared or scattered: every element a pass reads was written by
+// the pass before it in the same block.
+// Blocks of k_planes_fast that fit an SM's 228 KB of shared memory (1 KB reserved per
+// block), at most 4: the register budget per thread follows from it.
+template <int N, class C>
+constexpr int planes_blocks_per_sm() {
+  const int P = N | 1;
+  const int bytes = (int)sizeof(C) * (N + N * P) + (v_in_smem_t<C>(N) ? (int)sizeof(C) / 2 * N * N : 0) + 4 * N;
+  const int fit = 233472 / (bytes + 1024);
+  return fit < 1 ? 1 : (fit > 4 ? 4 : fit);
+}
+
 template <int N, class C = double2>
-__global__ void __launch_bounds__(256, 4) k_planes_fast(const OpTables* __restrict__ tabs, BoxGeo g, Batch b) {
+__global__ void __launch_bounds__(256, planes_blocks_per_sm<N, C>()) k_planes_fast(const OpTables* __restrict__ tabs,
+                                                                                  BoxGeo g, Batch b) {
   using T = RealOf<C>;
+  using Pl = fast::Plan<N>;
+  static_assert(Pl::nst == 2, "two-stage plans");
+  constexpr int R1 = Pl::radix[0], R2 = Pl::radix[1];
   const OpTables& t = tabs[blockIdx.z];
   const CallArgs a = resolve(b.a[blockIdx.z]);
   const int unit = blockIdx.x, z = blockIdx.y;
@@ -211,38 +235,35 @@ __global__ void __launch_bounds__(256, 4) k_planes_fast(const OpTables* __restri
   const C* twg = tw_axis<C>(g, 0);
   for (int i = threadIdx.x; i < N; i += blockDim.x) tw[i] = twg[i];
   for (int i = threadIdx.x; i < nx; i += blockDim.x) rows[i] = t.xact[i] * P;
-  for (int i = threadIdx.x; i < N * P; i += blockDim.x) pl[i] = to_elem<C>(0.0, 0.0);
   __syncthreads();
-  C* row = sticks_of<C>(t) + ((int64_t)unit * N + z) * t.S;
-  for (int s = threadIdx.x; s < t.S; s += blockDim.x) pl[t.stick_plane[s]] = row[s];
-  __syncthreads();
-  fast::pass<N, 1, 1>(pl, nx, LineOffTable{rows}, tw);
-  asm volatile("cp.async.wait_all;\n" ::);
-  __syncthreads();
+  fast::StageIo<C> io;
+  io.tab = t.line_stick;
+  io.row = sticks_of<C>(t) + ((int64_t)unit * N + z) * t.S;
+  io.xb = t.xbits;
   const int lane = threadIdx.x & 31;
   int first, count;
-  fast::owned_lines(N, &first, &count);
+  fast::owned_lines(nx, &first, &count);
   if (count > 0) {
-    if constexpr (fast::Plan<N>::nst == 2) {
+    fast::stage<N, R1, 1, 1, 1, fast::kInGlobal>(pl, first, count, LineOffTable{rows}, tw, lane, io);
+    fast::stage<N, R2, R1, 1, 1>(pl, first, count, LineOffTable{rows}, tw, lane);
+  }
+  asm volatile("cp.async.wait_all;\n" ::);
+  __syncthreads();
+  {
+    int xf, xc;
+    fast::owned_lines(N, &xf, &xc);
+    if (xc > 0) {
       // line = column y, element = x: weight V(x, y, z)
       auto wgt = [&](int y, int x) -> T { return VS ? vs[y * N + x] : v[y * N + x]; };
-      fast::inverse_weight_forward<N, P>(pl, first, count, LineOffCols{}, tw, wgt, lane);
-    } else {
-      fast::group<N, 1, P>(pl, first, count, LineOffCols{}, tw, lane);
-      for (int e = lane; e < count * N; e += 32) {
-        const int li = e / N, x = e - li * N, y = first + li;
-        const T w = VS ? vs[y * N + x] : v[y * N + x];
-        C& p = pl[x * P + y];
-        p.x *= w;
-        p.y *= w;
-      }
-      __syncwarp();
-      fast::group<N, -1, P>(pl, first, count, LineOffCols{}, tw, lane);
+      fast::inverse_weight_forward<N, P, true>(pl, xf, xc, LineOffCols{}, tw, wgt, lane, io);
     }
   }
   __syncthreads();
-  fast::pass<N, -1, 1>(pl, nx, LineOffTable{rows}, tw);
-  for (int s = threadIdx.x; s < t.S; s += blockDim.x) row[s] = pl[t.stick_plane[s]];
+  fast::owned_lines(nx, &first, &count);
+  if (count > 0) {
+    fast::stage<N, R1, 1, -1, 1>(pl, first, count, LineOffTable{rows}, tw, lane);
+    fast::stage<N, R2, R1, -1, 1, fast::kOutGlobal>(pl, first, count, LineOffTable{rows}, tw, lane, io);
+  }
 }
 
 // ---------------------------------------------------------------- pass 3

@@ -6,8 +6,9 @@
 //   * every large product (rotations V C, Gram blocks V^H W, corrections, the H apply
 //     of the correction blocks) is ONE launch over all k points (blockIdx.z = k);
 //   * the small reduced problem of each k point -- bordered Cholesky with the pivot
-//     rule, A = L^-1 H_r L^-H, Householder tridiagonalisation, implicit QL with
-//     Wilkinson shifts, C = L^-H Y -- and every control decision (contraction,
+//     rule, A = L^-1 H_r L^-H, Householder tridiagonalisation, the tridiagonal
+//     eigenproblem by bisection and inverse iteration, C = L^-H Y -- and every control
+//     decision (contraction,
 //     dropped corrections, repair, convergence) run in a one-block-per-k "control"
 //     kernel, which writes the dimensions and pointers of the next large products into
 //     per-k descriptors in device memory;
@@ -28,6 +29,7 @@
 
 #include "blas_dev.cuh"
 #include "gemm_tiles.cuh"
+#include "tridiag_dev.cuh"
 #include "op_internal.h"
 
 namespace bg {
@@ -37,8 +39,6 @@ constexpr double kEps = 2.220446049250313e-16;
 constexpr double kPivotRatioMin = kEps / 1e-12;   // crates/dft-solvers/src/lean_davidson.rs:62-70
 constexpr double kDependence = 1e-12;             // crates/dft-numerics/src/linalg.rs:12
 constexpr int kCtlThreads = 256;
-constexpr int kQlMaxIter = 60;
-constexpr int kRotBuffer = 4096;  // QL rotations recorded between applications
 
 // Errors recorded by a k point's control kernel (status = -id).
 enum : int {
@@ -71,6 +71,7 @@ struct Cx<double> {
   __device__ static double div(double a, double r) { return a / r; }
   __device__ static double dot_re(double a, double b) { return a * b; }
   __device__ static double shfl_down(double a, int o) { return __shfl_down_sync(0xffffffffu, a, o); }
+  __device__ static double shfl_xor(double a, int o) { return __shfl_xor_sync(0xffffffffu, a, o); }
 };
 template <>
 struct Cx<double2> {
@@ -94,6 +95,9 @@ struct Cx<double2> {
   __device__ static double2 shfl_down(double2 a, int o) {
     return make_double2(__shfl_down_sync(0xffffffffu, a.x, o), __shfl_down_sync(0xffffffffu, a.y, o));
   }
+  __device__ static double2 shfl_xor(double2 a, int o) {
+    return make_double2(__shfl_xor_sync(0xffffffffu, a.x, o), __shfl_xor_sync(0xffffffffu, a.y, o));
+  }
 };
 
 // ------------------------------------------------------------------ device state
@@ -110,8 +114,9 @@ struct Bufs {
   D *hv, *hp, *hq;               // cap: Householder vectors
   int *active, *map, *conv, *order;  // cap
   D* part;                       // split-K partials
-  double* rot;                   // QL rotations (s, c) recorded between applications
-  int* rot_i;                    // their first column i
+  double *e2, *wu;               // cap: tridiagonal solver (squared couplings, eigenvalues by block)
+  int *starts, *clusters;        // cap + 1: its blocks and clusters
+  double* tri;                   // 5 cap kCtlThreads: its per-thread LU strips
   const double* diag;            // rows
   int rows;
 };
@@ -242,16 +247,42 @@ __device__ bool chol_extend(const D* S, int ld, D* L, int m0, int m, int* flag) 
   return ok;
 }
 
-// B <- L^-1 B (L lower m x m, B m x ncols), one thread per column.
+// Lanes that share one column of a triangular solve, or one row or column of a
+// Householder product (partial sums combined by shuffles within the group).
+constexpr int kSolveLanes = 4;
+constexpr int kHouseLanes = 8;
+
+template <class D, int G>
+__device__ __forceinline__ D group_sum(D v) {
+  for (int o = G / 2; o > 0; o >>= 1) v = Cx<D>::add(v, Cx<D>::shfl_xor(v, o));
+  return v;
+}
+
+// rdiag[i] = 1 / L[i][i] (the real diagonal of a Cholesky factor).
 template <class D>
-__device__ void trsm_lower(const D* L, int ldl, D* B, int ldb, int m, int ncols) {
+__device__ void reciprocal_diagonal(const D* L, int ldl, int m, double* rdiag) {
+  for (int i = threadIdx.x; i < m; i += blockDim.x) rdiag[i] = 1.0 / Cx<D>::real(L[i + (size_t)i * ldl]);
+  __syncthreads();
+}
+
+// B <- L^-1 B (L lower m x m, B m x ncols): kSolveLanes lanes per column split each
+// row's dot product; rdiag from reciprocal_diagonal.
+template <class D>
+__device__ void trsm_lower(const D* L, int ldl, D* B, int ldb, int m, int ncols, const double* rdiag) {
   using X = Cx<D>;
-  for (int c = threadIdx.x; c < ncols; c += blockDim.x) {
-    D* b = B + (size_t)c * ldb;
+  constexpr int G = kSolveLanes;
+  const int g = threadIdx.x % G, per = blockDim.x / G;
+  for (int c0 = 0; c0 < ncols; c0 += per) {
+    const int c = c0 + threadIdx.x / G;
+    const bool act = c < ncols;
+    D* b = B + (size_t)(act ? c : 0) * ldb;
     for (int i = 0; i < m; ++i) {
-      D x = b[i];
-      for (int k = 0; k < i; ++k) x = X::sub(x, X::mul(L[i + (size_t)k * ldl], b[k]));
-      b[i] = X::div(x, X::real(L[i + (size_t)i * ldl]));
+      D part = X::zero();
+      if (act)
+        for (int k = g; k < i; k += G) part = X::add(part, X::mul(L[i + (size_t)k * ldl], b[k]));
+      part = group_sum<D, G>(part);
+      if (act && g == 0) b[i] = X::scale(rdiag[i], X::sub(b[i], part));
+      __syncwarp();
     }
   }
   __syncthreads();
@@ -259,14 +290,21 @@ __device__ void trsm_lower(const D* L, int ldl, D* B, int ldb, int m, int ncols)
 
 // B <- L^-H B.
 template <class D>
-__device__ void trsm_lower_adjoint(const D* L, int ldl, D* B, int ldb, int m, int ncols) {
+__device__ void trsm_lower_adjoint(const D* L, int ldl, D* B, int ldb, int m, int ncols, const double* rdiag) {
   using X = Cx<D>;
-  for (int c = threadIdx.x; c < ncols; c += blockDim.x) {
-    D* b = B + (size_t)c * ldb;
+  constexpr int G = kSolveLanes;
+  const int g = threadIdx.x % G, per = blockDim.x / G;
+  for (int c0 = 0; c0 < ncols; c0 += per) {
+    const int c = c0 + threadIdx.x / G;
+    const bool act = c < ncols;
+    D* b = B + (size_t)(act ? c : 0) * ldb;
     for (int i = m - 1; i >= 0; --i) {
-      D x = b[i];
-      for (int k = i + 1; k < m; ++k) x = X::sub(x, X::mul(X::conj(L[k + (size_t)i * ldl]), b[k]));
-      b[i] = X::div(x, X::real(L[i + (size_t)i * ldl]));
+      D part = X::zero();
+      if (act)
+        for (int k = i + 1 + g; k < m; k += G) part = X::add(part, X::mul(X::conj(L[k + (size_t)i * ldl]), b[k]));
+      part = group_sum<D, G>(part);
+      if (act && g == 0) b[i] = X::scale(rdiag[i], X::sub(b[i], part));
+      __syncwarp();
     }
   }
   __syncthreads();
@@ -283,14 +321,14 @@ __device__ void adjoint(const D* src, D* dst, int ld, int m) {
 }
 
 // Hermitian eigensolver of the m x m matrix A (ld lda, overwritten), eigenvalues
-// ascending in w, eigenvectors in V (ld ldv); the algorithm of the host solver
-// (dense_host.h heev): Householder reduction to a Hermitian tridiagonal matrix, a
-// unitary diagonal scaling to a real symmetric one, implicit QL with Wilkinson shifts,
-// back-transformation.  Work arrays come from the k point's Bufs (ld ldq = cap).
-// Parallel layout: the Householder products and rank-2 updates over rows/elements; QL
-// runs its scalar recurrence on thread 0, which records each sweep's rotations, and
-// every thread then applies them to its own rows of Z.  Returns false on a non-finite
-// input or a QL sweep count above 60 for one eigenvalue.
+// ascending in w, eigenvectors in V (ld ldv): Householder reduction to a Hermitian
+// tridiagonal matrix and the unitary diagonal scaling to a real symmetric one as in the
+// host solver (dense_host.h heev), whose implicit QL is a serial rotation chase; here
+// the tridiagonal eigenpairs come from tri::eig (bisection by lane groups, inverse
+// iteration by clusters), then the back-transformation.  Work arrays come from the k
+// point's Bufs (ld ldq = cap).  The eigenpairs agree with the host solver's to rounding
+// (eigenvectors of a degenerate level up to a rotation inside it, as between any two
+// stable eigensolvers).  Returns false on a non-finite input.
 template <class D>
 __device__ bool heev(D* A, int lda, int m, double* w, D* V, int ldv, const Bufs<D>& b, int ldq, double* red,
                      int* sh) {
@@ -320,6 +358,9 @@ __device__ bool heev(D* A, int lda, int m, double* w, D* V, int ldv, const Bufs<
   D* v = b.hv;
   D* p = b.hp;
   D* q = b.hq;
+  // Q is stored transposed (Q[c + r ldq] holds row r, column c), so that the reflector
+  // update of each row reads contiguous entries.
+  const int hg = threadIdx.x % kHouseLanes, hper = blockDim.x / kHouseLanes;
   for (int k = 0; k + 2 < m; ++k) {
     const int L = m - k - 1;
     D* x = A + (k + 1) + (size_t)k * lda;
@@ -336,21 +377,19 @@ __device__ bool heev(D* A, int lda, int m, double* w, D* V, int ldv, const Bufs<
     const D phase = ax0 > 0.0 ? X::div(x0, ax0) : X::one();
     const D alpha = X::scale(-xn, phase);
     for (int i = threadIdx.x; i < L; i += blockDim.x) v[i] = i == 0 ? X::sub(x0, alpha) : x[i];
+    // |v|^2 = |x|^2 - |x0|^2 + (|x0| + |x|)^2
+    const double beta = 1.0 / (xn * (xn + ax0));
     __syncthreads();
-    part = 0.0;
-    for (int i = threadIdx.x; i < L; i += blockDim.x) part += X::abs2(v[i]);
-    const double vn2 = block_sum(part, red);
-    if (vn2 == 0.0) {
-      if (threadIdx.x == 0) b.off[k] = x0;
-      __syncthreads();
-      continue;
-    }
-    const double beta = 2.0 / vn2;
-    // p = beta B v, B = A[k+1:, k+1:]
-    for (int i = threadIdx.x; i < L; i += blockDim.x) {
+    // p = beta B v, entry i from column i of the Hermitian B (contiguous)
+    for (int i0 = 0; i0 < L; i0 += hper) {
+      const int i = i0 + threadIdx.x / kHouseLanes;
       D acc = X::zero();
-      for (int j = 0; j < L; ++j) acc = X::add(acc, X::mul(A[(k + 1 + i) + (size_t)(k + 1 + j) * lda], v[j]));
-      p[i] = X::scale(beta, acc);
+      if (i < L) {
+        const D* col = A + (k + 1) + (size_t)(k + 1 + i) * lda;
+        for (int j = hg; j < L; j += kHouseLanes) acc = X::add(acc, X::mul(X::conj(col[j]), v[j]));
+      }
+      acc = group_sum<D, kHouseLanes>(acc);
+      if (i < L && hg == 0) p[i] = X::scale(beta, acc);
     }
     __syncthreads();
     part = 0.0;
@@ -364,20 +403,20 @@ __device__ bool heev(D* A, int lda, int m, double* w, D* V, int ldv, const Bufs<
       a = X::sub(a, X::add(X::mul(v[i], X::conj(q[j])), X::mul(q[i], X::conj(v[j]))));
     }
     if (threadIdx.x == 0) b.off[k] = alpha;
-    __syncthreads();
     for (int i = threadIdx.x; i < L; i += blockDim.x) {
       x[i] = X::zero();
       A[k + (size_t)(k + 1 + i) * lda] = X::zero();
     }
-    // Q <- Q H on columns k+1..m-1
-    for (int r = threadIdx.x; r < m; r += blockDim.x) {
+    // Q <- Q H on columns k+1..m-1, one row per lane group
+    for (int r0 = 0; r0 < m; r0 += hper) {
+      const int r = r0 + threadIdx.x / kHouseLanes;
+      D* row = Q + (k + 1) + (size_t)(r < m ? r : 0) * ldq;
       D acc = X::zero();
-      for (int j = 0; j < L; ++j) acc = X::add(acc, X::mul(Q[r + (size_t)(k + 1 + j) * ldq], v[j]));
-      acc = X::scale(beta, acc);
-      for (int j = 0; j < L; ++j) {
-        D& e = Q[r + (size_t)(k + 1 + j) * ldq];
-        e = X::sub(e, X::mul(acc, X::conj(v[j])));
-      }
+      if (r < m)
+        for (int j = hg; j < L; j += kHouseLanes) acc = X::add(acc, X::mul(row[j], v[j]));
+      acc = X::scale(beta, group_sum<D, kHouseLanes>(acc));
+      if (r < m)
+        for (int j = hg; j < L; j += kHouseLanes) row[j] = X::sub(row[j], X::mul(acc, X::conj(v[j])));
     }
     __syncthreads();
   }
@@ -395,122 +434,25 @@ __device__ bool heev(D* A, int lda, int m, double* w, D* V, int ldv, const Bufs<
     }
     e[m - 1] = 0.0;
   }
-  double* Z = b.Z;
-  for (int t = threadIdx.x; t < m * m; t += blockDim.x) {
-    const int i = t % m, j = t / m;
-    Z[i + (size_t)j * ldq] = i == j ? 1.0 : 0.0;
-  }
   __syncthreads();
-  // implicit QL (the recurrence of the host's tridiagonal_ql).  Thread 0 runs the
-  // scalar recurrence for as many sweeps as the rotation buffer holds, recording each
-  // rotation (i, s, c); then every thread applies the recorded rotations, in order, to
-  // its rows of Z.  The same rotations in the same order as applying them sweep by
-  // sweep, with one block barrier per buffer instead of two per sweep.
-  const int cap_rot = kRotBuffer + 4 * ldq;
-  int* s_m = sh;  // sh[0]: recorded rotations, sh[1]: finished, sh[2]: failed
-  int ql_l = 0, ql_iter = 0;  // thread 0's position in the recurrence
-  for (;;) {
-    if (threadIdx.x == 0) {
-      int nrec = 0, fail = 0;
-      while (ql_l < m && nrec + m <= cap_rot) {
-        const int l = ql_l;
-        int mm;
-        for (mm = l; mm < m - 1; ++mm) {
-          const double dd = fabs(d[mm]) + fabs(d[mm + 1]);
-          if (fabs(e[mm]) <= kEps * dd) break;
-        }
-        if (mm == l) {
-          ++ql_l;
-          ql_iter = 0;
-          continue;
-        }
-        if (ql_iter++ == kQlMaxIter) {
-          fail = 1;
-          break;
-        }
-        double g = (d[l + 1] - d[l]) / (2.0 * e[l]);
-        double r = hypot(g, 1.0);
-        g = d[mm] - d[l] + e[l] / (g + (g >= 0.0 ? r : -r));
-        double sn = 1.0, c = 1.0, pp = 0.0;
-        bool broke = false;
-        for (int i = mm - 1; i >= l; --i) {
-          const double f = sn * e[i];
-          const double bb = c * e[i];
-          // r = |(f, g)| and (sn, c) = (f, g) / r with one reciprocal square root: the
-          // operands are bounded by the reduced matrix's norm, far from overflow, and
-          // the recurrence runs on one thread, where every dependent instruction counts
-          const double t2 = f * f + g * g;
-          if (t2 == 0.0) {
-            e[i + 1] = 0.0;
-            d[i + 1] -= pp;
-            e[mm] = 0.0;
-            broke = true;
-            break;
-          }
-          const double rinv = rsqrt(t2);
-          r = t2 * rinv;
-          e[i + 1] = r;
-          sn = f * rinv;
-          c = g * rinv;
-          g = d[i + 1] - pp;
-          r = (d[i] - g) * sn + 2.0 * c * bb;
-          pp = sn * r;
-          d[i + 1] = g + pp;
-          g = c * r - bb;
-          b.rot[2 * nrec] = sn;
-          b.rot[2 * nrec + 1] = c;
-          b.rot_i[nrec] = i;
-          ++nrec;
-        }
-        if (!broke) {
-          d[l] -= pp;
-          e[l] = g;
-          e[mm] = 0.0;
-        }
-      }
-      s_m[0] = nrec;
-      s_m[1] = ql_l >= m;
-      s_m[2] = fail;
-    }
-    __syncthreads();
-    const int nrec = s_m[0], finished = s_m[1], fail = s_m[2];
-    // apply in order; consecutive rotations (i, i+1), (i-1, i) pass column i's value
-    // in a register
-    for (int row = threadIdx.x; row < m; row += blockDim.x) {
-      int t = 0;
-      while (t < nrec) {
-        int i = b.rot_i[t];
-        double carry = Z[row + (size_t)(i + 1) * ldq];
-        for (;;) {
-          const double sn = b.rot[2 * t], c = b.rot[2 * t + 1];
-          const double zi = Z[row + (size_t)i * ldq];
-          Z[row + (size_t)(i + 1) * ldq] = sn * zi + c * carry;
-          carry = c * zi - sn * carry;
-          ++t;
-          if (t == nrec || b.rot_i[t] != i - 1) break;
-          i = b.rot_i[t];
-        }
-        Z[row + (size_t)i * ldq] = carry;
-      }
-    }
-    __syncthreads();
-    if (fail) return false;
-    if (finished) break;
-  }
+  double* Z = b.Z;
+  tri::eig<kCtlThreads>(m, d, e, b.e2, b.wu, b.starts, b.clusters, Z, ldq, b.tri, sh);
+  const double* wu = b.wu;
   // stable ascending order of the eigenvalues (rank of each entry)
   for (int i = threadIdx.x; i < m; i += blockDim.x) {
     int rank = 0;
-    const double di = d[i];
-    for (int j = 0; j < m; ++j) rank += (d[j] < di) || (d[j] == di && j < i);
+    const double di = wu[i];
+    for (int j = 0; j < m; ++j) rank += (wu[j] < di) || (wu[j] == di && j < i);
     b.order[rank] = i;
   }
   __syncthreads();
-  for (int c = threadIdx.x; c < m; c += blockDim.x) w[c] = d[b.order[c]];
+  for (int c = threadIdx.x; c < m; c += blockDim.x) w[c] = wu[b.order[c]];
+  // V = Q diag(s) Z[:, order]: lanes take consecutive columns (Z row-major, Q transposed)
   for (int t = threadIdx.x; t < m * m; t += blockDim.x) {
-    const int r = t % m, c = t / m;
+    const int c = t % m, r = t / m;
     const int src = b.order[c];
     D acc = X::zero();
-    for (int k = 0; k < m; ++k) acc = X::add(acc, X::mul(Q[r + (size_t)k * ldq], X::scale(Z[k + (size_t)src * ldq], s[k])));
+    for (int k = 0; k < m; ++k) acc = X::add(acc, X::mul(Q[k + (size_t)r * ldq], X::scale(Z[(size_t)k * ldq + src], s[k])));
     V[r + (size_t)c * ldv] = acc;
   }
   __syncthreads();
@@ -527,12 +469,14 @@ __device__ bool eigen(const Bufs<D>& b, int cap, int m, double* red, int* sh) {
     b.A[i + (size_t)j * cap] = b.Hr[i + (size_t)j * cap];
   }
   __syncthreads();
-  trsm_lower(b.L, cap, b.A, cap, m, m);
+  reciprocal_diagonal(b.L, cap, m, b.e2);
+  trsm_lower(b.L, cap, b.A, cap, m, m, b.e2);
   adjoint(b.A, b.Y, cap, m);
-  trsm_lower(b.L, cap, b.Y, cap, m, m);
+  trsm_lower(b.L, cap, b.Y, cap, m, m, b.e2);
   adjoint(b.Y, b.A, cap, m);
   if (!heev(b.A, cap, m, b.w, b.Y, cap, b, cap, red, sh)) return false;
-  trsm_lower_adjoint(b.L, cap, b.Y, cap, m, m);
+  reciprocal_diagonal(b.L, cap, m, b.e2);   // heev used e2 as scratch
+  trsm_lower_adjoint(b.L, cap, b.Y, cap, m, m, b.e2);
   for (int t = threadIdx.x; t < m * m; t += blockDim.x) {
     const int i = t % m, j = t / m;
     b.C[i + (size_t)j * cap] = b.Y[i + (size_t)j * cap];
@@ -677,11 +621,15 @@ __global__ void __launch_bounds__(kCtlThreads, 1) k_dv_ctl(int phase, const Bufs
     double* fp = reinterpret_cast<double*>(dp + 5 * c);
     b.td = fp;
     b.te = fp + c;
+    b.e2 = fp + 2 * c;
+    b.wu = fp + 3 * c;
     int* ip = reinterpret_cast<int*>(fp + 4 * c);
-    b.order = ip + c;
+    b.order = ip;
+    b.starts = ip + c;
+    b.clusters = ip + 2 * c + 1;
     if (o.smem_matrices) {
       // small capacities: the eigensolver's matrices in shared memory as well
-      D* mp = reinterpret_cast<D*>(ip + 2 * c + (2 * c & 2));  // 16-byte aligned
+      D* mp = reinterpret_cast<D*>(ip + ((3 * c + 2 + 3) & ~3));  // 16-byte aligned
       const size_t cc = (size_t)c * c;
       b.A = mp;
       b.Y = mp + cc;
@@ -1076,7 +1024,7 @@ class KsetSolver {
     return BG_EDEVICE;
   }
   static size_t vec_smem(int cap) {
-    return (size_t)cap * (5 * sizeof(D) + 4 * sizeof(double) + 2 * sizeof(int)) + 16;
+    return (size_t)cap * (5 * sizeof(D) + 4 * sizeof(double)) + sizeof(int) * (size_t)((3 * cap + 2 + 3) & ~3);
   }
   static size_t mat_smem(int cap) { return (size_t)cap * cap * (3 * sizeof(D) + sizeof(double)); }
   // A, Y, Q and Z join the vectors in shared memory when all fit in 200 KB.
@@ -1174,7 +1122,7 @@ int KsetSolver<T>::prepare() {
         (rc = alloc(&b.off, cap)) || (rc = alloc(&b.ph, cap)) || (rc = alloc(&b.hv, cap)) || (rc = alloc(&b.hp, cap)) ||
         (rc = alloc(&b.hq, cap)) || (rc = alloc(&b.active, cap)) || (rc = alloc(&b.map, cap)) ||
         (rc = alloc(&b.conv, cap)) || (rc = alloc(&b.order, cap)) || (rc = alloc(&b.part, 2 * (size_t)slot_elems_)) ||
-        (rc = alloc(&b.rot, 2 * ((size_t)kRotBuffer + 4 * cap))) || (rc = alloc(&b.rot_i, (size_t)kRotBuffer + 4 * cap)))
+        (rc = alloc(&b.tri, 5 * (size_t)cap * kCtlThreads)))
       return rc;
     double* dg = nullptr;
     if ((rc = alloc(&dg, b.rows))) return rc;

@@ -127,6 +127,7 @@ class GpuScf:
             self.diag_static.append(torch.from_numpy(np.ascontiguousarray(d)).to(dev))
             x0 = w.random_block(pw.npw, w.bands, seed_offset=100 + i, real=gamma)
             self.starts.append(torch.from_numpy(np.ascontiguousarray(x0.T)).to(dev))
+        self._starts0 = [x.clone() for x in self.starts]
         self.gamma = self.ops[0].is_real()
         self.kset = KPointSet(self.ops, self.ctx)
         self.v_ion = torch.from_numpy(np.ascontiguousarray(w.ionic_potential())).to(dev)
@@ -140,8 +141,9 @@ class GpuScf:
         self.fields = FieldGrid(w.rows, dims, self.ctx)
         self.fields.set_sphere(flat)
         g2 = np.ascontiguousarray(dens.kpg2[keep])
-        self.mixer = Broyden(g2, np.ones(g2.size, bool), self.volume, self.electrons, self.volume,
-                             Profile(beta=self.o.beta, history=self.o.history), self.ctx)
+        self._new_mixer = lambda: Broyden(g2, np.ones(g2.size, bool), self.volume, self.electrons, self.volume,
+                                          Profile(beta=self.o.beta, history=self.o.history), self.ctx)
+        self.mixer = self._new_mixer()
         s = self.stream.cuda_stream
         for op in self.ops:
             op.set_stream(s)
@@ -187,21 +189,20 @@ class GpuScf:
         dr2 = self.mixer.metric(fres, fres)
         return sols, rho, y, fres, dr2, energy, ts
 
+    def reset(self) -> None:
+        """Back to the state after construction: the start blocks and an empty mixer (the
+        operators, the k-point set and its captured Davidson graphs stay)."""
+        self.starts = [s.clone() for s in self._starts0]
+        self.mixer.close()
+        self.mixer = self._new_mixer()
+        self.mixer.set_stream(self.stream.cuda_stream)
+
     def warm_up(self) -> None:
-        """One map of the start density per apply precision that run() will use, with the
-        start blocks put back afterwards: loads the kernels and captures the Davidson
-        iteration graphs, one-time costs of the process, so that a timed run() after it
-        measures the SCF alone."""
-        torch = self.torch
-        saved = [s.clone() for s in self.starts]
-        kinds = ["fp64"] + (["fp32"] if self.o.fp32_ethr_ry is not None else [])
-        with torch.cuda.stream(self.stream):
-            n = torch.full(self.dims, self.electrons / self.volume, dtype=torch.float64, device=self.dev)
-            x = self.fields.sphere_forward(n)
-            for p in kinds:
-                self._map(n, x, 1e-2, True, p)
-                self.starts = [s.clone() for s in saved]
-            torch.cuda.synchronize()
+        """One whole SCF followed by reset(): loads every kernel and captures the Davidson
+        iteration graph of each apply precision the schedule uses, one-time costs of the
+        process, so that a timed run() after it measures the SCF alone."""
+        self.run()
+        self.reset()
 
     def run(self) -> ScfResult:
         torch = self.torch

@@ -464,7 +464,8 @@ def scf_leg(workload_name, ctx, fp32_ethr_ry=None):
            "ms_per_map": 1000.0 * res.seconds / max(maps, 1), "energy_ha": res.energy_ha,
            "free_energy_ha": res.free_energy_ha, "h_columns": int(sum(r.h_columns for r in res.records)),
            "dr2_ry": res.records[-1].dr2_ry if res.records else None,
-           "fp32_maps": sum(r.precision == "fp32" for r in res.records), "natoms": w.natoms}
+           "fp32_maps": sum(r.precision == "fp32" for r in res.records), "natoms": w.natoms,
+           "map_ms": [round(1000.0 * r.seconds, 2) for r in res.records]}
     if fp32_ethr_ry is not None:
         out["fp32_ethr_ry"] = fp32_ethr_ry
     return out
