@@ -116,7 +116,6 @@ struct Bufs {
   D* part;                       // split-K partials
   double *e2, *wu;               // cap: tridiagonal solver (squared couplings, eigenvalues by block)
   int *starts, *clusters;        // cap + 1: its blocks and clusters
-  double* tri;                   // 5 cap kCtlThreads: its per-thread LU strips
   const double* diag;            // rows
   int rows;
 };
@@ -436,7 +435,9 @@ __device__ bool heev(D* A, int lda, int m, double* w, D* V, int ldv, const Bufs<
   }
   __syncthreads();
   double* Z = b.Z;
-  tri::eig<kCtlThreads>(m, d, e, b.e2, b.wu, b.starts, b.clusters, Z, ldq, b.tri, sh);
+  // A is free once the tridiagonal is read: it holds the inverse iteration's LU strips
+  tri::eig<kCtlThreads>(m, d, e, b.e2, b.wu, b.starts, b.clusters, Z, ldq, reinterpret_cast<double*>(A),
+                        (int)((size_t)ldq * ldq * sizeof(D) / sizeof(double)), sh);
   const double* wu = b.wu;
   // stable ascending order of the eigenvalues (rank of each entry)
   for (int i = threadIdx.x; i < m; i += blockDim.x) {
@@ -1122,7 +1123,7 @@ int KsetSolver<T>::prepare() {
         (rc = alloc(&b.off, cap)) || (rc = alloc(&b.ph, cap)) || (rc = alloc(&b.hv, cap)) || (rc = alloc(&b.hp, cap)) ||
         (rc = alloc(&b.hq, cap)) || (rc = alloc(&b.active, cap)) || (rc = alloc(&b.map, cap)) ||
         (rc = alloc(&b.conv, cap)) || (rc = alloc(&b.order, cap)) || (rc = alloc(&b.part, 2 * (size_t)slot_elems_)) ||
-        (rc = alloc(&b.tri, 5 * (size_t)cap * kCtlThreads)))
+        false)
       return rc;
     double* dg = nullptr;
     if ((rc = alloc(&dg, b.rows))) return rc;

@@ -12,7 +12,8 @@
 // (row-major, so that the threads of different clusters touch adjacent words), j < m,
 // eigenpairs in ascending order inside each unreduced block (blocks in row order); Z is
 // zero outside each vector's block.  Scratch: e2 (m doubles, shared), starts and clusters (m + 1 ints
-// each, shared), lu (5 m NT doubles, global, one strip per thread).
+// each, shared), lu (lu_doubles, best in shared memory: 4 m doubles per thread that works
+// on a cluster at the same time, so at least 4 m).
 #pragma once
 
 namespace bg {
@@ -24,44 +25,41 @@ constexpr int kMaxRounds = 100;
 constexpr int kInverseIterations = 5;
 constexpr int kExtraIterations = 1;   // after the growth criterion is met
 
-// Sturm counts of the eigenvalues below xa and below xb of block [s, s + n): the sign
-// changes along the leading principal minors p_0 = 1, p_1 = d_s - x,
+// Sturm counts of the eigenvalues below each of the C shifts x[c] in block [s, s + n):
+// the sign changes along the leading principal minors p_0 = 1, p_1 = d_s - x,
 // p_r+1 = (d_s+r - x) p_r - e_s+r-1^2 p_r-1 (a zero minor takes the sign opposite to its
 // predecessor).  The recurrence has one fused multiply-add on its dependent chain (no
-// division), two shifts run interleaved, and a pair of minors is rescaled by an exact
+// division), the C shifts run interleaved, and a pair of minors is rescaled by an exact
 // power of two when it leaves [2^-500, 2^500].
-__device__ __forceinline__ void sturm2(const double* d, const double* e2, int s, int n, double xa, double xb,
-                                       int* ca, int* cb) {
-  double pa = d[s] - xa, pb = d[s] - xb, qa = 1.0, qb = 1.0;  // p_r, p_r-1
-  bool sa = pa <= 0.0, sb = pb <= 0.0;                         // sign bit of p_r (zero: opposite of p_0 > 0)
-  int a = sa, b = sb;
+template <int C>
+__device__ __forceinline__ void sturm(const double* d, const double* e2, int s, int n, const double (&x)[C],
+                                      int (&cnt)[C]) {
+  double p[C], q[C];
+  bool sg[C];
+#pragma unroll
+  for (int c = 0; c < C; ++c) {
+    p[c] = d[s] - x[c];
+    q[c] = 1.0;
+    sg[c] = p[c] <= 0.0;
+    cnt[c] = sg[c];
+  }
   for (int i = s + 1; i < s + n; ++i) {
     const double di = d[i], ei = e2[i - 1];
-    const double ra = fma(di - xa, pa, -ei * qa);
-    const double rb = fma(di - xb, pb, -ei * qb);
-    qa = pa;
-    pa = ra;
-    qb = pb;
-    pb = rb;
-    const bool na = pa == 0.0 ? !sa : pa < 0.0;
-    const bool nb = pb == 0.0 ? !sb : pb < 0.0;
-    a += na != sa;
-    b += nb != sb;
-    sa = na;
-    sb = nb;
-    if (!(fabs(pa) < 0x1p500) || fabs(pa) < 0x1p-500) {
-      const int ex = ilogb(pa == 0.0 ? qa : pa);
-      pa = scalbn(pa, -ex);
-      qa = scalbn(qa, -ex);
-    }
-    if (!(fabs(pb) < 0x1p500) || fabs(pb) < 0x1p-500) {
-      const int ex = ilogb(pb == 0.0 ? qb : pb);
-      pb = scalbn(pb, -ex);
-      qb = scalbn(qb, -ex);
+#pragma unroll
+    for (int c = 0; c < C; ++c) {
+      const double r = fma(di - x[c], p[c], -ei * q[c]);
+      q[c] = p[c];
+      p[c] = r;
+      const bool ng = r == 0.0 ? !sg[c] : r < 0.0;
+      cnt[c] += ng != sg[c];
+      sg[c] = ng;
+      if (!(fabs(r) < 0x1p500) || fabs(r) < 0x1p-500) {
+        const int ex = ilogb(r == 0.0 ? q[c] : r);
+        p[c] = scalbn(p[c], -ex);
+        q[c] = scalbn(q[c], -ex);
+      }
     }
   }
-  *ca = a;
-  *cb = b;
 }
 
 // Block of eigenvalue j (blocks listed by their first rows in starts[0..nb]).
@@ -102,7 +100,8 @@ __device__ __forceinline__ double start_entry(int j, int r) {
 
 template <int NT>
 __device__ void eig(int m, const double* __restrict__ d, const double* __restrict__ e, double* e2, double* wu,
-                    int* starts, int* clusters, double* Z, int ldz, double* __restrict__ lu, int* sh) {
+                    int* starts, int* clusters, double* Z, int ldz, double* __restrict__ lu, int lu_doubles,
+                    int* sh) {
   // 1. splits where a coupling is negligible against its neighbours; squared couplings
   if (threadIdx.x == 0) {
     int nb = 0;
@@ -125,7 +124,9 @@ __device__ void eig(int m, const double* __restrict__ d, const double* __restric
   for (int i = 0; i + 1 < m; ++i) e2max = fmax(e2max, e2[i]);
   const double pivmin = kSafeMin * e2max;
 
-  // 2. eigenvalues: G lanes per eigenvalue, each counting two shifts per round
+  // 2. eigenvalues: G lanes per eigenvalue, each counting kShifts shifts per round;
+  //    located to 2 eps max(|lo|, |hi|) + eps |T_b|_1
+  constexpr int kShifts = 4;
   int G = 1;
   while (G < 32 && 2 * G * m <= NT) G *= 2;
   const int NG = NT / G, gid = threadIdx.x / G, lig = threadIdx.x % G;
@@ -134,7 +135,7 @@ __device__ void eig(int m, const double* __restrict__ d, const double* __restric
     const int j = j0 + gid;
     const bool act = j < m;
     int s = 0, n = 1, i = 0;
-    double lo = 0.0, hi = 0.0, nrm;
+    double lo = 0.0, hi = 0.0, nrm = 0.0;
     if (act) {
       const int b = block_of(starts, nb, j);
       s = starts[b];
@@ -143,17 +144,24 @@ __device__ void eig(int m, const double* __restrict__ d, const double* __restric
       gershgorin(d, e, s, n, pivmin, &lo, &hi, &nrm);
     }
     bool done = !act;
-    const int K = 2 * G;
+    const int K = kShifts * G;
+    const double atol = kUlp * nrm + 2.0 * pivmin;
     for (int it = 0; it < kMaxRounds; ++it) {
       if (!done) {
-        if (hi - lo <= 2.0 * kUlp * fmax(fabs(lo), fabs(hi)) + 2.0 * pivmin) {
+        if (hi - lo <= 2.0 * kUlp * fmax(fabs(lo), fabs(hi)) + atol) {
           done = true;
         } else {
           const double h = (hi - lo) / (K + 1);
-          const int r0 = 2 * lig;
-          int c0, c1;
-          sturm2(d, e2, s, n, lo + (r0 + 1) * h, lo + (r0 + 2) * h, &c0, &c1);
-          int rf = c0 > i ? r0 : (c1 > i ? r0 + 1 : K);
+          const int r0 = kShifts * lig;
+          double xs[kShifts];
+          int cs[kShifts];
+#pragma unroll
+          for (int c = 0; c < kShifts; ++c) xs[c] = lo + (r0 + c + 1) * h;
+          sturm<kShifts>(d, e2, s, n, xs, cs);
+          int rf = K;
+#pragma unroll
+          for (int c = kShifts - 1; c >= 0; --c)
+            if (cs[c] > i) rf = r0 + c;
           for (int o = G >> 1; o > 0; o >>= 1) rf = min(rf, __shfl_xor_sync(gmask, rf, o));
           const double nlo = rf > 0 ? lo + rf * h : lo;
           const double nhi = rf < K ? lo + (rf + 1) * h : hi;
@@ -185,8 +193,13 @@ __device__ void eig(int m, const double* __restrict__ d, const double* __restric
   __syncthreads();
   const int nc = sh[1];
 
-  // 4. eigenvectors: one cluster per thread, inverse iteration on its block
-  for (int cidx = threadIdx.x; cidx < nc; cidx += NT) {
+  // 4. eigenvectors: one cluster per thread, inverse iteration on its block.  A thread's
+  //    LU strips (reciprocal pivots, first and second superdiagonals of U, multipliers)
+  //    hold 4 m doubles, so at most lu_doubles / (4 m) threads work at a time.  A row
+  //    swap at elimination step r < n - 2 leaves a nonzero second superdiagonal (the
+  //    couplings inside a block are nonzero); the swap at step n - 2 is kept apart.
+  const int P = max(1, min(NT, lu_doubles / (4 * m)));
+  for (int cidx = threadIdx.x; cidx < nc && threadIdx.x < P; cidx += P) {
     const int ja = clusters[cidx], jb = clusters[cidx + 1];
     const int b = block_of(starts, nb, ja);
     const int s = starts[b], n = starts[b + 1] - s;
@@ -198,80 +211,81 @@ __device__ void eig(int m, const double* __restrict__ d, const double* __restric
     gershgorin(d, e, s, n, pivmin, &gl, &gu, &onenrm);
     const double pertol = 10.0 * kUlp * onenrm, tiny = kUlp * onenrm;
     const double dtpcrt = sqrt(0.1 / n);
-    // this thread's strips: U diagonal, first and second superdiagonals, multipliers, pivots
-    double* u0 = lu + threadIdx.x;
-    double* u1 = u0 + (size_t)m * NT;
-    double* u2 = u1 + (size_t)m * NT;
-    double* lm = u2 + (size_t)m * NT;
-    double* pv = lm + (size_t)m * NT;
+    double* ur = lu + threadIdx.x;
+    double* u1 = ur + (size_t)m * P;
+    double* u2 = u1 + (size_t)m * P;
+    double* lm = u2 + (size_t)m * P;
     double xprev = 0.0;
     for (int j = ja; j < jb; ++j) {
       double x = wu[j];
       if (j > ja && x - xprev < pertol) x = xprev + pertol;
       xprev = x;
-      // LU with partial pivoting of T_b - x I
-      double ai = d[s] - x, bi = e[s];
+      // LU with partial pivoting of T_b - x I; pivots below eps |T|_1 are raised to it
+      // (the solve then grows along the eigenvector) and kept as reciprocals
+      double ai = d[s] - x, bi = e[s], ulast = 0.0;
+      bool last_swap = false;
       for (int r = 0; r + 1 < n; ++r) {
         const double ci = e[s + r], an = d[s + r + 1] - x, bn = r + 2 < n ? e[s + r + 1] : 0.0;
-        double l;
+        double l, piv;
         if (fabs(ai) >= fabs(ci)) {
           l = ai != 0.0 ? ci / ai : 0.0;
-          u0[(size_t)r * NT] = ai;
-          u1[(size_t)r * NT] = bi;
-          u2[(size_t)r * NT] = 0.0;
-          pv[(size_t)r * NT] = 0.0;
+          piv = ai;
+          u1[(size_t)r * P] = bi;
+          u2[(size_t)r * P] = 0.0;
           ai = an - l * bi;
           bi = bn;
         } else {
           l = ai / ci;
-          u0[(size_t)r * NT] = ci;
-          u1[(size_t)r * NT] = an;
-          u2[(size_t)r * NT] = bn;
-          pv[(size_t)r * NT] = 1.0;
+          piv = ci;
+          u1[(size_t)r * P] = an;
+          u2[(size_t)r * P] = bn;
           ai = bi - l * an;
           bi = -l * bn;
+          if (r + 2 == n) last_swap = true;
         }
-        lm[(size_t)r * NT] = l;
+        if (fabs(piv) < tiny) piv = piv < 0.0 ? -tiny : tiny;
+        ur[(size_t)r * P] = 1.0 / piv;
+        lm[(size_t)r * P] = l;
       }
-      u0[(size_t)(n - 1) * NT] = ai;
-      // pivots below eps |T|_1 raised to it (the solve then grows along the eigenvector);
-      // the back substitution multiplies by their reciprocals
-      double ulast = 0.0;
-      for (int r = 0; r < n; ++r) {
-        double u = u0[(size_t)r * NT];
-        if (fabs(u) < tiny) u = u < 0.0 ? -tiny : tiny;
-        if (r == n - 1) ulast = fabs(u);
-        u0[(size_t)r * NT] = 1.0 / u;
-      }
+      if (fabs(ai) < tiny) ai = ai < 0.0 ? -tiny : tiny;
+      ulast = fabs(ai);
+      ur[(size_t)(n - 1) * P] = 1.0 / ai;
       // z(r) below stands for Z[(s + r) ldz + j]
       double* zc = Z + (size_t)s * ldz + j;
       auto z = [&](int r) -> double& { return zc[(size_t)r * ldz]; };
-      for (int r = 0; r < n; ++r) z(r) = start_entry(j, r);
+      double asum = 0.0;
+      for (int r = 0; r < n; ++r) {
+        const double v = start_entry(j, r);
+        z(r) = v;
+        asum += fabs(v);
+      }
       int checks = 0;
       for (int its = 0; its < kInverseIterations; ++its) {
-        double asum = 0.0;
-        for (int r = 0; r < n; ++r) asum += fabs(z(r));
         const double scl = n * onenrm * fmax(kUlp, ulast) / asum;
-        for (int r = 0; r < n; ++r) z(r) *= scl;
-        // L^-1 P
+        // L^-1 P (scaled right-hand side); the running entry rides in a register
+        double zr = z(0) * scl;
         for (int r = 0; r + 1 < n; ++r) {
-          if (pv[(size_t)r * NT] != 0.0) {
-            const double t = z(r);
-            z(r) = z(r + 1);
-            z(r + 1) = t;
+          double zn = z(r + 1) * scl;
+          const bool sw = r + 2 < n ? u2[(size_t)r * P] != 0.0 : last_swap;
+          if (sw) {
+            const double t = zr;
+            zr = zn;
+            zn = t;
           }
-          z(r + 1) -= lm[(size_t)r * NT] * z(r);
+          z(r) = zr;
+          zr = zn - lm[(size_t)r * P] * zr;
         }
-        // U^-1 (u0 holds the reciprocal pivots); the two previous entries ride in registers
-        double z1 = z(n - 1) * u0[(size_t)(n - 1) * NT];
+        z(n - 1) = zr;
+        // U^-1; the two previous entries ride in registers
+        double z1 = zr * ur[(size_t)(n - 1) * P];
         z(n - 1) = z1;
-        double z0 = (z(n - 2) - u1[(size_t)(n - 2) * NT] * z1) * u0[(size_t)(n - 2) * NT];
+        double z0 = (z(n - 2) - u1[(size_t)(n - 2) * P] * z1) * ur[(size_t)(n - 2) * P];
         z(n - 2) = z0;
         for (int r = n - 3; r >= 0; --r) {
-          const double zr = (z(r) - u1[(size_t)r * NT] * z0 - u2[(size_t)r * NT] * z1) * u0[(size_t)r * NT];
-          z(r) = zr;
+          const double v = (z(r) - u1[(size_t)r * P] * z0 - u2[(size_t)r * P] * z1) * ur[(size_t)r * P];
+          z(r) = v;
           z1 = z0;
-          z0 = zr;
+          z0 = v;
         }
         // against the cluster's earlier vectors
         for (int jj = ja; jj < j; ++jj) {
@@ -281,15 +295,21 @@ __device__ void eig(int m, const double* __restrict__ d, const double* __restric
           for (int r = 0; r < n; ++r) z(r) -= dot * y[(size_t)r * ldz];
         }
         double zmax = 0.0;
-        for (int r = 0; r < n; ++r) zmax = fmax(zmax, fabs(z(r)));
+        asum = 0.0;
+        for (int r = 0; r < n; ++r) {
+          const double a = fabs(z(r));
+          zmax = fmax(zmax, a);
+          asum += a;
+        }
         if (zmax >= dtpcrt && ++checks > kExtraIterations) break;
       }
       double nn = 0.0, big = 0.0, sgn = 1.0;
       for (int r = 0; r < n; ++r) {
-        nn += z(r) * z(r);
-        if (fabs(z(r)) > big) {
-          big = fabs(z(r));
-          sgn = z(r) < 0.0 ? -1.0 : 1.0;
+        const double v = z(r);
+        nn += v * v;
+        if (fabs(v) > big) {
+          big = fabs(v);
+          sgn = v < 0.0 ? -1.0 : 1.0;
         }
       }
       const double inv = sgn / sqrt(nn);
