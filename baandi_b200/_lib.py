@@ -114,6 +114,8 @@ SIGNATURES = {
     "bg_kset_create": [_p, _i32, _p, _pp],
     "bg_kset_destroy": [_p],
     "bg_kset_apply": [_p, _p, _p, _p, _i32, _i32],
+    "bg_kset_set_potential_ptr": [_p, _p, _u64, _i32],
+    "bg_kset_band_density_sum": [_p, _p, _i64, _p, ctypes.c_double, _p, _i32, _i32],
     "bg_kset_sync": [_p],
     "bg_kset_stream": [_p, _pp],
     "bg_kset_set_stream": [_p, _p],

@@ -574,12 +574,9 @@ int bg_op_set_potential(bg_op* op, const double* v, uint64_t epoch) {
       }
   cudaError_t e = cudaMemcpyAsync(const_cast<double*>(op->t.vt), vt.data(), vt.size() * sizeof(double),
                                   cudaMemcpyHostToDevice, op->stream);
-  if (e == cudaSuccess) {
-    launch_potential_float(op->t.vt, op->g, const_cast<float*>(op->t.vtf), op->stream);
-    e = cudaGetLastError();
-  }
   if (e == cudaSuccess) e = cudaStreamSynchronize(op->stream);
   if (e != cudaSuccess) return cuda_fail(op->ctx, e, "set_potential");
+  op->vtf_valid = false;
   op->epoch = epoch;
   op->has_epoch = true;
   return BG_OK;
@@ -609,6 +606,10 @@ int bg_op_apply_block(bg_op* op, const double* x, double* y, int64_t rows, int64
     dy = static_cast<double*>(op->ys->p);
     e = cudaMemcpyAsync(const_cast<double*>(dx), x, dpc * cols * sizeof(double), cudaMemcpyHostToDevice, op->stream);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "copy in");
+  }
+  if (precision == BG_PREC_FP32) {
+    int rc = ensure_potential_float(op, op->stream);
+    if (rc) return rc;
   }
   if (op->is_dense) {
     int rc = dense_apply(op, dx, dy, cols);
@@ -727,11 +728,8 @@ int bg_op_set_potential_ptr(bg_op* op, const double* v, uint64_t epoch, int32_t 
   if ((rc = transpose_grid(op, v, op->vchange))) return rc;
   e = cudaMemcpyAsync(const_cast<double*>(op->t.vt), op->vchange, sizeof(double) * op->g.vstride * op->dims[2],
                       cudaMemcpyDeviceToDevice, op->stream);
-  if (e == cudaSuccess) {
-    launch_potential_float(op->t.vt, op->g, const_cast<float*>(op->t.vtf), op->stream);
-    e = cudaGetLastError();
-  }
   if (e != cudaSuccess) return cuda_fail(op->ctx, e, "set_potential");
+  op->vtf_valid = false;
   op->epoch = epoch;
   op->has_epoch = true;
   return BG_OK;
@@ -837,15 +835,17 @@ int bg_op_band_density_sum(bg_op* op, const double* x, int64_t rows, int64_t col
     }
     e = cudaMemcpyAsync(op->dens_w, weights, cols * sizeof(double), cudaMemcpyHostToDevice, op->stream);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "copy in");
-    CallArgs a;
+    Batch bt;
+    bt.nk = 1;
+    CallArgs& a = bt.a[0];
     a.x = dx;
     a.y = nullptr;
     a.ldx = a.ldy = (int64_t)dpc;
     a.cols = (int)cols;
     a.units = units;
-    op->launches += launch_density(op->d_tabs, op->gamma ? 1 : 0, op->t.ngroups, op->g, a, op->dens_w, per_chunk,
-                                   op->dens_part, op->stream);
-    launch_density_reduce(op->dens_part, chunks, op->g, volume, accumulate, dd, op->stream);
+    op->launches += launch_density(op->d_tabs, op->gamma ? 1 : 0, op->t.ngroups, op->g, bt, op->dens_w, 0, per_chunk,
+                                   chunks, op->dens_part, op->stream);
+    launch_density_reduce(op->dens_part, 1, chunks, op->g, volume, accumulate, dd, op->stream);
     op->launches += 1;
     e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(ctx, e, "kernel launch");
@@ -863,6 +863,15 @@ int bg_op_band_density_sum(bg_op* op, const double* x, int64_t rows, int64_t col
 
 namespace bg {
 // Launch the local and nonlocal stages of operators [k0, k1) of a set on one stream.
+int ensure_potential_float(bg_op* op, cudaStream_t s) {
+  if (op->vtf_valid || op->is_dense) return BG_OK;
+  launch_potential_float(op->t.vt, op->g, const_cast<float*>(op->t.vtf), s);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(op->ctx, e, "kernel launch");
+  op->vtf_valid = true;
+  return BG_OK;
+}
+
 int enqueue_range(bg_kset* ks, int k0, int k1, const CallArgs* args, const int64_t* cols, cudaStream_t s,
                   StageEvents* ev, int fp32) {
   Batch bt;
@@ -959,9 +968,132 @@ int bg_kset_destroy(bg_kset* ks) {
     if (ks->work_done[i]) cudaEventDestroy(ks->work_done[i]);
   }
   if (ks->dv_cache && ks->dv_free) ks->dv_free(ks->dv_cache);
+  cudaFree(ks->d_vts);
+  cudaFree(ks->dens_part);
+  cudaFree(ks->dens_w);
   cudaFree(ks->d_tabs);
   cudaFree(ks->d_nl);
   delete ks;
+  return BG_OK;
+}
+
+int bg_kset_set_potential_ptr(bg_kset* ks, const double* v, uint64_t epoch, int32_t ptr_kind) {
+  if (!ks || !v) return fail(ks ? ks->ctx : nullptr, BG_EINVAL, "null argument");
+  bg_ctx* ctx = ks->ctx;
+  if (ks->dense) return fail(ctx, BG_EINVAL, "a dense operator has no potential grid");
+  if (ptr_kind != BG_PTR_HOST && ptr_kind != BG_PTR_DEVICE) return fail(ctx, BG_EINVAL, "pointer kind");
+  const int n = (int)ks->ops.size();
+  for (int k = 0; k < n; ++k) {
+    const bg_op* op = ks->ops[k];
+    if (op->has_epoch && epoch <= op->epoch) return fail(ctx, BG_EEPOCH, "potential epoch must increase");
+  }
+  if (ptr_kind == BG_PTR_HOST) {
+    for (int k = 0; k < n; ++k)
+      if (int rc = bg_op_set_potential(ks->ops[k], v, epoch)) return rc;
+    return BG_OK;
+  }
+  cudaError_t e = cudaSetDevice(ctx->device);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaSetDevice");
+  bg_op* op0 = ks->ops[0];
+  const size_t vdoubles = (size_t)ks->g.vstride * ks->g.n2;
+  int rc = ensure_buf(op0, &op0->vchange, vdoubles);
+  if (rc) return rc;
+  if (!ks->d_vts) {
+    std::vector<double*> h(n);
+    for (int k = 0; k < n; ++k) h[k] = const_cast<double*>(ks->ops[k]->t.vt);
+    void* p = nullptr;
+    if ((e = cudaMalloc(&p, n * sizeof(double*))) != cudaSuccess) return cuda_fail(ctx, e, "cudaMalloc");
+    ks->d_vts = static_cast<double**>(p);
+    if ((e = cudaMemcpy(ks->d_vts, h.data(), n * sizeof(double*), cudaMemcpyHostToDevice)) != cudaSuccess)
+      return cuda_fail(ctx, e, "cudaMemcpy");
+  }
+  // transposed and checked once in a scratch copy (a rejected potential leaves the old
+  // one everywhere), then copied to every operator
+  launch_potential_transpose(v, ks->g, op0->vchange, op0->t.err, ks->stream);
+  e = cudaMemcpyAsync(op0->err_host, op0->t.err, sizeof(int), cudaMemcpyDeviceToHost, ks->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ks->stream);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "set_potential");
+  if (op0->err_host[0]) {
+    cudaMemsetAsync(op0->t.err, 0, sizeof(int), ks->stream);
+    cudaStreamSynchronize(ks->stream);
+    return fail(ctx, BG_ENONFINITE, "non-finite potential value");
+  }
+  launch_broadcast(op0->vchange, (int64_t)vdoubles, ks->d_vts, n, ks->stream);
+  if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(ctx, e, "kernel launch");
+  ks->launches += 2;
+  for (int k = 0; k < n; ++k) {
+    bg_op* op = ks->ops[k];
+    op->vtf_valid = false;
+    op->epoch = epoch;
+    op->has_epoch = true;
+  }
+  return BG_OK;
+}
+
+int bg_kset_band_density_sum(bg_kset* ks, const double* const* x, int64_t cols, const double* weights, double volume,
+                             double* density, int32_t accumulate, int32_t ptr_kind) {
+  if (!ks || !density) return fail(ks ? ks->ctx : nullptr, BG_EINVAL, "null argument");
+  bg_ctx* ctx = ks->ctx;
+  if (ptr_kind != BG_PTR_DEVICE) return fail(ctx, BG_EINVAL, "the set's band density takes device blocks and grid");
+  if (ks->dense) return fail(ctx, BG_EINVAL, "a dense operator has no grid");
+  const int n = (int)ks->ops.size();
+  for (int k = 0; k < n; ++k)
+    if (cols < 0 || cols > ks->ops[k]->cap) return fail(ctx, BG_ESHAPE, "block shape");
+  if (cols > 0 && (!x || !weights)) return fail(ctx, BG_EINVAL, "null argument");
+  for (int k = 0; cols > 0 && k < n; ++k)
+    if (!x[k]) return fail(ctx, BG_EINVAL, "null block");
+  if (!std::isfinite(volume) || volume <= 0.0) return fail(ctx, BG_ESHAPE, "volume must be finite and positive");
+  for (int64_t i = 0; i < cols * n; ++i)
+    if (!std::isfinite(weights[i]) || weights[i] < 0.0)
+      return fail(ctx, BG_ESHAPE, "band weights must be finite and non-negative");
+  cudaError_t e = cudaSetDevice(ctx->device);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaSetDevice");
+  const BoxGeo& g = ks->g;
+  const size_t pts = (size_t)g.n0 * g.n1 * g.n2;
+  if (cols == 0) {
+    if (!accumulate && (e = cudaMemsetAsync(density, 0, pts * sizeof(double), ks->stream)) != cudaSuccess)
+      return cuda_fail(ctx, e, "memset");
+    return BG_OK;
+  }
+  const int units = ks->gamma ? (int)((cols + 1) / 2) : (int)cols;
+  // enough (plane, chunk, k) blocks for two waves of 148 SMs; chunks sum in order
+  const int want = std::max(1, std::min(units, (2 * 148 + g.n2 * n - 1) / (g.n2 * n)));
+  const int per_chunk = (units + want - 1) / want;
+  const int chunks = (units + per_chunk - 1) / per_chunk;
+  auto grow = [&](double** p, size_t* have, size_t need) -> int {
+    if (*have >= need) return BG_OK;
+    cudaFree(*p);
+    *p = nullptr;
+    *have = 0;
+    void* q = nullptr;
+    cudaError_t ee = cudaMalloc(&q, need * sizeof(double));
+    if (ee != cudaSuccess) return cuda_fail(ctx, ee, "cudaMalloc");
+    *p = static_cast<double*>(q);
+    *have = need;
+    return BG_OK;
+  };
+  int rc;
+  if ((rc = grow(&ks->dens_part, &ks->dens_part_doubles, (size_t)n * chunks * pts))) return rc;
+  if ((rc = grow(&ks->dens_w, &ks->dens_w_doubles, (size_t)n * cols))) return rc;
+  e = cudaMemcpyAsync(ks->dens_w, weights, (size_t)n * cols * sizeof(double), cudaMemcpyHostToDevice, ks->stream);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "copy in");
+  Batch bt;
+  bt.nk = n;
+  for (int k = 0; k < n; ++k) {
+    const bg_op* op = ks->ops[k];
+    const int64_t dpc = op->gamma ? op->rows : 2 * op->rows;
+    CallArgs& a = bt.a[k];
+    a.x = x[k];
+    a.y = nullptr;
+    a.ldx = a.ldy = dpc;
+    a.cols = (int)cols;
+    a.units = units;
+  }
+  ks->launches += launch_density(ks->d_tabs, ks->gamma, ks->max_groups, g, bt, ks->dens_w, (int)cols, per_chunk,
+                                 chunks, ks->dens_part, ks->stream);
+  launch_density_reduce(ks->dens_part, n, chunks, g, volume, accumulate, density, ks->stream);
+  ks->launches += 1;
+  if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(ctx, e, "kernel launch");
   return BG_OK;
 }
 
@@ -989,6 +1121,16 @@ int bg_kset_apply(bg_kset* ks, const double* const* x, double* const* y, const i
   }
   cudaError_t e = cudaSetDevice(ctx->device);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaSetDevice");
+  if (fp32) {
+    bool converted = false;
+    for (int k = 0; k < n; ++k) {
+      converted = converted || !ks->ops[k]->vtf_valid;
+      if (int rc = ensure_potential_float(ks->ops[k], ks->stream)) return rc;
+    }
+    // the host-buffer path runs on its own streams
+    if (converted && ptr_kind == BG_PTR_HOST && (e = cudaStreamSynchronize(ks->stream)) != cudaSuccess)
+      return cuda_fail(ctx, e, "FP32 potential");
+  }
   std::vector<CallArgs> args(n);
   for (int k = 0; k < n; ++k) {
     bg_op* op = ks->ops[k];

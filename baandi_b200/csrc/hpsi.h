@@ -129,16 +129,18 @@ bool fp32_supported(const BoxGeo& g);
 int launch_nonlocal(const NlDev* nl, int gamma, const NlShape& sh, int max_rows, const Batch& b, cudaStream_t s,
                     StageEvents* ev);
 
-// Band density of one operator's block: part[c][z][y n0 + x] = sum over the units of
-// chunk c (in unit order) of w |psi(r)|^2, psi the unscaled inverse transform
-// (Gamma: w_a Re^2 + w_b Im^2 of a column pair).  `weights` is a device array of
-// a.cols values; chunks of `per_chunk` units.  Uses the stick buffer of tabs[0].
-int launch_density(const OpTables* tabs, int gamma, int max_groups, const BoxGeo& g, const CallArgs& a,
-                   const double* weights, int per_chunk, double* part, cudaStream_t s);
-// out[x][y][z] (C order; = or +=) = scale * sum_c part[c][z][y n0 + x] in chunk order.
-void launch_density_reduce(const double* part, int chunks, const BoxGeo& g, double scale, int accumulate,
+// Band densities of the blocks of a batch (k = 0 .. b.nk - 1, operator tables tabs[k]
+// and their stick buffers): part[k][c][z][y n0 + x] = sum over the units of chunk c of
+// block k (in unit order) of w |psi(r)|^2, psi the unscaled inverse transform (Gamma:
+// w_a Re^2 + w_b Im^2 of a column pair).  weights: device array, block k's column
+// weights at k wstride; `chunks` chunks of `per_chunk` units per block.
+int launch_density(const OpTables* tabs, int gamma, int max_groups, const BoxGeo& g, const Batch& b,
+                   const double* weights, int wstride, int per_chunk, int chunks, double* part, cudaStream_t s);
+// out (= or +=) the per-k chunk sums of part / volume, k points in order.
+void launch_density_reduce(const double* part, int nk, int chunks, const BoxGeo& g, double volume, int accumulate,
                            double* out, cudaStream_t s);
-// vt[z vstride + y n0 + x] = v[x][y][z] (C order, device); *err |= 2 on a non-finite value.
+// Copy n doubles from src to each of the ndst device pointers in dst (a device array).
+void launch_broadcast(const double* src, int64_t n, double* const* dst, int ndst, cudaStream_t s);
 void launch_potential_transpose(const double* v, const BoxGeo& g, double* vt, int* err, cudaStream_t s);
 // vtf = (float) vt plane by plane (the FP32 apply's potential).
 void launch_potential_float(const double* vt, const BoxGeo& g, float* vtf, cudaStream_t s);

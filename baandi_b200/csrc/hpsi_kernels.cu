@@ -497,12 +497,13 @@ __device__ __forceinline__ void density_weights(const CallArgs& a, int gamma, co
 // One block per SM's worth of registers: inside the loop over units the compiler keeps
 // the butterfly indices of every stage live across iterations (no spills at <= 255).
 template <int N>
-__global__ void __launch_bounds__(256, 1) k_density_planes_fast(const OpTables* __restrict__ tabs, BoxGeo g, CallArgs a,
-                                                              int gamma, const double* __restrict__ w, int per_chunk,
-                                                              double* __restrict__ part) {
-  const OpTables& t = tabs[0];
-  const int z = blockIdx.x, chunk = blockIdx.y;
-  const int u0 = chunk * per_chunk, u1 = min(a.units, u0 + per_chunk);
+__global__ void __launch_bounds__(256, 1) k_density_planes_fast(const OpTables* __restrict__ tabs, BoxGeo g, Batch b,
+                                                              int gamma, const double* __restrict__ w, int wstride,
+                                                              int per_chunk, double* __restrict__ part) {
+  const OpTables& t = tabs[blockIdx.z];
+  const CallArgs& a = b.a[blockIdx.z];
+  w += (int64_t)blockIdx.z * wstride;
+  const int z = blockIdx.x, chunk = blockIdx.y + blockIdx.z * gridDim.y;
   constexpr int P = fast::pitch_of<N>();
   extern __shared__ double2 sm[];
   double2* tw = sm;
@@ -512,6 +513,9 @@ __global__ void __launch_bounds__(256, 1) k_density_planes_fast(const OpTables* 
   for (int i = threadIdx.x; i < N; i += blockDim.x) tw[i] = g.tw0[i];
   for (int i = threadIdx.x; i < nx; i += blockDim.x) rows[i] = t.xact[i] * P;
   double* acc = part + ((int64_t)chunk * N + z) * (N * N);
+  const int u0 = blockIdx.y * per_chunk, u1 = min(a.units, u0 + per_chunk);
+  if (u0 >= u1)  // a k point with fewer units than the widest: its chunk adds nothing
+    for (int i = threadIdx.x; i < N * N; i += blockDim.x) acc[i] = 0.0;
   for (int unit = u0; unit < u1; ++unit) {
     for (int i = threadIdx.x; i < N * P; i += blockDim.x) pl[i] = make_double2(0.0, 0.0);
     __syncthreads();
@@ -534,12 +538,14 @@ __global__ void __launch_bounds__(256, 1) k_density_planes_fast(const OpTables* 
   }
 }
 
-__global__ void __launch_bounds__(256, 1) k_density_planes(const OpTables* __restrict__ tabs, BoxGeo g, CallArgs a,
-                                                        int gamma, const double* __restrict__ w, int per_chunk,
-                                                        double* __restrict__ part) {
-  const OpTables& t = tabs[0];
-  const int z = blockIdx.x, chunk = blockIdx.y;
-  const int u0 = chunk * per_chunk, u1 = min(a.units, u0 + per_chunk);
+__global__ void __launch_bounds__(256, 1) k_density_planes(const OpTables* __restrict__ tabs, BoxGeo g, Batch b,
+                                                        int gamma, const double* __restrict__ w, int wstride,
+                                                        int per_chunk, double* __restrict__ part) {
+  const OpTables& t = tabs[blockIdx.z];
+  const CallArgs& a = b.a[blockIdx.z];
+  w += (int64_t)blockIdx.z * wstride;
+  const int z = blockIdx.x, chunk = blockIdx.y + blockIdx.z * gridDim.y;
+  const int u0 = blockIdx.y * per_chunk, u1 = min(a.units, u0 + per_chunk);
   extern __shared__ double2 sm[];
   double2* tw0 = sm;
   double2* tw1 = tw0 + g.n0;
@@ -548,6 +554,8 @@ __global__ void __launch_bounds__(256, 1) k_density_planes(const OpTables* __res
   for (int i = threadIdx.x; i < g.n1; i += blockDim.x) tw1[i] = g.tw1[i];
   const int np = g.n0 * g.pitch, pts = g.n0 * g.n1;
   double* acc = part + ((int64_t)chunk * g.n2 + z) * pts;
+  if (u0 >= u1)
+    for (int i = threadIdx.x; i < pts; i += blockDim.x) acc[i] = 0.0;
   for (int unit = u0; unit < u1; ++unit) {
     for (int i = threadIdx.x; i < np; i += blockDim.x) pl[i] = make_double2(0.0, 0.0);
     __syncthreads();
@@ -569,19 +577,25 @@ __global__ void __launch_bounds__(256, 1) k_density_planes(const OpTables* __res
   }
 }
 
-// out[x][y][z] (= or +=) sum_c part[c][z][y n0 + x] / volume, chunks in order.
-__global__ void k_density_reduce(const double* __restrict__ part, int chunks, int n0, int n1, int n2, double volume,
-                                 int accumulate, double* __restrict__ out) {
+// out[x][y][z] (= or +=) sum_k (sum_c part[k][c][z][y n0 + x]) / volume: chunks in
+// order inside each k point, k points added one after the other (the arithmetic of one
+// call per k point accumulating into out).
+__global__ void k_density_reduce(const double* __restrict__ part, int nk, int chunks, int n0, int n1, int n2,
+                                 double volume, int accumulate, double* __restrict__ out) {
   const int64_t pts = (int64_t)n0 * n1, total = pts * n2;
   for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < total; p += (int64_t)gridDim.x * blockDim.x) {
     const int z = (int)(p % n2);
     const int64_t xy = p / n2;
     const int y = (int)(xy % n1), x = (int)(xy / n1);
     const int64_t q = (int64_t)z * pts + (int64_t)y * n0 + x;
-    double s = 0.0;
-    for (int c = 0; c < chunks; ++c) s += part[c * total + q];
-    s /= volume;
-    out[p] = accumulate ? out[p] + s : s;
+    double o = accumulate ? out[p] : 0.0;
+    for (int k = 0; k < nk; ++k) {
+      double s = 0.0;
+      for (int c = 0; c < chunks; ++c) s += part[((int64_t)k * chunks + c) * total + q];
+      s /= volume;
+      o = (k == 0 && !accumulate) ? s : o + s;
+    }
+    out[p] = o;
   }
 }
 
@@ -720,48 +734,59 @@ size_t density_smem_bytes(const BoxGeo& g) {
 }
 
 template <int N>
-static void density_kernels(const OpTables* tabs, int gamma, int max_groups, const BoxGeo& g, const CallArgs& a,
-                            const double* w, int per_chunk, double* part, cudaStream_t s) {
-  Batch b;
-  b.nk = 1;
-  b.a[0] = a;
+static void density_kernels(const OpTables* tabs, int gamma, int max_groups, const BoxGeo& g, const Batch& b,
+                            int max_units, const double* w, int wstride, int per_chunk, int chunks, double* part,
+                            cudaStream_t s) {
   constexpr int st = N == 0 ? 256 : 128;
-  const dim3 sgrid(max_groups, a.units, 1);
+  const dim3 sgrid(max_groups, max_units, b.nk);
   const size_t ss = stick_smem_bytes(g), ds = density_smem_bytes(g);
   if (gamma)
     k_sticks_inverse<true, N><<<sgrid, st, ss, s>>>(tabs, g, b);
   else
     k_sticks_inverse<false, N><<<sgrid, st, ss, s>>>(tabs, g, b);
-  const dim3 dgrid(g.n2, (a.units + per_chunk - 1) / per_chunk, 1);
+  const dim3 dgrid(g.n2, chunks, b.nk);
   if constexpr (N != 0) {
     if (g.n0 == N && g.n1 == N) {
-      k_density_planes_fast<N><<<dgrid, 256, ds, s>>>(tabs, g, a, gamma, w, per_chunk, part);
+      k_density_planes_fast<N><<<dgrid, 256, ds, s>>>(tabs, g, b, gamma, w, wstride, per_chunk, part);
       return;
     }
   }
-  k_density_planes<<<dgrid, 256, ds, s>>>(tabs, g, a, gamma, w, per_chunk, part);
+  k_density_planes<<<dgrid, 256, ds, s>>>(tabs, g, b, gamma, w, wstride, per_chunk, part);
 }
 
-int launch_density(const OpTables* tabs, int gamma, int max_groups, const BoxGeo& g, const CallArgs& a,
-                   const double* weights, int per_chunk, double* part, cudaStream_t s) {
-  if (a.units == 0) return 0;
+int launch_density(const OpTables* tabs, int gamma, int max_groups, const BoxGeo& g, const Batch& b,
+                   const double* weights, int wstride, int per_chunk, int chunks, double* part, cudaStream_t s) {
+  int max_units = 0;
+  for (int k = 0; k < b.nk; ++k) max_units = max(max_units, b.a[k].units);
+  if (max_units == 0 || b.nk == 0) return 0;
   switch (g.n2) {
-    case 25: density_kernels<25>(tabs, gamma, max_groups, g, a, weights, per_chunk, part, s); break;
-    case 45: density_kernels<45>(tabs, gamma, max_groups, g, a, weights, per_chunk, part, s); break;
-    case 54: density_kernels<54>(tabs, gamma, max_groups, g, a, weights, per_chunk, part, s); break;
-    case 60: density_kernels<60>(tabs, gamma, max_groups, g, a, weights, per_chunk, part, s); break;
-    case 72: density_kernels<72>(tabs, gamma, max_groups, g, a, weights, per_chunk, part, s); break;
-    case 108: density_kernels<108>(tabs, gamma, max_groups, g, a, weights, per_chunk, part, s); break;
-    default: density_kernels<0>(tabs, gamma, max_groups, g, a, weights, per_chunk, part, s); break;
+#define BG_DENS(NN) \
+  case NN: density_kernels<NN>(tabs, gamma, max_groups, g, b, max_units, weights, wstride, per_chunk, chunks, part, s); break;
+    BG_DENS(25) BG_DENS(45) BG_DENS(54) BG_DENS(60) BG_DENS(72) BG_DENS(108)
+#undef BG_DENS
+    default: density_kernels<0>(tabs, gamma, max_groups, g, b, max_units, weights, wstride, per_chunk, chunks, part, s); break;
   }
   return 2;
 }
 
-void launch_density_reduce(const double* part, int chunks, const BoxGeo& g, double volume, int accumulate,
+void launch_density_reduce(const double* part, int nk, int chunks, const BoxGeo& g, double volume, int accumulate,
                            double* out, cudaStream_t s) {
   const int64_t total = (int64_t)g.n0 * g.n1 * g.n2;
   const int blocks = (int)std::min<int64_t>((total + 255) / 256, 148 * 8);
-  k_density_reduce<<<blocks, 256, 0, s>>>(part, chunks, g.n0, g.n1, g.n2, volume, accumulate, out);
+  k_density_reduce<<<blocks, 256, 0, s>>>(part, nk, chunks, g.n0, g.n1, g.n2, volume, accumulate, out);
+}
+
+// dst[j][i] = src[i] for every destination j (blockIdx.y).
+__global__ void k_broadcast(const double* __restrict__ src, int64_t n, double* const* __restrict__ dst) {
+  double* d = dst[blockIdx.y];
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    d[i] = src[i];
+}
+
+void launch_broadcast(const double* src, int64_t n, double* const* dst, int ndst, cudaStream_t s) {
+  if (n <= 0 || ndst <= 0) return;
+  const int bx = (int)std::min<int64_t>((n + 255) / 256, std::max(1, 2 * 148 / ndst + 1));
+  k_broadcast<<<dim3(bx, ndst), 256, 0, s>>>(src, n, dst);
 }
 
 void launch_potential_transpose(const double* v, const BoxGeo& g, double* vt, int* err, cudaStream_t s) {

@@ -1340,6 +1340,9 @@ extern "C" int bg_kset_davidson_solve(bg_kset* ks, const double* const* start, c
           o.apply_precision == BG_PREC_FP32 ? 1 : 0};
   const bool graph = (o.flags & 1) == 0;
   int rc;
+  if (o.apply_precision == BG_PREC_FP32)  // the FP32 potential copies, on the set's stream
+    for (bg_op* kop : ks->ops)
+      if ((rc = ensure_potential_float(kop, ks->stream))) return rc;
   std::string err;
   int64_t launches = 0;
   // The solver (device work arrays, descriptors and the captured iteration graph) lives

@@ -59,6 +59,7 @@ struct bg_op {
   double* dens_w = nullptr;
   double* dens_part = nullptr;
   int dens_chunks = 0;  // chunks dens_part holds
+  bool vtf_valid = false;  // t.vtf (the FP32 apply's potential) matches t.vt
 };
 
 
@@ -85,6 +86,12 @@ struct bg_kset {
   // bg_kset_davidson_solve's solver (work arrays and iteration graph), kept between solves
   void* dv_cache = nullptr;
   void (*dv_free)(void*) = nullptr;
+  // bg_kset_set_potential_ptr / bg_kset_band_density_sum buffers (lazily allocated)
+  double** d_vts = nullptr;     // every operator's t.vt
+  double* dens_part = nullptr;  // [k][chunk][grid]
+  size_t dens_part_doubles = 0;
+  double* dens_w = nullptr;     // [k][column]
+  size_t dens_w_doubles = 0;
 };
 
 namespace bg {
@@ -92,6 +99,8 @@ namespace bg {
 // (cols[k]: the widest block of operator k, used to size the grids).
 int enqueue_range(bg_kset* ks, int k0, int k1, const CallArgs* args, const int64_t* cols, cudaStream_t s,
                   StageEvents* ev, int fp32 = 0);
+// Convert the operator's potential to its FP32 copy on stream s if the copy is stale.
+int ensure_potential_float(bg_op* op, cudaStream_t s);
 // Failure message on the context (or the thread's context-free slot) and status.
 int fail(bg_ctx* ctx, int code, const std::string& msg);
 int cuda_fail(bg_ctx* ctx, cudaError_t e, const char* what);

@@ -378,6 +378,44 @@ class KPointSet:
                        L.BG_PTR_DEVICE)
         return ys
 
+    def set_potential_device(self, values, epoch: int):
+        """The potential of every operator from one CUDA float64 C-order grid
+        (bg_kset_set_potential_ptr): checked and transposed once, copied to each
+        operator on the set's stream."""
+        self.ops[0]._grid_tensor(values, "potential")
+        self._check(self._lib.bg_kset_set_potential_ptr(self.handle, ctypes.c_void_p(values.data_ptr()), int(epoch),
+                                                        L.BG_PTR_DEVICE))
+        for op in self.ops:
+            op._epoch = int(epoch)
+
+    def band_density_sum(self, xs, weights, volume: float, out=None, accumulate: bool = False):
+        """sum over k of ops[k].band_density_sum(xs[k], weights[k], volume) in one batched
+        launch per stage (bg_kset_band_density_sum): xs CUDA blocks shaped (m, npw_k),
+        weights (n_k, m) on the host, out a CUDA float64 grid."""
+        import torch
+        n = len(self.ops)
+        if len(xs) != n:
+            raise SolverError(L.BG_ESHAPE, "one block per operator")
+        cols = None
+        for op, x in zip(self.ops, xs):
+            px, c, kind = op._block_kind(x)
+            if kind != L.BG_PTR_DEVICE:
+                raise SolverError(L.BG_ESHAPE, "the set's band density takes CUDA blocks")
+            if cols is not None and c != cols:
+                raise SolverError(L.BG_ESHAPE, "every block has the same columns")
+            cols = c
+        w = np.ascontiguousarray(np.asarray(weights, dtype=np.float64).reshape(n, -1))
+        if w.shape[1] != cols:
+            raise SolverError(L.BG_ESHAPE, "one weight per column of each block")
+        if out is None:
+            out = torch.zeros(self.ops[0].dims, dtype=torch.float64, device=xs[0].device)
+        self.ops[0]._grid_tensor(out, "out")
+        xa = (ctypes.c_void_p * n)(*[x.data_ptr() for x in xs])
+        self._check(self._lib.bg_kset_band_density_sum(self.handle, ctypes.cast(xa, ctypes.c_void_p), int(cols), _p(w),
+                                                       float(volume), ctypes.c_void_p(out.data_ptr()),
+                                                       1 if accumulate else 0, L.BG_PTR_DEVICE))
+        return out
+
     def set_stream(self, stream_ptr: int):
         self._check(self._lib.bg_kset_set_stream(self.handle, ctypes.c_void_p(stream_ptr)))
 

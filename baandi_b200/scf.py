@@ -128,6 +128,9 @@ class GpuScf:
             x0 = w.random_block(pw.npw, w.bands, seed_offset=100 + i, real=gamma)
             self.starts.append(torch.from_numpy(np.ascontiguousarray(x0.T)).to(dev))
         self._starts0 = [x.clone() for x in self.starts]
+        # the static diagonals back to back: the shift by v0 is one launch per map
+        self._diag_flat = torch.cat(self.diag_static)
+        self._diag_offsets = np.cumsum([0] + [d.numel() for d in self.diag_static])
         self.gamma = self.ops[0].is_real()
         self.kset = KPointSet(self.ops, self.ctx)
         self.v_ion = torch.from_numpy(np.ascontiguousarray(w.ionic_potential())).to(dev)
@@ -164,9 +167,13 @@ class GpuScf:
         v = self.v_ion + f.hxc
         v0 = float(v.mean())
         self.epoch += 1
-        for op in self.ops:
-            op.set_owned_potential_device(v, self.epoch)
-        diags = [d + v0 for d in self.diag_static] if self.o.preconditioner != "tpa" else self.diag_static
+        self.kset.set_potential_device(v, self.epoch)
+        if self.o.preconditioner != "tpa":
+            flat = self._diag_flat + v0
+            o = self._diag_offsets
+            diags = [flat[o[k]:o[k + 1]] for k in range(len(self.ops))]
+        else:
+            diags = self.diag_static
         opts = DV.Options(self.w.bands, ethr / 2.0, self.nocc, first_step=first_step,
                           max_iterations=self.o.davidson_max_iterations, preconditioner=self.o.preconditioner,
                           apply_precision=precision or self.precision_at(ethr))
@@ -176,12 +183,9 @@ class GpuScf:
             occ = [self.occupations] * len(sols)
         else:
             occ, _, ts = fermi_dirac([s.eigenvalues for s in sols], self.weights, self.electrons, self.o.smearing_ha)
-        rho = torch.zeros(self.dims, dtype=torch.float64, device=self.dev)
-        band_sum = 0.0
-        for k, (op, sol) in enumerate(zip(self.ops, sols)):
-            wk = self.weights[k] * occ[k]
-            op.band_density_sum(sol.eigenvectors, wk, self.volume, out=rho, accumulate=k > 0)
-            band_sum += float(np.dot(wk, sol.eigenvalues))
+        wk = np.stack([self.weights[k] * occ[k] for k in range(len(sols))])
+        rho = self.kset.band_density_sum([s.eigenvectors for s in sols], wk, self.volume)
+        band_sum = sum(float(np.dot(wk[k], sols[k].eigenvalues)) for k in range(len(sols)))
         energy = band_sum - f.hartree + f.xc - f.xc_integral + self.ewald
         y = self.fields.sphere_forward(rho)
         y[self.g0] = self.electrons / self.volume

@@ -254,6 +254,21 @@ int bg_kset_destroy(bg_kset* set);
  * pointer kinds and precision as bg_op_apply_block. */
 int bg_kset_apply(bg_kset* set, const double* const* x, double* const* y, const int64_t* cols,
                   int32_t ptr_kind, int32_t precision);
+/* The potential of every operator of the set from one C-order grid: the per-k install
+ * of bg_op_set_potential_ptr (the reference installs V in each k point's Hamiltonian,
+ * crates/dft-engine/src/refscf/k_map.rs:136-210 with map.rs:200-260) done once for the
+ * set: transposed and checked once (one wait; a non-finite grid leaves every operator's
+ * potential as it was, BG_ENONFINITE), then copied to each operator on the set's
+ * stream.  epoch must exceed every operator's.  BG_PTR_HOST installs per operator. */
+int bg_kset_set_potential_ptr(bg_kset* set, const double* v, uint64_t epoch, int32_t ptr_kind);
+/* density (= or, accumulate != 0, +=) sum over the set's k points of
+ * bg_op_band_density_sum(k, x[k], cols, weights + k cols, volume): the k-summed band
+ * density of a map (reference k_map.rs:136-210 with band_density_sum,
+ * crates/dft-physics/src/distributed_complex.rs:485-547) in one batched launch per
+ * stage, k points added in order.  Device blocks (layout of bg_kset_apply) and device
+ * grid (BG_PTR_DEVICE only); weights on the host, n_k x cols, finite and >= 0. */
+int bg_kset_band_density_sum(bg_kset* set, const double* const* x, int64_t cols, const double* weights,
+                             double volume, double* density, int32_t accumulate, int32_t ptr_kind);
 int bg_kset_sync(bg_kset* set);
 int bg_kset_stream(const bg_kset* set, void** stream);
 int bg_kset_set_stream(bg_kset* set, void* stream);
