@@ -250,3 +250,37 @@ class GpuScf:
         result.records = records
         result.seconds = time.perf_counter() - t0
         return result
+
+
+def main(argv=None) -> int:
+    """Time-to-solution of one workload: warm-up run, then the timed run (inside a CUDA
+    profiler range, so `ncu --profile-from-start off` sees the timed run alone)."""
+    import argparse
+
+    import torch
+
+    from . import systems
+    p = argparse.ArgumentParser(description="SCF time-to-solution on one GPU")
+    p.add_argument("--workload", default="si8", choices=sorted(systems.WORKLOADS))
+    p.add_argument("--ha-per-atom", type=float, default=1e-6, help="convergence threshold per atom (Ha)")
+    p.add_argument("--smearing", type=float, default=0.01, help="Fermi-Dirac width (Ha); 0 for fixed occupations")
+    p.add_argument("--fp32-ethr", type=float, default=None, help="FP32 local applies while ethr (Ry) >= this")
+    a = p.parse_args(argv)
+    w = systems.WORKLOADS[a.workload]()
+    opts = ScfOptions(threshold_ha=a.ha_per_atom * w.natoms, smearing_ha=a.smearing or None, fp32_ethr_ry=a.fp32_ethr)
+    scf = GpuScf(w, None, opts)
+    scf.warm_up()
+    torch.cuda.synchronize()
+    torch.cuda.cudart().cudaProfilerStart()
+    r = scf.run()
+    torch.cuda.cudart().cudaProfilerStop()
+    print(f"{w.name}: converged={r.converged} maps={len(r.records)} seconds={r.seconds:.4f} "
+          f"energy={r.energy_ha:.12f} Ha free_energy={r.free_energy_ha:.12f} Ha")
+    for m in r.records:
+        print(f"  map {m.iteration:2d} {m.kind:8s} {m.precision} ethr={m.ethr_ry:.2e} dr2={m.dr2_ry:.2e} "
+              f"h_columns={m.h_columns} davidson_iterations={m.davidson_iterations} {1000 * m.seconds:.2f} ms")
+    return 0 if r.converged else 1
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())
