@@ -101,6 +101,79 @@ __device__ __forceinline__ void tn_tile(const D* __restrict__ A, int64_t lda, co
     }
 }
 
+// 48 x 48 tiles of P = A^H B for the Davidson's Grams (m, n <= the basis capacity, 48 for
+// the k-point cells): 256 threads; thread (ti, tj) = (lane mod 16, 2 warp + lane / 16)
+// owns outputs i = i0 + ti + 16 a, j = j0 + 3 tj + b (a, b < 3).  A warp's columns are
+// uniform, so a warp whose columns all lie at or beyond n skips the arithmetic; the 16 A
+// entries a warp reads per row are shared by its two half-warps and its B entries are two
+// words, so shared memory serves 9 complex multiply-adds per thread with 8 wavefronts per
+// warp.  kBK48 rows per cp.async step, double-buffered (24 KB of shared memory).
+constexpr int kBK48 = 8;
+template <class D>
+__device__ __forceinline__ void tn_tile48(const D* __restrict__ A, int64_t lda, const D* __restrict__ B,
+                                          int64_t ldb, int i0, int j0, int m, int n, int64_t r0, int64_t r1,
+                                          D* __restrict__ P, int64_t ldp) {
+  __shared__ __align__(16) D As[2][kBK48][48];
+  __shared__ __align__(16) D Bs[2][kBK48][48];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int ti = lane & 15, tj = 2 * warp + (lane >> 4);
+  const bool warp_live = j0 + 6 * warp < n;
+  D acc[3][3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a)
+#pragma unroll
+    for (int b = 0; b < 3; ++b) acc[a][b] = Arith<D>::zero();
+  auto load = [&](int buf, int64_t rb) {
+    for (int e = tid; e < 2 * kBK48 * 48; e += 256) {
+      const int mat = e / (kBK48 * 48), idx = e - mat * (kBK48 * 48);
+      const int rr = idx % kBK48, c = idx / kBK48;
+      const int64_t r = rb + rr;
+      D* dst = mat == 0 ? &As[buf][rr][c] : &Bs[buf][rr][c];
+      const bool ok = r < r1 && (mat == 0 ? i0 + c < m : j0 + c < n);
+      if (ok)
+        async_copy(dst, mat == 0 ? A + (int64_t)(i0 + c) * lda + r : B + (int64_t)(j0 + c) * ldb + r);
+      else
+        *dst = Arith<D>::zero();
+    }
+    async_commit();
+  };
+  const int64_t steps = (r1 - r0 + kBK48 - 1) / kBK48;
+  if (steps > 0) load(0, r0);
+  for (int64_t s = 0; s < steps; ++s) {
+    const int cur = s & 1;
+    if (s + 1 < steps) {
+      load(cur ^ 1, r0 + (s + 1) * kBK48);
+      async_wait<1>();
+    } else {
+      async_wait<0>();
+    }
+    __syncthreads();
+    if (warp_live) {
+#pragma unroll
+      for (int rr = 0; rr < kBK48; ++rr) {
+        D a[3], b[3];
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+          a[q] = As[cur][rr][ti + 16 * q];
+          b[q] = Bs[cur][rr][3 * tj + q];
+        }
+#pragma unroll
+        for (int x = 0; x < 3; ++x)
+#pragma unroll
+          for (int y = 0; y < 3; ++y) acc[x][y] = Arith<D>::cmac(acc[x][y], a[x], b[y]);
+      }
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int x = 0; x < 3; ++x)
+#pragma unroll
+    for (int y = 0; y < 3; ++y) {
+      const int i = i0 + ti + 16 * x, j = j0 + 3 * tj + y;
+      if (i < m && j < n) P[(int64_t)j * ldp + i] = acc[x][y];
+    }
+}
+
 // 128 threads; thread (tr, tc) owns rows r0 + 16a + tr and columns j0 + 8b + tc of a
 // 64 x 32 tile of C (rows x n, ldc); A: rows x k (lda), B: k x n (ldb).
 template <class D>

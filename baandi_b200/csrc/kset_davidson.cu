@@ -505,18 +505,18 @@ __global__ void __launch_bounds__(128) k_dv_nn(const Bufs<D>* __restrict__ bufs,
 // Split-K partial Gram products: part[slot][s][j][i] = sum over row slice s of
 // conj(A[r][i]) B[r][j]; blockIdx.z = (slot * nk + k) * ks + s.
 template <class D>
-__global__ void __launch_bounds__(64) k_dv_tn(const Bufs<D>* __restrict__ bufs, const TN<D>* __restrict__ desc, int nk,
+__global__ void __launch_bounds__(256, 2) k_dv_tn(const Bufs<D>* __restrict__ bufs, const TN<D>* __restrict__ desc, int nk,
                                               int ks, int64_t slot_elems) {
   const int zz = blockIdx.z / ks, sidx = blockIdx.z % ks;
   const int slot = zz / nk, k = zz % nk;
   const TN<D> d = desc[zz];
-  if (d.m <= 0 || d.n <= 0 || (int)blockIdx.x * 32 >= d.m || (int)blockIdx.y * 32 >= d.n) return;
+  if (d.m <= 0 || d.n <= 0 || (int)blockIdx.x * 48 >= d.m || (int)blockIdx.y * 48 >= d.n) return;
   const int64_t rows = bufs[k].rows;
   int64_t chunk = (rows + ks - 1) / ks;
   chunk = ((chunk + 31) / 32) * 32;
   const int64_t r0 = min(rows, (int64_t)sidx * chunk), r1 = min(rows, r0 + chunk);
   D* part = bufs[k].part + slot * slot_elems + (int64_t)sidx * d.m * d.n;
-  tiles::tn_tile<D>(d.A, rows, d.B, rows, blockIdx.x * 32, blockIdx.y * 32, d.m, d.n, r0, r1, part, d.m);
+  tiles::tn_tile48<D>(d.A, rows, d.B, rows, blockIdx.x * 48, blockIdx.y * 48, d.m, d.n, r0, r1, part, d.m);
 }
 
 // G[i + j ldg] = sum_s part[slot][s][j][i] in slice order.
@@ -1042,8 +1042,8 @@ class KsetSolver {
     return 1;
   }
   int64_t tn(int nslots) {
-    const unsigned t = (unsigned)((o_.cap + 31) / 32);
-    k_dv_tn<D><<<dim3(t, t, (unsigned)(nslots * nk_ * ksplit_)), 64, 0, s_>>>(d_bufs_, d_tn_, nk_, ksplit_,
+    const unsigned t = (unsigned)((o_.cap + 47) / 48);
+    k_dv_tn<D><<<dim3(t, t, (unsigned)(nslots * nk_ * ksplit_)), 256, 0, s_>>>(d_bufs_, d_tn_, nk_, ksplit_,
                                                                              slot_elems_);
     const unsigned blocks = (unsigned)std::min<int64_t>(((int64_t)o_.cap * o_.cap + 255) / 256, 64);
     k_dv_tn_sum<D><<<dim3(blocks, 1, (unsigned)(nslots * nk_)), 256, 0, s_>>>(d_bufs_, d_tn_, nk_, ksplit_,
@@ -1105,9 +1105,10 @@ int KsetSolver<T>::prepare() {
   hb_.resize(nk_);
   max_rows_ = 0;
   for (int k = 0; k < nk_; ++k) max_rows_ = std::max<int>(max_rows_, (int)ks_->ops[k]->rows);
-  const int64_t tiles = (int64_t)((cap + 31) / 32) * ((cap + 31) / 32);
-  ksplit_ = (int)std::max<int64_t>(1, std::min<int64_t>((8 * 148 + tiles * nk_ - 1) / (tiles * nk_), 32));
-  ksplit_ = (int)std::max<int64_t>(1, std::min<int64_t>(ksplit_, (max_rows_ + 255) / 256));
+  // Gram row slices: about four 256-thread blocks per SM over all (tile, k) pairs
+  const int64_t tiles = (int64_t)((cap + 47) / 48) * ((cap + 47) / 48);
+  ksplit_ = (int)std::max<int64_t>(1, std::min<int64_t>((4 * 148 + tiles * nk_ - 1) / (tiles * nk_), 32));
+  ksplit_ = (int)std::max<int64_t>(1, std::min<int64_t>(ksplit_, (max_rows_ + 127) / 128));
   slot_elems_ = (int64_t)ksplit_ * cap * cap;
   const size_t cc = (size_t)cap * cap;
   for (int k = 0; k < nk_; ++k) {
