@@ -494,12 +494,27 @@ __device__ __forceinline__ void density_weights(const CallArgs& a, int gamma, co
   }
 }
 
-// One block per SM's worth of registers: inside the loop over units the compiler keeps
-// the butterfly indices of every stage live across iterations (no spills at <= 255).
+// Blocks of k_density_planes_fast per SM: 2 up to 45^3 planes (128 registers), 1 above,
+// where the loop over units keeps more stage indices live than 128 registers hold.
 template <int N>
-__global__ void __launch_bounds__(256, 1) k_density_planes_fast(const OpTables* __restrict__ tabs, BoxGeo g, Batch b,
-                                                              int gamma, const double* __restrict__ w, int wstride,
-                                                              int per_chunk, double* __restrict__ part) {
+constexpr int density_blocks_per_sm() {
+  return N <= 45 ? 2 : 1;
+}
+
+// One block per (z plane, chunk of units, k point).  Per unit: the y inverse on the x
+// rows holding sticks (first stage straight from the stick row), the x inverse on every
+// column y (rows without sticks are zero and not loaded), then w |psi|^2 added point by
+// point.  Up to 4 points per thread the sums stay in registers and the block writes its
+// slice once; larger planes add into the slice in global memory unit by unit.
+template <int N>
+__global__ void __launch_bounds__(256, density_blocks_per_sm<N>()) k_density_planes_fast(
+    const OpTables* __restrict__ tabs, BoxGeo g, Batch b, int gamma, const double* __restrict__ w, int wstride,
+    int per_chunk, double* __restrict__ part) {
+  using Pl = fast::Plan<N>;
+  static_assert(Pl::nst == 2, "two-stage plans");
+  constexpr int R1 = Pl::radix[0], R2 = Pl::radix[1];
+  constexpr int QP = (N * N + 255) / 256;
+  constexpr bool REG = QP <= 4;
   const OpTables& t = tabs[blockIdx.z];
   const CallArgs& a = b.a[blockIdx.z];
   w += (int64_t)blockIdx.z * wstride;
@@ -514,27 +529,62 @@ __global__ void __launch_bounds__(256, 1) k_density_planes_fast(const OpTables* 
   for (int i = threadIdx.x; i < nx; i += blockDim.x) rows[i] = t.xact[i] * P;
   double* acc = part + ((int64_t)chunk * N + z) * (N * N);
   const int u0 = blockIdx.y * per_chunk, u1 = min(a.units, u0 + per_chunk);
-  if (u0 >= u1)  // a k point with fewer units than the widest: its chunk adds nothing
+  double racc[REG ? QP : 1];
+#pragma unroll
+  for (int q = 0; q < (REG ? QP : 1); ++q) racc[q] = 0.0;
+  if (u0 >= u1 && !REG)  // a k point with fewer units than the widest: its chunk adds nothing
     for (int i = threadIdx.x; i < N * N; i += blockDim.x) acc[i] = 0.0;
+  __syncthreads();
+  fast::StageIo<double2> io;
+  io.tab = t.line_stick;
+  io.xb = t.xbits;
+  const int lane = threadIdx.x & 31;
   for (int unit = u0; unit < u1; ++unit) {
-    for (int i = threadIdx.x; i < N * P; i += blockDim.x) pl[i] = make_double2(0.0, 0.0);
-    __syncthreads();
-    const double2* row = t.sbuf + ((int64_t)unit * N + z) * t.S;
-    for (int s = threadIdx.x; s < t.S; s += blockDim.x) pl[t.stick_plane[s]] = row[s];
-    __syncthreads();
-    fast::pass<N, 1, 1>(pl, nx, LineOffTable{rows}, tw);
-    fast::pass<N, 1, P>(pl, N, LineOffCols{}, tw);
-    double wa, wb;
-    density_weights(a, gamma, w, unit, &wa, &wb);
-    for (int i = threadIdx.x; i < N * N; i += blockDim.x) {
-      const int y = i / N, x = i - y * N;
-      const double2 p = pl[x * P + y];
-      double d = unit == u0 ? 0.0 : acc[i];
-      d += wa * (p.x * p.x);
-      d += wb * (p.y * p.y);
-      acc[i] = d;
+    io.row = t.sbuf + ((int64_t)unit * N + z) * t.S;
+    int first, count;
+    fast::owned_lines(nx, &first, &count);
+    if (count > 0) {
+      fast::stage<N, R1, 1, 1, 1, fast::kInGlobal>(pl, first, count, LineOffTable{rows}, tw, lane, io);
+      fast::stage<N, R2, R1, 1, 1>(pl, first, count, LineOffTable{rows}, tw, lane);
     }
     __syncthreads();
+    fast::owned_lines(N, &first, &count);
+    if (count > 0) {
+      fast::stage<N, R1, 1, 1, P, fast::kInMask>(pl, first, count, LineOffCols{}, tw, lane, io);
+      fast::stage<N, R2, R1, 1, P>(pl, first, count, LineOffCols{}, tw, lane);
+    }
+    __syncthreads();
+    double wa, wb;
+    density_weights(a, gamma, w, unit, &wa, &wb);
+    if constexpr (REG) {
+#pragma unroll
+      for (int q = 0; q < QP; ++q) {
+        const int i = threadIdx.x + 256 * q;
+        if (i < N * N) {
+          const int y = i / N, x = i - y * N;
+          const double2 p = pl[x * P + y];
+          racc[q] += wa * (p.x * p.x);
+          racc[q] += wb * (p.y * p.y);
+        }
+      }
+    } else {
+      for (int i = threadIdx.x; i < N * N; i += blockDim.x) {
+        const int y = i / N, x = i - y * N;
+        const double2 p = pl[x * P + y];
+        double d = unit == u0 ? 0.0 : acc[i];
+        d += wa * (p.x * p.x);
+        d += wb * (p.y * p.y);
+        acc[i] = d;
+      }
+    }
+    __syncthreads();
+  }
+  if constexpr (REG) {
+#pragma unroll
+    for (int q = 0; q < QP; ++q) {
+      const int i = threadIdx.x + 256 * q;
+      if (i < N * N) acc[i] = racc[q];
+    }
   }
 }
 
