@@ -184,7 +184,7 @@ __device__ __forceinline__ D warp_sum(D v) {
 // columns m0..m-1 with the reference's pivot rule (squared pivot over the overlap
 // diagonal >= eps / 1e-12, crates/dft-solvers/src/lean_davidson.rs:62-70).  The part of
 // the new rows left of m0 is a right-looking forward substitution, parallel over the new
-// rows and columns; the new diagonal block is factored by warp 0.
+// rows and columns; the new diagonal block is factored right-looking by the whole block.
 template <class D>
 __device__ bool chol_extend(const D* S, int ld, D* L, int m0, int m, int* flag) {
   using X = Cx<D>;
@@ -212,33 +212,46 @@ __device__ bool chol_extend(const D* S, int ld, D* L, int m0, int m, int* flag) 
     }
   }
   __syncthreads();
-  if (threadIdx.x < 32) {
-    const int lane = threadIdx.x;
-    bool ok = true;
-    for (int j = m0; j < m && ok; ++j) {
-      for (int k = m0; k < j; ++k) {
-        D part = X::zero();
-        for (int p = lane; p < k; p += 32) part = X::add(part, X::mul(L[j + (size_t)p * ld], X::conj(L[k + (size_t)p * ld])));
-        part = warp_sum(part);
-        if (lane == 0) L[j + (size_t)k * ld] = X::div(X::sub(S[j + (size_t)k * ld], part), X::real(L[k + (size_t)k * ld]));
-        __syncwarp();
-      }
-      double dp = 0.0;
-      for (int p = lane; p < j; p += 32) dp += X::abs2(L[j + (size_t)p * ld]);
-      for (int o = 16; o > 0; o >>= 1) dp += __shfl_down_sync(0xffffffffu, dp, o);
-      dp = __shfl_sync(0xffffffffu, dp, 0);
-      const double sjj = X::real(S[j + (size_t)j * ld]);
-      const double d = sjj - dp;
-      const double ratio = d / sjj;
-      if (!(ratio >= kPivotRatioMin) || !isfinite(ratio)) {
-        ok = false;
-      } else {
-        if (lane == 0) L[j + (size_t)j * ld] = X::from_real(sqrt(d));
-        for (int i = lane; i < j; i += 32) L[i + (size_t)j * ld] = X::zero();
-      }
-      __syncwarp();
+  // the new diagonal block: D = S22 - L21 L21^H in the lower triangle of L's block, then a
+  // right-looking factorisation, one pivot per step (its ratio to the overlap diagonal
+  // checked by the reference's rule), the column below scaled and the trailing lower
+  // triangle updated in parallel
+  const int nr = m - m0;
+  for (int t = threadIdx.x; t < nr * nr; t += blockDim.x) {
+    const int j = m0 + t % nr, k = m0 + t / nr;
+    if (k > j) {
+      L[j + (size_t)k * ld] = X::zero();
+      continue;
     }
-    if (lane == 0) *flag = ok ? 1 : 0;
+    D acc = S[j + (size_t)k * ld];
+    for (int p = 0; p < m0; ++p) acc = X::sub(acc, X::mul(L[j + (size_t)p * ld], X::conj(L[k + (size_t)p * ld])));
+    L[j + (size_t)k * ld] = acc;
+  }
+  for (int t = threadIdx.x; t < m0 * nr; t += blockDim.x)  // above the new block
+    L[t % m0 + (size_t)(m0 + t / m0) * ld] = X::zero();
+  if (threadIdx.x == 0) *flag = 1;
+  __syncthreads();
+  for (int j = m0; j < m; ++j) {
+    const double sjj = X::real(S[j + (size_t)j * ld]);
+    const double dj = X::real(L[j + (size_t)j * ld]);
+    const double ratio = dj / sjj;
+    if (!(ratio >= kPivotRatioMin) || !isfinite(ratio)) {
+      if (threadIdx.x == 0) *flag = 0;
+      break;  // uniform: every thread read the same pivot
+    }
+    const double ljj = sqrt(dj), inv = 1.0 / ljj;
+    __syncthreads();  // every thread has read the pivot before it is replaced
+    if (threadIdx.x == 0) L[j + (size_t)j * ld] = X::from_real(ljj);
+    for (int i = j + 1 + (int)threadIdx.x; i < m; i += blockDim.x)
+      L[i + (size_t)j * ld] = X::scale(inv, L[i + (size_t)j * ld]);
+    __syncthreads();
+    const int rest = m - j - 1;
+    for (int t = threadIdx.x; t < rest * rest; t += blockDim.x) {
+      const int i = j + 1 + t % rest, k = j + 1 + t / rest;
+      if (k <= i)
+        L[i + (size_t)k * ld] = X::sub(L[i + (size_t)k * ld], X::mul(L[i + (size_t)j * ld], X::conj(L[k + (size_t)j * ld])));
+    }
+    __syncthreads();
   }
   __syncthreads();
   const bool ok = *flag != 0;
@@ -435,9 +448,11 @@ __device__ bool heev(D* A, int lda, int m, double* w, D* V, int ldv, const Bufs<
   }
   __syncthreads();
   double* Z = b.Z;
-  // A is free once the tridiagonal is read: it holds the inverse iteration's LU strips
-  tri::eig<kCtlThreads>(m, d, e, b.e2, b.wu, b.starts, b.clusters, Z, ldq, reinterpret_cast<double*>(A),
-                        (int)((size_t)ldq * ldq * sizeof(D) / sizeof(double)), sh);
+  // A (read into d, e) and V (written by the back-transform below) are free here: they
+  // hold the inverse iteration's LU strips
+  const int mat_doubles = (int)((size_t)ldq * ldq * sizeof(D) / sizeof(double));
+  tri::eig<kCtlThreads>(m, d, e, b.e2, b.wu, b.starts, b.clusters, Z, ldq, reinterpret_cast<double*>(A), mat_doubles,
+                        reinterpret_cast<double*>(V), mat_doubles, sh);
   const double* wu = b.wu;
   // stable ascending order of the eigenvalues (rank of each entry)
   for (int i = threadIdx.x; i < m; i += blockDim.x) {

@@ -5,15 +5,20 @@
 // pivmin safeguard, Gershgorin brackets, shifted LU with partial pivoting, the cluster
 // tolerance 1e-3 |T|_1 and the 10 eps |T|_1 separation of shifts inside a cluster), laid
 // out for a GPU block: every eigenvalue is bracketed by a group of lanes that each count
-// two shifts per round, and every cluster of eigenvectors is one thread's serial work.
+// four shifts per round; every eigenvector is one thread's inverse iteration, and the
+// vectors of a cluster are then orthonormalised in order (Gram-Schmidt twice) by one
+// thread.  Shifts inside a run of eigenvalues closer than 10 eps |T|_1 are spread by that
+// amount and the start vectors differ, so the iterates of a near-degenerate cluster span
+// its invariant subspace; components outside it shrink by (shift error / gap)^2 over the
+// two solves.
 //
 // Input: d (m diagonal entries) and e (m - 1 couplings, e[i] between i and i+1, any sign)
 // in shared memory.  Output: wu[j] and eigenvector j in Z, entry r at Z[r ldz + j]
 // (row-major, so that the threads of different clusters touch adjacent words), j < m,
 // eigenpairs in ascending order inside each unreduced block (blocks in row order); Z is
 // zero outside each vector's block.  Scratch: e2 (m doubles, shared), starts and clusters (m + 1 ints
-// each, shared), lu (lu_doubles, best in shared memory: 4 m doubles per thread that works
-// on a cluster at the same time, so at least 4 m).
+// each, shared), lu1 and lu2 (lu*_doubles each, best in shared memory: 4 m doubles for
+// every eigenvector computed at the same time, so together at least 4 m).
 #pragma once
 
 namespace bg {
@@ -25,12 +30,22 @@ constexpr int kMaxRounds = 100;
 constexpr int kInverseIterations = 5;
 constexpr int kExtraIterations = 1;   // after the growth criterion is met
 
+// 2^-e(v) for the binary exponent e(v) of a finite nonzero v (bits of an IEEE double):
+// an exact power of two that brings |v| into [1, 2).
+__device__ __forceinline__ double exponent_scale(double v) {
+  const long long bits = __double_as_longlong(v);
+  const long long e = (bits >> 52) & 0x7ff;                 // biased exponent, 1..2046 here
+  return __longlong_as_double((long long)(2046 - e) << 52);  // 2^(1023 - e)
+}
+
 // Sturm counts of the eigenvalues below each of the C shifts x[c] in block [s, s + n):
 // the sign changes along the leading principal minors p_0 = 1, p_1 = d_s - x,
 // p_r+1 = (d_s+r - x) p_r - e_s+r-1^2 p_r-1 (a zero minor takes the sign opposite to its
 // predecessor).  The recurrence has one fused multiply-add on its dependent chain (no
-// division), the C shifts run interleaved, and a pair of minors is rescaled by an exact
-// power of two when it leaves [2^-500, 2^500].
+// division) and the C shifts run interleaved.  After every 8 steps each pair of minors is
+// rescaled by an exact power of two (from the larger one's exponent bits, no branch): 8
+// steps grow a minor by at most (2 |T|_1)^8, far inside the exponent range for the
+// reduced matrices here (|T|_1 well below 2^60).
 template <int C>
 __device__ __forceinline__ void sturm(const double* d, const double* e2, int s, int n, const double (&x)[C],
                                       int (&cnt)[C]) {
@@ -43,7 +58,7 @@ __device__ __forceinline__ void sturm(const double* d, const double* e2, int s, 
     sg[c] = p[c] <= 0.0;
     cnt[c] = sg[c];
   }
-  for (int i = s + 1; i < s + n; ++i) {
+  auto step = [&](int i) {
     const double di = d[i], ei = e2[i - 1];
 #pragma unroll
     for (int c = 0; c < C; ++c) {
@@ -53,13 +68,21 @@ __device__ __forceinline__ void sturm(const double* d, const double* e2, int s, 
       const bool ng = r == 0.0 ? !sg[c] : r < 0.0;
       cnt[c] += ng != sg[c];
       sg[c] = ng;
-      if (!(fabs(r) < 0x1p500) || fabs(r) < 0x1p-500) {
-        const int ex = ilogb(r == 0.0 ? q[c] : r);
-        p[c] = scalbn(p[c], -ex);
-        q[c] = scalbn(q[c], -ex);
-      }
+    }
+  };
+  int i = s + 1;
+  for (; i + 8 <= s + n; i += 8) {
+#pragma unroll
+    for (int u = 0; u < 8; ++u) step(i + u);
+#pragma unroll
+    for (int c = 0; c < C; ++c) {
+      const double big = fmax(fabs(p[c]), fabs(q[c]));
+      const double f = exponent_scale(big);
+      p[c] *= f;
+      q[c] *= f;
     }
   }
+  for (; i < s + n; ++i) step(i);
 }
 
 // Block of eigenvalue j (blocks listed by their first rows in starts[0..nb]).
@@ -100,8 +123,8 @@ __device__ __forceinline__ double start_entry(int j, int r) {
 
 template <int NT>
 __device__ void eig(int m, const double* __restrict__ d, const double* __restrict__ e, double* e2, double* wu,
-                    int* starts, int* clusters, double* Z, int ldz, double* __restrict__ lu, int lu_doubles,
-                    int* sh) {
+                    int* starts, int* clusters, double* Z, int ldz, double* __restrict__ lu1, int lu1_doubles,
+                    double* __restrict__ lu2, int lu2_doubles, int* sh) {
   // 1. splits where a coupling is negligible against its neighbours; squared couplings
   if (threadIdx.x == 0) {
     int nb = 0;
@@ -193,127 +216,161 @@ __device__ void eig(int m, const double* __restrict__ d, const double* __restric
   __syncthreads();
   const int nc = sh[1];
 
-  // 4. eigenvectors: one cluster per thread, inverse iteration on its block.  A thread's
-  //    LU strips (reciprocal pivots, first and second superdiagonals of U, multipliers)
-  //    hold 4 m doubles, so at most lu_doubles / (4 m) threads work at a time.  A row
-  //    swap at elimination step r < n - 2 leaves a nonzero second superdiagonal (the
-  //    couplings inside a block are nonzero); the swap at step n - 2 is kept apart.
-  const int P = max(1, min(NT, lu_doubles / (4 * m)));
-  for (int cidx = threadIdx.x; cidx < nc && threadIdx.x < P; cidx += P) {
-    const int ja = clusters[cidx], jb = clusters[cidx + 1];
-    const int b = block_of(starts, nb, ja);
+  // 4. eigenvectors: one thread per eigenvector, inverse iteration on its block.  A
+  //    thread's LU strips (reciprocal pivots, first and second superdiagonals of U,
+  //    multipliers) hold 4 m doubles, so at most (lu1 + lu2) / (4 m) threads work at a
+  //    time.  A row swap at elimination step r < n - 2 leaves a nonzero second
+  //    superdiagonal (the couplings inside a block are nonzero); the swap at step n - 2 is
+  //    kept apart.
+  const int P1 = lu1_doubles / (4 * m), P2 = lu2_doubles / (4 * m);
+  const int P = max(1, min(NT, P1 + P2));
+  for (int j = threadIdx.x; j < m && threadIdx.x < P; j += P) {
+    const int b = block_of(starts, nb, j);
     const int s = starts[b], n = starts[b + 1] - s;
     if (n == 1) {
-      Z[(size_t)s * ldz + ja] = 1.0;
+      Z[(size_t)s * ldz + j] = 1.0;
       continue;
     }
     double gl, gu, onenrm;
     gershgorin(d, e, s, n, pivmin, &gl, &gu, &onenrm);
     const double pertol = 10.0 * kUlp * onenrm, tiny = kUlp * onenrm;
     const double dtpcrt = sqrt(0.1 / n);
-    double* ur = lu + threadIdx.x;
-    double* u1 = ur + (size_t)m * P;
-    double* u2 = u1 + (size_t)m * P;
-    double* lm = u2 + (size_t)m * P;
-    double xprev = 0.0;
-    for (int j = ja; j < jb; ++j) {
-      double x = wu[j];
-      if (j > ja && x - xprev < pertol) x = xprev + pertol;
-      xprev = x;
-      // LU with partial pivoting of T_b - x I; pivots below eps |T|_1 are raised to it
-      // (the solve then grows along the eigenvector) and kept as reciprocals
-      double ai = d[s] - x, bi = e[s], ulast = 0.0;
-      bool last_swap = false;
-      for (int r = 0; r + 1 < n; ++r) {
-        const double ci = e[s + r], an = d[s + r + 1] - x, bn = r + 2 < n ? e[s + r + 1] : 0.0;
-        double l, piv;
-        if (fabs(ai) >= fabs(ci)) {
-          l = ai != 0.0 ? ci / ai : 0.0;
-          piv = ai;
-          u1[(size_t)r * P] = bi;
-          u2[(size_t)r * P] = 0.0;
-          ai = an - l * bi;
-          bi = bn;
-        } else {
-          l = ai / ci;
-          piv = ci;
-          u1[(size_t)r * P] = an;
-          u2[(size_t)r * P] = bn;
-          ai = bi - l * an;
-          bi = -l * bn;
-          if (r + 2 == n) last_swap = true;
-        }
-        if (fabs(piv) < tiny) piv = piv < 0.0 ? -tiny : tiny;
-        ur[(size_t)r * P] = 1.0 / piv;
-        lm[(size_t)r * P] = l;
+    const bool first_region = (int)threadIdx.x < P1;
+    const int ps = first_region ? P1 : P2;
+    double* ur = first_region ? lu1 + threadIdx.x : lu2 + (threadIdx.x - P1);
+    double* u1 = ur + (size_t)m * ps;
+    double* u2 = u1 + (size_t)m * ps;
+    double* lm = u2 + (size_t)m * ps;
+    // shift: spread by pertol along a run of eigenvalues closer than pertol
+    int jr = j;
+    while (jr > s && wu[jr] - wu[jr - 1] < pertol) --jr;
+    const double x = wu[j] + (j - jr) * pertol;
+    // LU with partial pivoting of T_b - x I; pivots below eps |T|_1 are raised to it
+    // (the solve then grows along the eigenvector) and kept as reciprocals
+    double ai = d[s] - x, bi = e[s], ulast = 0.0;
+    bool last_swap = false;
+    for (int r = 0; r + 1 < n; ++r) {
+      const double ci = e[s + r], an = d[s + r + 1] - x, bn = r + 2 < n ? e[s + r + 1] : 0.0;
+      double l, piv;
+      if (fabs(ai) >= fabs(ci)) {
+        l = ai != 0.0 ? ci / ai : 0.0;
+        piv = ai;
+        u1[(size_t)r * ps] = bi;
+        u2[(size_t)r * ps] = 0.0;
+        ai = an - l * bi;
+        bi = bn;
+      } else {
+        l = ai / ci;
+        piv = ci;
+        u1[(size_t)r * ps] = an;
+        u2[(size_t)r * ps] = bn;
+        ai = bi - l * an;
+        bi = -l * bn;
+        if (r + 2 == n) last_swap = true;
       }
-      if (fabs(ai) < tiny) ai = ai < 0.0 ? -tiny : tiny;
-      ulast = fabs(ai);
-      ur[(size_t)(n - 1) * P] = 1.0 / ai;
-      // z(r) below stands for Z[(s + r) ldz + j]
-      double* zc = Z + (size_t)s * ldz + j;
-      auto z = [&](int r) -> double& { return zc[(size_t)r * ldz]; };
-      double asum = 0.0;
-      for (int r = 0; r < n; ++r) {
-        const double v = start_entry(j, r);
+      if (fabs(piv) < tiny) piv = piv < 0.0 ? -tiny : tiny;
+      ur[(size_t)r * ps] = 1.0 / piv;
+      lm[(size_t)r * ps] = l;
+    }
+    if (fabs(ai) < tiny) ai = ai < 0.0 ? -tiny : tiny;
+    ulast = fabs(ai);
+    ur[(size_t)(n - 1) * ps] = 1.0 / ai;
+    // z(r) below stands for Z[(s + r) ldz + j]
+    double* zc = Z + (size_t)s * ldz + j;
+    auto z = [&](int r) -> double& { return zc[(size_t)r * ldz]; };
+    double asum = 0.0;
+    for (int r = 0; r < n; ++r) {
+      const double v = start_entry(j, r);
+      z(r) = v;
+      asum += fabs(v);
+    }
+    int checks = 0;
+    for (int its = 0; its < kInverseIterations; ++its) {
+      const double scl = n * onenrm * fmax(kUlp, ulast) / asum;
+      // L^-1 P (scaled right-hand side); the running entry rides in a register
+      double zr = z(0) * scl;
+      for (int r = 0; r + 1 < n; ++r) {
+        double zn = z(r + 1) * scl;
+        const bool sw = r + 2 < n ? u2[(size_t)r * ps] != 0.0 : last_swap;
+        if (sw) {
+          const double t = zr;
+          zr = zn;
+          zn = t;
+        }
+        z(r) = zr;
+        zr = zn - lm[(size_t)r * ps] * zr;
+      }
+      // U^-1; the two previous entries ride in registers
+      double z1 = zr * ur[(size_t)(n - 1) * ps];
+      z(n - 1) = z1;
+      double z0 = (z(n - 2) - u1[(size_t)(n - 2) * ps] * z1) * ur[(size_t)(n - 2) * ps];
+      z(n - 2) = z0;
+      double zmax = fmax(fabs(z1), fabs(z0));
+      asum = fabs(z1) + fabs(z0);
+      for (int r = n - 3; r >= 0; --r) {
+        const double v = (z(r) - u1[(size_t)r * ps] * z0 - u2[(size_t)r * ps] * z1) * ur[(size_t)r * ps];
         z(r) = v;
+        z1 = z0;
+        z0 = v;
+        zmax = fmax(zmax, fabs(v));
         asum += fabs(v);
       }
-      int checks = 0;
-      for (int its = 0; its < kInverseIterations; ++its) {
-        const double scl = n * onenrm * fmax(kUlp, ulast) / asum;
-        // L^-1 P (scaled right-hand side); the running entry rides in a register
-        double zr = z(0) * scl;
-        for (int r = 0; r + 1 < n; ++r) {
-          double zn = z(r + 1) * scl;
-          const bool sw = r + 2 < n ? u2[(size_t)r * P] != 0.0 : last_swap;
-          if (sw) {
-            const double t = zr;
-            zr = zn;
-            zn = t;
+      if (zmax >= dtpcrt && ++checks > kExtraIterations) break;
+    }
+    double nn = 0.0;
+    for (int r = 0; r < n; ++r) nn += z(r) * z(r);
+    const double inv = 1.0 / sqrt(nn);
+    for (int r = 0; r < n; ++r) z(r) *= inv;
+  }
+  __syncthreads();
+
+  // 5. each cluster's vectors orthonormalised in order (Gram-Schmidt, twice), then the
+  //    sign: the largest entry of every vector positive
+  for (int cidx = threadIdx.x; cidx < nc; cidx += NT) {
+    const int ja = clusters[cidx], jb = clusters[cidx + 1];
+    const int b = block_of(starts, nb, ja);
+    const int s = starts[b], n = starts[b + 1] - s;
+    for (int j = ja; j < jb; ++j) {
+      double* zc = Z + (size_t)s * ldz + j;
+      auto z = [&](int r) -> double& { return zc[(size_t)r * ldz]; };
+      for (int pass = 0; pass < 2 && j > ja; ++pass) {
+        // against the earlier vectors in chunks of 8: the 8 dot products of a chunk are
+        // independent chains (classical Gram-Schmidt inside a chunk, chunks in order)
+        for (int j0 = ja; j0 < j; j0 += 8) {
+          const int cnt = min(8, j - j0);
+          const double* y = Z + (size_t)s * ldz + j0;
+          double dots[8];
+#pragma unroll
+          for (int q = 0; q < 8; ++q) dots[q] = 0.0;
+          for (int r = 0; r < n; ++r) {
+            const double zr = z(r);
+#pragma unroll
+            for (int q = 0; q < 8; ++q)
+              if (q < cnt) dots[q] = fma(zr, y[(size_t)r * ldz + q], dots[q]);
           }
-          z(r) = zr;
-          zr = zn - lm[(size_t)r * P] * zr;
+          for (int r = 0; r < n; ++r) {
+            double v = z(r);
+#pragma unroll
+            for (int q = 0; q < 8; ++q)
+              if (q < cnt) v = fma(-dots[q], y[(size_t)r * ldz + q], v);
+            z(r) = v;
+          }
         }
-        z(n - 1) = zr;
-        // U^-1; the two previous entries ride in registers
-        double z1 = zr * ur[(size_t)(n - 1) * P];
-        z(n - 1) = z1;
-        double z0 = (z(n - 2) - u1[(size_t)(n - 2) * P] * z1) * ur[(size_t)(n - 2) * P];
-        z(n - 2) = z0;
-        for (int r = n - 3; r >= 0; --r) {
-          const double v = (z(r) - u1[(size_t)r * P] * z0 - u2[(size_t)r * P] * z1) * ur[(size_t)r * P];
-          z(r) = v;
-          z1 = z0;
-          z0 = v;
-        }
-        // against the cluster's earlier vectors
-        for (int jj = ja; jj < j; ++jj) {
-          const double* y = Z + (size_t)s * ldz + jj;
-          double dot = 0.0;
-          for (int r = 0; r < n; ++r) dot += z(r) * y[(size_t)r * ldz];
-          for (int r = 0; r < n; ++r) z(r) -= dot * y[(size_t)r * ldz];
-        }
-        double zmax = 0.0;
-        asum = 0.0;
-        for (int r = 0; r < n; ++r) {
-          const double a = fabs(z(r));
-          zmax = fmax(zmax, a);
-          asum += a;
-        }
-        if (zmax >= dtpcrt && ++checks > kExtraIterations) break;
+        double nn = 0.0;
+        for (int r = 0; r < n; ++r) nn += z(r) * z(r);
+        const double inv = 1.0 / sqrt(nn);
+        for (int r = 0; r < n; ++r) z(r) *= inv;
       }
-      double nn = 0.0, big = 0.0, sgn = 1.0;
+      double big = 0.0, sgn = 1.0;
       for (int r = 0; r < n; ++r) {
         const double v = z(r);
-        nn += v * v;
         if (fabs(v) > big) {
           big = fabs(v);
           sgn = v < 0.0 ? -1.0 : 1.0;
         }
       }
-      const double inv = sgn / sqrt(nn);
-      for (int r = 0; r < n; ++r) z(r) *= inv;
+      if (sgn < 0.0)
+        for (int r = 0; r < n; ++r) z(r) = -z(r);
     }
   }
   __syncthreads();
