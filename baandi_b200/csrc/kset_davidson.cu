@@ -938,6 +938,62 @@ __global__ void __launch_bounds__(kCtlThreads, 1) k_dv_ctl(int phase, const Bufs
   if (threadIdx.x == 0) ctl[k] = c;
 }
 
+// ------------------------------------------------------------------ start and outputs
+// Per-k pointers of a solve's inputs and outputs (device array, one entry per k point).
+struct IoPtrs {
+  const void* start;   // device start block (rows x n), or null (copied from the host)
+  const double* diag;  // device diagonal, or null
+  void* vectors;       // device output block, or null (copied to the host)
+  const int* err;      // the operator's device error word
+};
+
+// Zero S, H_r, L, C of every k point and copy its start block and diagonal from device
+// pointers: one launch instead of six stream operations per k point.  blockIdx.y = k.
+template <class D>
+__global__ void k_dv_init(const Bufs<D>* __restrict__ bufs, const IoPtrs* __restrict__ io, int n, int cap) {
+  const int k = blockIdx.y;
+  const Bufs<D>& b = bufs[k];
+  const int64_t cc = (int64_t)cap * cap, rn = (int64_t)b.rows * n;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  const int64_t t0 = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  for (int64_t t = t0; t < 4 * cc; t += stride) {
+    D* m = t < cc ? b.S : (t < 2 * cc ? b.Hr : (t < 3 * cc ? b.L : b.C));
+    m[t % cc] = Cx<D>::zero();
+  }
+  const IoPtrs p = io[k];
+  if (p.start) {
+    const D* src = static_cast<const D*>(p.start);
+    for (int64_t t = t0; t < rn; t += stride) b.V[t] = src[t];
+  }
+  if (p.diag)
+    for (int64_t t = t0; t < b.rows; t += stride) const_cast<double*>(b.diag)[t] = p.diag[t];
+}
+
+// Outputs of every k point: X to the device output block, and the eigenvalues,
+// convergence flags and the operator's error word gathered for one read by the host
+// (out: nk n values, then nk n flags and nk error words as doubles).  blockIdx.y = k.
+template <class D>
+__global__ void k_dv_out(const Bufs<D>* __restrict__ bufs, const IoPtrs* __restrict__ io, int n, int nk,
+                         double* __restrict__ out) {
+  const int k = blockIdx.y;
+  const Bufs<D>& b = bufs[k];
+  const IoPtrs p = io[k];
+  const int64_t rn = (int64_t)b.rows * n;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  const int64_t t0 = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (p.vectors) {
+    D* dst = static_cast<D*>(p.vectors);
+    for (int64_t t = t0; t < rn; t += stride) dst[t] = b.X[t];
+  }
+  if (blockIdx.x == 0) {
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+      out[(int64_t)k * n + i] = b.w[i];
+      out[(int64_t)nk * n + (int64_t)k * n + i] = (double)b.conv[i];
+    }
+    if (threadIdx.x == 0) out[2 * (int64_t)nk * n + k] = (double)*p.err;
+  }
+}
+
 // ------------------------------------------------------------------ host side
 template <class T>
 struct DevOf;
@@ -987,6 +1043,8 @@ class KsetSolver {
     }
     for (void* p : dev_) cudaFree(p);
     if (h_ctl_) cudaFreeHost(h_ctl_);
+    if (h_out_) cudaFreeHost(h_out_);
+    if (h_io_) cudaFreeHost(h_io_);
   }
   int run(const double* const* start, const double* const* diagonal, int32_t ptr_kind, double* const* values,
           double* const* vectors, int32_t* const* converged, bg_davidson_stats* stats);
@@ -1007,6 +1065,10 @@ class KsetSolver {
   Bufs<D>* d_bufs_ = nullptr;
   Ctl* d_ctl_ = nullptr;
   Ctl* h_ctl_ = nullptr;
+  IoPtrs* d_io_ = nullptr;
+  IoPtrs* h_io_ = nullptr;
+  double* d_out_ = nullptr;
+  double* h_out_ = nullptr;
   NN<D>* d_nn_ = nullptr;
   TN<D>* d_tn_ = nullptr;
   CP<D>* d_cp_ = nullptr;
@@ -1150,6 +1212,10 @@ int KsetSolver<T>::prepare() {
       (rc = alloc(&d_dyn_, nk_)) || (rc = alloc(&d_opts_, 1)))
     return rc;
   if ((rc = cuda(cudaMallocHost(&h_ctl_, sizeof(Ctl) * nk_), "cudaMallocHost"))) return rc;
+  if ((rc = alloc(&d_io_, nk_)) || (rc = alloc(&d_out_, (size_t)nk_ * (2 * n + 1)))) return rc;
+  if ((rc = cuda(cudaMallocHost(&h_io_, sizeof(IoPtrs) * nk_), "cudaMallocHost")) ||
+      (rc = cuda(cudaMallocHost(&h_out_, sizeof(double) * nk_ * (2 * n + 1)), "cudaMallocHost")))
+    return rc;
   if ((rc = cuda(cudaFuncSetAttribute((const void*)k_dv_ctl<D>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)ctl_smem()),
                  "cudaFuncSetAttribute")))
@@ -1188,20 +1254,25 @@ int KsetSolver<T>::run(const double* const* start, const double* const* diagonal
   s_ = ks_->stream;
   launches_ = 0;
   if (!prepared_ && (rc = prepare())) return rc;
-  const size_t cc = (size_t)cap * cap;
+  // the pinned pointer table may still feed a copy of the previous solve
+  if ((rc = cuda(cudaStreamSynchronize(s_), "start"))) return rc;
   for (int k = 0; k < nk_; ++k) {
-    const Bufs<D>& b = hb_[k];
-    if ((rc = cuda(cudaMemsetAsync(b.S, 0, sizeof(D) * cc, s_), "memset")) ||
-        (rc = cuda(cudaMemsetAsync(b.Hr, 0, sizeof(D) * cc, s_), "memset")) ||
-        (rc = cuda(cudaMemsetAsync(b.L, 0, sizeof(D) * cc, s_), "memset")) ||
-        (rc = cuda(cudaMemsetAsync(b.C, 0, sizeof(D) * cc, s_), "memset")))
-      return rc;
-    const cudaMemcpyKind kind = ptr_kind == BG_PTR_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
-    if ((rc = cuda(cudaMemcpyAsync(b.V, start[k], sizeof(D) * (size_t)b.rows * n, kind, s_), "copy in")) ||
-        (rc = cuda(cudaMemcpyAsync(const_cast<double*>(b.diag), diagonal[k], sizeof(double) * b.rows, kind, s_),
-                   "copy in")))
-      return rc;
+    const bool dev = ptr_kind == BG_PTR_DEVICE;
+    h_io_[k] = IoPtrs{dev ? start[k] : nullptr, dev ? diagonal[k] : nullptr, dev ? vectors[k] : nullptr,
+                      ks_->ops[k]->t.err};
+    if (!dev) {  // host inputs: one copy each
+      const Bufs<D>& b = hb_[k];
+      if ((rc = cuda(cudaMemcpyAsync(b.V, start[k], sizeof(D) * (size_t)b.rows * n, cudaMemcpyHostToDevice, s_),
+                     "copy in")) ||
+          (rc = cuda(cudaMemcpyAsync(const_cast<double*>(b.diag), diagonal[k], sizeof(double) * b.rows,
+                                     cudaMemcpyHostToDevice, s_), "copy in")))
+        return rc;
+    }
   }
+  if ((rc = cuda(cudaMemcpyAsync(d_io_, h_io_, sizeof(IoPtrs) * nk_, cudaMemcpyHostToDevice, s_), "upload")))
+    return rc;
+  k_dv_init<D><<<dim3(64, nk_), 256, 0, s_>>>(d_bufs_, d_io_, n, cap);
+  launches_ += 1;
   if ((rc = cuda(cudaMemcpyAsync(d_opts_, &o_, sizeof(Opts), cudaMemcpyHostToDevice, s_), "upload"))) return rc;
   // start: H V and the Grams of the start block, descriptors written from the host
   std::vector<Ctl> c0(nk_);
@@ -1259,21 +1330,23 @@ int KsetSolver<T>::run(const double* const* start, const double* const* diagonal
   // X = V C[:, :n]; outputs
   launches_ += ctl(kFinal) + nn(1);
   if ((rc = poll(&done))) return rc;
-  std::vector<double> w(n);
-  std::vector<int> cv(n);
+  k_dv_out<D><<<dim3(64, nk_), 256, 0, s_>>>(d_bufs_, d_io_, n, nk_, d_out_);
+  launches_ += 1;
+  const size_t outn = (size_t)nk_ * (2 * n + 1);
+  if ((rc = cuda(cudaMemcpyAsync(h_out_, d_out_, sizeof(double) * outn, cudaMemcpyDeviceToHost, s_), "copy out")))
+    return rc;
+  if (ptr_kind != BG_PTR_DEVICE)
+    for (int k = 0; k < nk_; ++k)
+      if ((rc = cuda(cudaMemcpyAsync(vectors[k], hb_[k].X, sizeof(D) * (size_t)hb_[k].rows * n,
+                                     cudaMemcpyDeviceToHost, s_), "copy out")))
+        return rc;
+  if ((rc = cuda(cudaStreamSynchronize(s_), "copy out"))) return rc;
   for (int k = 0; k < nk_; ++k) {
-    const Bufs<D>& b = hb_[k];
-    const cudaMemcpyKind kind = ptr_kind == BG_PTR_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
-    if ((rc = cuda(cudaMemcpyAsync(vectors[k], b.X, sizeof(D) * (size_t)b.rows * n, kind, s_), "copy out")) ||
-        (rc = cuda(cudaMemcpyAsync(w.data(), b.w, sizeof(double) * n, cudaMemcpyDeviceToHost, s_), "copy out")) ||
-        (rc = cuda(cudaMemcpyAsync(cv.data(), b.conv, sizeof(int) * n, cudaMemcpyDeviceToHost, s_), "copy out")) ||
-        (rc = cuda(cudaStreamSynchronize(s_), "copy out")))
-      return rc;
     const Ctl& c = h_ctl_[k];
     bg_davidson_stats st{};
     for (int i = 0; i < n; ++i) {
-      values[k][i] = w[i];
-      converged[k][i] = c.iterations > 0 ? cv[i] : 0;
+      values[k][i] = h_out_[(size_t)k * n + i];
+      converged[k][i] = c.iterations > 0 ? (int)h_out_[(size_t)nk_ * n + (size_t)k * n + i] : 0;
       st.converged_count += converged[k][i];
     }
     st.iterations = c.iterations;
@@ -1287,13 +1360,8 @@ int KsetSolver<T>::run(const double* const* start, const double* const* diagonal
   }
   // a non-finite block met by the applies
   for (int k = 0; k < nk_; ++k) {
-    bg_op* op = ks_->ops[k];
-    int errw = 0;
-    if ((rc = cuda(cudaMemcpyAsync(&errw, op->t.err, sizeof(int), cudaMemcpyDeviceToHost, s_), "error word")) ||
-        (rc = cuda(cudaStreamSynchronize(s_), "error word")))
-      return rc;
-    if (errw) {
-      cudaMemsetAsync(op->t.err, 0, sizeof(int), s_);
+    if (h_out_[2 * (size_t)nk_ * n + k] != 0.0) {
+      cudaMemsetAsync(ks_->ops[k]->t.err, 0, sizeof(int), s_);
       cudaStreamSynchronize(s_);
       err_ = "non-finite block in a Davidson apply (k point " + std::to_string(k) + ")";
       return BG_ENONFINITE;

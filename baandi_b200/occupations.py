@@ -3,8 +3,11 @@
 Restates crates/dft-physics/src/occupations.rs:57-235 for one channel of capacity 2:
 the fraction p(x) = 1 / (1 + e^x) and entropy s(x) = ln(1 + e^-|x|) + |x| q (q the
 smaller tail) from exp(-|x|) only; the chemical potential is bracketed by widening
-[e_min - w, e_max + w] from w = theta, then bisected until the weighted count is within
-1e-13 of the target; TS = theta sum_k w_k 2 s((e - mu) / theta).
+[e_min - w, e_max + w] from w = theta, then located until the weighted count is within
+1e-13 of the target; TS = theta sum_k w_k 2 s((e - mu) / theta).  The reference bisects;
+here each step takes the Newton step on the count (slope sum_k w_k 2 p (1 - p) / theta)
+when it falls inside the bracket and the midpoint otherwise, so the same stopping rule is
+met in a few steps instead of about forty.
 """
 from __future__ import annotations
 
@@ -32,9 +35,16 @@ def fermi_dirac(energies, weights, electrons: float, theta_ha: float, tolerance=
     if not (0.0 < electrons < 2.0 * e.shape[1] * w.sum()):
         raise ValueError("no finite chemical potential for this electron count")
 
+    ef = e.ravel()
+    wf = np.broadcast_to((2.0 * w)[:, None], e.shape).ravel()
+
+    def fractions(mu):
+        x = (ef - mu) / theta_ha
+        t = np.exp(-np.abs(x))
+        return np.where(x >= 0.0, t, 1.0) / (1.0 + t), t
+
     def number(mu):
-        p, _ = _fraction_entropy((e - mu) / theta_ha)
-        return float(np.sum(w[:, None] * 2.0 * p))
+        return float(wf @ fractions(mu)[0])
 
     lo_e, hi_e = float(e.min()), float(e.max())
     width = theta_ha
@@ -46,18 +56,24 @@ def fermi_dirac(energies, weights, electrons: float, theta_ha: float, tolerance=
     else:
         raise ValueError("unable to bracket the chemical potential")
     mu = None
+    x = 0.5 * lo + 0.5 * hi
     for _ in range(max_iterations):
-        mid = 0.5 * lo + 0.5 * hi
-        count = number(mid)
+        p, t = fractions(x)
+        count = float(wf @ p)
         if abs(count - electrons) <= tolerance * electrons:
-            mu = mid
-            break
-        if mid in (lo, hi):
+            mu = x
             break
         if count < electrons:
-            lo = mid
+            lo = x
         else:
-            hi = mid
+            hi = x
+        slope = float(wf @ (t / (1.0 + t) ** 2)) / theta_ha
+        nxt = x - (count - electrons) / slope if slope > 0.0 else lo - 1.0
+        if not (lo < nxt < hi):
+            nxt = 0.5 * lo + 0.5 * hi
+            if nxt in (lo, hi):
+                break
+        x = nxt
     if mu is None:
         raise ValueError("the electron count did not converge")
     p, s = _fraction_entropy((e - mu) / theta_ha)
