@@ -969,6 +969,9 @@ int bg_kset_destroy(bg_kset* ks) {
   }
   if (ks->dv_cache && ks->dv_free) ks->dv_free(ks->dv_cache);
   cudaFree(ks->d_vts);
+  cudaFree(ks->d_errs);
+  cudaFree(ks->d_errv);
+  if (ks->h_errv) cudaFreeHost(ks->h_errv);
   cudaFree(ks->dens_part);
   cudaFree(ks->dens_w);
   cudaFree(ks->d_tabs);
@@ -1190,18 +1193,28 @@ int bg_kset_apply(bg_kset* ks, const double* const* x, double* const* y, const i
 
 int bg_kset_sync(bg_kset* ks) {
   if (!ks) return BG_EINVAL;
-  cudaError_t e = cudaStreamSynchronize(ks->stream);
-  if (e != cudaSuccess) return cuda_fail(ks->ctx, e, "k-point set");
-  int bad = 0;
-  for (bg_op* op : ks->ops) {
-    e = cudaMemcpy(op->err_host, op->t.err, sizeof(int), cudaMemcpyDeviceToHost);
-    if (e != cudaSuccess) return cuda_fail(ks->ctx, e, "k-point set");
-    if (op->err_host[0]) {
-      bad = 1;
-      cudaMemset(op->t.err, 0, sizeof(int));
-    }
+  const int n = (int)ks->ops.size();
+  cudaError_t e = cudaSetDevice(ks->ctx->device);
+  if (e != cudaSuccess) return cuda_fail(ks->ctx, e, "cudaSetDevice");
+  if (!ks->d_errs) {  // every operator's error word, read and cleared by one small kernel
+    std::vector<int*> h(n);
+    for (int k = 0; k < n; ++k) h[k] = ks->ops[k]->t.err;
+    void* p = nullptr;
+    if ((e = cudaMalloc(&p, n * sizeof(int*))) != cudaSuccess) return cuda_fail(ks->ctx, e, "cudaMalloc");
+    ks->d_errs = static_cast<int**>(p);
+    if ((e = cudaMalloc(&p, n * sizeof(int))) != cudaSuccess) return cuda_fail(ks->ctx, e, "cudaMalloc");
+    ks->d_errv = static_cast<int*>(p);
+    if ((e = cudaMallocHost(&p, n * sizeof(int))) != cudaSuccess) return cuda_fail(ks->ctx, e, "cudaMallocHost");
+    ks->h_errv = static_cast<int*>(p);
+    if ((e = cudaMemcpy(ks->d_errs, h.data(), n * sizeof(int*), cudaMemcpyHostToDevice)) != cudaSuccess)
+      return cuda_fail(ks->ctx, e, "cudaMemcpy");
   }
-  if (bad) return fail(ks->ctx, BG_ENONFINITE, "non-finite input coefficient");
+  launch_gather_errors(ks->d_errs, n, ks->d_errv, ks->stream);
+  e = cudaMemcpyAsync(ks->h_errv, ks->d_errv, n * sizeof(int), cudaMemcpyDeviceToHost, ks->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ks->stream);
+  if (e != cudaSuccess) return cuda_fail(ks->ctx, e, "k-point set");
+  for (int k = 0; k < n; ++k)
+    if (ks->h_errv[k]) return fail(ks->ctx, BG_ENONFINITE, "non-finite input coefficient");
   return BG_OK;
 }
 

@@ -139,6 +139,8 @@ int launch_density(const OpTables* tabs, int gamma, int max_groups, const BoxGeo
 // out (= or +=) the per-k chunk sums of part / volume, k points in order.
 void launch_density_reduce(const double* part, int nk, int chunks, const BoxGeo& g, double volume, int accumulate,
                            double* out, cudaStream_t s);
+// out[i] = *err[i], then *err[i] = 0 (the operators' error words, read and cleared).
+void launch_gather_errors(int* const* err, int n, int* out, cudaStream_t s);
 // Copy n doubles from src to each of the ndst device pointers in dst (a device array).
 void launch_broadcast(const double* src, int64_t n, double* const* dst, int ndst, cudaStream_t s);
 void launch_potential_transpose(const double* v, const BoxGeo& g, double* vt, int* err, cudaStream_t s);

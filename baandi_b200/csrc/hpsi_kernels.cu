@@ -826,6 +826,17 @@ void launch_density_reduce(const double* part, int nk, int chunks, const BoxGeo&
   k_density_reduce<<<blocks, 256, 0, s>>>(part, nk, chunks, g.n0, g.n1, g.n2, volume, accumulate, out);
 }
 
+__global__ void k_gather_errors(int* const* __restrict__ err, int n, int* __restrict__ out) {
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    out[i] = *err[i];
+    *err[i] = 0;
+  }
+}
+
+void launch_gather_errors(int* const* err, int n, int* out, cudaStream_t s) {
+  k_gather_errors<<<1, 64, 0, s>>>(err, n, out);
+}
+
 // dst[j][i] = src[i] for every destination j (blockIdx.y).
 __global__ void k_broadcast(const double* __restrict__ src, int64_t n, double* const* __restrict__ dst) {
   double* d = dst[blockIdx.y];

@@ -80,7 +80,7 @@ struct bg_kset {
   bg::StageEvents ev;
   int64_t launches = 0;
   // host-buffer applies: copy-in, compute and copy-out streams pipelined over chunks
-  static constexpr int kChunks = 4;
+  static constexpr int kChunks = 12;
   cudaStream_t pipe[3] = {nullptr, nullptr, nullptr};
   cudaEvent_t in_done[kChunks] = {}, work_done[kChunks] = {};
   // bg_kset_davidson_solve's solver (work arrays and iteration graph), kept between solves
@@ -92,6 +92,10 @@ struct bg_kset {
   size_t dens_part_doubles = 0;
   double* dens_w = nullptr;     // [k][column]
   size_t dens_w_doubles = 0;
+  // bg_kset_sync: every operator's error word, gathered for one read
+  int** d_errs = nullptr;
+  int* d_errv = nullptr;
+  int* h_errv = nullptr;
 };
 
 namespace bg {
