@@ -82,8 +82,18 @@ __device__ __forceinline__ C to_elem(double x, double y) {
 }
 
 // ---------------------------------------------------------------- pass 1
+// Blocks of the stick kernels per SM from their shared memory (twiddles and 32 lines of
+// pitch N|1), at most 8: more groups in flight keep more stick rows moving.
+template <int N, class C>
+constexpr int sticks_blocks_per_sm() {
+  if (N == 0) return 1;
+  const int bytes = (int)sizeof(C) * (N + 32 * (N | 1));
+  const int fit = 233472 / (bytes + 1024);
+  return fit < 1 ? 1 : (fit > 8 ? 8 : fit);
+}
+
 template <bool GAMMA, int N, class C = double2>
-__global__ void __launch_bounds__(N == 0 ? 256 : 128, N == 0 ? 1 : 6) k_sticks_inverse(const OpTables* __restrict__ tabs, BoxGeo g, Batch b) {
+__global__ void __launch_bounds__(N == 0 ? 256 : 128, sticks_blocks_per_sm<N, C>()) k_sticks_inverse(const OpTables* __restrict__ tabs, BoxGeo g, Batch b) {
   static_assert(N != 0 || sizeof(C) == sizeof(double2), "the runtime-plan engine is FP64 only");
   const OpTables& t = tabs[blockIdx.z];
   const CallArgs a = resolve(b.a[blockIdx.z]);
@@ -101,6 +111,8 @@ __global__ void __launch_bounds__(N == 0 ? 256 : 128, N == 0 ? 1 : 6) k_sticks_i
   bool bad = false;
   if (!GAMMA) {
     const double2* x = reinterpret_cast<const double2*>(a.x + (int64_t)unit * a.ldx);
+    // unrolled so that several entry-then-value load chains are in flight per thread
+#pragma unroll 4
     for (int e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
       const int2 en = t.entries[e];
       const double2 v = x[en.x];
@@ -112,6 +124,7 @@ __global__ void __launch_bounds__(N == 0 ? 256 : 128, N == 0 ? 1 : 6) k_sticks_i
     const bool hasb = ca + 1 < a.cols;
     const double* xa = a.x + (int64_t)ca * a.ldx;
     const double* xb = a.x + (int64_t)(hasb ? ca + 1 : ca) * a.ldx;
+#pragma unroll 4
     for (int e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
       const int2 en = t.entries[e];
       const int code = en.x;
@@ -268,7 +281,7 @@ __global__ void __launch_bounds__(256, planes_blocks_per_sm<N, C>()) k_planes_fa
 
 // ---------------------------------------------------------------- pass 3
 template <bool GAMMA, int N, class C = double2>
-__global__ void __launch_bounds__(N == 0 ? 256 : 128, N == 0 ? 1 : 6) k_sticks_forward(const OpTables* __restrict__ tabs, BoxGeo g, Batch b) {
+__global__ void __launch_bounds__(N == 0 ? 256 : 128, sticks_blocks_per_sm<N, C>()) k_sticks_forward(const OpTables* __restrict__ tabs, BoxGeo g, Batch b) {
   static_assert(N != 0 || sizeof(C) == sizeof(double2), "the runtime-plan engine is FP64 only");
   const OpTables& t = tabs[blockIdx.z];
   const CallArgs a = resolve(b.a[blockIdx.z]);
@@ -281,14 +294,17 @@ __global__ void __launch_bounds__(N == 0 ? 256 : 128, N == 0 ? 1 : 6) k_sticks_f
   const C* twg = tw_axis<C>(g, 2);
   for (int i = threadIdx.x; i < g.n2; i += blockDim.x) tw[i] = twg[i];
   const C* in = sticks_of<C>(t) + (int64_t)unit * g.n2 * t.S + s0;
+  // the group's stick rows straight into shared memory, every copy in flight at once
   for (int i = threadIdx.x; i < cnt * g.n2; i += blockDim.x) {
     const int z = i / cnt, sl = i - z * cnt;
-    st[sl * g.ld2 + z] = in[(int64_t)z * t.S + sl];
+    tiles::async_copy(&st[sl * g.ld2 + z], &in[(int64_t)z * t.S + sl]);
   }
+  tiles::async_commit();
+  tiles::async_wait<0>();
+  __syncthreads();
   if constexpr (N == 0) {
     fft_lines<-1>(st, cnt, LineOffStride{g.ld2}, 1, g.p2, tw);
   } else {
-    __syncthreads();
     fast::pass<N, -1, 1>(st, cnt, LineOffStride{fast::pitch_of<N>()}, tw);
   }
   const double s = g.inv_n;
@@ -346,6 +362,7 @@ __global__ void __launch_bounds__(N == 0 ? 256 : 128, N == 0 ? 1 : 6) k_sticks_f
     const int e0 = t.grp_entry[grp], e1 = t.grp_entry[grp + 1];
     const double2* x = reinterpret_cast<const double2*>(a.x + (int64_t)unit * a.ldx);
     double2* y = reinterpret_cast<double2*>(a.y + (int64_t)unit * a.ldy);
+#pragma unroll 4
     for (int e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
       const int2 en = t.entries[e];
       const double2 h = make_double2(st[en.y].x, st[en.y].y);
@@ -361,6 +378,7 @@ __global__ void __launch_bounds__(N == 0 ? 256 : 128, N == 0 ? 1 : 6) k_sticks_f
     const double* xb = a.x + (int64_t)(hasb ? ca + 1 : ca) * a.ldx;
     double* ya = a.y + (int64_t)ca * a.ldy;
     double* yb = a.y + (int64_t)(hasb ? ca + 1 : ca) * a.ldy;
+#pragma unroll 4
     for (int e = r0 + threadIdx.x; e < r1; e += blockDim.x) {
       const int4 rp = t.reps[e];
       const int r = rp.x;
