@@ -102,10 +102,8 @@ namespace {
 
 // Split of the P^H X reduction over rows: enough (tile, split) blocks for about eight
 // 64-thread tile blocks per SM (148 SMs), chunks a multiple of 32 rows.
-// Row slices of the split-K projection: about four 256-thread blocks per SM over all
-// 48 x 48 (projector, column) tiles.
 int ksplit_tiles(int64_t rows, int64_t tiles, int* kchunk, int64_t ks_cap = 1 << 30) {
-  int64_t ks = std::max<int64_t>(1, (4 * 148 + tiles - 1) / tiles);
+  int64_t ks = std::max<int64_t>(1, (8 * 148 + tiles - 1) / tiles);
   ks = std::min<int64_t>(ks, std::max<int64_t>(1, ks_cap));
   ks = std::min<int64_t>(ks, (rows + 31) / 32);
   int64_t chunk = (rows + ks - 1) / ks;
@@ -116,8 +114,8 @@ int ksplit_tiles(int64_t rows, int64_t tiles, int* kchunk, int64_t ks_cap = 1 <<
 }
 
 int ksplit_for(int64_t rows, int nproj, int64_t cols, int* kchunk) {
-  const int64_t tiles = ((nproj + 47) / 48) * ((cols + 47) / 48);
-  int64_t ks = std::max<int64_t>(1, (4 * 148 + tiles - 1) / tiles);
+  const int64_t tiles = ((nproj + 31) / 32) * ((cols + 31) / 32);
+  int64_t ks = std::max<int64_t>(1, (8 * 148 + tiles - 1) / tiles);
   ks = std::min<int64_t>(ks, (rows + 31) / 32);
   int64_t chunk = (rows + ks - 1) / ks;
   chunk = ((chunk + 31) / 32) * 32;
@@ -892,7 +890,7 @@ int enqueue_range(bg_kset* ks, int k0, int k1, const CallArgs* args, const int64
     NlShape sh = ks->shape;
     int64_t tiles = 0, cap = 1 << 30;
     for (int k = k0; k < k1; ++k) {
-      tiles += ((sh.nproj + 47) / 48) * ((cols[k] + 47) / 48);
+      tiles += ((sh.nproj + 31) / 32) * ((cols[k] + 31) / 32);
       if (cols[k] > 0) cap = std::min<int64_t>(cap, ks->ops[k]->part_cols / cols[k]);
     }
     sh.ksplit = ksplit_tiles(max_rows, std::max<int64_t>(tiles, 1), &sh.kchunk, cap);
