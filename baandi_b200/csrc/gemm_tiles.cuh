@@ -176,7 +176,7 @@ __device__ __forceinline__ void tn_tile48(const D* __restrict__ A, int64_t lda, 
 
 // 128 threads; thread (tr, tc) owns rows r0 + 16a + tr and columns j0 + 8b + tc of a
 // 64 x 32 tile of C (rows x n, ldc); A: rows x k (lda), B: k x n (ldb).
-template <class D>
+template <class D, bool SKIP_EMPTY = false>
 __device__ __forceinline__ void nn_tile(const D* __restrict__ A, int64_t lda, const D* __restrict__ B,
                                         int64_t ldb, D* __restrict__ C, int64_t ldc, int64_t rows, int n, int k,
                                         int64_t r0, int j0, bool accumulate) {
@@ -213,6 +213,10 @@ __device__ __forceinline__ void nn_tile(const D* __restrict__ A, int64_t lda, co
     }
     async_commit();
   };
+  // SKIP_EMPTY: the 8-column groups of the tile beyond n (the same for every thread) skip
+  // their multiply-adds (pays where n is often below the tile width, the Davidson's
+  // rotations of n <= bands columns)
+  const int ny = SKIP_EMPTY ? min(4, (n - j0 + 7) / 8) : 4;
   const int steps = (k + kBK - 1) / kBK;
   if (steps > 0) load(0, 0);
   for (int s = 0; s < steps; ++s) {
@@ -233,9 +237,11 @@ __device__ __forceinline__ void nn_tile(const D* __restrict__ A, int64_t lda, co
         b[q] = Bs[cur][p][q * 8 + tc];
       }
 #pragma unroll
-      for (int x = 0; x < 4; ++x)
+      for (int y = 0; y < 4; ++y)
+        if (y < ny) {
 #pragma unroll
-        for (int y = 0; y < 4; ++y) acc[x][y] = Arith<D>::mac(acc[x][y], a[x], b[y]);
+          for (int x = 0; x < 4; ++x) acc[x][y] = Arith<D>::mac(acc[x][y], a[x], b[y]);
+        }
     }
     __syncthreads();
   }

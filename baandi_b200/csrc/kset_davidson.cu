@@ -514,7 +514,7 @@ __global__ void __launch_bounds__(128) k_dv_nn(const Bufs<D>* __restrict__ bufs,
   const int64_t r0 = (int64_t)blockIdx.x * 64;
   const int j0 = blockIdx.y * 32;
   if (d.n <= 0 || j0 >= d.n || r0 >= rows) return;
-  tiles::nn_tile<D>(d.A, rows, d.B, d.ldb, d.C, rows, rows, d.n, d.k, r0, j0, d.accumulate != 0);
+  tiles::nn_tile<D, true>(d.A, rows, d.B, d.ldb, d.C, rows, rows, d.n, d.k, r0, j0, d.accumulate != 0);
 }
 
 // Split-K partial Gram products: part[slot][s][j][i] = sum over row slice s of
@@ -616,7 +616,7 @@ enum Phase : int {
 constexpr int kNnSlots = 2, kTnSlots = 2, kCpSlots = 3;
 
 template <class D>
-__global__ void __launch_bounds__(kCtlThreads, 1) k_dv_ctl(int phase, const Bufs<D>* __restrict__ bufs, Ctl* ctl,
+__global__ void __launch_bounds__(kCtlThreads, 1) k_dv_ctl(int phase, Bufs<D>* __restrict__ bufs, Ctl* ctl,
                                                         NN<D>* nn, TN<D>* tn, CP<D>* cp, DynCols* dyn,
                                                         const Opts* __restrict__ opts, int nk, int gamma) {
   using X = Cx<D>;
@@ -700,18 +700,32 @@ __global__ void __launch_bounds__(kCtlThreads, 1) k_dv_ctl(int phase, const Bufs
       if (threadIdx.x == 0) {
         c.contract = c.contract || (c.m + c.nact > cap && c.m > n);
         if (c.contract) {
+          // X = V C[:, :n], HX = HV C[:, :n] become the basis: the refresh phase exchanges
+          // the buffers (no copy), so the Grams read X and HX
           nn[0 * nk + k] = NN<D>{b.V, b.C, b.X, cap, n, c.m, 0};
           nn[1 * nk + k] = NN<D>{b.HV, b.C, b.HX, cap, n, c.m, 0};
-          cp[0 * nk + k] = CP<D>{b.X, b.V, n, 0};
-          cp[1 * nk + k] = CP<D>{b.HX, b.HV, n, 0};
-          tn[0 * nk + k] = TN<D>{b.V, b.V, b.S, cap, n, n};
-          tn[1 * nk + k] = TN<D>{b.V, b.HV, b.Hr, cap, n, n};
+          tn[0 * nk + k] = TN<D>{b.X, b.X, b.S, cap, n, n};
+          tn[1 * nk + k] = TN<D>{b.X, b.HX, b.Hr, cap, n, n};
         }
       }
       break;
     }
     case kRefresh: {
       if (c.contract) {
+        {
+          D* t = b.V;
+          b.V = b.X;
+          b.X = t;
+          t = b.HV;
+          b.HV = b.HX;
+          b.HX = t;
+        }
+        if (threadIdx.x == 0) {
+          bufs[k].V = b.V;
+          bufs[k].X = b.X;
+          bufs[k].HV = b.HV;
+          bufs[k].HX = b.HX;
+        }
         if (!chol_extend(b.S, cap, b.L, 0, n, &sh[4])) {
           set_err(kErrBasisDependent);
           break;
@@ -1146,7 +1160,7 @@ class KsetSolver {
   }
   int64_t iteration() {
     int64_t l = 0;
-    l += ctl(kBegin) + nn(2) + cp(0, 2) + tn(2);
+    l += ctl(kBegin) + nn(2) + tn(2);
     l += ctl(kRefresh) + nn(2) + corr();
     l += ctl(kSelect) + cp(0, 1) + tn(1);
     l += ctl(kExtend) + cp(0, 1) + nn(2) + cp(1, 2);
@@ -1330,6 +1344,9 @@ int KsetSolver<T>::run(const double* const* start, const double* const* diagonal
   // X = V C[:, :n]; outputs
   launches_ += ctl(kFinal) + nn(1);
   if ((rc = poll(&done))) return rc;
+  // contractions exchange V and X (and HV and HX) on the device: refresh the host mirror
+  if ((rc = cuda(cudaMemcpy(hb_.data(), d_bufs_, sizeof(Bufs<D>) * nk_, cudaMemcpyDeviceToHost), "buffers")))
+    return rc;
   k_dv_out<D><<<dim3(64, nk_), 256, 0, s_>>>(d_bufs_, d_io_, n, nk_, d_out_);
   launches_ += 1;
   const size_t outn = (size_t)nk_ * (2 * n + 1);
