@@ -174,6 +174,19 @@ __device__ __forceinline__ double block_sum(double v, double* red) {
   return t;
 }
 
+// Block sum with one barrier: warp partials go to `slot` (32 doubles) and every thread adds
+// them in warp order.  A slot may be written again only after another barrier, so two
+// successive calls use different slots unless a barrier lies between them.
+__device__ __forceinline__ double block_sum1(double v, double* slot) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (lane == 0) slot[warp] = v;
+  __syncthreads();
+  double t = 0.0;
+  for (int i = 0; i < (int)(blockDim.x >> 5); ++i) t += slot[i];
+  return t;
+}
+
 template <class D>
 __device__ __forceinline__ D warp_sum(D v) {
   for (int o = 16; o > 0; o >>= 1) v = Cx<D>::add(v, Cx<D>::shfl_down(v, o));
@@ -378,7 +391,7 @@ __device__ bool heev(D* A, int lda, int m, double* w, D* V, int ldv, const Bufs<
     D* x = A + (k + 1) + (size_t)k * lda;
     double part = 0.0;
     for (int i = threadIdx.x; i < L; i += blockDim.x) part += X::abs2(x[i]);
-    const double xn = sqrt(block_sum(part, red));
+    const double xn = sqrt(block_sum1(part, red));
     if (xn == 0.0) {
       if (threadIdx.x == 0) b.off[k] = X::zero();
       __syncthreads();
@@ -406,7 +419,7 @@ __device__ bool heev(D* A, int lda, int m, double* w, D* V, int ldv, const Bufs<
     __syncthreads();
     part = 0.0;
     for (int i = threadIdx.x; i < L; i += blockDim.x) part += X::dot_re(v[i], p[i]);
-    const double K = 0.5 * beta * block_sum(part, red);
+    const double K = 0.5 * beta * block_sum1(part, red + 32);
     for (int i = threadIdx.x; i < L; i += blockDim.x) q[i] = X::sub(p[i], X::scale(K, v[i]));
     __syncthreads();
     for (int t = threadIdx.x; t < L * L; t += blockDim.x) {
@@ -656,7 +669,7 @@ __global__ void __launch_bounds__(kCtlThreads, 1) k_dv_ctl(int phase, Bufs<D>* _
   const int cap = o.cap, n = o.n;
   const int64_t rows = b.rows;
   __shared__ Ctl c;
-  __shared__ double red[32];
+  __shared__ double red[64];  // two reduction slots
   __shared__ int sh[8];
   if (threadIdx.x == 0) {
     c = ctl[k];
