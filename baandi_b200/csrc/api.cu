@@ -845,8 +845,9 @@ int bg_op_band_density_sum(bg_op* op, const double* x, int64_t rows, int64_t col
     a.units = units;
     op->launches += launch_density(op->d_tabs, op->gamma ? 1 : 0, op->t.ngroups, op->g, bt, op->dens_w, 0, per_chunk,
                                    chunks, op->dens_part, op->stream);
-    launch_density_reduce(op->dens_part, 1, chunks, op->g, volume, accumulate, dd, op->stream);
-    op->launches += 1;
+    if ((rc = ensure_buf(op, &op->dens_ksum, pts))) return rc;
+    launch_density_reduce(op->dens_part, 1, chunks, op->g, volume, accumulate, op->dens_ksum, dd, op->stream);
+    op->launches += 2;
     e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(ctx, e, "kernel launch");
   }
@@ -973,6 +974,7 @@ int bg_kset_destroy(bg_kset* ks) {
   cudaFree(ks->d_errv);
   if (ks->h_errv) cudaFreeHost(ks->h_errv);
   cudaFree(ks->dens_part);
+  cudaFree(ks->dens_ksum);
   cudaFree(ks->dens_w);
   cudaFree(ks->d_tabs);
   cudaFree(ks->d_nl);
@@ -1059,8 +1061,11 @@ int bg_kset_band_density_sum(bg_kset* ks, const double* const* x, int64_t cols, 
     return BG_OK;
   }
   const int units = ks->gamma ? (int)((cols + 1) / 2) : (int)cols;
-  // enough (plane, chunk, k) blocks for two waves of 148 SMs; chunks sum in order
-  const int want = std::max(1, std::min(units, (2 * 148 + g.n2 * n - 1) / (g.n2 * n)));
+  // one unit per (plane, chunk, k) block while the partial slices fit in 1 GiB (the plane
+  // kernel then carries nothing across units and runs four blocks per SM); otherwise
+  // enough blocks for two waves of 148 SMs.  Chunks sum in order.
+  const bool one = (double)n * units * pts * sizeof(double) <= 1073741824.0;
+  const int want = one ? units : std::max(1, std::min(units, (2 * 148 + g.n2 * n - 1) / (g.n2 * n)));
   const int per_chunk = (units + want - 1) / want;
   const int chunks = (units + per_chunk - 1) / per_chunk;
   auto grow = [&](double** p, size_t* have, size_t need) -> int {
@@ -1078,6 +1083,7 @@ int bg_kset_band_density_sum(bg_kset* ks, const double* const* x, int64_t cols, 
   int rc;
   if ((rc = grow(&ks->dens_part, &ks->dens_part_doubles, (size_t)n * chunks * pts))) return rc;
   if ((rc = grow(&ks->dens_w, &ks->dens_w_doubles, (size_t)n * cols))) return rc;
+  if ((rc = grow(&ks->dens_ksum, &ks->dens_ksum_doubles, (size_t)n * pts))) return rc;
   e = cudaMemcpyAsync(ks->dens_w, weights, (size_t)n * cols * sizeof(double), cudaMemcpyHostToDevice, ks->stream);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "copy in");
   Batch bt;
@@ -1094,8 +1100,8 @@ int bg_kset_band_density_sum(bg_kset* ks, const double* const* x, int64_t cols, 
   }
   ks->launches += launch_density(ks->d_tabs, ks->gamma, ks->max_groups, g, bt, ks->dens_w, (int)cols, per_chunk,
                                  chunks, ks->dens_part, ks->stream);
-  launch_density_reduce(ks->dens_part, n, chunks, g, volume, accumulate, density, ks->stream);
-  ks->launches += 1;
+  launch_density_reduce(ks->dens_part, n, chunks, g, volume, accumulate, ks->dens_ksum, density, ks->stream);
+  ks->launches += 2;
   if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(ctx, e, "kernel launch");
   return BG_OK;
 }

@@ -136,9 +136,10 @@ int launch_nonlocal(const NlDev* nl, int gamma, const NlShape& sh, int max_rows,
 // weights at k wstride; `chunks` chunks of `per_chunk` units per block.
 int launch_density(const OpTables* tabs, int gamma, int max_groups, const BoxGeo& g, const Batch& b,
                    const double* weights, int wstride, int per_chunk, int chunks, double* part, cudaStream_t s);
-// out (= or +=) the per-k chunk sums of part / volume, k points in order.
+// out (= or +=) the per-k chunk sums of part / volume, k points in order; ksum: scratch of
+// nk grids (the per-k sums).
 void launch_density_reduce(const double* part, int nk, int chunks, const BoxGeo& g, double volume, int accumulate,
-                           double* out, cudaStream_t s);
+                           double* ksum, double* out, cudaStream_t s);
 // out[i] = *err[i], then *err[i] = 0 (the operators' error words, read and cleared).
 void launch_gather_errors(int* const* err, int n, int* out, cudaStream_t s);
 // Copy n doubles from src to each of the ndst device pointers in dst (a device array).

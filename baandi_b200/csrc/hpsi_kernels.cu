@@ -524,15 +524,15 @@ constexpr int density_blocks_per_sm() {
 // column y (rows without sticks are zero and not loaded), then w |psi|^2 added point by
 // point.  Up to 4 points per thread the sums stay in registers and the block writes its
 // slice once; larger planes add into the slice in global memory unit by unit.
-template <int N>
-__global__ void __launch_bounds__(256, density_blocks_per_sm<N>()) k_density_planes_fast(
+template <int N, bool ONE = false>
+__global__ void __launch_bounds__(256, ONE ? 4 : density_blocks_per_sm<N>()) k_density_planes_fast(
     const OpTables* __restrict__ tabs, BoxGeo g, Batch b, int gamma, const double* __restrict__ w, int wstride,
     int per_chunk, double* __restrict__ part) {
   using Pl = fast::Plan<N>;
   static_assert(Pl::nst == 2, "two-stage plans");
   constexpr int R1 = Pl::radix[0], R2 = Pl::radix[1];
   constexpr int QP = (N * N + 255) / 256;
-  constexpr bool REG = QP <= 4;
+  constexpr bool REG = !ONE && QP <= 4;
   const OpTables& t = tabs[blockIdx.z];
   const CallArgs& a = b.a[blockIdx.z];
   w += (int64_t)blockIdx.z * wstride;
@@ -557,7 +557,8 @@ __global__ void __launch_bounds__(256, density_blocks_per_sm<N>()) k_density_pla
   io.tab = t.line_stick;
   io.xb = t.xbits;
   const int lane = threadIdx.x & 31;
-  for (int unit = u0; unit < u1; ++unit) {
+  // ONE (one unit per block): no state is carried across units
+  for (int unit = u0; unit < (ONE ? min(u1, u0 + 1) : u1); ++unit) {
     io.row = t.sbuf + ((int64_t)unit * N + z) * t.S;
     int first, count;
     fast::owned_lines(nx, &first, &count);
@@ -645,29 +646,39 @@ __global__ void __launch_bounds__(256, 1) k_density_planes(const OpTables* __res
   }
 }
 
-// out[x][y][z] (= or +=) sum_k (sum_c part[k][c][z][y n0 + x]) / volume: chunks in
-// order inside each k point, k points added one after the other (the arithmetic of one
-// call per k point accumulating into out).
-__global__ void k_density_reduce(const double* __restrict__ part, int nk, int chunks, int n0, int n1, int n2,
-                                 double volume, int accumulate, double* __restrict__ out) {
+// ksum[k][q] = (sum_c part[k][c][q]) / volume, chunks in order (q in the partial slices'
+// z, y, x order); blockIdx.y = k, so the k points' chains run side by side.
+__global__ void k_density_sum_chunks(const double* __restrict__ part, int chunks, int64_t total, double volume,
+                                     double* __restrict__ ksum) {
+  const int k = blockIdx.y;
+  const double* pk = part + (int64_t)k * chunks * total;
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < total; q += (int64_t)gridDim.x * blockDim.x) {
+    double s = 0.0;
+#pragma unroll 8
+    for (int c = 0; c < chunks; ++c) s += pk[(int64_t)c * total + q];
+    ksum[(int64_t)k * total + q] = s / volume;
+  }
+}
+
+// out[x][y][z] (= or +=) sum_k ksum[k][z][y n0 + x], k points added one after the other
+// (the arithmetic of one call per k point accumulating into out).
+__global__ void k_density_sum_k(const double* __restrict__ ksum, int nk, int n0, int n1, int n2, int accumulate,
+                                double* __restrict__ out) {
   const int64_t pts = (int64_t)n0 * n1, total = pts * n2;
-  for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < total; p += (int64_t)gridDim.x * blockDim.x) {
-    const int z = (int)(p % n2);
-    const int64_t xy = p / n2;
-    const int y = (int)(xy % n1), x = (int)(xy / n1);
-    const int64_t q = (int64_t)z * pts + (int64_t)y * n0 + x;
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < total; q += (int64_t)gridDim.x * blockDim.x) {
+    const int z = (int)(q / pts);
+    const int64_t xy = q - (int64_t)z * pts;
+    const int y = (int)(xy / n0), x = (int)(xy - (int64_t)y * n0);
+    const int64_t p = ((int64_t)x * n1 + y) * n2 + z;
     double o = accumulate ? out[p] : 0.0;
     for (int k = 0; k < nk; ++k) {
-      double s = 0.0;
-      for (int c = 0; c < chunks; ++c) s += part[((int64_t)k * chunks + c) * total + q];
-      s /= volume;
+      const double s = ksum[(int64_t)k * total + q];
       o = (k == 0 && !accumulate) ? s : o + s;
     }
     out[p] = o;
   }
 }
 
-// vt[z vstride + y n0 + x] = v[(x n1 + y) n2 + z]; non-finite values set bit 1 of err.
 __global__ void k_potential_transpose(const double* __restrict__ v, int n0, int n1, int n2, int vstride,
                                       double* __restrict__ vt, int* err) {
   const int64_t pts = (int64_t)n0 * n1, total = pts * n2;
@@ -815,7 +826,10 @@ static void density_kernels(const OpTables* tabs, int gamma, int max_groups, con
   const dim3 dgrid(g.n2, chunks, b.nk);
   if constexpr (N != 0) {
     if (g.n0 == N && g.n1 == N) {
-      k_density_planes_fast<N><<<dgrid, 256, ds, s>>>(tabs, g, b, gamma, w, wstride, per_chunk, part);
+      if (per_chunk == 1)
+        k_density_planes_fast<N, true><<<dgrid, 256, ds, s>>>(tabs, g, b, gamma, w, wstride, per_chunk, part);
+      else
+        k_density_planes_fast<N><<<dgrid, 256, ds, s>>>(tabs, g, b, gamma, w, wstride, per_chunk, part);
       return;
     }
   }
@@ -838,10 +852,12 @@ int launch_density(const OpTables* tabs, int gamma, int max_groups, const BoxGeo
 }
 
 void launch_density_reduce(const double* part, int nk, int chunks, const BoxGeo& g, double volume, int accumulate,
-                           double* out, cudaStream_t s) {
+                           double* ksum, double* out, cudaStream_t s) {
   const int64_t total = (int64_t)g.n0 * g.n1 * g.n2;
+  const int bx = (int)std::min<int64_t>((total + 255) / 256, std::max<int64_t>(1, 148 * 8 / std::max(nk, 1) + 1));
+  k_density_sum_chunks<<<dim3(bx, nk), 256, 0, s>>>(part, chunks, total, volume, ksum);
   const int blocks = (int)std::min<int64_t>((total + 255) / 256, 148 * 8);
-  k_density_reduce<<<blocks, 256, 0, s>>>(part, nk, chunks, g.n0, g.n1, g.n2, volume, accumulate, out);
+  k_density_sum_k<<<blocks, 256, 0, s>>>(ksum, nk, g.n0, g.n1, g.n2, accumulate, out);
 }
 
 __global__ void k_gather_errors(int* const* __restrict__ err, int n, int* __restrict__ out) {
@@ -924,6 +940,8 @@ static void configure_one(cudaError_t& e, size_t plane_smem, size_t stick_smem) 
     if constexpr (GAMMA) {
       set((const void*)k_density_planes_fast<N>, plane_smem);
       carve((const void*)k_density_planes_fast<N>);
+      set((const void*)k_density_planes_fast<N, true>, plane_smem);
+      carve((const void*)k_density_planes_fast<N, true>);
     }
   }
 }

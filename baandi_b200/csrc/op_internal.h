@@ -58,6 +58,7 @@ struct bg_op {
   double* grid = nullptr;
   double* dens_w = nullptr;
   double* dens_part = nullptr;
+  double* dens_ksum = nullptr;  // one grid: the reduction's per-k sum
   int dens_chunks = 0;  // chunks dens_part holds
   bool vtf_valid = false;  // t.vtf (the FP32 apply's potential) matches t.vt
 };
@@ -90,6 +91,8 @@ struct bg_kset {
   double** d_vts = nullptr;     // every operator's t.vt
   double* dens_part = nullptr;  // [k][chunk][grid]
   size_t dens_part_doubles = 0;
+  double* dens_ksum = nullptr;  // [k][grid]
+  size_t dens_ksum_doubles = 0;
   double* dens_w = nullptr;     // [k][column]
   size_t dens_w_doubles = 0;
   // bg_kset_sync: every operator's error word, gathered for one read
