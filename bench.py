@@ -361,6 +361,16 @@ def run_ours(args):
                 "algorithmic_bytes_per_launch": sbytes[dname],
                 "fp64_tflops": sflops[dname] / (avg_ms[dom] / 1000.0) / 1e12,
                 "stage_ms": {s: float(m) for s, m in zip(STAGES, avg_ms)}}
+    # The plane kernel's bound in time: max(bytes / HBM peak, flops / FP64 peak); the FP64
+    # peak is nominal (148 SMs x 64 FP64 fused multiply-adds per clock at the maximum SM
+    # clock), the copy peak the measured one.
+    fp64_peak = 148 * 64 * 2 * 1.965e9 / 1e12
+    t_bytes = sbytes[dname] / (hbm_peak * 1e9) * 1e3
+    t_flops = sflops[dname] / (fp64_peak * 1e12) * 1e3
+    roofline.update({"fp64_peak_tflops": fp64_peak, "fp64_peak_kind": "nominal",
+                     "fp64_frac": roofline["fp64_tflops"] / fp64_peak,
+                     "bound_ms": max(t_bytes, t_flops), "bound_by": "fp64" if t_flops > t_bytes else "hbm",
+                     "frac_of_bound": max(t_bytes, t_flops) / avg_ms[dom]})
 
     # CPU baseline: rank 0, N=1 only
     cpu = None
