@@ -291,6 +291,7 @@ int build_op(bg_ctx* ctx, const bg_basis_desc* b, const bg_projectors* pr, int64
   T.S = S;
   T.ngroups = ngroups;
   T.nxact = (int)xact.size();
+  T.yper = plane_lines_per_warp(n0, n1, T.nxact);
   int rc;
   int* d_int;
   if ((rc = upload(op.get(), grp_stick.data(), grp_stick.size(), &d_int))) return rc;

@@ -404,6 +404,53 @@ __device__ __forceinline__ void owned_lines(int nlines, int* first, int* count) 
   *count = min(nlines, *first + per) - *first;
 }
 
+// Whole lines per round of a radix-R stage on lines of N (one butterfly per lane).
+__host__ __device__ constexpr int lines_per_round(int N, int R) { return N / R <= 32 ? 32 / (N / R) : 1; }
+
+// Lines per warp for a pass of a two-stage plan whose radix-R1 round loop runs A times
+// and whose span-R1 round loop (the radix-R2 stage, or the fused middle of
+// inverse_weight_forward) runs B times, LA and LB whole lines per round; warps own
+// contiguous blocks of that many lines.  A round issues the same instructions whether its
+// lines fill the warp or not, so the count is chosen from ceil(L / warps) upwards to
+// minimise the rounds all warps run together, with the busiest warp running no more rounds
+// than at ceil(L / warps).  27 lines of 45 on 8 warps: blocks of 6,6,6,6,3 lines run 14
+// rounds of the two stages, blocks of 4,..,4,3 run 20.  Evaluated at compile time or on
+// the host: the search is too long to repeat in every block.
+__host__ __device__ constexpr int balanced_lines(int LA, int LB, int A, int B, int nlines, int nw) {
+  if (nlines <= 0) return 1;
+  const int base = (nlines + nw - 1) / nw;
+  int best = base, best_total = 0, limit = 0;
+  for (int per = base; per <= nlines && per < base + LA * LB; ++per) {
+    int total = 0, worst = 0;
+    for (int f = 0; f < nlines; f += per) {
+      const int c = per < nlines - f ? per : nlines - f;
+      const int r = A * ((c + LA - 1) / LA) + B * ((c + LB - 1) / LB);
+      total += r;
+      worst = worst > r ? worst : r;
+    }
+    if (per == base) {
+      best_total = total;
+      limit = worst;
+    } else if (worst <= limit && total < best_total) {
+      best = per;
+      best_total = total;
+    }
+  }
+  return best;
+}
+template <int N, int A, int B>
+__host__ __device__ constexpr int balanced_lines(int nlines, int nw) {
+  return balanced_lines(lines_per_round(N, Plan<N>::radix[0]), lines_per_round(N, Plan<N>::radix[1]), A, B, nlines,
+                        nw);
+}
+
+// This warp's block of `per` lines of a pass over nlines lines.
+__device__ __forceinline__ void owned_block(int nlines, int per, int* first, int* count) {
+  const int warp = threadIdx.x >> 5;
+  *first = min(nlines, warp * per);
+  *count = min(nlines, *first + per) - *first;
+}
+
 // A whole pass over nlines lines; ends with __syncthreads.
 template <int N, int SIGN, int ES, class Off, class C>
 __device__ __forceinline__ void pass(C* base, int nlines, Off off, const C* __restrict__ tw) {

@@ -255,7 +255,7 @@ __global__ void __launch_bounds__(256, planes_blocks_per_sm<N, C>()) k_planes_fa
   io.xb = t.xbits;
   const int lane = threadIdx.x & 31;
   int first, count;
-  fast::owned_lines(nx, &first, &count);
+  fast::owned_block(nx, t.yper, &first, &count);
   if (count > 0) {
     fast::stage<N, R1, 1, 1, 1, fast::kInGlobal>(pl, first, count, LineOffTable{rows}, tw, lane, io);
     fast::stage<N, R2, R1, 1, 1>(pl, first, count, LineOffTable{rows}, tw, lane);
@@ -264,7 +264,8 @@ __global__ void __launch_bounds__(256, planes_blocks_per_sm<N, C>()) k_planes_fa
   __syncthreads();
   {
     int xf, xc;
-    fast::owned_lines(N, &xf, &xc);
+    constexpr int xper = fast::balanced_lines<N, 2, 1>(N, 8);
+    fast::owned_block(N, xper, &xf, &xc);
     if (xc > 0) {
       // line = column y, element = x: weight V(x, y, z)
       auto wgt = [&](int y, int x) -> T { return VS ? vs[y * N + x] : v[y * N + x]; };
@@ -272,7 +273,7 @@ __global__ void __launch_bounds__(256, planes_blocks_per_sm<N, C>()) k_planes_fa
     }
   }
   __syncthreads();
-  fast::owned_lines(nx, &first, &count);
+  fast::owned_block(nx, t.yper, &first, &count);
   if (count > 0) {
     fast::stage<N, R1, 1, -1, 1>(pl, first, count, LineOffTable{rows}, tw, lane);
     fast::stage<N, R2, R1, -1, 1, fast::kOutGlobal>(pl, first, count, LineOffTable{rows}, tw, lane, io);
@@ -561,13 +562,14 @@ __global__ void __launch_bounds__(256, ONE ? 4 : density_blocks_per_sm<N>()) k_d
   for (int unit = u0; unit < (ONE ? min(u1, u0 + 1) : u1); ++unit) {
     io.row = t.sbuf + ((int64_t)unit * N + z) * t.S;
     int first, count;
-    fast::owned_lines(nx, &first, &count);
+    fast::owned_block(nx, t.yper, &first, &count);
     if (count > 0) {
       fast::stage<N, R1, 1, 1, 1, fast::kInGlobal>(pl, first, count, LineOffTable{rows}, tw, lane, io);
       fast::stage<N, R2, R1, 1, 1>(pl, first, count, LineOffTable{rows}, tw, lane);
     }
     __syncthreads();
-    fast::owned_lines(N, &first, &count);
+    constexpr int xper = fast::balanced_lines<N, 1, 1>(N, 8);
+    fast::owned_block(N, xper, &first, &count);
     if (count > 0) {
       fast::stage<N, R1, 1, 1, P, fast::kInMask>(pl, first, count, LineOffCols{}, tw, lane, io);
       fast::stage<N, R2, R1, 1, P>(pl, first, count, LineOffCols{}, tw, lane);
@@ -707,6 +709,19 @@ static size_t plane_smem_bytes_f32(const BoxGeo& g) {
          (v_in_smem_t<float2>(g.n0) ? sizeof(float) * (size_t)g.n0 * g.n1 : 0) + sizeof(int) * (size_t)g.n0;
 }
 static size_t stick_smem_bytes_f32(const BoxGeo& g) { return sizeof(float2) * ((size_t)g.n2 + (size_t)g.sg * g.ld2); }
+
+int plane_lines_per_warp(int n0, int n1, int nlines) {
+  if (n0 != n1) return 1;
+  switch (n0) {
+    case 25: return fast::balanced_lines<25, 1, 1>(nlines, 8);
+    case 45: return fast::balanced_lines<45, 1, 1>(nlines, 8);
+    case 54: return fast::balanced_lines<54, 1, 1>(nlines, 8);
+    case 60: return fast::balanced_lines<60, 1, 1>(nlines, 8);
+    case 72: return fast::balanced_lines<72, 1, 1>(nlines, 8);
+    case 108: return fast::balanced_lines<108, 1, 1>(nlines, 8);
+    default: return 1;
+  }
+}
 
 bool fp32_supported(const BoxGeo& g) {
   if (g.n0 != g.n1 || g.n1 != g.n2) return false;
