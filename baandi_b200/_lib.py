@@ -19,7 +19,8 @@ BG_EDEVICE = 4
 BG_ETIMEOUT = 5
 BG_EINVAL = 6
 BG_ENOMEM = 7
-BG_PRECOND_SMOOTH, BG_PRECOND_TPA, BG_PRECOND_RITZ_SHIFT = 0, 1, 2
+BG_PRECOND_SMOOTH, BG_PRECOND_TPA, BG_PRECOND_RITZ_SHIFT, BG_PRECOND_LEARNED = 0, 1, 2, 3
+BG_LEARNED_PARAMS = 4609
 BG_PTR_HOST = 0
 BG_PTR_DEVICE = 1
 BG_PREC_FP64, BG_PREC_FP32 = 0, 1
@@ -58,7 +59,13 @@ class DavidsonOptions(ctypes.Structure):
 
 class DavidsonStats(ctypes.Structure):
     _fields_ = [("iterations", _i32), ("reduced_solves", _i32), ("h_calls", _i64), ("h_columns", _i64),
-                ("repairs", _i32), ("contractions", _i32), ("dropped", _i32), ("converged_count", _i32)]
+                ("repairs", _i32), ("contractions", _i32), ("dropped", _i32), ("converged_count", _i32),
+                ("fallbacks", _i32), ("reserved", _i32)]
+
+
+class LearnedSamples(ctypes.Structure):
+    _fields_ = [("n", _i64), ("ncols", _i32), ("feats", _p), ("base", _p), ("a", _p), ("z", _p), ("col", _p),
+                ("ecol", _p)]
 
 
 class MixerProfile(ctypes.Structure):
@@ -125,6 +132,12 @@ SIGNATURES = {
     "bg_davidson_solve": [_p, _p, _p, ctypes.POINTER(DavidsonOptions), _p, _p, _p, ctypes.POINTER(DavidsonStats)],
     "bg_kset_davidson_solve": [_p, _p, _p, ctypes.POINTER(DavidsonOptions), _i32, _p, _p, _p, _p],
     "bg_op_create_dense": [_p, _i64, _p, _i32, _i64, _pp],
+    "bg_learned_set": [_p, _p],
+    "bg_learned_clear": [_p],
+    "bg_learned_samples_build": [_p, _i64, _i32, _i32, _p, _p, _p, _p, _p, _i32, _i64,
+                                 ctypes.POINTER(LearnedSamples), _p],
+    "bg_learned_loss_grad": [_p, ctypes.POINTER(LearnedSamples), _p, _p, _p, _p, _p],
+    "bg_learned_adam": [_p, _p, _p, _p, _p, _p, _i32, ctypes.c_float, _p],
     "bg_local_apply_noalloc": [_p, _i64, _p, _p, _p, _p, _p, _i64, _p],
     "bg_setup_volume": [_p, ctypes.POINTER(_dbl)],
     "bg_setup_basis": [_p, _dbl, _p, _i64, ctypes.POINTER(_i64), _p, _p, _p],

@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include "learned.cuh"
 
 namespace bg {
 
@@ -74,14 +75,17 @@ __device__ __forceinline__ double block_sum256(double v, double* red) {
 // Correction of one band column from its Ritz vector x and H x (rows entries):
 // kind 0 (smooth) out = (hx - e x) / d(diag, e); kind 1 (TPA) out = -(hx - e x)
 // tpa(diag, s) with s = max(0.1, sum |x|^2 diag / sum |x|^2), diag = kinetic;
-// kind 2 (Ritz shift) out = -(hx - e x) / max(diag - e, 0.1).  Returns |out|^2 (all
-// threads of the 256-thread block).
-template <class D>
+// kind 2 (Ritz shift) out = -(hx - e x) / max(diag - e, 0.1); kind 3 (learned) the TPA
+// factor times exp(clamp(m(f))) of the per-G network whose parameters `net` holds as
+// floats in shared memory (learned.cuh).  Returns |out|^2 (all threads of the 256-thread
+// block).
+template <class D, bool LEARNED = false>
 __device__ double correction_column(const D* __restrict__ x, const D* __restrict__ hx,
                                     const double* __restrict__ diag, double e, int kind, int64_t rows,
-                                    D* __restrict__ out, double* red) {
-  double scale = 0.0;
-  if (kind == 1) {
+                                    D* __restrict__ out, double* red, const float* net = nullptr) {
+  if constexpr (LEARNED) kind = 3;
+  double scale = 0.0, rms = 0.0;
+  if (kind == 1 || kind == 3) {
     double w = 0.0, wt = 0.0;
     for (int64_t r = threadIdx.x; r < rows; r += blockDim.x) {
       const double a = Arith<D>::norm2(x[r]);
@@ -92,12 +96,23 @@ __device__ double correction_column(const D* __restrict__ x, const D* __restrict
     wt = block_sum256(wt, red);
     scale = fmax(wt / w, 0.1);
   }
+  if (LEARNED) {
+    double q = 0.0;
+    for (int64_t r = threadIdx.x; r < rows; r += blockDim.x)
+      q += Arith<D>::norm2(Arith<D>::add(hx[r], Arith<D>::scale(-e, x[r])));
+    rms = sqrt(block_sum256(q, red) / (double)rows);
+  }
   double acc = 0.0;
   for (int64_t r = threadIdx.x; r < rows; r += blockDim.x) {
     const D res = Arith<D>::add(hx[r], Arith<D>::scale(-e, x[r]));
     double f;
     if (kind == 1)
       f = -tpa_weight(diag[r], scale);
+    else if (LEARNED) {
+      float in[learned::kIn];
+      learned::features(diag[r], scale, e, rms > 0.0 ? sqrt(Arith<D>::norm2(res)) / rms : 1.0, in);
+      f = -tpa_weight(diag[r], scale) * learned::multiplier(learned::forward(net, in));
+    }
     else if (kind == 2)
       f = -1.0 / fmax(diag[r] - e, 0.1);
     else

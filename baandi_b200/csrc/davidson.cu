@@ -43,16 +43,19 @@ constexpr double kEps = 2.220446049250313e-16;
 constexpr double kDependence = 1e-12;  // crates/dft-numerics/src/linalg.rs:12
 
 // ------------------------------------------------------------------ kernels
-// E[:, j] = correction of band j (correction_column, preconditioner `kind`);
-// norms2[j] = |E[:, j]|^2.
-template <class D>
+// E[:, j] = correction of band j (correction_column, preconditioner `kind`; kind 3 reads
+// the learned network's BF16 parameters `net`); norms2[j] = |E[:, j]|^2.
+template <class D, bool LEARNED>
 __global__ void __launch_bounds__(256) k_corrections(const D* __restrict__ X, const D* __restrict__ HX, int64_t ld,
                                                      const double* __restrict__ diag, const double* __restrict__ lambda,
                                                      D* __restrict__ E, double* __restrict__ norms2, int64_t rows,
-                                                     int kind) {
+                                                     int kind, const __nv_bfloat16* __restrict__ net) {
   __shared__ double red[256];
+  __shared__ float wnet[LEARNED ? learned::kParams : 1];
+  if constexpr (LEARNED) learned::load_params(net, wnet);
   const int j = blockIdx.x;
-  const double n2 = correction_column(X + j * ld, HX + j * ld, diag, lambda[j], kind, rows, E + j * ld, red);
+  const double n2 =
+      correction_column<D, LEARNED>(X + j * ld, HX + j * ld, diag, lambda[j], kind, rows, E + j * ld, red, wnet);
   if (threadIdx.x == 0) norms2[j] = n2;
 }
 
@@ -88,6 +91,7 @@ class Solver {
   Solver(bg_op* op, int n, int cap, const bg_davidson_options& o) : op_(op), n_(n), cap_(cap), o_(o) {
     rows_ = op->rows;
     s_ = op->stream;
+    kind_ = o.preconditioner;
   }
   ~Solver() {
     for (void* p : dev_) cudaFree(p);
@@ -102,6 +106,7 @@ class Solver {
   int64_t rows_;
   int n_, cap_;
   bg_davidson_options o_;
+  int kind_;  // preconditioner in use: the learned one gives way to TPA when the solve stalls
   cudaStream_t s_;
   std::vector<void*> dev_;
   D *V_ = nullptr, *HV_ = nullptr, *X_ = nullptr, *HX_ = nullptr, *E_ = nullptr, *Er_ = nullptr, *HE_ = nullptr;
@@ -113,6 +118,9 @@ class Solver {
   std::vector<double> values_, old_;
   bg_davidson_stats stats_{};
   std::string err_;
+  static constexpr int kStallSteps = 5;
+  double best_change_ = INFINITY;
+  int stalled_ = 0;
 
   double band_threshold(int i) const {
     return (o_.first_step || i < o_.occupied) ? o_.threshold : std::max(5.0 * o_.threshold, 5e-6);
@@ -257,7 +265,11 @@ int Solver<T>::corrections(const std::vector<int>& active, int m, const double* 
   if (!rc) rc = rotate(HV_, m, cs.data(), k, HX_);
   if (rc) return rc;
   cudaMemcpyAsync(lam_, lam.data(), sizeof(double) * k, cudaMemcpyHostToDevice, s_);
-  k_corrections<D><<<k, 256, 0, s_>>>(X_, HX_, rows_, diag_, lam_, Er_, norms_, rows_, o_.preconditioner);
+  if (kind_ == BG_PRECOND_LEARNED)
+    k_corrections<D, true><<<k, 256, 0, s_>>>(X_, HX_, rows_, diag_, lam_, Er_, norms_, rows_, kind_,
+                                              static_cast<const __nv_bfloat16*>(op_->ctx->learned));
+  else
+    k_corrections<D, false><<<k, 256, 0, s_>>>(X_, HX_, rows_, diag_, lam_, Er_, norms_, rows_, kind_, nullptr);
   std::vector<double> n2(k);
   cudaMemcpyAsync(n2.data(), norms_, sizeof(double) * k, cudaMemcpyDeviceToHost, s_);
   if ((rc = sync("corrections"))) return rc;
@@ -442,12 +454,28 @@ int Solver<T>::run(const T* start, const double* diagonal, double* values_out, T
       // basis rotated to its Ritz vectors: C = I, values unchanged
     }
     active.clear();
+    double dmax = 0.0;
     for (int i = 0; i < n_; ++i) {
       const double change = std::fabs(values_[i] - old_[i]);
       conv[i] = change < band_threshold(i);
       if (!conv[i]) active.push_back(i);
+      dmax = std::max(dmax, change);
     }
     iterations = step + 1;
+    if (kind_ == BG_PRECOND_LEARNED && !active.empty()) {
+      // TPA fallback: the largest Ritz change has not fallen below its best for
+      // kStallSteps iterations, or half the iteration budget is spent
+      if (dmax < best_change_) {
+        best_change_ = dmax;
+        stalled_ = 0;
+      } else {
+        ++stalled_;
+      }
+      if (stalled_ >= kStallSteps || 2 * iterations >= o_.max_iterations) {
+        kind_ = BG_PRECOND_TPA;
+        stats_.fallbacks = 1;
+      }
+    }
     if (active.empty() || iterations == o_.max_iterations) break;
     if (m + (int)active.size() > cap_) {
       if ((rc = contract(m))) return rc;
@@ -488,9 +516,11 @@ extern "C" int bg_davidson_solve(bg_op* op, const double* start, const double* d
   // crates/dft-solvers/src/ref_davidson.rs:133-146
   const bool bad = n == 0 || n > dim || cap < std::min<int64_t>(2 * n, dim) || o.occupied > n || o.occupied < 0 ||
                    o.max_iterations <= 0 || !std::isfinite(o.threshold) || o.threshold <= 0.0 || cap > op->cap ||
-                   o.preconditioner < BG_PRECOND_SMOOTH || o.preconditioner > BG_PRECOND_RITZ_SHIFT ||
+                   o.preconditioner < BG_PRECOND_SMOOTH || o.preconditioner > BG_PRECOND_LEARNED ||
                    (o.apply_precision != BG_PREC_FP64 && o.apply_precision != BG_PREC_FP32);
   if (bad) return fail(op->ctx, BG_EINVAL, "reference Davidson dimensions/threshold/start (capacity must also fit the operator)");
+  if (o.preconditioner == BG_PRECOND_LEARNED && !op->ctx->learned)
+    return fail(op->ctx, BG_EINVAL, "learned preconditioner requested but no network was set (bg_learned_set)");
   const size_t per = op->gamma ? 1 : 2;
   for (size_t i = 0; i < (size_t)dim * n * per; ++i)
     if (!std::isfinite(start[i])) return fail(op->ctx, BG_ENONFINITE, "reference Davidson start not finite");

@@ -14,6 +14,10 @@ struct bg_ctx {
   int device = 0;
   std::string error;
   std::mutex mu;
+  void* learned = nullptr;  // BF16 parameters of the learned preconditioner (device), or null
+  ~bg_ctx() {
+    if (learned) cudaFree(learned);
+  }
 };
 
 struct DevBuf {

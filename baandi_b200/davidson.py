@@ -25,7 +25,7 @@ class Options:
     first_step: bool = False
     capacity: int = 0
     max_iterations: int = 20
-    preconditioner: str = "smooth"   # "smooth" (reference Davidson), "tpa", "ritz_shift"
+    preconditioner: str = "smooth"   # "smooth" (reference Davidson), "tpa", "ritz_shift", "learned"
     apply_precision: str = "fp64"    # "fp64", or "fp32" (the local part of every H apply in FP32)
 
     def band_threshold(self, band: int) -> float:
@@ -46,6 +46,7 @@ class Solution:
     repairs: int
     contractions: int
     dropped: int
+    fallbacks: int = 0   # 1: the learned preconditioner gave way to TPA
 
 
 def preconditioner_denominator(hamiltonian_diagonal_ha, eigenvalue_ha):
@@ -56,7 +57,8 @@ def preconditioner_denominator(hamiltonian_diagonal_ha, eigenvalue_ha):
     return 0.25 * (np.where(x >= 1.0, 2.0 * x, 2.0) + 1.0 / (np.hypot(z, 1.0) + z))
 
 
-PRECONDITIONERS = {"smooth": L.BG_PRECOND_SMOOTH, "tpa": L.BG_PRECOND_TPA, "ritz_shift": L.BG_PRECOND_RITZ_SHIFT}
+PRECONDITIONERS = {"smooth": L.BG_PRECOND_SMOOTH, "tpa": L.BG_PRECOND_TPA, "ritz_shift": L.BG_PRECOND_RITZ_SHIFT,
+                   "learned": L.BG_PRECOND_LEARNED}
 
 
 def _options(options: Options, flags: int = 0):
@@ -92,7 +94,7 @@ def solve(operator: _Operator, start: np.ndarray, hamiltonian_diagonal: np.ndarr
                                ctypes.byref(st))
     operator._check(rc)
     return Solution(vals, vecs, conv.astype(bool), st.iterations, st.reduced_solves, st.h_calls, st.h_columns,
-                    st.repairs, st.contractions, st.dropped)
+                    st.repairs, st.contractions, st.dropped, st.fallbacks)
 
 
 def solve_kset(kset, starts, diagonals, options: Options, graph: bool = True):

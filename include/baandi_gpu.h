@@ -298,10 +298,18 @@ typedef struct {
  *                          denominator (ref_davidson.rs:418-422); diagonal = H diagonal
  *   BG_PRECOND_TPA         -r tpa(t_g, s_j) with s_j = max(0.1, sum |X_gj|^2 t_g /
  *                          sum |X_gj|^2) (lib.rs:176-206); diagonal = kinetic t_g
- *   BG_PRECOND_RITZ_SHIFT  -r / max(h_g - lambda_j, 0.1); diagonal = H diagonal */
+ *   BG_PRECOND_RITZ_SHIFT  -r / max(h_g - lambda_j, 0.1); diagonal = H diagonal
+ *   BG_PRECOND_LEARNED     -r tpa(t_g, s_j) exp(clamp(m(f_gj), -3, 3)), m the context's
+ *                          per-G network (bg_learned_set) on f = (log max(t_g/s_j, 1e-4),
+ *                          log(t_g + 0.05), log s_j, lambda_j, log(|r_g| / rms_j r));
+ *                          diagonal = kinetic t_g.  bg_davidson_solve only.  The solve
+ *                          falls back to TPA (stats.fallbacks = 1) once the largest Ritz
+ *                          change has not fallen below its best for 5 iterations or half
+ *                          of max_iterations is spent. */
 #define BG_PRECOND_SMOOTH 0
 #define BG_PRECOND_TPA 1
 #define BG_PRECOND_RITZ_SHIFT 2
+#define BG_PRECOND_LEARNED 3
 
 typedef struct {
   int32_t iterations;
@@ -312,6 +320,8 @@ typedef struct {
   int32_t contractions;
   int32_t dropped;         /* corrections dropped as dependent or of vanishing norm     */
   int32_t converged_count;
+  int32_t fallbacks;       /* 1: the learned preconditioner gave way to TPA in this solve */
+  int32_t reserved;
 } bg_davidson_stats;
 
 /* Reference block Davidson (crates/dft-solvers/src/ref_davidson.rs:117-366 for the
@@ -349,6 +359,54 @@ int bg_kset_davidson_solve(bg_kset* set, const double* const* start, const doubl
  * is_complex), for fixtures and small exact tests of the solver. */
 int bg_op_create_dense(bg_ctx* ctx, int64_t rows, const double* h, int32_t is_complex, int64_t capacity,
                        bg_op** out);
+
+/* ------------------------------------------------------------ learned preconditioner */
+/* No counterpart in the reference (its Preconditioner seam, crates/dft-solvers/src/
+ * lib.rs:83-102, takes any correction; TPA is :176-207).  A per-G-vector network
+ * 5 -> 64 -> 64 -> 1 (GELU) with BF16 parameters and FP32 accumulation; its output m is
+ * a log-multiplier on the TPA factor (BG_PRECOND_LEARNED).  Parameter layout, one array of
+ * BG_LEARNED_PARAMS: W1 [64][5], b1 [64], W2 [64][64] (row = output), b2 [64], w3 [64],
+ * b3.  A network with w3 = 0 and b3 = 0 is exactly TPA. */
+#define BG_LEARNED_PARAMS 4609
+
+/* The context's network for BG_PRECOND_LEARNED: host FP32 parameters, rounded to BF16
+ * (nearest even) and copied to the device; non-finite parameters are rejected. */
+int bg_learned_set(bg_ctx* ctx, const float* params);
+int bg_learned_clear(bg_ctx* ctx);
+
+/* Training samples (device arrays of n entries; one sample per (row g, band j)):
+ * feats n x 5 inputs, base the TPA factor -tpa(t_g, s_j), a = |r_g|^2, z = conj(r_g) e_g
+ * (n interleaved complex floats), col the band's column; ecol[ncols] = |e_j|^2. */
+typedef struct {
+  int64_t n;
+  int32_t ncols;
+  float* feats;
+  float* base;
+  float* a;
+  float* z;
+  int32_t* col;
+  double* ecol;
+} bg_learned_samples;
+
+/* Samples of `cols` bands of one Davidson state into entries at .. at + cols*rows - 1 and
+ * columns col0 .. col0 + cols - 1: x the Ritz vectors, hx = H x, target e the ideal
+ * corrections, kinetic t_g, lambda the Ritz values; all device pointers, rows x cols
+ * column-major (interleaved complex when is_complex), on `stream` (cudaStream_t). */
+int bg_learned_samples_build(bg_ctx* ctx, int64_t rows, int32_t cols, int32_t is_complex, const double* x,
+                             const double* hx, const double* target, const double* kinetic,
+                             const double* lambda, int32_t col0, int64_t at, const bg_learned_samples* out,
+                             void* stream);
+/* loss = (1/ncols) sum_j (1 - |sum_g p_g z_g|^2 / (sum_g p_g^2 a_g |e_j|^2)) with
+ * p = base exp(clamp(m(feats), -3, 3)) under the BF16 parameters `net` (device), and its
+ * gradient with respect to them into grad (device, BG_LEARNED_PARAMS floats).  work:
+ * device, at least 6 ncols + 1 + (n + 1) / 2 doubles.  loss (host) may be NULL; when
+ * given, the call waits for the stream. */
+int bg_learned_loss_grad(bg_ctx* ctx, const bg_learned_samples* samples, const uint16_t* net, float* grad,
+                         double* work, double* loss, void* stream);
+/* One Adam step (beta 0.9 / 0.999, eps 1e-8, bias-corrected at `step` >= 1) on the FP32
+ * master parameters, with their BF16 rounding written to net (all device). */
+int bg_learned_adam(bg_ctx* ctx, float* master, float* m1, float* m2, const float* grad, uint16_t* net,
+                    int32_t step, float lr, void* stream);
 
 /* ------------------------------------------------------------ no-allocation apply */
 /* No counterpart in the reference.  The local and kinetic part of H x for one k point,
