@@ -136,3 +136,51 @@ def test_learned_argument_checks(ctx, problems):
     p[7] = np.nan
     with pytest.raises(SolverError):
         LP.install(ctx, p)
+
+
+def test_complex_samples_and_gradient_match_oracle(ctx):
+    """Complex rows (a Si8 k point): samples, loss and gradient against the oracle, with a
+    seeded target in place of the exact correction (parity does not need the spectrum)."""
+    from baandi_b200.hamiltonian import ComplexHamiltonian
+    w = W.si8_k444()
+    pw = w.plane_waves(w.kpoints[3][0])
+    op = ComplexHamiltonian.new_owned(pw, w.dims(), w.nonlocal_table(pw), 8, ctx)
+    op.set_owned_potential(w.ionic_potential(), 1)
+    x = w.random_block(pw.npw, 6, seed_offset=21)
+    hx = op.apply_block(x)
+    lam = np.real(np.sum(np.conj(x) * hx, axis=0))
+    e = 1e-3 * w.random_block(pw.npw, 6, seed_offset=22)
+    kin = op.kinetic_diagonal()
+    s = LP.Samples(x.size, 6)
+    s.add_state(ctx, x, hx, e, kin, lam)
+    ref = R.samples(x, hx, e, kin, lam)
+    feats, base, a, z, col, ecol = _host(s)
+    assert np.max(np.abs(feats - ref[0])) < 1e-6
+    assert np.max(np.abs(base - ref[1])) < 1e-7
+    assert np.max(np.abs(z - ref[3])) <= 1e-6 * np.max(np.abs(ref[3]))
+    assert np.max(np.abs(ecol - ref[5]) / ref[5]) < 1e-12
+    rng = np.random.default_rng(8)
+    p = LP.init_params(5)
+    p[LP.OW3:LP.OB3] = rng.normal(0, 0.3, LP.N_HID).astype(np.float32)
+    t = LP.Trainer(ctx, p)
+    loss = t.loss_grad(s)
+    rl, rg = R.loss_grad(LP.from_bf16_bits(LP.to_bf16_bits(p)).astype(np.float64), feats, base, a, z, col, ecol)
+    assert abs(loss - rl) <= 1e-6 * abs(rl)
+    assert np.linalg.norm(t.grad.cpu().numpy() - rg) <= 1e-5 * np.linalg.norm(rg)
+
+
+def test_start_network_is_tpa_on_a_complex_operator(ctx):
+    from baandi_b200.hamiltonian import ComplexHamiltonian
+    w = W.si8_k444()
+    pw = w.plane_waves(w.kpoints[5][0])
+    op = ComplexHamiltonian.new_owned(pw, w.dims(), w.nonlocal_table(pw), 48, ctx)
+    op.set_owned_potential(w.ionic_potential(), 1)
+    start = w.random_block(pw.npw, 24, seed_offset=3)
+    kin = op.kinetic_diagonal()
+    o = DV.Options(24, 1e-6, 16, max_iterations=8, preconditioner="tpa")
+    a = DV.solve(op, start, kin, o)
+    LP.install(ctx, LP.init_params(0))
+    o.preconditioner = "learned"
+    b = DV.solve(op, start, kin, o)
+    assert np.array_equal(a.eigenvalues, b.eigenvalues)
+    assert (a.iterations, a.h_columns) == (b.iterations, b.h_columns)
