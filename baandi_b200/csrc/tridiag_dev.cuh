@@ -5,9 +5,9 @@
 // pivmin safeguard, Gershgorin brackets, shifted LU with partial pivoting, the cluster
 // tolerance 1e-3 |T|_1 and the 10 eps |T|_1 separation of shifts inside a cluster), laid
 // out for a GPU block: every eigenvalue is bracketed by a group of lanes that each count
-// four shifts per round; every eigenvector is one thread's inverse iteration, and the
+// two shifts per round; every eigenvector is one thread's inverse iteration, and the
 // vectors of a cluster are then orthonormalised in order (Gram-Schmidt twice) by one
-// thread.  Shifts inside a run of eigenvalues closer than 10 eps |T|_1 are spread by that
+// warp, its lanes over the rows.  Shifts inside a run of eigenvalues closer than 10 eps |T|_1 are spread by that
 // amount and the start vectors differ, so the iterates of a near-degenerate cluster span
 // its invariant subspace; components outside it shrink by (shift error / gap)^2 over the
 // two solves.
@@ -148,8 +148,11 @@ __device__ void eig(int m, const double* __restrict__ d, const double* __restric
   const double pivmin = kSafeMin * e2max;
 
   // 2. eigenvalues: G lanes per eigenvalue, each counting kShifts shifts per round;
-  //    located to 2 eps max(|lo|, |hi|) + eps |T_b|_1
-  constexpr int kShifts = 4;
+  //    located to 2 eps max(|lo|, |hi|) + eps |T_b|_1.  A lane's Sturm step issues about
+  //    7 instructions per shift and the warps of one group are issue-bound, so the time of
+  //    a bracket goes as kShifts / log(G kShifts + 1): two shifts per lane beat four and
+  //    eight (35, 50 and 78 us per 34 x 34 solve on one B200)
+  constexpr int kShifts = 2;
   int G = 1;
   while (G < 32 && 2 * G * m <= NT) G *= 2;
   const int NG = NT / G, gid = threadIdx.x / G, lig = threadIdx.x % G;
@@ -325,52 +328,56 @@ __device__ void eig(int m, const double* __restrict__ d, const double* __restric
   __syncthreads();
 
   // 5. each cluster's vectors orthonormalised in order (Gram-Schmidt, twice), then the
-  //    sign: the largest entry of every vector positive
-  for (int cidx = threadIdx.x; cidx < nc; cidx += NT) {
-    const int ja = clusters[cidx], jb = clusters[cidx + 1];
-    const int b = block_of(starts, nb, ja);
-    const int s = starts[b], n = starts[b + 1] - s;
-    for (int j = ja; j < jb; ++j) {
-      double* zc = Z + (size_t)s * ldz + j;
-      auto z = [&](int r) -> double& { return zc[(size_t)r * ldz]; };
-      for (int pass = 0; pass < 2 && j > ja; ++pass) {
-        // against the earlier vectors in chunks of 8: the 8 dot products of a chunk are
-        // independent chains (classical Gram-Schmidt inside a chunk, chunks in order)
-        for (int j0 = ja; j0 < j; j0 += 8) {
-          const int cnt = min(8, j - j0);
-          const double* y = Z + (size_t)s * ldz + j0;
-          double dots[8];
-#pragma unroll
-          for (int q = 0; q < 8; ++q) dots[q] = 0.0;
-          for (int r = 0; r < n; ++r) {
-            const double zr = z(r);
-#pragma unroll
-            for (int q = 0; q < 8; ++q)
-              if (q < cnt) dots[q] = fma(zr, y[(size_t)r * ldz + q], dots[q]);
+  //    sign: the largest entry of every vector positive.  One warp per cluster, the lanes
+  //    over the rows; dot products and norms are warp sums.
+  {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int cidx = warp; cidx < nc; cidx += NT / 32) {
+      const int ja = clusters[cidx], jb = clusters[cidx + 1];
+      const int b = block_of(starts, nb, ja);
+      const int s = starts[b], n = starts[b + 1] - s;
+      const double* zb = Z + (size_t)s * ldz;
+      for (int j = ja; j < jb; ++j) {
+        double* zc = Z + (size_t)s * ldz + j;
+        for (int pass = 0; pass < 2 && j > ja; ++pass) {
+          for (int q = ja; q < j; ++q) {
+            double dot = 0.0;
+            for (int r = lane; r < n; r += 32) dot = fma(zc[(size_t)r * ldz], zb[(size_t)r * ldz + q], dot);
+            for (int o = 16; o > 0; o >>= 1) dot += __shfl_xor_sync(0xffffffffu, dot, o);
+            for (int r = lane; r < n; r += 32) zc[(size_t)r * ldz] = fma(-dot, zb[(size_t)r * ldz + q], zc[(size_t)r * ldz]);
+            __syncwarp();
           }
-          for (int r = 0; r < n; ++r) {
-            double v = z(r);
-#pragma unroll
-            for (int q = 0; q < 8; ++q)
-              if (q < cnt) v = fma(-dots[q], y[(size_t)r * ldz + q], v);
-            z(r) = v;
+          double nn = 0.0;
+          for (int r = lane; r < n; r += 32) nn = fma(zc[(size_t)r * ldz], zc[(size_t)r * ldz], nn);
+          for (int o = 16; o > 0; o >>= 1) nn += __shfl_xor_sync(0xffffffffu, nn, o);
+          const double inv = 1.0 / sqrt(nn);
+          for (int r = lane; r < n; r += 32) zc[(size_t)r * ldz] *= inv;
+          __syncwarp();
+        }
+        // sign: the first entry of largest magnitude positive
+        double big = -1.0;
+        int at = n;
+        for (int r = lane; r < n; r += 32) {
+          const double v = fabs(zc[(size_t)r * ldz]);
+          if (v > big) {
+            big = v;
+            at = r;
           }
         }
-        double nn = 0.0;
-        for (int r = 0; r < n; ++r) nn += z(r) * z(r);
-        const double inv = 1.0 / sqrt(nn);
-        for (int r = 0; r < n; ++r) z(r) *= inv;
-      }
-      double big = 0.0, sgn = 1.0;
-      for (int r = 0; r < n; ++r) {
-        const double v = z(r);
-        if (fabs(v) > big) {
-          big = fabs(v);
-          sgn = v < 0.0 ? -1.0 : 1.0;
+        for (int o = 16; o > 0; o >>= 1) {
+          const double ob = __shfl_xor_sync(0xffffffffu, big, o);
+          const int oa = __shfl_xor_sync(0xffffffffu, at, o);
+          if (ob > big || (ob == big && oa < at)) {
+            big = ob;
+            at = oa;
+          }
         }
+        const bool neg = zc[(size_t)at * ldz] < 0.0;
+        __syncwarp();
+        if (neg)
+          for (int r = lane; r < n; r += 32) zc[(size_t)r * ldz] = -zc[(size_t)r * ldz];
+        __syncwarp();
       }
-      if (sgn < 0.0)
-        for (int r = 0; r < n; ++r) z(r) = -z(r);
     }
   }
   __syncthreads();
