@@ -382,50 +382,64 @@ __device__ bool heev(D* A, int lda, int m, double* w, D* V, int ldv, const Bufs<
   __syncthreads();
   D* v = b.hv;
   D* p = b.hp;
-  D* q = b.hq;
   // Q is stored transposed (Q[c + r ldq] holds row r, column c), so that the reflector
   // update of each row reads contiguous entries.
   const int hg = threadIdx.x % kHouseLanes, hper = blockDim.x / kHouseLanes;
+  // Two block reductions per step and no other barrier: p = beta B v reads v straight from
+  // the column (v_0 = x_0 - alpha) and sums Re(v^H p) on the way (the K reduction's barrier
+  // also publishes p and v); the rank-2 update forms q = p - K v on the fly and sums the
+  // next column's squared norm, whose reduction closes the step.  red and red + 32 take
+  // the two reductions in turn, so a slot is never rewritten while it is still read.
+  double xn2 = 0.0;
+  if (m > 2) {
+    double part = 0.0;
+    for (int i = threadIdx.x; i < m - 1; i += blockDim.x) part += X::abs2(A[1 + i]);
+    xn2 = block_sum1(part, red + 32);
+  }
   for (int k = 0; k + 2 < m; ++k) {
     const int L = m - k - 1;
     D* x = A + (k + 1) + (size_t)k * lda;
-    double part = 0.0;
-    for (int i = threadIdx.x; i < L; i += blockDim.x) part += X::abs2(x[i]);
-    const double xn = sqrt(block_sum1(part, red));
+    const double xn = sqrt(xn2);
     if (xn == 0.0) {
       if (threadIdx.x == 0) b.off[k] = X::zero();
-      __syncthreads();
+      double part = 0.0;
+      for (int i = threadIdx.x; i + 1 < L; i += blockDim.x) part += X::abs2(A[(k + 2 + i) + (size_t)(k + 1) * lda]);
+      __syncthreads();  // the previous reduction in red + 32 has been read by every thread
+      xn2 = block_sum1(part, red + 32);
       continue;
     }
     const D x0 = x[0];
     const double ax0 = X::abs(x0);
     const D phase = ax0 > 0.0 ? X::div(x0, ax0) : X::one();
     const D alpha = X::scale(-xn, phase);
-    for (int i = threadIdx.x; i < L; i += blockDim.x) v[i] = i == 0 ? X::sub(x0, alpha) : x[i];
+    const D v0 = X::sub(x0, alpha);
+    for (int i = threadIdx.x; i < L; i += blockDim.x) v[i] = i == 0 ? v0 : x[i];
     // |v|^2 = |x|^2 - |x0|^2 + (|x0| + |x|)^2
     const double beta = 1.0 / (xn * (xn + ax0));
-    __syncthreads();
     // p = beta B v, entry i from column i of the Hermitian B (contiguous)
+    double part = 0.0;
     for (int i0 = 0; i0 < L; i0 += hper) {
       const int i = i0 + threadIdx.x / kHouseLanes;
       D acc = X::zero();
       if (i < L) {
         const D* col = A + (k + 1) + (size_t)(k + 1 + i) * lda;
-        for (int j = hg; j < L; j += kHouseLanes) acc = X::add(acc, X::mul(X::conj(col[j]), v[j]));
+        for (int j = hg; j < L; j += kHouseLanes) acc = X::add(acc, X::mul(X::conj(col[j]), j == 0 ? v0 : x[j]));
       }
       acc = group_sum<D, kHouseLanes>(acc);
-      if (i < L && hg == 0) p[i] = X::scale(beta, acc);
+      if (i < L && hg == 0) {
+        const D pi = X::scale(beta, acc);
+        p[i] = pi;
+        part += X::dot_re(i == 0 ? v0 : x[i], pi);
+      }
     }
-    __syncthreads();
-    part = 0.0;
-    for (int i = threadIdx.x; i < L; i += blockDim.x) part += X::dot_re(v[i], p[i]);
-    const double K = 0.5 * beta * block_sum1(part, red + 32);
-    for (int i = threadIdx.x; i < L; i += blockDim.x) q[i] = X::sub(p[i], X::scale(K, v[i]));
-    __syncthreads();
+    const double K = 0.5 * beta * block_sum1(part, red);
+    double nxt = 0.0;
     for (int t = threadIdx.x; t < L * L; t += blockDim.x) {
       const int i = t % L, j = t / L;
+      const D qi = X::sub(p[i], X::scale(K, v[i])), qj = X::sub(p[j], X::scale(K, v[j]));
       D& a = A[(k + 1 + i) + (size_t)(k + 1 + j) * lda];
-      a = X::sub(a, X::add(X::mul(v[i], X::conj(q[j])), X::mul(q[i], X::conj(v[j]))));
+      a = X::sub(a, X::add(X::mul(v[i], X::conj(qj)), X::mul(qi, X::conj(v[j]))));
+      if (j == 0 && i >= 1) nxt += X::abs2(a);
     }
     if (threadIdx.x == 0) b.off[k] = alpha;
     for (int i = threadIdx.x; i < L; i += blockDim.x) {
@@ -443,7 +457,7 @@ __device__ bool heev(D* A, int lda, int m, double* w, D* V, int ldv, const Bufs<
       if (r < m)
         for (int j = hg; j < L; j += kHouseLanes) row[j] = X::sub(row[j], X::mul(acc, X::conj(v[j])));
     }
-    __syncthreads();
+    xn2 = block_sum1(nxt, red + 32);  // the next column's |x|^2; its barrier closes the step
   }
   double* d = b.td;
   double* e = b.te;
