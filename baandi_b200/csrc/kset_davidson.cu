@@ -578,7 +578,10 @@ __global__ void k_dv_tn_sum(const Bufs<D>* __restrict__ bufs, const TN<D>* __res
   }
 }
 
-// dst[:, c] = src[:, c], or scale[c] src[:, map[c]] for a pick; blockIdx.y = column.
+// dst[:, c] = src[:, c], or scale[c] src[:, map[c]] for a pick; blockIdx.y = column.  A
+// thread moves kCopyUnroll rows per pass with its loads issued together, so a block's
+// descriptor reads are paid for once per kCopyUnroll x 256 rows.
+constexpr int kCopyUnroll = 4;
 template <class D>
 __global__ void k_dv_copy(const Bufs<D>* __restrict__ bufs, const CP<D>* __restrict__ desc, int nk) {
   const int z = blockIdx.z, k = z % nk;
@@ -590,8 +593,20 @@ __global__ void k_dv_copy(const Bufs<D>* __restrict__ bufs, const CP<D>* __restr
   const D* src = d.src + (int64_t)(d.pick ? b.map[c] : c) * rows;
   D* dst = d.dst + (int64_t)c * rows;
   const double sc = d.pick ? b.scale[c] : 1.0;
-  for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < rows; r += (int64_t)gridDim.x * blockDim.x)
-    dst[r] = d.pick ? Arith<D>::scale(sc, src[r]) : src[r];
+  const int64_t span = (int64_t)blockDim.x * kCopyUnroll;
+  for (int64_t r0 = blockIdx.x * span + threadIdx.x; r0 < rows; r0 += (int64_t)gridDim.x * span) {
+    D v[kCopyUnroll];
+#pragma unroll
+    for (int u = 0; u < kCopyUnroll; ++u) {
+      const int64_t r = r0 + (int64_t)u * blockDim.x;
+      if (r < rows) v[u] = src[r];
+    }
+#pragma unroll
+    for (int u = 0; u < kCopyUnroll; ++u) {
+      const int64_t r = r0 + (int64_t)u * blockDim.x;
+      if (r < rows) dst[r] = d.pick ? Arith<D>::scale(sc, v[u]) : v[u];
+    }
+  }
 }
 
 // Dense test operators: y[:, 0:cols] = H x for every k point, cols read from dyn.
@@ -1169,7 +1184,9 @@ class KsetSolver {
     return 2;
   }
   int64_t cp(int slot0, int nslots) {
-    const dim3 grid((unsigned)std::min((max_rows_ + 255) / 256, 64), (unsigned)o_.cap, (unsigned)(nslots * nk_));
+    const int64_t span = 256 * kCopyUnroll;
+    const dim3 grid((unsigned)std::min<int64_t>((max_rows_ + span - 1) / span, 64), (unsigned)o_.cap,
+                    (unsigned)(nslots * nk_));
     k_dv_copy<D><<<grid, 256, 0, s_>>>(d_bufs_, d_cp_ + (size_t)slot0 * nk_, nk_);
     return 1;
   }
