@@ -315,6 +315,7 @@ extern "C" int bg_learned_samples_build(bg_ctx* ctx, int64_t rows, int32_t cols,
     return lfail(ctx, BG_EINVAL, "learned samples: arguments");
   if (col0 + (int64_t)cols > out->ncols || at + (int64_t)cols * rows > out->n)
     return lfail(ctx, BG_EINVAL, "learned samples: output too small");
+  cudaSetDevice(ctx->device);
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   float* feats = out->feats + at * kIn;
   float2* z = reinterpret_cast<float2*>(out->z) + at;
@@ -340,11 +341,11 @@ extern "C" int bg_learned_loss_grad(bg_ctx* ctx, const bg_learned_samples* smp, 
   double* dloss = work + 6 * (size_t)nc;
   float* p = reinterpret_cast<float*>(work + 6 * (size_t)nc + 1);
   const auto* bnet = reinterpret_cast<const __nv_bfloat16*>(net);
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k_learned_backward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBwdSmem);
-    attr = true;
-  }
+  cudaSetDevice(ctx->device);
+  // per device and cheap: set on every call
+  if (cudaFuncSetAttribute(k_learned_backward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBwdSmem) !=
+      cudaSuccess)
+    return lcheck(ctx, "learned backward shared memory");
   cudaMemsetAsync(colsum, 0, sizeof(double) * 3 * (size_t)nc, s);
   cudaMemsetAsync(grad, 0, sizeof(float) * kParams, s);
   const int64_t fb = std::min<int64_t>((smp->n + 127) / 128, 148 * 8);
@@ -368,6 +369,7 @@ extern "C" int bg_learned_adam(bg_ctx* ctx, float* master, float* m1, float* m2,
                                int32_t step, float lr, void* stream) {
   if (!ctx || !master || !m1 || !m2 || !grad || !net || step < 1 || !(lr > 0.0f))
     return lfail(ctx, BG_EINVAL, "learned adam: arguments");
+  cudaSetDevice(ctx->device);
   k_learned_adam<<<(kParams + 255) / 256, 256, 0, static_cast<cudaStream_t>(stream)>>>(
       master, m1, m2, grad, reinterpret_cast<__nv_bfloat16*>(net), step, lr);
   return lcheck(ctx, "learned adam");
