@@ -527,7 +527,10 @@ extern "C" int bg_davidson_solve(bg_op* op, const double* start, const double* d
   for (int64_t i = 0; i < dim; ++i)
     if (!std::isfinite(diagonal[i])) return fail(op->ctx, BG_ENONFINITE, "reference Davidson diagonal not finite");
   if (!op->has_epoch) return fail(op->ctx, BG_EEPOCH, "potential was never set");
-  cudaSetDevice(op->ctx->device);
+  {
+    const cudaError_t de = cudaSetDevice(op->ctx->device);
+    if (de != cudaSuccess) return cuda_fail(op->ctx, de, "cudaSetDevice");
+  }
   int rc;
   std::string err;
   if (per == 1) {

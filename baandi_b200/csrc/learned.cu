@@ -290,7 +290,10 @@ extern "C" int bg_learned_set(bg_ctx* ctx, const float* params) {
     if (!std::isfinite(params[i])) return lfail(ctx, BG_ENONFINITE, "learned preconditioner parameters not finite");
     h[i] = to_bf16(params[i]);
   }
-  cudaSetDevice(ctx->device);
+  {
+    const cudaError_t de = cudaSetDevice(ctx->device);
+    if (de != cudaSuccess) return lfail(ctx, BG_EDEVICE, cudaGetErrorString(de));
+  }
   if (!ctx->learned && cudaMalloc(&ctx->learned, sizeof(uint16_t) * kParams) != cudaSuccess) {
     ctx->learned = nullptr;
     return lfail(ctx, BG_ENOMEM, "learned preconditioner parameters");
@@ -315,7 +318,10 @@ extern "C" int bg_learned_samples_build(bg_ctx* ctx, int64_t rows, int32_t cols,
     return lfail(ctx, BG_EINVAL, "learned samples: arguments");
   if (col0 + (int64_t)cols > out->ncols || at + (int64_t)cols * rows > out->n)
     return lfail(ctx, BG_EINVAL, "learned samples: output too small");
-  cudaSetDevice(ctx->device);
+  {
+    const cudaError_t de = cudaSetDevice(ctx->device);
+    if (de != cudaSuccess) return lfail(ctx, BG_EDEVICE, cudaGetErrorString(de));
+  }
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   float* feats = out->feats + at * kIn;
   float2* z = reinterpret_cast<float2*>(out->z) + at;
@@ -341,7 +347,10 @@ extern "C" int bg_learned_loss_grad(bg_ctx* ctx, const bg_learned_samples* smp, 
   double* dloss = work + 6 * (size_t)nc;
   float* p = reinterpret_cast<float*>(work + 6 * (size_t)nc + 1);
   const auto* bnet = reinterpret_cast<const __nv_bfloat16*>(net);
-  cudaSetDevice(ctx->device);
+  {
+    const cudaError_t de = cudaSetDevice(ctx->device);
+    if (de != cudaSuccess) return lfail(ctx, BG_EDEVICE, cudaGetErrorString(de));
+  }
   // per device and cheap: set on every call
   if (cudaFuncSetAttribute(k_learned_backward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBwdSmem) !=
       cudaSuccess)
@@ -369,7 +378,10 @@ extern "C" int bg_learned_adam(bg_ctx* ctx, float* master, float* m1, float* m2,
                                int32_t step, float lr, void* stream) {
   if (!ctx || !master || !m1 || !m2 || !grad || !net || step < 1 || !(lr > 0.0f))
     return lfail(ctx, BG_EINVAL, "learned adam: arguments");
-  cudaSetDevice(ctx->device);
+  {
+    const cudaError_t de = cudaSetDevice(ctx->device);
+    if (de != cudaSuccess) return lfail(ctx, BG_EDEVICE, cudaGetErrorString(de));
+  }
   k_learned_adam<<<(kParams + 255) / 256, 256, 0, static_cast<cudaStream_t>(stream)>>>(
       master, m1, m2, grad, reinterpret_cast<__nv_bfloat16*>(net), step, lr);
   return lcheck(ctx, "learned adam");

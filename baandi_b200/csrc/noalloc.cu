@@ -1,6 +1,7 @@
 // bg_local_apply_noalloc: the local and kinetic part of H x for one k point, with every
-// intermediate in a fixed scratch array that the library holds in device memory from
-// load time, so the call itself allocates nothing.
+// intermediate in a fixed scratch array that the library holds in device memory once its
+// module is loaded on a device (with CUDA's default lazy module loading that happens at
+// the first call on that device), so the call itself allocates nothing.
 //
 // Who needs it: callers whose device memory belongs to another runtime's pool (a
 // framework caching allocator, an inference server's arena) or that run after an
@@ -72,7 +73,14 @@ bool plan_for(int n, FftPlan* p) {
   return true;
 }
 
+// Error bits of the last call, cleared by k_na_zero and read back by the host after the
+// stream has finished: an fft_index entry outside [0, n0 n1 n2) (the access is skipped),
+// a non-finite input coefficient.
+constexpr int kErrIndex = 1, kErrNonfinite = 2;
+static __device__ int g_noalloc_err;
+
 __global__ void k_na_zero(double2* box, size_t n) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) g_noalloc_err = 0;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
     box[i] = make_double2(0.0, 0.0);
 }
@@ -80,10 +88,19 @@ __global__ void k_na_zero(double2* box, size_t n) {
 __global__ void k_na_scatter(double2* box, size_t nbox, const int32_t* __restrict__ idx, int64_t npw,
                              const double2* __restrict__ x, int64_t cols) {
   const size_t total = (size_t)npw * cols;
+  int err = 0;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
     const size_t c = i / npw, g = i - c * npw;
-    box[c * nbox + idx[g]] = x[i];
+    const int32_t f = idx[g];
+    const double2 v = x[i];
+    if (!isfinite(v.x) || !isfinite(v.y)) err |= kErrNonfinite;
+    if (f < 0 || (size_t)f >= nbox) {
+      err |= kErrIndex;
+      continue;
+    }
+    box[c * nbox + f] = v;
   }
+  if (err) atomicOr(&g_noalloc_err, err);
 }
 
 __global__ void k_na_multiply(double2* box, size_t nbox, const double* __restrict__ v, int64_t cols) {
@@ -101,7 +118,9 @@ __global__ void k_na_gather(const double2* box, size_t nbox, const int32_t* __re
   const size_t total = (size_t)npw * cols;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
     const size_t c = i / npw, g = i - c * npw;
-    const double2 h = box[c * nbox + idx[g]];
+    const int32_t f = idx[g];
+    // a row whose index is out of range has no grid value (flagged by the scatter pass)
+    const double2 h = (f >= 0 && (size_t)f < nbox) ? box[c * nbox + f] : make_double2(0.0, 0.0);
     const double2 xv = x[i];
     y[i] = make_double2(h.x * inv_n + kin[g] * xv.x, h.y * inv_n + kin[g] * xv.y);
   }
@@ -207,7 +226,7 @@ extern "C" int bg_local_apply_noalloc(const int32_t dims[3], int64_t npw, const 
     set_global_error("row or column count out of range");
     return BG_ESHAPE;
   }
-  if ((size_t)cols * nbox > kNoAllocBoxElems) {
+  if (cols > (int64_t)(kNoAllocBoxElems / nbox)) {
     set_global_error("cols * n0 * n1 * n2 exceeds the 32 MiB scratch of bg_local_apply_noalloc (2097152 complex values)");
     return BG_ESHAPE;
   }
@@ -229,6 +248,22 @@ extern "C" int bg_local_apply_noalloc(const int32_t dims[3], int64_t npw, const 
   if (e != cudaSuccess) {
     set_global_error(std::string("kernel launch: ") + cudaGetErrorString(e));
     return BG_EDEVICE;
+  }
+  // The error word is read once the stream's work is done (a pageable copy: no allocation).
+  int err = 0;
+  e = cudaMemcpyFromSymbolAsync(&err, g_noalloc_err, sizeof(int), 0, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) {
+    set_global_error(std::string("bg_local_apply_noalloc: ") + cudaGetErrorString(e));
+    return BG_EDEVICE;
+  }
+  if (err & kErrIndex) {
+    set_global_error("fft_index holds an entry outside [0, n0*n1*n2); those rows were skipped");
+    return BG_ESHAPE;
+  }
+  if (err & kErrNonfinite) {
+    set_global_error("nonfinite input block");
+    return BG_ENONFINITE;
   }
   return BG_OK;
 }

@@ -419,11 +419,14 @@ int bg_learned_adam(bg_ctx* ctx, float* master, float* m1, float* m2, const floa
  * (npw x cols complex, interleaved, column-major).  Intermediates live in one 32 MiB
  * scratch array that the library keeps on every device it is loaded on until the
  * process exits; cols*n0*n1*n2 must not exceed 2,097,152 (BG_ESHAPE otherwise).  The
- * first call on a device resolves the scratch array's device address (so make it
- * before any stream capture on that device).  The work is enqueued on `stream`
- * (cudaStream_t, NULL for the legacy stream).  Every call reuses the same scratch:
- * calls whose work may overlap on the GPU (other streams, other host threads) race and
- * must be serialised by the caller. */
+ * first call on a device loads the library's module there if CUDA's lazy loading has
+ * not done so yet (which reserves the 32 MiB) and resolves the scratch array's device
+ * address, so make it before any stream capture on that device.  The work runs on
+ * `stream` (cudaStream_t, NULL for the legacy stream) and the call returns once it has
+ * finished, reporting BG_ESHAPE if an fft_index entry lies outside [0, n0*n1*n2) (such
+ * rows are skipped, never accessed) and BG_ENONFINITE for a non-finite x.  Every call
+ * reuses the same scratch: calls whose work may overlap on the GPU (other streams,
+ * other host threads) race and must be serialised by the caller. */
 int bg_local_apply_noalloc(const int32_t dims[3], int64_t npw, const int32_t* fft_index,
                            const double* v_grid, const double* kinetic, const double* x, double* y,
                            int64_t cols, void* stream);

@@ -33,40 +33,48 @@ def lib():
         if not os.path.exists(_LIB):
             build()
         L = ctypes.CDLL(_LIB)
-        L.oracle_apply_complex.argtypes = [ctypes.c_int] * 3 + [ctypes.c_int64, _i64p, _f64p, _f64p, ctypes.c_int,
-                                                                _f64p, ctypes.c_int, _i32p, _f64p, _f64p, _f64p,
+        L.oracle_local_complex.argtypes = [ctypes.c_int] * 3 + [ctypes.c_int64, _i64p, _f64p, _f64p, _f64p, _f64p,
                                                                 ctypes.c_int, ctypes.c_int]
-        L.oracle_apply_gamma.argtypes = [ctypes.c_int] * 3 + [ctypes.c_int64, _i64p, ctypes.c_int64, _i64p, _i64p,
-                                                              _f64p, _f64p, ctypes.c_int, _f64p, ctypes.c_int, _i32p,
-                                                              _f64p, _f64p, _f64p, ctypes.c_int, ctypes.c_int]
+        L.oracle_local_gamma.argtypes = [ctypes.c_int] * 3 + [ctypes.c_int64, _i64p, ctypes.c_int64, _i64p, _i64p,
+                                                              _f64p, _f64p, _f64p, _f64p, ctypes.c_int, ctypes.c_int]
         L.oracle_fft3d.argtypes = [ctypes.c_int] * 3 + [_f64p, ctypes.c_int]
         _lib = L
     return _lib
 
 
-def _flat_couplings(nl):
-    ch = np.asarray(nl.channels, dtype=np.int32)
-    cp = np.concatenate([np.asarray(c, dtype=np.float64) for c in nl.couplings]) if nl.couplings else np.zeros(1)
-    return ch if len(ch) else np.zeros(1, np.int32), cp
+def _couple(nl, w):
+    """D per atom on the projections w (nproj x m): out_i = sum_j D_ij w_j within each atom's
+    channels (distributed_complex.rs:326-336; Gamma distributed_real_gamma.rs:1184-1195)."""
+    out = np.empty_like(w)
+    off, coff = 0, 0
+    flat = np.concatenate([np.asarray(c, dtype=np.float64).reshape(-1) for c in nl.couplings])
+    for cnt in nl.channels:
+        d = flat[coff:coff + cnt * cnt].reshape(cnt, cnt)
+        out[off:off + cnt] = d @ w[off:off + cnt]
+        off += cnt
+        coff += cnt * cnt
+    return out
 
 
 def apply_complex(dims, index, vgrid, kinetic, nl, x, threads=0):
-    """H x for one k point; x (npw, m) complex128. vgrid: real grid, C order."""
+    """H x for one k point; x (npw, m) complex128. vgrid: real grid, C order.  Local part and
+    kinetic in the C++ restatement; P (D (P^H x)) as dense products (numpy BLAS)."""
     x = np.asfortranarray(x, dtype=np.complex128)
     npw, m = x.shape
     xin = np.ascontiguousarray(x.T).view(np.float64).reshape(-1)
     y = np.zeros(npw * m * 2)
-    nproj = nl.table.shape[1] if nl is not None else 0
-    proj = (np.ascontiguousarray(nl.table.T).view(np.float64).reshape(-1) if nproj else np.zeros(2))
-    ch, cp = _flat_couplings(nl) if nproj else (np.zeros(1, np.int32), np.zeros(1))
-    rc = lib().oracle_apply_complex(int(dims[0]), int(dims[1]), int(dims[2]), npw,
+    rc = lib().oracle_local_complex(int(dims[0]), int(dims[1]), int(dims[2]), npw,
                                     np.ascontiguousarray(index, dtype=np.int64),
                                     np.ascontiguousarray(vgrid, dtype=np.float64).reshape(-1),
-                                    np.ascontiguousarray(kinetic, dtype=np.float64), nproj, proj,
-                                    len(nl.channels) if nproj else 0, ch, cp, xin, y, m, threads)
+                                    np.ascontiguousarray(kinetic, dtype=np.float64), xin, y, m, threads)
     if rc != 0:
-        raise ValueError("oracle_apply_complex: shape error")
-    return y.view(np.complex128).reshape(m, npw).T
+        raise ValueError("oracle_local_complex: shape error")
+    out = np.asfortranarray(y.view(np.complex128).reshape(m, npw).T)
+    if nl is not None and nl.table.shape[1]:
+        p = nl.table
+        w = (p.T @ x.conj()).conj()                 # P^H x
+        out += p @ _couple(nl, w)
+    return out
 
 
 def apply_gamma(dims, index, plus, minus, vgrid, kinetic_orc, proj_orc, nl, x, threads=0):
@@ -75,19 +83,19 @@ def apply_gamma(dims, index, plus, minus, vgrid, kinetic_orc, proj_orc, nl, x, t
     n, m = x.shape
     xin = np.ascontiguousarray(x.T).reshape(-1)
     y = np.zeros(n * m)
-    nproj = proj_orc.shape[1] if proj_orc is not None else 0
-    proj = np.ascontiguousarray(proj_orc.T).reshape(-1) if nproj else np.zeros(1)
-    ch, cp = _flat_couplings(nl) if nproj else (np.zeros(1, np.int32), np.zeros(1))
-    rc = lib().oracle_apply_gamma(int(dims[0]), int(dims[1]), int(dims[2]), n,
+    rc = lib().oracle_local_gamma(int(dims[0]), int(dims[1]), int(dims[2]), n,
                                   np.ascontiguousarray(index, dtype=np.int64), len(plus),
                                   np.ascontiguousarray(plus, dtype=np.int64),
                                   np.ascontiguousarray(minus, dtype=np.int64),
                                   np.ascontiguousarray(vgrid, dtype=np.float64).reshape(-1),
-                                  np.ascontiguousarray(kinetic_orc, dtype=np.float64), nproj, proj,
-                                  len(nl.channels) if nproj else 0, ch, cp, xin, y, m, threads)
+                                  np.ascontiguousarray(kinetic_orc, dtype=np.float64), xin, y, m, threads)
     if rc != 0:
-        raise ValueError("oracle_apply_gamma: shape error")
-    return y.reshape(m, n).T
+        raise ValueError("oracle_local_gamma: shape error")
+    out = np.asfortranarray(y.reshape(m, n).T)
+    if proj_orc is not None and proj_orc.shape[1]:
+        q = proj_orc.T @ x                          # P^T x
+        out += proj_orc @ _couple(nl, q)
+    return out
 
 
 def fft3d(grid, sign):

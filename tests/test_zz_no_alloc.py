@@ -3,11 +3,13 @@ device memory (their memory belongs to another runtime's pool, or allocation is
 forbidden after start-up because cudaMalloc/cudaFree can synchronise the device).
 
 The entry point takes only caller-owned buffers and keeps its intermediates in the
-library's fixed 32 MiB device scratch.  Its result must match the operator entry point
-(bg_op_apply_block of an operator without projectors: the same local + kinetic
-operator) within the FP64 tolerance of the parity tests, on two calls in a row (the
-scratch keeps the previous call's contents, so the second call checks that nothing
-stale leaks through).  This file is collected last on purpose."""
+library's fixed 32 MiB device scratch.  Its result must match the oracle's local +
+kinetic apply (the C++ FP64 restatement with no projectors) and the operator entry
+point (bg_op_apply_block of an operator without projectors) within the FP64 tolerance
+of the parity tests, on two calls in a row (the scratch keeps the previous call's
+contents, so the second call checks that nothing stale leaks through).  A grid index
+out of range is skipped and reported, never accessed.  This file is collected last on
+purpose."""
 import ctypes
 
 import numpy as np
@@ -17,6 +19,9 @@ from baandi_b200 import _lib
 from baandi_b200 import operands as O
 from baandi_b200 import systems as W
 from baandi_b200.hamiltonian import ComplexHamiltonian
+from oracle import oracle as OR
+from tests.helpers import oracle_inputs
+from oracle import setup_ref as S
 
 TOL = 1e-12
 
@@ -56,7 +61,50 @@ def test_noalloc_matches_operator_twice(ctx, name, kidx, cols):
         op.sync()
         a, b = y.cpu().numpy().T, ref.cpu().numpy().T
         err = float(np.max(np.linalg.norm(a - b, axis=0) / np.linalg.norm(b, axis=0)))
-        assert err <= TOL, f"call {call}: relative error {err:.3e}"
+        assert err <= TOL, f"call {call}: relative error {err:.3e} against the operator"
+        _, ob, _ = oracle_inputs(w, k)
+        oref = OR.apply_complex(dims, S.fft_flat(S.g_to_fft(ob, dims), dims), v, 0.5 * ob.kpg2, None,
+                                x.cpu().numpy().T)
+        err = float(np.max(np.linalg.norm(a - oref, axis=0) / np.linalg.norm(oref, axis=0)))
+        assert err <= TOL, f"call {call}: relative error {err:.3e} against the oracle"
+
+
+def test_noalloc_skips_and_reports_bad_index(ctx):
+    """One fft_index entry past the grid: that row is skipped (never accessed), the call
+    reports BG_ESHAPE, and every other row still equals the oracle's answer (the bad
+    row's coefficient is zero, so it contributes nothing to the others)."""
+    import torch
+    w = W.WORKLOADS["si2"]()
+    dims = w.dims()
+    pw = w.plane_waves()
+    _, ob, _ = oracle_inputs(w, (0.0, 0.0, 0.0))
+    v = w.ionic_potential()
+    dev = torch.device("cuda")
+    idx_h = O.fft_index(pw.miller, dims, pw.gamma).astype(np.int32)
+    bad = 17
+    idx_h[bad] = int(np.prod(dims)) + 5
+    x_h = w.random_block(pw.npw, 3, seed_offset=21)
+    x_h[bad, :] = 0.0
+    idx = torch.from_numpy(idx_h).to(dev)
+    vd = torch.from_numpy(np.ascontiguousarray(v).reshape(-1)).to(dev)
+    kin = torch.from_numpy(0.5 * pw.kpg2).to(dev)
+    x = torch.from_numpy(np.ascontiguousarray(x_h.T)).to(dev)
+    y = torch.zeros_like(x)
+    rc = _noalloc(dims, idx, vd, kin, x, y, torch.cuda.current_stream().cuda_stream)
+    assert rc == _lib.BG_ESHAPE
+    assert "outside" in _lib.last_error(None)
+    oref = OR.apply_complex(dims, S.fft_flat(S.g_to_fft(ob, dims), dims), v, 0.5 * ob.kpg2, None, x_h)
+    a = y.cpu().numpy().T
+    keep = np.ones(pw.npw, bool)
+    keep[bad] = False
+    err = float(np.max(np.linalg.norm(a[keep] - oref[keep], axis=0) / np.linalg.norm(oref[keep], axis=0)))
+    assert err <= TOL
+    # a non-finite coefficient is reported as well
+    x_h[3, 1] = np.nan
+    x = torch.from_numpy(np.ascontiguousarray(x_h.T)).to(dev)
+    idx_h[bad] = O.fft_index(pw.miller, dims, pw.gamma).astype(np.int32)[bad]
+    rc = _noalloc(dims, torch.from_numpy(idx_h).to(dev), vd, kin, x, y, torch.cuda.current_stream().cuda_stream)
+    assert rc == _lib.BG_ENONFINITE
 
 
 def test_noalloc_rejects_oversize(ctx):
