@@ -1,21 +1,25 @@
 #!/usr/bin/env python
 """Hamiltonian-apply benchmark: H psi throughput in bands/s on one B200 per rank.
 
-One step applies H to every k point of the workload, 2*bands columns each (the Davidson
-block width at capacity), through one batched launch per stage (bg_kset_apply).  The
-default workload is Si8 in the conventional cube, 4x4x4 k mesh reduced to 36 k points,
-40 Ry, 24 bands: 36 x 48 = 1728 band applies per step, FP64.
+One step applies H to one block of `bands` columns per k point (the largest block the
+Davidson applies at once: its start block or a full correction block) through one
+batched launch per stage (bg_kset_apply).  The default workload is the Si216 cell
+(3x3x3 diamond supercell, a = 30.78 Bohr, +-0.05 Bohr seeded displacements, Gamma
+complex path, 30 Ry, 108^3 grid, 80,725 plane waves, 864 projectors, 480 bands):
+480 band applies per step, FP64.
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload si8]
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload si216]
 
 Prints ONE JSON line on rank 0.  `value` is device-timed (CUDA events on the launching
 stream, inputs resident in HBM, L2 flushed between timed steps); `e2e` is the same
-metric through the public API with pinned host buffers (host->device copy of the step's
-inputs and device->host copy of H x inside the timed region).  `--impl reference` times
-the CPU restatement of the reference's apply on the host cores (the reference itself is
-Rust and cannot be built here).  Multi-GPU: every rank applies its own replica of the
-workload (independent k-point sets, no data-path collective; weak scaling); timing is
-the max over ranks.
+metric through the public API with the caller's pageable host buffers (host->device
+copy of the step's inputs and device->host copy of H x inside the timed region), and
+`e2e_pinned` the same with pinned host buffers.  `--impl reference` times the CPU
+restatement of the reference's apply on the host cores (the reference itself is Rust
+and cannot be built here); that arm builds its operands with the oracle's own setup
+and loads nothing from the product package.  Multi-GPU: every rank applies its own
+replica of the workload (independent k-point sets, no data-path collective; weak
+scaling); timing is the max over ranks.
 """
 from __future__ import annotations
 
@@ -45,7 +49,7 @@ def parse_args(argv=None):
     p.add_argument("--steps", type=int, default=20)
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", choices=("ours", "reference"), default="ours")
-    p.add_argument("--workload", default="si8")
+    p.add_argument("--workload", default="si216")
     p.add_argument("--cpu-seconds", type=float, default=10.0, help="bound of the CPU baseline sample")
     p.add_argument("--no-scf", action="store_true", help="skip the SCF time-to-solution leg")
     return p.parse_args(argv)
@@ -200,25 +204,31 @@ def load_traffic(kernel: str, workload: str):
 
 
 # ---------------------------------------------------------------- CPU arm
-def cpu_sample(w, kpts, cols, budget_s, threads):
-    """Time the oracle's C++ FP64 restatement of the apply on a bounded sample of the
-    workload; returns (bands/s, sample description, seconds)."""
+_CPU_CELLS = {}   # workload name -> (oracle cell, [(basis, projectors, grid index)] per k point)
+
+
+def cpu_sample(name, cols, budget_s, threads, seed_offset=0):
+    """Time the oracle's CPU FP64 restatement of the apply (local part in C++ with one
+    column per thread, nonlocal products in BLAS) on a bounded sample of the workload:
+    blocks of `cols` columns, k point after k point, until `budget_s` is spent.  Operands
+    come from the oracle's own setup (oracle/workloads_ref.py).  Returns (bands/s,
+    sample description, seconds, microseconds per band per thread)."""
     from oracle import oracle as OR
-    from oracle import setup_ref as S
-    dims = w.dims()
-    v = w.ionic_potential()
-    cell = S.Cell(w.rows)
-    species = []
-    for s in w.species:
-        p = s.pseudo
-        ps = S.Pseudo(p.z, p.r, p.rab, p.local, [S.Projector(l, u) for l, u in zip(p.l, p.beta)], p.dij)
-        species.append(S.Species(ps, s.positions))
+    from oracle import workloads_ref as R
+    if name not in _CPU_CELLS:
+        c = R.CELLS[name]()
+        ops = []
+        for k, _ in c.kpoints[:64]:
+            b = c.basis(k)
+            ops.append((b, c.nonlocal_table(b), c.fft_index(b)))
+        _CPU_CELLS[name] = (c, ops)
+    c, ops = _CPU_CELLS[name]
+    dims = c.dims()
+    v = c.ionic_potential()
     done_bands, spent, used = 0, 0.0, 0
-    for (k, _) in kpts:
-        b = S.basis_at_k(cell, w.ecut_ha, k)
-        nl = S.nonlocal_table(b, cell.volume, species)
-        idx = S.fft_flat(S.g_to_fft(b, dims), dims)
-        x = w.random_block(b.npw, cols, seed_offset=used)
+    for i in range(len(ops) * 64):
+        b, nl, idx = ops[i % len(ops)]
+        x = c.random_block(b.npw, cols, seed_offset=seed_offset + i)
         t0 = time.perf_counter()
         OR.apply_complex(dims, idx, v, 0.5 * b.kpg2, nl, x, threads=threads)
         spent += time.perf_counter() - t0
@@ -226,33 +236,39 @@ def cpu_sample(w, kpts, cols, budget_s, threads):
         used += 1
         if spent >= budget_s:
             break
-    return done_bands / spent, f"{used} of {len(kpts)} k points x {cols} columns", spent
+    rate = done_bands / spent
+    desc = f"{used} blocks of {cols} columns over {min(used, len(ops))} of {len(c.kpoints)} k points"
+    return rate, desc, spent, 1e6 * threads / rate
 
 
 def run_reference(args):
     rank, world, _ = dist_env()
     if rank != 0:
         return 0
-    w = build_workload(args.workload)
-    cols = 2 * w.bands
+    from oracle import workloads_ref as R
+    c = R.CELLS[args.workload]()
+    cols = c.bands
     threads = len(os.sched_getaffinity(0))
     per_step_budget = max(1.0, min(8.0, 150.0 / max(1, args.steps + args.warmup)))
     for _ in range(args.warmup):
-        cpu_sample(w, w.kpoints[:1], cols, 0.0, threads)
-    rates, samples = [], []
+        cpu_sample(args.workload, min(cols, threads), 0.0, threads)
+    rates, samples, per_band = [], [], []
     for _ in range(args.steps):
-        rate, desc, _ = cpu_sample(w, w.kpoints, cols, per_step_budget, threads)
+        rate, desc, _, us = cpu_sample(args.workload, cols, per_step_budget, threads)
         rates.append(rate)
         samples.append(desc)
+        per_band.append(us)
     value = statistics.median(rates)
     line = {
         "impl": "reference", "metric": "H psi apply throughput (FP64)", "value": value, "unit": "bands/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": 1000.0 * len(w.kpoints) * cols / value, "higher_is_better": True, "scaling": "weak",
+        "ms_per_step": 1000.0 * len(c.kpoints) * cols / value, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": w.name, "kpoints": len(w.kpoints), "columns_per_k": cols, "grid": w.dims()},
+        "config": {"workload": c.name, "kpoints": len(c.kpoints), "columns_per_k": cols, "grid": c.dims()},
         "cpu_baseline": {"value": value, "unit": "bands/s", "cores": threads, "kind": "port",
-                         "sample": samples[0] + " per step (oracle C++ FP64 restatement, OpenMP over columns)"},
+                         "us_per_band_per_thread": statistics.median(per_band),
+                         "sample": samples[0] + " per step (oracle CPU FP64 restatement: local part in C++, "
+                                                "one column per thread; nonlocal products in BLAS)"},
         "e2e": {"value": value, "unit": "bands/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -273,7 +289,7 @@ def run_ours(args):
     w = build_workload(args.workload)
     w.seed = shard_seeds(rank, w.seed)
     dims = w.dims()
-    cols = 2 * w.bands
+    cols = w.bands
     v = w.ionic_potential()
     ctx = H.Context(local)
     ops, xs, ys, shapes = [], [], [], []
@@ -324,29 +340,40 @@ def run_ours(args):
     kset.sync()
     fp32 = precision_leg(kset, xs, ys, stream, flush, args.steps, STAGES)
     total_ms = max_over_ranks(float(sum(step_ms)), dist, "cuda")
-    bands_step = len(w.kpoints) * cols
-    value = bands_step * args.steps * world / (total_ms / 1000.0)
+    value = len(w.kpoints) * cols * args.steps * world / (total_ms / 1000.0)
 
-    # end to end through the public API with pinned host buffers
+    # end to end through the public API: the caller's pageable host blocks (as the
+    # reference's ComplexMatrix storage is), then pinned ones
+    def e2e_run(hx, hy):
+        for _ in range(2):
+            kset.apply_blocks(hx, hy)
+        if dist:
+            dist.barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            kset.apply_blocks(hx, hy)
+        return bands_step * args.steps * world / max_over_ranks(time.perf_counter() - t0, dist, "cuda")
+
+    bands_step = len(w.kpoints) * cols
+    px = [np.asfortranarray(x.cpu().numpy().T) for x in xs]
+    py = [np.zeros_like(x, order="F") for x in px]
+    e2e_value = e2e_run(px, py)
+    h2d = sum(x.nbytes for x in px)
+    d2h = sum(y.nbytes for y in py)
+    del px, py
     hx, hy = [], []
     for x in xs:
         hx_t = torch.empty(x.shape, dtype=x.dtype, pin_memory=True)
         hx_t.copy_(x)
         hx.append(hx_t.numpy().T)
         hy.append(torch.empty(x.shape, dtype=x.dtype, pin_memory=True).numpy().T)
-    for _ in range(2):
-        kset.apply_blocks(hx, hy)
-    if dist:
-        dist.barrier()
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        kset.apply_blocks(hx, hy)
-    e2e_s = max_over_ranks(time.perf_counter() - t0, dist, "cuda")
-    e2e_value = bands_step * args.steps * world / e2e_s
-    h2d = sum(x.nbytes for x in hx)
-    d2h = sum(y.nbytes for y in hy)
+    e2e_pinned = e2e_run(hx, hy)
+    del hx, hy
 
-    # roofline of the dominant kernel
+    # roofline of the dominant kernel: HBM-bound stages against the measured copy peak;
+    # the FP64 products (projection, back-projection) against the nominal FP64 peak
+    # (148 SMs x 64 FP64 fused multiply-adds per clock at the maximum SM clock); every
+    # stage's time bound max(bytes / HBM peak, flops / FP64 peak) is listed as well.
     hbm_peak, _, peak_kind = load_peaks()
     sbytes = stage_bytes(shapes, dims, cols, nproj)
     xact = 0.5
@@ -354,31 +381,38 @@ def run_ours(args):
     avg_ms = stage_ms / args.steps
     dom = int(np.argmax(avg_ms))
     dname = STAGES[dom]
-    achieved = sbytes[dname] / (avg_ms[dom] / 1000.0) / 1e9
-    traffic = load_traffic(KERNELS[dname], w.name)
-    roofline = {"bound": "hbm", "kernel": KERNELS[dname], "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
-                "frac": achieved / hbm_peak, "peak_kind": peak_kind, "traffic": traffic,
-                "algorithmic_bytes_per_launch": sbytes[dname],
-                "fp64_tflops": sflops[dname] / (avg_ms[dom] / 1000.0) / 1e12,
-                "stage_ms": {s: float(m) for s, m in zip(STAGES, avg_ms)}}
-    # The plane kernel's bound in time: max(bytes / HBM peak, flops / FP64 peak); the FP64
-    # peak is nominal (148 SMs x 64 FP64 fused multiply-adds per clock at the maximum SM
-    # clock), the copy peak the measured one.
     fp64_peak = 148 * 64 * 2 * 1.965e9 / 1e12
-    t_bytes = sbytes[dname] / (hbm_peak * 1e9) * 1e3
-    t_flops = sflops[dname] / (fp64_peak * 1e12) * 1e3
-    roofline.update({"fp64_peak_tflops": fp64_peak, "fp64_peak_kind": "nominal",
-                     "fp64_frac": roofline["fp64_tflops"] / fp64_peak,
-                     "bound_ms": max(t_bytes, t_flops), "bound_by": "fp64" if t_flops > t_bytes else "hbm",
-                     "frac_of_bound": max(t_bytes, t_flops) / avg_ms[dom]})
+    bounds = {}
+    for i, st in enumerate(STAGES):
+        t_b = sbytes[st] / (hbm_peak * 1e9) * 1e3
+        t_f = sflops[st] / (fp64_peak * 1e12) * 1e3
+        bounds[st] = {"ms": float(avg_ms[i]), "bound_ms": max(t_b, t_f), "bound_by": "fp64" if t_f > t_b else "hbm",
+                      "frac_of_bound": max(t_b, t_f) / avg_ms[i] if avg_ms[i] > 0 else None}
+    traffic = load_traffic(KERNELS[dname], w.name)
+    if bounds[dname]["bound_by"] == "fp64":
+        achieved = sflops[dname] / (avg_ms[dom] / 1000.0) / 1e12
+        roofline = {"bound": "fp64", "kernel": KERNELS[dname], "achieved": achieved, "peak": fp64_peak,
+                    "unit": "TFLOP/s", "frac": achieved / fp64_peak, "peak_kind": "nominal (no measured FP64 peak)",
+                    "traffic": traffic, "algorithmic_flops_per_launch": sflops[dname],
+                    "hbm_gbs": sbytes[dname] / (avg_ms[dom] / 1000.0) / 1e9}
+    else:
+        achieved = sbytes[dname] / (avg_ms[dom] / 1000.0) / 1e9
+        roofline = {"bound": "hbm", "kernel": KERNELS[dname], "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+                    "frac": achieved / hbm_peak, "peak_kind": peak_kind, "traffic": traffic,
+                    "algorithmic_bytes_per_launch": sbytes[dname],
+                    "fp64_tflops": sflops[dname] / (avg_ms[dom] / 1000.0) / 1e12}
+    roofline.update({"stage_ms": {s_: float(m) for s_, m in zip(STAGES, avg_ms)}, "stage_bounds": bounds,
+                     "fp64_peak_tflops": fp64_peak, "frac_of_bound": bounds[dname]["frac_of_bound"],
+                     "bound_by": bounds[dname]["bound_by"]})
 
     # CPU baseline: rank 0, N=1 only
     cpu = None
     if rank == 0 and world == 1:
         threads = len(os.sched_getaffinity(0))
-        rate, desc, spent = cpu_sample(w, w.kpoints, cols, args.cpu_seconds, threads)
-        cpu = {"value": rate, "unit": "bands/s", "cores": threads, "kind": "port",
-               "sample": desc + f" ({spent:.1f} s; oracle C++ FP64 restatement, OpenMP over columns)"}
+        rate, desc, spent, us = cpu_sample(args.workload, cols, args.cpu_seconds, threads)
+        cpu = {"value": rate, "unit": "bands/s", "cores": threads, "kind": "port", "us_per_band_per_thread": us,
+               "sample": desc + f" ({spent:.1f} s; oracle CPU FP64 restatement: local part in C++, one column "
+                                "per thread; nonlocal products in BLAS)"}
     scf = None
     if rank == 0 and world == 1 and not args.no_scf and args.workload in ("si8", "si2"):
         scf = scf_leg(args.workload, ctx)
@@ -395,7 +429,10 @@ def run_ours(args):
                        "npw_min": min(s[0] for s in shapes), "npw_max": max(s[0] for s in shapes),
                        "nproj": nproj, "l2": "flushed between timed steps (256 MiB write)",
                        "parallelism": f"replica x{world}"},
-            "e2e": {"value": e2e_value, "unit": "bands/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "e2e": {"value": e2e_value, "unit": "bands/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "host_buffers": "pageable"},
+            "e2e_pinned": {"value": e2e_pinned, "unit": "bands/s", "h2d_bytes_per_step": h2d,
+                           "d2h_bytes_per_step": d2h},
             "gpu_launches": launches, "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks,
             "scf": scf, "fp32_local": fp32,
         }

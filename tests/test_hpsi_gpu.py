@@ -27,8 +27,9 @@ def _operator(w, k, cap, ctx):
 @pytest.mark.parametrize("name,kidx,cols", [
     ("si2", 0, 7), ("si2", 0, 16),
     ("si8", 0, 5), ("si8", 7, 6), ("si8", 35, 3),
-    ("si64", 0, 4),
+    ("si64", 0, 16),
     ("al32", 3, 4),
+    ("si216", 0, 4),
 ])
 def test_apply_matches_oracle(ctx, name, kidx, cols):
     w = W.WORKLOADS[name]()
