@@ -118,6 +118,13 @@ struct Bufs {
   int *starts, *clusters;        // cap + 1: its blocks and clusters
   const double* diag;            // rows
   int rows;
+  // reduced problem on many blocks (large capacities): L^H, inverse-iteration strips
+  // (4 cap x cap doubles), error bits, tridiagonal metadata (pivmin; block and cluster counts)
+  D* LT;
+  double* lu;
+  int* werr;
+  double* wmeta;
+  int* wimeta;
 };
 
 // Per-k control scalars.
@@ -125,6 +132,9 @@ struct Ctl {
   int m, nact, kept, status, iterations;
   int contract, repair, need_repair;
   int reduced_solves, h_calls, h_columns, repairs, contractions, dropped;
+  // requests to the many-block reduced problem: extend the factor from wc_m0 to wc_m1
+  // columns, solve the reduced problem of we_m columns (0: none)
+  int wc_m0, wc_m1, we_m;
 };
 
 // Descriptors of the large products of one slot (written by the control kernel).
@@ -156,6 +166,7 @@ struct Opts {
   int preconditioner;
   int smem_matrices;  // the control kernel keeps A, Y, Q, Z in shared memory
   int fp32;           // H applies with the FP32 local part
+  int wide;           // the reduced problem runs on many blocks (wide_rr.cuh)
 };
 
 // ------------------------------------------------------------------ block-wide small algebra
@@ -639,6 +650,14 @@ __global__ void __launch_bounds__(256) k_dv_corrections(const Bufs<D>* __restric
   if (threadIdx.x == 0) b.norms[j] = n2;
 }
 
+}  // namespace dv
+}  // namespace bg
+
+#include "wide_rr.cuh"
+
+namespace bg {
+namespace dv {
+
 // ------------------------------------------------------------------ control kernel
 enum Phase : int {
   kSetup = 0,   // after H V and the Grams of the start block: factor, eigensolve
@@ -653,6 +672,13 @@ enum Phase : int {
   kApply,       // repair border; the apply block
   kFinish,      // border H_r, eigensolve, convergence
   kFinal,       // X = V C[:, :n]
+  // with Opts::wide the phases above that factor or solve stop after posting a request
+  // to the many-block kernels; these phases take their results and finish the step
+  kSetupPost,
+  kRefreshPost,
+  kExtendPost,
+  kApplyPost,
+  kFinishPost,
 };
 
 constexpr int kNnSlots = 2, kTnSlots = 2, kCpSlots = 3;
@@ -720,8 +746,100 @@ __global__ void __launch_bounds__(kCtlThreads, 1) k_dv_ctl(int phase, Bufs<D>* _
     __syncthreads();
   };
   D* Vt = b.V + (int64_t)c.m * rows;    // first free basis column
+  // a request to the many-block reduced problem (its error bits cleared for it)
+  auto request = [&](int m0, int m1, int me) {
+    if (threadIdx.x == 0) {
+      c.wc_m0 = m0;
+      c.wc_m1 = m1;
+      c.we_m = me;
+      *bufs[k].werr = 0;
+    }
+  };
+  auto clear_request = [&]() {
+    if (threadIdx.x == 0) {
+      c.wc_m0 = 0;
+      c.wc_m1 = 0;
+      c.we_m = 0;
+    }
+  };
+  auto werr = [&]() -> int { return *(volatile int*)bufs[k].werr; };
+  // capacity check, the rotations of the active Ritz vectors (after any contraction)
+  auto refresh_tail = [&]() {
+    if (c.m + c.nact > cap && cap < rows) {
+      set_err(kErrCapacity);
+      return;
+    }
+    const int m = c.m, na = c.nact;
+    for (int t = threadIdx.x; t < m * na; t += blockDim.x) {
+      const int i = t % m, j = t / m;
+      b.P[i + (size_t)j * cap] = b.C[i + (size_t)b.active[j] * cap];
+    }
+    for (int j = threadIdx.x; j < na; j += blockDim.x) b.lam[j] = b.w[b.active[j]];
+    if (threadIdx.x == 0) {
+      nn[0 * nk + k] = NN<D>{b.V, b.P, b.X, cap, na, m, 0};
+      nn[1 * nk + k] = NN<D>{b.HV, b.P, b.HX, cap, na, m, 0};
+    }
+  };
+  // the repair's descriptors when the bordered factor could not be extended
+  auto extend_tail = [&](bool repair) {
+    const int m = c.m, kk = c.kept;
+    if (threadIdx.x == 0 && repair) {
+      c.repair = 1;
+      c.repairs += 1;
+      if (!c.need_repair) cp[0 * nk + k] = CP<D>{Vt, b.E, kk, 0};  // corrections were appended already
+      nn[0 * nk + k] = NN<D>{b.V, b.C, b.X, cap, m, m, 0};
+      nn[1 * nk + k] = NN<D>{b.HV, b.C, b.HX, cap, m, m, 0};
+      cp[1 * nk + k] = CP<D>{b.X, b.V, m, 0};
+      cp[2 * nk + k] = CP<D>{b.HX, b.HV, m, 0};
+    }
+  };
+  auto apply_tail = [&]() {
+    const int m = c.m, kk = c.kept;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) b.old[i] = b.w[i];
+    if (threadIdx.x == 0 && kk > 0) {
+      c.h_calls += 1;
+      c.h_columns += kk;
+      dyn[k] = DynCols{reinterpret_cast<const double*>(Vt), reinterpret_cast<double*>(b.HV + (int64_t)m * rows), kk,
+                       gamma ? (kk + 1) / 2 : kk};
+      tn[0 * nk + k] = TN<D>{b.V, b.HV + (int64_t)m * rows, b.Hr + (size_t)m * cap, cap, m + kk, kk};
+    }
+  };
+  auto finish_tail = [&](int kk) {
+    if (threadIdx.x == 0) {
+      if (kk > 0) {
+        c.m += kk;
+        c.reduced_solves += 1;
+      }
+      int na = 0;
+      for (int i = 0; i < n; ++i) {
+        const double thr = (o.first_step || i < o.occupied) ? o.threshold : fmax(5.0 * o.threshold, 5e-6);
+        const bool cv = fabs(b.w[i] - b.old[i]) < thr;
+        b.conv[i] = cv ? 1 : 0;
+        if (!cv) b.active[na++] = i;
+      }
+      c.nact = na;
+      c.iterations += 1;
+      if (na == 0 || c.iterations == o.max_iterations) {
+        c.status = 1;
+      } else if (c.m + na > cap) {
+        c.contract = 1;   // the reference contracts at the end of this iteration
+      }
+    }
+  };
+  auto setup_tail = [&]() {
+    if (threadIdx.x == 0) {
+      c.reduced_solves += 1;
+      c.m = n;
+      c.nact = n;
+      for (int i = 0; i < n; ++i) b.active[i] = i;
+    }
+  };
   switch (phase) {
     case kSetup: {
+      if (o.wide) {
+        request(0, n, n);
+        break;
+      }
       if (!chol_extend(b.S, cap, b.L, 0, n, &sh[4])) {
         set_err(kErrStartDependent);
         break;
@@ -730,12 +848,21 @@ __global__ void __launch_bounds__(kCtlThreads, 1) k_dv_ctl(int phase, Bufs<D>* _
         set_err(kErrEigen);
         break;
       }
-      if (threadIdx.x == 0) {
-        c.reduced_solves += 1;
-        c.m = n;
-        c.nact = n;
-        for (int i = 0; i < n; ++i) b.active[i] = i;
+      setup_tail();
+      break;
+    }
+    case kSetupPost: {
+      const int we = werr();
+      if (we & wide::kWErrPivot) {
+        set_err(kErrStartDependent);
+        break;
       }
+      if (we) {
+        set_err(kErrEigen);
+        break;
+      }
+      clear_request();
+      setup_tail();
       break;
     }
     case kBegin: {
@@ -768,6 +895,10 @@ __global__ void __launch_bounds__(kCtlThreads, 1) k_dv_ctl(int phase, Bufs<D>* _
           bufs[k].HV = b.HV;
           bufs[k].HX = b.HX;
         }
+        if (o.wide) {
+          request(0, n, n);
+          break;
+        }
         if (!chol_extend(b.S, cap, b.L, 0, n, &sh[4])) {
           set_err(kErrBasisDependent);
           break;
@@ -784,20 +915,31 @@ __global__ void __launch_bounds__(kCtlThreads, 1) k_dv_ctl(int phase, Bufs<D>* _
         }
         __syncthreads();
       }
-      if (c.m + c.nact > cap && cap < rows) {
-        set_err(kErrCapacity);
-        break;
+      if (o.wide) break;
+      refresh_tail();
+      break;
+    }
+    case kRefreshPost: {
+      if (c.we_m) {  // the contraction's factor and eigensolve
+        const int we = werr();
+        if (we & wide::kWErrPivot) {
+          set_err(kErrBasisDependent);
+          break;
+        }
+        if (we) {
+          set_err(kErrEigen);
+          break;
+        }
+        clear_request();
+        if (threadIdx.x == 0) {
+          c.contractions += 1;
+          c.reduced_solves += 1;
+          c.m = n;
+          c.contract = 0;
+        }
+        __syncthreads();
       }
-      const int m = c.m, na = c.nact;
-      for (int t = threadIdx.x; t < m * na; t += blockDim.x) {
-        const int i = t % m, j = t / m;
-        b.P[i + (size_t)j * cap] = b.C[i + (size_t)b.active[j] * cap];
-      }
-      for (int j = threadIdx.x; j < na; j += blockDim.x) b.lam[j] = b.w[b.active[j]];
-      if (threadIdx.x == 0) {
-        nn[0 * nk + k] = NN<D>{b.V, b.P, b.X, cap, na, m, 0};
-        nn[1 * nk + k] = NN<D>{b.HV, b.P, b.HX, cap, na, m, 0};
-      }
+      refresh_tail();
       break;
     }
     case kSelect: {
@@ -836,17 +978,21 @@ __global__ void __launch_bounds__(kCtlThreads, 1) k_dv_ctl(int phase, Bufs<D>* _
       bool repair = c.need_repair != 0;
       if (!repair) {
         mirror(b.S, m, m + kk);
+        if (o.wide) {
+          request(m, m + kk, 0);
+          break;
+        }
         if (!chol_extend(b.S, cap, b.L, m, m + kk, &sh[4])) repair = true;
       }
-      if (threadIdx.x == 0 && repair) {
-        c.repair = 1;
-        c.repairs += 1;
-        if (!c.need_repair) cp[0 * nk + k] = CP<D>{Vt, b.E, kk, 0};  // corrections were appended already
-        nn[0 * nk + k] = NN<D>{b.V, b.C, b.X, cap, m, m, 0};
-        nn[1 * nk + k] = NN<D>{b.HV, b.C, b.HX, cap, m, m, 0};
-        cp[1 * nk + k] = CP<D>{b.X, b.V, m, 0};
-        cp[2 * nk + k] = CP<D>{b.HX, b.HV, m, 0};
-      }
+      if (o.wide) break;
+      extend_tail(repair);
+      break;
+    }
+    case kExtendPost: {
+      bool repair = c.need_repair != 0;
+      if (!repair && c.wc_m1 > c.wc_m0) repair = werr() != 0;
+      clear_request();
+      extend_tail(repair);
       break;
     }
     case kRepair1: {
@@ -936,50 +1082,56 @@ __global__ void __launch_bounds__(kCtlThreads, 1) k_dv_ctl(int phase, Bufs<D>* _
       const int m = c.m, kk = c.kept;
       if (c.repair && kk > 0) {
         mirror(b.S, m, m + kk);
+        if (o.wide) {
+          request(m, m + kk, 0);
+          break;
+        }
         if (!chol_extend(b.S, cap, b.L, m, m + kk, &sh[4])) {
           set_err(kErrRepairDependent);
           break;
         }
       }
-      for (int i = threadIdx.x; i < n; i += blockDim.x) b.old[i] = b.w[i];
-      if (threadIdx.x == 0 && kk > 0) {
-        c.h_calls += 1;
-        c.h_columns += kk;
-        dyn[k] = DynCols{reinterpret_cast<const double*>(Vt), reinterpret_cast<double*>(b.HV + (int64_t)m * rows), kk,
-                         gamma ? (kk + 1) / 2 : kk};
-        tn[0 * nk + k] = TN<D>{b.V, b.HV + (int64_t)m * rows, b.Hr + (size_t)m * cap, cap, m + kk, kk};
+      if (o.wide) break;
+      apply_tail();
+      break;
+    }
+    case kApplyPost: {
+      if (c.wc_m1 > c.wc_m0) {
+        if (werr()) {
+          set_err(kErrRepairDependent);
+          break;
+        }
+        clear_request();
       }
+      apply_tail();
       break;
     }
     case kFinish: {
       const int kk = c.kept;
       if (kk > 0) {
         mirror(b.Hr, c.m, c.m + kk);
+        if (o.wide) {
+          request(0, 0, c.m + kk);
+          break;
+        }
         if (!eigen(b, cap, c.m + kk, red, sh)) {
           set_err(kErrEigen);
           break;
         }
       }
-      if (threadIdx.x == 0) {
-        if (kk > 0) {
-          c.m += kk;
-          c.reduced_solves += 1;
+      if (o.wide) break;
+      finish_tail(kk);
+      break;
+    }
+    case kFinishPost: {
+      if (c.we_m) {
+        if (werr()) {
+          set_err(kErrEigen);
+          break;
         }
-        int na = 0;
-        for (int i = 0; i < n; ++i) {
-          const double thr = (o.first_step || i < o.occupied) ? o.threshold : fmax(5.0 * o.threshold, 5e-6);
-          const bool cv = fabs(b.w[i] - b.old[i]) < thr;
-          b.conv[i] = cv ? 1 : 0;
-          if (!cv) b.active[na++] = i;
-        }
-        c.nact = na;
-        c.iterations += 1;
-        if (na == 0 || c.iterations == o.max_iterations) {
-          c.status = 1;
-        } else if (c.m + na > cap) {
-          c.contract = 1;   // the reference contracts at the end of this iteration
-        }
+        clear_request();
       }
+      finish_tail(c.kept);
       break;
     }
     case kFinal: {
@@ -1078,18 +1230,20 @@ template <class T>
 class KsetSolver {
  public:
   using D = typename DevOf<T>::type;
-  KsetSolver(bg_kset* ks, int n, int cap) : ks_(ks), nk_((int)ks->ops.size()) {
+  KsetSolver(bg_kset* ks, int n, int cap, bool wide) : ks_(ks), nk_((int)ks->ops.size()), wide_(wide) {
     o_.n = n;
     o_.cap = cap;
     o_.smem_matrices = small(cap) ? 1 : 0;
+    o_.wide = wide ? 1 : 0;
   }
-  bool matches(int n, int cap) const { return o_.n == n && o_.cap == cap; }
+  bool matches(int n, int cap, bool wide) const { return o_.n == n && o_.cap == cap && wide_ == wide; }
   // Per-call options (threshold, occupied, first_step, iterations, preconditioner).
   // The captured iteration holds the apply's kernels, so each apply precision keeps a
   // graph of its own.
   void set_options(const Opts& o, bool graph) {
     o_ = o;
     o_.smem_matrices = small(o.cap) ? 1 : 0;
+    o_.wide = wide_ ? 1 : 0;
     want_graph_ = graph;
   }
   ~KsetSolver() {
@@ -1110,6 +1264,10 @@ class KsetSolver {
  private:
   bg_kset* ks_;
   int nk_;
+  bool wide_ = false;
+  unsigned* d_bar_ = nullptr;   // grid barrier of the cooperative launches
+  double* d_wpart_ = nullptr;   // their per-block partial sums
+  int coop_blocks_ = 0;
   Opts o_;
   bool want_graph_ = true;
   bool prepared_ = false;
@@ -1194,6 +1352,14 @@ class KsetSolver {
     k_dv_corrections<D><<<dim3((unsigned)o_.n, (unsigned)nk_), 256, 0, s_>>>(d_bufs_, d_ctl_, d_opts_);
     return 1;
   }
+  // Many-block reduced problem (wide_rr.cuh): extension of the factor, then the
+  // eigensolve; each launch returns at once for k points without a request.
+  int64_t wchol() {
+    return wide::launch_chol<D>(d_bufs_, d_ctl_, nk_, o_.cap, coop_blocks_, d_bar_, s_);
+  }
+  int64_t weig() {
+    return wide::launch_eig<D>(d_bufs_, d_ctl_, nk_, o_.cap, coop_blocks_, d_bar_, d_wpart_, s_);
+  }
   int64_t apply() {
     if (ks_->dense) {
       const dim3 grid((unsigned)((max_rows_ + 63) / 64), (unsigned)((o_.n + 31) / 32), (unsigned)nk_);
@@ -1205,15 +1371,22 @@ class KsetSolver {
   int64_t iteration() {
     int64_t l = 0;
     l += ctl(kBegin) + nn(2) + tn(2);
-    l += ctl(kRefresh) + nn(2) + corr();
+    l += ctl(kRefresh);
+    if (wide_) l += wchol() + weig() + ctl(kRefreshPost);
+    l += nn(2) + corr();
     l += ctl(kSelect) + cp(0, 1) + tn(1);
-    l += ctl(kExtend) + cp(0, 1) + nn(2) + cp(1, 2);
+    l += ctl(kExtend);
+    if (wide_) l += wchol() + ctl(kExtendPost);
+    l += cp(0, 1) + nn(2) + cp(1, 2);
     l += ctl(kRepair1) + tn(1);
     l += ctl(kRepair2) + nn(1) + tn(1);
     l += ctl(kRepair3) + nn(1) + tn(1);
     l += ctl(kRepair4) + nn(1) + cp(0, 1) + tn(1);
-    l += ctl(kApply) + apply() + tn(1);
+    l += ctl(kApply);
+    if (wide_) l += wchol() + ctl(kApplyPost);
+    l += apply() + tn(1);
     l += ctl(kFinish);
+    if (wide_) l += weig() + ctl(kFinishPost);
     return l;
   }
   int prepare();
@@ -1264,6 +1437,16 @@ int KsetSolver<T>::prepare() {
     double* dg = nullptr;
     if ((rc = alloc(&dg, b.rows))) return rc;
     b.diag = dg;
+    if (wide_) {
+      if ((rc = alloc(&b.LT, cc)) || (rc = alloc(&b.lu, 4 * cc)) || (rc = alloc(&b.werr, 1)) ||
+          (rc = alloc(&b.wmeta, 8)) || (rc = alloc(&b.wimeta, 8)) || (rc = alloc(&b.e2, cap)) ||
+          (rc = alloc(&b.wu, cap)) || (rc = alloc(&b.starts, cap + 1)) || (rc = alloc(&b.clusters, cap + 1)))
+        return rc;
+    }
+  }
+  if (wide_) {
+    if ((rc = wide::prepare<D>(cap, &coop_blocks_, &err_))) return rc;
+    if ((rc = alloc(&d_bar_, 2)) || (rc = alloc(&d_wpart_, (size_t)coop_blocks_))) return rc;
   }
   if ((rc = alloc(&d_bufs_, nk_)) || (rc = alloc(&d_ctl_, nk_)) || (rc = alloc(&d_nn_, (size_t)kNnSlots * nk_)) ||
       (rc = alloc(&d_tn_, (size_t)kTnSlots * nk_)) || (rc = alloc(&d_cp_, (size_t)kCpSlots * nk_)) ||
@@ -1353,7 +1536,9 @@ int KsetSolver<T>::run(const double* const* start, const double* const* diagonal
       (rc = cuda(cudaMemcpyAsync(d_dyn_, dy.data(), sizeof(DynCols) * nk_, cudaMemcpyHostToDevice, s_), "upload")) ||
       (rc = cuda(cudaMemcpyAsync(d_tn_, t0.data(), sizeof(TN<D>) * t0.size(), cudaMemcpyHostToDevice, s_), "upload")))
     return rc;
+  if (wide_ && (rc = cuda(cudaMemsetAsync(d_bar_, 0, 2 * sizeof(unsigned), s_), "barrier"))) return rc;
   launches_ += apply() + tn(2) + ctl(kSetup);
+  if (wide_) launches_ += wchol() + weig() + ctl(kSetupPost);
   bool done = false;
   if ((rc = poll(&done))) return rc;
   // iterations: one captured graph replayed until every k point has finished
@@ -1431,6 +1616,105 @@ int KsetSolver<T>::run(const double* const* start, const double* const* diagonal
   return BG_OK;
 }
 
+// Generalised Hermitian eigenproblem H C = S C diag(w) of one m x m pencil through the
+// many-block path of the batched Davidson (wide_rr.cuh): the Cholesky factor of S with the
+// pivot rule, then A = L^-1 H L^-H, its eigenpairs and C = L^-H Y.
+template <class D>
+int reduced_eigh(int m, const double* S, const double* H, double* w, double* C, double* ms, std::string* err) {
+  std::vector<void*> mem;
+  auto alloc = [&](auto** p, size_t count) -> bool {
+    void* q = nullptr;
+    if (cudaMalloc(&q, std::max<size_t>(count, 1) * sizeof(**p)) != cudaSuccess) return false;
+    mem.push_back(q);
+    *p = static_cast<std::remove_reference_t<decltype(**p)>*>(q);
+    return true;
+  };
+  struct Free {
+    std::vector<void*>* m;
+    ~Free() {
+      for (void* p : *m) cudaFree(p);
+    }
+  } guard{&mem};
+  const int cap = m;
+  const size_t cc = (size_t)cap * cap;
+  Bufs<D> b{};
+  bool ok = alloc(&b.S, cc) && alloc(&b.Hr, cc) && alloc(&b.L, cc) && alloc(&b.C, cc) && alloc(&b.A, cc) &&
+            alloc(&b.Y, cc) && alloc(&b.Q, cc) && alloc(&b.Z, cc) && alloc(&b.LT, cc) && alloc(&b.lu, 4 * cc) &&
+            alloc(&b.w, cap) && alloc(&b.td, cap) && alloc(&b.te, cap) && alloc(&b.e2, cap) && alloc(&b.wu, cap) &&
+            alloc(&b.off, cap) && alloc(&b.ph, cap) && alloc(&b.hp, cap) && alloc(&b.starts, cap + 1) &&
+            alloc(&b.clusters, cap + 1) && alloc(&b.order, cap) && alloc(&b.werr, 1) && alloc(&b.wmeta, 8) &&
+            alloc(&b.wimeta, 8);
+  Bufs<D>* d_b = nullptr;
+  Ctl* d_c = nullptr;
+  unsigned* bar = nullptr;
+  double* part = nullptr;
+  int blocks = 0;
+  ok = ok && alloc(&d_b, 1) && alloc(&d_c, 1) && alloc(&bar, 2);
+  if (!ok) {
+    *err = "cudaMalloc failed";
+    return BG_ENOMEM;
+  }
+  int rc = wide::prepare<D>(cap, &blocks, err);
+  if (rc) return rc;
+  if (!alloc(&part, (size_t)blocks)) {
+    *err = "cudaMalloc failed";
+    return BG_ENOMEM;
+  }
+  Ctl c{};
+  c.wc_m0 = 0;
+  c.wc_m1 = m;
+  c.we_m = m;
+  cudaStream_t s = nullptr;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  cudaError_t e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreate(&e0);
+  if (e == cudaSuccess) e = cudaEventCreate(&e1);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(b.S, S, sizeof(D) * cc, cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(b.Hr, H, sizeof(D) * cc, cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(b.L, 0, sizeof(D) * cc, s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(b.werr, 0, sizeof(int), s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(bar, 0, 2 * sizeof(unsigned), s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(d_b, &b, sizeof b, cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(d_c, &c, sizeof c, cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) e = cudaEventRecord(e0, s);
+  if (e == cudaSuccess) {
+    wide::launch_chol<D>(d_b, d_c, 1, cap, blocks, bar, s);
+    wide::launch_eig<D>(d_b, d_c, 1, cap, blocks, bar, part, s);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaEventRecord(e1, s);
+  int werr = 0;
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&werr, b.werr, sizeof(int), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  float t = 0.0f;
+  if (e == cudaSuccess && ms) e = cudaEventElapsedTime(&t, e0, e1);
+  if (ms) *ms = t;
+  if (e == cudaSuccess && !werr) {
+    e = cudaMemcpy(w, b.w, sizeof(double) * m, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(C, b.C, sizeof(D) * cc, cudaMemcpyDeviceToHost);
+  }
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  if (s) cudaStreamDestroy(s);
+  if (e != cudaSuccess) {
+    *err = std::string("reduced eigensolve: ") + cudaGetErrorString(e);
+    return BG_EDEVICE;
+  }
+  if (werr & wide::kWErrBarrier) {
+    *err = "reduced eigensolve: a grid barrier gave up";
+    return BG_ETIMEOUT;
+  }
+  if (werr & wide::kWErrPivot) {
+    *err = "overlap is numerically dependent (pivot rule)";
+    return BG_ESHAPE;
+  }
+  if (werr) {
+    *err = "non-finite reduced matrix";
+    return BG_ENONFINITE;
+  }
+  return BG_OK;
+}
+
 }  // namespace dv
 }  // namespace bg
 
@@ -1484,6 +1768,9 @@ extern "C" int bg_kset_davidson_solve(bg_kset* ks, const double* const* start, c
   Opts op{(int)n, (int)cap, (int)o.occupied, o.first_step ? 1 : 0, o.max_iterations, o.threshold, o.preconditioner, 0,
           o.apply_precision == BG_PREC_FP32 ? 1 : 0};
   const bool graph = (o.flags & 1) == 0;
+  // the reduced problem on many blocks beyond capacity 128 (flags bit 1 forces it, bit 2
+  // keeps the one-block control kernel)
+  const bool wide = (o.flags & 2) != 0 || (cap > 128 && (o.flags & 4) == 0);
   int rc;
   if (o.apply_precision == BG_PREC_FP32)  // the FP32 potential copies, on the set's stream
     for (bg_op* kop : ks->ops)
@@ -1495,13 +1782,13 @@ extern "C" int bg_kset_davidson_solve(bg_kset* ks, const double* const* start, c
   auto solve = [&](auto* tag) -> int {
     using S = std::remove_pointer_t<decltype(tag)>;
     S* s = static_cast<S*>(ks->dv_cache);
-    if (s && !s->matches(op.n, op.cap)) {
+    if (s && !s->matches(op.n, op.cap, wide)) {
       ks->dv_free(ks->dv_cache);
       ks->dv_cache = nullptr;
       s = nullptr;
     }
     if (!s) {
-      s = new S(ks, op.n, op.cap);
+      s = new S(ks, op.n, op.cap, wide);
       ks->dv_cache = s;
       ks->dv_free = [](void* p) { delete static_cast<S*>(p); };
     }
@@ -1517,5 +1804,22 @@ extern "C" int bg_kset_davidson_solve(bg_kset* ks, const double* const* start, c
     rc = solve(static_cast<KsetSolver<std::complex<double>>*>(nullptr));
   ks->launches += launches;
   if (rc != BG_OK) return fail(ctx, rc, err.empty() ? "reference Davidson failed" : err);
+  return BG_OK;
+}
+
+extern "C" int bg_reduced_eigh(bg_ctx* ctx, int64_t m, int32_t is_complex, const double* s, const double* h,
+                               double* eigenvalues, double* vectors, double* device_ms) {
+  if (!ctx) return fail(nullptr, BG_EINVAL, "null context");
+  if (!s || !h || !eigenvalues || !vectors) return fail(ctx, BG_EINVAL, "null argument");
+  if (m < 1 || m > 1536) return fail(ctx, BG_ESHAPE, "reduced problem size must be in [1, 1536]");
+  const size_t n = (size_t)m * m * (is_complex ? 2 : 1);
+  for (size_t i = 0; i < n; ++i)
+    if (!std::isfinite(s[i]) || !std::isfinite(h[i])) return fail(ctx, BG_ENONFINITE, "non-finite pencil");
+  cudaError_t e = cudaSetDevice(ctx->device);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaSetDevice");
+  std::string err;
+  const int rc = is_complex ? reduced_eigh<double2>((int)m, s, h, eigenvalues, vectors, device_ms, &err)
+                            : reduced_eigh<double>((int)m, s, h, eigenvalues, vectors, device_ms, &err);
+  if (rc != BG_OK) return fail(ctx, rc, err);
   return BG_OK;
 }

@@ -1,0 +1,849 @@
+// Reduced problem of the batched Davidson on many thread blocks, for capacities beyond a
+// single control block (the Gamma-only supercells: capacity 2 x bands = 320 and 960).
+//
+// The algebra is that of the control kernel (kset_davidson.cu: chol_extend, eigen, heev),
+// crates/dft-numerics/src/linalg.rs:234-444 (bordered Cholesky, A = L^-1 H_r L^-H,
+// Hermitian eigensolver, C = L^-H Y) and crates/dft-solvers/src/lean_davidson.rs:62-70
+// (pivot rule), laid out over the whole GPU:
+//   * triangular solves: eight right-hand sides per block, staged in shared memory, the
+//     factor's columns streamed from L2 once per block (column sweep);
+//   * the new diagonal block of the bordered Cholesky factor: S22 - L21 L21^H by 16 x 16
+//     tiles, then a panel factorisation (32 columns; the panel by one block with the pivot
+//     rule, the rows below and the trailing lower triangle by every block) in one
+//     cooperative launch;
+//   * Householder tridiagonalisation: one cooperative launch, every block owning columns
+//     of the trailing matrix (matrix-vector product and rank-2 update) and rows of the
+//     accumulated unitary factor; two grid barriers per reflector;
+//   * tridiagonal eigenpairs: Sturm bisection by one warp per eigenvalue, inverse
+//     iteration by one thread per eigenvector, Gram-Schmidt inside clusters of close
+//     eigenvalues by one warp per cluster;
+//   * back-transformation Q diag(s) Z as a tiled product, then the back solve with L^H.
+// Requests come from the control kernel (Ctl::wc_* and Ctl::we_m); every kernel here
+// returns at once for a k point without one, so the launches sit in the captured
+// iteration graph at fixed shapes.  Grid barriers spin a bounded number of times and
+// then record kWErrBarrier and return (cooperative launches make every block resident,
+// so that does not happen in a healthy run).
+#pragma once
+
+namespace bg {
+namespace dv {
+namespace wide {
+
+constexpr int kT = 256;                 // threads per block
+constexpr int kSolveCols = 8;           // right-hand sides per block of a triangular solve
+constexpr int kPanel = 32;              // Cholesky panel width
+constexpr int kTile = 16;               // tiles of the border product
+constexpr double kWideOrtol = 1e-6;     // cluster gap relative to the block's 1-norm
+constexpr unsigned kSpinLimit = 1u << 24;
+
+enum : int { kWErrNonfinite = 1, kWErrBarrier = 2, kWErrPivot = 4 };
+enum : int { kSolveBorder = 0, kSolveLeft, kSolveRight, kSolveBack };
+
+// All blocks of a cooperative launch meet here; false once any barrier has given up.
+__device__ __forceinline__ bool grid_sync(unsigned* bar, int* err) {
+  __shared__ int s_ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int ok = 1;
+    if (*(volatile int*)err & kWErrBarrier) {
+      ok = 0;
+    } else {
+      volatile unsigned* vgen = bar + 1;
+      const unsigned gen = *vgen;
+      __threadfence();
+      const unsigned arrived = atomicAdd(bar, 1u);
+      if (arrived == gridDim.x - 1) {
+        atomicExch(bar, 0u);
+        __threadfence();
+        atomicAdd(bar + 1, 1u);
+      } else {
+        unsigned spins = 0;
+        while (*vgen == gen) {
+          if (++spins > kSpinLimit) {
+            atomicOr(err, kWErrBarrier);
+            ok = 0;
+            break;
+          }
+          __nanosleep(64);
+        }
+      }
+      __threadfence();
+    }
+    s_ok = ok;
+  }
+  __syncthreads();
+  return s_ok != 0;
+}
+
+// Loads that bypass L1 (data written by other blocks of a cooperative launch since the
+// last barrier must not come from a stale L1 line).
+__device__ __forceinline__ double ldcg(const double* p) { return __ldcg(p); }
+__device__ __forceinline__ double2 ldcg(const double2* p) { return __ldcg(p); }
+
+template <class D>
+__device__ __forceinline__ D warp_sum_d(D v) {
+  for (int o = 16; o > 0; o >>= 1) v = Cx<D>::add(v, Cx<D>::shfl_xor(v, o));
+  return v;
+}
+
+__device__ __forceinline__ double warp_sum_r(double v) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// ------------------------------------------------------------------ triangular solves
+// WHICH: kSolveBorder  T = L11^-1 S[0:m0, m0:m1], written as L[m0:m1, 0:m0] = T^H
+//        kSolveLeft    Y = L^-1 H_r                      (m columns)
+//        kSolveRight   A = L^-1 Y^H                      (= L^-1 H_r L^-H)
+//        kSolveBack    C = L^-H Y   (L^H from LT)
+// blockIdx.x = group of kSolveCols columns, blockIdx.y = k point.
+template <class D, int WHICH>
+__global__ void __launch_bounds__(kT) k_w_trsm(const Bufs<D>* __restrict__ bufs, const Ctl* __restrict__ ctl, int cap) {
+  using X = Cx<D>;
+  const int k = blockIdx.y;
+  const Bufs<D> b = bufs[k];
+  const Ctl c = ctl[k];
+  int m, ncols, col0 = 0;
+  if (WHICH == kSolveBorder) {
+    if (c.status != 0 || c.wc_m1 <= c.wc_m0 || c.wc_m0 == 0) return;
+    m = c.wc_m0;
+    ncols = c.wc_m1 - c.wc_m0;
+    col0 = c.wc_m0;
+  } else {
+    if (c.status != 0 || c.we_m == 0 || *(volatile int*)b.werr != 0) return;
+    m = c.we_m;
+    ncols = m;
+  }
+  const int j0 = blockIdx.x * kSolveCols;
+  if (j0 >= ncols) return;
+  const int nc = min(kSolveCols, ncols - j0);
+  extern __shared__ __align__(16) unsigned char w_sm[];
+  D* y = reinterpret_cast<D*>(w_sm);                        // [kSolveCols][cap]
+  double* rd = reinterpret_cast<double*>(y + (size_t)kSolveCols * cap);
+  const D* L = WHICH == kSolveBack ? b.LT : b.L;
+  for (int t = threadIdx.x; t < nc * m; t += kT) {
+    const int j = t / m, r = t - j * m;
+    const int cj = col0 + j0 + j;
+    D v;
+    if (WHICH == kSolveBorder) v = b.S[r + (size_t)cj * cap];
+    else if (WHICH == kSolveLeft) v = b.Hr[r + (size_t)cj * cap];
+    else if (WHICH == kSolveRight) v = X::conj(b.Y[cj + (size_t)r * cap]);
+    else v = b.Y[r + (size_t)cj * cap];
+    y[(size_t)j * cap + r] = v;
+  }
+  for (int r = threadIdx.x; r < m; r += kT) rd[r] = 1.0 / X::real(L[r + (size_t)r * cap]);
+  __syncthreads();
+  if (WHICH != kSolveBack) {
+    for (int p = 0; p < m; ++p) {
+      if ((int)threadIdx.x < nc) y[(size_t)threadIdx.x * cap + p] = X::scale(rd[p], y[(size_t)threadIdx.x * cap + p]);
+      __syncthreads();
+      const D* lc = L + (size_t)p * cap;
+      for (int r = p + 1 + threadIdx.x; r < m; r += kT) {
+        const D l = lc[r];
+        for (int j = 0; j < nc; ++j) y[(size_t)j * cap + r] = X::sub(y[(size_t)j * cap + r], X::mul(l, y[(size_t)j * cap + p]));
+      }
+      __syncthreads();
+    }
+  } else {
+    for (int p = m - 1; p >= 0; --p) {
+      if ((int)threadIdx.x < nc) y[(size_t)threadIdx.x * cap + p] = X::scale(rd[p], y[(size_t)threadIdx.x * cap + p]);
+      __syncthreads();
+      const D* lc = L + (size_t)p * cap;   // LT column p = conj of L's row p
+      for (int r = threadIdx.x; r < p; r += kT) {
+        const D l = lc[r];
+        for (int j = 0; j < nc; ++j) y[(size_t)j * cap + r] = X::sub(y[(size_t)j * cap + r], X::mul(l, y[(size_t)j * cap + p]));
+      }
+      __syncthreads();
+    }
+  }
+  for (int t = threadIdx.x; t < nc * m; t += kT) {
+    const int j = t / m, r = t - j * m;
+    const int cj = col0 + j0 + j;
+    const D v = y[(size_t)j * cap + r];
+    if (WHICH == kSolveBorder) b.L[cj + (size_t)r * cap] = X::conj(v);
+    else if (WHICH == kSolveLeft) b.Y[r + (size_t)cj * cap] = v;
+    else if (WHICH == kSolveRight) b.A[r + (size_t)cj * cap] = v;
+    else b.C[r + (size_t)cj * cap] = v;
+  }
+}
+
+inline size_t trsm_smem(int cap, size_t dsize) { return (size_t)kSolveCols * cap * dsize + (size_t)cap * sizeof(double); }
+
+// ------------------------------------------------------------------ bordered Cholesky
+// L[m0:m1, m0:m1] (lower) = S22 - L21 L21^H, zero above the diagonal; 16 x 16 tiles.
+template <class D>
+__global__ void __launch_bounds__(kTile* kTile) k_w_border(const Bufs<D>* __restrict__ bufs, const Ctl* __restrict__ ctl,
+                                                          int cap) {
+  using X = Cx<D>;
+  const int k = blockIdx.y;
+  const Ctl c = ctl[k];
+  if (c.status != 0 || c.wc_m1 <= c.wc_m0) return;
+  const Bufs<D> b = bufs[k];
+  const int m0 = c.wc_m0, nr = c.wc_m1 - c.wc_m0;
+  const int tiles = (nr + kTile - 1) / kTile;
+  if ((int)blockIdx.x >= tiles * tiles) return;
+  const int ti = blockIdx.x % tiles, tj = blockIdx.x / tiles;
+  if (tj > ti) {  // strictly above the diagonal: zeros
+    const int i = m0 + ti * kTile + threadIdx.x % kTile, j = m0 + tj * kTile + threadIdx.x / kTile;
+    if (i < c.wc_m1 && j < c.wc_m1) b.L[i + (size_t)j * cap] = X::zero();
+    return;
+  }
+  __shared__ D a[kTile][kTile + 1], bt[kTile][kTile + 1];
+  const int tx = threadIdx.x % kTile, ty = threadIdx.x / kTile;
+  const int i = m0 + ti * kTile + tx, j = m0 + tj * kTile + ty;
+  D acc = X::zero();
+  for (int p0 = 0; p0 < m0; p0 += kTile) {
+    // a[q][x] = L[i0 + x][p0 + q], bt[q][y] = L[j0 + y][p0 + q]
+    {
+      const int q = ty, p = p0 + q;
+      const int ia = m0 + ti * kTile + tx, jb = m0 + tj * kTile + tx;
+      a[q][tx] = (p < m0 && ia < c.wc_m1) ? b.L[ia + (size_t)p * cap] : X::zero();
+      bt[q][tx] = (p < m0 && jb < c.wc_m1) ? b.L[jb + (size_t)p * cap] : X::zero();
+    }
+    __syncthreads();
+#pragma unroll 4
+    for (int q = 0; q < kTile; ++q) acc = X::add(acc, X::mul(a[q][tx], X::conj(bt[q][ty])));
+    __syncthreads();
+  }
+  if (i < c.wc_m1 && j < c.wc_m1) b.L[i + (size_t)j * cap] = j <= i ? X::sub(b.S[i + (size_t)j * cap], acc) : X::zero();
+}
+
+// Factor the new diagonal block in place (panels of kPanel columns), the pivot rule on
+// every column: squared pivot over the overlap diagonal >= eps / 1e-12.  Cooperative.
+template <class D>
+__global__ void __launch_bounds__(kT) k_w_chol(const Bufs<D>* __restrict__ bufs, const Ctl* __restrict__ ctl, int nk,
+                                               int cap, unsigned* bar) {
+  using X = Cx<D>;
+  __shared__ D blk[kPanel][kPanel + 1];
+  __shared__ int s_fail;
+  const int gtid = blockIdx.x * kT + threadIdx.x, gthreads = gridDim.x * kT;
+  for (int k = 0; k < nk; ++k) {
+    const Ctl c = ctl[k];
+    if (c.status != 0 || c.wc_m1 <= c.wc_m0) continue;
+    const Bufs<D> b = bufs[k];
+    const int m0 = c.wc_m0, m1 = c.wc_m1;
+    for (int t = gtid; t < m0 * (m1 - m0); t += gthreads)  // above the new block
+      b.L[t % m0 + (size_t)(m0 + t / m0) * cap] = X::zero();
+    for (int p0 = m0; p0 < m1; p0 += kPanel) {
+      const int nb = min(kPanel, m1 - p0);
+      if (blockIdx.x == 0) {
+        for (int t = threadIdx.x; t < nb * nb; t += kT) {
+          const int i = t % nb, j = t / nb;
+          blk[i][j] = j <= i ? ldcg(b.L + (p0 + i) + (size_t)(p0 + j) * cap) : X::zero();
+        }
+        if (threadIdx.x == 0) s_fail = 0;
+        __syncthreads();
+        for (int j = 0; j < nb; ++j) {
+          const double dj = X::real(blk[j][j]);
+          const double ratio = dj / X::real(b.S[(p0 + j) + (size_t)(p0 + j) * cap]);
+          if (!(ratio >= kPivotRatioMin) || !isfinite(ratio)) {
+            if (threadIdx.x == 0) s_fail = 1;
+            break;  // uniform: every thread read the same pivot
+          }
+          const double ljj = sqrt(dj), inv = 1.0 / ljj;
+          __syncthreads();
+          if (threadIdx.x == 0) blk[j][j] = X::from_real(ljj);
+          for (int i = j + 1 + threadIdx.x; i < nb; i += kT) blk[i][j] = X::scale(inv, blk[i][j]);
+          __syncthreads();
+          const int rest = nb - j - 1;
+          for (int t = threadIdx.x; t < rest * rest; t += kT) {
+            const int i = j + 1 + t % rest, q = j + 1 + t / rest;
+            if (q <= i) blk[i][q] = X::sub(blk[i][q], X::mul(blk[i][j], X::conj(blk[q][j])));
+          }
+          __syncthreads();
+        }
+        __syncthreads();
+        for (int t = threadIdx.x; t < nb * nb; t += kT) {
+          const int i = t % nb, j = t / nb;
+          b.L[(p0 + i) + (size_t)(p0 + j) * cap] = j <= i ? blk[i][j] : X::zero();
+        }
+        if (threadIdx.x == 0 && s_fail) atomicOr(b.werr, kWErrPivot);
+      }
+      if (!grid_sync(bar, b.werr)) return;
+      if (*(volatile int*)b.werr & kWErrPivot) break;  // uniform after the barrier
+      // rows below the panel: L[i, p0:p0+nb] = A[i, p0:p0+nb] L_pp^-H
+      for (int i = p0 + nb + gtid; i < m1; i += gthreads) {
+        D r[kPanel];
+#pragma unroll
+        for (int q = 0; q < kPanel; ++q) r[q] = q < nb ? ldcg(b.L + i + (size_t)(p0 + q) * cap) : X::zero();
+#pragma unroll
+        for (int q = 0; q < kPanel; ++q) {
+          if (q < nb) {
+            D v = r[q];
+            for (int t = 0; t < q; ++t) v = X::sub(v, X::mul(r[t], X::conj(ldcg(b.L + (p0 + q) + (size_t)(p0 + t) * cap))));
+            r[q] = X::div(v, X::real(ldcg(b.L + (p0 + q) + (size_t)(p0 + q) * cap)));
+          }
+        }
+#pragma unroll
+        for (int q = 0; q < kPanel; ++q)
+          if (q < nb) b.L[i + (size_t)(p0 + q) * cap] = r[q];
+      }
+      if (!grid_sync(bar, b.werr)) return;
+      // trailing lower triangle
+      const int s0 = p0 + nb, R = m1 - s0;
+      for (int t = gtid; t < R * R; t += gthreads) {
+        const int i = s0 + t % R, j = s0 + t / R;
+        if (j > i) continue;
+        D acc = ldcg(b.L + i + (size_t)j * cap);
+        for (int q = 0; q < nb; ++q)
+          acc = X::sub(acc, X::mul(ldcg(b.L + i + (size_t)(p0 + q) * cap), X::conj(ldcg(b.L + j + (size_t)(p0 + q) * cap))));
+        b.L[i + (size_t)j * cap] = acc;
+      }
+      if (!grid_sync(bar, b.werr)) return;
+    }
+  }
+}
+
+// ------------------------------------------------------------------ eigensolver
+// Finite check, symmetrised rounding of A, Q = I (stored transposed), Z = 0.
+template <class D>
+__global__ void k_w_prep(const Bufs<D>* __restrict__ bufs, const Ctl* __restrict__ ctl, int cap) {
+  using X = Cx<D>;
+  const int k = blockIdx.y;
+  const Ctl c = ctl[k];
+  const Bufs<D> b = bufs[k];
+  if (c.status != 0 || c.we_m == 0 || *(volatile int*)b.werr != 0) return;
+  const int m = c.we_m;
+  int bad = 0;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < m * m; t += gridDim.x * blockDim.x) {
+    const int i = t % m, j = t / m;
+    bad |= !X::finite(b.A[i + (size_t)j * cap]);
+    if (i == j) {
+      b.A[i + (size_t)i * cap] = X::from_real(X::real(b.A[i + (size_t)i * cap]));
+    } else if (i > j) {
+      const D avg = X::scale(0.5, X::add(b.A[i + (size_t)j * cap], X::conj(b.A[j + (size_t)i * cap])));
+      b.A[i + (size_t)j * cap] = avg;
+      b.A[j + (size_t)i * cap] = X::conj(avg);
+    }
+    b.Q[i + (size_t)j * cap] = i == j ? X::one() : X::zero();
+    b.Z[i + (size_t)j * cap] = 0.0;
+  }
+  if (bad) atomicOr(b.werr, kWErrNonfinite);
+}
+
+// Householder reduction of the m x m Hermitian A to tridiagonal form; Q <- Q H_k.  Every
+// block owns columns (of the trailing matrix, one warp per column) and rows of Q.
+// Cooperative; shared memory: v and q (cap values each) and the block's partial sums.
+template <class D>
+__global__ void __launch_bounds__(kT) k_w_house(const Bufs<D>* __restrict__ bufs, const Ctl* __restrict__ ctl, int nk,
+                                                int cap, unsigned* bar, double* part) {
+  using X = Cx<D>;
+  extern __shared__ __align__(16) unsigned char w_sm[];
+  D* v = reinterpret_cast<D*>(w_sm);
+  D* q = v + cap;
+  __shared__ double red[kT / 32];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = kT / 32;
+  const int gw = blockIdx.x * nw + warp, gwarps = gridDim.x * nw;
+  for (int kk = 0; kk < nk; ++kk) {
+    const Ctl c = ctl[kk];
+    const Bufs<D> b = bufs[kk];
+    if (c.status != 0 || c.we_m == 0 || *(volatile int*)b.werr != 0) continue;   // uniform: set before this launch
+    const int m = c.we_m;
+    D* A = b.A;
+    for (int col = 0; col + 2 < m; ++col) {
+      const int L = m - col - 1;
+      const D* x = A + (col + 1) + (size_t)col * cap;
+      double part2 = 0.0;
+      for (int i = threadIdx.x; i < L; i += kT) {
+        const D xi = ldcg(x + i);
+        v[i] = xi;
+        part2 += X::abs2(xi);
+      }
+      part2 = warp_sum_r(part2);
+      if (lane == 0) red[warp] = part2;
+      __syncthreads();
+      double xn2 = 0.0;
+      for (int i = 0; i < nw; ++i) xn2 += red[i];
+      const double xn = sqrt(xn2);
+      if (xn == 0.0) {  // nothing to reflect; every block saw the same column
+        if (blockIdx.x == 0 && threadIdx.x == 0) b.off[col] = X::zero();
+        __syncthreads();
+        continue;
+      }
+      const D x0 = v[0];
+      const double ax0 = X::abs(x0);
+      const D phase = ax0 > 0.0 ? X::div(x0, ax0) : X::one();
+      const D alpha = X::scale(-xn, phase);
+      const double beta = 1.0 / (xn * (xn + ax0));
+      __syncthreads();
+      if (threadIdx.x == 0) v[0] = X::sub(x0, alpha);
+      __syncthreads();
+      // p_i = beta sum_j conj(B[j][i]) v_j, B = A[col+1:, col+1:]; warp gw owns the global
+      // columns g = gw (mod gwarps), so a column is always read and written by one warp
+      double pv = 0.0;
+      for (int g = gw; g < m; g += gwarps) {
+        if (g <= col) continue;
+        const int i = g - col - 1;
+        const D* ci = A + (col + 1) + (size_t)g * cap;
+        D acc = X::zero();
+        for (int j = lane; j < L; j += 32) acc = X::add(acc, X::mul(X::conj(ci[j]), v[j]));
+        acc = warp_sum_d(acc);
+        const D pi = X::scale(beta, acc);
+        if (lane == 0) {
+          b.hp[i] = pi;
+          pv += X::dot_re(v[i], pi);
+        }
+      }
+      pv = warp_sum_r(pv);
+      __syncthreads();
+      if (lane == 0) red[warp] = pv;
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        double sum = 0.0;
+        for (int i = 0; i < nw; ++i) sum += red[i];
+        part[blockIdx.x] = sum;
+      }
+      if (!grid_sync(bar, b.werr)) return;
+      double vp = 0.0;
+      for (int i = 0; i < (int)gridDim.x; ++i) vp += ldcg(part + i);
+      const double K = 0.5 * beta * vp;
+      for (int i = threadIdx.x; i < L; i += kT) q[i] = X::sub(ldcg(b.hp + i), X::scale(K, v[i]));
+      __syncthreads();
+      // B[:, i] -= v conj(q_i) + q conj(v_i) for the owned columns
+      for (int g = gw; g < m; g += gwarps) {
+        if (g <= col) continue;
+        const int i = g - col - 1;
+        D* ci = A + (col + 1) + (size_t)g * cap;
+        const D cq = X::conj(q[i]), cv = X::conj(v[i]);
+        for (int j = lane; j < L; j += 32) ci[j] = X::sub(ci[j], X::add(X::mul(v[j], cq), X::mul(q[j], cv)));
+      }
+      // Q rows (transposed storage: row r at Q + r cap): row <- row - beta (row . v) v^H
+      for (int r = gw; r < m; r += gwarps) {
+        D* row = b.Q + (col + 1) + (size_t)r * cap;
+        D acc = X::zero();
+        for (int j = lane; j < L; j += 32) acc = X::add(acc, X::mul(row[j], v[j]));
+        acc = X::scale(beta, warp_sum_d(acc));
+        for (int j = lane; j < L; j += 32) row[j] = X::sub(row[j], X::mul(acc, X::conj(v[j])));
+      }
+      if (blockIdx.x == 0 && threadIdx.x == 0) b.off[col] = alpha;
+      if (!grid_sync(bar, b.werr)) return;
+    }
+  }
+}
+
+inline size_t house_smem(int cap, size_t dsize) { return 2 * (size_t)cap * dsize; }
+
+// Tridiagonal data: d, |e|, phases s (so that T = diag(s)^H T_c diag(s) is real), splits
+// where a coupling is negligible, squared couplings, the pivmin safeguard.  One block per k.
+template <class D>
+__global__ void k_w_tri_setup(const Bufs<D>* __restrict__ bufs, const Ctl* __restrict__ ctl, int cap) {
+  using X = Cx<D>;
+  const int k = blockIdx.y;
+  const Ctl c = ctl[k];
+  const Bufs<D> b = bufs[k];
+  if (c.status != 0 || c.we_m == 0 || *(volatile int*)b.werr != 0) return;
+  const int m = c.we_m;
+  for (int i = threadIdx.x; i < m; i += blockDim.x) b.td[i] = X::real(b.A[i + (size_t)i * cap]);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    if (m >= 2) b.off[m - 2] = b.A[(m - 1) + (size_t)(m - 2) * cap];
+    D s = X::one();
+    b.ph[0] = s;
+    for (int i = 0; i + 1 < m; ++i) {
+      const double a = X::abs(b.off[i]);
+      b.te[i] = a;
+      s = a > 0.0 ? X::mul(s, X::div(b.off[i], a)) : s;
+      b.ph[i + 1] = s;
+    }
+    b.te[m - 1] = 0.0;
+    int nb = 0;
+    b.starts[nb++] = 0;
+    double e2max = 1.0;
+    for (int i = 0; i + 1 < m; ++i) {
+      if (fabs(b.te[i]) <= tri::kUlp * (fabs(b.td[i]) + fabs(b.td[i + 1]))) {
+        b.e2[i] = 0.0;
+        b.starts[nb++] = i + 1;
+      } else {
+        b.e2[i] = b.te[i] * b.te[i];
+        e2max = fmax(e2max, b.e2[i]);
+      }
+    }
+    b.starts[nb] = m;
+    b.wimeta[0] = nb;
+    b.wmeta[0] = tri::kSafeMin * e2max;  // pivmin
+  }
+}
+
+// Eigenvalues by Sturm bisection: one warp per eigenvalue, two shifts per lane per round.
+template <class D>
+__global__ void __launch_bounds__(kT) k_w_tri_values(const Bufs<D>* __restrict__ bufs, const Ctl* __restrict__ ctl) {
+  const int k = blockIdx.y;
+  const Ctl c = ctl[k];
+  const Bufs<D> b = bufs[k];
+  if (c.status != 0 || c.we_m == 0 || *(volatile int*)b.werr != 0) return;
+  const int m = c.we_m;
+  const int j = blockIdx.x * (kT / 32) + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+  if (j >= m) return;
+  const int nb = b.wimeta[0];
+  const double pivmin = b.wmeta[0];
+  const double* d = b.td;
+  const double* e = b.te;
+  const int bi = tri::block_of(b.starts, nb, j);
+  const int s = b.starts[bi], n = b.starts[bi + 1] - s, i = j - s;
+  double lo, hi, nrm;
+  tri::gershgorin(d, e, s, n, pivmin, &lo, &hi, &nrm);
+  constexpr int kShifts = 2, K = 2 * 32;
+  const double atol = tri::kUlp * nrm + 2.0 * pivmin;
+  for (int it = 0; it < tri::kMaxRounds; ++it) {
+    if (hi - lo <= 2.0 * tri::kUlp * fmax(fabs(lo), fabs(hi)) + atol) break;  // uniform in the warp
+    const double h = (hi - lo) / (K + 1);
+    const int r0 = kShifts * lane;
+    double xs[kShifts];
+    int cs[kShifts];
+#pragma unroll
+    for (int q = 0; q < kShifts; ++q) xs[q] = lo + (r0 + q + 1) * h;
+    tri::sturm<kShifts>(d, b.e2, s, n, xs, cs);
+    int rf = K;
+#pragma unroll
+    for (int q = kShifts - 1; q >= 0; --q)
+      if (cs[q] > i) rf = r0 + q;
+    for (int o = 16; o > 0; o >>= 1) rf = min(rf, __shfl_xor_sync(0xffffffffu, rf, o));
+    const double nlo = rf > 0 ? lo + rf * h : lo;
+    const double nhi = rf < K ? lo + (rf + 1) * h : hi;
+    lo = nlo;
+    hi = nhi;
+  }
+  if (lane == 0) b.wu[j] = 0.5 * (lo + hi);
+}
+
+// Clusters (consecutive eigenvalues of one block closer than kWideOrtol |T_b|_1), the
+// ascending order of all eigenvalues and w in that order.  One block per k.
+template <class D>
+__global__ void k_w_tri_clusters(const Bufs<D>* __restrict__ bufs, const Ctl* __restrict__ ctl) {
+  const int k = blockIdx.y;
+  const Ctl c = ctl[k];
+  const Bufs<D> b = bufs[k];
+  if (c.status != 0 || c.we_m == 0 || *(volatile int*)b.werr != 0) return;
+  const int m = c.we_m;
+  const int nb = b.wimeta[0];
+  const double pivmin = b.wmeta[0];
+  if (threadIdx.x == 0) {
+    int nc = 0;
+    for (int bi = 0; bi < nb; ++bi) {
+      const int s = b.starts[bi], n = b.starts[bi + 1] - s;
+      double gl, gu, nrm;
+      tri::gershgorin(b.td, b.te, s, n, pivmin, &gl, &gu, &nrm);
+      const double ortol = kWideOrtol * nrm;
+      b.clusters[nc++] = s;
+      for (int j = s + 1; j < s + n; ++j)
+        if (b.wu[j] - b.wu[j - 1] > ortol) b.clusters[nc++] = j;
+    }
+    b.clusters[nc] = m;
+    b.wimeta[1] = nc;
+  }
+  for (int i = threadIdx.x; i < m; i += blockDim.x) {
+    int rank = 0;
+    const double di = b.wu[i];
+    for (int j = 0; j < m; ++j) rank += (b.wu[j] < di) || (b.wu[j] == di && j < i);
+    b.order[rank] = i;
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < m; i += blockDim.x) b.w[i] = b.wu[b.order[i]];
+}
+
+// Inverse iteration, one thread per eigenvector (tri::eig step 4 with the LU strips in
+// global memory, strip entry r of thread j at lu[r cap + j]).  Z[r cap + j].
+template <class D>
+__global__ void __launch_bounds__(64) k_w_tri_vectors(const Bufs<D>* __restrict__ bufs, const Ctl* __restrict__ ctl,
+                                                      int cap) {
+  const int k = blockIdx.y;
+  const Ctl c = ctl[k];
+  const Bufs<D> b = bufs[k];
+  if (c.status != 0 || c.we_m == 0 || *(volatile int*)b.werr != 0) return;
+  const int m = c.we_m;
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= m) return;
+  const int nb = b.wimeta[0];
+  const double pivmin = b.wmeta[0];
+  const double* d = b.td;
+  const double* e = b.te;
+  const double* wu = b.wu;
+  double* Z = b.Z;
+  const int ldz = cap;
+  const int bi = tri::block_of(b.starts, nb, j);
+  const int s = b.starts[bi], n = b.starts[bi + 1] - s;
+  if (n == 1) {
+    Z[(size_t)s * ldz + j] = 1.0;
+    return;
+  }
+  double gl, gu, onenrm;
+  tri::gershgorin(d, e, s, n, pivmin, &gl, &gu, &onenrm);
+  const double pertol = 10.0 * tri::kUlp * onenrm, tiny = tri::kUlp * onenrm;
+  const double dtpcrt = sqrt(0.1 / n);
+  const size_t ps = (size_t)cap;
+  double* ur = b.lu + j;
+  double* u1 = ur + (size_t)cap * cap;
+  double* u2 = u1 + (size_t)cap * cap;
+  double* lm = u2 + (size_t)cap * cap;
+  int jr = j;
+  while (jr > s && wu[jr] - wu[jr - 1] < pertol) --jr;
+  const double x = wu[j] + (j - jr) * pertol;
+  double ai = d[s] - x, bi_ = e[s], ulast = 0.0;
+  bool last_swap = false;
+  for (int r = 0; r + 1 < n; ++r) {
+    const double ci = e[s + r], an = d[s + r + 1] - x, bn = r + 2 < n ? e[s + r + 1] : 0.0;
+    double l, piv;
+    if (fabs(ai) >= fabs(ci)) {
+      l = ai != 0.0 ? ci / ai : 0.0;
+      piv = ai;
+      u1[r * ps] = bi_;
+      u2[r * ps] = 0.0;
+      ai = an - l * bi_;
+      bi_ = bn;
+    } else {
+      l = ai / ci;
+      piv = ci;
+      u1[r * ps] = an;
+      u2[r * ps] = bn;
+      ai = bi_ - l * an;
+      bi_ = -l * bn;
+      if (r + 2 == n) last_swap = true;
+    }
+    if (fabs(piv) < tiny) piv = piv < 0.0 ? -tiny : tiny;
+    ur[r * ps] = 1.0 / piv;
+    lm[r * ps] = l;
+  }
+  if (fabs(ai) < tiny) ai = ai < 0.0 ? -tiny : tiny;
+  ulast = fabs(ai);
+  ur[(size_t)(n - 1) * ps] = 1.0 / ai;
+  double* zc = Z + (size_t)s * ldz + j;
+  auto z = [&](int r) -> double& { return zc[(size_t)r * ldz]; };
+  double asum = 0.0;
+  for (int r = 0; r < n; ++r) {
+    const double v = tri::start_entry(j, r);
+    z(r) = v;
+    asum += fabs(v);
+  }
+  int checks = 0;
+  for (int its = 0; its < tri::kInverseIterations; ++its) {
+    const double scl = n * onenrm * fmax(tri::kUlp, ulast) / asum;
+    double zr = z(0) * scl;
+    for (int r = 0; r + 1 < n; ++r) {
+      double zn = z(r + 1) * scl;
+      const bool sw = r + 2 < n ? u2[r * ps] != 0.0 : last_swap;
+      if (sw) {
+        const double t = zr;
+        zr = zn;
+        zn = t;
+      }
+      z(r) = zr;
+      zr = zn - lm[r * ps] * zr;
+    }
+    double z1 = zr * ur[(size_t)(n - 1) * ps];
+    z(n - 1) = z1;
+    double z0 = (z(n - 2) - u1[(size_t)(n - 2) * ps] * z1) * ur[(size_t)(n - 2) * ps];
+    z(n - 2) = z0;
+    double zmax = fmax(fabs(z1), fabs(z0));
+    asum = fabs(z1) + fabs(z0);
+    for (int r = n - 3; r >= 0; --r) {
+      const double v = (z(r) - u1[r * ps] * z0 - u2[r * ps] * z1) * ur[r * ps];
+      z(r) = v;
+      z1 = z0;
+      z0 = v;
+      zmax = fmax(zmax, fabs(v));
+      asum += fabs(v);
+    }
+    if (zmax >= dtpcrt && ++checks > tri::kExtraIterations) break;
+  }
+  double nn = 0.0;
+  for (int r = 0; r < n; ++r) nn += z(r) * z(r);
+  const double inv = 1.0 / sqrt(nn);
+  for (int r = 0; r < n; ++r) z(r) *= inv;
+}
+
+// Each cluster's vectors orthonormalised in order (Gram-Schmidt twice) and every vector's
+// largest entry made positive: one warp per cluster.
+template <class D>
+__global__ void __launch_bounds__(kT) k_w_tri_gs(const Bufs<D>* __restrict__ bufs, const Ctl* __restrict__ ctl, int cap) {
+  const int k = blockIdx.y;
+  const Ctl c = ctl[k];
+  const Bufs<D> b = bufs[k];
+  if (c.status != 0 || c.we_m == 0 || *(volatile int*)b.werr != 0) return;
+  const int cidx = blockIdx.x * (kT / 32) + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+  const int nc = b.wimeta[1], nb = b.wimeta[0];
+  if (cidx >= nc) return;
+  const int ldz = cap;
+  const int ja = b.clusters[cidx], jb = b.clusters[cidx + 1];
+  const int bi = tri::block_of(b.starts, nb, ja);
+  const int s = b.starts[bi], n = b.starts[bi + 1] - s;
+  const double* zb = b.Z + (size_t)s * ldz;
+  for (int j = ja; j < jb; ++j) {
+    double* zc = b.Z + (size_t)s * ldz + j;
+    for (int pass = 0; pass < 2 && j > ja; ++pass) {
+      for (int qv = ja; qv < j; ++qv) {
+        double dot = 0.0;
+        for (int r = lane; r < n; r += 32) dot = fma(zc[(size_t)r * ldz], zb[(size_t)r * ldz + qv], dot);
+        dot = warp_sum_r(dot);
+        for (int r = lane; r < n; r += 32) zc[(size_t)r * ldz] = fma(-dot, zb[(size_t)r * ldz + qv], zc[(size_t)r * ldz]);
+        __syncwarp();
+      }
+      double nn = 0.0;
+      for (int r = lane; r < n; r += 32) nn = fma(zc[(size_t)r * ldz], zc[(size_t)r * ldz], nn);
+      nn = warp_sum_r(nn);
+      const double inv = 1.0 / sqrt(nn);
+      for (int r = lane; r < n; r += 32) zc[(size_t)r * ldz] *= inv;
+      __syncwarp();
+    }
+    double big = -1.0;
+    int at = n;
+    for (int r = lane; r < n; r += 32) {
+      const double v = fabs(zc[(size_t)r * ldz]);
+      if (v > big) {
+        big = v;
+        at = r;
+      }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      const double ob = __shfl_xor_sync(0xffffffffu, big, o);
+      const int oa = __shfl_xor_sync(0xffffffffu, at, o);
+      if (ob > big || (ob == big && oa < at)) {
+        big = ob;
+        at = oa;
+      }
+    }
+    const bool neg = zc[(size_t)at * ldz] < 0.0;
+    __syncwarp();
+    if (neg)
+      for (int r = lane; r < n; r += 32) zc[(size_t)r * ldz] = -zc[(size_t)r * ldz];
+    __syncwarp();
+  }
+}
+
+// Y[r][c] = sum_q Q(r, q) s_q Z[q][order[c]] (r, c < m); 32 x 32 output tiles, q in
+// steps of 16 staged in shared memory.  Q is stored transposed (Q(r, q) at Q[q + r cap]).
+template <class D>
+__global__ void __launch_bounds__(kT) k_w_back(const Bufs<D>* __restrict__ bufs, const Ctl* __restrict__ ctl, int cap) {
+  using X = Cx<D>;
+  const int k = blockIdx.z;
+  const Ctl c = ctl[k];
+  const Bufs<D> b = bufs[k];
+  if (c.status != 0 || c.we_m == 0 || *(volatile int*)b.werr != 0) return;
+  const int m = c.we_m;
+  const int r0 = blockIdx.x * 32, c0 = blockIdx.y * 32;
+  if (r0 >= m || c0 >= m) return;
+  __shared__ D qs[32][17];
+  __shared__ D zs[16][33];
+  __shared__ int ord[32];
+  if (threadIdx.x < 32) ord[threadIdx.x] = c0 + threadIdx.x < m ? b.order[c0 + threadIdx.x] : 0;
+  const int tr = threadIdx.x % 32, tc = threadIdx.x / 32;  // rows tr, columns tc + 8 u
+  D acc[4] = {X::zero(), X::zero(), X::zero(), X::zero()};
+  __syncthreads();
+  for (int q0 = 0; q0 < m; q0 += 16) {
+    for (int t = threadIdx.x; t < 32 * 16; t += kT) {
+      const int rr = t / 16, qq = t % 16;
+      const int r = r0 + rr, q = q0 + qq;
+      qs[rr][qq] = (r < m && q < m) ? b.Q[q + (size_t)r * cap] : X::zero();
+    }
+    for (int t = threadIdx.x; t < 16 * 32; t += kT) {
+      const int qq = t / 32, cc = t % 32;
+      const int q = q0 + qq, col = c0 + cc;
+      zs[qq][cc] = (q < m && col < m) ? X::scale(b.Z[(size_t)q * cap + ord[cc]], b.ph[q]) : X::zero();
+    }
+    __syncthreads();
+#pragma unroll 4
+    for (int qq = 0; qq < 16; ++qq) {
+      const D a = qs[tr][qq];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) acc[u] = X::add(acc[u], X::mul(a, zs[qq][tc + 8 * u]));
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int u = 0; u < 4; ++u) {
+    const int r = r0 + tr, col = c0 + tc + 8 * u;
+    if (r < m && col < m) b.Y[r + (size_t)col * cap] = acc[u];
+  }
+}
+
+// LT = L^H (m x m).
+template <class D>
+__global__ void k_w_adjoint(const Bufs<D>* __restrict__ bufs, const Ctl* __restrict__ ctl, int cap) {
+  const int k = blockIdx.y;
+  const Ctl c = ctl[k];
+  const Bufs<D> b = bufs[k];
+  if (c.status != 0 || c.we_m == 0 || *(volatile int*)b.werr != 0) return;
+  const int m = c.we_m;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < m * m; t += gridDim.x * blockDim.x) {
+    const int i = t % m, j = t / m;
+    b.LT[i + (size_t)j * cap] = Cx<D>::conj(b.L[j + (size_t)i * cap]);
+  }
+}
+
+// ------------------------------------------------------------------ host side
+// Shared-memory limits of the kernels above 48 KB and the cooperative grid (one block per
+// SM, every one resident).
+template <class D>
+int prepare(int cap, int* coop_blocks, std::string* err) {
+  const int tsm = (int)trsm_smem(cap, sizeof(D));
+  cudaError_t e = cudaFuncSetAttribute((const void*)k_w_house<D>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)house_smem(cap, sizeof(D)));
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute((const void*)k_w_trsm<D, kSolveBorder>, cudaFuncAttributeMaxDynamicSharedMemorySize, tsm);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute((const void*)k_w_trsm<D, kSolveLeft>, cudaFuncAttributeMaxDynamicSharedMemorySize, tsm);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute((const void*)k_w_trsm<D, kSolveRight>, cudaFuncAttributeMaxDynamicSharedMemorySize, tsm);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute((const void*)k_w_trsm<D, kSolveBack>, cudaFuncAttributeMaxDynamicSharedMemorySize, tsm);
+  int dev = 0, sms = 0, occ_h = 0, occ_c = 0;
+  if (e == cudaSuccess) e = cudaGetDevice(&dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (e == cudaSuccess)
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_h, k_w_house<D>, kT, house_smem(cap, sizeof(D)));
+  if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_c, k_w_chol<D>, kT, 0);
+  if (e != cudaSuccess) {
+    *err = std::string("many-block reduced problem: ") + cudaGetErrorString(e);
+    return BG_EDEVICE;
+  }
+  if (occ_h < 1 || occ_c < 1 || sms < 1) {
+    *err = "the many-block reduced problem cannot place its blocks";
+    return BG_EDEVICE;
+  }
+  *coop_blocks = sms;
+  return BG_OK;
+}
+
+template <class... A>
+void coop_launch(void (*f)(A...), int blocks, size_t smem, cudaStream_t s, A... args) {
+  void* argv[] = {&args...};
+  cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(f), dim3((unsigned)blocks), dim3(kT), argv, smem, s);
+}
+
+// Extension of the factor for every k point with a request (3 launches).
+template <class D>
+int64_t launch_chol(Bufs<D>* bufs, Ctl* ctl, int nk, int cap, int coop_blocks, unsigned* bar, cudaStream_t s) {
+  const dim3 gs((unsigned)((cap + kSolveCols - 1) / kSolveCols), (unsigned)nk);
+  k_w_trsm<D, kSolveBorder><<<gs, kT, trsm_smem(cap, sizeof(D)), s>>>(bufs, ctl, cap);
+  const unsigned tiles = (unsigned)((cap + kTile - 1) / kTile);
+  k_w_border<D><<<dim3(tiles * tiles, (unsigned)nk), kTile * kTile, 0, s>>>(bufs, ctl, cap);
+  coop_launch(k_w_chol<D>, coop_blocks, 0, s, (const Bufs<D>*)bufs, (const Ctl*)ctl, nk, cap, bar);
+  return 3;
+}
+
+// Reduced eigenproblem for every k point with a request (12 launches).
+template <class D>
+int64_t launch_eig(Bufs<D>* bufs, Ctl* ctl, int nk, int cap, int coop_blocks, unsigned* bar, double* part,
+                   cudaStream_t s) {
+  const size_t tsm = trsm_smem(cap, sizeof(D));
+  const dim3 gs((unsigned)((cap + kSolveCols - 1) / kSolveCols), (unsigned)nk);
+  const dim3 gw((unsigned)((cap + 7) / 8), (unsigned)nk);
+  k_w_trsm<D, kSolveLeft><<<gs, kT, tsm, s>>>(bufs, ctl, cap);
+  k_w_trsm<D, kSolveRight><<<gs, kT, tsm, s>>>(bufs, ctl, cap);
+  k_w_prep<D><<<dim3(256, (unsigned)nk), 256, 0, s>>>(bufs, ctl, cap);
+  coop_launch(k_w_house<D>, coop_blocks, house_smem(cap, sizeof(D)), s, (const Bufs<D>*)bufs, (const Ctl*)ctl, nk,
+              cap, bar, part);
+  k_w_tri_setup<D><<<dim3(1, (unsigned)nk), 256, 0, s>>>(bufs, ctl, cap);
+  k_w_tri_values<D><<<gw, kT, 0, s>>>(bufs, ctl);
+  k_w_tri_clusters<D><<<dim3(1, (unsigned)nk), 256, 0, s>>>(bufs, ctl);
+  k_w_tri_vectors<D><<<dim3((unsigned)((cap + 63) / 64), (unsigned)nk), 64, 0, s>>>(bufs, ctl, cap);
+  k_w_tri_gs<D><<<gw, kT, 0, s>>>(bufs, ctl, cap);
+  const unsigned t32 = (unsigned)((cap + 31) / 32);
+  k_w_back<D><<<dim3(t32, t32, (unsigned)nk), kT, 0, s>>>(bufs, ctl, cap);
+  k_w_adjoint<D><<<dim3(256, (unsigned)nk), 256, 0, s>>>(bufs, ctl, cap);
+  k_w_trsm<D, kSolveBack><<<gs, kT, tsm, s>>>(bufs, ctl, cap);
+  return 12;
+}
+
+}  // namespace wide
+}  // namespace dv
+}  // namespace bg

@@ -97,11 +97,40 @@ def solve(operator: _Operator, start: np.ndarray, hamiltonian_diagonal: np.ndarr
                     st.repairs, st.contractions, st.dropped, st.fallbacks)
 
 
-def solve_kset(kset, starts, diagonals, options: Options, graph: bool = True):
+REDUCED_FLAGS = {"auto": 0, "wide": 2, "block": 4}
+
+
+def reduced_eigh(s, h, ctx=None):
+    """All eigenpairs of the Hermitian pencil H C = S C diag(w) (m x m, m <= 1536) by the
+    many-block path of the batched Davidson's reduced problem (bg_reduced_eigh): Cholesky
+    of S with the reference's pivot rule, A = L^-1 H L^-H, Householder tridiagonalisation,
+    bisection and inverse iteration, C = L^-H Y.  Returns (w ascending, C, device ms)."""
+    from .hamiltonian import default_context
+    ctx = ctx or default_context()
+    h = np.asarray(h)
+    complex_ = np.iscomplexobj(h) or np.iscomplexobj(s)
+    dt = np.complex128 if complex_ else np.float64
+    hm = np.asfortranarray(h, dtype=dt)
+    sm = np.asfortranarray(s, dtype=dt)
+    m = hm.shape[0]
+    if hm.shape != (m, m) or sm.shape != (m, m):
+        raise SolverError(L.BG_ESHAPE, "square pencil expected")
+    w = np.zeros(m)
+    c = np.zeros((m, m), dtype=dt, order="F")
+    ms = ctypes.c_double()
+    rc = L.load().bg_reduced_eigh(ctx.handle, m, 1 if complex_ else 0, sm.ctypes.data,
+                                  hm.ctypes.data, w.ctypes.data, c.ctypes.data, ctypes.byref(ms))
+    if rc != L.BG_OK:
+        raise SolverError(rc, f"{L.CODE_NAMES.get(rc, rc)}: {L.last_error(ctx.handle)}")
+    return w, c, ms.value
+
+
+def solve_kset(kset, starts, diagonals, options: Options, graph: bool = True, reduced: str = "auto"):
     """The reference Davidson for every k point of a KPointSet at once
     (bg_kset_davidson_solve): each large product is one launch over all k points, the
     reduced problems and control decisions run on the GPU, and an iteration is one
-    replayed CUDA graph (graph=False launches the same kernels one by one).  starts /
+    replayed CUDA graph (graph=False launches the same kernels one by one; reduced "wide"
+    or "block" forces the many-block or the one-block reduced problem).  starts /
     diagonals: one (rows_k x bands) block and one rows_k diagonal per k point, numpy
     (host) or CUDA tensors (device; blocks shaped (bands, rows_k) row-major, the layout
     of apply_block).  Returns one Solution per k point, eigenvectors on the same side."""
@@ -136,7 +165,7 @@ def solve_kset(kset, starts, diagonals, options: Options, graph: bool = True):
     vals = [np.zeros(n) for _ in range(nk)]
     conv = [np.zeros(n, np.int32) for _ in range(nk)]
     stats = (L.DavidsonStats * nk)()
-    o = _options(options, 0 if graph else 1)
+    o = _options(options, (0 if graph else 1) | REDUCED_FLAGS[reduced])
     arr = lambda lst, f: (ctypes.c_void_p * nk)(*[f(a) for a in lst])
     host = lambda a: a.ctypes.data
     rc = lib.bg_kset_davidson_solve(kset.handle, arr(x0, ptr), arr(dg, ptr), ctypes.byref(o), kind, arr(vals, host),

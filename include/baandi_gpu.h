@@ -341,19 +341,36 @@ int bg_davidson_solve(bg_op* op, const double* start, const double* diagonal,
  * (the reference solves the k points of a map one after another,
  * crates/dft-engine/src/refscf/k_map.rs:136-210, each with ref_davidson_complex.rs:
  * 798-1082).  Every large product is one launch over all k points, the reduced problem
- * (bordered Cholesky, Householder tridiagonalisation, implicit QL) and the control
- * decisions (contraction, dropped corrections, repair, convergence) run in a
- * one-block-per-k-point kernel, and one iteration is a CUDA graph replayed until all k
- * points finish.  Per-k arrays (nk = set size): start[k] rows_k x bands, diagonal[k]
+ * (bordered Cholesky, Householder tridiagonalisation, tridiagonal eigenpairs) and the
+ * control decisions (contraction, dropped corrections, repair, convergence) run in a
+ * one-block-per-k-point kernel -- beyond capacity 128 the factor and the eigensolve run
+ * on many blocks (cooperative launches, bg_reduced_eigh) -- and one iteration is a CUDA
+ * graph replayed until all k points finish.  Per-k arrays (nk = set size): start[k] rows_k x bands, diagonal[k]
  * rows_k, eigenvalues[k] bands, eigenvectors[k] rows_k x bands, converged[k] bands;
  * start/diagonal/eigenvectors have ptr_kind (eigenvalues and converged are host);
  * stats: nk entries or NULL.  options.flags bit 0 set: launch the iteration's
- * kernels directly instead of replaying the graph (same results).  The Davidson
+ * kernels directly instead of replaying the graph (same results); bit 1: the reduced
+ * problem on many blocks at any capacity; bit 2: on the one-block control kernel at any
+ * capacity.  The Davidson
  * capacity is the smallest over the k points; bands must fit every operator's capacity.
  * Errors name the k point; the solve runs on the set's stream and returns when done. */
 int bg_kset_davidson_solve(bg_kset* set, const double* const* start, const double* const* diagonal,
                            const bg_davidson_options* options, int32_t ptr_kind, double* const* eigenvalues,
                            double* const* eigenvectors, int32_t* const* converged, bg_davidson_stats* stats);
+
+/* The generalised Hermitian eigenproblem H C = S C diag(w) of one m x m pencil (m <=
+ * 1536; column-major host matrices, interleaved complex when is_complex), solved the way
+ * bg_kset_davidson_solve solves its reduced problem beyond capacity 128: the Cholesky
+ * factor of S with the reference's pivot rule (squared pivot over the overlap diagonal
+ * >= eps / 1e-12, crates/dft-solvers/src/lean_davidson.rs:62-70), A = L^-1 H L^-H, a
+ * Householder tridiagonalisation, bisection and inverse iteration, C = L^-H Y -- the
+ * reference's ComplexOverlapFactor::extend + solve_lowest_into
+ * (crates/dft-numerics/src/linalg.rs:276, :369) -- on many thread blocks of the
+ * context's device.  Outputs (host): all m eigenvalues ascending and the S-orthonormal
+ * eigenvectors (m x m).  device_ms (may be NULL): device time of the solve.  A
+ * dependent S returns BG_ESHAPE. */
+int bg_reduced_eigh(bg_ctx* ctx, int64_t m, int32_t is_complex, const double* s, const double* h,
+                    double* eigenvalues, double* vectors, double* device_ms);
 
 /* Dense operator y = H x of a rows x rows column-major matrix (interleaved complex when
  * is_complex), for fixtures and small exact tests of the solver. */
