@@ -13,7 +13,8 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libbaandi_b200.so")
-SOURCES = ["api.cu", "hpsi_kernels.cu", "davidson.cu", "noalloc.cu", "fields.cu", "kset_davidson.cu", "mixer.cu", "learned.cu", "setup.cpp"]
+SOURCES = ["api.cu", "hpsi_kernels.cu", "davidson.cu", "noalloc.cu", "fields.cu", "kset_davidson.cu", "mixer.cu",
+           "learned.cu", "gemm_tc.cu", "setup.cpp"]
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-lineinfo", "-O3", "-std=c++17",

@@ -65,6 +65,10 @@ class ScfOptions:
     # None: FP64 throughout.  FP32 applies carry a relative error near 1e-6, far below
     # the eigenvalue accuracy that a loose early ethr asks for.
     fp32_ethr_ry: float | None = None
+    # Thomas-Fermi screening g2 / (g2 + a) of the Broyden update (the reference's
+    # scf.reference_preconditioning = "tf", crates/dft-engine/src/refscf/broyden.rs:107-114);
+    # the supercells need it against long-wavelength charge sloshing
+    thomas_fermi: bool = False
 
 
 @dataclass
@@ -145,7 +149,8 @@ class GpuScf:
         self.fields.set_sphere(flat)
         g2 = np.ascontiguousarray(dens.kpg2[keep])
         self._new_mixer = lambda: Broyden(g2, np.ones(g2.size, bool), self.volume, self.electrons, self.volume,
-                                          Profile(beta=self.o.beta, history=self.o.history), self.ctx)
+                                          Profile(beta=self.o.beta, history=self.o.history,
+                                                  thomas_fermi=self.o.thomas_fermi), self.ctx)
         self.mixer = self._new_mixer()
         s = self.stream.cuda_stream
         for op in self.ops:

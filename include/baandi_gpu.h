@@ -372,6 +372,20 @@ int bg_kset_davidson_solve(bg_kset* set, const double* const* start, const doubl
 int bg_reduced_eigh(bg_ctx* ctx, int64_t m, int32_t is_complex, const double* s, const double* h,
                     double* eigenvalues, double* vectors, double* device_ms);
 
+/* Complex product on the tcgen05 tensor cores with BF16x3 split operands and FP32
+ * accumulation (the precision form's projector and subspace products; no counterpart
+ * in the reference, whose products are FP64 faer/MKL GEMMs, crates/dft-physics/src/
+ * distributed_complex.rs:284-338, crates/dft-solvers/src/ref_davidson_complex.rs:195,
+ * :277).  mode 0: C (op)= A^H B with A k x m, B k x n; mode 1: C (op)= A B with A m x k,
+ * B k x n.  op 0: C = product, 1: C += product, 2: C -= product.  Device pointers,
+ * column-major interleaved complex FP64 with leading dimensions in complex elements.
+ * Each FP64 value is split into bf16 hi + lo; a product keeps hi*hi + hi*lo + lo*hi, so
+ * an entry's error is about 1e-5 of sum_r |a_r| |b_r| (16 significant bits, FP32
+ * accumulation).  Runs on `stream` and returns when done (it allocates its split-K
+ * workspace per call). */
+int bg_zgemm_bf16x3(bg_ctx* ctx, int32_t mode, int64_t m, int64_t n, int64_t k, const double* a, int64_t lda,
+                    const double* b, int64_t ldb, double* c, int64_t ldc, int32_t op, void* stream);
+
 /* Dense operator y = H x of a rows x rows column-major matrix (interleaved complex when
  * is_complex), for fixtures and small exact tests of the solver. */
 int bg_op_create_dense(bg_ctx* ctx, int64_t rows, const double* h, int32_t is_complex, int64_t capacity,

@@ -103,7 +103,7 @@ class _K:
 
 
 def run(rows, species, ecut_ha, dims, kpoints, gamma_real, bands, v_ion, starts, ewald, threshold_ha=5e-9,
-        max_iterations=60, beta=0.7, history=8, davidson_max_iterations=20, smearing_ha=None):
+        max_iterations=60, beta=0.7, history=8, davidson_max_iterations=20, smearing_ha=None, thomas_fermi=False):
     cell = S.Cell(np.asarray(rows, dtype=np.float64))
     vol = cell.volume
     electrons = float(sum(s.pseudo.z * np.atleast_2d(s.positions).shape[0] for s in species))
@@ -116,7 +116,8 @@ def run(rows, species, ecut_ha, dims, kpoints, gamma_real, bands, v_ion, starts,
     flat = S.fft_flat(S.g_to_fft(dens, dims), dims)[keep]
     g2 = dens.kpg2[keep]
     g0 = int(np.nonzero(flat == 0)[0][0])
-    mixer = B.Broyden(g2, np.ones(len(g2), bool), vol, electrons, vol, beta=beta, history=history)
+    mixer = B.Broyden(g2, np.ones(len(g2), bool), vol, electrons, vol, beta=beta, history=history,
+                      thomas_fermi=thomas_fermi)
     npts = int(np.prod(dims))
 
     def forward(rho):
