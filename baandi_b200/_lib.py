@@ -23,7 +23,7 @@ BG_PRECOND_SMOOTH, BG_PRECOND_TPA, BG_PRECOND_RITZ_SHIFT, BG_PRECOND_LEARNED = 0
 BG_LEARNED_PARAMS = 4609
 BG_PTR_HOST = 0
 BG_PTR_DEVICE = 1
-BG_PREC_FP64, BG_PREC_FP32 = 0, 1
+BG_PREC_FP64, BG_PREC_FP32, BG_PREC_TENSOR = 0, 1, 2
 
 CODE_NAMES = {
     BG_ESHAPE: "BG_ESHAPE", BG_ENONFINITE: "BG_ENONFINITE", BG_EEPOCH: "BG_EEPOCH",
@@ -60,7 +60,7 @@ class DavidsonOptions(ctypes.Structure):
 class DavidsonStats(ctypes.Structure):
     _fields_ = [("iterations", _i32), ("reduced_solves", _i32), ("h_calls", _i64), ("h_columns", _i64),
                 ("repairs", _i32), ("contractions", _i32), ("dropped", _i32), ("converged_count", _i32),
-                ("fallbacks", _i32), ("reserved", _i32)]
+                ("fallbacks", _i32), ("tensor_iterations", _i32)]
 
 
 class LearnedSamples(ctypes.Structure):

@@ -556,6 +556,7 @@ int bg_op_destroy(bg_op* op) {
     if (op->ev.ev[i]) cudaEventDestroy(op->ev.ev[i]);
   if (op->own_stream && op->stream) cudaStreamDestroy(op->stream);
   if (op->err_host) cudaFreeHost(op->err_host);
+  op->tc.release();
   delete op;
   return BG_OK;
 }
@@ -587,8 +588,9 @@ int bg_op_apply_block(bg_op* op, const double* x, double* y, int64_t rows, int64
                       int32_t precision) {
   if (!op) return fail(nullptr, BG_EINVAL, "null operator");
   bg_ctx* ctx = op->ctx;
-  if (precision != BG_PREC_FP64 && precision != BG_PREC_FP32) return fail(ctx, BG_EINVAL, "unsupported precision");
-  if (precision == BG_PREC_FP32 && (op->is_dense || !fp32_supported(op->g)))
+  if (precision != BG_PREC_FP64 && precision != BG_PREC_FP32 && precision != BG_PREC_TENSOR)
+    return fail(ctx, BG_EINVAL, "unsupported precision");
+  if (precision != BG_PREC_FP64 && (op->is_dense || !fp32_supported(op->g)))
     return fail(ctx, BG_EINVAL, "the FP32 apply needs a cubic grid of 25, 45, 54, 60, 72 or 108 points");
   if (ptr_kind != BG_PTR_HOST && ptr_kind != BG_PTR_DEVICE) return fail(ctx, BG_EINVAL, "pointer kind");
   if (!op->has_epoch) return fail(ctx, BG_EEPOCH, "potential was never set");
@@ -608,10 +610,13 @@ int bg_op_apply_block(bg_op* op, const double* x, double* y, int64_t rows, int64
     e = cudaMemcpyAsync(const_cast<double*>(dx), x, dpc * cols * sizeof(double), cudaMemcpyHostToDevice, op->stream);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "copy in");
   }
-  if (precision == BG_PREC_FP32) {
+  if (precision != BG_PREC_FP64) {
     int rc = ensure_potential_float(op, op->stream);
     if (rc) return rc;
   }
+  const bool tensor_nl = precision == BG_PREC_TENSOR && !op->gamma && op->shape.nproj > 0;
+  if (tensor_nl && ensure_nonlocal_tc(&op->tc, 1, op->shape.nproj, (int)op->cap, (int)op->rows))
+    return fail(ctx, BG_ENOMEM, "tensor-core nonlocal buffers");
   if (op->is_dense) {
     int rc = dense_apply(op, dx, dy, cols);
     if (rc != BG_OK) return rc;
@@ -626,8 +631,10 @@ int bg_op_apply_block(bg_op* op, const double* x, double* y, int64_t rows, int64
   a.cols = (int)cols;
   a.units = op->gamma ? (int)((cols + 1) / 2) : (int)cols;
   op->launches += launch_local(op->d_tabs, op->gamma ? 1 : 0, op->t.ngroups, op->g, bt, op->stream, &op->ev,
-                               precision == BG_PREC_FP32 ? 1 : 0);
-  if (op->shape.nproj > 0) {
+                               precision != BG_PREC_FP64 ? 1 : 0);
+  if (tensor_nl) {
+    op->launches += launch_nonlocal_tc(op->d_nl, op->shape, (int)op->rows, (int)cols, bt, &op->tc, op->stream, &op->ev);
+  } else if (op->shape.nproj > 0) {
     NlShape sh = op->shape;
     sh.ksplit = ksplit_for(op->rows, sh.nproj, cols, &sh.kchunk);
     op->launches += launch_nonlocal(op->d_nl, op->gamma ? 1 : 0, sh, (int)op->rows, bt, op->stream, &op->ev);
@@ -875,7 +882,7 @@ int ensure_potential_float(bg_op* op, cudaStream_t s) {
 }
 
 int enqueue_range(bg_kset* ks, int k0, int k1, const CallArgs* args, const int64_t* cols, cudaStream_t s,
-                  StageEvents* ev, int fp32) {
+                  StageEvents* ev, int prec, TcNl* tc) {
   Batch bt;
   bt.nk = k1 - k0;
   int max_groups = 0, max_rows = 0;
@@ -887,8 +894,10 @@ int enqueue_range(bg_kset* ks, int k0, int k1, const CallArgs* args, const int64
     max_cols = std::max(max_cols, cols[k]);
   }
   if (max_cols == 0) return 0;
-  int launches = launch_local(ks->d_tabs + k0, ks->gamma, max_groups, ks->g, bt, s, ev, fp32);
-  if (ks->shape.nproj > 0) {
+  int launches = launch_local(ks->d_tabs + k0, ks->gamma, max_groups, ks->g, bt, s, ev, prec != BG_PREC_FP64 ? 1 : 0);
+  if (prec == BG_PREC_TENSOR && !ks->gamma && ks->shape.nproj > 0) {
+    launches += launch_nonlocal_tc(ks->d_nl + k0, ks->shape, max_rows, (int)max_cols, bt, tc ? tc : &ks->tc, s, ev);
+  } else if (ks->shape.nproj > 0) {
     NlShape sh = ks->shape;
     int64_t tiles = 0, cap = 1 << 30;
     for (int k = k0; k < k1; ++k) {
@@ -979,6 +988,7 @@ int bg_kset_destroy(bg_kset* ks) {
   cudaFree(ks->dens_w);
   cudaFree(ks->d_tabs);
   cudaFree(ks->d_nl);
+  ks->tc.release();
   delete ks;
   return BG_OK;
 }
@@ -1111,12 +1121,13 @@ int bg_kset_apply(bg_kset* ks, const double* const* x, double* const* y, const i
                   int32_t precision) {
   if (!ks || !x || !y || !cols) return fail(ks ? ks->ctx : nullptr, BG_EINVAL, "null argument");
   bg_ctx* ctx = ks->ctx;
-  if (precision != BG_PREC_FP64 && precision != BG_PREC_FP32) return fail(ctx, BG_EINVAL, "unsupported precision");
+  if (precision != BG_PREC_FP64 && precision != BG_PREC_FP32 && precision != BG_PREC_TENSOR)
+    return fail(ctx, BG_EINVAL, "unsupported precision");
   if (ptr_kind != BG_PTR_HOST && ptr_kind != BG_PTR_DEVICE) return fail(ctx, BG_EINVAL, "pointer kind");
   if (ks->dense) return fail(ctx, BG_EINVAL, "a set of dense operators only runs bg_kset_davidson_solve");
-  if (precision == BG_PREC_FP32 && !fp32_supported(ks->g))
+  if (precision != BG_PREC_FP64 && !fp32_supported(ks->g))
     return fail(ctx, BG_EINVAL, "the FP32 apply needs a cubic grid of 25, 45, 54, 60, 72 or 108 points");
-  const int fp32 = precision == BG_PREC_FP32 ? 1 : 0;
+  const int fp32 = precision != BG_PREC_FP64 ? 1 : 0;
   const int n = (int)ks->ops.size();
   Batch bt;
   bt.nk = n;
@@ -1157,8 +1168,11 @@ int bg_kset_apply(bg_kset* ks, const double* const* x, double* const* y, const i
     a.units = op->gamma ? (int)((cols[k] + 1) / 2) : (int)cols[k];
   }
   if (max_cols == 0) return BG_OK;
+  if (precision == BG_PREC_TENSOR && !ks->gamma && ks->shape.nproj > 0 &&
+      ensure_nonlocal_tc(&ks->tc, n, ks->shape.nproj, (int)max_cols, ks->max_rows))
+    return fail(ctx, BG_ENOMEM, "tensor-core nonlocal buffers");
   if (ptr_kind == BG_PTR_DEVICE) {
-    ks->launches += enqueue_range(ks, 0, n, args.data(), cols, ks->stream, &ks->ev, fp32);
+    ks->launches += enqueue_range(ks, 0, n, args.data(), cols, ks->stream, &ks->ev, precision);
     e = cudaGetLastError();
     return e == cudaSuccess ? BG_OK : cuda_fail(ctx, e, "kernel launch");
   }
@@ -1178,7 +1192,7 @@ int bg_kset_apply(bg_kset* ks, const double* const* x, double* const* y, const i
     }
     cudaEventRecord(ks->in_done[c], in);
     cudaStreamWaitEvent(work, ks->in_done[c], 0);
-    ks->launches += enqueue_range(ks, k0, k1, args.data(), cols, work, nullptr, fp32);
+    ks->launches += enqueue_range(ks, k0, k1, args.data(), cols, work, nullptr, precision);
     cudaEventRecord(ks->work_done[c], work);
     cudaStreamWaitEvent(out, ks->work_done[c], 0);
     for (int k = k0; k < k1; ++k) {

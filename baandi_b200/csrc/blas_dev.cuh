@@ -78,11 +78,12 @@ __device__ __forceinline__ double block_sum256(double v, double* red) {
 // kind 2 (Ritz shift) out = -(hx - e x) / max(diag - e, 0.1); kind 3 (learned) the TPA
 // factor times exp(clamp(m(f))) of the per-G network whose parameters `net` holds as
 // floats in shared memory (learned.cuh).  Returns |out|^2 (all threads of the 256-thread
-// block).
+// block); res2, when given, receives the raw residual's |HX_j - lambda_j X_j|^2.
 template <class D, bool LEARNED = false>
 __device__ double correction_column(const D* __restrict__ x, const D* __restrict__ hx,
                                     const double* __restrict__ diag, double e, int kind, int64_t rows,
-                                    D* __restrict__ out, double* red, const float* net = nullptr) {
+                                    D* __restrict__ out, double* red, const float* net = nullptr,
+                                    double* res2 = nullptr) {
   if constexpr (LEARNED) kind = 3;
   double scale = 0.0, rms = 0.0;
   if (kind == 1 || kind == 3) {
@@ -102,9 +103,10 @@ __device__ double correction_column(const D* __restrict__ x, const D* __restrict
       q += Arith<D>::norm2(Arith<D>::add(hx[r], Arith<D>::scale(-e, x[r])));
     rms = sqrt(block_sum256(q, red) / (double)rows);
   }
-  double acc = 0.0;
+  double acc = 0.0, racc = 0.0;
   for (int64_t r = threadIdx.x; r < rows; r += blockDim.x) {
     const D res = Arith<D>::add(hx[r], Arith<D>::scale(-e, x[r]));
+    if (res2) racc += Arith<D>::norm2(res);
     double f;
     if (kind == 1)
       f = -tpa_weight(diag[r], scale);
@@ -121,6 +123,7 @@ __device__ double correction_column(const D* __restrict__ x, const D* __restrict
     out[r] = v;
     acc += Arith<D>::norm2(v);
   }
+  if (res2) *res2 = block_sum256(racc, red);   // |HX_j - lambda_j X_j|^2 (every thread)
   return block_sum256(acc, red);
 }
 

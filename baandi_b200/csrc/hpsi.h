@@ -133,6 +133,23 @@ int plane_lines_per_warp(int n0, int n1, int nlines);
 int launch_nonlocal(const NlDev* nl, int gamma, const NlShape& sh, int max_rows, const Batch& b, cudaStream_t s,
                     StageEvents* ev);
 
+// Buffers of the tensor-core nonlocal products (precision form, complex operators):
+// the product descriptors of a batch (2 kMaxBatch), the split-K workspace and an error
+// word.  Sized by ensure_nonlocal_tc before any launch (and before a graph capture).
+struct TcNl {
+  void* desc = nullptr;
+  float* work = nullptr;
+  size_t work_floats = 0;
+  int* err = nullptr;
+  int ksplit = 1;
+  void release();
+};
+int ensure_nonlocal_tc(TcNl* tc, int nk, int nproj, int max_cols, int max_rows);
+// Enqueue y += P (D (P^H x)) with P^H x and P W as BF16x3 tensor-core products (the
+// coupling D in FP64); complex operators only.
+int launch_nonlocal_tc(const NlDev* nl, const NlShape& sh, int max_rows, int max_cols, const Batch& b, TcNl* tc,
+                       cudaStream_t s, StageEvents* ev);
+
 // Band densities of the blocks of a batch (k = 0 .. b.nk - 1, operator tables tabs[k]
 // and their stick buffers): part[k][c][z][y n0 + x] = sum over the units of chunk c of
 // block k (in unit order) of w |psi(r)|^2, psi the unscaled inverse transform (Gamma:

@@ -20,6 +20,7 @@
 // crates/dft-physics/src/distributed_real_gamma.rs:654-689 (pair pack), :1307-1347
 // (unpack + kinetic), :957-1017, 1184-1248 (nonlocal).
 #include "hpsi.h"
+#include "gemm_tc.cuh"
 #include "fft_fast.cuh"
 #include "gemm_tiles.cuh"
 
@@ -981,6 +982,74 @@ int configure_kernels(size_t plane_smem, size_t stick_smem) {
   configure_one<true, 108>(e, plane_smem, stick_smem);
   configure_one<false, 108>(e, plane_smem, stick_smem);
   return e == cudaSuccess ? 0 : 1;
+}
+
+// Descriptors of the tensor-core nonlocal products of every operator of a batch:
+// [k] P^H x into the projection buffer, [nk + k] y += P wd.  One thread per operator.
+__global__ void k_nl_tc_descs(const NlDev* __restrict__ nls, int nproj, Batch b, tc::ZDesc* __restrict__ out) {
+  const int k = threadIdx.x;
+  if (k >= b.nk) return;
+  const NlDev& nl = nls[k];
+  const CallArgs ca = resolve(b.a[k]);
+  const int cols = ca.cols;
+  const double2* p = reinterpret_cast<const double2*>(nl.p);
+  out[k] = tc::ZDesc{p, reinterpret_cast<const double2*>(ca.x), reinterpret_cast<double2*>(nl.part), nl.rows,
+                     ca.ldx / 2, nproj, cols > 0 ? nproj : 0, cols, nl.rows, tc::kStore};
+  out[b.nk + k] = tc::ZDesc{p, reinterpret_cast<const double2*>(nl.wd), reinterpret_cast<double2*>(ca.y), nl.rows,
+                            nproj, ca.ldy / 2, cols > 0 ? nl.rows : 0, cols, nproj, tc::kAdd};
+}
+
+void TcNl::release() {
+  cudaFree(desc);
+  cudaFree(work);
+  cudaFree(err);
+  desc = nullptr;
+  work = nullptr;
+  err = nullptr;
+  work_floats = 0;
+}
+
+int ensure_nonlocal_tc(TcNl* t, int nk, int nproj, int max_cols, int max_rows) {
+  cudaError_t e = tc::prepare_zgemm();
+  if (e != cudaSuccess) return 1;
+  if (!t->desc && cudaMalloc(&t->desc, sizeof(tc::ZDesc) * 2 * kMaxBatch) != cudaSuccess) return 1;
+  if (!t->err) {
+    if (cudaMalloc(&t->err, sizeof(int)) != cudaSuccess) return 1;
+    if (cudaMemset(t->err, 0, sizeof(int)) != cudaSuccess) return 1;
+  }
+  t->ksplit = tc::tn_ksplit(nk, nproj, max_cols, max_rows);
+  const size_t need = tc::tn_workspace_floats(nk, t->ksplit, nproj, max_cols);
+  if (need > t->work_floats) {
+    cudaFree(t->work);
+    t->work = nullptr;
+    t->work_floats = 0;
+    if (cudaMalloc(&t->work, need * sizeof(float)) != cudaSuccess) return 1;
+    t->work_floats = need;
+  }
+  return 0;
+}
+
+int launch_nonlocal_tc(const NlDev* nl, const NlShape& sh, int max_rows, int max_cols, const Batch& b, TcNl* t,
+                       cudaStream_t s, StageEvents* ev) {
+  if (sh.nproj == 0 || max_cols == 0 || b.nk == 0) return 0;
+  tc::ZDesc* d = static_cast<tc::ZDesc*>(t->desc);
+  int launches = 1;
+  k_nl_tc_descs<<<1, kMaxBatch, 0, s>>>(nl, sh.nproj, b, d);
+  {
+    StageScope sc(ev, 3, s);
+    launches += tc::launch_zgemm(tc::kTN, d, b.nk, sh.nproj, max_cols, max_rows, t->ksplit, t->work, t->err, s);
+  }
+  {
+    StageScope sc(ev, 4, s);
+    const dim3 cg(sh.natoms, max_cols, b.nk);
+    k_couple<double2><<<cg, ((sh.maxch + 31) / 32) * 32, 0, s>>>(nl, sh.nproj, 1, b);
+    launches += 1;
+  }
+  {
+    StageScope sc(ev, 5, s);
+    launches += tc::launch_zgemm(tc::kNN, d + b.nk, b.nk, max_rows, max_cols, sh.nproj, 1, nullptr, t->err, s);
+  }
+  return launches;
 }
 
 }  // namespace bg

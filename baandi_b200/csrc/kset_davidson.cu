@@ -28,6 +28,7 @@
 #include <vector>
 
 #include "blas_dev.cuh"
+#include "gemm_tc.cuh"
 #include "gemm_tiles.cuh"
 #include "tridiag_dev.cuh"
 #include "op_internal.h"
@@ -39,6 +40,9 @@ constexpr double kEps = 2.220446049250313e-16;
 constexpr double kPivotRatioMin = kEps / 1e-12;   // crates/dft-solvers/src/lean_davidson.rs:62-70
 constexpr double kDependence = 1e-12;             // crates/dft-numerics/src/linalg.rs:12
 constexpr int kCtlThreads = 256;
+// Precision form: the tensor-core phase of a solve hands over to FP64 once every active
+// band's residual |HX_j - lambda_j X_j| is below this.
+constexpr double kHandoverResidual = 1e-4;
 
 // Errors recorded by a k point's control kernel (status = -id).
 enum : int {
@@ -109,6 +113,7 @@ struct Bufs {
   D *Q;                          // Householder accumulation, cap x cap
   double* Z;                     // tridiagonal eigenvectors, cap x cap (real)
   double *w, *old, *lam, *norms, *scale, *td, *te;  // cap
+  double* rnorm;                 // cap: |HX_j - lambda_j X_j|^2 of the active bands
   D* off;                        // cap: Householder off-diagonal
   D* ph;                         // cap: phases of the real tridiagonal
   D *hv, *hp, *hq;               // cap: Householder vectors
@@ -139,11 +144,13 @@ struct Ctl {
 
 // Descriptors of the large products of one slot (written by the control kernel).
 template <class D>
+// prec 1: the product runs as BF16x3 on the tensor cores (precision form), else FP64.
 struct NN {  // C[:, 0:n] (+)= A[:, 0:k] B, B k x n (ld ldb); A and C ld rows
   const D* A;
   const D* B;
   D* C;
   int ldb, n, k, accumulate;
+  int prec;
 };
 template <class D>
 struct TN {  // G[0:m, 0:n] (ld ldg) = A[:, 0:m]^H B[:, 0:n]
@@ -151,6 +158,7 @@ struct TN {  // G[0:m, 0:n] (ld ldg) = A[:, 0:m]^H B[:, 0:n]
   const D* B;
   D* G;
   int ldg, m, n;
+  int prec;
 };
 template <class D>
 struct CP {  // dst[:, c] = src[:, c] (scale[c] src[:, map[c]] when pick)
@@ -167,6 +175,8 @@ struct Opts {
   int smem_matrices;  // the control kernel keeps A, Y, Q, Z in shared memory
   int fp32;           // H applies with the FP32 local part
   int wide;           // the reduced problem runs on many blocks (wide_rr.cuh)
+  int tensor;         // precision form: tensor-core applies, H Grams and rotations
+  double handover;    // precision form: stop once every active band's residual is below
 };
 
 // ------------------------------------------------------------------ block-wide small algebra
@@ -551,7 +561,7 @@ __global__ void __launch_bounds__(128) k_dv_nn(const Bufs<D>* __restrict__ bufs,
   const int rows = bufs[k].rows;
   const int64_t r0 = (int64_t)blockIdx.x * 64;
   const int j0 = blockIdx.y * 32;
-  if (d.n <= 0 || j0 >= d.n || r0 >= rows) return;
+  if (d.n <= 0 || d.prec || j0 >= d.n || r0 >= rows) return;
   tiles::nn_tile<D, true>(d.A, rows, d.B, d.ldb, d.C, rows, rows, d.n, d.k, r0, j0, d.accumulate != 0);
 }
 
@@ -563,7 +573,7 @@ __global__ void __launch_bounds__(256, 2) k_dv_tn(const Bufs<D>* __restrict__ bu
   const int zz = blockIdx.z / ks, sidx = blockIdx.z % ks;
   const int slot = zz / nk, k = zz % nk;
   const TN<D> d = desc[zz];
-  if (d.m <= 0 || d.n <= 0 || (int)blockIdx.x * 48 >= d.m || (int)blockIdx.y * 48 >= d.n) return;
+  if (d.m <= 0 || d.n <= 0 || d.prec || (int)blockIdx.x * 48 >= d.m || (int)blockIdx.y * 48 >= d.n) return;
   const int64_t rows = bufs[k].rows;
   int64_t chunk = (rows + ks - 1) / ks;
   chunk = ((chunk + 31) / 32) * 32;
@@ -578,7 +588,7 @@ __global__ void k_dv_tn_sum(const Bufs<D>* __restrict__ bufs, const TN<D>* __res
                             int64_t slot_elems) {
   const int zz = blockIdx.z, slot = zz / nk, k = zz % nk;
   const TN<D> d = desc[zz];
-  if (d.m <= 0 || d.n <= 0) return;
+  if (d.m <= 0 || d.n <= 0 || d.prec) return;
   const D* part = bufs[k].part + slot * slot_elems;
   const int64_t total = (int64_t)d.m * d.n;
   for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
@@ -646,8 +656,39 @@ __global__ void __launch_bounds__(256) k_dv_corrections(const Bufs<D>* __restric
   if (c.status != 0 || j >= c.nact) return;
   const Bufs<D>& b = bufs[k];
   const int64_t rows = b.rows;
-  const double n2 = correction_column(b.X + j * rows, b.HX + j * rows, b.diag, b.lam[j], kind, rows, b.Er + j * rows, red);
-  if (threadIdx.x == 0) b.norms[j] = n2;
+  double r2 = 0.0;
+  const double n2 = correction_column(b.X + j * rows, b.HX + j * rows, b.diag, b.lam[j], kind, rows, b.Er + j * rows, red,
+                                      nullptr, &r2);
+  if (threadIdx.x == 0) {
+    b.norms[j] = n2;
+    b.rnorm[j] = r2;
+  }
+}
+
+// Tensor-core descriptors of the products marked prec = 1 (complex blocks): one thread per
+// (slot, k point); the others get empty descriptors.
+template <class D>
+__global__ void k_dv_tc_descs(const Bufs<D>* __restrict__ bufs, const NN<D>* __restrict__ nn, int n_nn,
+                              const TN<D>* __restrict__ tn, int n_tn, int nk, tc::ZDesc* out_nn, tc::ZDesc* out_tn) {
+  const int z = blockIdx.x * blockDim.x + threadIdx.x;
+  const tc::ZDesc empty{nullptr, nullptr, nullptr, 1, 1, 1, 0, 0, 0, tc::kStore};
+  if (z < n_nn * nk) {
+    const NN<D> d = nn[z];
+    const int64_t rows = bufs[z % nk].rows;
+    out_nn[z] = (d.prec && d.n > 0 && d.k > 0)
+                    ? tc::ZDesc{reinterpret_cast<const double2*>(d.A), reinterpret_cast<const double2*>(d.B),
+                                reinterpret_cast<double2*>(d.C), rows, d.ldb, rows, (int)rows, d.n, d.k,
+                                d.accumulate ? tc::kAdd : tc::kStore}
+                    : empty;
+  }
+  if (z < n_tn * nk) {
+    const TN<D> d = tn[z];
+    const int64_t rows = bufs[z % nk].rows;
+    out_tn[z] = (d.prec && d.m > 0 && d.n > 0)
+                    ? tc::ZDesc{reinterpret_cast<const double2*>(d.A), reinterpret_cast<const double2*>(d.B),
+                                reinterpret_cast<double2*>(d.G), rows, rows, d.ldg, d.m, d.n, (int)rows, tc::kStore}
+                    : empty;
+  }
 }
 
 }  // namespace dv
@@ -746,6 +787,8 @@ __global__ void __launch_bounds__(kCtlThreads, 1) k_dv_ctl(int phase, Bufs<D>* _
     __syncthreads();
   };
   D* Vt = b.V + (int64_t)c.m * rows;    // first free basis column
+  // precision form: H Grams and rotations as tensor-core products (complex blocks)
+  const int tcp = (o.tensor != 0 && sizeof(D) == sizeof(double2)) ? 1 : 0;
   // a request to the many-block reduced problem (its error bits cleared for it)
   auto request = [&](int m0, int m1, int me) {
     if (threadIdx.x == 0) {
@@ -776,8 +819,8 @@ __global__ void __launch_bounds__(kCtlThreads, 1) k_dv_ctl(int phase, Bufs<D>* _
     }
     for (int j = threadIdx.x; j < na; j += blockDim.x) b.lam[j] = b.w[b.active[j]];
     if (threadIdx.x == 0) {
-      nn[0 * nk + k] = NN<D>{b.V, b.P, b.X, cap, na, m, 0};
-      nn[1 * nk + k] = NN<D>{b.HV, b.P, b.HX, cap, na, m, 0};
+      nn[0 * nk + k] = NN<D>{b.V, b.P, b.X, cap, na, m, 0, tcp};
+      nn[1 * nk + k] = NN<D>{b.HV, b.P, b.HX, cap, na, m, 0, tcp};
     }
   };
   // the repair's descriptors when the bordered factor could not be extended
@@ -801,7 +844,7 @@ __global__ void __launch_bounds__(kCtlThreads, 1) k_dv_ctl(int phase, Bufs<D>* _
       c.h_columns += kk;
       dyn[k] = DynCols{reinterpret_cast<const double*>(Vt), reinterpret_cast<double*>(b.HV + (int64_t)m * rows), kk,
                        gamma ? (kk + 1) / 2 : kk};
-      tn[0 * nk + k] = TN<D>{b.V, b.HV + (int64_t)m * rows, b.Hr + (size_t)m * cap, cap, m + kk, kk};
+      tn[0 * nk + k] = TN<D>{b.V, b.HV + (int64_t)m * rows, b.Hr + (size_t)m * cap, cap, m + kk, kk, tcp};
     }
   };
   auto finish_tail = [&](int kk) {
@@ -871,10 +914,10 @@ __global__ void __launch_bounds__(kCtlThreads, 1) k_dv_ctl(int phase, Bufs<D>* _
         if (c.contract) {
           // X = V C[:, :n], HX = HV C[:, :n] become the basis: the refresh phase exchanges
           // the buffers (no copy), so the Grams read X and HX
-          nn[0 * nk + k] = NN<D>{b.V, b.C, b.X, cap, n, c.m, 0};
-          nn[1 * nk + k] = NN<D>{b.HV, b.C, b.HX, cap, n, c.m, 0};
-          tn[0 * nk + k] = TN<D>{b.X, b.X, b.S, cap, n, n};
-          tn[1 * nk + k] = TN<D>{b.X, b.HX, b.Hr, cap, n, n};
+          nn[0 * nk + k] = NN<D>{b.V, b.C, b.X, cap, n, c.m, 0, tcp};
+          nn[1 * nk + k] = NN<D>{b.HV, b.C, b.HX, cap, n, c.m, 0, tcp};
+          tn[0 * nk + k] = TN<D>{b.X, b.X, b.S, cap, n, n, 0};
+          tn[1 * nk + k] = TN<D>{b.X, b.HX, b.Hr, cap, n, n, tcp};
         }
       }
       break;
@@ -943,6 +986,15 @@ __global__ void __launch_bounds__(kCtlThreads, 1) k_dv_ctl(int phase, Bufs<D>* _
       break;
     }
     case kSelect: {
+      if (o.tensor && o.handover > 0.0) {  // precision form: every active residual small enough
+        if (threadIdx.x == 0) {
+          double mx = 0.0;
+          for (int j = 0; j < c.nact; ++j) mx = fmax(mx, b.rnorm[j]);
+          if (mx < o.handover * o.handover) c.status = 2;
+        }
+        __syncthreads();
+        if (c.status != 0) break;
+      }
       if (threadIdx.x == 0) {
         int kept = 0;
         for (int j = 0; j < c.nact; ++j) {
@@ -1136,7 +1188,7 @@ __global__ void __launch_bounds__(kCtlThreads, 1) k_dv_ctl(int phase, Bufs<D>* _
     }
     case kFinal: {
       if (c.status < 0) break;
-      if (threadIdx.x == 0) nn[0 * nk + k] = NN<D>{b.V, b.C, b.X, cap, n, c.m, 0};
+      if (threadIdx.x == 0) nn[0 * nk + k] = NN<D>{b.V, b.C, b.X, cap, n, c.m, 0, tcp};
       break;
     }
     default:
@@ -1247,7 +1299,8 @@ class KsetSolver {
     want_graph_ = graph;
   }
   ~KsetSolver() {
-    for (int p = 0; p < 2; ++p) {
+    tcnl_.release();
+    for (int p = 0; p < 3; ++p) {
       if (exec_[p]) cudaGraphExecDestroy(exec_[p]);
       if (graph_[p]) cudaGraphDestroy(graph_[p]);
     }
@@ -1265,13 +1318,22 @@ class KsetSolver {
   bg_kset* ks_;
   int nk_;
   bool wide_ = false;
+  // precision form: the solver's own tensor-core nonlocal buffers and the descriptors and
+  // split-K workspace of its tensor-core Davidson products
+  TcNl tcnl_;
+  tc::ZDesc* d_tcnn_ = nullptr;
+  tc::ZDesc* d_tctn_ = nullptr;
+  float* tc_work_ = nullptr;
+  int* tc_err_ = nullptr;
+  int tc_ks_ = 1;
+  bool tc_ready_ = false;
   unsigned* d_bar_ = nullptr;   // grid barrier of the cooperative launches
   double* d_wpart_ = nullptr;   // their per-block partial sums
   int coop_blocks_ = 0;
   Opts o_;
   bool want_graph_ = true;
   bool prepared_ = false;
-  bool graph_tried_[2] = {false, false};   // by apply precision (0 FP64, 1 FP32)
+  bool graph_tried_[3] = {false, false, false};   // by precision (0 FP64, 1 FP32, 2 tensor)
   Opts* d_opts_ = nullptr;
   cudaStream_t s_ = nullptr;
   std::vector<void*> dev_;
@@ -1293,9 +1355,9 @@ class KsetSolver {
   int max_rows_ = 0;
   std::vector<CallArgs> args_;
   std::vector<int64_t> cols_;
-  cudaGraph_t graph_[2] = {nullptr, nullptr};
-  cudaGraphExec_t exec_[2] = {nullptr, nullptr};
-  int64_t per_iteration_[2] = {0, 0};
+  cudaGraph_t graph_[3] = {nullptr, nullptr, nullptr};
+  cudaGraphExec_t exec_[3] = {nullptr, nullptr, nullptr};
+  int64_t per_iteration_[3] = {0, 0, 0};
   int64_t launches_ = 0;
   std::string err_;
 
@@ -1330,8 +1392,11 @@ class KsetSolver {
   int64_t nn(int nslots) {
     const dim3 grid((unsigned)((max_rows_ + 63) / 64), (unsigned)((o_.cap + 31) / 32), (unsigned)(nslots * nk_));
     k_dv_nn<D><<<grid, 128, 0, s_>>>(d_bufs_, d_nn_, nk_);
-    return 1;
+    if (!tensor_products()) return 1;
+    k_dv_tc_descs<D><<<1, 128, 0, s_>>>(d_bufs_, d_nn_, nslots, d_tn_, 0, nk_, d_tcnn_, d_tctn_);
+    return 2 + tc::launch_zgemm(tc::kNN, d_tcnn_, nslots * nk_, max_rows_, o_.cap, o_.cap, 1, nullptr, tc_err_, s_);
   }
+  bool tensor_products() const { return o_.tensor && sizeof(D) == sizeof(double2) && tc_ready_; }
   int64_t tn(int nslots) {
     const unsigned t = (unsigned)((o_.cap + 47) / 48);
     k_dv_tn<D><<<dim3(t, t, (unsigned)(nslots * nk_ * ksplit_)), 256, 0, s_>>>(d_bufs_, d_tn_, nk_, ksplit_,
@@ -1339,7 +1404,29 @@ class KsetSolver {
     const unsigned blocks = (unsigned)std::min<int64_t>(((int64_t)o_.cap * o_.cap + 255) / 256, 64);
     k_dv_tn_sum<D><<<dim3(blocks, 1, (unsigned)(nslots * nk_)), 256, 0, s_>>>(d_bufs_, d_tn_, nk_, ksplit_,
                                                                               slot_elems_);
-    return 2;
+    if (!tensor_products()) return 2;
+    k_dv_tc_descs<D><<<1, 128, 0, s_>>>(d_bufs_, d_nn_, 0, d_tn_, nslots, nk_, d_tcnn_, d_tctn_);
+    return 3 + tc::launch_zgemm(tc::kTN, d_tctn_, nslots * nk_, o_.cap, o_.cap, max_rows_, tc_ks_, tc_work_, tc_err_,
+                                s_);
+  }
+  // Buffers of the precision form (once, before any capture).
+  int prepare_tensor() {
+    if (tc_ready_ || sizeof(D) != sizeof(double2)) return BG_OK;
+    int rc;
+    if ((rc = cuda(tc::prepare_zgemm(), "tensor-core product attributes"))) return rc;
+    const int slots = std::max(kNnSlots, kTnSlots);
+    tc_ks_ = tc::tn_ksplit(kTnSlots * nk_, o_.cap, o_.cap, max_rows_);
+    if ((rc = alloc(&d_tcnn_, (size_t)slots * nk_)) || (rc = alloc(&d_tctn_, (size_t)slots * nk_)) ||
+        (rc = alloc(&tc_work_, tc::tn_workspace_floats(kTnSlots * nk_, tc_ks_, o_.cap, o_.cap))) ||
+        (rc = alloc(&tc_err_, 1)))
+      return rc;
+    if ((rc = cuda(cudaMemset(tc_err_, 0, sizeof(int)), "tensor error word"))) return rc;
+    if (!ks_->gamma && ks_->shape.nproj > 0 && ensure_nonlocal_tc(&tcnl_, nk_, ks_->shape.nproj, o_.n, max_rows_)) {
+      err_ = "tensor-core nonlocal buffers";
+      return BG_ENOMEM;
+    }
+    tc_ready_ = true;
+    return BG_OK;
   }
   int64_t cp(int slot0, int nslots) {
     const int64_t span = 256 * kCopyUnroll;
@@ -1366,7 +1453,8 @@ class KsetSolver {
       k_dv_dense<D><<<grid, 128, 0, s_>>>(d_dense_, d_bufs_, d_dyn_);
       return 1;
     }
-    return enqueue_range(ks_, 0, nk_, args_.data(), cols_.data(), s_, nullptr, o_.fp32);
+    return enqueue_range(ks_, 0, nk_, args_.data(), cols_.data(), s_, nullptr,
+                         o_.tensor ? BG_PREC_TENSOR : (o_.fp32 ? BG_PREC_FP32 : BG_PREC_FP64), &tcnl_);
   }
   int64_t iteration() {
     int64_t l = 0;
@@ -1429,6 +1517,7 @@ int KsetSolver<T>::prepare() {
         (rc = alloc(&b.P, cc)) || (rc = alloc(&b.Q, cc)) || (rc = alloc(&b.Z, cc)) || (rc = alloc(&b.w, cap)) ||
         (rc = alloc(&b.old, cap)) || (rc = alloc(&b.lam, cap)) || (rc = alloc(&b.norms, cap)) ||
         (rc = alloc(&b.scale, cap)) || (rc = alloc(&b.td, cap)) || (rc = alloc(&b.te, cap)) ||
+        (rc = alloc(&b.rnorm, cap)) ||
         (rc = alloc(&b.off, cap)) || (rc = alloc(&b.ph, cap)) || (rc = alloc(&b.hv, cap)) || (rc = alloc(&b.hp, cap)) ||
         (rc = alloc(&b.hq, cap)) || (rc = alloc(&b.active, cap)) || (rc = alloc(&b.map, cap)) ||
         (rc = alloc(&b.conv, cap)) || (rc = alloc(&b.order, cap)) || (rc = alloc(&b.part, 2 * (size_t)slot_elems_)) ||
@@ -1495,6 +1584,7 @@ int KsetSolver<T>::run(const double* const* start, const double* const* diagonal
   s_ = ks_->stream;
   launches_ = 0;
   if (!prepared_ && (rc = prepare())) return rc;
+  if (o_.tensor && (rc = prepare_tensor())) return rc;
   // the pinned pointer table may still feed a copy of the previous solve
   if ((rc = cuda(cudaStreamSynchronize(s_), "start"))) return rc;
   for (int k = 0; k < nk_; ++k) {
@@ -1530,7 +1620,7 @@ int KsetSolver<T>::run(const double* const* start, const double* const* diagonal
     dy[k] = DynCols{reinterpret_cast<const double*>(b.V), reinterpret_cast<double*>(b.HV), n,
                     ks_->gamma ? (n + 1) / 2 : n};
     t0[k] = TN<D>{b.V, b.V, b.S, cap, n, n};
-    t0[(size_t)nk_ + k] = TN<D>{b.V, b.HV, b.Hr, cap, n, n};
+    t0[(size_t)nk_ + k] = TN<D>{b.V, b.HV, b.Hr, cap, n, n, (o_.tensor && sizeof(D) == sizeof(double2)) ? 1 : 0};
   }
   if ((rc = cuda(cudaMemcpyAsync(d_ctl_, c0.data(), sizeof(Ctl) * nk_, cudaMemcpyHostToDevice, s_), "upload")) ||
       (rc = cuda(cudaMemcpyAsync(d_dyn_, dy.data(), sizeof(DynCols) * nk_, cudaMemcpyHostToDevice, s_), "upload")) ||
@@ -1542,7 +1632,7 @@ int KsetSolver<T>::run(const double* const* start, const double* const* diagonal
   bool done = false;
   if ((rc = poll(&done))) return rc;
   // iterations: one captured graph replayed until every k point has finished
-  const int gp = o_.fp32 ? 1 : 0;
+  const int gp = o_.tensor ? 2 : (o_.fp32 ? 1 : 0);
   if (want_graph_ && !graph_tried_[gp]) {
     graph_tried_[gp] = true;
     cudaStreamCaptureStatus st;
@@ -1761,18 +1851,20 @@ extern "C" int bg_kset_davidson_solve(bg_kset* ks, const double* const* start, c
   }
   cudaError_t e = cudaSetDevice(ctx->device);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaSetDevice");
-  if (o.apply_precision != BG_PREC_FP64 && o.apply_precision != BG_PREC_FP32)
+  if (o.apply_precision != BG_PREC_FP64 && o.apply_precision != BG_PREC_FP32 && o.apply_precision != BG_PREC_TENSOR)
     return fail(ctx, BG_EINVAL, "unsupported apply precision");
-  if (o.apply_precision == BG_PREC_FP32 && (ks->dense || !fp32_supported(ks->g)))
+  if (o.apply_precision != BG_PREC_FP64 && (ks->dense || !fp32_supported(ks->g)))
     return fail(ctx, BG_EINVAL, "the FP32 apply needs a cubic grid of 25, 45, 54, 60, 72 or 108 points");
   Opts op{(int)n, (int)cap, (int)o.occupied, o.first_step ? 1 : 0, o.max_iterations, o.threshold, o.preconditioner, 0,
-          o.apply_precision == BG_PREC_FP32 ? 1 : 0};
+          o.apply_precision != BG_PREC_FP64 ? 1 : 0};
+  op.tensor = o.apply_precision == BG_PREC_TENSOR ? 1 : 0;
+  op.handover = op.tensor ? kHandoverResidual : 0.0;
   const bool graph = (o.flags & 1) == 0;
   // the reduced problem on many blocks beyond capacity 128 (flags bit 1 forces it, bit 2
   // keeps the one-block control kernel)
   const bool wide = (o.flags & 2) != 0 || (cap > 128 && (o.flags & 4) == 0);
   int rc;
-  if (o.apply_precision == BG_PREC_FP32)  // the FP32 potential copies, on the set's stream
+  if (o.apply_precision != BG_PREC_FP64)  // the FP32 potential copies, on the set's stream
     for (bg_op* kop : ks->ops)
       if ((rc = ensure_potential_float(kop, ks->stream))) return rc;
   std::string err;
@@ -1793,9 +1885,34 @@ extern "C" int bg_kset_davidson_solve(bg_kset* ks, const double* const* start, c
       ks->dv_free = [](void* p) { delete static_cast<S*>(p); };
     }
     s->set_options(op, graph);
-    const int r = s->run(start, diagonal, ptr_kind, eigenvalues, eigenvectors, converged, stats);
+    int r = s->run(start, diagonal, ptr_kind, eigenvalues, eigenvectors, converged, stats);
     err = s->error();
     launches = s->launches();
+    if (r != BG_OK || !op.tensor) return r;
+    // precision form: the FP64 phase from the tensor phase's Ritz vectors
+    std::vector<bg_davidson_stats> first(stats ? (size_t)nk : 0);
+    if (stats) std::copy(stats, stats + nk, first.begin());
+    Opts o64 = op;
+    o64.fp32 = 0;
+    o64.tensor = 0;
+    o64.handover = 0.0;
+    s->set_options(o64, graph);
+    r = s->run(eigenvectors, diagonal, ptr_kind, eigenvalues, eigenvectors, converged, stats);
+    err = s->error();
+    launches += s->launches();
+    if (stats)
+      for (int k = 0; k < nk; ++k) {
+        bg_davidson_stats& st = stats[k];
+        const bg_davidson_stats& f = first[k];
+        st.tensor_iterations = f.iterations;
+        st.iterations += f.iterations;
+        st.reduced_solves += f.reduced_solves;
+        st.h_calls += f.h_calls;
+        st.h_columns += f.h_columns;
+        st.repairs += f.repairs;
+        st.contractions += f.contractions;
+        st.dropped += f.dropped;
+      }
     return r;
   };
   if (ks->gamma)

@@ -65,6 +65,7 @@ struct bg_op {
   double* dens_ksum = nullptr;  // one grid: the reduction's per-k sum
   int dens_chunks = 0;  // chunks dens_part holds
   bool vtf_valid = false;  // t.vtf (the FP32 apply's potential) matches t.vt
+  bg::TcNl tc;             // tensor-core nonlocal products (BG_PREC_TENSOR)
 };
 
 
@@ -103,13 +104,16 @@ struct bg_kset {
   int** d_errs = nullptr;
   int* d_errv = nullptr;
   int* h_errv = nullptr;
+  bg::TcNl tc;  // tensor-core nonlocal products (BG_PREC_TENSOR)
 };
 
 namespace bg {
 // Launch the local and nonlocal stages of operators [k0, k1) of a set on one stream
 // (cols[k]: the widest block of operator k, used to size the grids).
+// prec: BG_PREC_FP64, BG_PREC_FP32 or BG_PREC_TENSOR (tensor buffers sized beforehand
+// by ensure_nonlocal_tc on tc, or on ks->tc when tc is null).
 int enqueue_range(bg_kset* ks, int k0, int k1, const CallArgs* args, const int64_t* cols, cudaStream_t s,
-                  StageEvents* ev, int fp32 = 0);
+                  StageEvents* ev, int prec = 0, TcNl* tc = nullptr);
 // Convert the operator's potential to its FP32 copy on stream s if the copy is stale.
 int ensure_potential_float(bg_op* op, cudaStream_t s);
 // Failure message on the context (or the thread's context-free slot) and status.

@@ -26,7 +26,10 @@ class Options:
     capacity: int = 0
     max_iterations: int = 20
     preconditioner: str = "smooth"   # "smooth" (reference Davidson), "tpa", "ritz_shift", "learned"
-    apply_precision: str = "fp64"    # "fp64", or "fp32" (the local part of every H apply in FP32)
+    # "fp64"; "fp32" (the local part of every H apply in FP32); "tensor" (solve_kset only:
+    # the precision form, tensor-core applies, H Grams and rotations until every active
+    # residual is below 1e-4, then the FP64 solve from those Ritz vectors)
+    apply_precision: str = "fp64"
 
     def band_threshold(self, band: int) -> float:
         if self.first_step or band < self.occupied:
@@ -47,6 +50,7 @@ class Solution:
     contractions: int
     dropped: int
     fallbacks: int = 0   # 1: the learned preconditioner gave way to TPA
+    tensor_iterations: int = 0   # precision form: iterations before the FP64 handover
 
 
 def preconditioner_denominator(hamiltonian_diagonal_ha, eigenvalue_ha):
@@ -57,6 +61,7 @@ def preconditioner_denominator(hamiltonian_diagonal_ha, eigenvalue_ha):
     return 0.25 * (np.where(x >= 1.0, 2.0 * x, 2.0) + 1.0 / (np.hypot(z, 1.0) + z))
 
 
+PRECISIONS = {"fp64": L.BG_PREC_FP64, "fp32": L.BG_PREC_FP32, "tensor": L.BG_PREC_TENSOR}
 PRECONDITIONERS = {"smooth": L.BG_PRECOND_SMOOTH, "tpa": L.BG_PRECOND_TPA, "ritz_shift": L.BG_PRECOND_RITZ_SHIFT,
                    "learned": L.BG_PRECOND_LEARNED}
 
@@ -64,11 +69,11 @@ PRECONDITIONERS = {"smooth": L.BG_PRECOND_SMOOTH, "tpa": L.BG_PRECOND_TPA, "ritz
 def _options(options: Options, flags: int = 0):
     if options.preconditioner not in PRECONDITIONERS:
         raise SolverError(L.BG_EINVAL, f"preconditioner {options.preconditioner!r}")
-    if options.apply_precision not in ("fp64", "fp32"):
+    if options.apply_precision not in PRECISIONS:
         raise SolverError(L.BG_EINVAL, f"apply precision {options.apply_precision!r}")
     return L.DavidsonOptions(options.bands, options.threshold, options.occupied, 1 if options.first_step else 0,
                              options.capacity, options.max_iterations, flags, PRECONDITIONERS[options.preconditioner],
-                             L.BG_PREC_FP32 if options.apply_precision == "fp32" else L.BG_PREC_FP64)
+                             PRECISIONS[options.apply_precision])
 
 
 def solve(operator: _Operator, start: np.ndarray, hamiltonian_diagonal: np.ndarray, options: Options) -> Solution:
@@ -172,5 +177,6 @@ def solve_kset(kset, starts, diagonals, options: Options, graph: bool = True, re
                                     arr(vecs, ptr), arr(conv, host), stats)
     kset._check(rc)
     return [Solution(vals[k], vecs[k], conv[k].astype(bool), stats[k].iterations, stats[k].reduced_solves,
-                     stats[k].h_calls, stats[k].h_columns, stats[k].repairs, stats[k].contractions, stats[k].dropped)
+                     stats[k].h_calls, stats[k].h_columns, stats[k].repairs, stats[k].contractions, stats[k].dropped,
+                     stats[k].fallbacks, stats[k].tensor_iterations)
             for k in range(nk)]

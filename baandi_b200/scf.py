@@ -69,6 +69,10 @@ class ScfOptions:
     # scf.reference_preconditioning = "tf", crates/dft-engine/src/refscf/broyden.rs:107-114);
     # the supercells need it against long-wavelength charge sloshing
     thomas_fermi: bool = False
+    # the precision form on every map: each Davidson solve starts with tensor-core applies,
+    # H Grams and rotations (BF16x3, FP32 local part) and hands over to FP64 once every
+    # active band's residual is below 1e-4 (convergence judged in FP64)
+    tensor: bool = False
 
 
 @dataclass
@@ -82,7 +86,8 @@ class MapRecord:
     h_columns: int
     davidson_iterations: int
     seconds: float
-    precision: str = "fp64"   # of the local part of the H applies
+    precision: str = "fp64"   # of the H applies: fp64, fp32 (local part) or tensor (precision form)
+    tensor_iterations: int = 0  # precision form: Davidson iterations before the FP64 handover
 
 
 @dataclass
@@ -162,6 +167,8 @@ class GpuScf:
         torch.cuda.synchronize()
 
     def precision_at(self, ethr: float) -> str:
+        if self.o.tensor:
+            return "tensor"
         f = self.o.fp32_ethr_ry
         return "fp32" if f is not None and ethr >= f else "fp64"
 
@@ -233,7 +240,8 @@ class GpuScf:
                     sols, rho, y, fres, dr2, energy, ts = self._map(n, x, ethr, it == 1 and not redo)
                     records.append(MapRecord(it, "retry" if redo else "ordinary", dr2, energy, ts, ethr,
                                              sum(s.h_columns for s in sols), max(s.iterations for s in sols),
-                                             time.perf_counter() - tm, self.precision_at(ethr)))
+                                             time.perf_counter() - tm, self.precision_at(ethr),
+                                             max(s.tensor_iterations for s in sols)))
                     self.starts = [s.eigenvectors for s in sols]
                     if it == 1 and not redo and dr2 < ethr * max(self.electrons, 1.0):
                         ethr = next_ethr_ry(ethr, dr2, self.electrons)

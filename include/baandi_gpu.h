@@ -48,6 +48,9 @@ extern "C" {
  * grid of 25, 45, 54, 60, 72 or 108 points. */
 #define BG_PREC_FP64 0
 #define BG_PREC_FP32 1
+#define BG_PREC_TENSOR 2  /* FP32 local part; P^H x and P W as BF16x3 tensor-core
+                             products (complex operators; a Gamma-real operator keeps
+                             its nonlocal part in FP64) */
 
 typedef struct bg_ctx bg_ctx;
 typedef struct bg_op bg_op;
@@ -287,7 +290,12 @@ typedef struct {
   int32_t max_iterations; /* correction iterations (reference default 20)               */
   int32_t flags;          /* bg_kset_davidson_solve: bit 0 launches directly (no graph)  */
   int32_t preconditioner; /* BG_PRECOND_*                                                */
-  int32_t apply_precision; /* BG_PREC_* of the solver's H applies                        */
+  int32_t apply_precision; /* BG_PREC_* of the solver's H applies; BG_PREC_TENSOR in
+                              bg_kset_davidson_solve is the precision form: a first phase
+                              with tensor-core applies, H Grams and rotations (overlap
+                              Grams, factor and eigensolve FP64) until every active band's
+                              residual |HX_j - lambda_j X_j| is below 1e-4, then the FP64
+                              solve from its Ritz vectors (convergence judged in FP64) */
   int32_t reserved[1];
 } bg_davidson_options;
 
@@ -321,7 +329,7 @@ typedef struct {
   int32_t dropped;         /* corrections dropped as dependent or of vanishing norm     */
   int32_t converged_count;
   int32_t fallbacks;       /* 1: the learned preconditioner gave way to TPA in this solve */
-  int32_t reserved;
+  int32_t tensor_iterations; /* BG_PREC_TENSOR: iterations before the FP64 handover       */
 } bg_davidson_stats;
 
 /* Reference block Davidson (crates/dft-solvers/src/ref_davidson.rs:117-366 for the
