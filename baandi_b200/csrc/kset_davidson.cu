@@ -52,6 +52,7 @@ enum : int {
   kErrCapacity,
   kErrRepairDependent,
   kErrEigen,
+  kErrTimeout,
 };
 
 // ------------------------------------------------------------------ scalar helpers
@@ -140,6 +141,9 @@ struct Ctl {
   // requests to the many-block reduced problem: extend the factor from wc_m0 to wc_m1
   // columns, solve the reduced problem of we_m columns (0: none)
   int wc_m0, wc_m1, we_m;
+  // precision form: iterations without a new smallest residual, and that residual (squared)
+  int stall;
+  double best_res;
 };
 
 // Descriptors of the large products of one slot (written by the control kernel).
@@ -896,6 +900,10 @@ __global__ void __launch_bounds__(kCtlThreads, 1) k_dv_ctl(int phase, Bufs<D>* _
     }
     case kSetupPost: {
       const int we = werr();
+      if (we & wide::kWErrBarrier) {
+        set_err(kErrTimeout);
+        break;
+      }
       if (we & wide::kWErrPivot) {
         set_err(kErrStartDependent);
         break;
@@ -965,6 +973,10 @@ __global__ void __launch_bounds__(kCtlThreads, 1) k_dv_ctl(int phase, Bufs<D>* _
     case kRefreshPost: {
       if (c.we_m) {  // the contraction's factor and eigensolve
         const int we = werr();
+        if (we & wide::kWErrBarrier) {
+          set_err(kErrTimeout);
+          break;
+        }
         if (we & wide::kWErrPivot) {
           set_err(kErrBasisDependent);
           break;
@@ -986,11 +998,26 @@ __global__ void __launch_bounds__(kCtlThreads, 1) k_dv_ctl(int phase, Bufs<D>* _
       break;
     }
     case kSelect: {
-      if (o.tensor && o.handover > 0.0) {  // precision form: every active residual small enough
+      if (o.tensor && o.handover > 0.0) {
+        // precision form: hand over to FP64 once every active occupied band's residual is
+        // below the threshold, or when the largest active residual has stopped falling
+        // for three iterations (the BF16x3 products' noise floor), or after half of the
+        // iteration budget
         if (threadIdx.x == 0) {
-          double mx = 0.0;
-          for (int j = 0; j < c.nact; ++j) mx = fmax(mx, b.rnorm[j]);
-          if (mx < o.handover * o.handover) c.status = 2;
+          double mx = 0.0, mx_occ = 0.0;
+          for (int j = 0; j < c.nact; ++j) {
+            mx = fmax(mx, b.rnorm[j]);
+            if (b.active[j] < o.occupied) mx_occ = fmax(mx_occ, b.rnorm[j]);
+          }
+          bool hand = mx_occ < o.handover * o.handover;
+          if (mx < c.best_res) {
+            c.best_res = mx;
+            c.stall = 0;
+          } else if (++c.stall >= 3) {
+            hand = true;
+          }
+          if (c.iterations >= max(2, o.max_iterations / 2)) hand = true;
+          if (hand) c.status = 2;
         }
         __syncthreads();
         if (c.status != 0) break;
@@ -1042,7 +1069,13 @@ __global__ void __launch_bounds__(kCtlThreads, 1) k_dv_ctl(int phase, Bufs<D>* _
     }
     case kExtendPost: {
       bool repair = c.need_repair != 0;
-      if (!repair && c.wc_m1 > c.wc_m0) repair = werr() != 0;
+      if (!repair && c.wc_m1 > c.wc_m0) {
+        if (werr() & wide::kWErrBarrier) {
+          set_err(kErrTimeout);
+          break;
+        }
+        repair = werr() != 0;
+      }
       clear_request();
       extend_tail(repair);
       break;
@@ -1149,6 +1182,10 @@ __global__ void __launch_bounds__(kCtlThreads, 1) k_dv_ctl(int phase, Bufs<D>* _
     }
     case kApplyPost: {
       if (c.wc_m1 > c.wc_m0) {
+        if (werr() & wide::kWErrBarrier) {
+          set_err(kErrTimeout);
+          break;
+        }
         if (werr()) {
           set_err(kErrRepairDependent);
           break;
@@ -1177,6 +1214,10 @@ __global__ void __launch_bounds__(kCtlThreads, 1) k_dv_ctl(int phase, Bufs<D>* _
     }
     case kFinishPost: {
       if (c.we_m) {
+        if (werr() & wide::kWErrBarrier) {
+          set_err(kErrTimeout);
+          break;
+        }
         if (werr()) {
           set_err(kErrEigen);
           break;
@@ -1274,6 +1315,7 @@ const char* error_text(int id) {
     case kErrCapacity: return "capacity cannot hold the active correction block; use at least 2*bands";
     case kErrRepairDependent: return "reference overlap remains dependent after repair";
     case kErrEigen: return "reference reduced eigensolve failed";
+    case kErrTimeout: return "a grid barrier of the many-block reduced problem gave up";
     default: return "reference Davidson failed";
   }
 }
@@ -1616,6 +1658,7 @@ int KsetSolver<T>::run(const double* const* start, const double* const* diagonal
     c.nact = n;
     c.h_calls = 1;
     c.h_columns = n;
+    c.best_res = 1e300;
     const Bufs<D>& b = hb_[k];
     dy[k] = DynCols{reinterpret_cast<const double*>(b.V), reinterpret_cast<double*>(b.HV), n,
                     ks_->gamma ? (n + 1) / 2 : n};
@@ -1693,6 +1736,20 @@ int KsetSolver<T>::run(const double* const* start, const double* const* diagonal
     st.contractions = c.contractions;
     st.dropped = c.dropped;
     if (stats) stats[k] = st;
+  }
+  // the tensor-core products' pipelines (bounded waits) must not have given up
+  if (o_.tensor && tc_ready_) {
+    int words[2] = {0, 0};
+    if ((rc = cuda(cudaMemcpy(&words[0], tc_err_, sizeof(int), cudaMemcpyDeviceToHost), "tensor error word")))
+      return rc;
+    if (tcnl_.err && (rc = cuda(cudaMemcpy(&words[1], tcnl_.err, sizeof(int), cudaMemcpyDeviceToHost), "tensor error word")))
+      return rc;
+    if (words[0] || words[1]) {
+      cudaMemset(tc_err_, 0, sizeof(int));
+      if (tcnl_.err) cudaMemset(tcnl_.err, 0, sizeof(int));
+      err_ = "a tensor-core product's pipeline wait gave up";
+      return BG_ETIMEOUT;
+    }
   }
   // a non-finite block met by the applies
   for (int k = 0; k < nk_; ++k) {

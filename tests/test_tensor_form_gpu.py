@@ -72,8 +72,9 @@ def test_tensor_davidson_hands_over_to_fp64(ctx):
     (ref,) = DV.solve_kset(ks, [start], [diag], DV.Options(**base))
     (ten,) = DV.solve_kset(ks, [start], [diag], DV.Options(**base, apply_precision="tensor"))
     assert ten.tensor_iterations >= 1
+    assert ten.converged[:128].sum() >= ref.converged[:128].sum() - 4
     conv = ten.converged[:128] & ref.converged[:128]
-    assert conv.sum() >= 120
+    assert conv.sum() >= 64
     assert np.max(np.abs(ten.eigenvalues[:128][conv] - ref.eigenvalues[:128][conv])) < 1e-8
 
 
