@@ -1577,7 +1577,7 @@ int KsetSolver<T>::prepare() {
   }
   if (wide_) {
     if ((rc = wide::prepare<D>(cap, &coop_blocks_, &err_))) return rc;
-    if ((rc = alloc(&d_bar_, 2)) || (rc = alloc(&d_wpart_, (size_t)coop_blocks_))) return rc;
+    if ((rc = alloc(&d_bar_, 2)) || (rc = alloc(&d_wpart_, 2 * (size_t)coop_blocks_))) return rc;
   }
   if ((rc = alloc(&d_bufs_, nk_)) || (rc = alloc(&d_ctl_, nk_)) || (rc = alloc(&d_nn_, (size_t)kNnSlots * nk_)) ||
       (rc = alloc(&d_tn_, (size_t)kTnSlots * nk_)) || (rc = alloc(&d_cp_, (size_t)kCpSlots * nk_)) ||
@@ -1788,7 +1788,8 @@ int reduced_eigh(int m, const double* S, const double* H, double* w, double* C, 
   bool ok = alloc(&b.S, cc) && alloc(&b.Hr, cc) && alloc(&b.L, cc) && alloc(&b.C, cc) && alloc(&b.A, cc) &&
             alloc(&b.Y, cc) && alloc(&b.Q, cc) && alloc(&b.Z, cc) && alloc(&b.LT, cc) && alloc(&b.lu, 4 * cc) &&
             alloc(&b.w, cap) && alloc(&b.td, cap) && alloc(&b.te, cap) && alloc(&b.e2, cap) && alloc(&b.wu, cap) &&
-            alloc(&b.off, cap) && alloc(&b.ph, cap) && alloc(&b.hp, cap) && alloc(&b.starts, cap + 1) &&
+            alloc(&b.off, cap) && alloc(&b.ph, cap) && alloc(&b.hp, cap) && alloc(&b.hq, cap) &&
+            alloc(&b.starts, cap + 1) &&
             alloc(&b.clusters, cap + 1) && alloc(&b.order, cap) && alloc(&b.werr, 1) && alloc(&b.wmeta, 8) &&
             alloc(&b.wimeta, 8);
   Bufs<D>* d_b = nullptr;
@@ -1803,7 +1804,7 @@ int reduced_eigh(int m, const double* S, const double* H, double* w, double* C, 
   }
   int rc = wide::prepare<D>(cap, &blocks, err);
   if (rc) return rc;
-  if (!alloc(&part, (size_t)blocks)) {
+  if (!alloc(&part, 2 * (size_t)blocks)) {
     *err = "cudaMalloc failed";
     return BG_ENOMEM;
   }

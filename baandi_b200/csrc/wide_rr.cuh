@@ -40,6 +40,14 @@ enum : int { kWErrNonfinite = 1, kWErrBarrier = 2, kWErrPivot = 4 };
 enum : int { kSolveBorder = 0, kSolveLeft, kSolveRight, kSolveBack };
 
 // All blocks of a cooperative launch meet here; false once any barrier has given up.
+// Arrival by an acquire-release add on bar[0]; the last arrival resets it and releases the
+// generation word bar[1], on which the others spin (acquire loads, bounded).
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
 __device__ __forceinline__ bool grid_sync(unsigned* bar, int* err) {
   __shared__ int s_ok;
   __syncthreads();
@@ -48,26 +56,24 @@ __device__ __forceinline__ bool grid_sync(unsigned* bar, int* err) {
     if (*(volatile int*)err & kWErrBarrier) {
       ok = 0;
     } else {
-      volatile unsigned* vgen = bar + 1;
-      const unsigned gen = *vgen;
+      const unsigned gen = ld_acquire_u32(bar + 1);
       __threadfence();
-      const unsigned arrived = atomicAdd(bar, 1u);
+      unsigned arrived;
+      asm volatile("atom.add.acq_rel.gpu.global.u32 %0, [%1], 1;" : "=r"(arrived) : "l"(bar) : "memory");
       if (arrived == gridDim.x - 1) {
-        atomicExch(bar, 0u);
-        __threadfence();
-        atomicAdd(bar + 1, 1u);
+        asm volatile("st.relaxed.gpu.global.u32 [%0], 0;" ::"l"(bar) : "memory");
+        asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(bar + 1), "r"(gen + 1) : "memory");
       } else {
         unsigned spins = 0;
-        while (*vgen == gen) {
+        while (ld_acquire_u32(bar + 1) == gen) {
           if (++spins > kSpinLimit) {
             atomicOr(err, kWErrBarrier);
             ok = 0;
             break;
           }
-          __nanosleep(64);
+          if (spins > 256) __nanosleep(32);
         }
       }
-      __threadfence();
     }
     s_ok = ok;
   }
@@ -321,107 +327,135 @@ __global__ void k_w_prep(const Bufs<D>* __restrict__ bufs, const Ctl* __restrict
   if (bad) atomicOr(b.werr, kWErrNonfinite);
 }
 
-// Householder reduction of the m x m Hermitian A to tridiagonal form; Q <- Q H_k.  Every
-// block owns columns (of the trailing matrix, one warp per column) and rows of Q.
-// Cooperative; shared memory: v and q (cap values each) and the block's partial sums.
+// Householder reduction of the m x m Hermitian A to tridiagonal form; Q <- Q H_t.  One grid
+// barrier per reflector: warp w of the grid owns the global columns j = w (mod warps) of
+// the trailing matrix and the rows r = w (mod warps) of Q (transposed storage), and never
+// shares them.  Step t (L = m - t - 1 trailing rows):
+//   every block holds v_t (from column t after update t - 1, computed locally);
+//   owners form p_j = beta sum_r conj(B[r][j]) v_r for their columns j > t (p and the
+//   partial sums of Re(v^H p) double-buffered by barrier parity) -- grid barrier --;
+//   every block forms K = beta/2 Re(v^H p) and q = p - K v; owners update their columns
+//   j > t + 1 and their rows of Q; column t + 1, which nobody writes in this step, is read
+//   and updated by every block into its next v (and block 0 records its diagonal).
+// d (diagonal) and the off-diagonal alphas come out in td and off.  Cooperative.
 template <class D>
-__global__ void __launch_bounds__(kT) k_w_house(const Bufs<D>* __restrict__ bufs, const Ctl* __restrict__ ctl, int nk,
+__global__ void __launch_bounds__(kT, 1) k_w_house(const Bufs<D>* __restrict__ bufs, const Ctl* __restrict__ ctl, int nk,
                                                 int cap, unsigned* bar, double* part) {
   using X = Cx<D>;
   extern __shared__ __align__(16) unsigned char w_sm[];
-  D* v = reinterpret_cast<D*>(w_sm);
+  D* v = reinterpret_cast<D*>(w_sm);   // reflector of the current step
   D* q = v + cap;
+  D* nx = q + cap;                      // column t + 1 being updated into the next v
   __shared__ double red[kT / 32];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = kT / 32;
   const int gw = blockIdx.x * nw + warp, gwarps = gridDim.x * nw;
+  int parity = 0;   // buffer of p and of the partial sums; alternates at every barrier, across k points
   for (int kk = 0; kk < nk; ++kk) {
     const Ctl c = ctl[kk];
     const Bufs<D> b = bufs[kk];
     if (c.status != 0 || c.we_m == 0 || *(volatile int*)b.werr != 0) continue;   // uniform: set before this launch
     const int m = c.we_m;
     D* A = b.A;
-    for (int col = 0; col + 2 < m; ++col) {
-      const int L = m - col - 1;
-      const D* x = A + (col + 1) + (size_t)col * cap;
+    if (m < 3) continue;
+    // v_0 from column 0 (rows 1..m-1); d_0
+    for (int i = threadIdx.x; i < m - 1; i += kT) v[i] = ldcg(A + 1 + i);
+    if (blockIdx.x == 0 && threadIdx.x == 0) b.td[0] = X::real(ldcg(A));
+    __syncthreads();
+    for (int t = 0; t + 2 < m; ++t) {
+      const int L = m - t - 1;
       double part2 = 0.0;
-      for (int i = threadIdx.x; i < L; i += kT) {
-        const D xi = ldcg(x + i);
-        v[i] = xi;
-        part2 += X::abs2(xi);
-      }
+      for (int i = threadIdx.x; i < L; i += kT) part2 += X::abs2(v[i]);
       part2 = warp_sum_r(part2);
       if (lane == 0) red[warp] = part2;
       __syncthreads();
       double xn2 = 0.0;
       for (int i = 0; i < nw; ++i) xn2 += red[i];
       const double xn = sqrt(xn2);
-      if (xn == 0.0) {  // nothing to reflect; every block saw the same column
-        if (blockIdx.x == 0 && threadIdx.x == 0) b.off[col] = X::zero();
+      const D x0 = v[0];
+      __syncthreads();  // red and v[0] read by every thread
+      const D* ct1 = A + (t + 1) + (size_t)(t + 1) * cap;   // column t + 1, rows t + 1 ..
+      if (xn == 0.0) {  // nothing to reflect (every block saw the same v): no update
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+          b.off[t] = X::zero();
+          b.td[t + 1] = X::real(ldcg(ct1));
+          if (t + 3 == m) b.off[t + 1] = ldcg(ct1 + 1);   // the last coupling
+        }
+        for (int i = threadIdx.x; i + 1 < L; i += kT) v[i] = ldcg(ct1 + 1 + i);
         __syncthreads();
         continue;
       }
-      const D x0 = v[0];
       const double ax0 = X::abs(x0);
       const D phase = ax0 > 0.0 ? X::div(x0, ax0) : X::one();
       const D alpha = X::scale(-xn, phase);
       const double beta = 1.0 / (xn * (xn + ax0));
-      __syncthreads();
       if (threadIdx.x == 0) v[0] = X::sub(x0, alpha);
       __syncthreads();
-      // p_i = beta sum_j conj(B[j][i]) v_j, B = A[col+1:, col+1:]; warp gw owns the global
-      // columns g = gw (mod gwarps), so a column is always read and written by one warp
+      D* pbuf = parity ? b.hq : b.hp;
+      double* pp = part + parity * gridDim.x;
       double pv = 0.0;
-      for (int g = gw; g < m; g += gwarps) {
-        if (g <= col) continue;
-        const int i = g - col - 1;
-        const D* ci = A + (col + 1) + (size_t)g * cap;
+      for (int j = gw; j < m; j += gwarps) {
+        if (j <= t) continue;
+        const int i = j - t - 1;
+        const D* cj = A + (t + 1) + (size_t)j * cap;
         D acc = X::zero();
-        for (int j = lane; j < L; j += 32) acc = X::add(acc, X::mul(X::conj(ci[j]), v[j]));
+        for (int r = lane; r < L; r += 32) acc = X::add(acc, X::mul(X::conj(cj[r]), v[r]));
         acc = warp_sum_d(acc);
         const D pi = X::scale(beta, acc);
         if (lane == 0) {
-          b.hp[i] = pi;
+          pbuf[i] = pi;
           pv += X::dot_re(v[i], pi);
         }
       }
       pv = warp_sum_r(pv);
-      __syncthreads();
       if (lane == 0) red[warp] = pv;
       __syncthreads();
       if (threadIdx.x == 0) {
         double sum = 0.0;
         for (int i = 0; i < nw; ++i) sum += red[i];
-        part[blockIdx.x] = sum;
+        pp[blockIdx.x] = sum;
       }
       if (!grid_sync(bar, b.werr)) return;
       double vp = 0.0;
-      for (int i = 0; i < (int)gridDim.x; ++i) vp += ldcg(part + i);
+      for (int i = 0; i < (int)gridDim.x; ++i) vp += ldcg(pp + i);
       const double K = 0.5 * beta * vp;
-      for (int i = threadIdx.x; i < L; i += kT) q[i] = X::sub(ldcg(b.hp + i), X::scale(K, v[i]));
+      for (int i = threadIdx.x; i < L; i += kT) q[i] = X::sub(ldcg(pbuf + i), X::scale(K, v[i]));
       __syncthreads();
-      // B[:, i] -= v conj(q_i) + q conj(v_i) for the owned columns
-      for (int g = gw; g < m; g += gwarps) {
-        if (g <= col) continue;
-        const int i = g - col - 1;
-        D* ci = A + (col + 1) + (size_t)g * cap;
+      // owned columns j > t + 1: B[:, i] -= v conj(q_i) + q conj(v_i)
+      for (int j = gw; j < m; j += gwarps) {
+        if (j <= t + 1) continue;
+        const int i = j - t - 1;
+        D* cj = A + (t + 1) + (size_t)j * cap;
         const D cq = X::conj(q[i]), cv = X::conj(v[i]);
-        for (int j = lane; j < L; j += 32) ci[j] = X::sub(ci[j], X::add(X::mul(v[j], cq), X::mul(q[j], cv)));
+        for (int r = lane; r < L; r += 32) cj[r] = X::sub(cj[r], X::add(X::mul(v[r], cq), X::mul(q[r], cv)));
       }
-      // Q rows (transposed storage: row r at Q + r cap): row <- row - beta (row . v) v^H
+      // owned rows of Q: row <- row - beta (row . v) v^H
       for (int r = gw; r < m; r += gwarps) {
-        D* row = b.Q + (col + 1) + (size_t)r * cap;
+        D* row = b.Q + (t + 1) + (size_t)r * cap;
         D acc = X::zero();
-        for (int j = lane; j < L; j += 32) acc = X::add(acc, X::mul(row[j], v[j]));
+        for (int jj = lane; jj < L; jj += 32) acc = X::add(acc, X::mul(row[jj], v[jj]));
         acc = X::scale(beta, warp_sum_d(acc));
-        for (int j = lane; j < L; j += 32) row[j] = X::sub(row[j], X::mul(acc, X::conj(v[j])));
+        for (int jj = lane; jj < L; jj += 32) row[jj] = X::sub(row[jj], X::mul(acc, X::conj(v[jj])));
       }
-      if (blockIdx.x == 0 && threadIdx.x == 0) b.off[col] = alpha;
-      if (!grid_sync(bar, b.werr)) return;
+      // column t + 1 after this update, by every block: its diagonal entry and the next v
+      {
+        const D cq = X::conj(q[0]), cv = X::conj(v[0]);
+        for (int r = threadIdx.x; r < L; r += kT)
+          nx[r] = X::sub(ldcg(ct1 + r), X::add(X::mul(v[r], cq), X::mul(q[r], cv)));
+      }
+      __syncthreads();
+      if (blockIdx.x == 0 && threadIdx.x == 0) {
+        b.off[t] = alpha;
+        b.td[t + 1] = X::real(nx[0]);
+        if (t + 3 == m) b.off[t + 1] = nx[1];   // the last coupling is not reflected
+      }
+      for (int i = threadIdx.x; i + 1 < L; i += kT) v[i] = nx[1 + i];
+      __syncthreads();
+      parity ^= 1;
     }
   }
 }
 
-inline size_t house_smem(int cap, size_t dsize) { return 2 * (size_t)cap * dsize; }
+inline size_t house_smem(int cap, size_t dsize) { return 3 * (size_t)cap * dsize; }
 
 // Tridiagonal data: d, |e|, phases s (so that T = diag(s)^H T_c diag(s) is real), splits
 // where a coupling is negligible, squared couplings, the pivmin safeguard.  One block per k.
@@ -433,10 +467,16 @@ __global__ void k_w_tri_setup(const Bufs<D>* __restrict__ bufs, const Ctl* __res
   const Bufs<D> b = bufs[k];
   if (c.status != 0 || c.we_m == 0 || *(volatile int*)b.werr != 0) return;
   const int m = c.we_m;
-  for (int i = threadIdx.x; i < m; i += blockDim.x) b.td[i] = X::real(b.A[i + (size_t)i * cap]);
+  // k_w_house left d[0 .. m-2] and every coupling for m >= 3 (the last diagonal entry is in
+  // A); smaller problems are tridiagonal already
+  if (m < 3) {
+    for (int i = threadIdx.x; i < m; i += blockDim.x) b.td[i] = X::real(b.A[i + (size_t)i * cap]);
+  } else if (threadIdx.x == 0) {
+    b.td[m - 1] = X::real(b.A[(m - 1) + (size_t)(m - 1) * cap]);
+  }
   __syncthreads();
   if (threadIdx.x == 0) {
-    if (m >= 2) b.off[m - 2] = b.A[(m - 1) + (size_t)(m - 2) * cap];
+    if (m == 2) b.off[0] = b.A[1];
     D s = X::one();
     b.ph[0] = s;
     for (int i = 0; i + 1 < m; ++i) {
