@@ -1788,7 +1788,7 @@ int reduced_eigh(int m, const double* S, const double* H, double* w, double* C, 
   bool ok = alloc(&b.S, cc) && alloc(&b.Hr, cc) && alloc(&b.L, cc) && alloc(&b.C, cc) && alloc(&b.A, cc) &&
             alloc(&b.Y, cc) && alloc(&b.Q, cc) && alloc(&b.Z, cc) && alloc(&b.LT, cc) && alloc(&b.lu, 4 * cc) &&
             alloc(&b.w, cap) && alloc(&b.td, cap) && alloc(&b.te, cap) && alloc(&b.e2, cap) && alloc(&b.wu, cap) &&
-            alloc(&b.off, cap) && alloc(&b.ph, cap) && alloc(&b.hp, cap) && alloc(&b.hq, cap) &&
+            alloc(&b.off, cap) && alloc(&b.ph, cap) && alloc(&b.hp, cap) && alloc(&b.hq, cap) && alloc(&b.hv, cap) &&
             alloc(&b.starts, cap + 1) &&
             alloc(&b.clusters, cap + 1) && alloc(&b.order, cap) && alloc(&b.werr, 1) && alloc(&b.wmeta, 8) &&
             alloc(&b.wimeta, 8);

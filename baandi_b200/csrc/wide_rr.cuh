@@ -12,12 +12,13 @@
 //     rule, the rows below and the trailing lower triangle by every block) in one
 //     cooperative launch;
 //   * Householder tridiagonalisation: one cooperative launch, every block owning columns
-//     of the trailing matrix (matrix-vector product and rank-2 update) and rows of the
-//     accumulated unitary factor; two grid barriers per reflector;
+//     of the trailing matrix (matrix-vector product and rank-2 update), one grid barrier
+//     per reflector;
 //   * tridiagonal eigenpairs: Sturm bisection by one warp per eigenvalue, inverse
 //     iteration by one thread per eigenvector, Gram-Schmidt inside clusters of close
 //     eigenvalues by one warp per cluster;
-//   * back-transformation Q diag(s) Z as a tiled product, then the back solve with L^H.
+//   * back-transformation: the stored reflectors applied to diag(s) Z, a warp per column,
+//     then the back solve with L^H.
 // Requests come from the control kernel (Ctl::wc_* and Ctl::we_m); every kernel here
 // returns at once for a k point without one, so the launches sit in the captured
 // iteration graph at fixed shapes.  Grid barriers spin a bounded number of times and
@@ -301,7 +302,7 @@ __global__ void __launch_bounds__(kT) k_w_chol(const Bufs<D>* __restrict__ bufs,
 }
 
 // ------------------------------------------------------------------ eigensolver
-// Finite check, symmetrised rounding of A, Q = I (stored transposed), Z = 0.
+// Finite check, symmetrised rounding of A, Z = 0.
 template <class D>
 __global__ void k_w_prep(const Bufs<D>* __restrict__ bufs, const Ctl* __restrict__ ctl, int cap) {
   using X = Cx<D>;
@@ -321,22 +322,22 @@ __global__ void k_w_prep(const Bufs<D>* __restrict__ bufs, const Ctl* __restrict
       b.A[i + (size_t)j * cap] = avg;
       b.A[j + (size_t)i * cap] = X::conj(avg);
     }
-    b.Q[i + (size_t)j * cap] = i == j ? X::one() : X::zero();
     b.Z[i + (size_t)j * cap] = 0.0;
   }
   if (bad) atomicOr(b.werr, kWErrNonfinite);
 }
 
-// Householder reduction of the m x m Hermitian A to tridiagonal form; Q <- Q H_t.  One grid
-// barrier per reflector: warp w of the grid owns the global columns j = w (mod warps) of
-// the trailing matrix and the rows r = w (mod warps) of Q (transposed storage), and never
-// shares them.  Step t (L = m - t - 1 trailing rows):
+// Householder reduction of the m x m Hermitian A to tridiagonal form, A = Q T Q^H with
+// Q = H_0 H_1 ... H_{m-3}, H_t = I - beta_t v_t v_t^H (v_t in column t of Q below the
+// diagonal, beta_t in hv[t]).  One grid barrier per reflector: warp w of the grid owns the
+// global columns j = w (mod warps) of the trailing matrix and never shares them.  Step t
+// (L = m - t - 1 trailing rows):
 //   every block holds v_t (from column t after update t - 1, computed locally);
 //   owners form p_j = beta sum_r conj(B[r][j]) v_r for their columns j > t (p and the
 //   partial sums of Re(v^H p) double-buffered by barrier parity) -- grid barrier --;
 //   every block forms K = beta/2 Re(v^H p) and q = p - K v; owners update their columns
-//   j > t + 1 and their rows of Q; column t + 1, which nobody writes in this step, is read
-//   and updated by every block into its next v (and block 0 records its diagonal).
+//   j > t + 1; column t + 1, which nobody writes in this step, is read and updated by
+//   every block into its next v (and block 0 records its diagonal and the reflector).
 // d (diagonal) and the off-diagonal alphas come out in td and off.  Cooperative.
 template <class D>
 __global__ void __launch_bounds__(kT, 1) k_w_house(const Bufs<D>* __restrict__ bufs, const Ctl* __restrict__ ctl, int nk,
@@ -376,6 +377,7 @@ __global__ void __launch_bounds__(kT, 1) k_w_house(const Bufs<D>* __restrict__ b
       const D* ct1 = A + (t + 1) + (size_t)(t + 1) * cap;   // column t + 1, rows t + 1 ..
       if (xn == 0.0) {  // nothing to reflect (every block saw the same v): no update
         if (blockIdx.x == 0 && threadIdx.x == 0) {
+          b.hv[t] = X::zero();   // identity reflector
           b.off[t] = X::zero();
           b.td[t + 1] = X::real(ldcg(ct1));
           if (t + 3 == m) b.off[t + 1] = ldcg(ct1 + 1);   // the last coupling
@@ -428,13 +430,10 @@ __global__ void __launch_bounds__(kT, 1) k_w_house(const Bufs<D>* __restrict__ b
         const D cq = X::conj(q[i]), cv = X::conj(v[i]);
         for (int r = lane; r < L; r += 32) cj[r] = X::sub(cj[r], X::add(X::mul(v[r], cq), X::mul(q[r], cv)));
       }
-      // owned rows of Q: row <- row - beta (row . v) v^H
-      for (int r = gw; r < m; r += gwarps) {
-        D* row = b.Q + (t + 1) + (size_t)r * cap;
-        D acc = X::zero();
-        for (int jj = lane; jj < L; jj += 32) acc = X::add(acc, X::mul(row[jj], v[jj]));
-        acc = X::scale(beta, warp_sum_d(acc));
-        for (int jj = lane; jj < L; jj += 32) row[jj] = X::sub(row[jj], X::mul(acc, X::conj(v[jj])));
+      // reflector t (v and beta) kept for the back-transformation: v in column t of Q
+      if (blockIdx.x == 0) {
+        for (int r = threadIdx.x; r < L; r += kT) b.Q[(t + 1 + r) + (size_t)t * cap] = v[r];
+        if (threadIdx.x == 0) b.hv[t] = X::from_real(beta);
       }
       // column t + 1 after this update, by every block: its diagonal entry and the next v
       {
@@ -749,51 +748,55 @@ __global__ void __launch_bounds__(kT) k_w_tri_gs(const Bufs<D>* __restrict__ buf
   }
 }
 
-// Y[r][c] = sum_q Q(r, q) s_q Z[q][order[c]] (r, c < m); 32 x 32 output tiles, q in
-// steps of 16 staged in shared memory.  Q is stored transposed (Q(r, q) at Q[q + r cap]).
+// Y[:, c] = H_0 H_1 ... H_{m-3} (s . Z[:, order[c]]) for c < m: kBackCols columns per
+// block, one warp per column; each reflector is staged once per block in shared memory
+// (double-buffered, one barrier per reflector) and applied by every warp to its column.
+constexpr int kBackCols = 6;  // (6 + 2) x 1536 x 16 bytes of shared memory at the largest capacity
 template <class D>
 __global__ void __launch_bounds__(kT) k_w_back(const Bufs<D>* __restrict__ bufs, const Ctl* __restrict__ ctl, int cap) {
   using X = Cx<D>;
-  const int k = blockIdx.z;
+  const int k = blockIdx.y;
   const Ctl c = ctl[k];
   const Bufs<D> b = bufs[k];
   if (c.status != 0 || c.we_m == 0 || *(volatile int*)b.werr != 0) return;
   const int m = c.we_m;
-  const int r0 = blockIdx.x * 32, c0 = blockIdx.y * 32;
-  if (r0 >= m || c0 >= m) return;
-  __shared__ D qs[32][17];
-  __shared__ D zs[16][33];
-  __shared__ int ord[32];
-  if (threadIdx.x < 32) ord[threadIdx.x] = c0 + threadIdx.x < m ? b.order[c0 + threadIdx.x] : 0;
-  const int tr = threadIdx.x % 32, tc = threadIdx.x / 32;  // rows tr, columns tc + 8 u
-  D acc[4] = {X::zero(), X::zero(), X::zero(), X::zero()};
+  const int c0 = blockIdx.x * kBackCols;
+  if (c0 >= m) return;
+  extern __shared__ __align__(16) unsigned char w_sm[];
+  D* z = reinterpret_cast<D*>(w_sm);          // [kBackCols][cap]
+  D* vb = z + (size_t)kBackCols * cap;        // two reflector buffers of cap
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int col = c0 + warp;
+  const bool act = warp < kBackCols && col < m;
+  D* zc = z + (size_t)warp * cap;
+  if (act) {
+    const int src = b.order[col];
+    for (int r = lane; r < m; r += 32) zc[r] = X::scale(b.Z[(size_t)r * cap + src], b.ph[r]);
+  }
+  const int last = m - 3;
+  if (last >= 0)
+    for (int r = threadIdx.x; r < m - last - 1; r += kT) vb[r] = b.Q[(last + 1 + r) + (size_t)last * cap];
   __syncthreads();
-  for (int q0 = 0; q0 < m; q0 += 16) {
-    for (int t = threadIdx.x; t < 32 * 16; t += kT) {
-      const int rr = t / 16, qq = t % 16;
-      const int r = r0 + rr, q = q0 + qq;
-      qs[rr][qq] = (r < m && q < m) ? b.Q[q + (size_t)r * cap] : X::zero();
-    }
-    for (int t = threadIdx.x; t < 16 * 32; t += kT) {
-      const int qq = t / 32, cc = t % 32;
-      const int q = q0 + qq, col = c0 + cc;
-      zs[qq][cc] = (q < m && col < m) ? X::scale(b.Z[(size_t)q * cap + ord[cc]], b.ph[q]) : X::zero();
-    }
-    __syncthreads();
-#pragma unroll 4
-    for (int qq = 0; qq < 16; ++qq) {
-      const D a = qs[tr][qq];
-#pragma unroll
-      for (int u = 0; u < 4; ++u) acc[u] = X::add(acc[u], X::mul(a, zs[qq][tc + 8 * u]));
+  for (int t = last, buf = 0; t >= 0; --t, buf ^= 1) {
+    const int L = m - t - 1;
+    const D* v = vb + (size_t)buf * cap;
+    // stage the next reflector into the other buffer while this one is applied
+    if (t > 0)
+      for (int r = threadIdx.x; r < L + 1; r += kT) vb[(size_t)(buf ^ 1) * cap + r] = b.Q[(t + r) + (size_t)(t - 1) * cap];
+    const double beta = X::real(b.hv[t]);
+    if (act && beta != 0.0) {
+      D acc = X::zero();
+      for (int r = lane; r < L; r += 32) acc = X::add(acc, X::mul(X::conj(v[r]), zc[t + 1 + r]));
+      acc = X::scale(beta, warp_sum_d(acc));
+      for (int r = lane; r < L; r += 32) zc[t + 1 + r] = X::sub(zc[t + 1 + r], X::mul(v[r], acc));
     }
     __syncthreads();
   }
-#pragma unroll
-  for (int u = 0; u < 4; ++u) {
-    const int r = r0 + tr, col = c0 + tc + 8 * u;
-    if (r < m && col < m) b.Y[r + (size_t)col * cap] = acc[u];
-  }
+  if (act)
+    for (int r = lane; r < m; r += 32) b.Y[r + (size_t)col * cap] = zc[r];
 }
+
+inline size_t back_smem(int cap, size_t dsize) { return ((size_t)kBackCols + 2) * cap * dsize; }
 
 // LT = L^H (m x m).
 template <class D>
@@ -817,6 +820,9 @@ int prepare(int cap, int* coop_blocks, std::string* err) {
   const int tsm = (int)trsm_smem(cap, sizeof(D));
   cudaError_t e = cudaFuncSetAttribute((const void*)k_w_house<D>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)house_smem(cap, sizeof(D)));
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute((const void*)k_w_back<D>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)back_smem(cap, sizeof(D)));
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute((const void*)k_w_trsm<D, kSolveBorder>, cudaFuncAttributeMaxDynamicSharedMemorySize, tsm);
   if (e == cudaSuccess)
@@ -877,8 +883,8 @@ int64_t launch_eig(Bufs<D>* bufs, Ctl* ctl, int nk, int cap, int coop_blocks, un
   k_w_tri_clusters<D><<<dim3(1, (unsigned)nk), 256, 0, s>>>(bufs, ctl);
   k_w_tri_vectors<D><<<dim3((unsigned)((cap + 63) / 64), (unsigned)nk), 64, 0, s>>>(bufs, ctl, cap);
   k_w_tri_gs<D><<<gw, kT, 0, s>>>(bufs, ctl, cap);
-  const unsigned t32 = (unsigned)((cap + 31) / 32);
-  k_w_back<D><<<dim3(t32, t32, (unsigned)nk), kT, 0, s>>>(bufs, ctl, cap);
+  k_w_back<D><<<dim3((unsigned)((cap + kBackCols - 1) / kBackCols), (unsigned)nk), kT, back_smem(cap, sizeof(D)), s>>>(
+      bufs, ctl, cap);
   k_w_adjoint<D><<<dim3(256, (unsigned)nk), 256, 0, s>>>(bufs, ctl, cap);
   k_w_trsm<D, kSolveBack><<<gs, kT, tsm, s>>>(bufs, ctl, cap);
   return 12;
