@@ -1918,9 +1918,9 @@ extern "C" int bg_kset_davidson_solve(bg_kset* ks, const double* const* start, c
   op.tensor = o.apply_precision == BG_PREC_TENSOR ? 1 : 0;
   op.handover = op.tensor ? kHandoverResidual : 0.0;
   const bool graph = (o.flags & 1) == 0;
-  // the reduced problem on many blocks beyond capacity 128 (flags bit 1 forces it, bit 2
-  // keeps the one-block control kernel)
-  const bool wide = (o.flags & 2) != 0 || (cap > 128 && (o.flags & 4) == 0);
+  // the reduced problem on many blocks for capacities 129 .. 1152 (flags bit 1 forces it,
+  // bit 2 keeps the one-block control kernel)
+  const bool wide = (o.flags & 2) != 0 || (cap > 128 && cap <= wide::kMaxCap && (o.flags & 4) == 0);
   int rc;
   if (o.apply_precision != BG_PREC_FP64)  // the FP32 potential copies, on the set's stream
     for (bg_op* kop : ks->ops)
@@ -1986,7 +1986,7 @@ extern "C" int bg_reduced_eigh(bg_ctx* ctx, int64_t m, int32_t is_complex, const
                                double* eigenvalues, double* vectors, double* device_ms) {
   if (!ctx) return fail(nullptr, BG_EINVAL, "null context");
   if (!s || !h || !eigenvalues || !vectors) return fail(ctx, BG_EINVAL, "null argument");
-  if (m < 1 || m > 1536) return fail(ctx, BG_ESHAPE, "reduced problem size must be in [1, 1536]");
+  if (m < 1 || m > wide::kMaxCap) return fail(ctx, BG_ESHAPE, "reduced problem size must be in [1, 1152]");
   const size_t n = (size_t)m * m * (is_complex ? 2 : 1);
   for (size_t i = 0; i < n; ++i)
     if (!std::isfinite(s[i]) || !std::isfinite(h[i])) return fail(ctx, BG_ENONFINITE, "non-finite pencil");

@@ -36,6 +36,7 @@ constexpr int kPanel = 32;              // Cholesky panel width
 constexpr int kTile = 16;               // tiles of the border product
 constexpr double kWideOrtol = 1e-6;     // cluster gap relative to the block's 1-norm
 constexpr unsigned kSpinLimit = 1u << 24;
+constexpr int kMaxCap = 1152;           // the Householder kernel's columns fit in shared memory
 
 enum : int { kWErrNonfinite = 1, kWErrBarrier = 2, kWErrPivot = 4 };
 enum : int { kSolveBorder = 0, kSolveLeft, kSolveRight, kSolveBack };
@@ -329,27 +330,30 @@ __global__ void k_w_prep(const Bufs<D>* __restrict__ bufs, const Ctl* __restrict
 
 // Householder reduction of the m x m Hermitian A to tridiagonal form, A = Q T Q^H with
 // Q = H_0 H_1 ... H_{m-3}, H_t = I - beta_t v_t v_t^H (v_t in column t of Q below the
-// diagonal, beta_t in hv[t]).  One grid barrier per reflector: warp w of the grid owns the
-// global columns j = w (mod warps) of the trailing matrix and never shares them.  Step t
-// (L = m - t - 1 trailing rows):
-//   every block holds v_t (from column t after update t - 1, computed locally);
-//   owners form p_j = beta sum_r conj(B[r][j]) v_r for their columns j > t (p and the
-//   partial sums of Re(v^H p) double-buffered by barrier parity) -- grid barrier --;
+// diagonal, beta_t in hv[t]).  One grid barrier per reflector.  Block b owns the columns
+// j = b (mod blocks) of A and keeps them in shared memory (slot j / blocks), so the
+// matrix-vector products and rank-2 updates of the trailing matrix never leave the SM;
+// warp w of a block works on its slots w, w + 8, ...  Step t (L = m - t - 1 rows):
+//   every block holds v_t (column t after update t - 1, formed locally);
+//   owners form p_j = beta sum_r conj(B[r][j]) v_r for their columns j > t and write p
+//   and their partial sums of Re(v^H p) (double-buffered by barrier parity) -- barrier --;
 //   every block forms K = beta/2 Re(v^H p) and q = p - K v; owners update their columns
-//   j > t + 1; column t + 1, which nobody writes in this step, is read and updated by
-//   every block into its next v (and block 0 records its diagonal and the reflector).
-// d (diagonal) and the off-diagonal alphas come out in td and off.  Cooperative.
+//   j > t + 1, and the owner of column t + 2 writes it to A for every block to read at the
+//   next step; column t + 1 (not updated by its owner in this step) is read from A and
+//   updated by every block into its next v.  Block 0 records d, the couplings and the
+//   reflectors.  At the end the owners write their columns back to A.  Cooperative.
 template <class D>
-__global__ void __launch_bounds__(kT, 1) k_w_house(const Bufs<D>* __restrict__ bufs, const Ctl* __restrict__ ctl, int nk,
-                                                int cap, unsigned* bar, double* part) {
+__global__ void __launch_bounds__(kT, 1) k_w_house(const Bufs<D>* __restrict__ bufs, const Ctl* __restrict__ ctl,
+                                                   int nk, int cap, int slots, unsigned* bar, double* part) {
   using X = Cx<D>;
   extern __shared__ __align__(16) unsigned char w_sm[];
   D* v = reinterpret_cast<D*>(w_sm);   // reflector of the current step
   D* q = v + cap;
   D* nx = q + cap;                      // column t + 1 being updated into the next v
+  D* own = nx + cap;                    // owned columns: slot s at own + s cap
   __shared__ double red[kT / 32];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = kT / 32;
-  const int gw = blockIdx.x * nw + warp, gwarps = gridDim.x * nw;
+  const int G = gridDim.x;
   int parity = 0;   // buffer of p and of the partial sums; alternates at every barrier, across k points
   for (int kk = 0; kk < nk; ++kk) {
     const Ctl c = ctl[kk];
@@ -358,7 +362,12 @@ __global__ void __launch_bounds__(kT, 1) k_w_house(const Bufs<D>* __restrict__ b
     const int m = c.we_m;
     D* A = b.A;
     if (m < 3) continue;
-    // v_0 from column 0 (rows 1..m-1); d_0
+    // owned columns into shared memory; v_0 from column 0 (rows 1..m-1); d_0
+    for (int s = 0; s < slots; ++s) {
+      const int j = blockIdx.x + G * s;
+      if (j >= m) break;
+      for (int r = threadIdx.x; r < m; r += kT) own[(size_t)s * cap + r] = ldcg(A + r + (size_t)j * cap);
+    }
     for (int i = threadIdx.x; i < m - 1; i += kT) v[i] = ldcg(A + 1 + i);
     if (blockIdx.x == 0 && threadIdx.x == 0) b.td[0] = X::real(ldcg(A));
     __syncthreads();
@@ -375,7 +384,12 @@ __global__ void __launch_bounds__(kT, 1) k_w_house(const Bufs<D>* __restrict__ b
       const D x0 = v[0];
       __syncthreads();  // red and v[0] read by every thread
       const D* ct1 = A + (t + 1) + (size_t)(t + 1) * cap;   // column t + 1, rows t + 1 ..
+      const int o2 = t + 2 < m ? (t + 2) % G : -1;            // owner block of column t + 2
       if (xn == 0.0) {  // nothing to reflect (every block saw the same v): no update
+        if ((int)blockIdx.x == o2) {
+          const D* src = own + (size_t)((t + 2) / G) * cap;
+          for (int r = threadIdx.x; r < L - 1; r += kT) A[(t + 2 + r) + (size_t)(t + 2) * cap] = src[t + 2 + r];
+        }
         if (blockIdx.x == 0 && threadIdx.x == 0) {
           b.hv[t] = X::zero();   // identity reflector
           b.off[t] = X::zero();
@@ -383,7 +397,7 @@ __global__ void __launch_bounds__(kT, 1) k_w_house(const Bufs<D>* __restrict__ b
           if (t + 3 == m) b.off[t + 1] = ldcg(ct1 + 1);   // the last coupling
         }
         for (int i = threadIdx.x; i + 1 < L; i += kT) v[i] = ldcg(ct1 + 1 + i);
-        __syncthreads();
+        if (!grid_sync(bar, b.werr)) return;   // column t + 2 written before it is read
         continue;
       }
       const double ax0 = X::abs(x0);
@@ -393,12 +407,13 @@ __global__ void __launch_bounds__(kT, 1) k_w_house(const Bufs<D>* __restrict__ b
       if (threadIdx.x == 0) v[0] = X::sub(x0, alpha);
       __syncthreads();
       D* pbuf = parity ? b.hq : b.hp;
-      double* pp = part + parity * gridDim.x;
+      double* pp = part + parity * G;
       double pv = 0.0;
-      for (int j = gw; j < m; j += gwarps) {
-        if (j <= t) continue;
+      for (int s = warp; s < slots; s += nw) {
+        const int j = blockIdx.x + G * s;
+        if (j >= m || j <= t) continue;
         const int i = j - t - 1;
-        const D* cj = A + (t + 1) + (size_t)j * cap;
+        const D* cj = own + (size_t)s * cap + (t + 1);
         D acc = X::zero();
         for (int r = lane; r < L; r += 32) acc = X::add(acc, X::mul(X::conj(cj[r]), v[r]));
         acc = warp_sum_d(acc);
@@ -418,17 +433,22 @@ __global__ void __launch_bounds__(kT, 1) k_w_house(const Bufs<D>* __restrict__ b
       }
       if (!grid_sync(bar, b.werr)) return;
       double vp = 0.0;
-      for (int i = 0; i < (int)gridDim.x; ++i) vp += ldcg(pp + i);
+      for (int i = 0; i < G; ++i) vp += ldcg(pp + i);
       const double K = 0.5 * beta * vp;
       for (int i = threadIdx.x; i < L; i += kT) q[i] = X::sub(ldcg(pbuf + i), X::scale(K, v[i]));
       __syncthreads();
-      // owned columns j > t + 1: B[:, i] -= v conj(q_i) + q conj(v_i)
-      for (int j = gw; j < m; j += gwarps) {
-        if (j <= t + 1) continue;
+      // owned columns j > t + 1: B[:, i] -= v conj(q_i) + q conj(v_i); column t + 2 to A
+      for (int s = warp; s < slots; s += nw) {
+        const int j = blockIdx.x + G * s;
+        if (j >= m || j <= t + 1) continue;
         const int i = j - t - 1;
-        D* cj = A + (t + 1) + (size_t)j * cap;
+        D* cj = own + (size_t)s * cap + (t + 1);
         const D cq = X::conj(q[i]), cv = X::conj(v[i]);
         for (int r = lane; r < L; r += 32) cj[r] = X::sub(cj[r], X::add(X::mul(v[r], cq), X::mul(q[r], cv)));
+        if (j == t + 2) {
+          __syncwarp();
+          for (int r = lane + 1; r < L; r += 32) A[(t + 1 + r) + (size_t)j * cap] = cj[r];
+        }
       }
       // reflector t (v and beta) kept for the back-transformation: v in column t of Q
       if (blockIdx.x == 0) {
@@ -451,10 +471,22 @@ __global__ void __launch_bounds__(kT, 1) k_w_house(const Bufs<D>* __restrict__ b
       __syncthreads();
       parity ^= 1;
     }
+    // owned columns back to A (the last diagonal entry is read from there)
+    for (int s = 0; s < slots; ++s) {
+      const int j = blockIdx.x + G * s;
+      if (j >= m) break;
+      for (int r = threadIdx.x; r < m; r += kT) A[r + (size_t)j * cap] = own[(size_t)s * cap + r];
+    }
+    if (!grid_sync(bar, b.werr)) return;   // before the next k point reuses the buffers
   }
 }
 
-inline size_t house_smem(int cap, size_t dsize) { return 3 * (size_t)cap * dsize; }
+// Columns per block of the Householder kernel and its shared memory (three vectors and
+// the owned columns).
+inline int house_slots(int cap, int blocks) { return (cap + blocks - 1) / blocks; }
+inline size_t house_smem(int cap, int blocks, size_t dsize) {
+  return ((size_t)house_slots(cap, blocks) + 3) * cap * dsize;
+}
 
 // Tridiagonal data: d, |e|, phases s (so that T = diag(s)^H T_c diag(s) is real), splits
 // where a coupling is negligible, squared couplings, the pivmin safeguard.  One block per k.
@@ -818,8 +850,16 @@ __global__ void k_w_adjoint(const Bufs<D>* __restrict__ bufs, const Ctl* __restr
 template <class D>
 int prepare(int cap, int* coop_blocks, std::string* err) {
   const int tsm = (int)trsm_smem(cap, sizeof(D));
-  cudaError_t e = cudaFuncSetAttribute((const void*)k_w_house<D>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)house_smem(cap, sizeof(D)));
+  int dev0 = 0, sms0 = 0;
+  cudaError_t e = cudaGetDevice(&dev0);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms0, cudaDevAttrMultiProcessorCount, dev0);
+  if (e == cudaSuccess && house_smem(cap, std::max(sms0, 1), sizeof(D)) > 220 * 1024) {
+    *err = "the many-block reduced problem keeps its columns in shared memory: capacity too large for this GPU";
+    return BG_EINVAL;
+  }
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute((const void*)k_w_house<D>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)house_smem(cap, std::max(sms0, 1), sizeof(D)));
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute((const void*)k_w_back<D>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)back_smem(cap, sizeof(D)));
@@ -835,7 +875,7 @@ int prepare(int cap, int* coop_blocks, std::string* err) {
   if (e == cudaSuccess) e = cudaGetDevice(&dev);
   if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   if (e == cudaSuccess)
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_h, k_w_house<D>, kT, house_smem(cap, sizeof(D)));
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_h, k_w_house<D>, kT, house_smem(cap, sms, sizeof(D)));
   if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_c, k_w_chol<D>, kT, 0);
   if (e != cudaSuccess) {
     *err = std::string("many-block reduced problem: ") + cudaGetErrorString(e);
@@ -876,8 +916,8 @@ int64_t launch_eig(Bufs<D>* bufs, Ctl* ctl, int nk, int cap, int coop_blocks, un
   k_w_trsm<D, kSolveLeft><<<gs, kT, tsm, s>>>(bufs, ctl, cap);
   k_w_trsm<D, kSolveRight><<<gs, kT, tsm, s>>>(bufs, ctl, cap);
   k_w_prep<D><<<dim3(256, (unsigned)nk), 256, 0, s>>>(bufs, ctl, cap);
-  coop_launch(k_w_house<D>, coop_blocks, house_smem(cap, sizeof(D)), s, (const Bufs<D>*)bufs, (const Ctl*)ctl, nk,
-              cap, bar, part);
+  coop_launch(k_w_house<D>, coop_blocks, house_smem(cap, coop_blocks, sizeof(D)), s, (const Bufs<D>*)bufs,
+              (const Ctl*)ctl, nk, cap, house_slots(cap, coop_blocks), bar, part);
   k_w_tri_setup<D><<<dim3(1, (unsigned)nk), 256, 0, s>>>(bufs, ctl, cap);
   k_w_tri_values<D><<<gw, kT, 0, s>>>(bufs, ctl);
   k_w_tri_clusters<D><<<dim3(1, (unsigned)nk), 256, 0, s>>>(bufs, ctl);

@@ -351,8 +351,8 @@ int bg_davidson_solve(bg_op* op, const double* start, const double* diagonal,
  * 798-1082).  Every large product is one launch over all k points, the reduced problem
  * (bordered Cholesky, Householder tridiagonalisation, tridiagonal eigenpairs) and the
  * control decisions (contraction, dropped corrections, repair, convergence) run in a
- * one-block-per-k-point kernel -- beyond capacity 128 the factor and the eigensolve run
- * on many blocks (cooperative launches, bg_reduced_eigh) -- and one iteration is a CUDA
+ * one-block-per-k-point kernel -- at capacities 129 .. 1152 the factor and the eigensolve
+ * run on many blocks (cooperative launches, bg_reduced_eigh) -- and one iteration is a CUDA
  * graph replayed until all k points finish.  Per-k arrays (nk = set size): start[k] rows_k x bands, diagonal[k]
  * rows_k, eigenvalues[k] bands, eigenvectors[k] rows_k x bands, converged[k] bands;
  * start/diagonal/eigenvectors have ptr_kind (eigenvalues and converged are host);
@@ -367,7 +367,7 @@ int bg_kset_davidson_solve(bg_kset* set, const double* const* start, const doubl
                            double* const* eigenvectors, int32_t* const* converged, bg_davidson_stats* stats);
 
 /* The generalised Hermitian eigenproblem H C = S C diag(w) of one m x m pencil (m <=
- * 1536; column-major host matrices, interleaved complex when is_complex), solved the way
+ * 1152; column-major host matrices, interleaved complex when is_complex), solved the way
  * bg_kset_davidson_solve solves its reduced problem beyond capacity 128: the Cholesky
  * factor of S with the reference's pivot rule (squared pivot over the overlap diagonal
  * >= eps / 1e-12, crates/dft-solvers/src/lean_davidson.rs:62-70), A = L^-1 H L^-H, a
