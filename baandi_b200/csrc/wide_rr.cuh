@@ -141,25 +141,55 @@ __global__ void __launch_bounds__(kT) k_w_trsm(const Bufs<D>* __restrict__ bufs,
   }
   for (int r = threadIdx.x; r < m; r += kT) rd[r] = 1.0 / X::real(L[r + (size_t)r * cap]);
   __syncthreads();
+  // Every thread owns the rows r = tid + kRows i; the factor's next column for those rows is
+  // loaded one step ahead, so its latency hides behind the current step.
+  constexpr int kRows = (kMaxCap + kT - 1) / kT;
+  D cur[kRows], nxt[kRows];
+  const int first = WHICH != kSolveBack ? 0 : m - 1;
+#pragma unroll
+  for (int i = 0; i < kRows; ++i) {
+    const int r = threadIdx.x + i * kT;
+    cur[i] = r < m ? L[r + (size_t)first * cap] : X::zero();
+  }
   if (WHICH != kSolveBack) {
     for (int p = 0; p < m; ++p) {
+      if (p + 1 < m) {
+#pragma unroll
+        for (int i = 0; i < kRows; ++i) {
+          const int r = threadIdx.x + i * kT;
+          nxt[i] = (r < m && r > p + 1) ? L[r + (size_t)(p + 1) * cap] : X::zero();
+        }
+      }
       if ((int)threadIdx.x < nc) y[(size_t)threadIdx.x * cap + p] = X::scale(rd[p], y[(size_t)threadIdx.x * cap + p]);
       __syncthreads();
-      const D* lc = L + (size_t)p * cap;
-      for (int r = p + 1 + threadIdx.x; r < m; r += kT) {
-        const D l = lc[r];
-        for (int j = 0; j < nc; ++j) y[(size_t)j * cap + r] = X::sub(y[(size_t)j * cap + r], X::mul(l, y[(size_t)j * cap + p]));
+#pragma unroll
+      for (int i = 0; i < kRows; ++i) {
+        const int r = threadIdx.x + i * kT;
+        if (r > p && r < m)
+          for (int j = 0; j < nc; ++j)
+            y[(size_t)j * cap + r] = X::sub(y[(size_t)j * cap + r], X::mul(cur[i], y[(size_t)j * cap + p]));
+        cur[i] = nxt[i];
       }
       __syncthreads();
     }
   } else {
     for (int p = m - 1; p >= 0; --p) {
+      if (p > 0) {
+#pragma unroll
+        for (int i = 0; i < kRows; ++i) {
+          const int r = threadIdx.x + i * kT;
+          nxt[i] = r < p - 1 ? L[r + (size_t)(p - 1) * cap] : X::zero();   // LT column p - 1
+        }
+      }
       if ((int)threadIdx.x < nc) y[(size_t)threadIdx.x * cap + p] = X::scale(rd[p], y[(size_t)threadIdx.x * cap + p]);
       __syncthreads();
-      const D* lc = L + (size_t)p * cap;   // LT column p = conj of L's row p
-      for (int r = threadIdx.x; r < p; r += kT) {
-        const D l = lc[r];
-        for (int j = 0; j < nc; ++j) y[(size_t)j * cap + r] = X::sub(y[(size_t)j * cap + r], X::mul(l, y[(size_t)j * cap + p]));
+#pragma unroll
+      for (int i = 0; i < kRows; ++i) {
+        const int r = threadIdx.x + i * kT;
+        if (r < p)
+          for (int j = 0; j < nc; ++j)
+            y[(size_t)j * cap + r] = X::sub(y[(size_t)j * cap + r], X::mul(cur[i], y[(size_t)j * cap + p]));
+        cur[i] = nxt[i];
       }
       __syncthreads();
     }
@@ -432,8 +462,15 @@ __global__ void __launch_bounds__(kT, 1) k_w_house(const Bufs<D>* __restrict__ b
         pp[blockIdx.x] = sum;
       }
       if (!grid_sync(bar, b.werr)) return;
+      // Re(v^H p) from the blocks' partial sums: loaded once per block, then the same fixed
+      // tree in every block (identical K everywhere)
+      double pr = 0.0;
+      for (int i = threadIdx.x; i < G; i += kT) pr += ldcg(pp + i);
+      pr = warp_sum_r(pr);
+      if (lane == 0) red[warp] = pr;
+      __syncthreads();
       double vp = 0.0;
-      for (int i = 0; i < G; ++i) vp += ldcg(pp + i);
+      for (int i = 0; i < nw; ++i) vp += red[i];
       const double K = 0.5 * beta * vp;
       for (int i = threadIdx.x; i < L; i += kT) q[i] = X::sub(ldcg(pbuf + i), X::scale(K, v[i]));
       __syncthreads();
