@@ -1947,7 +1947,18 @@ extern "C" int bg_kset_davidson_solve(bg_kset* ks, const double* const* start, c
     err = s->error();
     launches = s->launches();
     if (r != BG_OK || !op.tensor) return r;
-    // precision form: the FP64 phase from the tensor phase's Ritz vectors
+    // precision form: when the tensor phase converged every band by the Davidson's own
+    // Ritz-change criterion (loose thresholds, above the BF16x3 noise) it stands;
+    // otherwise (a handover, or bands left unconverged) the FP64 phase runs from its Ritz
+    // vectors and judges convergence in FP64
+    bool all = true;
+    for (int k = 0; k < nk && all; ++k)
+      for (int64_t i = 0; i < n && all; ++i) all = converged[k][i] != 0;
+    if (all) {
+      if (stats)
+        for (int k = 0; k < nk; ++k) stats[k].tensor_iterations = stats[k].iterations;
+      return r;
+    }
     std::vector<bg_davidson_stats> first(stats ? (size_t)nk : 0);
     if (stats) std::copy(stats, stats + nk, first.begin());
     Opts o64 = op;

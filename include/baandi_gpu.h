@@ -294,8 +294,10 @@ typedef struct {
                               bg_kset_davidson_solve is the precision form: a first phase
                               with tensor-core applies, H Grams and rotations (overlap
                               Grams, factor and eigensolve FP64) until every active band's
-                              residual |HX_j - lambda_j X_j| is below 1e-4, then the FP64
-                              solve from its Ritz vectors (convergence judged in FP64) */
+                              residual |HX_j - lambda_j X_j| is below 1e-4 (or stops
+                              falling), then the FP64 solve from its Ritz vectors
+                              (convergence judged in FP64); a tensor phase that converges
+                              every band by the Ritz-change criterion ends the solve */
   int32_t reserved[1];
 } bg_davidson_options;
 
