@@ -1000,9 +1000,9 @@ __global__ void __launch_bounds__(kCtlThreads, 1) k_dv_ctl(int phase, Bufs<D>* _
     case kSelect: {
       if (o.tensor && o.handover > 0.0) {
         // precision form: hand over to FP64 once every active occupied band's residual is
-        // below the threshold, or when the largest active residual has stopped falling
-        // for three iterations (the BF16x3 products' noise floor), or after half of the
-        // iteration budget
+        // below the threshold, or when their largest residual has stopped falling for three
+        // iterations (the BF16x3 products' noise floor), or after half of the iteration
+        // budget
         if (threadIdx.x == 0) {
           double mx = 0.0, mx_occ = 0.0;
           for (int j = 0; j < c.nact; ++j) {
@@ -1010,12 +1010,13 @@ __global__ void __launch_bounds__(kCtlThreads, 1) k_dv_ctl(int phase, Bufs<D>* _
             if (b.active[j] < o.occupied) mx_occ = fmax(mx_occ, b.rnorm[j]);
           }
           bool hand = mx_occ < o.handover * o.handover;
-          if (mx < c.best_res) {
-            c.best_res = mx;
+          if (mx_occ < c.best_res) {   // stagnation of the occupied bands, which decide the handover
+            c.best_res = mx_occ;
             c.stall = 0;
           } else if (++c.stall >= 3) {
             hand = true;
           }
+          (void)mx;
           if (c.iterations >= max(2, o.max_iterations / 2)) hand = true;
           if (hand) c.status = 2;
         }
