@@ -12,6 +12,7 @@
 #include <string>
 #include <vector>
 
+#include "gemm_tc.cuh"
 #include "op_internal.h"
 
 namespace bg {
@@ -408,6 +409,19 @@ int build_op(bg_ctx* ctx, const bg_basis_desc* b, const bg_projectors* pr, int64
     } else {
       op->diag = dfull;
       if ((rc = upload(op.get(), pr->table, (size_t)2 * npw * nproj, &d_dbl))) return rc;
+      // P as bf16 hi/lo panels for the tensor-core products of the precision form (split
+      // once: the table is constant for the operator's lifetime)
+      if ((rc = alloc(op.get(), tc::a_panel_bytes(nproj, npw), &vp))) return rc;
+      N.p_tn = static_cast<const unsigned char*>(vp);
+      if ((rc = alloc(op.get(), tc::a_panel_bytes((int)npw, nproj), &vp))) return rc;
+      N.p_nn = static_cast<const unsigned char*>(vp);
+      N.kt_tn = tc::k_tiles(npw);
+      N.kt_nn = tc::k_tiles(nproj);
+      const double2* pd = reinterpret_cast<const double2*>(d_dbl);
+      ce = tc::split_a(tc::kTN, pd, npw, nproj, (int)npw, const_cast<unsigned char*>(N.p_tn), nullptr);
+      if (ce == cudaSuccess)
+        ce = tc::split_a(tc::kNN, pd, npw, (int)npw, nproj, const_cast<unsigned char*>(N.p_nn), nullptr);
+      if (ce != cudaSuccess) return cuda_fail(ctx, ce, "projector panels");
     }
     N.p = d_dbl;
     op->shape.natoms = natoms;

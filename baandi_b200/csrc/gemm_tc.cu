@@ -1,18 +1,24 @@
 // BF16x3 complex products on the tcgen05 tensor cores (see gemm_tc.cuh).
 //
-// One CTA (256 threads, one per SM: 193 KB of shared memory) owns a 128 x 256 real
-// output tile (128 rows, 128 complex columns) accumulated in FP32 in tensor memory
-// (256 columns).  The K loop runs in stages of 32 complex (64 real) K values, double
-// buffered: all threads load the FP64 operands (coalesced), split them into bf16 hi and
-// lo parts and store them in the canonical K-major layout without swizzle (core matrices
-// of 8 rows x 16 bytes; chunk c of every row at c * rows * 16 bytes, row groups of 8
-// rows 128 bytes apart); one thread issues, per 16-wide K slice, the three products
-// hi*hi, hi*lo, lo*hi (tcgen05.mma kind::f16, BF16 inputs, M = 128, N <= 256) and
-// commits them to the stage's mbarrier, which the loaders wait on before they refill
-// that stage.  The epilogue reads the accumulator with tcgen05.ld (warp w reads lanes
-// 32 (w % 4) .. +31, column half w / 4) and writes FP32 partial tiles (kTN, split K)
-// or the FP64 result (kNN).  Every mbarrier wait is bounded; on expiry the kernel sets
-// the error word, waits (bounded) for its own MMAs, frees its tensor memory and returns.
+// Split pass (k_split_*): one thread per (tile, 16-byte row chunk) reads four complex
+// FP64 values (a K run of a column for kTN operands and B, four columns of a row for the
+// kNN A operand, whose rows are contiguous across neighbouring threads), rounds them to
+// FP32, forms the variant the real product needs and writes the bf16 hi and lo chunks;
+// consecutive threads write consecutive 16-byte chunks.
+//
+// Product pass (k_tc3): one CTA of 128 threads owns a 128 x trb real output tile (trb <=
+// 256 real columns, 128 complex) accumulated in FP32 in tensor memory.  Its K range
+// streams through a ring of kStages shared-memory stages (an A tile of 16 KB and a B tile
+// of trb x 128 bytes each): thread 0 waits for a stage to be free (its `empty` mbarrier,
+// signalled by tcgen05.commit), arms the stage's `full` mbarrier with the byte count and
+// issues two cp.async.bulk copies of the contiguous panel tiles; thread 32 waits on
+// `full`, issues per 16-wide K slice the three products hi*hi, hi*lo, lo*hi
+// (tcgen05.mma kind::f16, BF16 inputs, M = 128, N = trb) and commits them to `empty`.
+// After the last stage a commit to `done` releases the epilogue: warp w reads TMEM lanes
+// 32 w .. 32 w + 31 with tcgen05.ld and writes FP32 partial tiles (kTN, split K) or the
+// FP64 result (kNN).  Every mbarrier wait is bounded; on expiry the kernel sets the
+// error word, waits (bounded) for its own copies and MMAs in flight, frees its tensor
+// memory and returns.  No copy is multicast; the sources are this GPU's own memory.
 #include "gemm_tc.cuh"
 
 #include <cuda_bf16.h>
@@ -23,15 +29,16 @@ namespace bg {
 namespace tc {
 namespace {
 
-constexpr int kThreads = 256;
-constexpr uint32_t kABytes = kTileM * kStepK * 2 * 2;   // 128 rows x 64 real K x 2 B = 16 KB
-constexpr uint32_t kBBytes = kTileN * kStepK * 2 * 2;   // 256 rows x 64 real K x 2 B = 32 KB
-constexpr uint32_t kAChunk = kTileM * 16;               // bytes of one 8-element K chunk of A
-constexpr uint32_t kBChunk = kTileN * 16;
-constexpr uint32_t kStageBytes = 2 * kABytes + 2 * kBBytes;
-constexpr uint32_t kSmemBytes = 2 * kStageBytes + 1024;  // two stages, 1 KB for alignment
-constexpr uint32_t kTmemCols = 256;
+constexpr int kThreads = 128;
+constexpr int kStages = 4;
 constexpr unsigned kWaitLimit = 1u << 24;
+constexpr int kSms = 148;
+constexpr int kMaxChain = 256;  // K tiles accumulated by one CTA of a split-K product
+
+enum : int { kVarA = 0, kVarTnB = 1, kVarNnB = 2 };
+
+__host__ __device__ __forceinline__ size_t tile_bytes_d(int rows) { return (size_t)rows * kStepK * 4; }
+__host__ __device__ __forceinline__ int k_tiles_d(int64_t k) { return (int)((2 * k + kStepK - 1) / kStepK); }
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -68,6 +75,16 @@ __device__ __forceinline__ void mbar_init(uint32_t mbar, uint32_t count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(mbar), "r"(count) : "memory");
 }
 
+__device__ __forceinline__ void mbar_expect_tx(uint32_t mbar, uint32_t bytes) {
+  asm volatile(
+      "{\n\t"
+      ".reg .b64 st;\n\t"
+      "mbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n\t"
+      "}\n" ::"r"(mbar),
+      "r"(bytes)
+      : "memory");
+}
+
 __device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
   for (unsigned i = 0; i < kWaitLimit; ++i) {
     uint32_t ok;
@@ -85,168 +102,275 @@ __device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
   return false;
 }
 
-__device__ __forceinline__ uint32_t pack_bf16(double a, double b, uint32_t* lo) {
-  const __nv_bfloat16 ha = __float2bfloat16_rn((float)a), hb = __float2bfloat16_rn((float)b);
-  const __nv_bfloat16 la = __float2bfloat16_rn((float)(a - (double)__bfloat162float(ha)));
-  const __nv_bfloat16 lb = __float2bfloat16_rn((float)(b - (double)__bfloat162float(hb)));
-  *lo = (uint32_t)__bfloat16_as_ushort(la) | ((uint32_t)__bfloat16_as_ushort(lb) << 16);
-  return (uint32_t)__bfloat16_as_ushort(ha) | ((uint32_t)__bfloat16_as_ushort(hb) << 16);
+// Global -> shared bulk copy (16-byte aligned addresses, size a multiple of 16) that
+// completes its bytes on the stage's mbarrier.
+__device__ __forceinline__ void bulk_copy(uint32_t dst, const void* src, uint32_t bytes, uint32_t mbar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+               "l"(src), "r"(bytes), "r"(mbar)
+               : "memory");
 }
 
-__device__ __forceinline__ void st16(uint32_t saddr, uint32_t a, uint32_t b, uint32_t c, uint32_t d) {
-  asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(saddr), "r"(a), "r"(b), "r"(c), "r"(d) : "memory");
+// The K-tile range of split y (the last splits may be empty).
+__device__ __host__ __forceinline__ void split_range(int ktd, int ksplit, int y, int* kb, int* ke) {
+  const int chunk = (ktd + ksplit - 1) / ksplit;
+  *kb = min(ktd, y * chunk);
+  *ke = min(ktd, *kb + chunk);
 }
 
-__device__ __forceinline__ double2 ldg2(const double2* p) { return __ldg(p); }
+// ------------------------------------------------------------------ split pass
+// Source of a split: element (panel column j, complex K index k) at X[k sk + j sj];
+// panel row nvar j + v holds variant v of column j.
+struct SplitArgs {
+  const double2* X;
+  int64_t sk, sj;
+  int cols, K;
+  int nvar, var;
+  int R;    // rows per tile
+  int ktc;  // K tiles of the panel layout (row tile stride)
+  unsigned char* panel;
+};
 
-// The K range of split y of a kTN product (whole stages; the last split may be empty).
-__device__ __host__ __forceinline__ void split_range(int K, int ksplit, int y, int* kb, int* ke) {
-  int chunk = (K + ksplit - 1) / ksplit;
-  chunk = (chunk + kStepK - 1) / kStepK * kStepK;
-  *kb = min(K, y * chunk);
-  *ke = min(K, *kb + chunk);
+// bf16 pair (a, b) rounded to nearest, and the remainders a - hi, b - hi.
+__device__ __forceinline__ uint32_t bf2(float a, float b, float* ra, float* rb) {
+  const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+  const float2 f = __bfloat1622float2(h);
+  *ra = a - f.x;
+  *rb = b - f.y;
+  return *reinterpret_cast<const uint32_t*>(&h);
 }
+
+__device__ __forceinline__ void split_tile_rows(const SplitArgs& a, int rt, int64_t first, int64_t step) {
+  const int ktd = k_tiles_d(a.K);
+  const int R = a.R;
+  const int64_t items = (int64_t)ktd * 4 * R;
+  for (int64_t idx = first; idx < items; idx += step) {
+    const int kt = (int)(idx / (4 * R));
+    const int q = (int)(idx - (int64_t)kt * 4 * R);
+    const int c = q / R, r = q - c * R;
+    const int rg = rt * R + r;
+    const int j = rg / a.nvar, v = rg - j * a.nvar;
+    const int k0 = kt * (kStepK / 2) + 4 * c;
+    float f[8];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int k = k0 + u;
+      double2 x = make_double2(0.0, 0.0);
+      if (j < a.cols && k < a.K) x = __ldg(a.X + (int64_t)k * a.sk + (int64_t)j * a.sj);
+      const float re = (float)x.x, im = (float)x.y;
+      float p0 = re, p1 = im;
+      if (a.var == kVarTnB && v == 1) {  // conj(a) b, imaginary output part: (b_im, -b_re)
+        p0 = im;
+        p1 = -re;
+      } else if (a.var == kVarNnB) {     // a b: (b_re, -b_im) and (b_im, b_re)
+        if (v == 0) {
+          p1 = -im;
+        } else {
+          p0 = im;
+          p1 = re;
+        }
+      }
+      f[2 * u] = p0;
+      f[2 * u + 1] = p1;
+    }
+    uint4 hi, lo;
+    float l[8], rest[8];
+    hi.x = bf2(f[0], f[1], &l[0], &l[1]);
+    hi.y = bf2(f[2], f[3], &l[2], &l[3]);
+    hi.z = bf2(f[4], f[5], &l[4], &l[5]);
+    hi.w = bf2(f[6], f[7], &l[6], &l[7]);
+    lo.x = bf2(l[0], l[1], &rest[0], &rest[1]);
+    lo.y = bf2(l[2], l[3], &rest[2], &rest[3]);
+    lo.z = bf2(l[4], l[5], &rest[4], &rest[5]);
+    lo.w = bf2(l[6], l[7], &rest[6], &rest[7]);
+    unsigned char* tile = a.panel + ((size_t)rt * a.ktc + kt) * tile_bytes_d(R);
+    *reinterpret_cast<uint4*>(tile + 16 * (size_t)q) = hi;
+    *reinterpret_cast<uint4*>(tile + (size_t)R * 64 + 16 * (size_t)q) = lo;
+  }
+}
+
+__device__ __forceinline__ SplitArgs split_of(const ZDesc& d, int mode, int which, int R, int ktc,
+                                              unsigned char* panel) {
+  SplitArgs a;
+  a.K = d.K;
+  a.R = R;
+  a.ktc = ktc;
+  a.panel = panel;
+  if (which == 0) {
+    a.X = d.A;
+    a.cols = d.M;
+    a.nvar = 1;
+    a.var = kVarA;
+    if (mode == kTN) {
+      a.sk = 1;
+      a.sj = d.lda;
+    } else {
+      a.sk = d.lda;
+      a.sj = 1;
+    }
+  } else {
+    a.X = d.B;
+    a.cols = d.N;
+    a.nvar = 2;
+    a.var = mode == kTN ? kVarTnB : kVarNnB;
+    a.sk = 1;
+    a.sj = d.ldb;
+  }
+  return a;
+}
+
+// Split of operand `which` (0: A, 1: B) of every descriptor; blockIdx.y = row tile,
+// blockIdx.z = descriptor.
+__global__ void k_split_desc(const ZDesc* __restrict__ descs, int mode, int which, int R, int ktc, size_t stride,
+                             unsigned char* base) {
+  const ZDesc d = descs[blockIdx.z];
+  if (d.M <= 0 || d.N <= 0 || d.K <= 0) return;
+  if (which == 0 && d.a_split) return;
+  const SplitArgs a = split_of(d, mode, which, R, ktc, base + blockIdx.z * stride);
+  const int row_tiles = (a.nvar * a.cols + R - 1) / R;
+  if ((int)blockIdx.y >= row_tiles) return;
+  split_tile_rows(a, blockIdx.y, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, (int64_t)gridDim.x * blockDim.x);
+}
+
+__global__ void k_split_args(SplitArgs a) {
+  split_tile_rows(a, blockIdx.y, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, (int64_t)gridDim.x * blockDim.x);
+}
+
+unsigned split_blocks(int64_t items) {
+  return (unsigned)std::max<int64_t>(1, std::min<int64_t>(512, (items + 256 * 8 - 1) / (256 * 8)));
+}
+
+// ------------------------------------------------------------------ product pass
+struct Geo {
+  int ktc;  // K tiles of the launch's own panels
+  int trb;  // B tile rows
+  int ksplit;
+  int max_m, max_n;
+  size_t a_stride, b_stride;
+};
+
+__host__ __device__ __forceinline__ uint32_t stage_bytes(int trb) {
+  return (uint32_t)(tile_bytes_d(kTileM) + tile_bytes_d(trb));
+}
+inline size_t smem_bytes(int trb) { return (size_t)kStages * stage_bytes(trb) + 1024; }
 
 template <int MODE>
 __global__ void __launch_bounds__(kThreads, 1)
-    k_zgemm3(const ZDesc* __restrict__ descs, int ksplit, int max_m, int max_n, float* __restrict__ part, int* err) {
+    k_tc3(const ZDesc* __restrict__ descs, Geo g, const unsigned char* __restrict__ apan,
+          const unsigned char* __restrict__ bpan, float* __restrict__ part, int* err) {
   const ZDesc d = descs[blockIdx.z];
   if (d.M <= 0 || d.N <= 0 || d.K <= 0) return;
-  const int mt = (d.M + kTileM - 1) / kTileM, nt = (d.N + kTileN / 2 - 1) / (kTileN / 2);
-  if ((int)blockIdx.x >= mt * nt) return;
-  const int m0 = (blockIdx.x % mt) * kTileM, j0 = (blockIdx.x / mt) * (kTileN / 2);
-  int kb = 0, ke = d.K;
-  if (MODE == kTN) split_range(d.K, ksplit, blockIdx.y, &kb, &ke);
+  const int nr = 2 * d.N;
+  const int mt_n = (d.M + kTileM - 1) / kTileM, nt_n = (nr + g.trb - 1) / g.trb;
+  if ((int)blockIdx.x >= mt_n * nt_n) return;
+  const int mt = blockIdx.x % mt_n, nt = blockIdx.x / mt_n;
+  const int ktd = k_tiles_d(d.K);
+  int kb = 0, ke = ktd;
+  if (MODE == kTN) split_range(ktd, g.ksplit, blockIdx.y, &kb, &ke);
   if (ke <= kb) return;
-  const int steps = (ke - kb + kStepK - 1) / kStepK;
-  const int ncols = min(kTileN, 2 * (d.N - j0));          // real output columns of this tile
+  if (!d.a_split && g.a_stride == 0) {  // a launch for presplit A given a descriptor without its panel
+    if (threadIdx.x == 0) atomicExch(err, 2);
+    return;
+  }
+  const int steps = ke - kb;
+  const int ncols = min(g.trb, nr - nt * g.trb);  // real output columns of this tile
   const int nmma = (ncols + 15) / 16 * 16;
+  const uint32_t abytes = (uint32_t)tile_bytes_d(kTileM), bbytes = (uint32_t)tile_bytes_d(g.trb);
+  const unsigned char* a_src = d.a_split ? d.a_split + ((size_t)mt * d.a_kt + kb) * abytes
+                                         : apan + blockIdx.z * g.a_stride + ((size_t)mt * g.ktc + kb) * abytes;
+  const unsigned char* b_src = bpan + blockIdx.z * g.b_stride + ((size_t)nt * g.ktc + kb) * bbytes;
 
   extern __shared__ unsigned char dyn[];
-  __shared__ __align__(8) uint64_t mbar[3];
+  __shared__ __align__(8) uint64_t full[kStages], empty[kStages], done;
   __shared__ uint32_t tmem_slot;
-  __shared__ int s_fail;
+  __shared__ int s_fail, s_issued, s_consumed;
   unsigned char* base = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(dyn) + 1023) & ~(uintptr_t)1023);
   const uint32_t sbase = smem_addr(base);
+  const uint32_t sstage = stage_bytes(g.trb);
+  // tensor-memory columns: the accumulator's trb, rounded up to a power of two >= 32
+  uint32_t tcols = 32;
+  while (tcols < (uint32_t)g.trb) tcols <<= 1;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
 
   if (tid == 0) {
-    mbar_init(smem_addr(&mbar[0]), 1);
-    mbar_init(smem_addr(&mbar[1]), 1);
-    mbar_init(smem_addr(&mbar[2]), 1);
+    for (int s = 0; s < kStages; ++s) {
+      mbar_init(smem_addr(&full[s]), 1);
+      mbar_init(smem_addr(&empty[s]), 1);
+    }
+    mbar_init(smem_addr(&done), 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     s_fail = 0;
+    s_issued = 0;
+    s_consumed = 0;
   }
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(&tmem_slot)),
-                 "r"(kTmemCols));
+                 "r"(tcols));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = tmem_slot;
-  const uint32_t id = idesc(nmma);
-  bool ok = true;
 
-  for (int t = 0; t < steps; ++t) {
-    const int stg = t & 1;
-    const uint32_t sa_hi = sbase + stg * kStageBytes, sa_lo = sa_hi + kABytes;
-    const uint32_t sb_hi = sa_hi + 2 * kABytes, sb_lo = sb_hi + kBBytes;
-    if (t >= 2) {  // the MMAs of step t - 2 have released this stage (agreed by all threads)
-      const bool expired = !mbar_wait(smem_addr(&mbar[stg]), ((t - 2) >> 1) & 1);
-      if (__syncthreads_or(expired)) {
-        ok = false;
+  if (tid == 0) {  // producer
+    int t = 0;
+    for (; t < steps; ++t) {
+      const int s = t % kStages;
+      if (t >= kStages && !mbar_wait(smem_addr(&empty[s]), (uint32_t)((t / kStages - 1) & 1))) {
+        s_fail = 1;
         break;
       }
+      const uint32_t sa = sbase + s * sstage, sb = sa + abytes;
+      mbar_expect_tx(smem_addr(&full[s]), abytes + bbytes);
+      bulk_copy(sa, a_src + (size_t)t * abytes, abytes, smem_addr(&full[s]));
+      bulk_copy(sb, b_src + (size_t)t * bbytes, bbytes, smem_addr(&full[s]));
     }
-    const int k0 = kb + t * kStepK;
-    // loads first (32 independent 16-byte loads per thread), then split and store
-    double2 va[4][4], vb[4][4];
-#pragma unroll
-    for (int u = 0; u < 4; ++u) {
-      const int p = tid + u * kThreads;
-      const int r8 = p & 7, c = (p >> 3) & 7, g = p >> 6;
-      const int i = m0 + 8 * g + r8;
-      const int jl = 8 * g + r8, j = j0 + jl;
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const int k = k0 + 4 * c + q;
-        const bool kin = k < ke;
-        if (MODE == kTN)
-          va[u][q] = (kin && i < d.M) ? ldg2(d.A + k + (int64_t)i * d.lda) : make_double2(0.0, 0.0);
-        else
-          va[u][q] = (kin && i < d.M) ? ldg2(d.A + i + (int64_t)k * d.lda) : make_double2(0.0, 0.0);
-        vb[u][q] = (kin && j < d.N) ? ldg2(d.B + k + (int64_t)j * d.ldb) : make_double2(0.0, 0.0);
+    s_issued = t;
+  } else if (tid == 32) {  // MMA issuer
+    const uint32_t id = idesc(nmma);
+    int t = 0;
+    for (; t < steps; ++t) {
+      const int s = t % kStages;
+      if (!mbar_wait(smem_addr(&full[s]), (uint32_t)((t / kStages) & 1))) {
+        s_fail = 1;
+        break;
       }
-    }
-#pragma unroll
-    for (int u = 0; u < 4; ++u) {
-      const int p = tid + u * kThreads;
-      const int r8 = p & 7, c = (p >> 3) & 7, g = p >> 6;
-      uint32_t h[4], l[4];
-#pragma unroll
-      for (int q = 0; q < 4; ++q) h[q] = pack_bf16(va[u][q].x, va[u][q].y, &l[q]);
-      const uint32_t offa = c * kAChunk + g * 128 + r8 * 16;
-      st16(sa_hi + offa, h[0], h[1], h[2], h[3]);
-      st16(sa_lo + offa, l[0], l[1], l[2], l[3]);
-      // B rows 2 jl (real output part) and 2 jl + 1 (imaginary output part)
-      uint32_t h0[4], l0[4], h1[4], l1[4];
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const double re = vb[u][q].x, im = vb[u][q].y;
-        if (MODE == kTN) {  // conj(a) b: (a_re, a_im) . (b_re, b_im) and (b_im, -b_re)
-          h0[q] = pack_bf16(re, im, &l0[q]);
-          h1[q] = pack_bf16(im, -re, &l1[q]);
-        } else {            // a b: (b_re, -b_im) and (b_im, b_re)
-          h0[q] = pack_bf16(re, -im, &l0[q]);
-          h1[q] = pack_bf16(im, re, &l1[q]);
-        }
-      }
-      const int r0 = 2 * (8 * g + r8), r1 = r0 + 1;
-      const uint32_t offb0 = c * kBChunk + (r0 >> 3) * 128 + (r0 & 7) * 16;
-      const uint32_t offb1 = c * kBChunk + (r1 >> 3) * 128 + (r1 & 7) * 16;
-      st16(sb_hi + offb0, h0[0], h0[1], h0[2], h0[3]);
-      st16(sb_lo + offb0, l0[0], l0[1], l0[2], l0[3]);
-      st16(sb_hi + offb1, h1[0], h1[1], h1[2], h1[3]);
-      st16(sb_lo + offb1, l1[0], l1[1], l1[2], l1[3]);
-    }
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    __syncthreads();
-    if (tid == 0) {
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const uint32_t sa = sbase + s * sstage, sb = sa + abytes;
+      const uint32_t alo = sa + kTileM * 64, blo = sb + (uint32_t)g.trb * 64;
+      const uint32_t achunk = kTileM * 16, bchunk = (uint32_t)g.trb * 16;
 #pragma unroll
-      for (int s = 0; s < kStepK / 8; ++s) {  // 16 real K per slice: two chunks
-        const uint64_t ah = sdesc(sa_hi + 2 * s * kAChunk, kAChunk, 128);
-        const uint64_t al = sdesc(sa_lo + 2 * s * kAChunk, kAChunk, 128);
-        const uint64_t bh = sdesc(sb_hi + 2 * s * kBChunk, kBChunk, 128);
-        const uint64_t bl = sdesc(sb_lo + 2 * s * kBChunk, kBChunk, 128);
-        mma_bf16(tmem, ah, bh, id, (t > 0 || s > 0) ? 1u : 0u);
+      for (int sl = 0; sl < kStepK / 16; ++sl) {  // 16 real K per MMA: two 8-value chunks
+        const uint64_t ah = sdesc(sa + 2 * sl * achunk, achunk, 128);
+        const uint64_t al = sdesc(alo + 2 * sl * achunk, achunk, 128);
+        const uint64_t bh = sdesc(sb + 2 * sl * bchunk, bchunk, 128);
+        const uint64_t bl = sdesc(blo + 2 * sl * bchunk, bchunk, 128);
+        mma_bf16(tmem, ah, bh, id, (t > 0 || sl > 0) ? 1u : 0u);
         mma_bf16(tmem, ah, bl, id, 1u);
         mma_bf16(tmem, al, bh, id, 1u);
       }
-      commit(smem_addr(&mbar[stg]));
+      commit(smem_addr(&empty[s]));
     }
-  }
-  // every MMA issued so far done (bounded wait), then the accumulator is read
-  if (tid == 0) {
-    commit(smem_addr(&mbar[2]));
-    if (!mbar_wait(smem_addr(&mbar[2]), 0)) s_fail = 1;
+    s_consumed = t;
+    commit(smem_addr(&done));  // every MMA issued above
   }
   __syncthreads();
-  if (!ok && tid == 0) s_fail = 1;
+  if (tid == 32) {
+    if (!mbar_wait(smem_addr(&done), 0)) s_fail = 1;
+  }
+  if (tid == 0) {  // copies issued but never consumed (a failed wait): let them land
+    for (int t = s_consumed; t < s_issued; ++t)
+      if (!mbar_wait(smem_addr(&full[t % kStages]), (uint32_t)((t / kStages) & 1))) s_fail = 1;
+  }
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   if (s_fail) {
     if (tid == 0) atomicExch(err, 1);
   } else {
-    const int lg = warp & 3, half = warp >> 2;
-    const int i = m0 + 32 * lg + lane;
-    for (int cc = 0; cc < 8; ++cc) {
-      const int n0 = half * 128 + cc * 16;
-      if (n0 >= ncols) break;  // warp-uniform
+    const int i = mt * kTileM + 32 * warp + lane;
+    for (int n0 = 0; n0 < ncols; n0 += 16) {
       uint32_t r[16];
-      const uint32_t taddr = tmem + ((uint32_t)(32 * lg) << 16) + (uint32_t)n0;
+      const uint32_t taddr = tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)n0;
       asm volatile(
           "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
           "%15}, [%16];"
@@ -254,27 +378,25 @@ __global__ void __launch_bounds__(kThreads, 1)
             "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
           : "r"(taddr));
       asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-      if (i < d.M) {
-        if (MODE == kTN) {
-          float* dst = part + (((size_t)blockIdx.z * ksplit + blockIdx.y) * max_m + i) * (2 * (size_t)max_n) +
-                       2 * (size_t)j0 + n0;
+      if (i >= d.M) continue;
+      const int c0 = nt * g.trb + n0;  // real output column of r[0]
+      if (MODE == kTN) {
+        float* dst = part + (((size_t)blockIdx.z * g.ksplit + blockIdx.y) * g.max_m + i) * (2 * (size_t)g.max_n) + c0;
 #pragma unroll
-          for (int q = 0; q < 16; ++q)
-            if (n0 + q < ncols) dst[q] = __uint_as_float(r[q]);
-        } else {
+        for (int q = 0; q < 16; ++q)
+          if (n0 + q < ncols) dst[q] = __uint_as_float(r[q]);
+      } else {
 #pragma unroll
-          for (int q = 0; q < 8; ++q) {
-            const int j = j0 + (n0 >> 1) + q;
-            if (2 * q < ncols - n0) {
-              double2* cp = d.C + i + (int64_t)j * d.ldc;
-              const double re = (double)__uint_as_float(r[2 * q]), im = (double)__uint_as_float(r[2 * q + 1]);
-              if (d.op == kStore) {
-                *cp = make_double2(re, im);
-              } else {
-                const double2 o = *cp;
-                *cp = d.op == kAdd ? make_double2(o.x + re, o.y + im) : make_double2(o.x - re, o.y - im);
-              }
-            }
+        for (int q = 0; q < 8; ++q) {
+          if (n0 + 2 * q >= ncols) break;
+          const int j = (c0 >> 1) + q;
+          double2* cp = d.C + i + (int64_t)j * d.ldc;
+          const double re = (double)__uint_as_float(r[2 * q]), im = (double)__uint_as_float(r[2 * q + 1]);
+          if (d.op == kStore) {
+            *cp = make_double2(re, im);
+          } else {
+            const double2 o = *cp;
+            *cp = d.op == kAdd ? make_double2(o.x + re, o.y + im) : make_double2(o.x - re, o.y - im);
           }
         }
       }
@@ -282,7 +404,7 @@ __global__ void __launch_bounds__(kThreads, 1)
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
-  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols));
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(tcols));
 }
 
 // C (op)= sum over the splits of the FP32 partial tiles, in split order, in FP64.
@@ -290,10 +412,11 @@ __global__ void k_zreduce(const ZDesc* __restrict__ descs, int ksplit, int max_m
                           const float* __restrict__ part) {
   const ZDesc d = descs[blockIdx.y];
   if (d.M <= 0 || d.N <= 0 || d.K <= 0) return;
+  const int ktd = k_tiles_d(d.K);
   int used = 0;
   for (int y = 0; y < ksplit; ++y) {
     int kb, ke;
-    split_range(d.K, ksplit, y, &kb, &ke);
+    split_range(ktd, ksplit, y, &kb, &ke);
     if (ke > kb) used = y + 1;
   }
   const int64_t total = (int64_t)d.M * d.N;
@@ -315,39 +438,116 @@ __global__ void k_zreduce(const ZDesc* __restrict__ descs, int ksplit, int max_m
   }
 }
 
+inline size_t round256(size_t b) { return (b + 255) / 256 * 256; }
+
+struct Carve {
+  Geo g;
+  size_t b_off, part_off, total;
+};
+
+Carve carve(int mode, int ndesc, int max_m, int max_n, int max_k, int ksplit, bool a_presplit) {
+  Carve c;
+  c.g.ktc = k_tiles_d(max_k);
+  c.g.trb = b_tile_rows(max_n);
+  c.g.ksplit = mode == kTN ? std::max(ksplit, 1) : 1;
+  c.g.max_m = max_m;
+  c.g.max_n = max_n;
+  c.g.a_stride = a_presplit ? 0 : round256(a_panel_bytes(max_m, max_k));
+  c.g.b_stride = round256((size_t)((2 * max_n + c.g.trb - 1) / c.g.trb) * c.g.ktc * tile_bytes_d(c.g.trb));
+  c.b_off = (size_t)ndesc * c.g.a_stride;
+  c.part_off = c.b_off + (size_t)ndesc * c.g.b_stride;
+  c.total = c.part_off +
+            (mode == kTN ? round256((size_t)ndesc * c.g.ksplit * (size_t)max_m * 2 * (size_t)max_n * sizeof(float)) : 0);
+  return c;
+}
+
 }  // namespace
 
+size_t workspace_bytes(int mode, int ndesc, int max_m, int max_n, int max_k, int ksplit, bool a_presplit) {
+  return carve(mode, ndesc, max_m, max_n, max_k, ksplit, a_presplit).total;
+}
+
 cudaError_t prepare_zgemm() {
-  cudaError_t e = cudaFuncSetAttribute((const void*)k_zgemm3<kTN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)kSmemBytes);
+  const int smem = (int)smem_bytes(kTileNMax);
+  cudaError_t e = cudaFuncSetAttribute((const void*)k_tc3<kTN>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   if (e == cudaSuccess)
-    e = cudaFuncSetAttribute((const void*)k_zgemm3<kNN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBytes);
+    e = cudaFuncSetAttribute((const void*)k_tc3<kNN>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   return e;
 }
 
 int tn_ksplit(int ndesc, int max_m, int max_n, int max_k) {
-  const int tiles = ((max_m + kTileM - 1) / kTileM) * ((max_n + kTileN / 2 - 1) / (kTileN / 2)) * std::max(ndesc, 1);
-  int ks = (2 * 148 + tiles - 1) / tiles;
-  const int max_split = std::max(1, (max_k + 8 * kStepK - 1) / (8 * kStepK));  // at least 8 stages each
-  return std::max(1, std::min(ks, max_split));
+  const int trb = b_tile_rows(max_n);
+  const int64_t tiles = (int64_t)((max_m + kTileM - 1) / kTileM) * ((2 * max_n + trb - 1) / trb) * std::max(ndesc, 1);
+  const int ktd = k_tiles_d(max_k);
+  // The FP32 accumulation in tensor memory adds an error that grows with the number of
+  // K tiles a CTA accumulates: at most kMaxChain tiles (4,096 complex K) per split.
+  const int min_split = std::max(1, (ktd + kMaxChain - 1) / kMaxChain);
+  const int max_split = std::max(min_split, std::min(64, ktd / 16));  // at least 16 K tiles each
+  int best = min_split;
+  double best_eff = 0.0;
+  for (int ks = min_split; ks <= max_split; ++ks) {
+    const int64_t ctas = tiles * ks;
+    const int64_t waves = (ctas + kSms - 1) / kSms;
+    const double eff = (double)ctas / (double)(waves * kSms);
+    if (eff >= 0.9) return ks;
+    if (eff > best_eff + 1e-9) {
+      best_eff = eff;
+      best = ks;
+    }
+  }
+  return best;
 }
 
-int launch_zgemm(int mode, const ZDesc* d_desc, int ndesc, int max_m, int max_n, int max_k, int ksplit, float* work,
-                 int* err, cudaStream_t s) {
-  const unsigned tiles =
-      (unsigned)(((max_m + kTileM - 1) / kTileM) * ((max_n + kTileN / 2 - 1) / (kTileN / 2)));
-  if (tiles == 0 || ndesc == 0) return 0;
-  (void)max_k;
+int launch_zgemm(int mode, const ZDesc* d_desc, int ndesc, int max_m, int max_n, int max_k, int ksplit,
+                 bool a_presplit, void* work, int* err, cudaStream_t s) {
+  if (ndesc == 0 || max_m <= 0 || max_n <= 0 || max_k <= 0) return 0;
+  const Carve c = carve(mode, ndesc, max_m, max_n, max_k, ksplit, a_presplit);
+  unsigned char* w = static_cast<unsigned char*>(work);
+  int launches = 0;
+  if (!a_presplit) {
+    const unsigned rt = (unsigned)((max_m + kTileM - 1) / kTileM);
+    const unsigned gx = split_blocks((int64_t)c.g.ktc * 4 * kTileM);
+    k_split_desc<<<dim3(gx, rt, (unsigned)ndesc), 256, 0, s>>>(d_desc, mode, 0, kTileM, c.g.ktc, c.g.a_stride, w);
+    ++launches;
+  }
+  {
+    const unsigned rt = (unsigned)((2 * max_n + c.g.trb - 1) / c.g.trb);
+    const unsigned gx = split_blocks((int64_t)c.g.ktc * 4 * c.g.trb);
+    k_split_desc<<<dim3(gx, rt, (unsigned)ndesc), 256, 0, s>>>(d_desc, mode, 1, c.g.trb, c.g.ktc, c.g.b_stride,
+                                                               w + c.b_off);
+    ++launches;
+  }
+  const unsigned tiles = (unsigned)(((max_m + kTileM - 1) / kTileM) * ((2 * max_n + c.g.trb - 1) / c.g.trb));
+  const size_t smem = smem_bytes(c.g.trb);
+  float* part = reinterpret_cast<float*>(w + c.part_off);
   if (mode == kTN) {
-    k_zgemm3<kTN><<<dim3(tiles, (unsigned)ksplit, (unsigned)ndesc), kThreads, kSmemBytes, s>>>(d_desc, ksplit, max_m,
-                                                                                               max_n, work, err);
+    k_tc3<kTN><<<dim3(tiles, (unsigned)c.g.ksplit, (unsigned)ndesc), kThreads, smem, s>>>(d_desc, c.g, w, w + c.b_off,
+                                                                                          part, err);
     const int64_t total = (int64_t)max_m * max_n;
     const unsigned blocks = (unsigned)std::min<int64_t>((total + 255) / 256, 1024);
-    k_zreduce<<<dim3(blocks, (unsigned)ndesc), 256, 0, s>>>(d_desc, ksplit, max_m, max_n, work);
-    return 2;
+    k_zreduce<<<dim3(blocks, (unsigned)ndesc), 256, 0, s>>>(d_desc, c.g.ksplit, max_m, max_n, part);
+    return launches + 2;
   }
-  k_zgemm3<kNN><<<dim3(tiles, 1, (unsigned)ndesc), kThreads, kSmemBytes, s>>>(d_desc, 1, max_m, max_n, nullptr, err);
-  return 1;
+  k_tc3<kNN><<<dim3(tiles, 1, (unsigned)ndesc), kThreads, smem, s>>>(d_desc, c.g, w, w + c.b_off, nullptr, err);
+  return launches + 1;
+}
+
+cudaError_t split_a(int mode, const double2* A, int64_t lda, int M, int K, unsigned char* panel, cudaStream_t s) {
+  if (M <= 0 || K <= 0) return cudaSuccess;
+  SplitArgs a;
+  a.X = A;
+  a.K = K;
+  a.cols = M;
+  a.nvar = 1;
+  a.var = kVarA;
+  a.sk = mode == kTN ? 1 : lda;
+  a.sj = mode == kTN ? lda : 1;
+  a.R = kTileM;
+  a.ktc = k_tiles_d(K);
+  a.panel = panel;
+  const unsigned rt = (unsigned)((M + kTileM - 1) / kTileM);
+  k_split_args<<<dim3(split_blocks((int64_t)a.ktc * 4 * kTileM), rt), 256, 0, s>>>(a);
+  return cudaGetLastError();
 }
 
 }  // namespace tc
@@ -388,16 +588,16 @@ extern "C" int bg_zgemm_bf16x3(bg_ctx* ctx, int32_t mode, int64_t m, int64_t n, 
   const int ks = mode == tc::kTN ? tc::tn_ksplit(1, (int)m, (int)n, (int)k) : 1;
   tc::ZDesc* dd = nullptr;
   int* derr = nullptr;
-  float* work = nullptr;
-  const size_t wf = mode == tc::kTN ? tc::tn_workspace_floats(1, ks, (int)m, (int)n) : 0;
+  void* work = nullptr;
+  const size_t wb = tc::workspace_bytes(mode, 1, (int)m, (int)n, (int)k, ks, false);
   e = cudaMalloc(&dd, sizeof(tc::ZDesc));
   if (e == cudaSuccess) e = cudaMalloc(&derr, sizeof(int));
-  if (e == cudaSuccess && wf) e = cudaMalloc(&work, wf * sizeof(float));
+  if (e == cudaSuccess) e = cudaMalloc(&work, wb);
   int herr = 0;
   if (e == cudaSuccess) e = cudaMemcpyAsync(dd, &d, sizeof d, cudaMemcpyHostToDevice, s);
   if (e == cudaSuccess) e = cudaMemsetAsync(derr, 0, sizeof(int), s);
   if (e == cudaSuccess) {
-    tc::launch_zgemm(mode, dd, 1, (int)m, (int)n, (int)k, ks, work, derr, s);
+    tc::launch_zgemm(mode, dd, 1, (int)m, (int)n, (int)k, ks, false, work, derr, s);
     e = cudaGetLastError();
   }
   if (e == cudaSuccess) e = cudaMemcpyAsync(&herr, derr, sizeof(int), cudaMemcpyDeviceToHost, s);

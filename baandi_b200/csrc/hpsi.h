@@ -105,6 +105,11 @@ struct NlDev {
   const int* d_off;       // natoms coupling offsets
   const double* d;        // concatenated row-major D blocks
   int rows;
+  // complex operators: the projector table as bf16 hi/lo panels of the tensor-core
+  // products (gemm_tc.cuh): p_tn for P^H x (K = rows), p_nn for P W (K = nproj)
+  const unsigned char* p_tn;
+  const unsigned char* p_nn;
+  int kt_tn, kt_nn;
 };
 
 struct NlShape {
@@ -134,12 +139,13 @@ int launch_nonlocal(const NlDev* nl, int gamma, const NlShape& sh, int max_rows,
                     StageEvents* ev);
 
 // Buffers of the tensor-core nonlocal products (precision form, complex operators):
-// the product descriptors of a batch (2 kMaxBatch), the split-K workspace and an error
-// word.  Sized by ensure_nonlocal_tc before any launch (and before a graph capture).
+// the product descriptors of a batch (2 kMaxBatch), the workspace of the products (the
+// split x and coupled-projection panels, the split-K partial tiles) and an error word.
+// Sized by ensure_nonlocal_tc before any launch (and before a graph capture).
 struct TcNl {
   void* desc = nullptr;
-  float* work = nullptr;
-  size_t work_floats = 0;
+  void* work = nullptr;
+  size_t work_bytes = 0;
   int* err = nullptr;
   int ksplit = 1;
   void release();

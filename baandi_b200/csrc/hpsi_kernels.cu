@@ -985,7 +985,8 @@ int configure_kernels(size_t plane_smem, size_t stick_smem) {
 }
 
 // Descriptors of the tensor-core nonlocal products of every operator of a batch:
-// [k] P^H x into the projection buffer, [nk + k] y += P wd.  One thread per operator.
+// [k] P^H x into the projection buffer, [nk + k] y += P wd, P from the operator's
+// split panels.  One thread per operator.
 __global__ void k_nl_tc_descs(const NlDev* __restrict__ nls, int nproj, Batch b, tc::ZDesc* __restrict__ out) {
   const int k = threadIdx.x;
   if (k >= b.nk) return;
@@ -993,10 +994,10 @@ __global__ void k_nl_tc_descs(const NlDev* __restrict__ nls, int nproj, Batch b,
   const CallArgs ca = resolve(b.a[k]);
   const int cols = ca.cols;
   const double2* p = reinterpret_cast<const double2*>(nl.p);
-  out[k] = tc::ZDesc{p, reinterpret_cast<const double2*>(ca.x), reinterpret_cast<double2*>(nl.part), nl.rows,
-                     ca.ldx / 2, nproj, cols > 0 ? nproj : 0, cols, nl.rows, tc::kStore};
+  out[k] = tc::ZDesc{p,     reinterpret_cast<const double2*>(ca.x), reinterpret_cast<double2*>(nl.part), nl.rows,
+                     ca.ldx / 2, nproj, cols > 0 ? nproj : 0, cols, nl.rows, tc::kStore, nl.p_tn, nl.kt_tn};
   out[b.nk + k] = tc::ZDesc{p, reinterpret_cast<const double2*>(nl.wd), reinterpret_cast<double2*>(ca.y), nl.rows,
-                            nproj, ca.ldy / 2, cols > 0 ? nl.rows : 0, cols, nproj, tc::kAdd};
+                            nproj, ca.ldy / 2, cols > 0 ? nl.rows : 0, cols, nproj, tc::kAdd, nl.p_nn, nl.kt_nn};
 }
 
 void TcNl::release() {
@@ -1006,7 +1007,7 @@ void TcNl::release() {
   desc = nullptr;
   work = nullptr;
   err = nullptr;
-  work_floats = 0;
+  work_bytes = 0;
 }
 
 int ensure_nonlocal_tc(TcNl* t, int nk, int nproj, int max_cols, int max_rows) {
@@ -1018,13 +1019,16 @@ int ensure_nonlocal_tc(TcNl* t, int nk, int nproj, int max_cols, int max_rows) {
     if (cudaMemset(t->err, 0, sizeof(int)) != cudaSuccess) return 1;
   }
   t->ksplit = tc::tn_ksplit(nk, nproj, max_cols, max_rows);
-  const size_t need = tc::tn_workspace_floats(nk, t->ksplit, nproj, max_cols);
-  if (need > t->work_floats) {
+  // the projection and the back-projection run one after the other on one stream and
+  // share the workspace
+  const size_t need = std::max(tc::workspace_bytes(tc::kTN, nk, nproj, max_cols, max_rows, t->ksplit, true),
+                               tc::workspace_bytes(tc::kNN, nk, max_rows, max_cols, nproj, 1, true));
+  if (need > t->work_bytes) {
     cudaFree(t->work);
     t->work = nullptr;
-    t->work_floats = 0;
-    if (cudaMalloc(&t->work, need * sizeof(float)) != cudaSuccess) return 1;
-    t->work_floats = need;
+    t->work_bytes = 0;
+    if (cudaMalloc(&t->work, need) != cudaSuccess) return 1;
+    t->work_bytes = need;
   }
   return 0;
 }
@@ -1037,7 +1041,7 @@ int launch_nonlocal_tc(const NlDev* nl, const NlShape& sh, int max_rows, int max
   k_nl_tc_descs<<<1, kMaxBatch, 0, s>>>(nl, sh.nproj, b, d);
   {
     StageScope sc(ev, 3, s);
-    launches += tc::launch_zgemm(tc::kTN, d, b.nk, sh.nproj, max_cols, max_rows, t->ksplit, t->work, t->err, s);
+    launches += tc::launch_zgemm(tc::kTN, d, b.nk, sh.nproj, max_cols, max_rows, t->ksplit, true, t->work, t->err, s);
   }
   {
     StageScope sc(ev, 4, s);
@@ -1047,7 +1051,7 @@ int launch_nonlocal_tc(const NlDev* nl, const NlShape& sh, int max_rows, int max
   }
   {
     StageScope sc(ev, 5, s);
-    launches += tc::launch_zgemm(tc::kNN, d + b.nk, b.nk, max_rows, max_cols, sh.nproj, 1, nullptr, t->err, s);
+    launches += tc::launch_zgemm(tc::kNN, d + b.nk, b.nk, max_rows, max_cols, sh.nproj, 1, true, t->work, t->err, s);
   }
   return launches;
 }

@@ -43,6 +43,13 @@ constexpr int kCtlThreads = 256;
 // Precision form: the tensor-core phase of a solve hands over to FP64 once every active
 // band's residual |HX_j - lambda_j X_j| is below this.
 constexpr double kHandoverResidual = 1e-4;
+// A tensor-phase iteration after which the occupied bands' largest |r|^2 is not below
+// this fraction of the best so far (|r| down by less than 30 %) has stalled.
+constexpr double kStallFactor = 0.49;
+// The tensor phase's own convergence ends a solve only for thresholds (Ha) at or above
+// this; below it the BF16x3 noise in the Ritz values is not negligible and the FP64
+// phase judges convergence.
+constexpr double kTensorOnlyThreshold = 1e-5;
 
 // Errors recorded by a k point's control kernel (status = -id).
 enum : int {
@@ -1000,9 +1007,9 @@ __global__ void __launch_bounds__(kCtlThreads, 1) k_dv_ctl(int phase, Bufs<D>* _
     case kSelect: {
       if (o.tensor && o.handover > 0.0) {
         // precision form: hand over to FP64 once every active occupied band's residual is
-        // below the threshold, or when their largest residual has stopped falling for three
-        // iterations (the BF16x3 products' noise floor), or after half of the iteration
-        // budget
+        // below the threshold, or when their largest residual has fallen by less than 30 %
+        // in each of two iterations (the BF16x3 products' noise floor), or after half of the
+        // iteration budget
         if (threadIdx.x == 0) {
           double mx = 0.0, mx_occ = 0.0;
           for (int j = 0; j < c.nact; ++j) {
@@ -1010,12 +1017,12 @@ __global__ void __launch_bounds__(kCtlThreads, 1) k_dv_ctl(int phase, Bufs<D>* _
             if (b.active[j] < o.occupied) mx_occ = fmax(mx_occ, b.rnorm[j]);
           }
           bool hand = mx_occ < o.handover * o.handover;
-          if (mx_occ < c.best_res) {   // stagnation of the occupied bands, which decide the handover
-            c.best_res = mx_occ;
+          if (mx_occ < kStallFactor * c.best_res) {   // stagnation of the occupied bands
             c.stall = 0;
-          } else if (++c.stall >= 3) {
+          } else if (++c.stall >= 2) {
             hand = true;
           }
+          c.best_res = fmin(c.best_res, mx_occ);
           (void)mx;
           if (c.iterations >= max(2, o.max_iterations / 2)) hand = true;
           if (hand) c.status = 2;
@@ -1366,7 +1373,7 @@ class KsetSolver {
   TcNl tcnl_;
   tc::ZDesc* d_tcnn_ = nullptr;
   tc::ZDesc* d_tctn_ = nullptr;
-  float* tc_work_ = nullptr;
+  unsigned char* tc_work_ = nullptr;
   int* tc_err_ = nullptr;
   int tc_ks_ = 1;
   bool tc_ready_ = false;
@@ -1437,7 +1444,8 @@ class KsetSolver {
     k_dv_nn<D><<<grid, 128, 0, s_>>>(d_bufs_, d_nn_, nk_);
     if (!tensor_products()) return 1;
     k_dv_tc_descs<D><<<1, 128, 0, s_>>>(d_bufs_, d_nn_, nslots, d_tn_, 0, nk_, d_tcnn_, d_tctn_);
-    return 2 + tc::launch_zgemm(tc::kNN, d_tcnn_, nslots * nk_, max_rows_, o_.cap, o_.cap, 1, nullptr, tc_err_, s_);
+    return 2 + tc::launch_zgemm(tc::kNN, d_tcnn_, nslots * nk_, max_rows_, o_.cap, o_.cap, 1, false, tc_work_,
+                                tc_err_, s_);
   }
   bool tensor_products() const { return o_.tensor && sizeof(D) == sizeof(double2) && tc_ready_; }
   int64_t tn(int nslots) {
@@ -1449,8 +1457,8 @@ class KsetSolver {
                                                                               slot_elems_);
     if (!tensor_products()) return 2;
     k_dv_tc_descs<D><<<1, 128, 0, s_>>>(d_bufs_, d_nn_, 0, d_tn_, nslots, nk_, d_tcnn_, d_tctn_);
-    return 3 + tc::launch_zgemm(tc::kTN, d_tctn_, nslots * nk_, o_.cap, o_.cap, max_rows_, tc_ks_, tc_work_, tc_err_,
-                                s_);
+    return 3 + tc::launch_zgemm(tc::kTN, d_tctn_, nslots * nk_, o_.cap, o_.cap, max_rows_, tc_ks_, false, tc_work_,
+                                tc_err_, s_);
   }
   // Buffers of the precision form (once, before any capture).
   int prepare_tensor() {
@@ -1460,7 +1468,10 @@ class KsetSolver {
     const int slots = std::max(kNnSlots, kTnSlots);
     tc_ks_ = tc::tn_ksplit(kTnSlots * nk_, o_.cap, o_.cap, max_rows_);
     if ((rc = alloc(&d_tcnn_, (size_t)slots * nk_)) || (rc = alloc(&d_tctn_, (size_t)slots * nk_)) ||
-        (rc = alloc(&tc_work_, tc::tn_workspace_floats(kTnSlots * nk_, tc_ks_, o_.cap, o_.cap))) ||
+        (rc = alloc(&tc_work_, std::max(tc::workspace_bytes(tc::kTN, kTnSlots * nk_, o_.cap, o_.cap, max_rows_,
+                                                             tc_ks_, false),
+                                         tc::workspace_bytes(tc::kNN, kNnSlots * nk_, max_rows_, o_.cap, o_.cap, 1,
+                                                             false)))) ||
         (rc = alloc(&tc_err_, 1)))
       return rc;
     if ((rc = cuda(cudaMemset(tc_err_, 0, sizeof(int)), "tensor error word"))) return rc;
@@ -1949,10 +1960,10 @@ extern "C" int bg_kset_davidson_solve(bg_kset* ks, const double* const* start, c
     launches = s->launches();
     if (r != BG_OK || !op.tensor) return r;
     // precision form: when the tensor phase converged every band by the Davidson's own
-    // Ritz-change criterion (loose thresholds, above the BF16x3 noise) it stands;
+    // Ritz-change criterion at a loose threshold (kTensorOnlyThreshold) it stands;
     // otherwise (a handover, or bands left unconverged) the FP64 phase runs from its Ritz
     // vectors and judges convergence in FP64
-    bool all = true;
+    bool all = op.threshold >= kTensorOnlyThreshold;
     for (int k = 0; k < nk && all; ++k)
       for (int64_t i = 0; i < n && all; ++i) all = converged[k][i] != 0;
     if (all) {
