@@ -1,10 +1,10 @@
 // BF16x3 complex products on the tcgen05 tensor cores (see gemm_tc.cuh).
 //
-// Split pass (k_split_*): one thread per (tile, 16-byte row chunk) reads four complex
-// FP64 values (a K run of a column for kTN operands and B, four columns of a row for the
-// kNN A operand, whose rows are contiguous across neighbouring threads), rounds them to
-// FP32, forms the variant the real product needs and writes the bf16 hi and lo chunks;
-// consecutive threads write consecutive 16-byte chunks.
+// Split pass (k_split_*): one thread per (source column, K tile) reads 16 complex FP64
+// values (a K run of a column for kTN operands and B, a row across 16 columns for the kNN
+// A operand, whose rows are contiguous across neighbouring threads), rounds them to
+// FP32, forms the variants the real product needs and writes their bf16 hi and lo
+// chunks; neighbouring threads write neighbouring 16-byte chunks.
 //
 // Product pass (k_tc3): one CTA of 128 threads owns a 128 x trb real output tile (trb <=
 // 256 real columns, 128 complex) accumulated in FP32 in tensor memory.  Its K range
@@ -139,52 +139,65 @@ __device__ __forceinline__ uint32_t bf2(float a, float b, float* ra, float* rb) 
   return *reinterpret_cast<const uint32_t*>(&h);
 }
 
+// One thread per (source column j of the row tile, K tile): its 16 complex values (a
+// 256-byte run of the column, or one row across 16 columns for the kNN A operand) are
+// loaded together, then every variant row nvar j + v gets its four hi and four lo
+// chunks; neighbouring threads take neighbouring columns, so each chunk store of a warp
+// is contiguous.
 __device__ __forceinline__ void split_tile_rows(const SplitArgs& a, int rt, int64_t first, int64_t step) {
   const int ktd = k_tiles_d(a.K);
-  const int R = a.R;
-  const int64_t items = (int64_t)ktd * 4 * R;
+  const int R = a.R, per = R / a.nvar;  // source columns per row tile
+  const int64_t items = (int64_t)ktd * per;
   for (int64_t idx = first; idx < items; idx += step) {
-    const int kt = (int)(idx / (4 * R));
-    const int q = (int)(idx - (int64_t)kt * 4 * R);
-    const int c = q / R, r = q - c * R;
-    const int rg = rt * R + r;
-    const int j = rg / a.nvar, v = rg - j * a.nvar;
-    const int k0 = kt * (kStepK / 2) + 4 * c;
-    float f[8];
+    const int kt = (int)(idx / per);
+    const int jl = (int)(idx - (int64_t)kt * per);
+    const int j = rt * per + jl;
+    const int k0 = kt * (kStepK / 2);
+    double2 x[16];
 #pragma unroll
-    for (int u = 0; u < 4; ++u) {
-      const int k = k0 + u;
-      double2 x = make_double2(0.0, 0.0);
-      if (j < a.cols && k < a.K) x = __ldg(a.X + (int64_t)k * a.sk + (int64_t)j * a.sj);
-      const float re = (float)x.x, im = (float)x.y;
-      float p0 = re, p1 = im;
-      if (a.var == kVarTnB && v == 1) {  // conj(a) b, imaginary output part: (b_im, -b_re)
-        p0 = im;
-        p1 = -re;
-      } else if (a.var == kVarNnB) {     // a b: (b_re, -b_im) and (b_im, b_re)
-        if (v == 0) {
-          p1 = -im;
-        } else {
-          p0 = im;
-          p1 = re;
-        }
-      }
-      f[2 * u] = p0;
-      f[2 * u + 1] = p1;
+    for (int u = 0; u < 16; ++u) {
+      x[u] = make_double2(0.0, 0.0);
+      if (j < a.cols && k0 + u < a.K) x[u] = __ldg(a.X + (int64_t)(k0 + u) * a.sk + (int64_t)j * a.sj);
     }
-    uint4 hi, lo;
-    float l[8], rest[8];
-    hi.x = bf2(f[0], f[1], &l[0], &l[1]);
-    hi.y = bf2(f[2], f[3], &l[2], &l[3]);
-    hi.z = bf2(f[4], f[5], &l[4], &l[5]);
-    hi.w = bf2(f[6], f[7], &l[6], &l[7]);
-    lo.x = bf2(l[0], l[1], &rest[0], &rest[1]);
-    lo.y = bf2(l[2], l[3], &rest[2], &rest[3]);
-    lo.z = bf2(l[4], l[5], &rest[4], &rest[5]);
-    lo.w = bf2(l[6], l[7], &rest[6], &rest[7]);
     unsigned char* tile = a.panel + ((size_t)rt * a.ktc + kt) * tile_bytes_d(R);
-    *reinterpret_cast<uint4*>(tile + 16 * (size_t)q) = hi;
-    *reinterpret_cast<uint4*>(tile + (size_t)R * 64 + 16 * (size_t)q) = lo;
+    for (int v = 0; v < a.nvar; ++v) {
+      const int r = jl * a.nvar + v;
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        float f[8];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const float re = (float)x[4 * c + u].x, im = (float)x[4 * c + u].y;
+          float p0 = re, p1 = im;
+          if (a.var == kVarTnB && v == 1) {  // conj(a) b, imaginary output part: (b_im, -b_re)
+            p0 = im;
+            p1 = -re;
+          } else if (a.var == kVarNnB) {     // a b: (b_re, -b_im) and (b_im, b_re)
+            if (v == 0) {
+              p1 = -im;
+            } else {
+              p0 = im;
+              p1 = re;
+            }
+          }
+          f[2 * u] = p0;
+          f[2 * u + 1] = p1;
+        }
+        uint4 hi, lo;
+        float l[8], rest[8];
+        hi.x = bf2(f[0], f[1], &l[0], &l[1]);
+        hi.y = bf2(f[2], f[3], &l[2], &l[3]);
+        hi.z = bf2(f[4], f[5], &l[4], &l[5]);
+        hi.w = bf2(f[6], f[7], &l[6], &l[7]);
+        lo.x = bf2(l[0], l[1], &rest[0], &rest[1]);
+        lo.y = bf2(l[2], l[3], &rest[2], &rest[3]);
+        lo.z = bf2(l[4], l[5], &rest[4], &rest[5]);
+        lo.w = bf2(l[6], l[7], &rest[6], &rest[7]);
+        const size_t q = (size_t)c * R + r;  // chunk c of row r
+        *reinterpret_cast<uint4*>(tile + 16 * q) = hi;
+        *reinterpret_cast<uint4*>(tile + (size_t)R * 64 + 16 * q) = lo;
+      }
+    }
   }
 }
 
@@ -236,7 +249,7 @@ __global__ void k_split_args(SplitArgs a) {
 }
 
 unsigned split_blocks(int64_t items) {
-  return (unsigned)std::max<int64_t>(1, std::min<int64_t>(512, (items + 256 * 8 - 1) / (256 * 8)));
+  return (unsigned)std::max<int64_t>(1, std::min<int64_t>(1024, (items + 256 * 2 - 1) / (256 * 2)));
 }
 
 // ------------------------------------------------------------------ product pass
@@ -506,13 +519,13 @@ int launch_zgemm(int mode, const ZDesc* d_desc, int ndesc, int max_m, int max_n,
   int launches = 0;
   if (!a_presplit) {
     const unsigned rt = (unsigned)((max_m + kTileM - 1) / kTileM);
-    const unsigned gx = split_blocks((int64_t)c.g.ktc * 4 * kTileM);
+    const unsigned gx = split_blocks((int64_t)c.g.ktc * kTileM);
     k_split_desc<<<dim3(gx, rt, (unsigned)ndesc), 256, 0, s>>>(d_desc, mode, 0, kTileM, c.g.ktc, c.g.a_stride, w);
     ++launches;
   }
   {
     const unsigned rt = (unsigned)((2 * max_n + c.g.trb - 1) / c.g.trb);
-    const unsigned gx = split_blocks((int64_t)c.g.ktc * 4 * c.g.trb);
+    const unsigned gx = split_blocks((int64_t)c.g.ktc * (c.g.trb / 2));
     k_split_desc<<<dim3(gx, rt, (unsigned)ndesc), 256, 0, s>>>(d_desc, mode, 1, c.g.trb, c.g.ktc, c.g.b_stride,
                                                                w + c.b_off);
     ++launches;
@@ -546,7 +559,7 @@ cudaError_t split_a(int mode, const double2* A, int64_t lda, int M, int K, unsig
   a.ktc = k_tiles_d(K);
   a.panel = panel;
   const unsigned rt = (unsigned)((M + kTileM - 1) / kTileM);
-  k_split_args<<<dim3(split_blocks((int64_t)a.ktc * 4 * kTileM), rt), 256, 0, s>>>(a);
+  k_split_args<<<dim3(split_blocks((int64_t)a.ktc * kTileM), rt), 256, 0, s>>>(a);
   return cudaGetLastError();
 }
 

@@ -1007,24 +1007,21 @@ __global__ void __launch_bounds__(kCtlThreads, 1) k_dv_ctl(int phase, Bufs<D>* _
     case kSelect: {
       if (o.tensor && o.handover > 0.0) {
         // precision form: hand over to FP64 once every active occupied band's residual is
-        // below the threshold, or when their largest residual has fallen by less than 30 %
-        // in each of two iterations (the BF16x3 products' noise floor), or after half of the
-        // iteration budget
+        // below the handover residual, or when their largest residual has fallen by less
+        // than 30 % in each of two iterations (the BF16x3 products' noise floor), or after
+        // half of the iteration budget
         if (threadIdx.x == 0) {
-          double mx = 0.0, mx_occ = 0.0;
-          for (int j = 0; j < c.nact; ++j) {
-            mx = fmax(mx, b.rnorm[j]);
+          bool hand = c.iterations >= max(2, o.max_iterations / 2);
+          double mx_occ = 0.0;
+          for (int j = 0; j < c.nact; ++j)
             if (b.active[j] < o.occupied) mx_occ = fmax(mx_occ, b.rnorm[j]);
-          }
-          bool hand = mx_occ < o.handover * o.handover;
-          if (mx_occ < kStallFactor * c.best_res) {   // stagnation of the occupied bands
+          if (mx_occ < o.handover * o.handover) hand = true;
+          if (mx_occ < kStallFactor * c.best_res) {  // stagnation of the occupied bands
             c.stall = 0;
           } else if (++c.stall >= 2) {
             hand = true;
           }
           c.best_res = fmin(c.best_res, mx_occ);
-          (void)mx;
-          if (c.iterations >= max(2, o.max_iterations / 2)) hand = true;
           if (hand) c.status = 2;
         }
         __syncthreads();

@@ -41,6 +41,11 @@ from .mixer import Broyden, Profile
 from .occupations import fermi_dirac
 
 
+# Davidson thresholds (Ha) from which the precision form's tensor phase may end a solve on
+# its own (the solver's kTensorOnlyThreshold)
+TENSOR_ONLY_THRESHOLD_HA = 1e-5
+
+
 def next_ethr_ry(previous: float, dr2_ry: float, electrons: float) -> float:
     """crates/dft-engine/src/refscf/profile.rs:49-51."""
     return max(min(previous, 0.1 * dr2_ry / max(electrons, 1.0)), 1e-13)
@@ -69,10 +74,16 @@ class ScfOptions:
     # scf.reference_preconditioning = "tf", crates/dft-engine/src/refscf/broyden.rs:107-114);
     # the supercells need it against long-wavelength charge sloshing
     thomas_fermi: bool = False
-    # the precision form on every map: each Davidson solve starts with tensor-core applies,
-    # H Grams and rotations (BF16x3, FP32 local part) and hands over to FP64 once every
-    # active band's residual is below 1e-4 (convergence judged in FP64)
+    # the precision form: each Davidson solve starts with tensor-core applies, H Grams and
+    # rotations (BF16x3, FP32 local part) and hands over to FP64 once every active
+    # occupied band's residual is below 1e-4 or the residuals stall; at a Davidson
+    # threshold of TENSOR_ONLY_THRESHOLD_HA or more a tensor phase that converges every
+    # band ends the solve, below it convergence is judged in FP64.  tensor_switch_off:
+    # once a map below that threshold hands over within two tensor iterations (its start
+    # vectors were already at the BF16x3 noise floor), the remaining maps of the SCF run
+    # in FP64 from the start.
     tensor: bool = False
+    tensor_switch_off: bool = True
 
 
 @dataclass
@@ -104,6 +115,8 @@ class ScfResult:
 
 class GpuScf:
     """SCF of one workload (systems.Workload) on cuda:ctx.device."""
+
+    _tensor_live = True
 
     def __init__(self, workload, ctx: Context | None = None, options: ScfOptions | None = None):
         import torch
@@ -167,7 +180,7 @@ class GpuScf:
         torch.cuda.synchronize()
 
     def precision_at(self, ethr: float) -> str:
-        if self.o.tensor:
+        if self.o.tensor and self._tensor_live:
             return "tensor"
         f = self.o.fp32_ethr_ry
         return "fp32" if f is not None and ethr >= f else "fp64"
@@ -225,6 +238,7 @@ class GpuScf:
         o = self.o
         threshold_ry = 2.0 * o.threshold_ha
         t0 = time.perf_counter()
+        self._tensor_live = True
         with torch.cuda.stream(self.stream):
             n = torch.full(self.dims, self.electrons / self.volume, dtype=torch.float64, device=self.dev)
             x = self.fields.sphere_forward(n)
@@ -237,11 +251,17 @@ class GpuScf:
                 redo = False
                 while True:
                     tm = time.perf_counter()
-                    sols, rho, y, fres, dr2, energy, ts = self._map(n, x, ethr, it == 1 and not redo)
+                    prec = self.precision_at(ethr)
+                    sols, rho, y, fres, dr2, energy, ts = self._map(n, x, ethr, it == 1 and not redo, prec)
+                    t_its = max(s.tensor_iterations for s in sols)
                     records.append(MapRecord(it, "retry" if redo else "ordinary", dr2, energy, ts, ethr,
                                              sum(s.h_columns for s in sols), max(s.iterations for s in sols),
-                                             time.perf_counter() - tm, self.precision_at(ethr),
-                                             max(s.tensor_iterations for s in sols)))
+                                             time.perf_counter() - tm, prec, t_its))
+                    if (o.tensor_switch_off and prec == "tensor" and ethr / 2.0 < TENSOR_ONLY_THRESHOLD_HA
+                            and t_its <= 2):
+                        # the map's start was already at the tensor products' noise floor
+                        # (handover within two iterations): later maps start closer still
+                        self._tensor_live = False
                     self.starts = [s.eigenvectors for s in sols]
                     if it == 1 and not redo and dr2 < ethr * max(self.electrons, 1.0):
                         ethr = next_ethr_ry(ethr, dr2, self.electrons)

@@ -79,11 +79,13 @@ def test_tensor_davidson_hands_over_to_fp64(ctx):
 
 
 def test_tensor_scf_energy_matches_fp64(ctx):
-    """Si64 SCF to 1e-6 Ha/atom (Thomas-Fermi mixing, Fermi-Dirac 0.01 Ha): the precision
-    form's total energy within 1e-6 Ha/atom of the FP64 SCF."""
+    """Si64 SCF (Thomas-Fermi mixing, Fermi-Dirac 0.01 Ha): the precision form's total
+    energy within 1e-6 Ha/atom of the FP64 SCF.  Both run to 1e-7 Ha/atom, so that the two
+    trajectories' own convergence error (up to the SCF threshold each) stays well below
+    the bound and the comparison measures the precision form."""
     from baandi_b200.scf import GpuScf, ScfOptions
     w = W.si64_gamma()
-    o = dict(threshold_ha=1e-6 * w.natoms, smearing_ha=0.01, thomas_fermi=True)
+    o = dict(threshold_ha=1e-7 * w.natoms, smearing_ha=0.01, thomas_fermi=True)
     plain = GpuScf(w, ctx, ScfOptions(**o)).run()
     tensor = GpuScf(w, ctx, ScfOptions(**o, tensor=True)).run()
     assert plain.converged and tensor.converged
