@@ -131,6 +131,7 @@ SIGNATURES = {
     "bg_kset_stage_times": [_p, _p],
     "bg_davidson_solve": [_p, _p, _p, ctypes.POINTER(DavidsonOptions), _p, _p, _p, ctypes.POINTER(DavidsonStats)],
     "bg_kset_davidson_solve": [_p, _p, _p, ctypes.POINTER(DavidsonOptions), _i32, _p, _p, _p, _p],
+    "bg_kset_davidson_solve_hx": [_p, _p, _p, _p, ctypes.POINTER(DavidsonOptions), _p, _p, _p, _p, _p],
     "bg_op_create_dense": [_p, _i64, _p, _i32, _i64, _pp],
     "bg_reduced_eigh": [_p, _i64, _i32, _p, _p, _p, _p, _p],
     "bg_zgemm_bf16x3": [_p, _i32, _i64, _i64, _i64, _p, _i64, _p, _i64, _p, _i64, _i32, _p],

@@ -188,6 +188,7 @@ struct Opts {
   int wide;           // the reduced problem runs on many blocks (wide_rr.cuh)
   int tensor;         // precision form: tensor-core applies, H Grams and rotations
   double handover;    // precision form: stop once every active band's residual is below
+  int want_hx;        // the final phase also forms H X = HV C[:, :n]
 };
 
 // ------------------------------------------------------------------ block-wide small algebra
@@ -1234,7 +1235,10 @@ __global__ void __launch_bounds__(kCtlThreads, 1) k_dv_ctl(int phase, Bufs<D>* _
     }
     case kFinal: {
       if (c.status < 0) break;
-      if (threadIdx.x == 0) nn[0 * nk + k] = NN<D>{b.V, b.C, b.X, cap, n, c.m, 0, tcp};
+      if (threadIdx.x == 0) {
+        nn[0 * nk + k] = NN<D>{b.V, b.C, b.X, cap, n, c.m, 0, tcp};
+        if (o.want_hx) nn[1 * nk + k] = NN<D>{b.HV, b.C, b.HX, cap, n, c.m, 0, tcp};
+      }
       break;
     }
     default:
@@ -1247,10 +1251,12 @@ __global__ void __launch_bounds__(kCtlThreads, 1) k_dv_ctl(int phase, Bufs<D>* _
 // ------------------------------------------------------------------ start and outputs
 // Per-k pointers of a solve's inputs and outputs (device array, one entry per k point).
 struct IoPtrs {
-  const void* start;   // device start block (rows x n), or null (copied from the host)
-  const double* diag;  // device diagonal, or null
-  void* vectors;       // device output block, or null (copied to the host)
-  const int* err;      // the operator's device error word
+  const void* start;     // device start block (rows x n), or null (copied from the host)
+  const double* diag;    // device diagonal, or null
+  void* vectors;         // device output block, or null (copied to the host)
+  const int* err;        // the operator's device error word
+  const void* start_hx;  // device H of the start block (kept from an earlier solve), or null
+  void* vectors_hx;      // device output H X, or null
 };
 
 // Zero S, H_r, L, C of every k point and copy its start block and diagonal from device
@@ -1271,6 +1277,10 @@ __global__ void k_dv_init(const Bufs<D>* __restrict__ bufs, const IoPtrs* __rest
     const D* src = static_cast<const D*>(p.start);
     for (int64_t t = t0; t < rn; t += stride) b.V[t] = src[t];
   }
+  if (p.start_hx) {
+    const D* src = static_cast<const D*>(p.start_hx);
+    for (int64_t t = t0; t < rn; t += stride) b.HV[t] = src[t];
+  }
   if (p.diag)
     for (int64_t t = t0; t < b.rows; t += stride) const_cast<double*>(b.diag)[t] = p.diag[t];
 }
@@ -1290,6 +1300,10 @@ __global__ void k_dv_out(const Bufs<D>* __restrict__ bufs, const IoPtrs* __restr
   if (p.vectors) {
     D* dst = static_cast<D*>(p.vectors);
     for (int64_t t = t0; t < rn; t += stride) dst[t] = b.X[t];
+  }
+  if (p.vectors_hx) {
+    D* dst = static_cast<D*>(p.vectors_hx);
+    for (int64_t t = t0; t < rn; t += stride) dst[t] = b.HX[t];
   }
   if (blockIdx.x == 0) {
     for (int i = threadIdx.x; i < n; i += blockDim.x) {
@@ -1357,7 +1371,8 @@ class KsetSolver {
     if (h_io_) cudaFreeHost(h_io_);
   }
   int run(const double* const* start, const double* const* diagonal, int32_t ptr_kind, double* const* values,
-          double* const* vectors, int32_t* const* converged, bg_davidson_stats* stats);
+          double* const* vectors, int32_t* const* converged, bg_davidson_stats* stats,
+          const double* const* start_hx = nullptr, double* const* vectors_hx = nullptr);
   const std::string& error() const { return err_; }
   int64_t launches() const { return launches_; }
 
@@ -1629,9 +1644,11 @@ int KsetSolver<T>::prepare() {
 template <class T>
 int KsetSolver<T>::run(const double* const* start, const double* const* diagonal, int32_t ptr_kind,
                        double* const* values, double* const* vectors, int32_t* const* converged,
-                       bg_davidson_stats* stats) {
+                       bg_davidson_stats* stats, const double* const* start_hx, double* const* vectors_hx) {
   const int n = o_.n, cap = o_.cap;
   int rc;
+  const bool kept = start_hx != nullptr && ptr_kind == BG_PTR_DEVICE;
+  o_.want_hx = vectors_hx != nullptr && ptr_kind == BG_PTR_DEVICE ? 1 : 0;
   s_ = ks_->stream;
   launches_ = 0;
   if (!prepared_ && (rc = prepare())) return rc;
@@ -1641,7 +1658,7 @@ int KsetSolver<T>::run(const double* const* start, const double* const* diagonal
   for (int k = 0; k < nk_; ++k) {
     const bool dev = ptr_kind == BG_PTR_DEVICE;
     h_io_[k] = IoPtrs{dev ? start[k] : nullptr, dev ? diagonal[k] : nullptr, dev ? vectors[k] : nullptr,
-                      ks_->ops[k]->t.err};
+                      ks_->ops[k]->t.err, kept ? start_hx[k] : nullptr, o_.want_hx ? vectors_hx[k] : nullptr};
     if (!dev) {  // host inputs: one copy each
       const Bufs<D>& b = hb_[k];
       if ((rc = cuda(cudaMemcpyAsync(b.V, start[k], sizeof(D) * (size_t)b.rows * n, cudaMemcpyHostToDevice, s_),
@@ -1665,8 +1682,8 @@ int KsetSolver<T>::run(const double* const* start, const double* const* diagonal
     std::memset(&c, 0, sizeof c);
     c.m = n;
     c.nact = n;
-    c.h_calls = 1;
-    c.h_columns = n;
+    c.h_calls = kept ? 0 : 1;   // a kept H V needs no apply
+    c.h_columns = kept ? 0 : n;
     c.best_res = 1e300;
     const Bufs<D>& b = hb_[k];
     dy[k] = DynCols{reinterpret_cast<const double*>(b.V), reinterpret_cast<double*>(b.HV), n,
@@ -1679,7 +1696,7 @@ int KsetSolver<T>::run(const double* const* start, const double* const* diagonal
       (rc = cuda(cudaMemcpyAsync(d_tn_, t0.data(), sizeof(TN<D>) * t0.size(), cudaMemcpyHostToDevice, s_), "upload")))
     return rc;
   if (wide_ && (rc = cuda(cudaMemsetAsync(d_bar_, 0, 2 * sizeof(unsigned), s_), "barrier"))) return rc;
-  launches_ += apply() + tn(2) + ctl(kSetup);
+  launches_ += (kept ? 0 : apply()) + tn(2) + ctl(kSetup);
   if (wide_) launches_ += wchol() + weig() + ctl(kSetupPost);
   bool done = false;
   if ((rc = poll(&done))) return rc;
@@ -1713,7 +1730,7 @@ int KsetSolver<T>::run(const double* const* start, const double* const* diagonal
     if ((rc = poll(&done))) return rc;
   }
   // X = V C[:, :n]; outputs
-  launches_ += ctl(kFinal) + nn(1);
+  launches_ += ctl(kFinal) + nn(o_.want_hx ? 2 : 1);
   if ((rc = poll(&done))) return rc;
   // contractions exchange V and X (and HV and HX) on the device: refresh the host mirror
   if ((rc = cuda(cudaMemcpy(hb_.data(), d_bufs_, sizeof(Bufs<D>) * nk_, cudaMemcpyDeviceToHost), "buffers")))
@@ -1878,15 +1895,21 @@ int reduced_eigh(int m, const double* S, const double* H, double* w, double* C, 
 using namespace bg;
 using namespace bg::dv;
 
-extern "C" int bg_kset_davidson_solve(bg_kset* ks, const double* const* start, const double* const* diagonal,
-                                      const bg_davidson_options* options, int32_t ptr_kind, double* const* eigenvalues,
-                                      double* const* eigenvectors, int32_t* const* converged,
-                                      bg_davidson_stats* stats) {
+namespace {
+int kset_solve(bg_kset* ks, const double* const* start, const double* const* start_hx, const double* const* diagonal,
+               const bg_davidson_options* options, int32_t ptr_kind, double* const* eigenvalues,
+               double* const* eigenvectors, double* const* eigenvectors_hx, int32_t* const* converged,
+               bg_davidson_stats* stats) {
   if (!ks) return fail(nullptr, BG_EINVAL, "null k-point set");
   bg_ctx* ctx = ks->ctx;
   if (!start || !diagonal || !options || !eigenvalues || !eigenvectors || !converged)
     return fail(ctx, BG_EINVAL, "null argument");
   if (ptr_kind != BG_PTR_HOST && ptr_kind != BG_PTR_DEVICE) return fail(ctx, BG_EINVAL, "pointer kind");
+  if ((start_hx || eigenvectors_hx) && ptr_kind != BG_PTR_DEVICE)
+    return fail(ctx, BG_EINVAL, "kept H X blocks are device blocks");
+  for (int k = 0; k < (int)ks->ops.size(); ++k)
+    if ((start_hx && !start_hx[k]) || (eigenvectors_hx && !eigenvectors_hx[k]))
+      return fail(ctx, BG_EINVAL, "null per-k H X block");
   const bg_davidson_options o = *options;
   const int nk = (int)ks->ops.size();
   const int64_t n = o.bands;
@@ -1952,7 +1975,7 @@ extern "C" int bg_kset_davidson_solve(bg_kset* ks, const double* const* start, c
       ks->dv_free = [](void* p) { delete static_cast<S*>(p); };
     }
     s->set_options(op, graph);
-    int r = s->run(start, diagonal, ptr_kind, eigenvalues, eigenvectors, converged, stats);
+    int r = s->run(start, diagonal, ptr_kind, eigenvalues, eigenvectors, converged, stats, start_hx, eigenvectors_hx);
     err = s->error();
     launches = s->launches();
     if (r != BG_OK || !op.tensor) return r;
@@ -1975,7 +1998,8 @@ extern "C" int bg_kset_davidson_solve(bg_kset* ks, const double* const* start, c
     o64.tensor = 0;
     o64.handover = 0.0;
     s->set_options(o64, graph);
-    r = s->run(eigenvectors, diagonal, ptr_kind, eigenvalues, eigenvectors, converged, stats);
+    r = s->run(eigenvectors, diagonal, ptr_kind, eigenvalues, eigenvectors, converged, stats, nullptr,
+               eigenvectors_hx);
     err = s->error();
     launches += s->launches();
     if (stats)
@@ -2000,6 +2024,24 @@ extern "C" int bg_kset_davidson_solve(bg_kset* ks, const double* const* start, c
   ks->launches += launches;
   if (rc != BG_OK) return fail(ctx, rc, err.empty() ? "reference Davidson failed" : err);
   return BG_OK;
+}
+}  // namespace
+
+extern "C" int bg_kset_davidson_solve(bg_kset* ks, const double* const* start, const double* const* diagonal,
+                                      const bg_davidson_options* options, int32_t ptr_kind, double* const* eigenvalues,
+                                      double* const* eigenvectors, int32_t* const* converged,
+                                      bg_davidson_stats* stats) {
+  return kset_solve(ks, start, nullptr, diagonal, options, ptr_kind, eigenvalues, eigenvectors, nullptr, converged,
+                    stats);
+}
+
+extern "C" int bg_kset_davidson_solve_hx(bg_kset* ks, const double* const* start, const double* const* start_hx,
+                                         const double* const* diagonal, const bg_davidson_options* options,
+                                         double* const* eigenvalues, double* const* eigenvectors,
+                                         double* const* eigenvectors_hx, int32_t* const* converged,
+                                         bg_davidson_stats* stats) {
+  return kset_solve(ks, start, start_hx, diagonal, options, BG_PTR_DEVICE, eigenvalues, eigenvectors, eigenvectors_hx,
+                    converged, stats);
 }
 
 extern "C" int bg_reduced_eigh(bg_ctx* ctx, int64_t m, int32_t is_complex, const double* s, const double* h,

@@ -51,6 +51,7 @@ class Solution:
     dropped: int
     fallbacks: int = 0   # 1: the learned preconditioner gave way to TPA
     tensor_iterations: int = 0   # precision form: iterations before the FP64 handover
+    hx: object = None            # H applied to the eigenvectors (solve_kset with want_hx)
 
 
 def preconditioner_denominator(hamiltonian_diagonal_ha, eigenvalue_ha):
@@ -130,12 +131,16 @@ def reduced_eigh(s, h, ctx=None):
     return w, c, ms.value
 
 
-def solve_kset(kset, starts, diagonals, options: Options, graph: bool = True, reduced: str = "auto"):
+def solve_kset(kset, starts, diagonals, options: Options, graph: bool = True, reduced: str = "auto",
+               start_hx=None, want_hx: bool = False):
     """The reference Davidson for every k point of a KPointSet at once
     (bg_kset_davidson_solve): each large product is one launch over all k points, the
     reduced problems and control decisions run on the GPU, and an iteration is one
     replayed CUDA graph (graph=False launches the same kernels one by one; reduced "wide"
-    or "block" forces the many-block or the one-block reduced problem).  starts /
+    or "block" forces the many-block or the one-block reduced problem).  Device blocks
+    only: start_hx (one block per k point, H applied to the start block, e.g. kept from the
+    previous solve and updated with add_local_change) spares the start apply, and want_hx
+    returns H X of the eigenvectors in Solution.hx (bg_kset_davidson_solve_hx).  starts /
     diagonals: one (rows_k x bands) block and one rows_k diagonal per k point, numpy
     (host) or CUDA tensors (device; blocks shaped (bands, rows_k) row-major, the layout
     of apply_block).  Returns one Solution per k point, eigenvectors on the same side."""
@@ -173,10 +178,24 @@ def solve_kset(kset, starts, diagonals, options: Options, graph: bool = True, re
     o = _options(options, (0 if graph else 1) | REDUCED_FLAGS[reduced])
     arr = lambda lst, f: (ctypes.c_void_p * nk)(*[f(a) for a in lst])
     host = lambda a: a.ctypes.data
-    rc = lib.bg_kset_davidson_solve(kset.handle, arr(x0, ptr), arr(dg, ptr), ctypes.byref(o), kind, arr(vals, host),
-                                    arr(vecs, ptr), arr(conv, host), stats)
+    hxs = None
+    if start_hx is not None or want_hx:
+        if not device:
+            raise SolverError(L.BG_EINVAL, "kept H X blocks are device blocks")
+        if start_hx is not None:
+            start_hx = list(start_hx)
+            if len(start_hx) != nk or any(h.dtype != x.dtype or not h.is_cuda or not h.is_contiguous()
+                                          or h.shape != x.shape for h, x in zip(start_hx, x0)):
+                raise SolverError(L.BG_ESHAPE, "start_hx: one contiguous block shaped like its start per k point")
+        hxs = [torch.empty_like(x) for x in x0] if want_hx else None
+        rc = lib.bg_kset_davidson_solve_hx(kset.handle, arr(x0, ptr), arr(start_hx, ptr) if start_hx else None,
+                                           arr(dg, ptr), ctypes.byref(o), arr(vals, host), arr(vecs, ptr),
+                                           arr(hxs, ptr) if hxs else None, arr(conv, host), stats)
+    else:
+        rc = lib.bg_kset_davidson_solve(kset.handle, arr(x0, ptr), arr(dg, ptr), ctypes.byref(o), kind,
+                                        arr(vals, host), arr(vecs, ptr), arr(conv, host), stats)
     kset._check(rc)
     return [Solution(vals[k], vecs[k], conv[k].astype(bool), stats[k].iterations, stats[k].reduced_solves,
                      stats[k].h_calls, stats[k].h_columns, stats[k].repairs, stats[k].contractions, stats[k].dropped,
-                     stats[k].fallbacks, stats[k].tensor_iterations)
+                     stats[k].fallbacks, stats[k].tensor_iterations, hxs[k] if hxs else None)
             for k in range(nk)]

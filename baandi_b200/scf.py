@@ -84,6 +84,9 @@ class ScfOptions:
     # in FP64 from the start.
     tensor: bool = False
     tensor_switch_off: bool = True
+    # keep H X of each map's eigenvectors and start the next map's Davidson from it,
+    # updated by the potential change (no start apply)
+    kept_hx: bool = True
 
 
 @dataclass
@@ -117,6 +120,7 @@ class GpuScf:
     """SCF of one workload (systems.Workload) on cuda:ctx.device."""
 
     _tensor_live = True
+    _kept = None   # (potential, [H X per k point]) of the last map, for the next start
 
     def __init__(self, workload, ctx: Context | None = None, options: ScfOptions | None = None):
         import torch
@@ -193,6 +197,17 @@ class GpuScf:
         v0 = float(v.mean())
         self.epoch += 1
         self.kset.set_potential_device(v, self.epoch)
+        # kept HX (crates/dft-engine/src/refscf/kept_hx.rs:98-160): H of the start block is
+        # the previous map's H X brought to this potential, H_new x = H_old x + (V - V_old) x,
+        # so the Davidson start applies nothing
+        start_hx = None
+        if self.o.kept_hx and self._kept is not None:
+            v_old, hxs = self._kept
+            change = v - v_old
+            for op, xk, hxk in zip(self.ops, self.starts, hxs):
+                op.add_local_change(xk, change, hxk)
+            start_hx = hxs
+        self._kept = None
         if self.o.preconditioner != "tpa":
             flat = self._diag_flat + v0
             o = self._diag_offsets
@@ -202,7 +217,13 @@ class GpuScf:
         opts = DV.Options(self.w.bands, ethr / 2.0, self.nocc, first_step=first_step,
                           max_iterations=self.o.davidson_max_iterations, preconditioner=self.o.preconditioner,
                           apply_precision=precision or self.precision_at(ethr))
-        sols = DV.solve_kset(self.kset, self.starts, diags, opts, graph=self.o.graph)
+        sols = DV.solve_kset(self.kset, self.starts, diags, opts, graph=self.o.graph, start_hx=start_hx,
+                             want_hx=self.o.kept_hx)
+        # an H X is kept when the solve's final phase applied H in FP64
+        final_fp64 = opts.apply_precision == "fp64" or (
+            opts.apply_precision == "tensor" and all(sl.tensor_iterations < sl.iterations for sl in sols))
+        if self.o.kept_hx and final_fp64:
+            self._kept = (v, [sl.hx for sl in sols])
         ts = 0.0
         if self.o.smearing_ha is None:
             occ = [self.occupations] * len(sols)
@@ -222,6 +243,7 @@ class GpuScf:
         """Back to the state after construction: the start blocks and an empty mixer (the
         operators, the k-point set and its captured Davidson graphs stay)."""
         self.starts = [s.clone() for s in self._starts0]
+        self._kept = None
         self.mixer.close()
         self.mixer = self._new_mixer()
         self.mixer.set_stream(self.stream.cuda_stream)
@@ -239,6 +261,7 @@ class GpuScf:
         threshold_ry = 2.0 * o.threshold_ha
         t0 = time.perf_counter()
         self._tensor_live = True
+        self._kept = None
         with torch.cuda.stream(self.stream):
             n = torch.full(self.dims, self.electrons / self.volume, dtype=torch.float64, device=self.dev)
             x = self.fields.sphere_forward(n)
@@ -298,9 +321,16 @@ def main(argv=None) -> int:
     p.add_argument("--ha-per-atom", type=float, default=1e-6, help="convergence threshold per atom (Ha)")
     p.add_argument("--smearing", type=float, default=0.01, help="Fermi-Dirac width (Ha); 0 for fixed occupations")
     p.add_argument("--fp32-ethr", type=float, default=None, help="FP32 local applies while ethr (Ry) >= this")
+    p.add_argument("--tensor", action="store_true", help="the precision form (tensor-core phase, then FP64)")
+    p.add_argument("--thomas-fermi", action="store_true", help="Thomas-Fermi screening in the Broyden update")
+    p.add_argument("--no-kept-hx", action="store_true", help="apply H to every map's start block")
+    p.add_argument("--kernels", type=int, default=0,
+                   help="after the timed run, run once more under the CUDA activity tracer (torch.profiler) and "
+                        "print this many kernels by device time")
     a = p.parse_args(argv)
     w = systems.WORKLOADS[a.workload]()
-    opts = ScfOptions(threshold_ha=a.ha_per_atom * w.natoms, smearing_ha=a.smearing or None, fp32_ethr_ry=a.fp32_ethr)
+    opts = ScfOptions(threshold_ha=a.ha_per_atom * w.natoms, smearing_ha=a.smearing or None, fp32_ethr_ry=a.fp32_ethr,
+                      tensor=a.tensor, thomas_fermi=a.thomas_fermi, kept_hx=not a.no_kept_hx)
     scf = GpuScf(w, None, opts)
     scf.warm_up()
     torch.cuda.synchronize()
@@ -311,8 +341,46 @@ def main(argv=None) -> int:
           f"energy={r.energy_ha:.12f} Ha free_energy={r.free_energy_ha:.12f} Ha")
     for m in r.records:
         print(f"  map {m.iteration:2d} {m.kind:8s} {m.precision} ethr={m.ethr_ry:.2e} dr2={m.dr2_ry:.2e} "
-              f"h_columns={m.h_columns} davidson_iterations={m.davidson_iterations} {1000 * m.seconds:.2f} ms")
+              f"h_columns={m.h_columns} davidson_iterations={m.davidson_iterations} "
+              f"tensor_iterations={m.tensor_iterations} {1000 * m.seconds:.2f} ms")
+    if a.kernels > 0:
+        _kernel_table(scf, a.kernels)
     return 0 if r.converged else 1
+
+
+def _kernel_table(scf, top: int) -> None:
+    """One more SCF run (after reset) under torch.profiler's CUDA activity tracer: device
+    time per kernel name over the run, largest first."""
+    import collections
+    import json
+    import os
+    import re
+    import tempfile
+
+    import torch
+    from torch.profiler import ProfilerActivity, profile
+    scf.reset()
+    torch.cuda.synchronize()
+    with profile(activities=[ProfilerActivity.CUDA]) as prof:
+        scf.run()
+        torch.cuda.synchronize()
+    with tempfile.TemporaryDirectory() as d:
+        path = os.path.join(d, "trace.json")
+        prof.export_chrome_trace(path)
+        with open(path) as f:
+            events = json.load(f)["traceEvents"]
+    total, count = collections.defaultdict(float), collections.Counter()
+    for e in events:
+        if e.get("cat") not in ("kernel", "gpu_memcpy", "gpu_memset"):
+            continue
+        name = re.sub(r"void |bg::|dv::|wide::|tc::|\(anonymous namespace\)::", "", e["name"])
+        name = re.sub(r"\(.*", "", name)
+        total[name] += e["dur"]
+        count[name] += 1
+    busy = sum(total.values())
+    print(f"  device time {busy / 1e6:.3f} s over {sum(count.values())} launches and copies")
+    for name, us in sorted(total.items(), key=lambda kv: -kv[1])[:top]:
+        print(f"  {us / 1e3:10.1f} ms {100 * us / busy:5.1f}% {count[name]:6d}  {name}")
 
 
 if __name__ == "__main__":

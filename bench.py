@@ -415,9 +415,11 @@ def run_ours(args):
         cpu = {"value": rate, "unit": "bands/s", "cores": threads, "kind": "port", "us_per_band_per_thread": us,
                "sample": desc + f" ({spent:.1f} s; oracle CPU FP64 restatement: local part in C++, one column "
                                 "per thread; nonlocal products in BLAS)"}
-    scf = None
+    scf = scf64 = None
     if rank == 0 and world == 1 and not args.no_scf:
         scf = scf_leg(args.workload, ctx)
+        if args.workload != "si64":   # the other cell of the headline
+            scf64 = scf_leg("si64", ctx)
     reduced = None
     if rank == 0 and world == 1:
         reduced = reduced_leg(ctx, 2 * w.bands)
@@ -436,7 +438,7 @@ def run_ours(args):
             "e2e_pinned": {"value": e2e_pinned, "unit": "bands/s", "h2d_bytes_per_step": h2d,
                            "d2h_bytes_per_step": d2h},
             "gpu_launches": launches, "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks,
-            "scf": scf, "fp32_local": fp32, "tensor_apply": tensor, "reduced_solve": reduced,
+            "scf": scf, "scf_si64": scf64, "fp32_local": fp32, "tensor_apply": tensor, "reduced_solve": reduced,
         }
         print(json.dumps(line), flush=True)
     kset.close()

@@ -368,6 +368,21 @@ int bg_kset_davidson_solve(bg_kset* set, const double* const* start, const doubl
                            const bg_davidson_options* options, int32_t ptr_kind, double* const* eigenvalues,
                            double* const* eigenvectors, int32_t* const* converged, bg_davidson_stats* stats);
 
+/* Replaces solve_with_initial_hx (crates/dft-solvers/src/ref_davidson_complex.rs:641) as the
+ * SCF's kept-HX path uses it (crates/dft-engine/src/refscf/kept_hx.rs:98-160): the same
+ * solve as bg_kset_davidson_solve with device blocks only, where start_hx (NULL, or one
+ * rows x bands block per k point) holds H applied to the start block (kept from the
+ * previous solve and brought to the current potential with bg_op_add_local_change), so the
+ * start needs no apply, and eigenvectors_hx (NULL, or one block per k point) receives H
+ * applied to the returned eigenvectors.  With the precision form, eigenvectors_hx carries
+ * the final phase's precision (FP64 unless the tensor phase ended the solve:
+ * stats.tensor_iterations == stats.iterations); the FP64 phase after a handover applies H
+ * itself. */
+int bg_kset_davidson_solve_hx(bg_kset* set, const double* const* start, const double* const* start_hx,
+                              const double* const* diagonal, const bg_davidson_options* options,
+                              double* const* eigenvalues, double* const* eigenvectors, double* const* eigenvectors_hx,
+                              int32_t* const* converged, bg_davidson_stats* stats);
+
 /* The generalised Hermitian eigenproblem H C = S C diag(w) of one m x m pencil (m <=
  * 1152; column-major host matrices, interleaved complex when is_complex), solved the way
  * bg_kset_davidson_solve solves its reduced problem beyond capacity 128: the Cholesky

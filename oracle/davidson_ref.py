@@ -87,6 +87,7 @@ class Solution:
     converged: np.ndarray
     iterations: int = 0
     h_columns: int = 0
+    hx: np.ndarray | None = None   # H applied to the eigenvectors
     repairs: int = 0
     contractions: int = 0
     ritz_changes: list = field(default_factory=list)
@@ -115,8 +116,11 @@ def _eigen(Hr, L, m):
     return w, C
 
 
-def solve(apply, start, diagonal, opts: Options) -> Solution:
-    """apply(X) -> H X for a (rows, k) block; start (rows, n); diagonal (rows,)."""
+def solve(apply, start, diagonal, opts: Options, start_hx=None) -> Solution:
+    """apply(X) -> H X for a (rows, k) block; start (rows, n); diagonal (rows,).  start_hx:
+    H applied to the start block (the kept-HX start of
+    crates/dft-solvers/src/ref_davidson_complex.rs:641 solve_with_initial_hx), else it is
+    applied here.  The solution carries hx = H X of its eigenvectors (HV C)."""
     X0 = np.array(start)
     rows, n = X0.shape
     dt = X0.dtype
@@ -126,8 +130,12 @@ def solve(apply, start, diagonal, opts: Options) -> Solution:
     V = np.zeros((rows, cap), dt)
     HV = np.zeros((rows, cap), dt)
     V[:, :n] = X0
-    HV[:, :n] = apply(X0)
-    sol = Solution(None, None, None, h_columns=n)
+    if start_hx is None:
+        HV[:, :n] = apply(X0)
+        sol = Solution(None, None, None, h_columns=n)
+    else:
+        HV[:, :n] = np.asarray(start_hx)
+        sol = Solution(None, None, None, h_columns=0)
     S = np.zeros((cap, cap), dt)
     Hr = np.zeros((cap, cap), dt)
     L = np.zeros((cap, cap), dt)
@@ -230,6 +238,7 @@ def solve(apply, start, diagonal, opts: Options) -> Solution:
             contract(m)
     sol.eigenvalues = w[:n].copy()
     sol.eigenvectors = V[:, :m] @ C[:, :n]
+    sol.hx = HV[:, :m] @ C[:, :n]
     sol.converged = conv
     return sol
 

@@ -98,12 +98,24 @@ class _K:
             return lambda x: OR.apply_gamma(dims, self.idx, self.plus, self.minus, v, self.korc, self.porc, self.nl, x)
         return lambda x: OR.apply_complex(dims, self.idx, v, 0.5 * self.b.kpg2, self.nl, x)
 
+    def local_change(self, dims, dv):
+        """x -> (dv(r) x) on the plane-wave rows: the kept-HX update of
+        crates/dft-physics/src/distributed_complex.rs:388-420 (no kinetic, no projectors)."""
+        if self.gamma:
+            zk = np.zeros_like(self.korc)
+            return lambda x: OR.apply_gamma(dims, self.idx, self.plus, self.minus, dv, zk, None, self.nl, x)
+        zk = np.zeros_like(self.b.kpg2)
+        return lambda x: OR.apply_complex(dims, self.idx, dv, zk, None, x)
+
     def coefficients(self, x):
         return F.expand_orc(x, self.plus, self.minus) if self.gamma else x
 
 
 def run(rows, species, ecut_ha, dims, kpoints, gamma_real, bands, v_ion, starts, ewald, threshold_ha=5e-9,
-        max_iterations=60, beta=0.7, history=8, davidson_max_iterations=20, smearing_ha=None, thomas_fermi=False):
+        max_iterations=60, beta=0.7, history=8, davidson_max_iterations=20, smearing_ha=None, thomas_fermi=False,
+        kept_hx=True):
+    """The SCF outer loop.  kept_hx: each map's Davidson starts from the previous map's
+    H X brought to the new potential (crates/dft-engine/src/refscf/kept_hx.rs:98-160)."""
     cell = S.Cell(np.asarray(rows, dtype=np.float64))
     vol = cell.volume
     electrons = float(sum(s.pseudo.z * np.atleast_2d(s.positions).shape[0] for s in species))
@@ -132,6 +144,7 @@ def run(rows, species, ecut_ha, dims, kpoints, gamma_real, bands, v_ion, starts,
     x = forward(n)
     x[g0] = electrons / vol
     orbitals = [np.array(s) for s in starts]
+    kept = None
     ethr, last_dr2 = 1e-2, np.inf
     res = Result(np.nan, False, 0)
     for it in range(1, max_iterations + 1):
@@ -146,9 +159,14 @@ def run(rows, species, ecut_ha, dims, kpoints, gamma_real, bands, v_ion, starts,
             band_sum = 0.0
             sols = []
             for kk, (k, wk) in enumerate(zip(ks, weights)):
+                hx0 = None
+                if kept is not None:
+                    v_old, hxs = kept
+                    hx0 = hxs[kk] + k.local_change(dims, v - v_old)(orbitals[kk])
                 sols.append(D.solve(k.apply(dims, v), orbitals[kk], k.diag + v0,
                                     D.Options(bands, ethr / 2.0, nocc, first_step=(it == 1 and not redo),
-                                              max_iterations=davidson_max_iterations)))
+                                              max_iterations=davidson_max_iterations), start_hx=hx0))
+            kept = (v, [s.hx for s in sols]) if kept_hx else None
             ts = 0.0
             occs = [occ] * len(ks)
             if smearing_ha is not None:
