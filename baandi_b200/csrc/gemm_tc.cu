@@ -275,7 +275,8 @@ __global__ void __launch_bounds__(kThreads, 1)
   const int nr = 2 * d.N;
   const int mt_n = (d.M + kTileM - 1) / kTileM, nt_n = (nr + g.trb - 1) / g.trb;
   if ((int)blockIdx.x >= mt_n * nt_n) return;
-  const int mt = blockIdx.x % mt_n, nt = blockIdx.x / mt_n;
+  // CTAs that share an A tile (the large operand of kNN) are neighbours in launch order
+  const int mt = blockIdx.x / nt_n, nt = blockIdx.x % nt_n;
   const int ktd = k_tiles_d(d.K);
   int kb = 0, ke = ktd;
   if (MODE == kTN) split_range(ktd, g.ksplit, blockIdx.y, &kb, &ke);
@@ -381,35 +382,48 @@ __global__ void __launch_bounds__(kThreads, 1)
     if (tid == 0) atomicExch(err, 1);
   } else {
     const int i = mt * kTileM + 32 * warp + lane;
-    for (int n0 = 0; n0 < ncols; n0 += 16) {
-      uint32_t r[16];
-      const uint32_t taddr = tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)n0;
-      asm volatile(
-          "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
-          "%15}, [%16];"
-          : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-            "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-          : "r"(taddr));
-      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-      if (i >= d.M) continue;
-      const int c0 = nt * g.trb + n0;  // real output column of r[0]
-      if (MODE == kTN) {
-        float* dst = part + (((size_t)blockIdx.z * g.ksplit + blockIdx.y) * g.max_m + i) * (2 * (size_t)g.max_n) + c0;
+    const bool row = i < d.M;
+    // batches of 64 real columns: for += and -= the batch's 32 complex C values are loaded
+    // together (all in flight) before its accumulator columns are read
+    for (int nb = 0; nb < ncols; nb += 64) {
+      double2 o[32];
+      if (MODE == kNN && d.op != kStore && row) {
 #pragma unroll
-        for (int q = 0; q < 16; ++q)
-          if (n0 + q < ncols) dst[q] = __uint_as_float(r[q]);
-      } else {
+        for (int q = 0; q < 32; ++q)
+          if (nb + 2 * q < ncols) o[q] = d.C[i + (int64_t)((nt * g.trb + nb) / 2 + q) * d.ldc];
+      }
 #pragma unroll
-        for (int q = 0; q < 8; ++q) {
-          if (n0 + 2 * q >= ncols) break;
-          const int j = (c0 >> 1) + q;
-          double2* cp = d.C + i + (int64_t)j * d.ldc;
-          const double re = (double)__uint_as_float(r[2 * q]), im = (double)__uint_as_float(r[2 * q + 1]);
-          if (d.op == kStore) {
-            *cp = make_double2(re, im);
-          } else {
-            const double2 o = *cp;
-            *cp = d.op == kAdd ? make_double2(o.x + re, o.y + im) : make_double2(o.x - re, o.y - im);
+      for (int sub = 0; sub < 4; ++sub) {
+        const int n0 = nb + 16 * sub;
+        if (n0 >= ncols) break;  // warp-uniform
+        uint32_t r[16];
+        const uint32_t taddr = tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)n0;
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
+            "%14, %15}, [%16];"
+            : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+              "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+            : "r"(taddr));
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        if (!row) continue;
+        const int c0 = nt * g.trb + n0;  // real output column of r[0]
+        if (MODE == kTN) {
+          float* dst = part + (((size_t)blockIdx.z * g.ksplit + blockIdx.y) * g.max_m + i) * (2 * (size_t)g.max_n) + c0;
+#pragma unroll
+          for (int q = 0; q < 16; ++q)
+            if (n0 + q < ncols) dst[q] = __uint_as_float(r[q]);
+        } else {
+#pragma unroll
+          for (int q = 0; q < 8; ++q) {
+            if (n0 + 2 * q >= ncols) break;
+            const int j = (c0 >> 1) + q;
+            const double re = (double)__uint_as_float(r[2 * q]), im = (double)__uint_as_float(r[2 * q + 1]);
+            double2 v = make_double2(re, im);
+            if (d.op != kStore) {
+              const double2 old = o[8 * sub + q];
+              v = d.op == kAdd ? make_double2(old.x + re, old.y + im) : make_double2(old.x - re, old.y - im);
+            }
+            d.C[i + (int64_t)j * d.ldc] = v;
           }
         }
       }

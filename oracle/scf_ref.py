@@ -113,16 +113,23 @@ class _K:
 
 def run(rows, species, ecut_ha, dims, kpoints, gamma_real, bands, v_ion, starts, ewald, threshold_ha=5e-9,
         max_iterations=60, beta=0.7, history=8, davidson_max_iterations=20, smearing_ha=None, thomas_fermi=False,
-        kept_hx=True):
+        kept_hx=True, pool=None):
     """The SCF outer loop.  kept_hx: each map's Davidson starts from the previous map's
-    H X brought to the new potential (crates/dft-engine/src/refscf/kept_hx.rs:98-160)."""
+    H X brought to the new potential (crates/dft-engine/src/refscf/kept_hx.rs:98-160).
+    pool: k points split over ranks (an object with `local` (range of owned k points),
+    `gather_eigenvalues(list) -> every k point's list` and `sum_partials(array) -> sum over
+    ranks`, as the reference's KPool: crates/dft-engine/src/refscf/k_pool.rs:76-330);
+    `starts` then holds the owned k points' blocks only."""
     cell = S.Cell(np.asarray(rows, dtype=np.float64))
     vol = cell.volume
     electrons = float(sum(s.pseudo.z * np.atleast_2d(s.positions).shape[0] for s in species))
     nocc = int(np.ceil(electrons / 2 - 1e-12))
     occ = np.array([2.0 if b < nocc else 0.0 for b in range(bands)])
-    ks = [_K(cell, ecut_ha, k, dims, species, gamma_real and tuple(k) == (0.0, 0.0, 0.0)) for k, _ in kpoints]
-    weights = [wk for _, wk in kpoints]
+    local = pool.local if pool is not None else range(len(kpoints))
+    ks = [_K(cell, ecut_ha, kpoints[i][0], dims, species, gamma_real and tuple(kpoints[i][0]) == (0.0, 0.0, 0.0))
+          for i in local]
+    weights_all = [wk for _, wk in kpoints]
+    weights = [weights_all[i] for i in local]
     dens = S.basis_at_k(cell, 4.0 * ecut_ha)
     keep = np.array([half(m) for m in dens.miller.tolist()])
     flat = S.fft_flat(S.g_to_fft(dens, dims), dims)[keep]
@@ -168,12 +175,19 @@ def run(rows, species, ecut_ha, dims, kpoints, gamma_real, bands, v_ion, starts,
                                               max_iterations=davidson_max_iterations), start_hx=hx0))
             kept = (v, [s.hx for s in sols]) if kept_hx else None
             ts = 0.0
-            occs = [occ] * len(ks)
+            vals = [s.eigenvalues for s in sols]
+            if pool is not None:
+                vals = pool.gather_eigenvalues(vals)
+            occs = [occ] * len(vals)
             if smearing_ha is not None:
-                occs, ts = fermi_dirac([s.eigenvalues for s in sols], weights, electrons, smearing_ha)
-            for k, wk, sol, o in zip(ks, weights, sols, occs):
+                occs, ts = fermi_dirac(vals, weights_all, electrons, smearing_ha)
+            occ_local = occs[local.start:local.stop] if pool is not None else occs
+            for k, wk, sol, o in zip(ks, weights, sols, occ_local):
                 rho += F.band_density_sum(dims, k.idx, k.coefficients(sol.eigenvectors), wk * o, vol)
-                band_sum += float(np.dot(wk * o, sol.eigenvalues))
+            if pool is not None:
+                rho = pool.sum_partials(rho)
+            for wk, v, o in zip(weights_all, vals, occs):
+                band_sum += float(np.dot(wk * o, v))
             energy = band_sum - eh + ex - vx + ewald
             y = forward(rho)
             y[g0] = electrons / vol
@@ -189,7 +203,7 @@ def run(rows, species, ecut_ha, dims, kpoints, gamma_real, bands, v_ion, starts,
             break
         last_dr2 = dr2
         res.energy, res.iterations, res.free_energy = energy, it, energy - ts
-        res.eigenvalues = [s.eigenvalues for s in sols]
+        res.eigenvalues = vals
         if dr2 < 2.0 * threshold_ha:
             res.converged = True
             break
