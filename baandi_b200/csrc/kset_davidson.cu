@@ -43,6 +43,9 @@ constexpr int kCtlThreads = 256;
 // Precision form: the tensor-core phase of a solve hands over to FP64 once every active
 // band's residual |HX_j - lambda_j X_j| is below this.
 constexpr double kHandoverResidual = 1e-4;
+// Iterations without a new smallest Ritz change after which the learned preconditioner
+// gives way to TPA (the host-driven solver's rule).
+constexpr int kLearnedStall = 5;
 // A tensor-phase iteration after which the occupied bands' largest |r|^2 is not below
 // this fraction of the best so far (|r| down by less than 30 %) has stalled.
 constexpr double kStallFactor = 0.49;
@@ -151,6 +154,10 @@ struct Ctl {
   // precision form: iterations without a new smallest residual, and that residual (squared)
   int stall;
   double best_res;
+  // the preconditioner in use (the learned one gives way to TPA when the solve stalls),
+  // the smallest largest-Ritz-change so far and the iterations since it fell
+  int precond, pstall, fallbacks;
+  double best_change;
 };
 
 // Descriptors of the large products of one slot (written by the control kernel).
@@ -660,17 +667,26 @@ __global__ void __launch_bounds__(128) k_dv_dense(const D* const* __restrict__ H
 // solver's preconditioner), norms[j] = |Er[:, j]|^2.
 template <class D>
 __global__ void __launch_bounds__(256) k_dv_corrections(const Bufs<D>* __restrict__ bufs, const Ctl* __restrict__ ctl,
-                                                        const Opts* __restrict__ opts) {
+                                                        const Opts* __restrict__ opts,
+                                                        const __nv_bfloat16* __restrict__ net) {
   __shared__ double red[256];
-  const int kind = opts->preconditioner;
+  __shared__ float wnet[learned::kParams];
   const int j = blockIdx.x, k = blockIdx.y;
   const Ctl& c = ctl[k];
   if (c.status != 0 || j >= c.nact) return;
+  const int kind = c.precond;
   const Bufs<D>& b = bufs[k];
   const int64_t rows = b.rows;
   double r2 = 0.0;
-  const double n2 = correction_column(b.X + j * rows, b.HX + j * rows, b.diag, b.lam[j], kind, rows, b.Er + j * rows, red,
-                                      nullptr, &r2);
+  double n2;
+  if (kind == BG_PRECOND_LEARNED) {  // block-uniform: one k point per block row
+    learned::load_params(net, wnet);
+    n2 = correction_column<D, true>(b.X + j * rows, b.HX + j * rows, b.diag, b.lam[j], kind, rows, b.Er + j * rows,
+                                    red, wnet, &r2);
+  } else {
+    n2 = correction_column(b.X + j * rows, b.HX + j * rows, b.diag, b.lam[j], kind, rows, b.Er + j * rows, red,
+                           nullptr, &r2);
+  }
   if (threadIdx.x == 0) {
     b.norms[j] = n2;
     b.rnorm[j] = r2;
@@ -866,14 +882,31 @@ __global__ void __launch_bounds__(kCtlThreads, 1) k_dv_ctl(int phase, Bufs<D>* _
         c.reduced_solves += 1;
       }
       int na = 0;
+      double dmax = 0.0;
       for (int i = 0; i < n; ++i) {
         const double thr = (o.first_step || i < o.occupied) ? o.threshold : fmax(5.0 * o.threshold, 5e-6);
-        const bool cv = fabs(b.w[i] - b.old[i]) < thr;
+        const double change = fabs(b.w[i] - b.old[i]);
+        const bool cv = change < thr;
         b.conv[i] = cv ? 1 : 0;
         if (!cv) b.active[na++] = i;
+        dmax = fmax(dmax, change);
       }
       c.nact = na;
       c.iterations += 1;
+      if (c.precond == BG_PRECOND_LEARNED && na > 0) {
+        // TPA fallback of the learned preconditioner: the largest Ritz change has not
+        // fallen below its best for kLearnedStall iterations, or half the budget is spent
+        if (dmax < c.best_change) {
+          c.best_change = dmax;
+          c.pstall = 0;
+        } else {
+          ++c.pstall;
+        }
+        if (c.pstall >= kLearnedStall || 2 * c.iterations >= o.max_iterations) {
+          c.precond = BG_PRECOND_TPA;
+          c.fallbacks = 1;
+        }
+      }
       if (na == 0 || c.iterations == o.max_iterations) {
         c.status = 1;
       } else if (c.m + na > cap) {
@@ -1502,7 +1535,8 @@ class KsetSolver {
     return 1;
   }
   int64_t corr() {
-    k_dv_corrections<D><<<dim3((unsigned)o_.n, (unsigned)nk_), 256, 0, s_>>>(d_bufs_, d_ctl_, d_opts_);
+    k_dv_corrections<D><<<dim3((unsigned)o_.n, (unsigned)nk_), 256, 0, s_>>>(
+        d_bufs_, d_ctl_, d_opts_, static_cast<const __nv_bfloat16*>(ks_->ctx->learned));
     return 1;
   }
   // Many-block reduced problem (wide_rr.cuh): extension of the factor, then the
@@ -1685,6 +1719,8 @@ int KsetSolver<T>::run(const double* const* start, const double* const* diagonal
     c.h_calls = kept ? 0 : 1;   // a kept H V needs no apply
     c.h_columns = kept ? 0 : n;
     c.best_res = 1e300;
+    c.precond = o_.preconditioner;
+    c.best_change = 1e300;
     const Bufs<D>& b = hb_[k];
     dy[k] = DynCols{reinterpret_cast<const double*>(b.V), reinterpret_cast<double*>(b.HV), n,
                     ks_->gamma ? (n + 1) / 2 : n};
@@ -1761,6 +1797,7 @@ int KsetSolver<T>::run(const double* const* start, const double* const* diagonal
     st.repairs = c.repairs;
     st.contractions = c.contractions;
     st.dropped = c.dropped;
+    st.fallbacks = c.fallbacks;
     if (stats) stats[k] = st;
   }
   // the tensor-core products' pipelines (bounded waits) must not have given up
@@ -1915,7 +1952,7 @@ int kset_solve(bg_kset* ks, const double* const* start, const double* const* sta
   const int64_t n = o.bands;
   int64_t cap = o.capacity == 0 ? 2 * n : o.capacity;
   bool bad = n <= 0 || o.occupied > n || o.occupied < 0 || o.max_iterations <= 0 || !std::isfinite(o.threshold) ||
-             o.threshold <= 0.0 || o.preconditioner < BG_PRECOND_SMOOTH || o.preconditioner > BG_PRECOND_RITZ_SHIFT;
+             o.threshold <= 0.0 || o.preconditioner < BG_PRECOND_SMOOTH || o.preconditioner > BG_PRECOND_LEARNED;
   for (int k = 0; k < nk && !bad; ++k) {
     const bg_op* op = ks->ops[k];
     const int64_t rows = op->rows;
@@ -1926,6 +1963,8 @@ int kset_solve(bg_kset* ks, const double* const* start, const double* const* sta
   }
   if (bad || cap > 1536)
     return fail(ctx, BG_EINVAL, "reference Davidson dimensions/threshold (bands must fit every operator's capacity)");
+  if (o.preconditioner == BG_PRECOND_LEARNED && !ctx->learned)
+    return fail(ctx, BG_EINVAL, "learned preconditioner requested but no network was set (bg_learned_set)");
   for (int k = 0; k < nk; ++k) {
     if (!start[k] || !diagonal[k] || !eigenvalues[k] || !eigenvectors[k] || !converged[k])
       return fail(ctx, BG_EINVAL, "null per-k argument");

@@ -90,7 +90,7 @@ def main(argv=None) -> int:
         total, count = collections.defaultdict(float), collections.Counter()
         for e in events:
             if e.get("cat") == "kernel":
-                name = e["name"].split("(")[0].replace("void ", "")
+                name = e["name"].replace("(anonymous namespace)::", "").replace("void ", "").split("(")[0]
                 total[name] += e["dur"]
                 count[name] += 1
         per_call = sum(total.values()) / a.reps

@@ -38,6 +38,7 @@ from . import operands as O
 from .fields import FieldGrid
 from .hamiltonian import ComplexHamiltonian, Context, KPointSet, RealGammaHamiltonian, SolverError, default_context
 from .mixer import Broyden, Profile
+from .kpool import KPool
 from .occupations import fermi_dirac
 
 
@@ -122,7 +123,11 @@ class GpuScf:
     _tensor_live = True
     _kept = None   # (potential, [H X per k point]) of the last map, for the next start
 
-    def __init__(self, workload, ctx: Context | None = None, options: ScfOptions | None = None):
+    def __init__(self, workload, ctx: Context | None = None, options: ScfOptions | None = None, pool=None):
+        """pool: a kpool.KPool splitting the k points over ranks (one GPU each); this
+        process then builds and solves its own k points only, gathers every k point's
+        eigenvalues for the occupations and sums the density over ranks in a fixed order
+        (fields and mixer are replicated, bit for bit, on every rank)."""
         import torch
         self.torch = torch
         self.w = w = workload
@@ -141,15 +146,21 @@ class GpuScf:
         self.nocc = int(math.ceil(nocc - 1e-12))
         self.occupations = np.array([2.0 if b < self.nocc else 0.0 for b in range(w.bands)])
         cap = 2 * w.bands
+        self.pool = pool if pool is not None else KPool(len(w.kpoints))
+        if self.pool.nk != len(w.kpoints):
+            raise SolverError(L.BG_EINVAL, "the pool must cover the workload's k points")
+        self.weights_all = [wk for _, wk in w.kpoints]
         self.ops, self.weights, self.diag_static, self.starts = [], [], [], []
-        for i, (k, wk) in enumerate(w.kpoints):
+        for i in self.pool.local:
+            k, wk = w.kpoints[i]
             pw = w.plane_waves(k)
             gamma = w.gamma_real and pw.gamma
             cls = RealGammaHamiltonian if gamma else ComplexHamiltonian
             op = cls.new_owned(pw, dims, w.nonlocal_table(pw), cap, self.ctx)
             self.ops.append(op)
             self.weights.append(wk)
-            d = op.kinetic_diagonal() if self.o.preconditioner == "tpa" else op.diagonal_static()
+            # TPA and the learned form (a multiplier on TPA) take the kinetic diagonal
+            d = op.kinetic_diagonal() if self.o.preconditioner in ("tpa", "learned") else op.diagonal_static()
             self.diag_static.append(torch.from_numpy(np.ascontiguousarray(d)).to(dev))
             x0 = w.random_block(pw.npw, w.bands, seed_offset=100 + i, real=gamma)
             self.starts.append(torch.from_numpy(np.ascontiguousarray(x0.T)).to(dev))
@@ -208,7 +219,7 @@ class GpuScf:
                 op.add_local_change(xk, change, hxk)
             start_hx = hxs
         self._kept = None
-        if self.o.preconditioner != "tpa":
+        if self.o.preconditioner not in ("tpa", "learned"):
             flat = self._diag_flat + v0
             o = self._diag_offsets
             diags = [flat[o[k]:o[k + 1]] for k in range(len(self.ops))]
@@ -225,13 +236,17 @@ class GpuScf:
         if self.o.kept_hx and final_fp64:
             self._kept = (v, [sl.hx for sl in sols])
         ts = 0.0
+        vals = self.pool.gather_eigenvalues([s.eigenvalues for s in sols])   # every k point, in k order
         if self.o.smearing_ha is None:
-            occ = [self.occupations] * len(sols)
+            occ = [self.occupations] * len(vals)
         else:
-            occ, _, ts = fermi_dirac([s.eigenvalues for s in sols], self.weights, self.electrons, self.o.smearing_ha)
-        wk = np.stack([self.weights[k] * occ[k] for k in range(len(sols))])
+            occ, _, ts = fermi_dirac(vals, self.weights_all, self.electrons, self.o.smearing_ha)
+        loc = self.pool.local
+        wk = np.stack([self.weights_all[k] * occ[k] for k in loc])
         rho = self.kset.band_density_sum([s.eigenvectors for s in sols], wk, self.volume)
-        band_sum = sum(float(np.dot(wk[k], sols[k].eigenvalues)) for k in range(len(sols)))
+        rho = self.pool.sum_partials(rho)
+        band_sum = sum(float(np.dot(self.weights_all[k] * occ[k], vals[k])) for k in range(len(vals)))
+        self._eigenvalues = vals
         energy = band_sum - f.hartree + f.xc - f.xc_integral + self.ewald
         y = self.fields.sphere_forward(rho)
         y[self.g0] = self.electrons / self.volume
@@ -295,7 +310,7 @@ class GpuScf:
                 result.energy_ha = energy
                 result.free_energy_ha = energy - ts
                 result.iterations = it
-                result.eigenvalues = [s.eigenvalues for s in sols]
+                result.eigenvalues = self._eigenvalues
                 if dr2 < threshold_ry:
                     result.converged = True
                     break

@@ -89,20 +89,28 @@ def test_start_network_is_tpa_exactly(ctx, problems):
     assert (a.iterations, a.h_columns) == (b.iterations, b.h_columns)
 
 
-def test_trained_network_against_tpa_on_a_held_out_geometry(ctx, problems):
-    """Trained on 8 displaced Si2 geometries; on a ninth it lowers the correction loss
-    and the H columns the Davidson needs (occupied bands to 1e-8 Ha, four seeded
-    starts) against TPA, and reaches the same occupied eigenvalues."""
-    train, hp, hold_w = problems
+@pytest.fixture(scope="module")
+def trained(ctx, problems):
+    """The network trained on the 8 displaced geometries (600 Adam steps) and the
+    held-out correction loss before and after."""
+    train, hp, _ = problems
     samples = LP.build_samples(ctx, train)
     held = LP.build_samples(ctx, [hp])
     t = LP.Trainer(ctx, LP.init_params(0), lr=3e-3)
     before = t.loss_grad(held)
     for _ in range(600):
         t.step(samples)
-    after = t.loss_grad(held)
+    return t.params(), before, t.loss_grad(held)
+
+
+def test_trained_network_against_tpa_on_a_held_out_geometry(ctx, problems, trained):
+    """Trained on 8 displaced Si2 geometries; on a ninth it lowers the correction loss
+    and the H columns the Davidson needs (occupied bands to 1e-8 Ha, four seeded
+    starts) against TPA, and reaches the same occupied eigenvalues."""
+    train, hp, hold_w = problems
+    params, before, after = trained
     assert after < 0.95 * before, (before, after)
-    LP.install(ctx, t.params())
+    LP.install(ctx, params)
     cols = {"tpa": 0, "learned": 0}
     for so in (7, 11, 12, 13):
         start = hold_w.random_block(hp.op.global_len(), 8, seed_offset=so, real=True)
@@ -184,3 +192,55 @@ def test_start_network_is_tpa_on_a_complex_operator(ctx):
     b = DV.solve(op, start, kin, o)
     assert np.array_equal(a.eigenvalues, b.eigenvalues)
     assert (a.iterations, a.h_columns) == (b.iterations, b.h_columns)
+
+
+# ---- the batched solver (bg_kset_davidson_solve), the one the SCF runs
+
+def _kset_solve(ctx, hp, start, name, its=120):
+    from baandi_b200.hamiltonian import KPointSet
+    ks = KPointSet([hp.op], ctx)
+    o = DV.Options(8, 1e-8, 4, max_iterations=its, preconditioner=name)
+    (sol,) = DV.solve_kset(ks, [start], [hp.kinetic], o)
+    return sol
+
+
+def test_kset_start_network_is_tpa_exactly(ctx, problems):
+    _, hp, _ = problems
+    a = _kset_solve(ctx, hp, hp.start, "tpa", 40)
+    LP.install(ctx, LP.init_params(0))
+    b = _kset_solve(ctx, hp, hp.start, "learned", 40)
+    assert np.array_equal(a.eigenvalues, b.eigenvalues)
+    assert (a.iterations, a.h_columns) == (b.iterations, b.h_columns)
+
+
+def test_kset_trained_network_against_tpa(ctx, problems, trained):
+    """The batched solver with the trained network on the held-out geometry: fewer H
+    columns than TPA over four seeded starts, the same occupied eigenvalues."""
+    _, hp, hold_w = problems
+    LP.install(ctx, trained[0])
+    cols = {"tpa": 0, "learned": 0}
+    for so in (7, 11, 12, 13):
+        start = hold_w.random_block(hp.op.global_len(), 8, seed_offset=so, real=True)
+        for name in cols:
+            sol = _kset_solve(ctx, hp, start, name)
+            cols[name] += sol.h_columns
+            assert np.max(np.abs(sol.eigenvalues[:4] - hp.evals[:4])) < 1e-7
+    print(f"batched solver, H columns tpa {cols['tpa']} learned {cols['learned']}")
+    assert cols["learned"] < cols["tpa"]
+
+
+def test_kset_bad_network_falls_back_to_tpa(ctx, problems):
+    _, hp, _ = problems
+    bad = LP.init_params(0)
+    bad[LP.OW3:LP.OB3] = np.random.default_rng(9).normal(0.0, 50.0, LP.N_HID)
+    LP.install(ctx, bad)
+    sol = _kset_solve(ctx, hp, hp.start, "learned")
+    assert sol.fallbacks == 1
+    assert np.max(np.abs(sol.eigenvalues[:4] - hp.evals[:4])) < 1e-7
+
+
+def test_kset_learned_needs_a_network(ctx, problems):
+    _, hp, _ = problems
+    LP.clear(ctx)
+    with pytest.raises(SolverError):
+        _kset_solve(ctx, hp, hp.start, "learned", 5)
