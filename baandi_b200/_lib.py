@@ -131,6 +131,7 @@ SIGNATURES = {
     "bg_kset_stage_times": [_p, _p],
     "bg_davidson_solve": [_p, _p, _p, ctypes.POINTER(DavidsonOptions), _p, _p, _p, ctypes.POINTER(DavidsonStats)],
     "bg_kset_davidson_solve": [_p, _p, _p, ctypes.POINTER(DavidsonOptions), _i32, _p, _p, _p, _p],
+    "bg_autotune_report": [ctypes.c_char_p, _i64],
     "bg_kset_davidson_solve_hx": [_p, _p, _p, _p, ctypes.POINTER(DavidsonOptions), _p, _p, _p, _p, _p],
     "bg_op_create_dense": [_p, _i64, _p, _i32, _i64, _pp],
     "bg_reduced_eigh": [_p, _i64, _i32, _p, _p, _p, _p, _p],
@@ -184,6 +185,15 @@ def last_error(ctx=None) -> str:
     buf = ctypes.create_string_buffer(512)
     load().bg_last_error(ctx, buf, len(buf))
     return buf.value.decode(errors="replace")
+
+
+def autotune_report() -> list:
+    """The autotuner's decisions in this process (bg_autotune_report), parsed."""
+    import json
+    need = load().bg_autotune_report(None, 0)
+    buf = ctypes.create_string_buffer(max(int(need), 3))
+    load().bg_autotune_report(buf, len(buf))
+    return json.loads(buf.value.decode())
 
 
 def check(rc, ctx=None):

@@ -24,6 +24,11 @@
 #include <cuda_bf16.h>
 
 #include <algorithm>
+#include <cstdio>
+#include <mutex>
+#include <string>
+#include <utility>
+#include <vector>
 
 namespace bg {
 namespace tc {
@@ -502,6 +507,125 @@ cudaError_t prepare_zgemm() {
   return e;
 }
 
+namespace {
+// Split counts worth timing for a kTN product: every count from the accuracy bound's
+// minimum up that fills at least 80 % of whole waves of 148 SMs (at most six).
+std::vector<int> ksplit_candidates(int ndesc, int max_m, int max_n, int max_k) {
+  const int trb = b_tile_rows(max_n);
+  const int64_t tiles = (int64_t)((max_m + kTileM - 1) / kTileM) * ((2 * max_n + trb - 1) / trb) * std::max(ndesc, 1);
+  const int ktd = k_tiles_d(max_k);
+  const int min_split = std::max(1, (ktd + kMaxChain - 1) / kMaxChain);
+  const int max_split = std::max(min_split, std::min(64, ktd / 16));
+  std::vector<int> out;
+  for (int ks = min_split; ks <= max_split && out.size() < 6; ++ks) {
+    const int64_t ctas = tiles * ks;
+    const int64_t waves = (ctas + kSms - 1) / kSms;
+    if ((double)ctas / (double)(waves * kSms) >= 0.8) out.push_back(ks);
+  }
+  return out;
+}
+
+struct TuneEntry {
+  int ndesc, m, n, k, chosen;
+  std::vector<std::pair<int, float>> timed;  // (split count, ms per product pass)
+};
+std::mutex g_tune_mu;
+std::vector<TuneEntry> g_tuned;
+}  // namespace
+
+int tn_ksplit_tuned(int ndesc, int max_m, int max_n, int max_k) {
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    for (const TuneEntry& e : g_tuned)
+      if (e.ndesc == ndesc && e.m == max_m && e.n == max_n && e.k == max_k) return e.chosen;
+  }
+  const int rule = tn_ksplit(ndesc, max_m, max_n, max_k);
+  std::vector<int> cand = ksplit_candidates(ndesc, max_m, max_n, max_k);
+  if (std::find(cand.begin(), cand.end(), rule) == cand.end()) cand.push_back(rule);
+  TuneEntry entry{ndesc, max_m, max_n, max_k, rule, {}};
+  // scratch operands: zeroed panels (their values do not change the time), C and the
+  // descriptors; the largest candidate sizes the workspace
+  const int kmax = *std::max_element(cand.begin(), cand.end());
+  const size_t wb = workspace_bytes(kTN, ndesc, max_m, max_n, max_k, kmax, false);
+  const size_t cbytes = (size_t)ndesc * max_m * max_n * sizeof(double2);
+  void *work = nullptr, *c = nullptr, *dd = nullptr, *derr = nullptr;
+  cudaStream_t s = nullptr;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  bool ok = cudaMalloc(&work, wb) == cudaSuccess && cudaMalloc(&c, cbytes) == cudaSuccess &&
+            cudaMalloc(&dd, sizeof(ZDesc) * ndesc) == cudaSuccess && cudaMalloc(&derr, sizeof(int)) == cudaSuccess &&
+            cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) == cudaSuccess &&
+            cudaEventCreate(&e0) == cudaSuccess && cudaEventCreate(&e1) == cudaSuccess &&
+            prepare_zgemm() == cudaSuccess;
+  if (ok) {
+    std::vector<ZDesc> h((size_t)ndesc);
+    for (int z = 0; z < ndesc; ++z)
+      h[z] = ZDesc{nullptr, nullptr, static_cast<double2*>(c) + (size_t)z * max_m * max_n, max_k, max_k, max_m,
+                   max_m, max_n, max_k, kStore};
+    ok = cudaMemsetAsync(work, 0, wb, s) == cudaSuccess && cudaMemsetAsync(derr, 0, sizeof(int), s) == cudaSuccess &&
+         cudaMemcpyAsync(dd, h.data(), sizeof(ZDesc) * ndesc, cudaMemcpyHostToDevice, s) == cudaSuccess;
+  }
+  float best = 0.0f;
+  for (size_t i = 0; ok && i < cand.size(); ++i) {
+    const Carve cv = carve(kTN, ndesc, max_m, max_n, max_k, cand[i], false);
+    unsigned char* w = static_cast<unsigned char*>(work);
+    const unsigned tiles = (unsigned)(((max_m + kTileM - 1) / kTileM) * ((2 * max_n + cv.g.trb - 1) / cv.g.trb));
+    const int64_t total = (int64_t)max_m * max_n;
+    const unsigned rblocks = (unsigned)std::min<int64_t>((total + 255) / 256, 1024);
+    float t = 0.0f;
+    for (int rep = 0; rep < 3 && ok; ++rep) {  // the first launch warms, the best of two counts
+      ok = cudaEventRecord(e0, s) == cudaSuccess;
+      k_tc3<kTN><<<dim3(tiles, (unsigned)cv.g.ksplit, (unsigned)ndesc), kThreads, smem_bytes(cv.g.trb), s>>>(
+          static_cast<const ZDesc*>(dd), cv.g, w, w + cv.b_off, reinterpret_cast<float*>(w + cv.part_off),
+          static_cast<int*>(derr));
+      k_zreduce<<<dim3(rblocks, (unsigned)ndesc), 256, 0, s>>>(static_cast<const ZDesc*>(dd), cv.g.ksplit, max_m,
+                                                               max_n, reinterpret_cast<float*>(w + cv.part_off));
+      ok = ok && cudaEventRecord(e1, s) == cudaSuccess && cudaEventSynchronize(e1) == cudaSuccess;
+      float ms = 0.0f;
+      if (ok) ok = cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess;
+      if (rep == 1 || (rep == 2 && ms < t)) t = ms;
+    }
+    if (!ok) break;
+    entry.timed.push_back({cand[i], t});
+    if (i == 0 || t < best) {
+      best = t;
+      entry.chosen = cand[i];
+    }
+  }
+  int herr = 0;
+  if (ok && cudaMemcpy(&herr, derr, sizeof(int), cudaMemcpyDeviceToHost) == cudaSuccess && herr) ok = false;
+  if (!ok) entry.chosen = rule;  // a failed measurement keeps the rule's count
+  cudaGetLastError();
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  if (s) cudaStreamDestroy(s);
+  cudaFree(work);
+  cudaFree(c);
+  cudaFree(dd);
+  cudaFree(derr);
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  g_tuned.push_back(entry);
+  return entry.chosen;
+}
+
+std::string tuning_report() {
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  std::string out = "[";
+  for (size_t i = 0; i < g_tuned.size(); ++i) {
+    const TuneEntry& e = g_tuned[i];
+    char head[160];
+    std::snprintf(head, sizeof head, "%s{\"product\": \"A^H B\", \"ndesc\": %d, \"m\": %d, \"n\": %d, \"k\": %d, "
+                  "\"ksplit\": %d, \"timed_ms\": {", i ? ", " : "", e.ndesc, e.m, e.n, e.k, e.chosen);
+    out += head;
+    for (size_t j = 0; j < e.timed.size(); ++j) {
+      char item[48];
+      std::snprintf(item, sizeof item, "%s\"%d\": %.4f", j ? ", " : "", e.timed[j].first, e.timed[j].second);
+      out += item;
+    }
+    out += "}}";
+  }
+  return out + "]";
+}
+
 int tn_ksplit(int ndesc, int max_m, int max_n, int max_k) {
   const int trb = b_tile_rows(max_n);
   const int64_t tiles = (int64_t)((max_m + kTileM - 1) / kTileM) * ((2 * max_n + trb - 1) / trb) * std::max(ndesc, 1);
@@ -581,11 +705,21 @@ cudaError_t split_a(int mode, const double2* A, int64_t lda, int M, int K, unsig
 }  // namespace bg
 
 // ------------------------------------------------------------------ C ABI
+#include <cstring>
 #include <string>
 
 #include "op_internal.h"
 
 using namespace bg;
+
+extern "C" int bg_autotune_report(char* buf, int64_t capacity) {
+  const std::string r = tc::tuning_report();
+  if (!buf || capacity <= 0) return (int)r.size() + 1;
+  const size_t n = std::min<size_t>(r.size(), (size_t)capacity - 1);
+  std::memcpy(buf, r.data(), n);
+  buf[n] = 0;
+  return (int)r.size() + 1;
+}
 
 extern "C" int bg_zgemm_bf16x3(bg_ctx* ctx, int32_t mode, int64_t m, int64_t n, int64_t k, const double* a,
                                int64_t lda, const double* b, int64_t ldb, double* c, int64_t ldc, int32_t op,

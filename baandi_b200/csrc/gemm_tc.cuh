@@ -25,6 +25,7 @@
 
 #include <cstddef>
 #include <cstdint>
+#include <string>
 
 namespace bg {
 namespace tc {
@@ -75,8 +76,19 @@ size_t workspace_bytes(int mode, int ndesc, int max_m, int max_n, int max_k, int
 int launch_zgemm(int mode, const ZDesc* d_desc, int ndesc, int max_m, int max_n, int max_k, int ksplit,
                  bool a_presplit, void* work, int* err, cudaStream_t s);
 
-// A split count that fills whole waves of 148 SMs for a kTN product.
+// A split count that fills whole waves of 148 SMs for a kTN product (at most 4,096 complex
+// K per split).
 int tn_ksplit(int ndesc, int max_m, int max_n, int max_k);
+
+// The autotuner's split count for a kTN product of these bounds: the candidates that fill
+// whole waves (from the accuracy bound's minimum) timed once per shape on scratch panels
+// (product pass and reduction, CUDA events on a private stream, best of two after a warm
+// launch), the fastest kept for the process; the rule's count when a measurement fails.
+// Synchronous; never call it inside a stream capture.
+int tn_ksplit_tuned(int ndesc, int max_m, int max_n, int max_k);
+
+// The tuner's decisions so far as a JSON array.
+std::string tuning_report();
 
 // Writes A of a `mode` product (kTN: K x M, kNN: M x K, ld lda) as a panel of
 // a_panel_bytes(M, K) bytes (K tiles: k_tiles(K)).

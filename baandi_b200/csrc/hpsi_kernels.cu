@@ -1018,7 +1018,7 @@ int ensure_nonlocal_tc(TcNl* t, int nk, int nproj, int max_cols, int max_rows) {
     if (cudaMalloc(&t->err, sizeof(int)) != cudaSuccess) return 1;
     if (cudaMemset(t->err, 0, sizeof(int)) != cudaSuccess) return 1;
   }
-  t->ksplit = tc::tn_ksplit(nk, nproj, max_cols, max_rows);
+  t->ksplit = tc::tn_ksplit_tuned(nk, nproj, max_cols, max_rows);
   // the projection and the back-projection run one after the other on one stream and
   // share the workspace
   const size_t need = std::max(tc::workspace_bytes(tc::kTN, nk, nproj, max_cols, max_rows, t->ksplit, true),

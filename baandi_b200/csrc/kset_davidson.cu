@@ -571,15 +571,17 @@ __device__ bool eigen(const Bufs<D>& b, int cap, int m, double* red, int* sh) {
 // ------------------------------------------------------------------ batched large products
 // Descriptor arrays are laid out [slot][k]; blockIdx.z enumerates (slot, k).
 
-// C (+)= A B for every (slot, k) with a non-empty descriptor; 64 x 32 tiles.
+// C (+)= A B for every (slot, k) with a non-empty descriptor; 64 x 32 tiles.  blockIdx.x
+// runs over the column tiles, so the blocks that read one 64-row slice of the tall A
+// launch together and share it in L2.
 template <class D>
 __global__ void __launch_bounds__(128) k_dv_nn(const Bufs<D>* __restrict__ bufs, const NN<D>* __restrict__ desc,
                                                int nk) {
   const int z = blockIdx.z, k = z % nk;
   const NN<D> d = desc[z];
   const int rows = bufs[k].rows;
-  const int64_t r0 = (int64_t)blockIdx.x * 64;
-  const int j0 = blockIdx.y * 32;
+  const int64_t r0 = (int64_t)blockIdx.y * 64;
+  const int j0 = blockIdx.x * 32;
   if (d.n <= 0 || d.prec || j0 >= d.n || r0 >= rows) return;
   tiles::nn_tile<D, true>(d.A, rows, d.B, d.ldb, d.C, rows, rows, d.n, d.k, r0, j0, d.accumulate != 0);
 }
@@ -1485,7 +1487,7 @@ class KsetSolver {
     return 1;
   }
   int64_t nn(int nslots) {
-    const dim3 grid((unsigned)((max_rows_ + 63) / 64), (unsigned)((o_.cap + 31) / 32), (unsigned)(nslots * nk_));
+    const dim3 grid((unsigned)((o_.cap + 31) / 32), (unsigned)((max_rows_ + 63) / 64), (unsigned)(nslots * nk_));
     k_dv_nn<D><<<grid, 128, 0, s_>>>(d_bufs_, d_nn_, nk_);
     if (!tensor_products()) return 1;
     k_dv_tc_descs<D><<<1, 128, 0, s_>>>(d_bufs_, d_nn_, nslots, d_tn_, 0, nk_, d_tcnn_, d_tctn_);
@@ -1511,7 +1513,7 @@ class KsetSolver {
     int rc;
     if ((rc = cuda(tc::prepare_zgemm(), "tensor-core product attributes"))) return rc;
     const int slots = std::max(kNnSlots, kTnSlots);
-    tc_ks_ = tc::tn_ksplit(kTnSlots * nk_, o_.cap, o_.cap, max_rows_);
+    tc_ks_ = tc::tn_ksplit_tuned(kTnSlots * nk_, o_.cap, o_.cap, max_rows_);
     if ((rc = alloc(&d_tcnn_, (size_t)slots * nk_)) || (rc = alloc(&d_tctn_, (size_t)slots * nk_)) ||
         (rc = alloc(&tc_work_, std::max(tc::workspace_bytes(tc::kTN, kTnSlots * nk_, o_.cap, o_.cap, max_rows_,
                                                              tc_ks_, false),

@@ -438,6 +438,7 @@ def run_ours(args):
             "e2e_pinned": {"value": e2e_pinned, "unit": "bands/s", "h2d_bytes_per_step": h2d,
                            "d2h_bytes_per_step": d2h},
             "gpu_launches": launches, "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks,
+            "autotune": _lib_autotune(),
             "scf": scf, "scf_si64": scf64, "fp32_local": fp32, "tensor_apply": tensor, "reduced_solve": reduced,
         }
         print(json.dumps(line), flush=True)
@@ -487,6 +488,12 @@ def precision_leg(kset, xs, ys, stream, flush, steps, stages, precision=None):
     return {"value": bands * steps / (sum(ms) / 1000.0), "unit": "bands/s", "ms_per_step": sum(ms) / steps,
             "max_column_rel_diff_vs_fp64": err,
             "stage_ms": {s: float(m) for s, m in zip(stages, stage_ms / steps)}}
+
+
+def _lib_autotune():
+    """The split-K counts the library's autotuner chose in this run, with their timings."""
+    from baandi_b200 import _lib
+    return _lib.autotune_report()
 
 
 def scf_leg(workload_name, ctx):

@@ -383,6 +383,12 @@ int bg_kset_davidson_solve_hx(bg_kset* set, const double* const* start, const do
                               double* const* eigenvalues, double* const* eigenvectors, double* const* eigenvectors_hx,
                               int32_t* const* converged, bg_davidson_stats* stats);
 
+/* The autotuner's decisions so far (the split-K counts of the tensor-core A^H B products,
+ * timed once per shape when a precision-form apply or solve first needs them) as a JSON
+ * array with the measured times: written to buf (capacity bytes, NUL-terminated,
+ * truncated to fit); returns the bytes the whole report needs. */
+int bg_autotune_report(char* buf, int64_t capacity);
+
 /* The generalised Hermitian eigenproblem H C = S C diag(w) of one m x m pencil (m <=
  * 1152; column-major host matrices, interleaved complex when is_complex), solved the way
  * bg_kset_davidson_solve solves its reduced problem beyond capacity 128: the Cholesky

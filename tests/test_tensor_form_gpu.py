@@ -91,3 +91,28 @@ def test_tensor_scf_energy_matches_fp64(ctx):
     assert plain.converged and tensor.converged
     assert abs(tensor.energy_ha - plain.energy_ha) <= 1e-6 * w.natoms
     assert any(r.tensor_iterations > 0 for r in tensor.records)
+
+
+def test_autotuner_times_the_projection_split(ctx):
+    """A tensor-form apply tunes the split-K count of its projection once per shape: the
+    report lists the timed counts (each at least the accuracy bound's minimum of one split
+    per 4,096 complex K) and the fastest one is kept."""
+    w = W.si8_k444()
+    pw = w.plane_waves(w.kpoints[2][0])
+    nl = w.nonlocal_table(pw)
+    nproj = int(nl.table.shape[1])   # the table is (npw, nproj)
+    op = ComplexHamiltonian.new_owned(pw, w.dims(), nl, 24, ctx)
+    op.set_owned_potential(w.ionic_potential(), 1)
+    x = w.random_block(pw.npw, 24, seed_offset=4)
+    op.precision = L.BG_PREC_TENSOR
+    y = op.apply_block(x)
+    op.precision = L.BG_PREC_FP64
+    ref = op.apply_block(x)
+    assert np.max(np.linalg.norm(y - ref, axis=0) / np.linalg.norm(ref, axis=0)) < 2e-5
+    entries = [e for e in L.autotune_report() if e["m"] == nproj and e["k"] == pw.npw and e["n"] == 24]
+    assert len(entries) == 1
+    e = entries[0]
+    timed = {int(k): v for k, v in e["timed_ms"].items()}
+    assert timed and e["ksplit"] in timed
+    assert timed[e["ksplit"]] == min(timed.values())
+    assert min(timed) >= -(-2 * pw.npw // 32) // 256
