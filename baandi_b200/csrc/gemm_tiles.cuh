@@ -104,17 +104,26 @@ __device__ __forceinline__ void tn_tile(const D* __restrict__ A, int64_t lda, co
 // 48 x 48 tiles of P = A^H B for the Davidson's Grams (m, n <= the basis capacity, 48 for
 // the k-point cells): 256 threads; thread (ti, tj) = (lane mod 16, 2 warp + lane / 16)
 // owns outputs i = i0 + ti + 16 a, j = j0 + 3 tj + b (a, b < 3).  A warp's columns are
-// uniform, so a warp whose columns all lie at or beyond n skips the arithmetic; the 16 A
-// entries a warp reads per row are shared by its two half-warps and its B entries are two
-// words, so shared memory serves 9 complex multiply-adds per thread with 8 wavefronts per
-// warp.  kBK48 rows per cp.async step, double-buffered (24 KB of shared memory).
-constexpr int kBK48 = 8;
+// uniform, so a warp whose columns all lie at or beyond n skips the arithmetic.  The rows
+// stream through kStages48 shared-memory stages of kBK48 rows each, filled by cp.async
+// kStages48 - 1 stages ahead of the arithmetic; a stage holds each column's kBK48 rows
+// contiguously with a pitch of kBK48 + 1 elements, so both the fill (consecutive threads,
+// consecutive rows) and the arithmetic's reads (16 columns of one row per half-warp, 17
+// elements apart) meet no bank conflicts.  Dynamic shared memory: tn48_smem_bytes<D>().
+constexpr int kBK48 = 16;
+constexpr int kStages48 = 4;
+constexpr int kPitch48 = kBK48 + 1;
+template <class D>
+constexpr size_t tn48_smem_bytes() {
+  return (size_t)2 * kStages48 * 48 * kPitch48 * sizeof(D);
+}
 template <class D>
 __device__ __forceinline__ void tn_tile48(const D* __restrict__ A, int64_t lda, const D* __restrict__ B,
                                           int64_t ldb, int i0, int j0, int m, int n, int64_t r0, int64_t r1,
                                           D* __restrict__ P, int64_t ldp) {
-  __shared__ __align__(16) D As[2][kBK48][48];
-  __shared__ __align__(16) D Bs[2][kBK48][48];
+  extern __shared__ __align__(16) unsigned char tn48_smem[];
+  D* As = reinterpret_cast<D*>(tn48_smem);  // [stage][48 columns][kPitch48 rows]
+  D* Bs = As + kStages48 * 48 * kPitch48;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int ti = lane & 15, tj = 2 * warp + (lane >> 4);
   const bool warp_live = j0 + 6 * warp < n;
@@ -123,12 +132,13 @@ __device__ __forceinline__ void tn_tile48(const D* __restrict__ A, int64_t lda, 
   for (int a = 0; a < 3; ++a)
 #pragma unroll
     for (int b = 0; b < 3; ++b) acc[a][b] = Arith<D>::zero();
+  // one stage: kBK48 rows x 48 columns of A and of B, 6 elements per thread
   auto load = [&](int buf, int64_t rb) {
-    for (int e = tid; e < 2 * kBK48 * 48; e += 256) {
-      const int mat = e / (kBK48 * 48), idx = e - mat * (kBK48 * 48);
+    for (int e = tid; e < 2 * 48 * kBK48; e += 256) {
+      const int mat = e / (48 * kBK48), idx = e - mat * (48 * kBK48);
       const int rr = idx % kBK48, c = idx / kBK48;
       const int64_t r = rb + rr;
-      D* dst = mat == 0 ? &As[buf][rr][c] : &Bs[buf][rr][c];
+      D* dst = (mat == 0 ? As : Bs) + (buf * 48 + c) * kPitch48 + rr;
       const bool ok = r < r1 && (mat == 0 ? i0 + c < m : j0 + c < n);
       if (ok)
         async_copy(dst, mat == 0 ? A + (int64_t)(i0 + c) * lda + r : B + (int64_t)(j0 + c) * ldb + r);
@@ -138,24 +148,33 @@ __device__ __forceinline__ void tn_tile48(const D* __restrict__ A, int64_t lda, 
     async_commit();
   };
   const int64_t steps = (r1 - r0 + kBK48 - 1) / kBK48;
-  if (steps > 0) load(0, r0);
+  // one cp.async group per stage, empty ones past the end, so that waiting for all but
+  // the newest kStages48 - 2 groups always means the current stage has landed
+#pragma unroll
+  for (int s = 0; s < kStages48 - 1; ++s) {
+    if (s < steps)
+      load(s, r0 + s * kBK48);
+    else
+      async_commit();
+  }
   for (int64_t s = 0; s < steps; ++s) {
-    const int cur = s & 1;
-    if (s + 1 < steps) {
-      load(cur ^ 1, r0 + (s + 1) * kBK48);
-      async_wait<1>();
-    } else {
-      async_wait<0>();
-    }
-    __syncthreads();
+    async_wait<kStages48 - 2>();
+    __syncthreads();  // stage s visible to all; every thread is done with stage s - 1
+    const int64_t nxt = s + kStages48 - 1;
+    if (nxt < steps)
+      load((int)(nxt % kStages48), r0 + nxt * kBK48);  // refills the buffer of stage s - 1
+    else
+      async_commit();
     if (warp_live) {
+      const D* as = As + (int)(s % kStages48) * 48 * kPitch48;
+      const D* bs = Bs + (int)(s % kStages48) * 48 * kPitch48;
 #pragma unroll
       for (int rr = 0; rr < kBK48; ++rr) {
         D a[3], b[3];
 #pragma unroll
         for (int q = 0; q < 3; ++q) {
-          a[q] = As[cur][rr][ti + 16 * q];
-          b[q] = Bs[cur][rr][3 * tj + q];
+          a[q] = as[(ti + 16 * q) * kPitch48 + rr];
+          b[q] = bs[(3 * tj + q) * kPitch48 + rr];
         }
 #pragma unroll
         for (int x = 0; x < 3; ++x)
@@ -163,8 +182,8 @@ __device__ __forceinline__ void tn_tile48(const D* __restrict__ A, int64_t lda, 
           for (int y = 0; y < 3; ++y) acc[x][y] = Arith<D>::cmac(acc[x][y], a[x], b[y]);
       }
     }
-    __syncthreads();
   }
+  async_wait<0>();
 #pragma unroll
   for (int x = 0; x < 3; ++x)
 #pragma unroll

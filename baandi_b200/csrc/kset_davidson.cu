@@ -1497,8 +1497,8 @@ class KsetSolver {
   bool tensor_products() const { return o_.tensor && sizeof(D) == sizeof(double2) && tc_ready_; }
   int64_t tn(int nslots) {
     const unsigned t = (unsigned)((o_.cap + 47) / 48);
-    k_dv_tn<D><<<dim3(t, t, (unsigned)(nslots * nk_ * ksplit_)), 256, 0, s_>>>(d_bufs_, d_tn_, nk_, ksplit_,
-                                                                             slot_elems_);
+    k_dv_tn<D><<<dim3(t, t, (unsigned)(nslots * nk_ * ksplit_)), 256, tiles::tn48_smem_bytes<D>(), s_>>>(
+        d_bufs_, d_tn_, nk_, ksplit_, slot_elems_);
     const unsigned blocks = (unsigned)std::min<int64_t>(((int64_t)o_.cap * o_.cap + 255) / 256, 64);
     k_dv_tn_sum<D><<<dim3(blocks, 1, (unsigned)(nslots * nk_)), 256, 0, s_>>>(d_bufs_, d_tn_, nk_, ksplit_,
                                                                               slot_elems_);
@@ -1650,6 +1650,9 @@ int KsetSolver<T>::prepare() {
     return rc;
   if ((rc = cuda(cudaFuncSetAttribute((const void*)k_dv_ctl<D>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)ctl_smem()),
+                 "cudaFuncSetAttribute")) ||
+      (rc = cuda(cudaFuncSetAttribute((const void*)k_dv_tn<D>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)tiles::tn48_smem_bytes<D>()),
                  "cudaFuncSetAttribute")))
     return rc;
   if (ks_->dense) {
