@@ -103,10 +103,23 @@ namespace {
 
 // Split of the P^H X reduction over rows: enough (tile, split) blocks for about eight
 // 64-thread tile blocks per SM (148 SMs), chunks a multiple of 32 rows.
+// Row splits of the projection P^H X over `tiles` 48 x 48 output tiles (k_project: 256
+// threads, two blocks per SM): the smallest count whose blocks fill at least 85 % of
+// whole waves of 2 x 148 blocks, at least 128 rows per split; kchunk = rows per split.
 int ksplit_tiles(int64_t rows, int64_t tiles, int* kchunk, int64_t ks_cap = 1 << 30) {
-  int64_t ks = std::max<int64_t>(1, (8 * 148 + tiles - 1) / tiles);
-  ks = std::min<int64_t>(ks, std::max<int64_t>(1, ks_cap));
-  ks = std::min<int64_t>(ks, (rows + 31) / 32);
+  const int64_t slots = 2 * 148;
+  const int64_t max_ks = std::max<int64_t>(1, std::min<int64_t>({64, (rows + 127) / 128, ks_cap}));
+  int64_t ks = 1;
+  double best = 0.0;
+  for (int64_t k = 1; k <= max_ks; ++k) {
+    const int64_t blocks = tiles * k, waves = (blocks + slots - 1) / slots;
+    const double eff = (double)blocks / (double)(waves * slots);
+    if (eff > best + 1e-9) {
+      best = eff;
+      ks = k;
+    }
+    if (eff >= 0.85) break;
+  }
   int64_t chunk = (rows + ks - 1) / ks;
   chunk = ((chunk + 31) / 32) * 32;
   ks = (rows + chunk - 1) / chunk;
@@ -115,14 +128,7 @@ int ksplit_tiles(int64_t rows, int64_t tiles, int* kchunk, int64_t ks_cap = 1 <<
 }
 
 int ksplit_for(int64_t rows, int nproj, int64_t cols, int* kchunk) {
-  const int64_t tiles = ((nproj + 31) / 32) * ((cols + 31) / 32);
-  int64_t ks = std::max<int64_t>(1, (8 * 148 + tiles - 1) / tiles);
-  ks = std::min<int64_t>(ks, (rows + 31) / 32);
-  int64_t chunk = (rows + ks - 1) / ks;
-  chunk = ((chunk + 31) / 32) * 32;
-  ks = (rows + chunk - 1) / chunk;
-  *kchunk = (int)chunk;
-  return (int)ks;
+  return ksplit_tiles(rows, (int64_t)((nproj + 47) / 48) * ((cols + 47) / 48), kchunk);
 }
 
 // Build the stick plan, the tables and the nonlocal operands of one operator.
@@ -915,7 +921,7 @@ int enqueue_range(bg_kset* ks, int k0, int k1, const CallArgs* args, const int64
     NlShape sh = ks->shape;
     int64_t tiles = 0, cap = 1 << 30;
     for (int k = k0; k < k1; ++k) {
-      tiles += ((sh.nproj + 31) / 32) * ((cols[k] + 31) / 32);
+      tiles += ((sh.nproj + 47) / 48) * ((cols[k] + 47) / 48);
       if (cols[k] > 0) cap = std::min<int64_t>(cap, ks->ops[k]->part_cols / cols[k]);
     }
     sh.ksplit = ksplit_tiles(max_rows, std::max<int64_t>(tiles, 1), &sh.kchunk, cap);

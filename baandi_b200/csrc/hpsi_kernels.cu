@@ -440,17 +440,17 @@ struct Ops<double2> {
 
 // part[ks][c][p] = sum_{rows of chunk ks} P[p][row]^* X[c][row]; tile 32 p x 32 c.
 template <class T>
-__global__ void __launch_bounds__(64) k_project(const NlDev* __restrict__ nls, int nproj, int ksplit, int kchunk,
-                                                Batch b) {
+__global__ void __launch_bounds__(256, 2) k_project(const NlDev* __restrict__ nls, int nproj, int ksplit,
+                                                    int kchunk, Batch b) {
   const int kb = blockIdx.z / ksplit, ks = blockIdx.z - kb * ksplit;
   const NlDev& nl = nls[kb];
   const CallArgs ca = resolve(b.a[kb]);
   const int cols = ca.cols, rows = nl.rows;
-  if ((int)blockIdx.y * 32 >= cols) return;
+  if ((int)blockIdx.y * 48 >= cols) return;
   const int64_t r0 = (int64_t)ks * kchunk, r1 = min((int64_t)rows, r0 + kchunk);
-  tiles::tn_tile<T>(reinterpret_cast<const T*>(nl.p), rows, reinterpret_cast<const T*>(ca.x),
-                    ca.ldx / (int64_t)(sizeof(T) / sizeof(double)), blockIdx.x * 32, blockIdx.y * 32, nproj, cols, r0,
-                    r1, reinterpret_cast<T*>(nl.part) + (int64_t)ks * cols * nproj, nproj);
+  tiles::tn_tile48<T>(reinterpret_cast<const T*>(nl.p), rows, reinterpret_cast<const T*>(ca.x),
+                      ca.ldx / (int64_t)(sizeof(T) / sizeof(double)), blockIdx.x * 48, blockIdx.y * 48, nproj, cols,
+                      r0, r1, reinterpret_cast<T*>(nl.part) + (int64_t)ks * cols * nproj, nproj);
 }
 
 // wd[c][off+i] = sum_j D[i][j] (sum_ks part[ks][c][off+j]) for one (atom, column).
@@ -911,16 +911,22 @@ int launch_nonlocal(const NlDev* nl, int gamma, const NlShape& sh, int max_rows,
   int max_cols = 0;
   for (int k = 0; k < b.nk; ++k) max_cols = max(max_cols, b.a[k].cols);
   if (sh.nproj == 0 || max_cols == 0 || b.nk == 0) return 0;
-  const dim3 pg((sh.nproj + 31) / 32, (max_cols + 31) / 32, sh.ksplit * b.nk);
+  const dim3 pg((sh.nproj + 47) / 48, (max_cols + 47) / 48, sh.ksplit * b.nk);
   const dim3 cg(sh.natoms, max_cols, b.nk);
   const dim3 bg_((max_rows + 63) / 64, (max_cols + 31) / 32, b.nk);
   const int cth = ((sh.maxch + 31) / 32) * 32;
   if (gamma) {
-    { StageScope sc(ev, 3, s); k_project<double><<<pg, 64, 0, s>>>(nl, sh.nproj, sh.ksplit, sh.kchunk, b); }
+    {
+      StageScope sc(ev, 3, s);
+      k_project<double><<<pg, 256, tiles::tn48_smem_bytes<double>(), s>>>(nl, sh.nproj, sh.ksplit, sh.kchunk, b);
+    }
     { StageScope sc(ev, 4, s); k_couple<double><<<cg, cth, 0, s>>>(nl, sh.nproj, sh.ksplit, b); }
     { StageScope sc(ev, 5, s); k_back<double><<<bg_, 128, 0, s>>>(nl, sh.nproj, b); }
   } else {
-    { StageScope sc(ev, 3, s); k_project<double2><<<pg, 64, 0, s>>>(nl, sh.nproj, sh.ksplit, sh.kchunk, b); }
+    {
+      StageScope sc(ev, 3, s);
+      k_project<double2><<<pg, 256, tiles::tn48_smem_bytes<double2>(), s>>>(nl, sh.nproj, sh.ksplit, sh.kchunk, b);
+    }
     { StageScope sc(ev, 4, s); k_couple<double2><<<cg, cth, 0, s>>>(nl, sh.nproj, sh.ksplit, b); }
     { StageScope sc(ev, 5, s); k_back<double2><<<bg_, 128, 0, s>>>(nl, sh.nproj, b); }
   }
@@ -964,6 +970,12 @@ static void configure_one(cudaError_t& e, size_t plane_smem, size_t stick_smem) 
 
 int configure_kernels(size_t plane_smem, size_t stick_smem) {
   cudaError_t e = cudaSuccess;
+  e = cudaFuncSetAttribute((const void*)k_project<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)tiles::tn48_smem_bytes<double>());
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute((const void*)k_project<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)tiles::tn48_smem_bytes<double2>());
+  if (e != cudaSuccess) return 1;
   e = cudaFuncSetAttribute((const void*)k_planes, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)plane_smem);
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute((const void*)k_density_planes, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)plane_smem);
