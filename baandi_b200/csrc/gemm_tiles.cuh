@@ -277,6 +277,109 @@ __device__ __forceinline__ void nn_tile(const D* __restrict__ A, int64_t lda, co
     }
 }
 
+// 64 x 64 tiles of C (+)= A B, A tall (rows x k, column-major), B small (k x n): 256
+// threads; thread (tr, tc) = (tid mod 16, tid / 16) owns rows r0 + tr + 16 x and columns
+// j0 + tc + 16 y (x, y < 4).  The inner index streams through kStages64 shared-memory
+// stages of kBK rows of A (64 rows each, contiguous as in memory) and kBK entries of each
+// of 64 columns of B (a column's entries contiguous, pitch kBK + 1), filled by cp.async
+// kStages64 - 1 stages ahead; neither the fill nor the arithmetic's reads meet bank
+// conflicts.  SKIP_EMPTY skips the 16-column groups at or beyond n.  Dynamic shared
+// memory: nn64_smem_bytes<D>().
+constexpr int kStages64 = 3;
+constexpr int kPitchB64 = kBK + 1;
+template <class D>
+constexpr size_t nn64_smem_bytes() {
+  return (size_t)kStages64 * (kBK * 64 + 64 * kPitchB64) * sizeof(D);
+}
+template <class D, bool SKIP_EMPTY = false>
+__device__ __forceinline__ void nn_tile64(const D* __restrict__ A, int64_t lda, const D* __restrict__ B,
+                                          int64_t ldb, D* __restrict__ C, int64_t ldc, int64_t rows, int n, int k,
+                                          int64_t r0, int j0, bool accumulate) {
+  extern __shared__ __align__(16) unsigned char nn64_smem[];
+  D* As = reinterpret_cast<D*>(nn64_smem);     // [stage][kBK][64 rows]
+  D* Bs = As + kStages64 * kBK * 64;           // [stage][64 columns][kPitchB64]
+  const int tid = threadIdx.x;
+  const int tr = tid & 15, tc = tid >> 4;
+  D acc[4][4];
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) acc[a][b] = Arith<D>::zero();
+  auto load = [&](int buf, int pb) {
+    D* as = As + buf * kBK * 64;
+    D* bs = Bs + buf * 64 * kPitchB64;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {  // A: kBK x 64, consecutive threads on consecutive rows
+      const int e = tid + 256 * q;
+      const int rr = e & 63, p = e >> 6;
+      const int64_t r = r0 + rr;
+      D* d = as + p * 64 + rr;
+      if (r < rows && pb + p < k)
+        async_copy(d, A + (int64_t)(pb + p) * lda + r);
+      else
+        *d = Arith<D>::zero();
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {  // B: 64 columns x kBK, consecutive threads on consecutive entries
+      const int e = tid + 256 * q;
+      const int p = e & (kBK - 1), c = e >> 4;
+      D* d = bs + c * kPitchB64 + p;
+      if (pb + p < k && j0 + c < n)
+        async_copy(d, B + (int64_t)(j0 + c) * ldb + pb + p);
+      else
+        *d = Arith<D>::zero();
+    }
+    async_commit();
+  };
+  const int ny = SKIP_EMPTY ? min(4, max(0, (n - j0 - tc + 15) / 16)) : 4;
+  const int steps = (k + kBK - 1) / kBK;
+#pragma unroll
+  for (int s = 0; s < kStages64 - 1; ++s) {
+    if (s < steps)
+      load(s, s * kBK);
+    else
+      async_commit();
+  }
+  for (int s = 0; s < steps; ++s) {
+    async_wait<kStages64 - 2>();
+    __syncthreads();  // stage s visible to all; every thread is done with stage s - 1
+    const int nxt = s + kStages64 - 1;
+    if (nxt < steps)
+      load(nxt % kStages64, nxt * kBK);  // refills the buffer of stage s - 1
+    else
+      async_commit();
+    const D* as = As + (s % kStages64) * kBK * 64;
+    const D* bs = Bs + (s % kStages64) * 64 * kPitchB64;
+#pragma unroll
+    for (int p = 0; p < kBK; ++p) {
+      D a[4], b[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        a[q] = as[p * 64 + q * 16 + tr];
+        b[q] = bs[(q * 16 + tc) * kPitchB64 + p];
+      }
+#pragma unroll
+      for (int y = 0; y < 4; ++y)
+        if (y < ny) {
+#pragma unroll
+          for (int x = 0; x < 4; ++x) acc[x][y] = Arith<D>::mac(acc[x][y], a[x], b[y]);
+        }
+    }
+  }
+  async_wait<0>();
+#pragma unroll
+  for (int x = 0; x < 4; ++x)
+#pragma unroll
+    for (int y = 0; y < 4; ++y) {
+      const int64_t r = r0 + x * 16 + tr;
+      const int j = j0 + y * 16 + tc;
+      if (r < rows && j < n) {
+        D& out = C[(int64_t)j * ldc + r];
+        out = accumulate ? Arith<D>::add(out, acc[x][y]) : acc[x][y];
+      }
+    }
+}
+
 }  // namespace tiles
 }  // namespace bg
 

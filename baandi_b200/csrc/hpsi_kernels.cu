@@ -484,16 +484,16 @@ __global__ void k_couple(const NlDev* __restrict__ nls, int nproj, int ksplit, B
 
 // y[c][row] += sum_p P[p][row] wd[c][p]; tile 64 rows x 32 columns.
 template <class T>
-__global__ void __launch_bounds__(128) k_back(const NlDev* __restrict__ nls, int nproj, Batch b) {
+__global__ void __launch_bounds__(256, 2) k_back(const NlDev* __restrict__ nls, int nproj, Batch b) {
   const NlDev& nl = nls[blockIdx.z];
   const CallArgs ca = resolve(b.a[blockIdx.z]);
   const int cols = ca.cols, rows = nl.rows;
   const int64_t r0 = (int64_t)blockIdx.x * 64;
-  const int j0 = blockIdx.y * 32;
+  const int j0 = blockIdx.y * 64;
   if (r0 >= rows || j0 >= cols) return;
-  tiles::nn_tile<T>(reinterpret_cast<const T*>(nl.p), rows, reinterpret_cast<const T*>(nl.wd), nproj,
-                    reinterpret_cast<T*>(ca.y), ca.ldy / (int64_t)(sizeof(T) / sizeof(double)), rows, cols, nproj, r0,
-                    j0, true);
+  tiles::nn_tile64<T>(reinterpret_cast<const T*>(nl.p), rows, reinterpret_cast<const T*>(nl.wd), nproj,
+                      reinterpret_cast<T*>(ca.y), ca.ldy / (int64_t)(sizeof(T) / sizeof(double)), rows, cols, nproj,
+                      r0, j0, true);
 }
 
 // ---------------------------------------------------------------- band density
@@ -913,7 +913,7 @@ int launch_nonlocal(const NlDev* nl, int gamma, const NlShape& sh, int max_rows,
   if (sh.nproj == 0 || max_cols == 0 || b.nk == 0) return 0;
   const dim3 pg((sh.nproj + 47) / 48, (max_cols + 47) / 48, sh.ksplit * b.nk);
   const dim3 cg(sh.natoms, max_cols, b.nk);
-  const dim3 bg_((max_rows + 63) / 64, (max_cols + 31) / 32, b.nk);
+  const dim3 bg_((max_rows + 63) / 64, (max_cols + 63) / 64, b.nk);
   const int cth = ((sh.maxch + 31) / 32) * 32;
   if (gamma) {
     {
@@ -921,14 +921,17 @@ int launch_nonlocal(const NlDev* nl, int gamma, const NlShape& sh, int max_rows,
       k_project<double><<<pg, 256, tiles::tn48_smem_bytes<double>(), s>>>(nl, sh.nproj, sh.ksplit, sh.kchunk, b);
     }
     { StageScope sc(ev, 4, s); k_couple<double><<<cg, cth, 0, s>>>(nl, sh.nproj, sh.ksplit, b); }
-    { StageScope sc(ev, 5, s); k_back<double><<<bg_, 128, 0, s>>>(nl, sh.nproj, b); }
+    { StageScope sc(ev, 5, s); k_back<double><<<bg_, 256, tiles::nn64_smem_bytes<double>(), s>>>(nl, sh.nproj, b); }
   } else {
     {
       StageScope sc(ev, 3, s);
       k_project<double2><<<pg, 256, tiles::tn48_smem_bytes<double2>(), s>>>(nl, sh.nproj, sh.ksplit, sh.kchunk, b);
     }
     { StageScope sc(ev, 4, s); k_couple<double2><<<cg, cth, 0, s>>>(nl, sh.nproj, sh.ksplit, b); }
-    { StageScope sc(ev, 5, s); k_back<double2><<<bg_, 128, 0, s>>>(nl, sh.nproj, b); }
+    {
+      StageScope sc(ev, 5, s);
+      k_back<double2><<<bg_, 256, tiles::nn64_smem_bytes<double2>(), s>>>(nl, sh.nproj, b);
+    }
   }
   return 3;
 }
@@ -975,6 +978,12 @@ int configure_kernels(size_t plane_smem, size_t stick_smem) {
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute((const void*)k_project<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)tiles::tn48_smem_bytes<double2>());
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute((const void*)k_back<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)tiles::nn64_smem_bytes<double>());
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute((const void*)k_back<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)tiles::nn64_smem_bytes<double2>());
   if (e != cudaSuccess) return 1;
   e = cudaFuncSetAttribute((const void*)k_planes, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)plane_smem);
   if (e == cudaSuccess)

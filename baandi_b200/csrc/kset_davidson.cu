@@ -571,19 +571,19 @@ __device__ bool eigen(const Bufs<D>& b, int cap, int m, double* red, int* sh) {
 // ------------------------------------------------------------------ batched large products
 // Descriptor arrays are laid out [slot][k]; blockIdx.z enumerates (slot, k).
 
-// C (+)= A B for every (slot, k) with a non-empty descriptor; 64 x 32 tiles.  blockIdx.x
+// C (+)= A B for every (slot, k) with a non-empty descriptor; 64 x 64 tiles.  blockIdx.x
 // runs over the column tiles, so the blocks that read one 64-row slice of the tall A
 // launch together and share it in L2.
 template <class D>
-__global__ void __launch_bounds__(128) k_dv_nn(const Bufs<D>* __restrict__ bufs, const NN<D>* __restrict__ desc,
-                                               int nk) {
+__global__ void __launch_bounds__(256, 2) k_dv_nn(const Bufs<D>* __restrict__ bufs, const NN<D>* __restrict__ desc,
+                                                  int nk) {
   const int z = blockIdx.z, k = z % nk;
   const NN<D> d = desc[z];
   const int rows = bufs[k].rows;
   const int64_t r0 = (int64_t)blockIdx.y * 64;
-  const int j0 = blockIdx.x * 32;
+  const int j0 = blockIdx.x * 64;
   if (d.n <= 0 || d.prec || j0 >= d.n || r0 >= rows) return;
-  tiles::nn_tile<D, true>(d.A, rows, d.B, d.ldb, d.C, rows, rows, d.n, d.k, r0, j0, d.accumulate != 0);
+  tiles::nn_tile64<D, true>(d.A, rows, d.B, d.ldb, d.C, rows, rows, d.n, d.k, r0, j0, d.accumulate != 0);
 }
 
 // Split-K partial Gram products: part[slot][s][j][i] = sum over row slice s of
@@ -1487,8 +1487,8 @@ class KsetSolver {
     return 1;
   }
   int64_t nn(int nslots) {
-    const dim3 grid((unsigned)((o_.cap + 31) / 32), (unsigned)((max_rows_ + 63) / 64), (unsigned)(nslots * nk_));
-    k_dv_nn<D><<<grid, 128, 0, s_>>>(d_bufs_, d_nn_, nk_);
+    const dim3 grid((unsigned)((o_.cap + 63) / 64), (unsigned)((max_rows_ + 63) / 64), (unsigned)(nslots * nk_));
+    k_dv_nn<D><<<grid, 256, tiles::nn64_smem_bytes<D>(), s_>>>(d_bufs_, d_nn_, nk_);
     if (!tensor_products()) return 1;
     k_dv_tc_descs<D><<<1, 128, 0, s_>>>(d_bufs_, d_nn_, nslots, d_tn_, 0, nk_, d_tcnn_, d_tctn_);
     return 2 + tc::launch_zgemm(tc::kNN, d_tcnn_, nslots * nk_, max_rows_, o_.cap, o_.cap, 1, false, tc_work_,
@@ -1653,6 +1653,9 @@ int KsetSolver<T>::prepare() {
                  "cudaFuncSetAttribute")) ||
       (rc = cuda(cudaFuncSetAttribute((const void*)k_dv_tn<D>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)tiles::tn48_smem_bytes<D>()),
+                 "cudaFuncSetAttribute")) ||
+      (rc = cuda(cudaFuncSetAttribute((const void*)k_dv_nn<D>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)tiles::nn64_smem_bytes<D>()),
                  "cudaFuncSetAttribute")))
     return rc;
   if (ks_->dense) {
