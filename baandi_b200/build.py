@@ -18,7 +18,7 @@ SOURCES = ["api.cu", "hpsi_kernels.cu", "davidson.cu", "noalloc.cu", "fields.cu"
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-lineinfo", "-O3", "-std=c++17",
-    "-Xcompiler", "-fPIC,-ffp-contract=off,-O3",
+    "-Xcompiler", "-fPIC,-ffp-contract=off,-O3,-fopenmp",
     "-Xptxas", "-v",
 ]
 
@@ -46,7 +46,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
     if not force and not stale():
         return LIB
     tmp = LIB + ".tmp"
-    cmd = [nvcc(), *NVCC_FLAGS, "-shared", "-o", tmp] + [os.path.join(CSRC, s) for s in SOURCES] + ["-lcudart"]
+    cmd = [nvcc(), *NVCC_FLAGS, "-shared", "-o", tmp] + [os.path.join(CSRC, s) for s in SOURCES] + ["-lcudart", "-lgomp"]
     res = subprocess.run(cmd, capture_output=True, text=True)
     if res.returncode != 0:
         sys.stderr.write(res.stdout + res.stderr)

@@ -1,6 +1,7 @@
 // C ABI of libbaandi_b200.so: contexts, operators (tables in HBM, stick plan, FFT
 // plans, nonlocal operands) and the apply entry points.  See include/baandi_gpu.h.
 #include <cuda_runtime.h>
+#include <omp.h>
 
 #include <algorithm>
 #include <cmath>
@@ -64,6 +65,35 @@ int alloc(bg_op* op, size_t bytes, void** out, DevBuf** keep = nullptr) {
   if (keep) *keep = b.get();
   op->bufs.push_back(std::move(b));
   return BG_OK;
+}
+
+// Host-buffer chunks of bg_kset_apply: about an eighth of the call's x per chunk, within
+// these bounds (enough chunks to overlap, few enough launches).
+constexpr size_t kChunkMin = (size_t)4 << 20, kChunkMax = (size_t)64 << 20;
+
+// A host pointer the driver would stage itself (not page-locked or registered).
+bool host_is_pageable(const void* p) {
+  cudaPointerAttributes at{};
+  if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+    cudaGetLastError();
+    return true;
+  }
+  return at.type == cudaMemoryTypeUnregistered;
+}
+
+// memcpy split over the host threads (pageable <-> pinned staging).
+void parallel_copy(void* dst, const void* src, size_t bytes) {
+  const int nt = bytes < ((size_t)4 << 20) ? 1 : std::min(16, std::max(1, omp_get_max_threads()));
+  if (nt == 1) {
+    std::memcpy(dst, src, bytes);
+    return;
+  }
+  const size_t per = ((bytes + nt - 1) / nt + 4095) / 4096 * 4096;
+#pragma omp parallel for num_threads(nt) schedule(static)
+  for (int t = 0; t < nt; ++t) {
+    const size_t o = (size_t)t * per;
+    if (o < bytes) std::memcpy(static_cast<char*>(dst) + o, static_cast<const char*>(src) + o, std::min(per, bytes - o));
+  }
 }
 
 }  // namespace
@@ -998,6 +1028,12 @@ int bg_kset_destroy(bg_kset* ks) {
     if (ks->in_done[i]) cudaEventDestroy(ks->in_done[i]);
     if (ks->work_done[i]) cudaEventDestroy(ks->work_done[i]);
   }
+  for (int i = 0; i < 2; ++i) {
+    if (ks->stage_in[i]) cudaFreeHost(ks->stage_in[i]);
+    if (ks->stage_out[i]) cudaFreeHost(ks->stage_out[i]);
+    if (ks->in_copied[i]) cudaEventDestroy(ks->in_copied[i]);
+    if (ks->out_copied[i]) cudaEventDestroy(ks->out_copied[i]);
+  }
   if (ks->dv_cache && ks->dv_free) ks->dv_free(ks->dv_cache);
   cudaFree(ks->d_vts);
   cudaFree(ks->d_errs);
@@ -1196,33 +1232,163 @@ int bg_kset_apply(bg_kset* ks, const double* const* x, double* const* y, const i
     e = cudaGetLastError();
     return e == cudaSuccess ? BG_OK : cuda_fail(ctx, e, "kernel launch");
   }
-  // Host buffers: chunks of operators flow through copy-in, compute and copy-out streams,
-  // so the transfers of one chunk overlap the kernels of its neighbours.
-  const int nch = std::min(n, (int)bg_kset::kChunks);
-  cudaStream_t in = ks->pipe[0], work = ks->pipe[1], out = ks->pipe[2];
-  for (int c = 0; c < nch; ++c) {
-    const int k0 = (int)((int64_t)n * c / nch), k1 = (int)((int64_t)n * (c + 1) / nch);
-    for (int k = k0; k < k1; ++k) {
-      if (cols[k] == 0) continue;
-      bg_op* op = ks->ops[k];
-      const size_t dpc = op->gamma ? (size_t)op->rows : (size_t)2 * op->rows;
-      e = cudaMemcpyAsync(const_cast<double*>(args[k].x), x[k], dpc * cols[k] * sizeof(double),
-                          cudaMemcpyHostToDevice, in);
-      if (e != cudaSuccess) return cuda_fail(ctx, e, "copy in");
+  // Host buffers: chunks (whole operators of one set, up to kChunkBytes together, or
+  // column blocks of one operator larger than that) flow through copy-in, compute and
+  // copy-out streams, so the transfers of one chunk overlap the kernels of its neighbours.
+  // Pageable blocks go through pinned staging slots that host threads fill and drain while
+  // the GPU works on the neighbouring chunks; pinned blocks are copied directly.
+  struct Unit {
+    int k;
+    int64_t c0, c1;  // columns
+  };
+  struct Chunk {
+    int k0, k1;  // operators [k0, k1); a column block when k1 == k0 + 1 and the unit is partial
+    std::vector<Unit> units;
+    size_t bytes = 0;
+  };
+  auto dpc_of = [&](int k) { return ks->ops[k]->gamma ? (size_t)ks->ops[k]->rows : (size_t)2 * ks->ops[k]->rows; };
+  size_t total = 0;
+  for (int k = 0; k < n; ++k) total += dpc_of(k) * sizeof(double) * (size_t)cols[k];
+  const size_t kChunkBytes = std::min(kChunkMax, std::max(kChunkMin, total / 8));
+  std::vector<Chunk> chunks;
+  for (int k = 0; k < n; ++k) {
+    if (cols[k] == 0) continue;
+    const size_t bpc = dpc_of(k) * sizeof(double);
+    const size_t bytes = bpc * (size_t)cols[k];
+    if (bytes > kChunkBytes) {
+      // column blocks of about kChunkBytes (even starts, so Gamma column pairs stay whole)
+      int64_t nb = (int64_t)((bytes + kChunkBytes - 1) / kChunkBytes);
+      int64_t per = (cols[k] + nb - 1) / nb;
+      per += per & 1;
+      for (int64_t c0 = 0; c0 < cols[k]; c0 += per) {
+        Chunk ch;
+        ch.k0 = k;
+        ch.k1 = k + 1;
+        ch.units.push_back({k, c0, std::min(cols[k], c0 + per)});
+        ch.bytes = bpc * (size_t)(ch.units[0].c1 - c0);
+        chunks.push_back(ch);
+      }
+      continue;
     }
-    cudaEventRecord(ks->in_done[c], in);
-    cudaStreamWaitEvent(work, ks->in_done[c], 0);
-    ks->launches += enqueue_range(ks, k0, k1, args.data(), cols, work, nullptr, precision);
-    cudaEventRecord(ks->work_done[c], work);
-    cudaStreamWaitEvent(out, ks->work_done[c], 0);
-    for (int k = k0; k < k1; ++k) {
-      if (cols[k] == 0) continue;
-      bg_op* op = ks->ops[k];
-      const size_t dpc = op->gamma ? (size_t)op->rows : (size_t)2 * op->rows;
-      e = cudaMemcpyAsync(y[k], args[k].y, dpc * cols[k] * sizeof(double), cudaMemcpyDeviceToHost, out);
-      if (e != cudaSuccess) return cuda_fail(ctx, e, "copy out");
+    if (chunks.empty() || chunks.back().k1 != k || chunks.back().bytes + bytes > kChunkBytes ||
+        chunks.back().units.back().c1 != cols[chunks.back().units.back().k]) {
+      Chunk ch;
+      ch.k0 = k;
+      ch.k1 = k;
+      chunks.push_back(ch);
     }
+    chunks.back().units.push_back({k, 0, cols[k]});
+    chunks.back().k1 = k + 1;
+    chunks.back().bytes += bytes;
   }
+  // which side of each operator is pageable (staged) and the staging slots
+  std::vector<char> x_staged(n, 0), y_staged(n, 0);
+  size_t slot = 0;
+  for (int k = 0; k < n; ++k) {
+    if (cols[k] == 0) continue;
+    x_staged[k] = host_is_pageable(x[k]);
+    y_staged[k] = host_is_pageable(y[k]);
+  }
+  for (const Chunk& ch : chunks) slot = std::max(slot, ch.bytes);
+  bool any_staged = false;
+  for (int k = 0; k < n; ++k) any_staged = any_staged || x_staged[k] || y_staged[k];
+  if (any_staged && slot > ks->stage_bytes) {
+    for (int i = 0; i < 2; ++i) {
+      if (ks->stage_in[i]) cudaFreeHost(ks->stage_in[i]);
+      if (ks->stage_out[i]) cudaFreeHost(ks->stage_out[i]);
+      ks->stage_in[i] = ks->stage_out[i] = nullptr;
+    }
+    ks->stage_bytes = 0;
+    for (int i = 0; i < 2; ++i) {
+      if ((e = cudaMallocHost(&ks->stage_in[i], slot)) != cudaSuccess ||
+          (e = cudaMallocHost(&ks->stage_out[i], slot)) != cudaSuccess)
+        return cuda_fail(ctx, e, "pinned staging");
+      if (!ks->in_copied[i] && (e = cudaEventCreateWithFlags(&ks->in_copied[i], cudaEventDisableTiming)) != cudaSuccess)
+        return cuda_fail(ctx, e, "cudaEventCreate");
+      if (!ks->out_copied[i] && (e = cudaEventCreateWithFlags(&ks->out_copied[i], cudaEventDisableTiming)) != cudaSuccess)
+        return cuda_fail(ctx, e, "cudaEventCreate");
+    }
+    ks->stage_bytes = slot;
+  }
+  cudaStream_t in = ks->pipe[0], work = ks->pipe[1], out = ks->pipe[2];
+  int rc_drain = BG_OK;
+  std::vector<CallArgs> cargs(args);
+  std::vector<int64_t> ccols(cols, cols + n);
+  // the pageable outputs of chunk i wait in out slot i % 2 until the host copies them out
+  auto drain = [&](int i) -> int {
+    const Chunk& ch = chunks[i];
+    bool staged = false;
+    for (const Unit& u : ch.units) staged = staged || y_staged[u.k];
+    if (!staged) return BG_OK;
+    cudaError_t ee = cudaEventSynchronize(ks->out_copied[i % 2]);
+    if (ee != cudaSuccess) return cuda_fail(ctx, ee, "copy out");
+    size_t off = 0;
+    for (const Unit& u : ch.units) {
+      const size_t b = dpc_of(u.k) * sizeof(double) * (size_t)(u.c1 - u.c0);
+      if (y_staged[u.k])
+        parallel_copy(reinterpret_cast<char*>(y[u.k]) + dpc_of(u.k) * sizeof(double) * (size_t)u.c0,
+                      static_cast<const char*>(ks->stage_out[i % 2]) + off, b);
+      off += b;
+    }
+    return BG_OK;
+  };
+  for (int i = 0; i < (int)chunks.size(); ++i) {
+    const Chunk& ch = chunks[i];
+    const int sl = i % 2;
+    // copy in: pageable units packed into in slot sl once chunk i - 2 has left it
+    bool xst = false;
+    for (const Unit& u : ch.units) xst = xst || x_staged[u.k];
+    if (xst && i >= 2 && (e = cudaEventSynchronize(ks->in_copied[sl])) != cudaSuccess)
+      return cuda_fail(ctx, e, "copy in");
+    size_t off = 0;
+    for (const Unit& u : ch.units) {
+      const size_t dpc = dpc_of(u.k), b = dpc * sizeof(double) * (size_t)(u.c1 - u.c0);
+      const char* src = reinterpret_cast<const char*>(x[u.k]) + dpc * sizeof(double) * (size_t)u.c0;
+      char* dst = reinterpret_cast<char*>(const_cast<double*>(args[u.k].x)) + dpc * sizeof(double) * (size_t)u.c0;
+      if (x_staged[u.k]) {
+        char* st = static_cast<char*>(ks->stage_in[sl]) + off;
+        parallel_copy(st, src, b);
+        src = st;
+      }
+      if ((e = cudaMemcpyAsync(dst, src, b, cudaMemcpyHostToDevice, in)) != cudaSuccess)
+        return cuda_fail(ctx, e, "copy in");
+      off += b;
+    }
+    if (xst) cudaEventRecord(ks->in_copied[sl], in);
+    cudaEventRecord(ks->in_done[i % bg_kset::kChunks], in);
+    cudaStreamWaitEvent(work, ks->in_done[i % bg_kset::kChunks], 0);
+    // compute: whole operators, or the chunk's column block of one operator
+    for (const Unit& u : ch.units) {
+      const size_t dpc = dpc_of(u.k);
+      CallArgs& a = cargs[u.k];
+      a = args[u.k];
+      a.x = args[u.k].x + dpc * (size_t)u.c0;
+      a.y = args[u.k].y + dpc * (size_t)u.c0;
+      a.cols = (int)(u.c1 - u.c0);
+      a.units = ks->ops[u.k]->gamma ? (int)((a.cols + 1) / 2) : a.cols;
+      ccols[u.k] = u.c1 - u.c0;
+    }
+    ks->launches += enqueue_range(ks, ch.k0, ch.k1, cargs.data(), ccols.data(), work, nullptr, precision);
+    cudaEventRecord(ks->work_done[i % bg_kset::kChunks], work);
+    cudaStreamWaitEvent(out, ks->work_done[i % bg_kset::kChunks], 0);
+    // copy out: chunk i - 2's staged outputs leave out slot sl first
+    if (i >= 2 && (rc_drain = drain(i - 2)) != BG_OK) return rc_drain;
+    bool yst = false;
+    off = 0;
+    for (const Unit& u : ch.units) {
+      const size_t dpc = dpc_of(u.k), b = dpc * sizeof(double) * (size_t)(u.c1 - u.c0);
+      const char* src = reinterpret_cast<const char*>(args[u.k].y) + dpc * sizeof(double) * (size_t)u.c0;
+      char* dst = y_staged[u.k] ? static_cast<char*>(ks->stage_out[sl]) + off
+                                : reinterpret_cast<char*>(y[u.k]) + dpc * sizeof(double) * (size_t)u.c0;
+      yst = yst || y_staged[u.k];
+      if ((e = cudaMemcpyAsync(dst, src, b, cudaMemcpyDeviceToHost, out)) != cudaSuccess)
+        return cuda_fail(ctx, e, "copy out");
+      off += b;
+    }
+    if (yst) cudaEventRecord(ks->out_copied[sl], out);
+  }
+  for (int i = std::max(0, (int)chunks.size() - 2); i < (int)chunks.size(); ++i)
+    if ((rc_drain = drain(i)) != BG_OK) return rc_drain;
   e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(ctx, e, "kernel launch");
   for (int i = 0; i < 3; ++i) {

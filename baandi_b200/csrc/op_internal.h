@@ -86,9 +86,16 @@ struct bg_kset {
   bg::StageEvents ev;
   int64_t launches = 0;
   // host-buffer applies: copy-in, compute and copy-out streams pipelined over chunks
+  // (whole operators, or column blocks of one), events reused cyclically
   static constexpr int kChunks = 12;
   cudaStream_t pipe[3] = {nullptr, nullptr, nullptr};
   cudaEvent_t in_done[kChunks] = {}, work_done[kChunks] = {};
+  // pageable host blocks: two pinned input and two pinned output staging slots, filled
+  // and drained by host threads, and the events that free them
+  void* stage_in[2] = {nullptr, nullptr};
+  void* stage_out[2] = {nullptr, nullptr};
+  size_t stage_bytes = 0;
+  cudaEvent_t in_copied[2] = {}, out_copied[2] = {};
   // bg_kset_davidson_solve's solver (work arrays and iteration graph), kept between solves
   void* dv_cache = nullptr;
   void (*dv_free)(void*) = nullptr;
