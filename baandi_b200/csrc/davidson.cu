@@ -93,9 +93,6 @@ class Solver {
     s_ = op->stream;
     kind_ = o.preconditioner;
   }
-  ~Solver() {
-    for (void* p : dev_) cudaFree(p);
-  }
 
   int run(const T* start, const double* diagonal, double* values_out, T* vectors_out, int32_t* converged,
           bg_davidson_stats* st);
@@ -108,7 +105,7 @@ class Solver {
   bg_davidson_options o_;
   int kind_;  // preconditioner in use: the learned one gives way to TPA when the solve stalls
   cudaStream_t s_;
-  std::vector<void*> dev_;
+  size_t next_ = 0;  // next arena slot
   D *V_ = nullptr, *HV_ = nullptr, *X_ = nullptr, *HX_ = nullptr, *E_ = nullptr, *Er_ = nullptr, *HE_ = nullptr;
   D *part_ = nullptr, *small_ = nullptr, *coef_ = nullptr;
   double *diag_ = nullptr, *lam_ = nullptr, *norms_ = nullptr, *scale_ = nullptr;
@@ -125,12 +122,22 @@ class Solver {
   double band_threshold(int i) const {
     return (o_.first_step || i < o_.occupied) ? o_.threshold : std::max(5.0 * o_.threshold, 5e-6);
   }
+  // The next work array from the operator's arena (allocated, or enlarged, only when this
+  // solve needs more than an earlier one did).
   template <class P>
   int alloc(P** p, size_t count) {
-    void* q = nullptr;
-    if (cudaMalloc(&q, std::max<size_t>(count, 1) * sizeof(P)) != cudaSuccess) return BG_ENOMEM;
-    dev_.push_back(q);
-    *p = static_cast<P*>(q);
+    const size_t bytes = std::max<size_t>(count, 1) * sizeof(P);
+    std::vector<std::unique_ptr<DevBuf>>& arena = op_->dv_arena;
+    if (next_ == arena.size()) arena.push_back(std::make_unique<DevBuf>());
+    DevBuf& b = *arena[next_++];
+    if (b.bytes < bytes) {
+      if (b.p) cudaFree(b.p);
+      b.p = nullptr;
+      b.bytes = 0;
+      if (cudaMalloc(&b.p, bytes) != cudaSuccess) return BG_ENOMEM;
+      b.bytes = bytes;
+    }
+    *p = static_cast<P*>(b.p);
     return BG_OK;
   }
   int check(const char* what) {

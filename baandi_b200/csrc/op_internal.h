@@ -66,6 +66,9 @@ struct bg_op {
   int dens_chunks = 0;  // chunks dens_part holds
   bool vtf_valid = false;  // t.vtf (the FP32 apply's potential) matches t.vt
   bg::TcNl tc;             // tensor-core nonlocal products (BG_PREC_TENSOR)
+  // device work arrays of bg_davidson_solve, kept between solves on this operator (the
+  // solver takes them in a fixed order and enlarges one only when a solve needs more)
+  std::vector<std::unique_ptr<DevBuf>> dv_arena;
 };
 
 
