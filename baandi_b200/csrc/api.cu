@@ -329,6 +329,7 @@ int build_op(bg_ctx* ctx, const bg_basis_desc* b, const bg_projectors* pr, int64
   T.ngroups = ngroups;
   T.nxact = (int)xact.size();
   T.yper = plane_lines_per_warp(n0, n1, T.nxact);
+  T.yper16 = plane_lines_per_warp(n0, n1, T.nxact, 16);
   int rc;
   int* d_int;
   if ((rc = upload(op.get(), grp_stick.data(), grp_stick.size(), &d_int))) return rc;

@@ -20,6 +20,7 @@ struct OpTables {
   int ngroups;    // stick groups
   int nxact;      // x rows of the plane holding at least one stick
   int yper;       // x rows per warp in the 8-warp plane kernels' y passes
+  int yper16;     // the same for the 16-warp plane kernels (one block per SM)
   const int* grp_stick;   // ngroups+1: first stick of each group
   const int* grp_entry;   // ngroups+1: entry range of each group
   const int2* entries;    // complex: (row g, pos); Gamma: (code, pos), code 0 for G=0,
@@ -131,9 +132,9 @@ int launch_local(const OpTables* tabs, int gamma, int max_groups, const BoxGeo& 
                  StageEvents* ev, int fp32 = 0);
 // The FP32 local apply needs a cubic box with a compile-time plan.
 bool fp32_supported(const BoxGeo& g);
-// x rows per warp for the y passes of the 8-warp plane kernels on an n0 x n1 plane with
-// nlines x rows holding sticks (1 where no compile-time plan covers the plane).
-int plane_lines_per_warp(int n0, int n1, int nlines);
+// x rows per warp for the y passes of the plane kernels (warps 8 or 16) on an n0 x n1
+// plane with nlines x rows holding sticks (1 where no compile-time plan covers the plane).
+int plane_lines_per_warp(int n0, int n1, int nlines, int warps = 8);
 // Enqueue y += P (D (P^H x)) (complex) or y += P (D (P^T x)) (Gamma).
 int launch_nonlocal(const NlDev* nl, int gamma, const NlShape& sh, int max_rows, const Batch& b, cudaStream_t s,
                     StageEvents* ev);

@@ -205,16 +205,22 @@ __global__ void __launch_bounds__(512) k_planes(const OpTables* __restrict__ tab
 // Blocks of k_planes_fast that fit an SM's 228 KB of shared memory (1 KB reserved per
 // block), at most 4: the register budget per thread follows from it.
 template <int N, class C>
-constexpr int planes_blocks_per_sm() {
+__host__ __device__ constexpr int planes_blocks_per_sm() {
   const int P = N | 1;
   const int bytes = (int)sizeof(C) * (N + N * P) + (v_in_smem_t<C>(N) ? (int)sizeof(C) / 2 * N * N : 0) + 4 * N;
   const int fit = 233472 / (bytes + 1024);
   return fit < 1 ? 1 : (fit > 4 ? 4 : fit);
 }
+// Threads of a k_planes_fast block: 16 warps where the plane allows one block per SM
+// (108^3: the block alone must hide the latencies), else 8.
+template <int N, class C>
+__host__ __device__ constexpr int planes_threads() {
+  return planes_blocks_per_sm<N, C>() == 1 ? 512 : 256;
+}
 
 template <int N, class C = double2>
-__global__ void __launch_bounds__(256, planes_blocks_per_sm<N, C>()) k_planes_fast(const OpTables* __restrict__ tabs,
-                                                                                  BoxGeo g, Batch b) {
+__global__ void __launch_bounds__(planes_threads<N, C>(), planes_blocks_per_sm<N, C>())
+    k_planes_fast(const OpTables* __restrict__ tabs, BoxGeo g, Batch b) {
   using T = RealOf<C>;
   using Pl = fast::Plan<N>;
   static_assert(Pl::nst == 2, "two-stage plans");
@@ -256,7 +262,9 @@ __global__ void __launch_bounds__(256, planes_blocks_per_sm<N, C>()) k_planes_fa
   io.xb = t.xbits;
   const int lane = threadIdx.x & 31;
   int first, count;
-  fast::owned_block(nx, t.yper, &first, &count);
+  constexpr int kWarps = planes_threads<N, C>() / 32;
+  // stick rows per warp (read again for the last pass rather than kept live across the x pass)
+  fast::owned_block(nx, kWarps == 16 ? t.yper16 : t.yper, &first, &count);
   if (count > 0) {
     fast::stage<N, R1, 1, 1, 1, fast::kInGlobal>(pl, first, count, LineOffTable{rows}, tw, lane, io);
     fast::stage<N, R2, R1, 1, 1>(pl, first, count, LineOffTable{rows}, tw, lane);
@@ -265,7 +273,7 @@ __global__ void __launch_bounds__(256, planes_blocks_per_sm<N, C>()) k_planes_fa
   __syncthreads();
   {
     int xf, xc;
-    constexpr int xper = fast::balanced_lines<N, 2, 1>(N, 8);
+    constexpr int xper = fast::balanced_lines<N, 2, 1>(N, kWarps);
     fast::owned_block(N, xper, &xf, &xc);
     if (xc > 0) {
       // line = column y, element = x: weight V(x, y, z)
@@ -274,7 +282,7 @@ __global__ void __launch_bounds__(256, planes_blocks_per_sm<N, C>()) k_planes_fa
     }
   }
   __syncthreads();
-  fast::owned_block(nx, t.yper, &first, &count);
+  fast::owned_block(nx, kWarps == 16 ? t.yper16 : t.yper, &first, &count);
   if (count > 0) {
     fast::stage<N, R1, 1, -1, 1>(pl, first, count, LineOffTable{rows}, tw, lane);
     fast::stage<N, R2, R1, -1, 1, fast::kOutGlobal>(pl, first, count, LineOffTable{rows}, tw, lane, io);
@@ -711,15 +719,15 @@ static size_t plane_smem_bytes_f32(const BoxGeo& g) {
 }
 static size_t stick_smem_bytes_f32(const BoxGeo& g) { return sizeof(float2) * ((size_t)g.n2 + (size_t)g.sg * g.ld2); }
 
-int plane_lines_per_warp(int n0, int n1, int nlines) {
+int plane_lines_per_warp(int n0, int n1, int nlines, int warps) {
   if (n0 != n1) return 1;
   switch (n0) {
-    case 25: return fast::balanced_lines<25, 1, 1>(nlines, 8);
-    case 45: return fast::balanced_lines<45, 1, 1>(nlines, 8);
-    case 54: return fast::balanced_lines<54, 1, 1>(nlines, 8);
-    case 60: return fast::balanced_lines<60, 1, 1>(nlines, 8);
-    case 72: return fast::balanced_lines<72, 1, 1>(nlines, 8);
-    case 108: return fast::balanced_lines<108, 1, 1>(nlines, 8);
+    case 25: return fast::balanced_lines<25, 1, 1>(nlines, warps);
+    case 45: return fast::balanced_lines<45, 1, 1>(nlines, warps);
+    case 54: return fast::balanced_lines<54, 1, 1>(nlines, warps);
+    case 60: return fast::balanced_lines<60, 1, 1>(nlines, warps);
+    case 72: return fast::balanced_lines<72, 1, 1>(nlines, warps);
+    case 108: return fast::balanced_lines<108, 1, 1>(nlines, warps);
     default: return 1;
   }
 }
@@ -760,7 +768,7 @@ static void local_kernels(const OpTables* tabs, const BoxGeo& g, const Batch& b,
     } else {
       StageScope sc(ev, 1, s);
       if (g.n0 == N && g.n1 == N)
-        k_planes_fast<N, C><<<pgrid, 256, ps, s>>>(tabs, g, b);
+        k_planes_fast<N, C><<<pgrid, planes_threads<N, C>(), ps, s>>>(tabs, g, b);
       else if constexpr (sizeof(C) == sizeof(double2))
         k_planes<<<pgrid, 512, ps, s>>>(tabs, g, b);
     }
