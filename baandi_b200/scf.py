@@ -44,7 +44,7 @@ from .occupations import fermi_dirac
 
 # Davidson thresholds (Ha) from which the precision form's tensor phase may end a solve on
 # its own (the solver's kTensorOnlyThreshold)
-TENSOR_ONLY_THRESHOLD_HA = 1e-5
+TENSOR_ONLY_THRESHOLD_HA = 1e-6
 
 
 def next_ethr_ry(previous: float, dr2_ry: float, electrons: float) -> float:
