@@ -414,18 +414,24 @@ int build_op(bg_ctx* ctx, const bg_basis_desc* b, const bg_projectors* pr, int64
     // static diagonal (complex: distributed_complex.rs:29-53; Gamma: refstart.rs:605-650)
     std::vector<double> dfull(npw);
     for (int64_t g = 0; g < npw; ++g) dfull[g] = b->kinetic[g];
-    for (int a = 0, off = 0; a < natoms; ++a) {
-      const int c = pr->channels[a];
-      const double* D = pr->couplings + d_off[a];
-      for (int i = 0; i < c; ++i)
-        for (int j = 0; j < c; ++j) {
-          const double d = D[i * c + j];
-          if (d == 0.0) continue;
-          const std::complex<double>* pi = P + (size_t)(off + i) * npw;
-          const std::complex<double>* pj = P + (size_t)(off + j) * npw;
-          for (int64_t g = 0; g < npw; ++g) dfull[g] += (d * pi[g] * std::conj(pj[g])).real();
-        }
-      off += c;
+    // blocks of G on the host threads; each G sums atoms and channel pairs in order
+    const int64_t gblk = 2048;
+#pragma omp parallel for schedule(dynamic)
+    for (int64_t g0 = 0; g0 < npw; g0 += gblk) {
+      const int64_t g1 = std::min(npw, g0 + gblk);
+      for (int a = 0, off = 0; a < natoms; ++a) {
+        const int c = pr->channels[a];
+        const double* D = pr->couplings + d_off[a];
+        for (int i = 0; i < c; ++i)
+          for (int j = 0; j < c; ++j) {
+            const double d = D[i * c + j];
+            if (d == 0.0) continue;
+            const std::complex<double>* pi = P + (size_t)(off + i) * npw;
+            const std::complex<double>* pj = P + (size_t)(off + j) * npw;
+            for (int64_t g = g0; g < g1; ++g) dfull[g] += (d * pi[g] * std::conj(pj[g])).real();
+          }
+        off += c;
+      }
     }
     if (gamma) {
       op->diag[0] = dfull[0];

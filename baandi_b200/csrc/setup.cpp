@@ -350,18 +350,29 @@ int projectors_build(double volume, int64_t npw, const double* kpg, const double
     for (int a = 0; a < nc; ++a)
       for (int b = 0; b < nc; ++b)
         if (ch[a].l == ch[b].l && ch[a].m == ch[b].m) coupling[(size_t)a * nc + b] = s.dij[ch[a].i * nb + ch[b].i];
+    // every atom's columns on its own host thread; the phase of (atom, G) is formed once
+    // for all of the atom's channels (the same arithmetic per element as one by one)
+    int bad = 0;
+#pragma omp parallel for schedule(dynamic) reduction(| : bad)
     for (int at = 0; at < s.natoms; ++at) {
       const double* tau = s.positions + 3 * at;
-      for (int c = 0; c < nc; ++c) {
-        for (int64_t g = 0; g < npw; ++g) {
-          const double ang = (kpg[3 * g] * tau[0] + kpg[3 * g + 1] * tau[1]) + kpg[3 * g + 2] * tau[2];
-          const std::complex<double> ph(std::cos(-ang), std::sin(-ang));
-          const std::complex<double> v = fac[(size_t)c * npw + g] * ph;
-          if (!std::isfinite(v.real()) || !std::isfinite(v.imag())) return BG_ENONFINITE;
-          table[(size_t)col * npw + g] = v;
-        }
-        ++col;
+      std::vector<std::complex<double>> ph((size_t)npw);
+      for (int64_t g = 0; g < npw; ++g) {
+        const double ang = (kpg[3 * g] * tau[0] + kpg[3 * g + 1] * tau[1]) + kpg[3 * g + 2] * tau[2];
+        ph[(size_t)g] = std::complex<double>(std::cos(-ang), std::sin(-ang));
       }
+      for (int c = 0; c < nc; ++c) {
+        std::complex<double>* out = table + (size_t)(col + (int64_t)at * nc + c) * npw;
+        for (int64_t g = 0; g < npw; ++g) {
+          const std::complex<double> v = fac[(size_t)c * npw + g] * ph[(size_t)g];
+          bad |= (!std::isfinite(v.real()) || !std::isfinite(v.imag())) ? 1 : 0;
+          out[g] = v;
+        }
+      }
+    }
+    if (bad) return BG_ENONFINITE;
+    for (int at = 0; at < s.natoms; ++at) {
+      col += nc;
       channels[atom++] = nc;
       std::copy(coupling.begin(), coupling.end(), couplings + coff);
       coff += coupling.size();
@@ -427,6 +438,10 @@ int ewald_energy(const Cell& cell, int natoms, const double* pos, const double* 
     zsum += charge[i];
     z2sum += charge[i] * charge[i];
   }
+  // the image sums of the pairs on the host threads, then added in pair order (the same
+  // result as one thread)
+  std::vector<long double> pair((size_t)natoms * natoms);
+#pragma omp parallel for schedule(dynamic)
   for (int i = 0; i < natoms; ++i)
     for (int j = 0; j < natoms; ++j) {
       const double d0[3] = {pos[3 * j] - pos[3 * i], pos[3 * j + 1] - pos[3 * i + 1], pos[3 * j + 2] - pos[3 * i + 2]};
@@ -441,8 +456,10 @@ int ewald_energy(const Cell& cell, int natoms, const double* pos, const double* 
             if (r > r_cut || (i == j && a == 0 && b == 0 && c == 0)) continue;
             acc += std::erfc(eta * r) / r;
           }
-      real += 0.5L * charge[i] * charge[j] * acc;
+      pair[(size_t)i * natoms + j] = acc;
     }
+  for (int i = 0; i < natoms; ++i)
+    for (int j = 0; j < natoms; ++j) real += 0.5L * charge[i] * charge[j] * pair[(size_t)i * natoms + j];
   for (int a = -ng[0]; a <= ng[0]; ++a)
     for (int b = -ng[1]; b <= ng[1]; ++b)
       for (int c = -ng[2]; c <= ng[2]; ++c) {

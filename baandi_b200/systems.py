@@ -9,6 +9,7 @@ numpy default_rng(2026 + workload number).
 from __future__ import annotations
 
 import math
+import os
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -98,9 +99,12 @@ class Workload:
         for s in self.species:
             ff = O.local_form_factor(s, vol, np.sqrt(q2u))[inv]
             sf = np.zeros(dens.npw, np.complex128)
-            for tau in np.atleast_2d(s.positions):
-                ang = dens.kpg @ tau
-                sf += np.exp(-1j * ang)
+            # the atoms' phase factors on the host threads (numpy releases the GIL), added in
+            # atom order: the same sum as one atom after another
+            taus = np.atleast_2d(s.positions)
+            for lo in range(0, len(taus), _PHASE_BATCH):
+                for term in _map_threads(lambda tau: np.exp(-1j * (dens.kpg @ tau)), taus[lo:lo + _PHASE_BATCH]):
+                    sf += term
             vg += ff * sf
         box = np.zeros(dims, np.complex128)
         idx = np.mod(dens.miller.astype(np.int64), np.asarray(dims)[None, :])
@@ -115,7 +119,26 @@ class Workload:
             x = rng.standard_normal((npw, cols))
             return np.asfortranarray(x / np.linalg.norm(x, axis=0, keepdims=True))
         th = rng.uniform(0.0, 2.0 * math.pi, size=(npw, cols))
-        return np.asfortranarray(np.exp(1j * th) / math.sqrt(npw))
+        out = np.empty((npw, cols), np.complex128, order="F")
+        scale = math.sqrt(npw)
+
+        def block(c0):
+            out[:, c0:c0 + 32] = np.exp(1j * th[:, c0:c0 + 32]) / scale
+        list(_map_threads(block, range(0, cols, 32)))
+        return out
+
+
+_PHASE_BATCH = 32
+
+
+def _map_threads(fn, items):
+    """fn over items on a pool of host threads, results in item order."""
+    from concurrent.futures import ThreadPoolExecutor
+    items = list(items)
+    if len(items) <= 1:
+        return [fn(x) for x in items]
+    with ThreadPoolExecutor(max_workers=min(16, os.cpu_count() or 1, len(items))) as ex:
+        return list(ex.map(fn, items))
 
 
 def _si_pseudo():
