@@ -151,6 +151,7 @@ SIGNATURES = {
     "bg_setup_projectors": [_dbl, _i64, _p, _p, _i32, ctypes.POINTER(SpeciesDesc), _p, _p, _p],
     "bg_setup_local_form_factor": [ctypes.POINTER(SpeciesDesc), _dbl, _i64, _p, _p],
     "bg_setup_ewald": [_p, _i32, _p, _p, ctypes.POINTER(_dbl)],
+    "bg_setup_atomic_charge": [_i64, _p, _p, _p, _dbl, _i64, _p, _p],
 }
 
 _lib = None

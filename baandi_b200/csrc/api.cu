@@ -1569,4 +1569,16 @@ int bg_setup_local_form_factor(const bg_species* species, double volume, int64_t
   return BG_OK;
 }
 
+int bg_setup_atomic_charge(int64_t mesh, const double* r, const double* rab, const double* rho_atom, double volume,
+                           int64_t n, const double* q, double* out) {
+  if (!r || !rab || !rho_atom || (n > 0 && (!q || !out)) || n < 0 || mesh < 2 || mesh > (1 << 20) ||
+      !(volume > 0.0))
+    return fail(nullptr, BG_EINVAL, "argument");
+  for (int64_t k = 0; k < n; ++k)
+    if (!std::isfinite(q[k]) || q[k] < 0.0) return fail(nullptr, BG_EINVAL, "wave number");
+  int rc = atomic_charge_transform((int)mesh, r, rab, rho_atom, volume, n, q, out);
+  if (rc) return fail(nullptr, rc, "atomic charge transform");
+  return BG_OK;
+}
+
 }  // extern "C"

@@ -52,6 +52,8 @@ int projectors_build(double volume, int64_t npw, const double* kpg, const double
                      const Species* sp, std::complex<double>* table, int32_t* channels, double* couplings);
 int local_form_factor(const Species& s, double volume, int64_t n, const double* g, double* out);
 int ewald_energy(const Cell& cell, int natoms, const double* pos, const double* charge, double* out);
+int atomic_charge_transform(int mesh, const double* r, const double* rab, const double* f, double volume,
+                            int64_t n, const double* q, double* out);
 
 // Thread-local message of the last failure outside a context.
 void set_global_error(const std::string& msg);

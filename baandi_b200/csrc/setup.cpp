@@ -400,6 +400,24 @@ int local_form_factor(const Species& s, double volume, int64_t n, const double* 
   return BG_OK;
 }
 
+// rho_atom(|G|) / Omega of PP_RHOATOM samples f (4 pi r^2 rho(r)): the integral of
+// f j0(q r) over the mesh (Simpson in the index with rab, j0 = 1 at q = 0), divided by the
+// volume; the exact per-shell quadrature of the atomic start density.  The q values run
+// on the host threads, each integral in the mesh's fixed order.
+int atomic_charge_transform(int mesh, const double* r, const double* rab, const double* f, double volume,
+                            int64_t n, const double* q, double* out) {
+  if (mesh < 2) return BG_EINVAL;
+  for (int i = 0; i < mesh; ++i)
+    if (!std::isfinite(r[i]) || !std::isfinite(rab[i]) || !std::isfinite(f[i])) return BG_ENONFINITE;
+#pragma omp parallel for schedule(static)
+  for (int64_t k = 0; k < n; ++k) {
+    const double qk = q[k];
+    out[k] = integrate(mesh, [&](int i) { return f[i] * (qk == 0.0 ? 1.0 : bessel(0, qk * r[i])) * rab[i]; }) /
+             volume;
+  }
+  return BG_OK;
+}
+
 // Ewald ion-ion energy of point charges in a neutralising background (Ha), the
 // standard split with eta = sqrt(pi) / Omega^(1/3) (the reference's default scheme,
 // crates/dft-physics/src/ewald.rs:1-10, 376-381): real-space erfc sum over lattice

@@ -11,7 +11,8 @@ Training pairs come from the solver itself: Davidson states (Ritz vectors X, val
 H X) taken after 1, 2, 3, ... iterations on seeded displaced geometries, each band paired
 with its ideal correction, the part of its Ritz vector outside the exact eigenspace it
 converges to (exact eigenpairs of the dense H built by applying the operator to the unit
-vectors).  The loss scores each band's correction by its squared cosine with the ideal
+vectors; for cells too large for a dense H, the eigenpairs of a tight FP64 Davidson over
+the tracked bands and a buffer of higher ones).  The loss scores each band's correction by its squared cosine with the ideal
 one (the Davidson ignores the scale of a correction); the loss, its gradient and the Adam
 step are device kernels (csrc/learned.cu).  The solver falls back to TPA when a solve
 stalls (stats.fallbacks).
@@ -220,6 +221,33 @@ def exact_problem(w, ctx, bands: int, capacity: int) -> Problem:
     return Problem(op, kin, ev.cpu().numpy(), vec.cpu().numpy(), start, bands)
 
 
+def converged_problem(w, ctx, bands: int, capacity: int, k_index: int = 0, buffer: int = 16,
+                      threshold: float = 1e-11, start_offset: int = 7) -> Problem:
+    """Operator of the workload's k point `k_index` (ionic potential) with the eigenpairs of
+    its lowest bands + buffer from the FP64 Davidson (smooth preconditioner) converged to
+    `threshold` Ha, in place of a dense H's.  The buffer keeps every tracked band's
+    eigenspace (and a cluster that reaches past the last band) inside the solved set."""
+    from . import davidson as DV
+    from .hamiltonian import ComplexHamiltonian, RealGammaHamiltonian
+    k = w.kpoints[k_index][0]
+    pw = w.plane_waves(k)
+    real = w.gamma_real and pw.gamma
+    cls = RealGammaHamiltonian if real else ComplexHamiltonian
+    nb = bands + buffer
+    op = cls.new_owned(pw, w.dims(), w.nonlocal_table(pw), max(capacity, 2 * nb), ctx)
+    v = w.ionic_potential()
+    op.set_owned_potential(v, 1)
+    rows = op.global_len()
+    x0 = w.random_block(rows, nb, seed_offset=3, real=real)
+    o = DV.Options(nb, threshold, nb, first_step=True, max_iterations=400)
+    sol = DV.solve(op, x0, op.diagonal_static() + float(np.mean(v)), o)
+    if not bool(np.all(sol.converged)):
+        raise RuntimeError("reference eigenpairs did not converge")
+    kin = op.kinetic_diagonal()
+    start = w.random_block(rows, bands, seed_offset=start_offset, real=real)
+    return Problem(op, kin, np.asarray(sol.eigenvalues), np.asarray(sol.eigenvectors), start, bands)
+
+
 def ideal_corrections(p: Problem, x: np.ndarray, tol: float = 1e-6) -> np.ndarray:
     """e_j = -(x_j - P_j x_j), P_j the projector on the exact eigenspace of eigenvalue j
     (eigenvalues within tol of it)."""
@@ -246,21 +274,29 @@ def davidson_states(p: Problem, iterations, threshold=1e-10):
 TRAIN_ITERATIONS = (1, 2, 3, 4, 5, 6, 8, 10, 13, 16, 20, 25, 30)
 
 
-def build_samples(ctx, problems, iterations=TRAIN_ITERATIONS, min_error=1e-12) -> Samples:
+def build_samples(ctx, problems, iterations=TRAIN_ITERATIONS, min_error=1e-12, bands_per_state=None,
+                  seed=0) -> Samples:
     """Samples of every problem's Davidson states; bands already exact (|e|^2 below
-    min_error) are left out."""
+    min_error) are left out.  problems: any iterable (a generator frees each problem's
+    operator once its states are taken).  iterations: one tuple for every problem, or a
+    callable problem index -> tuple.  bands_per_state: keep a seeded random subset of that many of
+    each state's remaining bands (None: all)."""
     states = []
-    for p in problems:
-        for x, hx, lam in davidson_states(p, iterations):
+    rng = np.random.default_rng(seed)
+    for i, p in enumerate(problems):
+        its = iterations(i) if callable(iterations) else iterations
+        for x, hx, lam in davidson_states(p, its):
             e = ideal_corrections(p, x)
             keep = np.nonzero(np.sum(np.abs(e) ** 2, axis=0) > min_error)[0]
+            if bands_per_state is not None and len(keep) > bands_per_state:
+                keep = np.sort(rng.choice(keep, bands_per_state, replace=False))
             if len(keep):
-                states.append((p, x[:, keep], hx[:, keep], e[:, keep], lam[keep]))
+                states.append((p.kinetic, x[:, keep], hx[:, keep], e[:, keep], lam[keep]))
     n = sum(x.shape[0] * x.shape[1] for _, x, _, _, _ in states)
     ncols = sum(x.shape[1] for _, x, _, _, _ in states)
     s = Samples(n, ncols)
-    for p, x, hx, e, lam in states:
-        s.add_state(ctx, x, hx, e, p.kinetic, lam)
+    for kin, x, hx, e, lam in states:
+        s.add_state(ctx, x, hx, e, kin, lam)
     return s
 
 

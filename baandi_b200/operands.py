@@ -112,6 +112,7 @@ class Pseudo:
     l: list
     beta: list
     dij: np.ndarray
+    rho_atom: np.ndarray | None = None  # PP_RHOATOM: 4 pi r^2 rho_atom(r) on the mesh
 
 
 @dataclass
@@ -190,9 +191,11 @@ def log_mesh(points: int = 1201, end: float = 12.0, r0: float = 0.02):
 
 
 def gaussian_pseudo(z: float, rc: float, l=(0, 1), r_beta=(1.0, 1.0), dij_diag=(3.0, 1.5),
-                    points: int = 1201) -> Pseudo:
+                    points: int = 1201, rho_radius: float | None = None) -> Pseudo:
     """Synthetic pseudopotential: local -Z erf(r/rc)/r and projectors r^l exp(-(r/r_beta)^2)
-    with a diagonal D (Ha)."""
+    with a diagonal D (Ha); with rho_radius R, the atomic charge rho(r) = Z exp(-(r/R)^2) /
+    (pi^(3/2) R^3) as PP_RHOATOM, 4 Z / (sqrt(pi) R^3) r^2 exp(-(r/R)^2) (the atomic variant
+    of the reference's synthetic fixtures, scripts/gen_synthetic_upf.py:64-65)."""
     r, rab = log_mesh(points)
     local = np.empty_like(r)
     local[0] = -2.0 * z / (rc * math.sqrt(math.pi))
@@ -202,4 +205,51 @@ def gaussian_pseudo(z: float, rc: float, l=(0, 1), r_beta=(1.0, 1.0), dij_diag=(
     dij = np.zeros(n * n)
     for i, d in enumerate(dij_diag):
         dij[i * n + i] = d
-    return Pseudo(z, r, rab, local, list(l), beta, dij)
+    rho = None
+    if rho_radius is not None:
+        rho = 4.0 * z / (math.sqrt(math.pi) * rho_radius ** 3) * r * r * np.exp(-(r / rho_radius) ** 2)
+    return Pseudo(z, r, rab, local, list(l), beta, dij, rho)
+
+
+def has_atomic_charge(p: Pseudo) -> bool:
+    """PP_RHOATOM on the whole mesh and not all zero (crates/dft-engine/src/refstart.rs:56-59)."""
+    return p.rho_atom is not None and len(p.rho_atom) == len(p.r) and bool(np.any(np.asarray(p.rho_atom) != 0.0))
+
+
+def atomic_charge_transform(p: Pseudo, vol: float, q: np.ndarray) -> np.ndarray:
+    """rho_atom(|G|) / Omega at the wave numbers q (bg_setup_atomic_charge)."""
+    q = np.ascontiguousarray(np.asarray(q, dtype=np.float64).reshape(-1))
+    out = np.zeros_like(q)
+    r = np.ascontiguousarray(p.r, dtype=np.float64)
+    rab = np.ascontiguousarray(p.rab, dtype=np.float64)
+    rho = np.ascontiguousarray(p.rho_atom, dtype=np.float64)
+    L.check(L.load().bg_setup_atomic_charge(len(r), _ptr(r), _ptr(rab), _ptr(rho), vol, len(q), _ptr(q), _ptr(out)))
+    return out
+
+
+def atomic_density(rows, ecut_ha: float, dims, species) -> np.ndarray | None:
+    """The atomic start density on the grid (C order), or None for the uniform start when any
+    species carries no atomic charge (crates/dft-engine/src/refstart.rs:704-757): rho(G) =
+    sum_s rho_s(|G|) S_s(G) / Omega over the 4 Ecut density sphere, n(r) = sum_G rho(G)
+    e^{iGr}, negative values set to 0, scaled so that sum n Omega / N_points = N_e."""
+    if not all(has_atomic_charge(s.pseudo) for s in species):
+        return None
+    vol = volume(rows)
+    dens = plane_waves(rows, 4.0 * ecut_ha)
+    q2u, inv = np.unique(dens.kpg2, return_inverse=True)
+    rg = np.zeros(dens.npw, np.complex128)
+    for s in species:
+        ff = atomic_charge_transform(s.pseudo, vol, np.sqrt(q2u))[inv]
+        sf = np.zeros(dens.npw, np.complex128)
+        for tau in np.atleast_2d(s.positions):
+            sf += np.exp(-1j * (dens.kpg @ tau))
+        rg += ff * sf
+    box = np.zeros(dims, np.complex128)
+    idx = np.mod(dens.miller.astype(np.int64), np.asarray(dims)[None, :])
+    box[idx[:, 0], idx[:, 1], idx[:, 2]] = rg
+    n = np.maximum(np.ascontiguousarray((np.fft.ifftn(box) * box.size).real), 0.0)
+    electrons = float(sum(s.pseudo.z * np.atleast_2d(s.positions).shape[0] for s in species))
+    charge = float(n.sum()) * vol / n.size
+    if not math.isfinite(charge) or charge <= 0.0:
+        raise ValueError("invalid atomic charge")
+    return n * (electrons / charge)

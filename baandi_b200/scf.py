@@ -21,7 +21,8 @@ host reads scalars only (eigenvalues for the band sum and occupations, energies,
 Occupations are fixed (2 per occupied band, insulators) or Fermi-Dirac
 (occupations.py; crates/dft-physics/src/occupations.rs), whose entropy term gives the
 free energy E - TS; the Davidson's occupied count is ceil(N_e / 2).  The start density
-is uniform (the reference's fallback when the species carry no atomic charge,
+is the superposition of atomic charges when every species carries one (PP_RHOATOM;
+refstart.rs:704-757, operands.atomic_density), else uniform (the reference's fallback,
 refstart.rs:725-735).
 """
 from __future__ import annotations
@@ -88,6 +89,9 @@ class ScfOptions:
     # keep H X of each map's eigenvectors and start the next map's Davidson from it,
     # updated by the potential change (no start apply)
     kept_hx: bool = True
+    # "auto": the atomic start density when every species carries an atomic charge, else
+    # uniform (the reference's rule, refstart.rs:704-712); "uniform": always uniform
+    start_density: str = "auto"
 
 
 @dataclass
@@ -171,6 +175,11 @@ class GpuScf:
         self.gamma = self.ops[0].is_real()
         self.kset = KPointSet(self.ops, self.ctx)
         self.v_ion = torch.from_numpy(np.ascontiguousarray(w.ionic_potential())).to(dev)
+        if self.o.start_density not in ("auto", "uniform"):
+            raise SolverError(L.BG_EINVAL, "start_density is 'auto' or 'uniform'")
+        n0 = w.start_density() if self.o.start_density == "auto" else None
+        self.start_kind = "uniform" if n0 is None else "atomic"
+        self._n0 = None if n0 is None else torch.from_numpy(np.ascontiguousarray(n0)).to(dev)
         self.ewald = O.ewald(w.rows, w.species)
         # mixed space: half of the density sphere (4 Ecut)
         dens = O.plane_waves(w.rows, 4.0 * w.ecut_ha)
@@ -278,7 +287,10 @@ class GpuScf:
         self._tensor_live = True
         self._kept = None
         with torch.cuda.stream(self.stream):
-            n = torch.full(self.dims, self.electrons / self.volume, dtype=torch.float64, device=self.dev)
+            if self._n0 is None:
+                n = torch.full(self.dims, self.electrons / self.volume, dtype=torch.float64, device=self.dev)
+            else:
+                n = self._n0.clone()
             x = self.fields.sphere_forward(n)
             x[self.g0] = self.electrons / self.volume
             ethr, last_dr2 = 1e-2, float("inf")

@@ -112,6 +112,11 @@ class Workload:
         v = np.fft.ifftn(box) * box.size
         return np.ascontiguousarray(v.real)
 
+    def start_density(self) -> np.ndarray | None:
+        """The atomic start density on the grid, or None (uniform) when a species has no
+        atomic charge."""
+        return O.atomic_density(self.rows, self.ecut_ha, self.dims(), self.species)
+
     def random_block(self, npw, cols, seed_offset=0, real=False):
         """Seeded random-phase columns c_G = e^{i theta}/sqrt(Npw) (real: ORC rows of unit norm)."""
         rng = np.random.default_rng(self.seed + seed_offset)
@@ -141,8 +146,8 @@ def _map_threads(fn, items):
         return list(ex.map(fn, items))
 
 
-def _si_pseudo():
-    return O.gaussian_pseudo(4.0, 0.45, l=(0, 1), r_beta=(1.0, 1.0), dij_diag=(3.0, 1.5))
+def _si_pseudo(rho_radius=None):
+    return O.gaussian_pseudo(4.0, 0.45, l=(0, 1), r_beta=(1.0, 1.0), dij_diag=(3.0, 1.5), rho_radius=rho_radius)
 
 
 def _al_pseudo():
@@ -171,6 +176,14 @@ def si2_gamma() -> Workload:
                     [((0.0, 0.0, 0.0), 1.0)], True, seed=2027)
 
 
+def si2_gamma_atomic(radius: float = 1.0) -> Workload:
+    """Si2 Gamma with a Gaussian atomic charge of `radius` Bohr: the atomic-density start."""
+    w = si2_gamma()
+    w.name = "si2_gamma_real_30ry_atomic"
+    w.species = [O.Species(_si_pseudo(rho_radius=radius), s.positions) for s in w.species]
+    return w
+
+
 def si8_k444() -> Workload:
     """Si8 conventional cube (a = 10.26), 4x4x4 mesh reduced by time reversal to 36 k, 40 Ry, 24 bands."""
     a = SI_A
@@ -189,14 +202,15 @@ def si64_gamma() -> Workload:
                     [((0.0, 0.0, 0.0), 1.0)], False, seed=2029)
 
 
-def al32_k222() -> Workload:
-    """Al32 fcc 2x2x2 conventional (a = 15.30), +-0.08 seeded noise, 2x2x2 mesh (8 k), 30 Ry, grid 60^3, 64 bands."""
-    rng = np.random.default_rng(2030)
+def al32_k222(geometry_seed: int = 2030) -> Workload:
+    """Al32 fcc 2x2x2 conventional (a = 15.30), +-0.08 seeded noise, 2x2x2 mesh (8 k), 30 Ry, grid 60^3, 64 bands.
+    geometry_seed: the seed of the displacements and start blocks (2030: the benchmark cell)."""
+    rng = np.random.default_rng(geometry_seed)
     a = 15.30
     pos = _supercell(FCC_FRAC, 2, a, 0.08, rng)
     ks = reduce_time_reversal(monkhorst_pack((2, 2, 2)))
     return Workload("al32_k222_30ry", np.diag([a, a, a]), [O.Species(_al_pseudo(), pos)], 15.0, 64, 48, ks, False,
-                    dims_override=[60, 60, 60], seed=2030)
+                    dims_override=[60, 60, 60], seed=geometry_seed)
 
 
 def si216_gamma() -> Workload:
@@ -209,5 +223,5 @@ def si216_gamma() -> Workload:
 
 
 WORKLOADS = {
-    "si2": si2_gamma, "si8": si8_k444, "si64": si64_gamma, "al32": al32_k222, "si216": si216_gamma,
+    "si2": si2_gamma, "si2_atomic": si2_gamma_atomic, "si8": si8_k444, "si64": si64_gamma, "al32": al32_k222, "si216": si216_gamma,
 }

@@ -536,6 +536,15 @@ int bg_setup_ewald(const double rows[9], int32_t natoms, const double* positions
 /* V_loc(|G|) (Ha) of one species at n wave numbers (crates/dft-upf/src/radial.rs:246-305). */
 int bg_setup_local_form_factor(const bg_species* species, double volume, int64_t n,
                                const double* g, double* out);
+/* Atomic charge form factor rho_atom(|G|) / Omega at n wave numbers q >= 0 from a species'
+ * PP_RHOATOM samples (4 pi r^2 rho(r)) on its radial mesh (r, rab; mesh points):
+ * out[k] = integral of rho_atom(r) j0(q_k r) dr / volume, Simpson in the mesh index with
+ * rab (crates/dft-upf/src/radial.rs:40-47), j0 = 1 at q = 0.  Replaces the rho channel
+ * of the reference's atomic start fields (crates/dft-engine/src/refstart.rs:1166-1230,
+ * the exact per-shell quadrature of the Gamma start).  BG_ENONFINITE for non-finite
+ * samples. */
+int bg_setup_atomic_charge(int64_t mesh, const double* r, const double* rab, const double* rho_atom,
+                           double volume, int64_t n, const double* q, double* out);
 
 #ifdef __cplusplus
 }

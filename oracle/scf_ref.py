@@ -113,13 +113,14 @@ class _K:
 
 def run(rows, species, ecut_ha, dims, kpoints, gamma_real, bands, v_ion, starts, ewald, threshold_ha=5e-9,
         max_iterations=60, beta=0.7, history=8, davidson_max_iterations=20, smearing_ha=None, thomas_fermi=False,
-        kept_hx=True, pool=None):
+        kept_hx=True, pool=None, start_density=None):
     """The SCF outer loop.  kept_hx: each map's Davidson starts from the previous map's
     H X brought to the new potential (crates/dft-engine/src/refscf/kept_hx.rs:98-160).
     pool: k points split over ranks (an object with `local` (range of owned k points),
     `gather_eigenvalues(list) -> every k point's list` and `sum_partials(array) -> sum over
     ranks`, as the reference's KPool: crates/dft-engine/src/refscf/k_pool.rs:76-330);
-    `starts` then holds the owned k points' blocks only."""
+    `starts` then holds the owned k points' blocks only.  start_density: the start n(r) on
+    the grid (setup_ref.atomic_density); None: uniform N_e / Omega (refstart.rs:704-757)."""
     cell = S.Cell(np.asarray(rows, dtype=np.float64))
     vol = cell.volume
     electrons = float(sum(s.pseudo.z * np.atleast_2d(s.positions).shape[0] for s in species))
@@ -147,7 +148,7 @@ def run(rows, species, ecut_ha, dims, kpoints, gamma_real, bands, v_ion, starts,
         grid[flat] = c
         return 2.0 * (np.fft.ifftn(grid.reshape(dims)) * npts).real - c[g0].real
 
-    n = np.full(dims, electrons / vol)
+    n = np.full(dims, electrons / vol) if start_density is None else np.asarray(start_density, dtype=np.float64)
     x = forward(n)
     x[g0] = electrons / vol
     orbitals = [np.array(s) for s in starts]

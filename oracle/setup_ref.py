@@ -270,6 +270,7 @@ class Pseudo:
     local: np.ndarray
     projectors: list
     dij: np.ndarray
+    rho_atom: np.ndarray | None = None  # PP_RHOATOM: 4 pi r^2 rho_atom(r) on the mesh
 
 
 def log_mesh(points: int, end: float = 12.0, r0: float = 0.02):
@@ -279,8 +280,9 @@ def log_mesh(points: int, end: float = 12.0, r0: float = 0.02):
     return r, rab
 
 
-def synthetic_pseudo(z: float, rc: float, channels, r_beta, dij_ha, points=1201) -> Pseudo:
-    """Gaussian-erf local part -Z erf(r/rc)/r (Ha) and r^l exp(-(r/r_beta)^2) projectors."""
+def synthetic_pseudo(z: float, rc: float, channels, r_beta, dij_ha, points=1201, rho_radius=None) -> Pseudo:
+    """Gaussian-erf local part -Z erf(r/rc)/r (Ha) and r^l exp(-(r/r_beta)^2) projectors;
+    with rho_radius, the Gaussian atomic charge of that radius as PP_RHOATOM."""
     r, rab = log_mesh(points)
     local = np.empty_like(r)
     local[0] = -2.0 * z / (rc * math.sqrt(math.pi))
@@ -288,7 +290,16 @@ def synthetic_pseudo(z: float, rc: float, channels, r_beta, dij_ha, points=1201)
     projs = []
     for l, rb in zip(channels, r_beta):
         projs.append(Projector(l, r ** (l + 1) * np.exp(-(r / rb) ** 2)))
-    return Pseudo(z, r, rab, local, projs, np.asarray(dij_ha, dtype=np.float64))
+    rho = None if rho_radius is None else gaussian_rho_atom(z, rho_radius, r)
+    return Pseudo(z, r, rab, local, projs, np.asarray(dij_ha, dtype=np.float64), rho)
+
+
+def gaussian_rho_atom(z: float, radius: float, r: np.ndarray) -> np.ndarray:
+    """4 pi r^2 rho(r) of the charge z spread as rho(r) = z exp(-(r/R)^2) / (pi^(3/2) R^3),
+    the atomic-charge variant of the reference's synthetic fixtures
+    (scripts/gen_synthetic_upf.py:64-65): 4 z / (sqrt(pi) R^3) r^2 exp(-(r/R)^2)."""
+    r = np.asarray(r, dtype=np.float64)
+    return 4.0 * z / (math.sqrt(math.pi) * radius ** 3) * r * r * np.exp(-(r / radius) ** 2)
 
 
 def reference_test_pseudo(points=801) -> Pseudo:
@@ -538,6 +549,60 @@ def local_form_factor(ps: Pseudo, volume: float, g: np.ndarray) -> np.ndarray:
         val[zero] = 4.0 * math.pi / volume * integral[zero] + math.pi * ps.z / volume
         res[s:s + 256] = val
     return out
+
+
+# ----------------------------------------------------------------------------- start density
+def has_atomic_charge(ps: Pseudo) -> bool:
+    """crates/dft-engine/src/refstart.rs:56-59: PP_RHOATOM on the whole mesh, not all zero."""
+    rho = ps.rho_atom
+    return rho is not None and len(rho) == len(ps.r) and bool(np.any(np.asarray(rho) != 0.0))
+
+
+def atomic_charge_transform(ps: Pseudo, volume: float, q: np.ndarray) -> np.ndarray:
+    """rho_atom(|G|) / Omega = (integral of PP_RHOATOM j0(q r) dr) / Omega on the mesh
+    (Simpson in the index with rab, radial.rs:40-47), the exact per-shell quadrature of the
+    reference's Gamma start (refstart.rs:1213-1226; j0 taken as 1 at q = 0)."""
+    n = len(ps.r)
+    w = simpson_weights(n) * ps.rab
+    rho = np.asarray(ps.rho_atom, dtype=np.float64)
+    q = np.asarray(q, dtype=np.float64).reshape(-1)
+    out = np.empty(q.size)
+    for s in range(0, q.size, 256):
+        qq = q[s:s + 256]
+        j0 = spherical_bessel(0, qq[:, None] * ps.r[None, :])
+        j0[qq == 0.0, :] = 1.0
+        out[s:s + 256] = ((rho[None, :] * j0) @ w) / volume
+    return out
+
+
+def atomic_density(cell: Cell, ecut_ha: float, dims, species):
+    """The reference's atomic start density (refstart.rs:704-757 with the rho channel of
+    atomic_fields :1166-1230), or None when any species carries no atomic charge (the
+    uniform start, refstart.rs:708-710, 725-735).  rho(G) = sum_s rho_s(|G|) S_s(G) / Omega
+    on the 4 Ecut density sphere; n(r) = sum_G rho(G) e^{iGr} on the grid (C order),
+    negative values set to 0, then scaled so that sum n Omega / N_points = N_e."""
+    if not all(has_atomic_charge(s.pseudo) for s in species):
+        return None
+    dens = basis_at_k(cell, 4.0 * ecut_ha)
+    q2u, inv = np.unique(dens.gnorm2, return_inverse=True)
+    rg = np.zeros(dens.npw, np.complex128)
+    for sp in species:
+        ff = atomic_charge_transform(sp.pseudo, cell.volume, np.sqrt(q2u))[inv]
+        sf = np.zeros(dens.npw, np.complex128)
+        for tau in np.atleast_2d(sp.positions):
+            ang = (dens.gcart[:, 0] * tau[0] + dens.gcart[:, 1] * tau[1]) + dens.gcart[:, 2] * tau[2]
+            sf += np.cos(-ang) + 1j * np.sin(-ang)
+        rg += ff * sf
+    box = np.zeros(dims, np.complex128)
+    idx = g_to_fft(dens, dims)
+    box[idx[:, 0], idx[:, 1], idx[:, 2]] = rg
+    n = np.ascontiguousarray((np.fft.ifftn(box) * box.size).real)
+    n = np.maximum(n, 0.0)
+    electrons = float(sum(s.pseudo.z * np.atleast_2d(s.positions).shape[0] for s in species))
+    charge = float(n.sum()) * cell.volume / n.size
+    if not np.isfinite(charge) or charge <= 0.0:
+        raise ValueError("invalid atomic charge")
+    return n * (electrons / charge)
 
 
 def ionic_local(density: Basis, volume: float, species) -> np.ndarray:

@@ -40,6 +40,7 @@ class Cell:
     gamma_real: bool
     override: list | None = None
     seed: int = 2026
+    rho_radius: float | None = None  # Gaussian atomic charge (PP_RHOATOM) of this radius
     _cache: dict = field(default_factory=dict, repr=False)
 
     @property
@@ -51,7 +52,8 @@ class Cell:
         return len(self.positions)
 
     def species(self):
-        ps = S.synthetic_pseudo(self.z, self.rc, (0, 1), (1.0, 1.0), np.diag([3.0, 1.5]).reshape(-1))
+        ps = S.synthetic_pseudo(self.z, self.rc, (0, 1), (1.0, 1.0), np.diag([3.0, 1.5]).reshape(-1),
+                                rho_radius=self.rho_radius)
         return [S.Species(ps, self.positions)]
 
     def dims(self):
@@ -117,6 +119,13 @@ def si2() -> Cell:
     rows = np.array([[0, a / 2, a / 2], [a / 2, 0, a / 2], [a / 2, a / 2, 0]])
     pos = np.array([[0, 0, 0], [a / 4, a / 4, a / 4]])
     return Cell("si2_gamma_real_30ry", rows, 4.0, 0.45, pos, 15.0, 8, [((0.0, 0.0, 0.0), 1.0)], True, seed=2027)
+
+
+def si2_atomic(radius: float = 1.0) -> Cell:
+    """Si2 with a Gaussian atomic charge of `radius` Bohr, the atomic-density start."""
+    c = si2()
+    c.rho_radius = radius
+    return c
 
 
 def si8() -> Cell:

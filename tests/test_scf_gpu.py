@@ -20,7 +20,8 @@ def _oracle_species(w):
     out = []
     for s in w.species:
         p = s.pseudo
-        ps = S.Pseudo(p.z, p.r, p.rab, p.local, [S.Projector(l, u) for l, u in zip(p.l, p.beta)], p.dij)
+        ps = S.Pseudo(p.z, p.r, p.rab, p.local, [S.Projector(l, u) for l, u in zip(p.l, p.beta)], p.dij,
+                      p.rho_atom)
         out.append(S.Species(ps, s.positions))
     return out
 
@@ -29,9 +30,13 @@ def _compare(w, threshold_ha, ctx, smearing_ha=None):
     gpu = GpuScf(w, ctx, ScfOptions(threshold_ha=threshold_ha, smearing_ha=smearing_ha))
     starts = [s.cpu().numpy().T.copy() for s in gpu.starts]
     res = gpu.run()
-    ref = scf_ref.run(w.rows, _oracle_species(w), w.ecut_ha, w.dims(), w.kpoints, w.gamma_real, w.bands,
+    sp = _oracle_species(w)
+    # the start density the oracle's own setup gives (None: uniform)
+    n0 = S.atomic_density(S.Cell(w.rows), w.ecut_ha, w.dims(), sp)
+    assert gpu.start_kind == ("uniform" if n0 is None else "atomic")
+    ref = scf_ref.run(w.rows, sp, w.ecut_ha, w.dims(), w.kpoints, w.gamma_real, w.bands,
                       w.ionic_potential(), starts, O.ewald(w.rows, w.species), threshold_ha=threshold_ha,
-                      smearing_ha=smearing_ha)
+                      smearing_ha=smearing_ha, start_density=n0)
     natoms = w.natoms
     assert res.converged and ref.converged
     assert abs(res.energy_ha - ref.energy) <= 1e-7 * natoms, (res.energy_ha, ref.energy)
@@ -52,6 +57,14 @@ def test_si2_gamma_scf_matches_oracle(ctx):
     the run uses Fermi-Dirac smearing of 0.01 Ha (the reference's metal setting)."""
     res, _ = _compare(W.si2_gamma(), 1e-8, ctx, smearing_ha=0.01)
     assert res.records[-1].dr2_ry < 2e-8
+
+
+def test_si2_scf_from_the_atomic_start_matches_oracle(ctx):
+    """Config 1's atomic-Gaussian start (Gaussian PP_RHOATOM of radius 1 Bohr; the start
+    density of refstart.rs:704-757) to 1e-8 Ha, Fermi-Dirac 0.01 Ha as above: the same
+    maps and energies as the oracle SCF from its own atomic start."""
+    res, ref = _compare(W.si2_gamma_atomic(), 1e-8, ctx, smearing_ha=0.01)
+    assert abs(res.records[0].dr2_ry - ref.dr2[0]) <= 1e-9 * ref.dr2[0]
 
 
 def test_si8_two_kpoint_scf_matches_oracle(ctx):
