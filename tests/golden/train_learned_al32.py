@@ -7,10 +7,11 @@ Needs one GPU.  Geometries: the Al32 cell (fcc 2x2x2 conventional, a = 15.30 Boh
 +-0.08 Bohr, seeds TRAIN_BASE + 0 .. TRAIN_BASE + geometries - 1.  Geometry g contributes
 its k point g % 8: the eigenpairs of the lowest 64 + 16 bands from a tight FP64 Davidson
 (REF_THRESHOLD Ha) stand in for the exact spectrum, and two TPA Davidson states of it
-(after TRAIN_ITERATIONS[g % 13] and TRAIN_ITERATIONS[(g + 6) % 13] iterations) give 8
-seeded bands each with |e|^2 above MIN_ERROR, paired with their ideal corrections e.
-600 full-batch Adam steps from TPA (zero output layer).  The held-out geometry (seed HELD_OUT, k points 0 and 5) scores the
-correction loss before and after; then the batched solver on all 8 of its k points
+(after its[g % n] and its[(g + n // 2) % n] iterations; its = TRAIN_ITERATIONS, n = 13,
+unless --iterations names others) give 8 seeded bands each with |e|^2 above MIN_ERROR,
+paired with their ideal corrections e.  600 full-batch Adam steps from TPA (zero output
+layer).  The held-out geometry (seed HELD_OUT, k points 0 and 5) scores the correction
+loss before and after; then the batched solver on all 8 of its k points
 counts H columns for TPA and the trained network (occupied bands to 1e-8 Ha), and with
 --scf both SCFs (Fermi-Dirac 0.01 Ha, to 1e-6 Ha/atom) are timed.
 
@@ -91,11 +92,15 @@ def main():
     ap.add_argument("--steps", type=int, default=600)
     ap.add_argument("--lr", type=float, default=3e-3)
     ap.add_argument("--scf", action="store_true")
+    ap.add_argument("--iterations", default=None,
+                    help="comma-separated Davidson iteration counts the states are drawn from "
+                         "(default: TRAIN_ITERATIONS)")
     ap.add_argument("--out", default=os.path.join(HERE, "learned_al32.npz"))
     a = ap.parse_args()
     from baandi_b200.hamiltonian import default_context
     ctx = default_context()
-    its = LP.TRAIN_ITERATIONS
+    its = LP.TRAIN_ITERATIONS if a.iterations is None else tuple(int(x) for x in a.iterations.split(","))
+    half = len(its) // 2
 
     def problems():
         for g in range(a.geometries):
@@ -104,7 +109,7 @@ def main():
                                        threshold=REF_THRESHOLD)
 
     t0 = time.perf_counter()
-    samples = LP.build_samples(ctx, problems(), iterations=lambda g: (its[g % len(its)], its[(g + 6) % len(its)]),
+    samples = LP.build_samples(ctx, problems(), iterations=lambda g: (its[g % len(its)], its[(g + half) % len(its)]),
                                min_error=MIN_ERROR, bands_per_state=8, seed=1)
     t_data = time.perf_counter() - t0
     hw = W.al32_k222(HELD_OUT)
