@@ -84,17 +84,21 @@ def test_batched_solver_reaches_tpa_eigenvalues(ctx):
 
 @pytest.mark.gpu
 def test_scf_with_the_network_reaches_the_tpa_energy(ctx):
-    """The held-out geometry's SCF (Fermi-Dirac 0.01 Ha, Thomas-Fermi mixing) to 1e-7
-    Ha/atom with TPA and with the network: energies within 1e-6 Ha/atom."""
+    """The held-out geometry's SCF (Fermi-Dirac 0.01 Ha, Thomas-Fermi mixing) to 1e-8
+    Ha/atom with TPA and with the network, each map's Davidson allowed 80 iterations (the
+    network's solves need more than the default 20 to reach their threshold): energies
+    within 1e-6 Ha/atom."""
     from baandi_b200.scf import GpuScf, ScfOptions
     w = W.al32_k222(HELD_OUT)
     LP.install(ctx, _fixture()["params"])
     e = {}
     for name in ("tpa", "learned"):
-        o = ScfOptions(threshold_ha=1e-7 * w.natoms, smearing_ha=0.01, thomas_fermi=True, preconditioner=name)
+        o = ScfOptions(threshold_ha=1e-8 * w.natoms, smearing_ha=0.01, thomas_fermi=True, preconditioner=name,
+                       davidson_max_iterations=80)
         r = GpuScf(w, ctx, o).run()
         assert r.converged
         e[name] = r.energy_ha
         print(f"SCF {name}: {r.iterations} maps, {sum(m.h_columns for m in r.records)} H columns, "
-              f"{r.seconds:.3f} s, E = {r.energy_ha:.9f} Ha")
+              f"{r.seconds:.3f} s, E = {r.energy_ha:.9f} Ha, Davidson iterations per map "
+              f"{[m.davidson_iterations for m in r.records]}")
     assert abs(e["learned"] - e["tpa"]) <= 1e-6 * w.natoms
