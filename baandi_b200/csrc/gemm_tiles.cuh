@@ -1,9 +1,12 @@
-// FP64 tall-skinny products on the CUDA cores (real double or complex double2), with
-// shared-memory tiles filled by cp.async one step ahead of the arithmetic and a 4 x 4
-// register tile per thread.  FP64 on sm_100a runs at the same rate on the CUDA cores as
-// through DMMA, and tcgen05 has no FP64 kind.
-//   tn_tile: P = A[r0:r1, :]^H B[r0:r1, :] for one 32 x 32 output tile (split over rows)
-//   nn_tile: C (+)= A B for one 64-row x 32-column output tile, A tall, B small
+// FP64 tall-skinny products (real double or complex double2) with shared-memory tiles
+// filled by cp.async ahead of the arithmetic.  tcgen05 has no FP64 kind; the FP64 tensor
+// path of sm_100a is mma.sync m8n8k4 f64 (DMMA), whose peak matches the CUDA cores' DFMA
+// (37 TFLOP/s measured against 34 for a DFMA loop on one B200) but which issues 256
+// multiply-adds per warp instruction instead of 32, so the hot tiles use it.
+//   tn_tile / nn_tile (DFMA, 4 x 4 register tiles): the small generic products
+//     (32 x 32 Gram tiles, 64 x 32 rotation tiles)
+//   tn_tile48_mma: P = A^H B, 48 x 48 tiles (projections P^H X, Davidson Grams)
+//   nn_tile64_mma: C (+)= A B, 64 x 64 tiles (back-projection P W, Davidson rotations)
 #pragma once
 #include <cuda_runtime.h>
 
@@ -101,44 +104,60 @@ __device__ __forceinline__ void tn_tile(const D* __restrict__ A, int64_t lda, co
     }
 }
 
-// 48 x 48 tiles of P = A^H B for the Davidson's Grams (m, n <= the basis capacity, 48 for
-// the k-point cells): 256 threads; thread (ti, tj) = (lane mod 16, 2 warp + lane / 16)
-// owns outputs i = i0 + ti + 16 a, j = j0 + 3 tj + b (a, b < 3).  A warp's columns are
-// uniform, so a warp whose columns all lie at or beyond n skips the arithmetic.  The rows
-// stream through kStages48 shared-memory stages of kBK48 rows each, filled by cp.async
-// kStages48 - 1 stages ahead of the arithmetic; a stage holds each column's kBK48 rows
-// contiguously with a pitch of kBK48 + 1 elements, so both the fill (consecutive threads,
-// consecutive rows) and the arithmetic's reads (16 columns of one row per half-warp, 17
-// elements apart) meet no bank conflicts.  Dynamic shared memory: tn48_smem_bytes<D>().
+// 48 x 48 tiles of P = A^H B for the Davidson's Grams and the projections (m, n up to the
+// basis capacity or the projector count): the rows stream through shared-memory stages of
+// kBK48 rows each, filled by cp.async ahead of the arithmetic.
 constexpr int kBK48 = 16;
-constexpr int kStages48 = 4;
-constexpr int kPitch48 = kBK48 + 1;
+
+// tn_tile48_mma: P[j * ldp + i] = sum over rows r0 .. r1 - 1 of conj(A[r][i0 + i]) B[r][j0 + j]
+// for the valid i < m - i0, j < n - j0, with mma.sync m8n8k4 f64 (DMMA) on fragments read
+// from shared memory.  One DMMA does 256 multiply-adds per warp
+// instruction against 32 for DFMA, so the FP64 pipe is no longer held back by issue
+// slots and operand reads.  256 threads = 8 warps: warp w takes the K half g = w / 4 of
+// every 16-row stage (k-steps 2g and 2g + 1 of 4 rows each) and the 24 x 24 output block
+// (wi, wj) = ((w / 2) % 2, w % 2), 3 x 3 MMA tiles of 8 x 8; the two halves' sums meet in
+// shared memory at the end (half 1 stores, half 0 adds and writes P).  A stage holds each
+// column's 16 rows with a pitch of 20 elements, so the fragment reads (8 columns x 4 rows
+// per warp) meet no bank conflicts for double and double2.  Fragments of m8n8k4 (row.col,
+// f64): A (8 x 4) lane holds (m, k) = (lane / 4, lane % 4); B (4 x 8) (k, n) = (lane % 4,
+// lane / 4); C (8 x 8) (m, n) = (lane / 4, 2 (lane % 4) + e), e = 0, 1.  Complex:
+// Re += ar br + ai bi, Im += ar bi - ai br (four real DMMAs; A^H conjugates A).
+constexpr int kStagesM = 3;
+constexpr int kPitchM = kBK48 + 4;
 template <class D>
-constexpr size_t tn48_smem_bytes() {
-  return (size_t)2 * kStages48 * 48 * kPitch48 * sizeof(D);
+constexpr size_t tn48m_smem_bytes() {
+  return (size_t)2 * kStagesM * 48 * kPitchM * sizeof(D);
+}
+__device__ __forceinline__ void dmma8x8x4(double& c0, double& c1, double a, double b) {
+  asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+      : "+d"(c0), "+d"(c1)
+      : "d"(a), "d"(b));
 }
 template <class D>
-__device__ __forceinline__ void tn_tile48(const D* __restrict__ A, int64_t lda, const D* __restrict__ B,
-                                          int64_t ldb, int i0, int j0, int m, int n, int64_t r0, int64_t r1,
-                                          D* __restrict__ P, int64_t ldp) {
+__device__ __forceinline__ void tn_tile48_mma(const D* __restrict__ A, int64_t lda, const D* __restrict__ B,
+                                              int64_t ldb, int i0, int j0, int m, int n, int64_t r0, int64_t r1,
+                                              D* __restrict__ P, int64_t ldp) {
+  constexpr bool kComplex = sizeof(D) == 16;
   extern __shared__ __align__(16) unsigned char tn48_smem[];
-  D* As = reinterpret_cast<D*>(tn48_smem);  // [stage][48 columns][kPitch48 rows]
-  D* Bs = As + kStages48 * 48 * kPitch48;
+  D* As = reinterpret_cast<D*>(tn48_smem);  // [stage][48 columns][kPitchM rows]
+  D* Bs = As + kStagesM * 48 * kPitchM;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int ti = lane & 15, tj = 2 * warp + (lane >> 4);
-  const bool warp_live = j0 + 6 * warp < n;
-  D acc[3][3];
+  const int g = warp >> 2, wi = (warp >> 1) & 1, wj = warp & 1;
+  const int fm = lane >> 2, fk = lane & 3;
+  const bool warp_live = i0 + 24 * wi < m && j0 + 24 * wj < n;
+  double cre[3][3][2], cim[3][3][2];
 #pragma unroll
-  for (int a = 0; a < 3; ++a)
+  for (int x = 0; x < 3; ++x)
 #pragma unroll
-    for (int b = 0; b < 3; ++b) acc[a][b] = Arith<D>::zero();
-  // one stage: kBK48 rows x 48 columns of A and of B, 6 elements per thread
+    for (int y = 0; y < 3; ++y)
+#pragma unroll
+      for (int e = 0; e < 2; ++e) cre[x][y][e] = cim[x][y][e] = 0.0;
   auto load = [&](int buf, int64_t rb) {
     for (int e = tid; e < 2 * 48 * kBK48; e += 256) {
       const int mat = e / (48 * kBK48), idx = e - mat * (48 * kBK48);
       const int rr = idx % kBK48, c = idx / kBK48;
       const int64_t r = rb + rr;
-      D* dst = (mat == 0 ? As : Bs) + (buf * 48 + c) * kPitch48 + rr;
+      D* dst = (mat == 0 ? As : Bs) + (buf * 48 + c) * kPitchM + rr;
       const bool ok = r < r1 && (mat == 0 ? i0 + c < m : j0 + c < n);
       if (ok)
         async_copy(dst, mat == 0 ? A + (int64_t)(i0 + c) * lda + r : B + (int64_t)(j0 + c) * ldb + r);
@@ -148,49 +167,84 @@ __device__ __forceinline__ void tn_tile48(const D* __restrict__ A, int64_t lda, 
     async_commit();
   };
   const int64_t steps = (r1 - r0 + kBK48 - 1) / kBK48;
-  // one cp.async group per stage, empty ones past the end, so that waiting for all but
-  // the newest kStages48 - 2 groups always means the current stage has landed
+  // one cp.async group per stage, empty ones past the end (as in tn_tile48)
 #pragma unroll
-  for (int s = 0; s < kStages48 - 1; ++s) {
+  for (int s = 0; s < kStagesM - 1; ++s) {
     if (s < steps)
       load(s, r0 + s * kBK48);
     else
       async_commit();
   }
   for (int64_t s = 0; s < steps; ++s) {
-    async_wait<kStages48 - 2>();
-    __syncthreads();  // stage s visible to all; every thread is done with stage s - 1
-    const int64_t nxt = s + kStages48 - 1;
+    async_wait<kStagesM - 2>();
+    __syncthreads();  // stage s visible to all; every warp is done with stage s - 1
+    const int64_t nxt = s + kStagesM - 1;
     if (nxt < steps)
-      load((int)(nxt % kStages48), r0 + nxt * kBK48);  // refills the buffer of stage s - 1
+      load((int)(nxt % kStagesM), r0 + nxt * kBK48);  // refills the buffer of stage s - 1
     else
       async_commit();
     if (warp_live) {
-      const D* as = As + (int)(s % kStages48) * 48 * kPitch48;
-      const D* bs = Bs + (int)(s % kStages48) * 48 * kPitch48;
+      const D* as = As + (int)(s % kStagesM) * 48 * kPitchM + (24 * wi + fm) * kPitchM + 8 * g + fk;
+      const D* bs = Bs + (int)(s % kStagesM) * 48 * kPitchM + (24 * wj + fm) * kPitchM + 8 * g + fk;
 #pragma unroll
-      for (int rr = 0; rr < kBK48; ++rr) {
+      for (int kk = 0; kk < 2; ++kk) {
         D a[3], b[3];
 #pragma unroll
         for (int q = 0; q < 3; ++q) {
-          a[q] = as[(ti + 16 * q) * kPitch48 + rr];
-          b[q] = bs[(3 * tj + q) * kPitch48 + rr];
+          a[q] = as[8 * q * kPitchM + 4 * kk];
+          b[q] = bs[8 * q * kPitchM + 4 * kk];
         }
 #pragma unroll
         for (int x = 0; x < 3; ++x)
 #pragma unroll
-          for (int y = 0; y < 3; ++y) acc[x][y] = Arith<D>::cmac(acc[x][y], a[x], b[y]);
+          for (int y = 0; y < 3; ++y) {
+            if constexpr (kComplex) {
+              dmma8x8x4(cre[x][y][0], cre[x][y][1], a[x].x, b[y].x);
+              dmma8x8x4(cre[x][y][0], cre[x][y][1], a[x].y, b[y].y);
+              dmma8x8x4(cim[x][y][0], cim[x][y][1], a[x].x, b[y].y);
+              dmma8x8x4(cim[x][y][0], cim[x][y][1], -a[x].y, b[y].x);
+            } else {
+              dmma8x8x4(cre[x][y][0], cre[x][y][1], a[x], b[y]);
+            }
+          }
       }
     }
   }
   async_wait<0>();
+  __syncthreads();  // every stage consumed: the A stages hold the K halves' meeting place
+  D* red = As;      // [48 columns][48 rows] of the tile, local indices
+  if (g == 1 && warp_live) {
 #pragma unroll
-  for (int x = 0; x < 3; ++x)
+    for (int x = 0; x < 3; ++x)
 #pragma unroll
-    for (int y = 0; y < 3; ++y) {
-      const int i = i0 + ti + 16 * x, j = j0 + 3 * tj + y;
-      if (i < m && j < n) P[(int64_t)j * ldp + i] = acc[x][y];
-    }
+      for (int y = 0; y < 3; ++y)
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+          const int i = 24 * wi + 8 * x + fm, j = 24 * wj + 8 * y + 2 * fk + e;
+          if constexpr (kComplex)
+            red[j * 48 + i] = make_double2(cre[x][y][e], cim[x][y][e]);
+          else
+            red[j * 48 + i] = cre[x][y][e];
+        }
+  }
+  __syncthreads();
+  if (g == 0 && warp_live) {
+#pragma unroll
+    for (int x = 0; x < 3; ++x)
+#pragma unroll
+      for (int y = 0; y < 3; ++y)
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+          const int i = 24 * wi + 8 * x + fm, j = 24 * wj + 8 * y + 2 * fk + e;
+          if (i0 + i < m && j0 + j < n) {
+            const D h = red[j * 48 + i];
+            if constexpr (kComplex)
+              P[(int64_t)(j0 + j) * ldp + i0 + i] = make_double2(cre[x][y][e] + h.x, cim[x][y][e] + h.y);
+            else
+              P[(int64_t)(j0 + j) * ldp + i0 + i] = cre[x][y][e] + h;
+          }
+        }
+  }
 }
 
 // 128 threads; thread (tr, tc) owns rows r0 + 16a + tr and columns j0 + 8b + tc of a
@@ -277,43 +331,56 @@ __device__ __forceinline__ void nn_tile(const D* __restrict__ A, int64_t lda, co
     }
 }
 
-// 64 x 64 tiles of C (+)= A B, A tall (rows x k, column-major), B small (k x n): 256
-// threads; thread (tr, tc) = (tid mod 16, tid / 16) owns rows r0 + tr + 16 x and columns
-// j0 + tc + 16 y (x, y < 4).  The inner index streams through kStages64 shared-memory
-// stages of kBK rows of A (64 rows each, contiguous as in memory) and kBK entries of each
-// of 64 columns of B (a column's entries contiguous, pitch kBK + 1), filled by cp.async
-// kStages64 - 1 stages ahead; neither the fill nor the arithmetic's reads meet bank
-// conflicts.  SKIP_EMPTY skips the 16-column groups at or beyond n.  Dynamic shared
-// memory: nn64_smem_bytes<D>().
+// 64 x 64 tiles of C (+)= A B, A tall (rows x k, column-major), B small (k x n): the inner
+// index streams through kStages64 shared-memory stages of kBK entries, filled by cp.async
+// kStages64 - 1 stages ahead.
 constexpr int kStages64 = 3;
-constexpr int kPitchB64 = kBK + 1;
+
+// nn_tile64_mma: C (+)= A B for one 64 x 64 tile (rows r0 .., columns j0 ..) with
+// mma.sync m8n8k4 f64.  8 warps: warp w owns rows r0 + 32 (w % 2) ..
+// + 31 and columns j0 + 16 (w / 2) .. + 15, 4 x 2 MMA tiles of 8 x 8; each 16-entry
+// stage is 4 k-steps of 4.  Shared memory holds A's stage rows with a pitch of 66
+// (complex) or 68 (real) elements and B's columns with a pitch of 20, so the fragment
+// reads (A: 8 rows x 4 inner indices; B: 4 inner indices x 8 columns) meet no bank
+// conflicts.  Complex: Re += ar br - ai bi, Im += ar bi + ai br.  SKIP_EMPTY skips the
+// warps whose 16 columns lie at or beyond n.  Dynamic shared memory: nn64m_smem_bytes<D>().
 template <class D>
-constexpr size_t nn64_smem_bytes() {
-  return (size_t)kStages64 * (kBK * 64 + 64 * kPitchB64) * sizeof(D);
+__host__ __device__ constexpr int nn_pitch_a() {
+  return sizeof(D) == 16 ? 66 : 68;
+}
+template <class D>
+constexpr size_t nn64m_smem_bytes() {
+  return (size_t)kStages64 * (kBK * nn_pitch_a<D>() + 64 * kPitchM) * sizeof(D);
 }
 template <class D, bool SKIP_EMPTY = false>
-__device__ __forceinline__ void nn_tile64(const D* __restrict__ A, int64_t lda, const D* __restrict__ B,
-                                          int64_t ldb, D* __restrict__ C, int64_t ldc, int64_t rows, int n, int k,
-                                          int64_t r0, int j0, bool accumulate) {
+__device__ __forceinline__ void nn_tile64_mma(const D* __restrict__ A, int64_t lda, const D* __restrict__ B,
+                                              int64_t ldb, D* __restrict__ C, int64_t ldc, int64_t rows, int n,
+                                              int k, int64_t r0, int j0, bool accumulate) {
+  constexpr bool kComplex = sizeof(D) == 16;
+  constexpr int PA = nn_pitch_a<D>();
   extern __shared__ __align__(16) unsigned char nn64_smem[];
-  D* As = reinterpret_cast<D*>(nn64_smem);     // [stage][kBK][64 rows]
-  D* Bs = As + kStages64 * kBK * 64;           // [stage][64 columns][kPitchB64]
-  const int tid = threadIdx.x;
-  const int tr = tid & 15, tc = tid >> 4;
-  D acc[4][4];
+  D* As = reinterpret_cast<D*>(nn64_smem);  // [stage][kBK][PA]: 64 rows of A per inner index
+  D* Bs = As + kStages64 * kBK * PA;        // [stage][64 columns][kPitchM]
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int wr = warp & 1, wc = warp >> 1;
+  const int fm = lane >> 2, fk = lane & 3;
+  const bool live = !SKIP_EMPTY || j0 + 16 * wc < n;
+  double cre[4][2][2], cim[4][2][2];
 #pragma unroll
-  for (int a = 0; a < 4; ++a)
+  for (int x = 0; x < 4; ++x)
 #pragma unroll
-    for (int b = 0; b < 4; ++b) acc[a][b] = Arith<D>::zero();
+    for (int y = 0; y < 2; ++y)
+#pragma unroll
+      for (int e = 0; e < 2; ++e) cre[x][y][e] = cim[x][y][e] = 0.0;
   auto load = [&](int buf, int pb) {
-    D* as = As + buf * kBK * 64;
-    D* bs = Bs + buf * 64 * kPitchB64;
+    D* as = As + buf * kBK * PA;
+    D* bs = Bs + buf * 64 * kPitchM;
 #pragma unroll
     for (int q = 0; q < 4; ++q) {  // A: kBK x 64, consecutive threads on consecutive rows
       const int e = tid + 256 * q;
       const int rr = e & 63, p = e >> 6;
       const int64_t r = r0 + rr;
-      D* d = as + p * 64 + rr;
+      D* d = as + p * PA + rr;
       if (r < rows && pb + p < k)
         async_copy(d, A + (int64_t)(pb + p) * lda + r);
       else
@@ -323,7 +390,7 @@ __device__ __forceinline__ void nn_tile64(const D* __restrict__ A, int64_t lda, 
     for (int q = 0; q < 4; ++q) {  // B: 64 columns x kBK, consecutive threads on consecutive entries
       const int e = tid + 256 * q;
       const int p = e & (kBK - 1), c = e >> 4;
-      D* d = bs + c * kPitchB64 + p;
+      D* d = bs + c * kPitchM + p;
       if (pb + p < k && j0 + c < n)
         async_copy(d, B + (int64_t)(j0 + c) * ldb + pb + p);
       else
@@ -331,7 +398,6 @@ __device__ __forceinline__ void nn_tile64(const D* __restrict__ A, int64_t lda, 
     }
     async_commit();
   };
-  const int ny = SKIP_EMPTY ? min(4, max(0, (n - j0 - tc + 15) / 16)) : 4;
   const int steps = (k + kBK - 1) / kBK;
 #pragma unroll
   for (int s = 0; s < kStages64 - 1; ++s) {
@@ -342,42 +408,58 @@ __device__ __forceinline__ void nn_tile64(const D* __restrict__ A, int64_t lda, 
   }
   for (int s = 0; s < steps; ++s) {
     async_wait<kStages64 - 2>();
-    __syncthreads();  // stage s visible to all; every thread is done with stage s - 1
+    __syncthreads();  // stage s visible to all; every warp is done with stage s - 1
     const int nxt = s + kStages64 - 1;
     if (nxt < steps)
       load(nxt % kStages64, nxt * kBK);  // refills the buffer of stage s - 1
     else
       async_commit();
-    const D* as = As + (s % kStages64) * kBK * 64;
-    const D* bs = Bs + (s % kStages64) * 64 * kPitchB64;
+    if (live) {
+      const D* as = As + (s % kStages64) * kBK * PA + fk * PA + 32 * wr + fm;
+      const D* bs = Bs + (s % kStages64) * 64 * kPitchM + (16 * wc + fm) * kPitchM + fk;
 #pragma unroll
-    for (int p = 0; p < kBK; ++p) {
-      D a[4], b[4];
+      for (int kk = 0; kk < kBK / 4; ++kk) {
+        D a[4], b[2];
 #pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        a[q] = as[p * 64 + q * 16 + tr];
-        b[q] = bs[(q * 16 + tc) * kPitchB64 + p];
+        for (int q = 0; q < 4; ++q) a[q] = as[4 * kk * PA + 8 * q];
+#pragma unroll
+        for (int q = 0; q < 2; ++q) b[q] = bs[8 * q * kPitchM + 4 * kk];
+#pragma unroll
+        for (int x = 0; x < 4; ++x)
+#pragma unroll
+          for (int y = 0; y < 2; ++y) {
+            if constexpr (kComplex) {
+              dmma8x8x4(cre[x][y][0], cre[x][y][1], a[x].x, b[y].x);
+              dmma8x8x4(cre[x][y][0], cre[x][y][1], -a[x].y, b[y].y);
+              dmma8x8x4(cim[x][y][0], cim[x][y][1], a[x].x, b[y].y);
+              dmma8x8x4(cim[x][y][0], cim[x][y][1], a[x].y, b[y].x);
+            } else {
+              dmma8x8x4(cre[x][y][0], cre[x][y][1], a[x], b[y]);
+            }
+          }
       }
-#pragma unroll
-      for (int y = 0; y < 4; ++y)
-        if (y < ny) {
-#pragma unroll
-          for (int x = 0; x < 4; ++x) acc[x][y] = Arith<D>::mac(acc[x][y], a[x], b[y]);
-        }
     }
   }
   async_wait<0>();
+  if (!live) return;
 #pragma unroll
   for (int x = 0; x < 4; ++x)
 #pragma unroll
-    for (int y = 0; y < 4; ++y) {
-      const int64_t r = r0 + x * 16 + tr;
-      const int j = j0 + y * 16 + tc;
-      if (r < rows && j < n) {
-        D& out = C[(int64_t)j * ldc + r];
-        out = accumulate ? Arith<D>::add(out, acc[x][y]) : acc[x][y];
+    for (int y = 0; y < 2; ++y)
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const int64_t r = r0 + 32 * wr + 8 * x + fm;
+        const int j = j0 + 16 * wc + 8 * y + 2 * fk + e;
+        if (r < rows && j < n) {
+          D v;
+          if constexpr (kComplex)
+            v = make_double2(cre[x][y][e], cim[x][y][e]);
+          else
+            v = cre[x][y][e];
+          D& out = C[(int64_t)j * ldc + r];
+          out = accumulate ? Arith<D>::add(out, v) : v;
+        }
       }
-    }
 }
 
 }  // namespace tiles

@@ -456,7 +456,7 @@ __global__ void __launch_bounds__(256, 2) k_project(const NlDev* __restrict__ nl
   const int cols = ca.cols, rows = nl.rows;
   if ((int)blockIdx.y * 48 >= cols) return;
   const int64_t r0 = (int64_t)ks * kchunk, r1 = min((int64_t)rows, r0 + kchunk);
-  tiles::tn_tile48<T>(reinterpret_cast<const T*>(nl.p), rows, reinterpret_cast<const T*>(ca.x),
+  tiles::tn_tile48_mma<T>(reinterpret_cast<const T*>(nl.p), rows, reinterpret_cast<const T*>(ca.x),
                       ca.ldx / (int64_t)(sizeof(T) / sizeof(double)), blockIdx.x * 48, blockIdx.y * 48, nproj, cols,
                       r0, r1, reinterpret_cast<T*>(nl.part) + (int64_t)ks * cols * nproj, nproj);
 }
@@ -499,7 +499,7 @@ __global__ void __launch_bounds__(256, 2) k_back(const NlDev* __restrict__ nls, 
   const int64_t r0 = (int64_t)blockIdx.x * 64;
   const int j0 = blockIdx.y * 64;
   if (r0 >= rows || j0 >= cols) return;
-  tiles::nn_tile64<T>(reinterpret_cast<const T*>(nl.p), rows, reinterpret_cast<const T*>(nl.wd), nproj,
+  tiles::nn_tile64_mma<T>(reinterpret_cast<const T*>(nl.p), rows, reinterpret_cast<const T*>(nl.wd), nproj,
                       reinterpret_cast<T*>(ca.y), ca.ldy / (int64_t)(sizeof(T) / sizeof(double)), rows, cols, nproj,
                       r0, j0, true);
 }
@@ -926,19 +926,19 @@ int launch_nonlocal(const NlDev* nl, int gamma, const NlShape& sh, int max_rows,
   if (gamma) {
     {
       StageScope sc(ev, 3, s);
-      k_project<double><<<pg, 256, tiles::tn48_smem_bytes<double>(), s>>>(nl, sh.nproj, sh.ksplit, sh.kchunk, b);
+      k_project<double><<<pg, 256, tiles::tn48m_smem_bytes<double>(), s>>>(nl, sh.nproj, sh.ksplit, sh.kchunk, b);
     }
     { StageScope sc(ev, 4, s); k_couple<double><<<cg, cth, 0, s>>>(nl, sh.nproj, sh.ksplit, b); }
-    { StageScope sc(ev, 5, s); k_back<double><<<bg_, 256, tiles::nn64_smem_bytes<double>(), s>>>(nl, sh.nproj, b); }
+    { StageScope sc(ev, 5, s); k_back<double><<<bg_, 256, tiles::nn64m_smem_bytes<double>(), s>>>(nl, sh.nproj, b); }
   } else {
     {
       StageScope sc(ev, 3, s);
-      k_project<double2><<<pg, 256, tiles::tn48_smem_bytes<double2>(), s>>>(nl, sh.nproj, sh.ksplit, sh.kchunk, b);
+      k_project<double2><<<pg, 256, tiles::tn48m_smem_bytes<double2>(), s>>>(nl, sh.nproj, sh.ksplit, sh.kchunk, b);
     }
     { StageScope sc(ev, 4, s); k_couple<double2><<<cg, cth, 0, s>>>(nl, sh.nproj, sh.ksplit, b); }
     {
       StageScope sc(ev, 5, s);
-      k_back<double2><<<bg_, 256, tiles::nn64_smem_bytes<double2>(), s>>>(nl, sh.nproj, b);
+      k_back<double2><<<bg_, 256, tiles::nn64m_smem_bytes<double2>(), s>>>(nl, sh.nproj, b);
     }
   }
   return 3;
@@ -982,16 +982,16 @@ static void configure_one(cudaError_t& e, size_t plane_smem, size_t stick_smem) 
 int configure_kernels(size_t plane_smem, size_t stick_smem) {
   cudaError_t e = cudaSuccess;
   e = cudaFuncSetAttribute((const void*)k_project<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)tiles::tn48_smem_bytes<double>());
+                           (int)tiles::tn48m_smem_bytes<double>());
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute((const void*)k_project<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)tiles::tn48_smem_bytes<double2>());
+                             (int)tiles::tn48m_smem_bytes<double2>());
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute((const void*)k_back<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)tiles::nn64_smem_bytes<double>());
+                             (int)tiles::nn64m_smem_bytes<double>());
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute((const void*)k_back<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)tiles::nn64_smem_bytes<double2>());
+                             (int)tiles::nn64m_smem_bytes<double2>());
   if (e != cudaSuccess) return 1;
   e = cudaFuncSetAttribute((const void*)k_planes, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)plane_smem);
   if (e == cudaSuccess)

@@ -584,7 +584,7 @@ __global__ void __launch_bounds__(256, 2) k_dv_nn(const Bufs<D>* __restrict__ bu
   const int64_t r0 = (int64_t)blockIdx.y * 64;
   const int j0 = blockIdx.x * 64;
   if (d.n <= 0 || d.prec || j0 >= d.n || r0 >= rows) return;
-  tiles::nn_tile64<D, true>(d.A, rows, d.B, d.ldb, d.C, rows, rows, d.n, d.k, r0, j0, d.accumulate != 0);
+  tiles::nn_tile64_mma<D, true>(d.A, rows, d.B, d.ldb, d.C, rows, rows, d.n, d.k, r0, j0, d.accumulate != 0);
 }
 
 // Split-K partial Gram products: part[slot][s][j][i] = sum over row slice s of
@@ -601,7 +601,7 @@ __global__ void __launch_bounds__(256, 2) k_dv_tn(const Bufs<D>* __restrict__ bu
   chunk = ((chunk + 31) / 32) * 32;
   const int64_t r0 = min(rows, (int64_t)sidx * chunk), r1 = min(rows, r0 + chunk);
   D* part = bufs[k].part + slot * slot_elems + (int64_t)sidx * d.m * d.n;
-  tiles::tn_tile48<D>(d.A, rows, d.B, rows, blockIdx.x * 48, blockIdx.y * 48, d.m, d.n, r0, r1, part, d.m);
+  tiles::tn_tile48_mma<D>(d.A, rows, d.B, rows, blockIdx.x * 48, blockIdx.y * 48, d.m, d.n, r0, r1, part, d.m);
 }
 
 // G[i + j ldg] = sum_s part[slot][s][j][i] in slice order.
@@ -1489,7 +1489,7 @@ class KsetSolver {
   }
   int64_t nn(int nslots) {
     const dim3 grid((unsigned)((o_.cap + 63) / 64), (unsigned)((max_rows_ + 63) / 64), (unsigned)(nslots * nk_));
-    k_dv_nn<D><<<grid, 256, tiles::nn64_smem_bytes<D>(), s_>>>(d_bufs_, d_nn_, nk_);
+    k_dv_nn<D><<<grid, 256, tiles::nn64m_smem_bytes<D>(), s_>>>(d_bufs_, d_nn_, nk_);
     if (!tensor_products()) return 1;
     k_dv_tc_descs<D><<<1, 128, 0, s_>>>(d_bufs_, d_nn_, nslots, d_tn_, 0, nk_, d_tcnn_, d_tctn_);
     return 2 + tc::launch_zgemm(tc::kNN, d_tcnn_, nslots * nk_, max_rows_, o_.cap, o_.cap, 1, false, tc_work_,
@@ -1498,7 +1498,7 @@ class KsetSolver {
   bool tensor_products() const { return o_.tensor && sizeof(D) == sizeof(double2) && tc_ready_; }
   int64_t tn(int nslots) {
     const unsigned t = (unsigned)((o_.cap + 47) / 48);
-    k_dv_tn<D><<<dim3(t, t, (unsigned)(nslots * nk_ * ksplit_)), 256, tiles::tn48_smem_bytes<D>(), s_>>>(
+    k_dv_tn<D><<<dim3(t, t, (unsigned)(nslots * nk_ * ksplit_)), 256, tiles::tn48m_smem_bytes<D>(), s_>>>(
         d_bufs_, d_tn_, nk_, ksplit_, slot_elems_);
     const unsigned blocks = (unsigned)std::min<int64_t>(((int64_t)o_.cap * o_.cap + 255) / 256, 64);
     k_dv_tn_sum<D><<<dim3(blocks, 1, (unsigned)(nslots * nk_)), 256, 0, s_>>>(d_bufs_, d_tn_, nk_, ksplit_,
@@ -1653,10 +1653,10 @@ int KsetSolver<T>::prepare() {
                                       (int)ctl_smem()),
                  "cudaFuncSetAttribute")) ||
       (rc = cuda(cudaFuncSetAttribute((const void*)k_dv_tn<D>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)tiles::tn48_smem_bytes<D>()),
+                                      (int)tiles::tn48m_smem_bytes<D>()),
                  "cudaFuncSetAttribute")) ||
       (rc = cuda(cudaFuncSetAttribute((const void*)k_dv_nn<D>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)tiles::nn64_smem_bytes<D>()),
+                                      (int)tiles::nn64m_smem_bytes<D>()),
                  "cudaFuncSetAttribute")))
     return rc;
   if (ks_->dense) {
