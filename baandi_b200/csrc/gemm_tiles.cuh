@@ -107,23 +107,26 @@ __device__ __forceinline__ void tn_tile(const D* __restrict__ A, int64_t lda, co
 // 48 x 48 tiles of P = A^H B for the Davidson's Grams and the projections (m, n up to the
 // basis capacity or the projector count): the rows stream through shared-memory stages of
 // kBK48 rows each, filled by cp.async ahead of the arithmetic.
-constexpr int kBK48 = 16;
+constexpr int kBK48 = 32;
 
 // tn_tile48_mma: P[j * ldp + i] = sum over rows r0 .. r1 - 1 of conj(A[r][i0 + i]) B[r][j0 + j]
 // for the valid i < m - i0, j < n - j0, with mma.sync m8n8k4 f64 (DMMA) on fragments read
-// from shared memory.  One DMMA does 256 multiply-adds per warp
-// instruction against 32 for DFMA, so the FP64 pipe is no longer held back by issue
-// slots and operand reads.  256 threads = 8 warps: warp w takes the K half g = w / 4 of
-// every 16-row stage (k-steps 2g and 2g + 1 of 4 rows each) and the 24 x 24 output block
-// (wi, wj) = ((w / 2) % 2, w % 2), 3 x 3 MMA tiles of 8 x 8; the two halves' sums meet in
-// shared memory at the end (half 1 stores, half 0 adds and writes P).  A stage holds each
-// column's 16 rows with a pitch of 20 elements, so the fragment reads (8 columns x 4 rows
+// from shared memory.  One DMMA does 256 multiply-adds per warp instruction against 32
+// for DFMA, so the FP64 pipe is no longer held back by issue slots and operand reads.
+// 256 threads = 8 warps: warp w takes the K half g = w / 4 of every 32-row stage (four
+// k-steps of 4 rows each) and the 24 x 24 output block (wi, wj) = ((w / 2) % 2, w % 2),
+// 3 x 3 MMA tiles of 8 x 8; the two halves' sums meet in shared memory at the end (half 1
+// stores, half 0 adds and writes P).  Two stages, double buffered: 32-row stages give each
+// warp four k-steps per barrier (16-row stages with three buffers measured 11.16 against
+// 9.63 ms for the Si216 projection) and still fit two CTAs per SM.  A stage holds each
+// column's 32 rows with a pitch of 36 elements, so the fragment reads (8 columns x 4 rows
 // per warp) meet no bank conflicts for double and double2.  Fragments of m8n8k4 (row.col,
 // f64): A (8 x 4) lane holds (m, k) = (lane / 4, lane % 4); B (4 x 8) (k, n) = (lane % 4,
 // lane / 4); C (8 x 8) (m, n) = (lane / 4, 2 (lane % 4) + e), e = 0, 1.  Complex:
 // Re += ar br + ai bi, Im += ar bi - ai br (four real DMMAs; A^H conjugates A).
-constexpr int kStagesM = 3;
+constexpr int kStagesM = 2;
 constexpr int kPitchM = kBK48 + 4;
+constexpr int kPitchNB = kBK + 4;  // nn_tile64_mma's B columns
 template <class D>
 constexpr size_t tn48m_smem_bytes() {
   return (size_t)2 * kStagesM * 48 * kPitchM * sizeof(D);
@@ -184,10 +187,10 @@ __device__ __forceinline__ void tn_tile48_mma(const D* __restrict__ A, int64_t l
     else
       async_commit();
     if (warp_live) {
-      const D* as = As + (int)(s % kStagesM) * 48 * kPitchM + (24 * wi + fm) * kPitchM + 8 * g + fk;
-      const D* bs = Bs + (int)(s % kStagesM) * 48 * kPitchM + (24 * wj + fm) * kPitchM + 8 * g + fk;
+      const D* as = As + (int)(s % kStagesM) * 48 * kPitchM + (24 * wi + fm) * kPitchM + (kBK48 / 2) * g + fk;
+      const D* bs = Bs + (int)(s % kStagesM) * 48 * kPitchM + (24 * wj + fm) * kPitchM + (kBK48 / 2) * g + fk;
 #pragma unroll
-      for (int kk = 0; kk < 2; ++kk) {
+      for (int kk = 0; kk < kBK48 / 8; ++kk) {
         D a[3], b[3];
 #pragma unroll
         for (int q = 0; q < 3; ++q) {
@@ -350,7 +353,7 @@ __host__ __device__ constexpr int nn_pitch_a() {
 }
 template <class D>
 constexpr size_t nn64m_smem_bytes() {
-  return (size_t)kStages64 * (kBK * nn_pitch_a<D>() + 64 * kPitchM) * sizeof(D);
+  return (size_t)kStages64 * (kBK * nn_pitch_a<D>() + 64 * kPitchNB) * sizeof(D);
 }
 template <class D, bool SKIP_EMPTY = false>
 __device__ __forceinline__ void nn_tile64_mma(const D* __restrict__ A, int64_t lda, const D* __restrict__ B,
@@ -360,7 +363,7 @@ __device__ __forceinline__ void nn_tile64_mma(const D* __restrict__ A, int64_t l
   constexpr int PA = nn_pitch_a<D>();
   extern __shared__ __align__(16) unsigned char nn64_smem[];
   D* As = reinterpret_cast<D*>(nn64_smem);  // [stage][kBK][PA]: 64 rows of A per inner index
-  D* Bs = As + kStages64 * kBK * PA;        // [stage][64 columns][kPitchM]
+  D* Bs = As + kStages64 * kBK * PA;        // [stage][64 columns][kPitchNB]
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int wr = warp & 1, wc = warp >> 1;
   const int fm = lane >> 2, fk = lane & 3;
@@ -374,7 +377,7 @@ __device__ __forceinline__ void nn_tile64_mma(const D* __restrict__ A, int64_t l
       for (int e = 0; e < 2; ++e) cre[x][y][e] = cim[x][y][e] = 0.0;
   auto load = [&](int buf, int pb) {
     D* as = As + buf * kBK * PA;
-    D* bs = Bs + buf * 64 * kPitchM;
+    D* bs = Bs + buf * 64 * kPitchNB;
 #pragma unroll
     for (int q = 0; q < 4; ++q) {  // A: kBK x 64, consecutive threads on consecutive rows
       const int e = tid + 256 * q;
@@ -390,7 +393,7 @@ __device__ __forceinline__ void nn_tile64_mma(const D* __restrict__ A, int64_t l
     for (int q = 0; q < 4; ++q) {  // B: 64 columns x kBK, consecutive threads on consecutive entries
       const int e = tid + 256 * q;
       const int p = e & (kBK - 1), c = e >> 4;
-      D* d = bs + c * kPitchM + p;
+      D* d = bs + c * kPitchNB + p;
       if (pb + p < k && j0 + c < n)
         async_copy(d, B + (int64_t)(j0 + c) * ldb + pb + p);
       else
@@ -416,14 +419,14 @@ __device__ __forceinline__ void nn_tile64_mma(const D* __restrict__ A, int64_t l
       async_commit();
     if (live) {
       const D* as = As + (s % kStages64) * kBK * PA + fk * PA + 32 * wr + fm;
-      const D* bs = Bs + (s % kStages64) * 64 * kPitchM + (16 * wc + fm) * kPitchM + fk;
+      const D* bs = Bs + (s % kStages64) * 64 * kPitchNB + (16 * wc + fm) * kPitchNB + fk;
 #pragma unroll
       for (int kk = 0; kk < kBK / 4; ++kk) {
         D a[4], b[2];
 #pragma unroll
         for (int q = 0; q < 4; ++q) a[q] = as[4 * kk * PA + 8 * q];
 #pragma unroll
-        for (int q = 0; q < 2; ++q) b[q] = bs[8 * q * kPitchM + 4 * kk];
+        for (int q = 0; q < 2; ++q) b[q] = bs[8 * q * kPitchNB + 4 * kk];
 #pragma unroll
         for (int x = 0; x < 4; ++x)
 #pragma unroll
